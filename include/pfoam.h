@@ -1,0 +1,193 @@
+/*
+ * pfoam.h -- C ABI of libpfoam, the B200 (sm_100a) implementation of the
+ * Power Foam rendering hot path.
+ *
+ * Conventions (every entry point):
+ *   - all array arguments are DEVICE pointers, C-contiguous, in the layouts
+ *     stated beside each argument; sizes are int64 element counts;
+ *   - `stream` is a cudaStream_t passed as void* (NULL = legacy stream);
+ *   - nothing is allocated and nothing synchronises with the host: scratch
+ *     memory is passed in by the caller (see the *_workspace_size queries);
+ *   - the return value is a host-side status (PF_OK or PF_ERR_*) covering
+ *     argument validation and launch errors; conditions discovered on the
+ *     device (buffer overflow, walk step cap, ...) are written to a device
+ *     status word the caller reads when it chooses;
+ *   - pf_last_error() describes the last non-zero return on this thread.
+ *
+ * Each entry point names the reference interface it replaces
+ * (file:line inside theialab/powerfoam).
+ */
+#ifndef PFOAM_H
+#define PFOAM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PF_OK 0
+#define PF_ERR_OVERFLOW 1  /* (tile, primitive) pairs exceeded the capacity */
+#define PF_ERR_STEP_CAP 2  /* a cell walk reached max_steps */
+#define PF_ERR_ARGS 3      /* invalid argument */
+#define PF_ERR_CUDA 4      /* CUDA launch / runtime error */
+#define PF_ERR_SEED 5      /* a proposal seed landed outside every cell */
+
+#define PF_ABI_VERSION 1
+
+/* Pinhole camera: powerfoam/camera.py:8-16 (WarpCamera) / :181-189
+ * (TorchCamera).  |up| = tan(vfov/2), |right| = |up| * width / height and the
+ * view direction is normalize(cross(up, right)). */
+typedef struct pf_camera {
+    float eye[3];
+    float right[3];
+    float up[3];
+    int32_t width;
+    int32_t height;
+} pf_camera;
+
+/* Inputs shared by the rasterizer entry points.  Replaces the argument list
+ * of Rasterizer._forward / benchmark / visualize (powerfoam/rasterize.py:
+ * 1587-1603, 1982-1996, 2133-2146) after their torch.cat packing. */
+typedef struct pf_raster_inputs {
+    pf_camera cam;
+    int32_t tile_width;          /* tile edge in pixels (reference: 8) */
+    int32_t n_sites;             /* texel sites per primitive, <= 8 */
+    int64_t n_prims;
+    const float *spheres;        /* (N,4) f32: centre xyz, radius */
+    const void *nsigmas;         /* (N,4): normal xyz, density; f32 or f16 */
+    const void *texel_sites;     /* (N,S,3) f32 or f16 */
+    const void *texel_rgb;       /* (N,S,3) f32 or f16 */
+    const void *texel_height;    /* (N,S)   f32 or f16 */
+    int32_t attr_half;           /* 1: the four arrays above are f16 */
+    const int32_t *adjacency;          /* (E) neighbour ids */
+    const int32_t *adjacency_offsets;  /* (N+1) */
+    const uint16_t *adjacency_diff;    /* (E,4) f16 bits; see each entry */
+    const int64_t *tile_offsets; /* (T+1), T = ceil(H/tw)*ceil(W/tw) */
+    const int32_t *tile_prims;   /* sorted primitive ids per tile */
+    const float *depth_quantiles; /* (H,W,Q) or NULL */
+    int32_t n_quantiles;
+    const float *ray_gt;         /* (H,W,3) or NULL */
+    float transmittance_threshold;
+} pf_raster_inputs;
+
+/* ---------------------------------------------------------------------- */
+int pf_abi_version(void);
+const char *pf_last_error(void);
+
+/* Pack per-primitive attributes into the float4 layouts the kernels read:
+ * spheres = (points, radii), nsigmas = (normals, density).
+ * Replaces the torch.cat calls of rasterize.py:1619-1620. */
+int pf_pack_prims(const float *points, const float *radii, const float *normals, const float *density,
+                  int64_t n_prims, float *spheres, float *nsigmas, void *stream);
+
+/* ---------------------------------------------------------------------- */
+/* Binning.  Replaces rasterize.py:1671-1768: count_visible_pinhole_kernel
+ * (:140-200), torch.cumsum + offsets[-1].item() (:1713-1714),
+ * write_visible_pinhole_kernel (:293-363), the prim_visible_mask scatter
+ * (:1761-1765) and torch.argsort(sort_keys) + gather (:1767-1768).
+ * Order: by tile, then by the float32 bits of |c - eye|^2 - r^2, then by
+ * ascending primitive index (the reference leaves ties unordered).
+ * On overflow (*n_pairs > pair_capacity) the tile lists are emptied and
+ * *status is set to PF_ERR_OVERFLOW; *n_pairs always holds the true count. */
+int pf_bin_workspace_size(int64_t n_prims, int64_t pair_capacity, size_t *bytes);
+int pf_bin(const pf_camera *cam, int32_t tile_width, const float *spheres, int64_t n_prims, void *workspace,
+           size_t workspace_bytes, int64_t pair_capacity, int64_t *tile_offsets, int32_t *tile_prims,
+           int64_t *sort_keys /* (capacity) or NULL */, uint8_t *prim_visible /* (N) or NULL */,
+           int64_t *n_pairs /* device scalar */, int32_t *status /* device scalar */, void *stream);
+
+/* ---------------------------------------------------------------------- */
+/* Neighbour encodings.
+ * pf_adjacency_prefetch: (half(c_j - c_i), half(r_j)); replaces
+ *   prefetch_adjacency_kernel, rasterize.py:580-606.
+ * pf_adjacency_power_diff: (half(c_j - c_i), half(pm_j - pm_i)) with
+ *   pm = (|c|^2 - r^2)/2; replaces benchmark.py:296-302. */
+int pf_adjacency_prefetch(const float *spheres, const int32_t *adjacency, const int32_t *adjacency_offsets,
+                          int64_t n_prims, uint16_t *adjacency_diff, void *stream);
+int pf_adjacency_power_diff(const float *points, const float *radii, const int32_t *adjacency,
+                            const int32_t *adjacency_offsets, int64_t n_prims, uint16_t *adjacency_diff,
+                            void *stream);
+
+/* ---------------------------------------------------------------------- */
+/* Differentiable rasterizer.  Replaces forward_kernel (rasterize.py:892-1146)
+ * and the launch in Rasterizer._forward (:1795-1825).  adjacency_diff is the
+ * pf_adjacency_prefetch encoding; attributes are f32.  Outputs (H,W[,3|Q]):
+ * color, log_t, normal_distance, normal, quantile_depths (-1 where not
+ * reached; NULL if no quantiles); contrib / point_err (N) (point_err may be
+ * NULL); early_stop (T) per-tile stop index used by the backward. */
+int pf_raster_forward(const pf_raster_inputs *in, int32_t return_point_err, float *color, float *log_t,
+                      float *normal_distance, float *normal, float *quantile_depths, float *contrib,
+                      float *point_err, int32_t *early_stop, void *stream);
+
+/* Hand-written adjoint.  Replaces backward_kernel (rasterize.py:1150-1514) and
+ * Rasterizer._backward (:1861-1980): dL/dlog_t = -dL/dopacity * exp(log_t),
+ * gradients zeroed first and non-finite entries zeroed at the end.
+ * grad_normal_distance / grad_normal / grad_quantile_depths / grad_contrib
+ * may be NULL (treated as zero).  Outputs are written, not accumulated. */
+int pf_raster_backward(const pf_raster_inputs *in, const int32_t *early_stop, const float *log_t,
+                       const float *grad_color, const float *grad_opacity, const float *grad_normal_distance,
+                       const float *grad_normal, const float *grad_quantile_depths, const float *grad_contrib,
+                       float *grad_points, float *grad_radii, float *grad_normals, float *grad_density,
+                       float *grad_texel_sites, float *grad_texel_rgb, float *grad_texel_height, void *stream);
+
+/* Forward colour only.  Replaces benchmark_kernel (rasterize.py:614-734) as
+ * launched by Rasterizer.benchmark (:2116-2131): adjacency_diff is the
+ * pf_adjacency_power_diff encoding; attributes f32 or f16. */
+int pf_raster_benchmark(const pf_raster_inputs *in, float *color, void *stream);
+
+/* Viewer path, headless.  Replaces visualization_kernel (rasterize.py:738-888)
+ * as launched by Rasterizer.visualize (:2133-2285). */
+int pf_raster_visualize(const pf_raster_inputs *in, int32_t max_intersections, float depth_quantile,
+                        float bkgd_r, float bkgd_g, float bkgd_b, float *color, float *depth, float *normal,
+                        float *alpha, int32_t *intersections, void *stream);
+
+/* ---------------------------------------------------------------------- */
+/* Cell-walk ray tracer.  Replaces benchmark_kernel (powerfoam/raytrace.py:
+ * 115-241) launched by RayTracer.benchmark (:247-309).  Adds: per-ray start
+ * cells (start_cells, NULL = every ray starts at start_idx), a step cap
+ * (PF_ERR_STEP_CAP in *status), depth / normal / log_t outputs and an
+ * optional visited-cell log (visit_cap entries per ray, -1 padded). */
+typedef struct pf_trace_inputs {
+    pf_camera cam;
+    int32_t n_sites;
+    int32_t attr_half;
+    int64_t n_prims;
+    const float *spheres;
+    const void *nsigmas;
+    const void *texel_sites;
+    const void *texel_rgb;
+    const void *texel_height;
+    const int32_t *adjacency;
+    const int32_t *adjacency_offsets;
+    const uint16_t *adjacency_diff;   /* pf_adjacency_power_diff encoding */
+    int32_t start_idx;
+    const int32_t *start_cells;       /* (H*W) or NULL */
+    float transmittance_threshold;
+    int32_t max_steps;
+    float depth_quantile;
+} pf_trace_inputs;
+
+int pf_trace_forward(const pf_trace_inputs *in, float *color, float *log_t, float *depth, float *normal,
+                     int32_t *depth_seg, float *depth_sigma, int32_t *visit_log, int32_t visit_cap,
+                     int32_t *visit_count, int32_t *status, void *stream);
+
+/* Start cell of benchmark.py:320-324: argmin_i |p_i - eye|^2 - r_i^2 (first
+ * index on ties).  workspace: pf_start_cell_workspace_size bytes. */
+int pf_start_cell_workspace_size(int64_t n_prims, size_t *bytes);
+int pf_start_cell(const float *points, const float *radii, int64_t n_prims, const float *eye_host,
+                  void *workspace, size_t workspace_bytes, int32_t *out_idx, void *stream);
+
+/* ---------------------------------------------------------------------- */
+/* Texel colour pre-step for the synthetic scenes: degree-3 real SH (16
+ * coefficients per channel, constants of powerfoam/sh_utils.py:4-50) at
+ * normalize(p - eye), + 0.5, clamped at 0, broadcast to the S sites.
+ * Stands where the reference evaluates its per-view colour function
+ * (scene.py:331-335 / benchmark.py:390-399). */
+int pf_sh_texel_rgb(const float *points, const float *sh /* (N,16,3) */, int64_t n_prims, int32_t n_sites,
+                    const float *eye_host, float *texel_rgb, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PFOAM_H */
