@@ -1,0 +1,378 @@
+"""Benchmark: differentiable rasterizer forward + backward at 1M primitives 1080p.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (one step = one training iteration of the rendering path on one
+view): 1,048,576 primitives drawn from a 32-component Gaussian mixture
+(sigma 0.15) plus 10 % uniform background, r log-uniform in [0.002, 0.02],
+degree-3 SH colours; one 1920x1080 pinhole camera with a 50 degree vertical
+field of view on a radius-3 orbit; the step evaluates the per-view texel
+colours, rasterizes (pack, bin, neighbour encoding, composite), takes an L2
+loss against a seeded uniform target image and runs the adjoint to gradients
+of every primitive attribute.  Data are synthetic (seeded); the scene (256 MB
+of primitive attributes) is larger than L2, so no flush is needed.
+
+With N > 1 (torchrun, one process per GPU, NCCL) every rank renders its own
+view of the same scene and the per-primitive gradients are summed across ranks
+with one NCCL all-reduce per step (data-parallel over views): weak scaling.
+
+--impl reference times the reference algorithm on the host cores: the CPU
+restatement of the reference kernels (oracle/, OpenMP), on a bounded sample of
+the same frame (binning of every primitive plus compositing forward + adjoint
+of a random sample of tiles), scaled to frames/s.
+"""
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+import torch  # noqa: E402
+
+METRIC = "fwd+bwd ms/iter, FPS @1M prims 1080p; proposal vs plain trace @≥50dB PSNR"
+UNIT = "frames/s (fwd+bwd iterations/s)"
+WORKLOAD = "raster1m"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--tile", type=int, default=8)
+    p.add_argument("--cpu-sample-tiles", type=int, default=0, help="tiles composited by the CPU baseline")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+def load_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:  # noqa: BLE001
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:  # noqa: BLE001
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:  # noqa: BLE001
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for nme, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nme)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ----------------------------------------------------------------------------
+def build_workload(device, seed_offset=0, tile=8):
+    from powerfoam_b200 import synthetic
+    from powerfoam_b200.adjacency import CechBuilder
+
+    cfg = synthetic.CONFIGS[WORKLOAD]
+    scene = synthetic.make_scene(cfg["n"], seed=cfg["seed"], mixture=cfg["mixture"], sigma=cfg["sigma"],
+                                 r_range=cfg["r_range"], device=device)
+    cam = synthetic.orbit_camera(100 + seed_offset, cfg["width"], cfg["height"], cfg["vfov"], device=device)
+    adj, adj_off = CechBuilder(device)(scene["points"], scene["radii"])
+    g = torch.Generator().manual_seed(200 + seed_offset)
+    target = torch.rand((cfg["height"], cfg["width"], 3), generator=g)
+    return cfg, scene, cam, adj, adj_off, target
+
+
+class Args:
+    is_pinhole = True
+    render_objective = "volume"
+    num_texel_sites = 8
+
+
+def make_step(R, scene, cam, adj, adj_off, target_dev, world):
+    from powerfoam_b200 import synthetic
+
+    names = ["points", "radii", "density", "normals", "texel_sites", "texel_height"]
+    params = {k: scene[k].clone().requires_grad_(True) for k in names}
+
+    def step(target=None):
+        t = target_dev if target is None else target
+        for p in params.values():
+            p.grad = None
+        rgb = synthetic.texel_rgb(scene, cam).requires_grad_(True)
+        out = R.forward(cam, None, params["points"], params["radii"], params["density"], params["normals"],
+                        params["texel_sites"], rgb, params["texel_height"], adj, adj_off, None, False)
+        loss = ((out[0] - t) ** 2).sum()
+        loss.backward()
+        if world > 1:
+            grads = [params[k].grad.reshape(-1) for k in names] + [rgb.grad.reshape(-1)]
+            flat = torch.cat(grads)
+            torch.distributed.all_reduce(flat)
+        return loss
+
+    return step, params
+
+
+def algorithmic_bytes(stats, H, W):
+    """Per-launch algorithmic HBM bytes of the compositing forward and adjoint
+    (the per-unit figures: 256 B of primitive record per visited (tile, prim)
+    pair, 8 B per neighbour face record, 4 B per list entry; per pixel 32 B of
+    forward outputs and 36 B of adjoint inputs; 2 x 256 B read-modify-write of
+    the gradient record per pair with a contributing pixel)."""
+    bins = stats["bins"]
+    es = stats["early_stop"].long()
+    offs = bins.tile_offsets
+    T = es.shape[0]
+    lens = offs[1:] - offs[:-1]
+    tile_of = torch.repeat_interleave(torch.arange(T, device=offs.device), lens)
+    pos = torch.arange(bins.n_pairs, device=offs.device) - offs[:-1][tile_of]
+    visited = pos < es[tile_of]
+    prims = bins.tile_prims.long()[visited]
+    ao = stats["adjacency_offsets"].long()
+    deg = (ao[prims + 1] - ao[prims]).sum().item()
+    V = int(visited.sum().item())
+    U = int(stats["contrib_pairs"].long().sum().item())
+    N = stats["n_prims"]
+    fwd = 256 * V + 8 * deg + 4 * V + 8 * (T + 1) + 32 * H * W + 4 * N
+    bwd = 256 * V + 8 * deg + 4 * V + 36 * H * W + 2 * 256 * U
+    return dict(fwd=fwd, bwd=bwd, V=V, U=U, deg=deg, pairs=bins.n_pairs, T=T)
+
+
+def cpu_baseline(cfg, scene, cam, adj, adj_off, target, sample_tiles, tile=8):
+    """The oracle (CPU restatement, OpenMP) on a bounded sample of the frame:
+    binning of every primitive + forward/adjoint compositing of a random
+    sample of tiles; returns frames/s scaled to the whole frame."""
+    from oracle import oracle as orc
+    from powerfoam_b200 import synthetic
+
+    rgb = synthetic.texel_rgb(scene, cam).cpu().numpy()
+    sc = {k: v.cpu().numpy() for k, v in scene.items()}
+    adj_np, off_np = adj.cpu().numpy(), adj_off.cpu().numpy()
+    oc = orc.camera(cam.eye.cpu().numpy(), cam.right.cpu().numpy(), cam.up.cpu().numpy(), cam.width, cam.height)
+    sph = np.concatenate([sc["points"], sc["radii"][:, None]], -1).astype(np.float32)
+    nsig = np.concatenate([sc["normals"], sc["density"][:, None]], -1).astype(np.float32)
+    rgbh = np.concatenate([rgb, sc["texel_height"][..., None]], -1).astype(np.float32)
+    t0 = time.perf_counter()
+    keys, prims, offs, _ = orc.bin(oc, sph, tile)
+    ad = orc.prefetch_adjacency(sph, adj_np, off_np)
+    t_bin = time.perf_counter() - t0
+    T = offs.shape[0] - 1
+    rng = np.random.default_rng(0)
+    sample = np.sort(rng.choice(T, size=min(sample_tiles, T), replace=False))
+    new_prims = np.concatenate([prims[offs[t]:offs[t + 1]] for t in sample]) if len(sample) else prims[:0]
+    lens = np.zeros(T, np.int64)
+    lens[sample] = offs[sample + 1] - offs[sample]
+    new_offs = np.concatenate([[0], np.cumsum(lens)]).astype(np.int64)
+    t1 = time.perf_counter()
+    o = orc.raster_forward(oc, tile, sph, nsig, sc["texel_sites"], rgbh, adj_np, off_np, ad, new_offs, new_prims)
+    g_c = (2 * (o["color"] - target.numpy())).astype(np.float32)
+    z = np.zeros_like(o["log_t"])
+    orc.raster_backward(oc, tile, sph, nsig, sc["texel_sites"], rgbh, adj_np, off_np, ad, new_offs, new_prims,
+                        o["early_stop"], o["log_t"], g_c, z, z, np.zeros_like(o["normal"]),
+                        np.zeros(sph.shape[0], np.float32))
+    t_comp = time.perf_counter() - t1
+    t_frame = t_bin + t_comp * T / max(len(sample), 1)
+    return dict(value=1.0 / t_frame, unit=UNIT, cores=orc.num_threads(), kind="port",
+                sample=(f"oracle binning of all {sph.shape[0]} prims ({t_bin:.2f}s) + forward/adjoint of "
+                        f"{len(sample)}/{T} random tiles ({t_comp:.2f}s), scaled to the full frame"))
+
+
+def reference_arm(args, rank, world):
+    if rank != 0:
+        return
+    from oracle import oracle as orc
+
+    orc.build()
+    dev = "cuda" if torch.cuda.is_available() else "cpu"
+    cfg, scene, cam, adj, adj_off, target = build_workload(dev, 0, args.tile)
+    sample = args.cpu_sample_tiles or 200
+    for _ in range(args.warmup):
+        cpu_baseline(cfg, scene, cam, adj, adj_off, target, max(sample // 10, 1), args.tile)
+    vals = [cpu_baseline(cfg, scene, cam, adj, adj_off, target, sample, args.tile) for _ in range(args.steps)]
+    v = statistics.median([x["value"] for x in vals])
+    cb = dict(vals[-1])
+    cb["value"] = v
+    line = dict(metric=METRIC, value=v, unit=UNIT, n_gpus=world, steps=args.steps, warmup=args.warmup,
+                ms_per_step=1000.0 / v, higher_is_better=True, scaling="weak", vs_baseline=None, dtype="f32",
+                data="synthetic", impl="reference",
+                config=dict(workload=WORKLOAD, prims=cfg["n"], width=cfg["width"], height=cfg["height"],
+                            tile=args.tile, parallelism="cpu-openmp"),
+                cpu_baseline=cb, e2e=dict(value=v, unit=UNIT, h2d_bytes_per_step=0, d2h_bytes_per_step=0))
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        reference_arm(args, rank, world)
+        return
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
+    from powerfoam_b200 import rasterize
+
+    cfg, scene, cam, adj, adj_off, target = build_workload(dev, rank, args.tile)
+    target_dev = target.to(dev)
+    R = rasterize.Rasterizer(Args(), dev, tile_width=args.tile)
+    step, params = make_step(R, scene, cam, adj, adj_off, target_dev, world)
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    barrier()
+
+    # per-call device times of the compositing kernels, recorded live
+    events = {"pf_raster_forward": [], "pf_raster_backward": []}
+    pending = {}
+
+    def hook(name, phase):
+        e = torch.cuda.Event(enable_timing=True)
+        e.record()
+        if phase == "begin":
+            pending[name] = e
+        else:
+            events[name].append((pending.pop(name), e))
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    barrier()
+    rasterize.PROFILE_HOOK = hook
+    start = torch.cuda.Event(enable_timing=True)
+    end = torch.cuda.Event(enable_timing=True)
+    start.record()
+    for _ in range(args.steps):
+        loss = step()
+    end.record()
+    barrier()
+    rasterize.PROFILE_HOOK = None
+    clk = clocks.stop()
+    ms = start.elapsed_time(end) / args.steps
+    if world > 1:
+        t = torch.tensor([ms], device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * 1000.0 / ms
+    fwd_ms = statistics.mean(a.elapsed_time(b) for a, b in events["pf_raster_forward"])
+    bwd_ms = statistics.mean(a.elapsed_time(b) for a, b in events["pf_raster_backward"])
+
+    # end to end through the public API: host target image in, loss out
+    target_host = target.pin_memory()
+    loss_host = torch.empty(args.steps, dtype=torch.float32).pin_memory()
+    t_dev = torch.empty_like(target_dev)
+    barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for i in range(args.steps):
+        t_dev.copy_(target_host, non_blocking=True)
+        loss = step(t_dev)
+        loss_host[i].copy_(loss.detach(), non_blocking=True)
+    e1.record()
+    barrier()
+    e2e_ms = e0.elapsed_time(e1) / args.steps
+    if world > 1:
+        t = torch.tensor([e2e_ms], device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+
+    # statistics of one step for the roofline (outside the timed regions)
+    R.collect_stats = True
+    step()
+    torch.cuda.synchronize()
+    st = algorithmic_bytes(R.last_stats, cfg["height"], cfg["width"])
+    R.collect_stats = False
+    peak, peak_kind = load_peaks()
+    dominant = "pf_raster_backward" if bwd_ms >= fwd_ms else "pf_raster_forward"
+    dom_ms = max(bwd_ms, fwd_ms)
+    dom_bytes = st["bwd"] if dominant == "pf_raster_backward" else st["fwd"]
+    achieved = dom_bytes / (dom_ms * 1e-3) / 1e9
+
+    line = dict(metric=METRIC, value=value, unit=UNIT, n_gpus=world, steps=args.steps, warmup=max(args.warmup, 3),
+                ms_per_step=ms, higher_is_better=True, scaling="weak", vs_baseline=None, dtype="f32",
+                data="synthetic (seeded scene, orbit camera, uniform target)",
+                config=dict(workload=WORKLOAD, prims=cfg["n"], width=cfg["width"], height=cfg["height"],
+                            tile=args.tile, vfov=cfg["vfov"], pairs=st["pairs"], visited_pairs=st["V"],
+                            l2="inputs larger than L2 (256 MB of primitive records), no flush",
+                            parallelism=f"view-dp{world}"),
+                clocks=clk,
+                e2e=dict(value=world * 1000.0 / e2e_ms, unit=UNIT, h2d_bytes_per_step=target.numel() * 4,
+                         d2h_bytes_per_step=4),
+                roofline=dict(bound="hbm", kernel=dominant, achieved=achieved, peak=peak, unit="GB/s",
+                              frac=achieved / peak, peak_source=peak_kind, traffic=None,
+                              algorithmic_bytes=dom_bytes, ms=dom_ms, fwd_ms=fwd_ms, bwd_ms=bwd_ms),
+                gpu_launches=None)
+    # kernels per step: pack 1, bin 31 (+3 per extra tile-sort pass), prefetch 1, SH 1, forward 1,
+    # backward 1 + 7 sanitise
+    T = st["T"]
+    tile_passes = max(0, (int(T - 1).bit_length() + 7) // 8)
+    bin_k = 1 + 4 * 5 + 1 + 3 + 1 + tile_passes * 5 + 1
+    line["gpu_launches"] = args.steps * (1 + bin_k + 1 + 1 + 1 + 1 + 7)
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(cfg, scene, cam, adj, adj_off, target, args.cpu_sample_tiles or 200,
+                                            args.tile)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -36,6 +36,12 @@ extern "C" {
 
 #define PF_ABI_VERSION 1
 
+#if defined(__GNUC__)
+#define PF_API __attribute__((visibility("default")))
+#else
+#define PF_API
+#endif
+
 /* Pinhole camera: powerfoam/camera.py:8-16 (WarpCamera) / :181-189
  * (TorchCamera).  |up| = tan(vfov/2), |right| = |up| * width / height and the
  * view direction is normalize(cross(up, right)). */
@@ -73,13 +79,13 @@ typedef struct pf_raster_inputs {
 } pf_raster_inputs;
 
 /* ---------------------------------------------------------------------- */
-int pf_abi_version(void);
-const char *pf_last_error(void);
+PF_API int pf_abi_version(void);
+PF_API const char *pf_last_error(void);
 
 /* Pack per-primitive attributes into the float4 layouts the kernels read:
  * spheres = (points, radii), nsigmas = (normals, density).
  * Replaces the torch.cat calls of rasterize.py:1619-1620. */
-int pf_pack_prims(const float *points, const float *radii, const float *normals, const float *density,
+PF_API int pf_pack_prims(const float *points, const float *radii, const float *normals, const float *density,
                   int64_t n_prims, float *spheres, float *nsigmas, void *stream);
 
 /* ---------------------------------------------------------------------- */
@@ -91,8 +97,8 @@ int pf_pack_prims(const float *points, const float *radii, const float *normals,
  * ascending primitive index (the reference leaves ties unordered).
  * On overflow (*n_pairs > pair_capacity) the tile lists are emptied and
  * *status is set to PF_ERR_OVERFLOW; *n_pairs always holds the true count. */
-int pf_bin_workspace_size(int64_t n_prims, int64_t pair_capacity, size_t *bytes);
-int pf_bin(const pf_camera *cam, int32_t tile_width, const float *spheres, int64_t n_prims, void *workspace,
+PF_API int pf_bin_workspace_size(int64_t n_prims, int64_t pair_capacity, size_t *bytes);
+PF_API int pf_bin(const pf_camera *cam, int32_t tile_width, const float *spheres, int64_t n_prims, void *workspace,
            size_t workspace_bytes, int64_t pair_capacity, int64_t *tile_offsets, int32_t *tile_prims,
            int64_t *sort_keys /* (capacity) or NULL */, uint8_t *prim_visible /* (N) or NULL */,
            int64_t *n_pairs /* device scalar */, int32_t *status /* device scalar */, void *stream);
@@ -103,29 +109,51 @@ int pf_bin(const pf_camera *cam, int32_t tile_width, const float *spheres, int64
  *   prefetch_adjacency_kernel, rasterize.py:580-606.
  * pf_adjacency_power_diff: (half(c_j - c_i), half(pm_j - pm_i)) with
  *   pm = (|c|^2 - r^2)/2; replaces benchmark.py:296-302. */
-int pf_adjacency_prefetch(const float *spheres, const int32_t *adjacency, const int32_t *adjacency_offsets,
+PF_API int pf_adjacency_prefetch(const float *spheres, const int32_t *adjacency, const int32_t *adjacency_offsets,
                           int64_t n_prims, uint16_t *adjacency_diff, void *stream);
-int pf_adjacency_power_diff(const float *points, const float *radii, const int32_t *adjacency,
+PF_API int pf_adjacency_power_diff(const float *points, const float *radii, const int32_t *adjacency,
                             const int32_t *adjacency_offsets, int64_t n_prims, uint16_t *adjacency_diff,
                             void *stream);
+
+/* Čech adjacency: j is a neighbour of i iff their AABBs overlap and
+ * |c_i - c_j| < r_i + r_j with c, r recovered from the AABB.  Replaces
+ * AABBTree.update + build_cech_complex (powerfoam/bvh.py:72-123, Warp BVH
+ * query kernels :7-69); lists are in ascending neighbour order.  As for
+ * binning, *n_edges always receives the true count and on overflow
+ * (*n_edges > edge_capacity) the offsets are zeroed and *status is set to
+ * PF_ERR_OVERFLOW. */
+PF_API int pf_cech_workspace_size(int64_t n_prims, size_t *bytes);
+PF_API int pf_cech_adjacency(const float *points, const float *radii, int64_t n_prims, void *workspace,
+                             size_t workspace_bytes, int64_t edge_capacity, int32_t *adjacency /* (capacity) */,
+                             int32_t *adjacency_offsets /* (N+1) */, int64_t *n_edges /* device */,
+                             int32_t *status /* device */, void *stream);
+
+/* Morton order of the primitives (stable on equal codes).  Replaces
+ * morton_sort (powerfoam/geometry.py:7-85, Warp radix_sort_pairs). */
+PF_API int pf_morton_workspace_size(int64_t n_prims, size_t *bytes);
+PF_API int pf_morton_sort(const float *points, int64_t n_prims, void *workspace, size_t workspace_bytes,
+                          int32_t *permutation, void *stream);
 
 /* ---------------------------------------------------------------------- */
 /* Differentiable rasterizer.  Replaces forward_kernel (rasterize.py:892-1146)
  * and the launch in Rasterizer._forward (:1795-1825).  adjacency_diff is the
  * pf_adjacency_prefetch encoding; attributes are f32.  Outputs (H,W[,3|Q]):
  * color, log_t, normal_distance, normal, quantile_depths (-1 where not
- * reached; NULL if no quantiles); contrib / point_err (N) (point_err may be
- * NULL); early_stop (T) per-tile stop index used by the backward. */
-int pf_raster_forward(const pf_raster_inputs *in, int32_t return_point_err, float *color, float *log_t,
-                      float *normal_distance, float *normal, float *quantile_depths, float *contrib,
-                      float *point_err, int32_t *early_stop, void *stream);
+ * reached; NULL if no quantiles), err (the "surface" objective's per-pixel
+ * expected squared error, rasterize.py:1076-1079, 1138-1141; NULL to skip);
+ * contrib / point_err (N) (point_err may be NULL); early_stop (T) per-tile
+ * stop index used by the backward; tile_contrib_pairs (T, optional) counts
+ * the (tile, primitive) pairs in which at least one pixel composited. */
+PF_API int pf_raster_forward(const pf_raster_inputs *in, int32_t return_point_err, float *color, float *log_t,
+                      float *normal_distance, float *normal, float *quantile_depths, float *err, float *contrib,
+                      float *point_err, int32_t *early_stop, int32_t *tile_contrib_pairs, void *stream);
 
 /* Hand-written adjoint.  Replaces backward_kernel (rasterize.py:1150-1514) and
  * Rasterizer._backward (:1861-1980): dL/dlog_t = -dL/dopacity * exp(log_t),
  * gradients zeroed first and non-finite entries zeroed at the end.
  * grad_normal_distance / grad_normal / grad_quantile_depths / grad_contrib
  * may be NULL (treated as zero).  Outputs are written, not accumulated. */
-int pf_raster_backward(const pf_raster_inputs *in, const int32_t *early_stop, const float *log_t,
+PF_API int pf_raster_backward(const pf_raster_inputs *in, const int32_t *early_stop, const float *log_t,
                        const float *grad_color, const float *grad_opacity, const float *grad_normal_distance,
                        const float *grad_normal, const float *grad_quantile_depths, const float *grad_contrib,
                        float *grad_points, float *grad_radii, float *grad_normals, float *grad_density,
@@ -134,11 +162,11 @@ int pf_raster_backward(const pf_raster_inputs *in, const int32_t *early_stop, co
 /* Forward colour only.  Replaces benchmark_kernel (rasterize.py:614-734) as
  * launched by Rasterizer.benchmark (:2116-2131): adjacency_diff is the
  * pf_adjacency_power_diff encoding; attributes f32 or f16. */
-int pf_raster_benchmark(const pf_raster_inputs *in, float *color, void *stream);
+PF_API int pf_raster_benchmark(const pf_raster_inputs *in, float *color, void *stream);
 
 /* Viewer path, headless.  Replaces visualization_kernel (rasterize.py:738-888)
  * as launched by Rasterizer.visualize (:2133-2285). */
-int pf_raster_visualize(const pf_raster_inputs *in, int32_t max_intersections, float depth_quantile,
+PF_API int pf_raster_visualize(const pf_raster_inputs *in, int32_t max_intersections, float depth_quantile,
                         float bkgd_r, float bkgd_g, float bkgd_b, float *color, float *depth, float *normal,
                         float *alpha, int32_t *intersections, void *stream);
 
@@ -168,14 +196,14 @@ typedef struct pf_trace_inputs {
     float depth_quantile;
 } pf_trace_inputs;
 
-int pf_trace_forward(const pf_trace_inputs *in, float *color, float *log_t, float *depth, float *normal,
+PF_API int pf_trace_forward(const pf_trace_inputs *in, float *color, float *log_t, float *depth, float *normal,
                      int32_t *depth_seg, float *depth_sigma, int32_t *visit_log, int32_t visit_cap,
                      int32_t *visit_count, int32_t *status, void *stream);
 
 /* Start cell of benchmark.py:320-324: argmin_i |p_i - eye|^2 - r_i^2 (first
  * index on ties).  workspace: pf_start_cell_workspace_size bytes. */
-int pf_start_cell_workspace_size(int64_t n_prims, size_t *bytes);
-int pf_start_cell(const float *points, const float *radii, int64_t n_prims, const float *eye_host,
+PF_API int pf_start_cell_workspace_size(int64_t n_prims, size_t *bytes);
+PF_API int pf_start_cell(const float *points, const float *radii, int64_t n_prims, const float *eye_host,
                   void *workspace, size_t workspace_bytes, int32_t *out_idx, void *stream);
 
 /* ---------------------------------------------------------------------- */
@@ -184,7 +212,7 @@ int pf_start_cell(const float *points, const float *radii, int64_t n_prims, cons
  * normalize(p - eye), + 0.5, clamped at 0, broadcast to the S sites.
  * Stands where the reference evaluates its per-view colour function
  * (scene.py:331-335 / benchmark.py:390-399). */
-int pf_sh_texel_rgb(const float *points, const float *sh /* (N,16,3) */, int64_t n_prims, int32_t n_sites,
+PF_API int pf_sh_texel_rgb(const float *points, const float *sh /* (N,16,3) */, int64_t n_prims, int32_t n_sites,
                     const float *eye_host, float *texel_rgb, void *stream);
 
 #ifdef __cplusplus

@@ -112,7 +112,8 @@ def power_adjacency_diff(points, radii, adj, adj_off):
 
 
 def raster_forward(cam, tile_width, spheres, nsigmas, sites, rgbh, adj, adj_off, adj_diff, tile_offsets,
-                   tile_prims, depth_q=None, ray_gt=None, thr=1e-3, return_point_err=False, prec="f32"):
+                   tile_prims, depth_q=None, ray_gt=None, thr=1e-3, return_point_err=False, surface=False,
+                   prec="f32"):
     N = spheres.shape[0]
     S = sites.shape[1]
     H, W = cam.height, cam.width
@@ -124,12 +125,13 @@ def raster_forward(cam, tile_width, spheres, nsigmas, sites, rgbh, adj, adj_off,
     gt = None if ray_gt is None else _c(ray_gt, F32)
     out = dict(color=np.zeros((H, W, 3), F32), log_t=np.zeros((H, W), F32), normal_distance=np.zeros((H, W), F32),
                normal=np.zeros((H, W, 3), F32), quantile_depths=-np.ones((H, W, max(Q, 1)), F32),
-               contrib=np.zeros(N, F32), point_err=np.zeros(N, F32), early_stop=np.zeros(T, np.int32))
+               contrib=np.zeros(N, F32), point_err=np.zeros(N, F32), early_stop=np.zeros(T, np.int32),
+               err=np.zeros((H, W), F32) if surface else None)
     rc = _fn("orc_raster_forward", prec)(
         ctypes.byref(cam), ctypes.c_int(tile_width), ctypes.c_int64(N), *[_p(a) for a in args[:4]], ctypes.c_int(S),
         *[_p(a) for a in args[4:]], _p(dq), ctypes.c_int(Q), _p(gt), ctypes.c_float(thr),
         ctypes.c_int(int(return_point_err)), _p(out["color"]), _p(out["log_t"]), _p(out["normal_distance"]),
-        _p(out["normal"]), _p(out["quantile_depths"]), _p(out["contrib"]), _p(out["point_err"]),
+        _p(out["normal"]), _p(out["quantile_depths"]), _p(out["err"]), _p(out["contrib"]), _p(out["point_err"]),
         _p(out["early_stop"]))
     assert rc == 0
     if Q == 0:

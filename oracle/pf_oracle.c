@@ -658,7 +658,7 @@ static void plane_bwd(v3 o, v3 d, real _t_near, v3 po, v3 pn, real radius, int h
 typedef struct {
     v3 d;
     int oob, pi, pj;
-    real log_t, nd;
+    real log_t, nd, err;
     v3 rgb, normal;
     int qi;
     real q;
@@ -685,7 +685,7 @@ int FN(orc_raster_forward)(const orc_camera *camera, int TW, int64_t N, const fl
                            const int64_t *tile_offsets, const int32_t *tile_prims, const float *depth_q,
                            int Q, const float *ray_gt, float thr, int return_point_err, float *color,
                            float *log_t_out, float *nd_out, float *normal_out, float *qdepth_out,
-                           float *contrib, float *point_err, int32_t *early_stop) {
+                           float *err_out, float *contrib, float *point_err, int32_t *early_stop) {
     (void)N; (void)adj;
     cam_t cam = cam_load(camera);
     int tiles_h = 1 + (cam.H - 1) / TW, tiles_w = 1 + (cam.W - 1) / TW;
@@ -702,7 +702,8 @@ int FN(orc_raster_forward)(const orc_camera *camera, int TW, int64_t N, const fl
             a->log_t = 0; a->nd = 0; a->rgb = mk(0, 0, 0); a->normal = mk(0, 0, 0);
             int64_t px = (int64_t)a->pi * cam.W + a->pj;
             if (depth_q) { a->qi = 0; a->q = (real)depth_q[px * Q + 0]; } else { a->qi = 0; a->q = 0; }
-            if (return_point_err) a->gt = ld3(ray_gt + 3 * px);
+            a->err = 0;
+            if (return_point_err || err_out) a->gt = ld3(ray_gt + 3 * px);
         }
         int nq = depth_q ? Q : 0;
         int64_t start = tile_offsets[tile], end = tile_offsets[tile + 1];
@@ -752,6 +753,10 @@ int FN(orc_raster_forward)(const orc_camera *camera, int TW, int64_t N, const fl
                     real dlt = -sigma * dt;
                     real alpha = K(1.0) - r_exp(dlt);
                     real trans = r_exp(a->log_t);
+                    if (err_out) {
+                        v3 de = vsub(pr.rgb, a->gt);
+                        a->err += dot(de, de) * alpha * trans;
+                    }
                     a->rgb = vadd(a->rgb, smul(trans, smul(alpha, pr.rgb)));
                     a->log_t += dlt;
                     ATOMIC_ADD(contrib[prim], alpha * trans / HW);
@@ -787,6 +792,10 @@ int FN(orc_raster_forward)(const orc_camera *camera, int TW, int64_t N, const fl
             normal_out[3 * px + 0] = (float)a->normal.x;
             normal_out[3 * px + 1] = (float)a->normal.y;
             normal_out[3 * px + 2] = (float)a->normal.z;
+            if (err_out) {
+                v3 de = vsub(mk(0, 0, 0), a->gt);
+                err_out[px] = (float)(a->err + dot(de, de) * r_exp(a->log_t));
+            }
         }
         free(L);
     }

@@ -1,0 +1,183 @@
+"""ctypes binding of libpfoam (include/pfoam.h).
+
+The library is the only compute path: if it is missing or fails to load, every
+operation raises.  Tensors cross the boundary as raw device pointers; the
+current torch stream is passed as the cudaStream_t.
+"""
+
+import ctypes
+import os
+
+import torch
+
+from . import build as _build
+
+LIB_PATH = _build.LIB_PATH
+
+PF_OK = 0
+PF_ERR_OVERFLOW = 1
+PF_ERR_STEP_CAP = 2
+PF_ERR_ARGS = 3
+PF_ERR_CUDA = 4
+PF_ERR_SEED = 5
+
+_ERR_NAMES = {
+    PF_ERR_OVERFLOW: "PF_ERR_OVERFLOW",
+    PF_ERR_STEP_CAP: "PF_ERR_STEP_CAP",
+    PF_ERR_ARGS: "PF_ERR_ARGS",
+    PF_ERR_CUDA: "PF_ERR_CUDA",
+    PF_ERR_SEED: "PF_ERR_SEED",
+}
+
+c_f = ctypes.c_float
+c_i32 = ctypes.c_int32
+c_i64 = ctypes.c_int64
+c_vp = ctypes.c_void_p
+
+
+class PfCamera(ctypes.Structure):
+    _fields_ = [("eye", c_f * 3), ("right", c_f * 3), ("up", c_f * 3), ("width", c_i32), ("height", c_i32)]
+
+
+class PfRasterInputs(ctypes.Structure):
+    _fields_ = [
+        ("cam", PfCamera),
+        ("tile_width", c_i32),
+        ("n_sites", c_i32),
+        ("n_prims", c_i64),
+        ("spheres", c_vp),
+        ("nsigmas", c_vp),
+        ("texel_sites", c_vp),
+        ("texel_rgb", c_vp),
+        ("texel_height", c_vp),
+        ("attr_half", c_i32),
+        ("adjacency", c_vp),
+        ("adjacency_offsets", c_vp),
+        ("adjacency_diff", c_vp),
+        ("tile_offsets", c_vp),
+        ("tile_prims", c_vp),
+        ("depth_quantiles", c_vp),
+        ("n_quantiles", c_i32),
+        ("ray_gt", c_vp),
+        ("transmittance_threshold", c_f),
+    ]
+
+
+class PfTraceInputs(ctypes.Structure):
+    _fields_ = [
+        ("cam", PfCamera),
+        ("n_sites", c_i32),
+        ("attr_half", c_i32),
+        ("n_prims", c_i64),
+        ("spheres", c_vp),
+        ("nsigmas", c_vp),
+        ("texel_sites", c_vp),
+        ("texel_rgb", c_vp),
+        ("texel_height", c_vp),
+        ("adjacency", c_vp),
+        ("adjacency_offsets", c_vp),
+        ("adjacency_diff", c_vp),
+        ("start_idx", c_i32),
+        ("start_cells", c_vp),
+        ("transmittance_threshold", c_f),
+        ("max_steps", c_i32),
+        ("depth_quantile", c_f),
+    ]
+
+
+# name -> argtypes (all return int)
+_SIGS = {
+    "pf_abi_version": [],
+    "pf_pack_prims": [c_vp, c_vp, c_vp, c_vp, c_i64, c_vp, c_vp, c_vp],
+    "pf_bin_workspace_size": [c_i64, c_i64, ctypes.POINTER(ctypes.c_size_t)],
+    "pf_bin": [ctypes.POINTER(PfCamera), c_i32, c_vp, c_i64, c_vp, ctypes.c_size_t, c_i64, c_vp, c_vp, c_vp, c_vp,
+               c_vp, c_vp, c_vp],
+    "pf_adjacency_prefetch": [c_vp, c_vp, c_vp, c_i64, c_vp, c_vp],
+    "pf_adjacency_power_diff": [c_vp, c_vp, c_vp, c_vp, c_i64, c_vp, c_vp],
+    "pf_raster_forward": [ctypes.POINTER(PfRasterInputs), c_i32, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp,
+                          c_vp, c_vp, c_vp],
+    "pf_raster_backward": [ctypes.POINTER(PfRasterInputs), c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp,
+                           c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp],
+    "pf_raster_benchmark": [ctypes.POINTER(PfRasterInputs), c_vp, c_vp],
+    "pf_raster_visualize": [ctypes.POINTER(PfRasterInputs), c_i32, c_f, c_f, c_f, c_f, c_vp, c_vp, c_vp, c_vp, c_vp,
+                            c_vp],
+    "pf_trace_forward": [ctypes.POINTER(PfTraceInputs), c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_i32, c_vp, c_vp,
+                         c_vp],
+    "pf_start_cell_workspace_size": [c_i64, ctypes.POINTER(ctypes.c_size_t)],
+    "pf_start_cell": [c_vp, c_vp, c_i64, ctypes.POINTER(c_f), c_vp, ctypes.c_size_t, c_vp, c_vp],
+    "pf_sh_texel_rgb": [c_vp, c_vp, c_i64, c_i32, ctypes.POINTER(c_f), c_vp, c_vp],
+    "pf_cech_workspace_size": [c_i64, ctypes.POINTER(ctypes.c_size_t)],
+    "pf_cech_adjacency": [c_vp, c_vp, c_i64, c_vp, ctypes.c_size_t, c_i64, c_vp, c_vp, c_vp, c_vp, c_vp],
+    "pf_morton_workspace_size": [c_i64, ctypes.POINTER(ctypes.c_size_t)],
+    "pf_morton_sort": [c_vp, c_i64, c_vp, ctypes.c_size_t, c_vp, c_vp],
+}
+
+_lib = None
+
+
+def load(build_if_missing=True):
+    """Load libpfoam.so (building it first when the toolchain is here)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if build_if_missing and _build.needs_build():
+        try:
+            _build.build()
+        except Exception as e:  # noqa: BLE001
+            if not os.path.exists(LIB_PATH):
+                raise RuntimeError(f"libpfoam.so is missing and could not be built: {e}") from e
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"libpfoam.so not found at {LIB_PATH}; run python -m powerfoam_b200.build")
+    lib = ctypes.CDLL(LIB_PATH)
+    for name, args in _SIGS.items():
+        f = getattr(lib, name)
+        f.argtypes = args
+        f.restype = ctypes.c_int
+    lib.pf_last_error.restype = ctypes.c_char_p
+    lib.pf_last_error.argtypes = []
+    _lib = lib
+    return lib
+
+
+def exported_symbols():
+    return sorted(_SIGS) + ["pf_last_error"]
+
+
+class PfError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"{_ERR_NAMES.get(code, code)}: {msg}")
+        self.code = code
+
+
+def check(rc):
+    if rc != PF_OK:
+        raise PfError(rc, load().pf_last_error().decode())
+
+
+def call(name, *args):
+    check(getattr(load(), name)(*args))
+
+
+def ptr(t):
+    """Device pointer of a tensor (None -> NULL)."""
+    if t is None:
+        return None
+    if not t.is_cuda:
+        raise ValueError("Only CUDA tensors are supported as inputs")
+    return t.data_ptr()
+
+
+def stream_ptr():
+    return torch.cuda.current_stream().cuda_stream
+
+
+def make_camera(eye, right, up, width, height):
+    c = PfCamera()
+    e, r, u = (torch.as_tensor(v).detach().float().cpu().tolist() for v in (eye, right, up))
+    for i in range(3):
+        c.eye[i] = e[i]
+        c.right[i] = r[i]
+        c.up[i] = u[i]
+    c.width = int(width)
+    c.height = int(height)
+    return c

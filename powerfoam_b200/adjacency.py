@@ -1,0 +1,120 @@
+"""Neighbour structures consumed by the render kernels.
+
+* ``power_adjacency_diff`` -- (E,4) float16 (c_j - c_i, pm_j - pm_i),
+  benchmark.py:296-302, on the GPU.
+* ``start_cell`` -- argmin_i |p_i - eye|^2 - r_i^2, benchmark.py:320-324, on
+  the GPU.
+* ``build_power_adjacency`` -- weighted-Delaunay edges through the lower hull
+  of the lifted points (benchmark.py:25-83), via scipy's Qhull on the host, as
+  the reference does; meant for small scenes.
+"""
+
+import numpy as np
+import torch
+
+from . import _lib
+
+
+def power_adjacency_diff(points, radii, adjacency, adjacency_offsets):
+    points = points.float().contiguous()
+    radii = radii.float().contiguous()
+    adjacency = adjacency.to(torch.int32).contiguous()
+    adjacency_offsets = adjacency_offsets.to(torch.int32).contiguous()
+    out = torch.empty((adjacency.shape[0], 4), dtype=torch.float16, device=points.device)
+    _lib.call("pf_adjacency_power_diff", _lib.ptr(points), _lib.ptr(radii), _lib.ptr(adjacency),
+              _lib.ptr(adjacency_offsets), points.shape[0], _lib.ptr(out), _lib.stream_ptr())
+    return out
+
+
+def start_cell(points, radii, eye, as_tensor=False):
+    points = points.float().contiguous()
+    radii = radii.float().contiguous()
+    ws = torch.empty(256, dtype=torch.uint8, device=points.device)
+    out = torch.empty(1, dtype=torch.int32, device=points.device)
+    e = (_lib.ctypes.c_float * 3)(*[float(v) for v in torch.as_tensor(eye).float().cpu().tolist()])
+    _lib.call("pf_start_cell", _lib.ptr(points), _lib.ptr(radii), points.shape[0], e, _lib.ptr(ws), ws.numel(),
+              _lib.ptr(out), _lib.stream_ptr())
+    return out if as_tensor else int(out.item())
+
+
+def build_power_adjacency(points, radii, alpha_complex=False):
+    """Weighted Delaunay adjacency (benchmark.py:25-83): lift (p, |p|^2 - r^2)
+    to 4-D, keep the facets of the convex hull whose normal points down in the
+    lifted coordinate, take the tetrahedra's edges; with ``alpha_complex`` keep
+    only edges whose balls overlap.  Returns (adjacency int32 (E), offsets int32
+    (N+1)) grouped by source vertex (neighbours ascending)."""
+    from scipy.spatial import ConvexHull
+
+    p = points.detach().cpu().double()
+    r = radii.detach().cpu().double()
+    lifted = torch.cat([p, (p.norm(dim=-1) ** 2 - r**2)[:, None]], dim=-1).numpy()
+    hull = ConvexHull(lifted)
+    simp = hull.simplices[hull.equations[:, 3] < 0]
+    pairs = np.concatenate([simp[:, [a, b]] for a, b in ((0, 1), (1, 2), (2, 0), (0, 3), (1, 3), (2, 3))], 0)
+    pairs = np.unique(np.sort(pairs, axis=1), axis=0)
+    if alpha_complex:
+        d = np.linalg.norm(p.numpy()[pairs[:, 0]] - p.numpy()[pairs[:, 1]], axis=-1)
+        pairs = pairs[d < (r.numpy()[pairs[:, 0]] + r.numpy()[pairs[:, 1]])]
+    directed = np.concatenate([pairs, pairs[:, ::-1]], 0)
+    order = np.lexsort((directed[:, 1], directed[:, 0]))
+    directed = directed[order]
+    n = points.shape[0]
+    counts = np.bincount(directed[:, 0], minlength=n)
+    offsets = np.concatenate([[0], np.cumsum(counts)]).astype(np.int32)
+    dev = points.device
+    return (torch.from_numpy(directed[:, 1].astype(np.int32)).to(dev), torch.from_numpy(offsets).to(dev))
+
+
+class CechBuilder:
+    """GPU Čech adjacency (bvh.py:72-123 semantics) with a reusable workspace;
+    lists ascending.  Like the reference's build_cech_complex (.item() at
+    bvh.py:110), it reads the edge count once to size the output."""
+
+    def __init__(self, device):
+        self.device = torch.device(device)
+        self.ws = None
+        self.capacity = 0
+
+    def __call__(self, points, radii):
+        points = points.float().contiguous()
+        radii = radii.float().contiguous()
+        n = points.shape[0]
+        nbytes = _lib.ctypes.c_size_t(0)
+        _lib.call("pf_cech_workspace_size", n, _lib.ctypes.byref(nbytes))
+        if self.ws is None or self.ws.numel() < nbytes.value:
+            self.ws = torch.empty(nbytes.value, dtype=torch.uint8, device=self.device)
+        cap = max(self.capacity, 16 * n, 1 << 16)
+        while True:
+            adj = torch.empty(cap, dtype=torch.int32, device=self.device)
+            off = torch.empty(n + 1, dtype=torch.int32, device=self.device)
+            scalars = torch.zeros(2, dtype=torch.int64, device=self.device)
+            status = scalars[1:].view(torch.int32)[:1]
+            _lib.call("pf_cech_adjacency", _lib.ptr(points), _lib.ptr(radii), n, _lib.ptr(self.ws), self.ws.numel(),
+                      cap, _lib.ptr(adj), _lib.ptr(off), _lib.ptr(scalars[:1]), _lib.ptr(status), _lib.stream_ptr())
+            e = int(scalars[0].item())
+            if e <= cap:
+                break
+            if e >= (1 << 31) - 1:
+                raise _lib.PfError(_lib.PF_ERR_OVERFLOW, f"{e} adjacency entries exceed int32 offsets")
+            cap = min(1 << (int(e * 1.25) - 1).bit_length(), (1 << 31) - 1)
+        self.capacity = max(self.capacity, cap)
+        return adj[:e], off
+
+
+def cech_adjacency(points, radii):
+    return CechBuilder(points.device)(points, radii)
+
+
+def morton_sort(points):
+    """Permutation (int32) ordering the points along the Morton curve
+    (geometry.py:50-85)."""
+    points = points.float().contiguous()
+    n = points.shape[0]
+    if n == 0:
+        return torch.zeros(0, dtype=torch.int32, device=points.device)
+    nbytes = _lib.ctypes.c_size_t(0)
+    _lib.call("pf_morton_workspace_size", n, _lib.ctypes.byref(nbytes))
+    ws = torch.empty(nbytes.value, dtype=torch.uint8, device=points.device)
+    perm = torch.empty(n, dtype=torch.int32, device=points.device)
+    _lib.call("pf_morton_sort", _lib.ptr(points), n, _lib.ptr(ws), ws.numel(), _lib.ptr(perm), _lib.stream_ptr())
+    return perm

@@ -1,0 +1,403 @@
+// pf_adjacency.cu -- Čech adjacency (overlapping balls) and Morton ordering.
+//
+// The reference builds the Čech adjacency by querying a Warp BVH over the
+// spheres' AABBs (powerfoam/bvh.py:7-123): j is a neighbour of i iff their
+// AABBs overlap and |c_i - c_j| < r_i + r_j, with c and r recovered from the
+// AABB (c = (lo + hi) / 2, r = (hi.x - lo.x) / 2).  Here the same predicate is
+// evaluated over a uniform grid of cell edge 2 * max r: primitives are sorted
+// by cell with the library's radix sort, every primitive scans the 27 cells
+// around its own, counts, a scan sizes the lists, a second pass writes them
+// and each list is sorted ascending (the reference's order is the BVH
+// traversal order; ascending order is the canonical form used everywhere
+// here).  The pair count stays on the device: the caller passes a capacity
+// and reads *n_edges to grow it, exactly as for binning.
+//
+// morton_sort follows powerfoam/geometry.py:7-85: 21-bit quantisation per
+// axis over the bounding box, code = x << 2 | y << 1 | z interleaved, stable
+// sort of the primitive ids by the 63-bit code.
+#include <algorithm>
+
+#include "pf_common.cuh"
+#include "pf_sort.cuh"
+#include "pf_api.h"
+
+namespace pf {
+
+struct CechGrid {
+    float lo_x, lo_y, lo_z, inv_h;
+    int nx, ny, nz;
+};
+
+__global__ void bounds_kernel(const float* __restrict__ pts, const float* __restrict__ radii, int64_t N,
+                              float* __restrict__ out /* lo3, hi3, rmax */) {
+    __shared__ float s[7][32];
+    float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY}, rm = 0.f;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += (int64_t)gridDim.x * blockDim.x) {
+        for (int k = 0; k < 3; k++) {
+            float v = pts[3 * i + k];
+            lo[k] = fminf(lo[k], v);
+            hi[k] = fmaxf(hi[k], v);
+        }
+        if (radii) rm = fmaxf(rm, radii[i]);
+    }
+    float v[7] = {lo[0], lo[1], lo[2], hi[0], hi[1], hi[2], rm};
+    for (int k = 0; k < 7; k++) {
+        float x = v[k];
+        for (int o = 16; o > 0; o >>= 1) {
+            float y = __shfl_xor_sync(0xffffffffu, x, o);
+            x = k < 3 ? fminf(x, y) : fmaxf(x, y);
+        }
+        v[k] = x;
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0)
+        for (int k = 0; k < 7; k++) s[k][warp] = v[k];
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < (int)(blockDim.x >> 5); w++)
+            for (int k = 0; k < 7; k++) v[k] = k < 3 ? fminf(v[k], s[k][w]) : fmaxf(v[k], s[k][w]);
+        // float atomics on order-preserving ints
+        for (int k = 0; k < 7; k++) {
+            int* dst = (int*)&out[k];
+            float x = v[k];
+            int xi = __float_as_int(x);
+            int key = xi >= 0 ? xi : (xi ^ 0x7fffffff);
+            if (k < 3) atomicMin(dst, key);
+            else atomicMax(dst, key);
+        }
+    }
+}
+
+PF_D float from_key(int key) { return __int_as_float(key >= 0 ? key : (key ^ 0x7fffffff)); }
+
+__global__ void bounds_init_kernel(float* out) {
+    int* o = (int*)out;
+    int pinf = __float_as_int(INFINITY);
+    int ninf_key = __float_as_int(-INFINITY) ^ 0x7fffffff;
+    for (int k = 0; k < 3; k++) o[k] = pinf;
+    for (int k = 3; k < 7; k++) o[k] = ninf_key;
+    o[6] = 0;  // rmax >= 0
+}
+
+// grid from the bounds (device side, no host round trip)
+__global__ void grid_kernel(const float* __restrict__ bkeys, int max_cells_log2, CechGrid* __restrict__ g) {
+    const int* k = (const int*)bkeys;
+    float lo[3], hi[3];
+    for (int i = 0; i < 3; i++) {
+        lo[i] = from_key(k[i]);
+        hi[i] = from_key(k[3 + i]);
+    }
+    float rmax = from_key(k[6]);
+    float h = fmaxf(2.0f * rmax * 1.0001f, 1e-6f);
+    // bound the number of cells; a coarser grid only costs extra distance
+    // tests.  Non-finite bounds (or a runaway) fall back to a single cell.
+    g->nx = g->ny = g->nz = 1;
+    for (int it = 0; it < 256; it++) {
+        double nx = floor((double)(hi[0] - lo[0]) / h) + 1, ny = floor((double)(hi[1] - lo[1]) / h) + 1,
+               nz = floor((double)(hi[2] - lo[2]) / h) + 1;
+        if (!(nx * ny * nz < 1e30)) break;
+        if (nx * ny * nz < (double)(1ll << max_cells_log2)) {
+            g->nx = (int)nx;
+            g->ny = (int)ny;
+            g->nz = (int)nz;
+            break;
+        }
+        h *= 1.25f;
+    }
+    if (g->nx == 1 && g->ny == 1 && g->nz == 1) h = INFINITY;
+    g->lo_x = lo[0];
+    g->lo_y = lo[1];
+    g->lo_z = lo[2];
+    g->inv_h = 1.0f / h;
+}
+
+PF_D int cell_coord(float v, float lo, float inv_h, int n) {
+    float f = floorf((v - lo) * inv_h);
+    int c = (f == f) ? __float2int_rz(f) : 0;
+    return c < 0 ? 0 : (c >= n ? n - 1 : c);
+}
+
+__global__ void cell_key_kernel(const float* __restrict__ pts, int64_t N, const CechGrid* __restrict__ gp,
+                                uint32_t* __restrict__ key, uint32_t* __restrict__ idx) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    CechGrid g = *gp;
+    int cx = cell_coord(pts[3 * i], g.lo_x, g.inv_h, g.nx);
+    int cy = cell_coord(pts[3 * i + 1], g.lo_y, g.inv_h, g.ny);
+    int cz = cell_coord(pts[3 * i + 2], g.lo_z, g.inv_h, g.nz);
+    key[i] = (uint32_t)((cz * g.ny + cy) * g.nx + cx);
+    idx[i] = (uint32_t)i;
+}
+
+__global__ void cell_ranges_kernel(const uint32_t* __restrict__ key, int64_t N, const CechGrid* __restrict__ gp,
+                                   int32_t* __restrict__ cell_start) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i > N) return;
+    CechGrid g = *gp;
+    int64_t ncell = (int64_t)g.nx * g.ny * g.nz;
+    int64_t lo = (i == 0) ? 0 : (int64_t)key[i - 1] + 1;
+    int64_t hi = (i == N) ? ncell : (int64_t)key[i];
+    for (int64_t c = lo; c <= hi; c++) cell_start[c] = (int32_t)i;
+}
+
+// bvh.py:7-69 predicate, with the AABB test of the BVH query
+struct Ball {
+    float lo[3], hi[3];
+    v3 c;
+    float r;
+};
+
+PF_D Ball make_ball(const float* pts, const float* radii, int64_t i) {
+    Ball b;
+    float r = radii[i];
+    for (int k = 0; k < 3; k++) {
+        float p = pts[3 * i + k];
+        b.lo[k] = p - r;
+        b.hi[k] = p + r;
+    }
+    b.c = mk(0.5f * (b.lo[0] + b.hi[0]), 0.5f * (b.lo[1] + b.hi[1]), 0.5f * (b.lo[2] + b.hi[2]));
+    b.r = 0.5f * (b.hi[0] - b.lo[0]);
+    return b;
+}
+
+PF_D bool overlaps(const Ball& a, const Ball& b) {
+    for (int k = 0; k < 3; k++)
+        if (!(a.lo[k] <= b.hi[k] && a.hi[k] >= b.lo[k])) return false;
+    return length(a.c - b.c) < a.r + b.r;
+}
+
+template <bool WRITE>
+__global__ void cech_kernel(const float* __restrict__ pts, const float* __restrict__ radii, int64_t N,
+                            const CechGrid* __restrict__ gp, const int32_t* __restrict__ cell_start,
+                            const uint32_t* __restrict__ sorted_idx, int32_t* __restrict__ counts,
+                            const int64_t* __restrict__ offsets, const int64_t* __restrict__ total, int64_t capacity,
+                            int32_t* __restrict__ adj) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    if (WRITE && *total > capacity) return;
+    CechGrid g = *gp;
+    Ball bi = make_ball(pts, radii, i);
+    int cx = cell_coord(pts[3 * i], g.lo_x, g.inv_h, g.nx);
+    int cy = cell_coord(pts[3 * i + 1], g.lo_y, g.inv_h, g.ny);
+    int cz = cell_coord(pts[3 * i + 2], g.lo_z, g.inv_h, g.nz);
+    int64_t pos = WRITE ? offsets[i] : 0;
+    int n = 0;
+    for (int dz = -1; dz <= 1; dz++) {
+        int z = cz + dz;
+        if (z < 0 || z >= g.nz) continue;
+        for (int dy = -1; dy <= 1; dy++) {
+            int y = cy + dy;
+            if (y < 0 || y >= g.ny) continue;
+            for (int dx = -1; dx <= 1; dx++) {
+                int x = cx + dx;
+                if (x < 0 || x >= g.nx) continue;
+                int64_t c = ((int64_t)z * g.ny + y) * g.nx + x;
+                for (int32_t s = cell_start[c]; s < cell_start[c + 1]; s++) {
+                    int64_t j = sorted_idx[s];
+                    if (j == i) continue;
+                    Ball bj = make_ball(pts, radii, j);
+                    if (overlaps(bi, bj)) {
+                        if (WRITE) adj[pos + n] = (int32_t)j;
+                        n++;
+                    }
+                }
+            }
+        }
+    }
+    if (!WRITE) {
+        counts[i] = n;
+    } else {
+        // ascending order of each list
+        int32_t* a = adj + pos;
+        for (int u = 1; u < n; u++) {
+            int32_t v = a[u];
+            int w = u - 1;
+            while (w >= 0 && a[w] > v) {
+                a[w + 1] = a[w];
+                w--;
+            }
+            a[w + 1] = v;
+        }
+    }
+}
+
+__global__ void offsets_i32_kernel(const int64_t* __restrict__ off64, int64_t N, const int64_t* __restrict__ total,
+                                   int64_t capacity, int32_t* __restrict__ off32, int32_t* __restrict__ status) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i > N) return;
+    int64_t t = *total;
+    if (t > capacity) {
+        off32[i] = 0;
+        if (i == 0) atomicMax(status, PF_ERR_OVERFLOW);
+        return;
+    }
+    off32[i] = (int32_t)(i == N ? t : off64[i]);
+}
+
+// ---------------------------------------------------------------------------
+// Morton codes (geometry.py:7-47)
+PF_D uint64_t expand_bits(uint64_t v) {
+    v = v & 0x00000000001FFFFFull;
+    v = (v | (v << 32)) & 0x001F00000000FFFFull;
+    v = (v | (v << 16)) & 0x001F0000FF0000FFull;
+    v = (v | (v << 8)) & 0x100F00F00F00F00Full;
+    v = (v | (v << 4)) & 0x10C30C30C30C30C3ull;
+    v = (v | (v << 2)) & 0x1249249249249249ull;
+    return v;
+}
+
+__global__ void morton_kernel(const float* __restrict__ pts, int64_t N, const float* __restrict__ bkeys,
+                              uint32_t* __restrict__ code_lo, uint32_t* __restrict__ code_hi,
+                              uint32_t* __restrict__ idx) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    const int* k = (const int*)bkeys;
+    float lower[3], dims[3];
+    for (int a = 0; a < 3; a++) {
+        lower[a] = from_key(k[a]);
+        float upper = from_key(k[3 + a]);
+        dims[a] = fmax_t(upper - lower[a], 1e-6f);
+    }
+    const float res = 2097152.0f;
+    uint64_t q[3];
+    for (int a = 0; a < 3; a++) {
+        float nrm = (pts[3 * i + a] - lower[a]) / dims[a];
+        float x = fmin_t(fmax_t(nrm * res, 0.0f), res - 1.0f);
+        q[a] = expand_bits((uint64_t)x);
+    }
+    uint64_t code = q[0] * 4 + q[1] * 2 + q[2];
+    code_lo[i] = (uint32_t)(code & 0xffffffffull);
+    code_hi[i] = (uint32_t)(code >> 32);
+    idx[i] = (uint32_t)i;
+}
+
+__global__ void gather_u32_kernel(const uint32_t* __restrict__ src, const uint32_t* __restrict__ perm, int64_t N,
+                                  uint32_t* __restrict__ dst) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < N) dst[i] = src[perm[i]];
+}
+
+static size_t align_up(size_t x) { return (x + 255) & ~(size_t)255; }
+
+struct CechLayout {
+    size_t bounds, grid, key0, idx0, key1, idx1, cell_start, counts, off64, spart, rhist, rpart, bytes;
+};
+
+constexpr int kMaxCellsLog2 = 22;
+
+static CechLayout cech_layout(int64_t N) {
+    CechLayout L;
+    size_t o = 0;
+    auto take = [&](size_t b) {
+        size_t r = o;
+        o = align_up(o + b);
+        return r;
+    };
+    L.bounds = take(64);
+    L.grid = take(sizeof(CechGrid));
+    L.key0 = take(4 * (size_t)N);
+    L.idx0 = take(4 * (size_t)N);
+    L.key1 = take(4 * (size_t)N);
+    L.idx1 = take(4 * (size_t)N);
+    L.cell_start = take(4 * (((size_t)1 << kMaxCellsLog2) + 1));
+    L.counts = take(4 * (size_t)N);
+    L.off64 = take(8 * (size_t)(N + 1));
+    L.spart = take(8 * (size_t)(scan_blocks(N) + 2));
+    int64_t rb = radix_blocks(N);
+    L.rhist = take(4 * (size_t)(256 * rb));
+    L.rpart = take(4 * (size_t)(scan_blocks(256 * rb) + 1));
+    L.bytes = o;
+    return L;
+}
+
+}  // namespace pf
+
+using namespace pf;
+
+extern "C" int pf_cech_workspace_size(int64_t n_prims, size_t* bytes) {
+    if (!bytes || n_prims < 0) return pf_fail(PF_ERR_ARGS, "pf_cech_workspace_size: bad arguments");
+    *bytes = cech_layout(n_prims).bytes;
+    return PF_OK;
+}
+
+extern "C" int pf_cech_adjacency(const float* points, const float* radii, int64_t n_prims, void* workspace,
+                                 size_t workspace_bytes, int64_t edge_capacity, int32_t* adjacency,
+                                 int32_t* adjacency_offsets, int64_t* n_edges, int32_t* status, void* stream) {
+    if (n_prims <= 0 || !points || !radii || !adjacency_offsets || !n_edges || !status || edge_capacity < 0 ||
+        edge_capacity >= ((int64_t)1 << 31) || (edge_capacity > 0 && !adjacency))
+        return pf_fail(PF_ERR_ARGS, "pf_cech_adjacency: bad arguments");
+    CechLayout L = cech_layout(n_prims);
+    if (!workspace || workspace_bytes < L.bytes) return pf_fail(PF_ERR_ARGS, "pf_cech_adjacency: workspace too small");
+    cudaStream_t st = (cudaStream_t)stream;
+    char* ws = (char*)workspace;
+    float* bounds = (float*)(ws + L.bounds);
+    CechGrid* grid = (CechGrid*)(ws + L.grid);
+    uint32_t *key0 = (uint32_t*)(ws + L.key0), *idx0 = (uint32_t*)(ws + L.idx0);
+    uint32_t *key1 = (uint32_t*)(ws + L.key1), *idx1 = (uint32_t*)(ws + L.idx1);
+    int32_t* cell_start = (int32_t*)(ws + L.cell_start);
+    int32_t* counts = (int32_t*)(ws + L.counts);
+    int64_t* off64 = (int64_t*)(ws + L.off64);
+    int64_t* spart = (int64_t*)(ws + L.spart);
+    RadixScratch rs{(uint32_t*)(ws + L.rhist), (uint32_t*)(ws + L.rpart)};
+    const int64_t N = n_prims;
+    const unsigned gN = (unsigned)((N + 255) / 256);
+    bounds_init_kernel<<<1, 1, 0, st>>>(bounds);
+    bounds_kernel<<<(unsigned)std::min<int64_t>(gN, 148 * 8), 256, 0, st>>>(points, radii, N, bounds);
+    grid_kernel<<<1, 1, 0, st>>>(bounds, kMaxCellsLog2, grid);
+    cell_key_kernel<<<gN, 256, 0, st>>>(points, N, grid, key0, idx0);
+    uint32_t* kf = radix_final_key_buffer(key0, key1, kMaxCellsLog2);
+    uint32_t* vf = kf == key0 ? idx0 : idx1;
+    radix_sort_pairs(key0, idx0, key1, idx1, kf, vf, N, nullptr, kMaxCellsLog2, rs, st);
+    cell_ranges_kernel<<<(unsigned)((N + 1 + 255) / 256), 256, 0, st>>>(kf, N, grid, cell_start);
+    cech_kernel<false><<<gN, 256, 0, st>>>(points, radii, N, grid, cell_start, vf, counts, nullptr, nullptr, 0,
+                                           nullptr);
+    exclusive_scan<int32_t, int64_t>(counts, off64, N, spart, n_edges, st);
+    cech_kernel<true><<<gN, 256, 0, st>>>(points, radii, N, grid, cell_start, vf, nullptr, off64, n_edges,
+                                          edge_capacity, adjacency);
+    offsets_i32_kernel<<<(unsigned)((N + 1 + 255) / 256), 256, 0, st>>>(off64, N, n_edges, edge_capacity,
+                                                                        adjacency_offsets, status);
+    return pf_check_launch("pf_cech_adjacency");
+}
+
+extern "C" int pf_morton_workspace_size(int64_t n_prims, size_t* bytes) {
+    if (!bytes || n_prims < 0) return pf_fail(PF_ERR_ARGS, "pf_morton_workspace_size: bad arguments");
+    int64_t rb = radix_blocks(n_prims);
+    *bytes = align_up(64) + 6 * align_up(4 * (size_t)n_prims) + align_up(4 * (size_t)(256 * rb)) +
+             align_up(4 * (size_t)(scan_blocks(256 * rb) + 1));
+    return PF_OK;
+}
+
+extern "C" int pf_morton_sort(const float* points, int64_t n_prims, void* workspace, size_t workspace_bytes,
+                              int32_t* permutation, void* stream) {
+    size_t need = 0;
+    if (pf_morton_workspace_size(n_prims, &need) != PF_OK) return PF_ERR_ARGS;
+    if (n_prims <= 0 || !points || !permutation || !workspace || workspace_bytes < need)
+        return pf_fail(PF_ERR_ARGS, "pf_morton_sort: bad arguments");
+    cudaStream_t st = (cudaStream_t)stream;
+    char* ws = (char*)workspace;
+    size_t o = 0;
+    auto take = [&](size_t b) {
+        char* r = ws + o;
+        o += align_up(b);
+        return r;
+    };
+    const int64_t N = n_prims;
+    float* bounds = (float*)take(64);
+    uint32_t* lo = (uint32_t*)take(4 * N);
+    uint32_t* hi = (uint32_t*)take(4 * N);
+    uint32_t* idx0 = (uint32_t*)take(4 * N);
+    uint32_t* k1 = (uint32_t*)take(4 * N);
+    uint32_t* idx1 = (uint32_t*)take(4 * N);
+    uint32_t* hi_s = (uint32_t*)take(4 * N);
+    int64_t rb = radix_blocks(N);
+    RadixScratch rs{(uint32_t*)take(4 * 256 * rb), (uint32_t*)take(4 * (scan_blocks(256 * rb) + 1))};
+    const unsigned gN = (unsigned)((N + 255) / 256);
+    bounds_init_kernel<<<1, 1, 0, st>>>(bounds);
+    bounds_kernel<<<(unsigned)std::min<int64_t>(gN, 148 * 8), 256, 0, st>>>(points, nullptr, N, bounds);
+    morton_kernel<<<gN, 256, 0, st>>>(points, N, bounds, lo, hi, idx0);
+    // LSD: low 32 bits (4 passes) then high 31 bits carried through a gather
+    radix_sort_pairs(lo, idx0, k1, idx1, lo, idx0, N, nullptr, 32, rs, st);
+    gather_u32_kernel<<<gN, 256, 0, st>>>(hi, idx0, N, hi_s);
+    radix_sort_pairs(hi_s, idx0, k1, idx1, hi_s, (uint32_t*)permutation, N, nullptr, 32, rs, st);
+    return pf_check_launch("pf_morton_sort");
+}

@@ -1,0 +1,319 @@
+// pf_bin.cu -- tile binning: count -> depth sort -> scan -> emit -> tile sort.
+//
+// Replaces rasterize.py:1671-1768 (count_visible_pinhole_kernel :140-200,
+// cumsum + .item(), write_visible_pinhole_kernel :293-363, argsort :1767).
+// The reference sorts 64-bit (tile << 32 | depth bits) keys with an unstable
+// argsort over pairs emitted in atomic order.  Here the order is fixed to
+// (tile, depth bits, primitive index) and reached with two cheaper stable
+// sorts: primitives are first sorted by their 32-bit depth key (N items, four
+// 8-bit passes), the pairs are then emitted in that order and stably sorted by
+// tile (ceil(log2 T) bits).  Nothing here waits on the host: the pair count
+// stays on the device and a grid sized for the caller's capacity reads it.
+#include "pf_common.cuh"
+#include "pf_sort.cuh"
+#include "pf_api.h"
+
+namespace pf {
+
+// camera.py:79-128 proj_sphere_to_obb
+struct Obb {
+    float uc, vc, r1, r2, vx, vy;
+};
+
+PF_D Obb proj_sphere_to_obb(const Cam& cam, v3 center, float radius) {
+    v3 C = center - cam.eye;
+    float C2 = dot(C, C);
+    float R = radius;
+    float R2 = R * R;
+    v3 X = cam.right, Y = cam.up;
+    v3 Z = normalize(cross(Y, X));
+    float cx = dot(C, X), cy = dot(C, Y), cz = dot(C, Z);
+    // x ** 2.0 taken as the correctly rounded square
+    float a = cx * cx - (C2 - R2) * dot(X, X);
+    float b = cy * cy - (C2 - R2) * dot(Y, Y);
+    float f = cz * cz - (C2 - R2) * dot(Z, Z);
+    float c = 2.0f * cx * cy;
+    float d = 2.0f * cx * cz;
+    float e = 2.0f * cy * cz;
+    float denom = 4.0f * a * b - c * c;
+    Obb o;
+    if (fabsf(denom) < 1e-8f) {
+        o.uc = 0.f; o.vc = 0.f; o.r1 = 0.f; o.r2 = 0.f; o.vx = 1.f; o.vy = 0.f;
+        return o;
+    }
+    float uc = (c * e - 2.0f * b * d) / denom;
+    float vc = (c * d - 2.0f * a * e) / denom;
+    float F0 = a * uc * uc + b * vc * vc + c * uc * vc + d * uc + e * vc + f;
+    float term_sqrt = sqrtf((a - b) * (a - b) + c * c);
+    float l1 = (a + b + term_sqrt) / 2.0f;
+    float l2 = (a + b - term_sqrt) / 2.0f;
+    float r1 = sqrtf(-F0 / l1);
+    float r2 = sqrtf(-F0 / l2);
+    float vx = 0.5f * c;
+    float vy = l1 - a;
+    float norm = sqrtf(vx * vx + vy * vy);
+    if (norm < 1e-6f) {
+        vx = 1.0f;
+        vy = 0.0f;
+    } else {
+        vx = vx / norm;
+        vy = vy / norm;
+    }
+    o.uc = uc; o.vc = vc; o.r1 = r1; o.r2 = r2; o.vx = vx; o.vy = vy;
+    return o;
+}
+
+// camera.py:131-178 verify_tile_obb_intersection
+PF_D bool tile_obb(int tile_i, int tile_j, const Cam& cam, int TW, const Obb& o) {
+    float u_min = 2.0f * (float)(tile_j * TW) / (float)(cam.W - 1) - 1.0f;
+    float u_max = 2.0f * (float)((tile_j + 1) * TW) / (float)(cam.W - 1) - 1.0f;
+    float v_max = 1.0f - 2.0f * (float)(tile_i * TW) / (float)(cam.H - 1);
+    float v_min = 1.0f - 2.0f * (float)((tile_i + 1) * TW) / (float)(cam.H - 1);
+    float u_center = (u_min + u_max) * 0.5f;
+    float v_center = (v_min + v_max) * 0.5f;
+    float eu = (u_max - u_min) * 0.5f;
+    float ev = (v_max - v_min) * 0.5f;
+    float du = u_center - o.uc;
+    float dv = v_center - o.vc;
+    float p1 = du * o.vx + dv * o.vy;
+    float t1 = eu * fabsf(o.vx) + ev * fabsf(o.vy);
+    if (fabsf(p1) > o.r1 + t1) return false;
+    float p2 = du * -o.vy + dv * o.vx;
+    float t2 = eu * fabsf(-o.vy) + ev * fabsf(o.vx);
+    if (fabsf(p2) > o.r2 + t2) return false;
+    return true;
+}
+
+// rasterize.py:150-200: cull, project, tile range.  Returns false if culled.
+struct TileRange {
+    int ti0, ti1, tj0, tj1;
+    Obb o;
+};
+
+PF_D bool prim_tile_range(const Cam& cam, int TW, v3 center, float radius, TileRange& tr) {
+    v3 v = center - cam.eye;
+    v3 forward = cross(cam.up, cam.right);
+    if (length(v) < 4.0f * radius || dot(v, forward) < 0.1f) return false;
+    Obb o = proj_sphere_to_obb(cam, center, radius);
+    float extent_u = fabsf(o.vx * o.r1) + fabsf(o.vy * o.r2);
+    float extent_v = fabsf(o.vy * o.r1) + fabsf(o.vx * o.r2);
+    float u_min = o.uc - extent_u, u_max = o.uc + extent_u;
+    float v_min = o.vc - extent_v, v_max = o.vc + extent_v;
+    float j_min_f = (u_min + 1.0f) * 0.5f * (float)(cam.W - 1);
+    float j_max_f = (u_max + 1.0f) * 0.5f * (float)(cam.W - 1);
+    float i_min_f = (1.0f - v_max) * 0.5f * (float)(cam.H - 1);
+    float i_max_f = (1.0f - v_min) * 0.5f * (float)(cam.H - 1);
+    int i_min = imax(sat_f2i(floorf(i_min_f)), 0);
+    int i_max = imin(sat_f2i(ceilf(i_max_f)), cam.H - 1);
+    int j_min = imax(sat_f2i(floorf(j_min_f)), 0);
+    int j_max = imin(sat_f2i(ceilf(j_max_f)), cam.W - 1);
+    // Warp's integer // is C division (truncation toward zero)
+    tr.ti0 = i_min / TW;
+    tr.ti1 = i_max / TW;
+    tr.tj0 = j_min / TW;
+    tr.tj1 = j_max / TW;
+    tr.o = o;
+    return true;
+}
+
+__global__ void bin_count_kernel(pf_camera camera, int TW, const float4* __restrict__ spheres, int64_t N,
+                                 int32_t* __restrict__ counts, uint32_t* __restrict__ depth_key,
+                                 uint32_t* __restrict__ depth_by_prim, uint32_t* __restrict__ idx) {
+    int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= N) return;
+    Cam cam = load_cam(camera);
+    float4 s = spheres[p];
+    v3 c = mk(s.x, s.y, s.z);
+    v3 v = c - cam.eye;
+    float pow_dist = dot(v, v) - s.w * s.w;
+    depth_key[p] = __float_as_uint(pow_dist);
+    depth_by_prim[p] = __float_as_uint(pow_dist);
+    idx[p] = (uint32_t)p;
+    int n = 0;
+    TileRange tr;
+    if (prim_tile_range(cam, TW, c, s.w, tr)) {
+        for (int ti = tr.ti0; ti <= tr.ti1; ti++)
+            for (int tj = tr.tj0; tj <= tr.tj1; tj++)
+                if (tile_obb(ti, tj, cam, TW, tr.o)) n++;
+    }
+    counts[p] = n;
+}
+
+__global__ void gather_counts_kernel(const uint32_t* __restrict__ order, const int32_t* __restrict__ counts,
+                                     int64_t N, int32_t* __restrict__ sorted_counts) {
+    int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < N) sorted_counts[k] = counts[order[k]];
+}
+
+__global__ void bin_emit_kernel(pf_camera camera, int TW, const float4* __restrict__ spheres, int64_t N,
+                                const uint32_t* __restrict__ order, const int32_t* __restrict__ sorted_counts,
+                                const int64_t* __restrict__ offsets, const int64_t* __restrict__ total,
+                                int64_t capacity, uint32_t* __restrict__ tile_key, uint32_t* __restrict__ pair_prim,
+                                uint8_t* __restrict__ prim_visible) {
+    int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= N) return;
+    if (*total > capacity) return;
+    if (sorted_counts[k] == 0) return;
+    uint32_t p = order[k];
+    if (prim_visible) prim_visible[p] = 1;
+    Cam cam = load_cam(camera);
+    int tiles_h = 1 + (cam.H - 1) / TW;
+    float4 s = spheres[p];
+    v3 c = mk(s.x, s.y, s.z);
+    int64_t pos = offsets[k];
+    TileRange tr;
+    if (!prim_tile_range(cam, TW, c, s.w, tr)) return;
+    for (int ti = tr.ti0; ti <= tr.ti1; ti++)
+        for (int tj = tr.tj0; tj <= tr.tj1; tj++)
+            if (tile_obb(ti, tj, cam, TW, tr.o)) {
+                tile_key[pos] = (uint32_t)(ti + tj * tiles_h);
+                pair_prim[pos] = p;
+                pos++;
+            }
+}
+
+// tile_offsets[t] = first sorted position with tile >= t; also the optional
+// 64-bit reference keys.  Grid over capacity; the live count is on device.
+__global__ void tile_ranges_kernel(const uint32_t* __restrict__ tile_key, const int32_t* __restrict__ prims,
+                                   const uint32_t* __restrict__ depth_key, const int64_t* __restrict__ total,
+                                   int64_t capacity, int64_t T, int64_t* __restrict__ tile_offsets,
+                                   int64_t* __restrict__ sort_keys, int32_t* __restrict__ status) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    int64_t n = *total;
+    if (n > capacity) {
+        // overflow: empty every list, report
+        for (int64_t t = i; t <= T; t += (int64_t)gridDim.x * blockDim.x) tile_offsets[t] = 0;
+        if (i == 0) atomicMax(status, PF_ERR_OVERFLOW);
+        return;
+    }
+    if (i > n) return;
+    int64_t lo = (i == 0) ? 0 : (int64_t)tile_key[i - 1] + 1;
+    int64_t hi = (i == n) ? T : (int64_t)tile_key[i];
+    for (int64_t t = lo; t <= hi; t++) tile_offsets[t] = i;
+    if (i < n && sort_keys) sort_keys[i] = ((int64_t)tile_key[i] << 32) | (int64_t)depth_key[prims[i]];
+}
+
+__global__ void pack_prims_kernel(const float* __restrict__ points, const float* __restrict__ radii,
+                                  const float* __restrict__ normals, const float* __restrict__ density, int64_t N,
+                                  float4* __restrict__ spheres, float4* __restrict__ nsigmas) {
+    int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= N) return;
+    if (spheres) spheres[p] = make_float4(points[3 * p], points[3 * p + 1], points[3 * p + 2], radii[p]);
+    if (nsigmas) nsigmas[p] = make_float4(normals[3 * p], normals[3 * p + 1], normals[3 * p + 2], density[p]);
+}
+
+// ---------------------------------------------------------------------------
+struct BinLayout {
+    size_t counts, dprim, dkey0, idx0, dkey1, idx1, scounts, offsets, spart, pkey0, pprim0, pkey1, pprim1, rhist, rpart,
+        total;
+    size_t bytes;
+};
+
+static size_t align_up(size_t x) { return (x + 255) & ~(size_t)255; }
+
+static BinLayout bin_layout(int64_t N, int64_t cap) {
+    BinLayout L;
+    size_t o = 0;
+    auto take = [&](size_t b) {
+        size_t r = o;
+        o = align_up(o + b);
+        return r;
+    };
+    L.counts = take(4 * (size_t)N);
+    L.dprim = take(4 * (size_t)N);
+    L.dkey0 = take(4 * (size_t)N);
+    L.idx0 = take(4 * (size_t)N);
+    L.dkey1 = take(4 * (size_t)N);
+    L.idx1 = take(4 * (size_t)N);
+    L.scounts = take(4 * (size_t)N);
+    L.offsets = take(8 * (size_t)N);
+    L.spart = take(8 * (size_t)(scan_blocks(N) + 1));
+    L.pkey0 = take(4 * (size_t)cap);
+    L.pprim0 = take(4 * (size_t)cap);
+    L.pkey1 = take(4 * (size_t)cap);
+    L.pprim1 = take(4 * (size_t)cap);
+    int64_t rb = radix_blocks(cap > N ? cap : N);
+    L.rhist = take(4 * (size_t)(256 * rb));
+    L.rpart = take(4 * (size_t)(scan_blocks(256 * rb) + 1));
+    L.total = take(8);
+    L.bytes = o;
+    return L;
+}
+
+}  // namespace pf
+
+using namespace pf;
+
+extern "C" int pf_bin_workspace_size(int64_t n_prims, int64_t pair_capacity, size_t* bytes) {
+    if (n_prims < 0 || pair_capacity < 0 || pair_capacity >= (int64_t)1 << 31 || !bytes)
+        return pf_fail(PF_ERR_ARGS, "pf_bin_workspace_size: bad arguments");
+    *bytes = bin_layout(n_prims, pair_capacity).bytes;
+    return PF_OK;
+}
+
+extern "C" int pf_pack_prims(const float* points, const float* radii, const float* normals, const float* density,
+                             int64_t n_prims, float* spheres, float* nsigmas, void* stream) {
+    if (n_prims < 0) return pf_fail(PF_ERR_ARGS, "pf_pack_prims: n_prims < 0");
+    if (n_prims == 0) return PF_OK;
+    if ((spheres && (!points || !radii)) || (nsigmas && (!normals || !density)))
+        return pf_fail(PF_ERR_ARGS, "pf_pack_prims: missing input");
+    cudaStream_t st = (cudaStream_t)stream;
+    pack_prims_kernel<<<(unsigned)((n_prims + 255) / 256), 256, 0, st>>>(points, radii, normals, density, n_prims,
+                                                                        (float4*)spheres, (float4*)nsigmas);
+    return pf_check_launch("pf_pack_prims");
+}
+
+extern "C" int pf_bin(const pf_camera* cam, int32_t tile_width, const float* spheres, int64_t n_prims,
+                      void* workspace, size_t workspace_bytes, int64_t pair_capacity, int64_t* tile_offsets,
+                      int32_t* tile_prims, int64_t* sort_keys, uint8_t* prim_visible, int64_t* n_pairs,
+                      int32_t* status, void* stream) {
+    if (!cam || tile_width <= 0 || n_prims < 0 || pair_capacity < 0 || pair_capacity >= (int64_t)1 << 31 ||
+        !tile_offsets || !n_pairs || !status || (n_prims > 0 && !spheres) || (pair_capacity > 0 && !tile_prims))
+        return pf_fail(PF_ERR_ARGS, "pf_bin: bad arguments");
+    if (cam->width < 2 || cam->height < 2) return pf_fail(PF_ERR_ARGS, "pf_bin: image must be at least 2x2");
+    BinLayout L = bin_layout(n_prims, pair_capacity);
+    if (workspace_bytes < L.bytes || (!workspace && L.bytes)) return pf_fail(PF_ERR_ARGS, "pf_bin: workspace too small");
+    cudaStream_t st = (cudaStream_t)stream;
+    char* ws = (char*)workspace;
+    int32_t* counts = (int32_t*)(ws + L.counts);
+    uint32_t* dprim = (uint32_t*)(ws + L.dprim);
+    uint32_t* dkey0 = (uint32_t*)(ws + L.dkey0);
+    uint32_t* idx0 = (uint32_t*)(ws + L.idx0);
+    uint32_t* dkey1 = (uint32_t*)(ws + L.dkey1);
+    uint32_t* idx1 = (uint32_t*)(ws + L.idx1);
+    int32_t* scounts = (int32_t*)(ws + L.scounts);
+    int64_t* offsets = (int64_t*)(ws + L.offsets);
+    int64_t* spart = (int64_t*)(ws + L.spart);
+    uint32_t* pkey0 = (uint32_t*)(ws + L.pkey0);
+    uint32_t* pprim0 = (uint32_t*)(ws + L.pprim0);
+    uint32_t* pkey1 = (uint32_t*)(ws + L.pkey1);
+    uint32_t* pprim1 = (uint32_t*)(ws + L.pprim1);
+    RadixScratch rs{(uint32_t*)(ws + L.rhist), (uint32_t*)(ws + L.rpart)};
+    const int TW = tile_width;
+    const int64_t tiles_h = 1 + (cam->height - 1) / TW, tiles_w = 1 + (cam->width - 1) / TW;
+    const int64_t T = tiles_h * tiles_w;
+    if (prim_visible && n_prims) cudaMemsetAsync(prim_visible, 0, (size_t)n_prims, st);
+    if (n_prims == 0) {
+        cudaMemsetAsync(n_pairs, 0, 8, st);
+        cudaMemsetAsync(tile_offsets, 0, 8 * (size_t)(T + 1), st);
+        return pf_check_launch("pf_bin");
+    }
+    const unsigned gN = (unsigned)((n_prims + 255) / 256);
+    bin_count_kernel<<<gN, 256, 0, st>>>(*cam, TW, (const float4*)spheres, n_prims, counts, dkey0, dprim, idx0);
+    // stable sort of primitives by depth bits: 4 passes, result back in (dkey0, idx0)
+    radix_sort_pairs(dkey0, idx0, dkey1, idx1, dkey0, idx0, n_prims, nullptr, 32, rs, st);
+    gather_counts_kernel<<<gN, 256, 0, st>>>(idx0, counts, n_prims, scounts);
+    exclusive_scan<int32_t, int64_t>(scounts, offsets, n_prims, spart, n_pairs, st);
+    bin_emit_kernel<<<gN, 256, 0, st>>>(*cam, TW, (const float4*)spheres, n_prims, idx0, scounts, offsets, n_pairs,
+                                        pair_capacity, pkey0, pprim0, prim_visible);
+    // stable sort of the pairs by tile
+    int bits = 0;
+    while (((int64_t)1 << bits) < T) bits++;
+    uint32_t* kf = radix_final_key_buffer(pkey0, pkey1, bits);
+    radix_sort_pairs(pkey0, pprim0, pkey1, pprim1, kf, (uint32_t*)tile_prims, pair_capacity, n_pairs, bits, rs, st);
+    int64_t nthreads = pair_capacity + 1;
+    tile_ranges_kernel<<<(unsigned)((nthreads + 255) / 256), 256, 0, st>>>(kf, tile_prims, dprim, n_pairs,
+                                                                           pair_capacity, T, tile_offsets,
+                                                                           sort_keys, status);
+    return pf_check_launch("pf_bin");
+}

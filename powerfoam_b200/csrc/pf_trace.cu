@@ -1,0 +1,346 @@
+// pf_trace.cu -- cell-walk ray tracer (powerfoam/raytrace.py:115-241),
+// start-cell search (benchmark.py:320-324) and the SH texel colour pre-step.
+//
+// One thread per ray, threads laid out tile by tile (8 x 8 rays per two warps)
+// as the reference launches them, so neighbouring lanes walk neighbouring
+// cells.  The walk is bounded by max_steps; a ray that reaches the cap stops
+// and raises PF_ERR_STEP_CAP in the status word instead of looping forever.
+#include <algorithm>
+
+#include "pf_common.cuh"
+#include "pf_api.h"
+
+namespace pf {
+
+struct TraceParams {
+    Cam cam;
+    int S;
+    int64_t N;
+    const float4* spheres;
+    const void* nsig;
+    const void* sites;
+    const void* rgb;
+    const void* height;
+    const int32_t* adj;
+    const int32_t* adj_off;
+    const uint2* adj_diff;
+    int32_t start_idx;
+    const int32_t* start_cells;
+    float thr;
+    int max_steps;
+    float depth_q;
+};
+
+template <typename A>
+PF_D float ldT(const A* p, int64_t i);
+template <>
+PF_D float ldT<float>(const float* p, int64_t i) { return __ldg(p + i); }
+template <>
+PF_D float ldT<__half>(const __half* p, int64_t i) { return __half2float(p[i]); }
+
+// rasterize.py:62-137 / raytrace.py:42-113 plane_intersection_fwd_local
+template <typename A>
+PF_D PlaneRes plane_local(v3 o, v3 d, float t_near, v3 po, v3 pn, float radius, const A* sites, const A* rgbs,
+                          const A* heights, int S) {
+    PlaneRes r;
+    float _dp;
+    float _t_surf = ray_plane(o, d, po, pn, 0.0f, _dp);
+    float _tq = _dp >= 0.0f ? t_near : fmax_t(t_near, _t_surf);
+    v3 _pt = o + _tq * d;
+    float inv_r2 = 1.0f / (radius * radius);
+    float hsum = 0.f, _wsum = 0.f;
+    for (int i = 0; i < S; i++) {
+        v3 df = _pt - mk(ldT(sites, 3 * i), ldT(sites, 3 * i + 1), ldT(sites, 3 * i + 2));
+        float dist_sq = dot(df, df) * inv_r2;
+        float w = expf(-kTemp * dist_sq);
+        hsum += w * ldT(heights, i);
+        _wsum += w;
+    }
+    _wsum = fmax_t(_wsum, 1e-20f);
+    float height = hsum / _wsum;
+    float dp;
+    float t_surf = ray_plane(o, d, po, pn, height, dp);
+    float tq = dp >= 0.0f ? t_near : fmax_t(t_near, t_surf);
+    v3 pt = o + tq * d;
+    v3 rgb_sum = mk(0.f, 0.f, 0.f);
+    float wsum = 0.f;
+    for (int i = 0; i < S; i++) {
+        v3 df = pt - mk(ldT(sites, 3 * i), ldT(sites, 3 * i + 1), ldT(sites, 3 * i + 2));
+        float dist_sq = dot(df, df) * inv_r2;
+        float w = expf(-kTemp * dist_sq);
+        rgb_sum = rgb_sum + w * mk(ldT(rgbs, 3 * i), ldT(rgbs, 3 * i + 1), ldT(rgbs, 3 * i + 2));
+        wsum += w;
+    }
+    wsum = fmax_t(wsum, 1e-20f);
+    r._t_surf = _t_surf;
+    r._dp = _dp;
+    r.height = height;
+    r._wsum = _wsum;
+    r.t_surf = t_surf;
+    r.dp = dp;
+    r.rgb = rgb_sum / wsum;
+    r.wsum = wsum;
+    return r;
+}
+
+// thread -> pixel in the reference's 8 x 8 tile order
+PF_D bool trace_pixel(const Cam& cam, int64_t tid, int& pi, int& pj) {
+    int tiles_h = 1 + (cam.H - 1) / 8;
+    int64_t tile = tid / 64;
+    int l = (int)(tid % 64);
+    int ti = (int)(tile % tiles_h), tj = (int)(tile / tiles_h);
+    pi = ti * 8 + l % 8;
+    pj = tj * 8 + l / 8;
+    return pi < cam.H && pj < cam.W;
+}
+
+template <typename A>
+__global__ void __launch_bounds__(128)
+trace_fwd_kernel(TraceParams P, int64_t nthreads, float* __restrict__ color, float* __restrict__ log_t_out,
+                 float* __restrict__ depth, float* __restrict__ normal, int32_t* __restrict__ depth_seg,
+                 float* __restrict__ depth_sigma, int32_t* __restrict__ visit_log, int visit_cap,
+                 int32_t* __restrict__ visit_count, int32_t* __restrict__ status) {
+    int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (tid >= nthreads) return;
+    int pi, pj;
+    if (!trace_pixel(P.cam, tid, pi, pj)) return;
+    const int64_t px = (int64_t)pi * P.cam.W + pj;
+    const v3 o = P.cam.eye;
+    const v3 d = ray_dir(P.cam, pi, pj);
+    const A* nsig = (const A*)P.nsig;
+    v3 rgb = mk(0.f, 0.f, 0.f), nacc = mk(0.f, 0.f, 0.f);
+    float log_t = 0.f;
+    int32_t prim = P.start_cells ? P.start_cells[px] : P.start_idx;
+    float pt_near = 0.f;
+    int steps = 0, seg = 0, st = PF_OK;
+    int32_t dseg = -1;
+    float dout = 0.f, dsig = 0.f;
+    for (;;) {
+        float trans = expf(log_t);
+        if (trans < P.thr || prim == kNoCell) break;
+        if (steps >= P.max_steps) {
+            st = PF_ERR_STEP_CAP;
+            break;
+        }
+        if (prim < 0 || prim >= P.N) {
+            st = PF_ERR_ARGS;
+            break;
+        }
+        if (visit_log && steps < visit_cap) visit_log[px * visit_cap + steps] = prim;
+        steps++;
+        const float4 s4 = __ldg(&P.spheres[prim]);
+        const v3 center = mk(s4.x, s4.y, s4.z);
+        const float radius = s4.w;
+        float tn, tf;
+        bool hit = ray_sphere(o, d, center, radius, tn, tf);
+        v3 v = center - o;
+        if (length(v) < 4.0f * radius) hit = false;
+        int32_t next = kNoCell;
+        float pt_far = 1e10f;
+        const int32_t a0 = __ldg(&P.adj_off[prim]), a1 = __ldg(&P.adj_off[prim + 1]);
+        for (int32_t e = a0; e < a1; e++) {
+            uint2 raw = __ldg(&P.adj_diff[e]);
+            v3 diff = mk(h2f((uint16_t)(raw.x & 0xffffu)), h2f((uint16_t)(raw.x >> 16)), h2f((uint16_t)(raw.y & 0xffffu)));
+            Face f = make_face_pm(o, diff, h2f((uint16_t)(raw.y >> 16)));
+            float dp = dot(d, f.n);
+            float t_face = f.num / dp;
+            if (dp >= 0.0f && t_face < pt_far) {
+                next = __ldg(&P.adj[e]);
+                pt_far = t_face;
+            }
+            tf = dp >= 0.0f ? fmin_t(t_face, tf) : tf;
+            tn = dp < 0.0f ? fmax_t(t_face, tn) : tn;
+        }
+        v3 pn = mk(ldT(nsig, 4 * (int64_t)prim), ldT(nsig, 4 * (int64_t)prim + 1), ldT(nsig, 4 * (int64_t)prim + 2));
+        float sigma = ldT(nsig, 4 * (int64_t)prim + 3);
+        if (!hit || tn > tf || sigma < 1e-3f) {
+            prim = next;
+            pt_near = fmax_t(pt_near, pt_far);
+            continue;
+        }
+        int64_t b3 = (int64_t)prim * P.S * 3;
+        PlaneRes pr = plane_local<A>(o, d, tn, center, pn, radius, (const A*)P.sites + b3, (const A*)P.rgb + b3,
+                                     (const A*)P.height + (int64_t)prim * P.S, P.S);
+        tf = pr.dp >= 0.0f ? fmin_t(pr.t_surf, tf) : tf;
+        tn = pr.dp < 0.0f ? fmax_t(pr.t_surf, tn) : tn;
+        prim = next;
+        pt_near = fmax_t(pt_near, pt_far);
+        float dt = tf - tn;
+        if (dt > 0.0f) {
+            float dlt = -sigma * dt;
+            float alpha = 1.0f - expf(dlt);
+            rgb = rgb + trans * (alpha * pr.rgb);
+            nacc = nacc + (alpha * trans) * pn;
+            log_t += dlt;
+            if (dseg < 0 && expf(log_t) < P.depth_q) {
+                dout = tn + logf(trans / P.depth_q) / sigma;
+                dseg = seg;
+                dsig = sigma;
+            }
+            seg++;
+        }
+    }
+    color[3 * px] = rgb.x;
+    color[3 * px + 1] = rgb.y;
+    color[3 * px + 2] = rgb.z;
+    if (log_t_out) log_t_out[px] = log_t;
+    if (depth) depth[px] = dout;
+    if (normal) {
+        normal[3 * px] = nacc.x;
+        normal[3 * px + 1] = nacc.y;
+        normal[3 * px + 2] = nacc.z;
+    }
+    if (depth_seg) depth_seg[px] = dseg;
+    if (depth_sigma) depth_sigma[px] = dsig;
+    if (visit_count) visit_count[px] = steps;
+    if (visit_log)
+        for (int k = steps; k < visit_cap; k++) visit_log[px * visit_cap + k] = -1;
+    if (st != PF_OK && status) atomicMax(status, st);
+}
+
+// ---------------------------------------------------------------------------
+// start cell: argmin_i (|p_i - eye|)^2 - r_i^2, first index on ties.  The
+// float is mapped to an order-preserving uint32 and packed above the index,
+// so one 64-bit atomicMin per block finds the first minimum.
+PF_D uint32_t orderable(float f) {
+    uint32_t u = __float_as_uint(f);
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+
+__global__ void start_cell_kernel(const float* __restrict__ pts, const float* __restrict__ radii, int64_t N, v3 eye,
+                                  unsigned long long* __restrict__ best) {
+    __shared__ unsigned long long sb;
+    if (threadIdx.x == 0) sb = ~0ull;
+    __syncthreads();
+    unsigned long long mine = ~0ull;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += (int64_t)gridDim.x * blockDim.x) {
+        float dx = pts[3 * i] - eye.x, dy = pts[3 * i + 1] - eye.y, dz = pts[3 * i + 2] - eye.z;
+        float n = sqrtf(dx * dx + dy * dy + dz * dz);
+        float v = n * n - radii[i] * radii[i];
+        unsigned long long key = ((unsigned long long)orderable(v) << 32) | (unsigned long long)(uint32_t)i;
+        mine = key < mine ? key : mine;
+    }
+    atomicMin(&sb, mine);
+    __syncthreads();
+    if (threadIdx.x == 0) atomicMin(best, sb);
+}
+
+__global__ void start_cell_finish_kernel(const unsigned long long* __restrict__ best, int32_t* __restrict__ out) {
+    *out = (int32_t)(*best & 0xffffffffull);
+}
+
+// ---------------------------------------------------------------------------
+// degree-3 real SH colour pre-step (constants of powerfoam/sh_utils.py:4-50)
+__global__ void sh_texel_rgb_kernel(const float* __restrict__ pts, const float* __restrict__ sh, int64_t N, int S,
+                                    v3 eye, float* __restrict__ out) {
+    int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= N) return;
+    const float C0 = 0.28209479177387814f, C1 = 0.4886025119029199f;
+    const float C2[5] = {1.0925484305920792f, -1.0925484305920792f, 0.31539156525252005f, -1.0925484305920792f,
+                         0.5462742152960396f};
+    const float C3[7] = {-0.5900435899266435f, 2.890611442640554f, -0.4570457994644658f, 0.3731763325901154f,
+                         -0.4570457994644658f, 1.445305721320277f, -0.5900435899266435f};
+    v3 dir = normalize(mk(pts[3 * p], pts[3 * p + 1], pts[3 * p + 2]) - eye);
+    float x = dir.x, y = dir.y, z = dir.z;
+    float xx = x * x, yy = y * y, zz = z * z;
+    float b[16];
+    b[0] = C0;
+    b[1] = -C1 * y;
+    b[2] = C1 * z;
+    b[3] = -C1 * x;
+    b[4] = C2[0] * (x * y);
+    b[5] = C2[1] * (y * z);
+    b[6] = C2[2] * (2.0f * zz - xx - yy);
+    b[7] = C2[3] * (x * z);
+    b[8] = C2[4] * (xx - yy);
+    b[9] = C3[0] * y * (3.0f * xx - yy);
+    b[10] = C3[1] * (x * y) * z;
+    b[11] = C3[2] * y * (4.0f * zz - xx - yy);
+    b[12] = C3[3] * z * (2.0f * zz - 3.0f * xx - 3.0f * yy);
+    b[13] = C3[4] * x * (4.0f * zz - xx - yy);
+    b[14] = C3[5] * z * (xx - yy);
+    b[15] = C3[6] * x * (xx - 3.0f * yy);
+    const float* c = sh + p * 48;
+    for (int ch = 0; ch < 3; ch++) {
+        float acc = 0.f;
+#pragma unroll
+        for (int k = 0; k < 16; k++) acc += b[k] * c[k * 3 + ch];
+        acc = acc + 0.5f;
+        acc = acc > 0.0f ? acc : 0.0f;
+        for (int s = 0; s < S; s++) out[(p * S + s) * 3 + ch] = acc;
+    }
+}
+
+}  // namespace pf
+
+using namespace pf;
+
+extern "C" int pf_trace_forward(const pf_trace_inputs* in, float* color, float* log_t, float* depth, float* normal,
+                                int32_t* depth_seg, float* depth_sigma, int32_t* visit_log, int32_t visit_cap,
+                                int32_t* visit_count, int32_t* status, void* stream) {
+    if (!in || !color) return pf_fail(PF_ERR_ARGS, "pf_trace_forward: missing argument");
+    if (in->cam.width < 2 || in->cam.height < 2) return pf_fail(PF_ERR_ARGS, "image must be at least 2x2");
+    if (in->n_sites < 0 || in->n_sites > kMaxSites) return pf_fail(PF_ERR_ARGS, "n_sites must be in [0, 8]");
+    if (in->max_steps <= 0) return pf_fail(PF_ERR_ARGS, "max_steps must be positive");
+    if (visit_log && visit_cap <= 0) return pf_fail(PF_ERR_ARGS, "visit_cap must be positive with a visit log");
+    if (in->n_prims <= 0) return pf_fail(PF_ERR_ARGS, "pf_trace_forward: no primitives");
+    if (!in->start_cells && (in->start_idx < 0 || in->start_idx >= in->n_prims) && in->start_idx != kNoCell)
+        return pf_fail(PF_ERR_ARGS, "start_idx out of range");
+    TraceParams P;
+    P.cam = load_cam(in->cam);
+    P.S = in->n_sites;
+    P.N = in->n_prims;
+    P.spheres = (const float4*)in->spheres;
+    P.nsig = in->nsigmas;
+    P.sites = in->texel_sites;
+    P.rgb = in->texel_rgb;
+    P.height = in->texel_height;
+    P.adj = in->adjacency;
+    P.adj_off = in->adjacency_offsets;
+    P.adj_diff = (const uint2*)in->adjacency_diff;
+    P.start_idx = in->start_idx;
+    P.start_cells = in->start_cells;
+    P.thr = in->transmittance_threshold;
+    P.max_steps = in->max_steps;
+    P.depth_q = in->depth_quantile;
+    int64_t tiles = (int64_t)(1 + (in->cam.height - 1) / 8) * (1 + (in->cam.width - 1) / 8);
+    int64_t n = tiles * 64;
+    unsigned grid = (unsigned)((n + 127) / 128);
+    cudaStream_t st = (cudaStream_t)stream;
+    if (in->attr_half)
+        trace_fwd_kernel<__half><<<grid, 128, 0, st>>>(P, n, color, log_t, depth, normal, depth_seg, depth_sigma,
+                                                       visit_log, visit_cap, visit_count, status);
+    else
+        trace_fwd_kernel<float><<<grid, 128, 0, st>>>(P, n, color, log_t, depth, normal, depth_seg, depth_sigma,
+                                                      visit_log, visit_cap, visit_count, status);
+    return pf_check_launch("pf_trace_forward");
+}
+
+extern "C" int pf_start_cell_workspace_size(int64_t n_prims, size_t* bytes) {
+    if (!bytes || n_prims < 0) return pf_fail(PF_ERR_ARGS, "pf_start_cell_workspace_size: bad arguments");
+    *bytes = 256;
+    return PF_OK;
+}
+
+extern "C" int pf_start_cell(const float* points, const float* radii, int64_t n_prims, const float* eye_host,
+                             void* workspace, size_t workspace_bytes, int32_t* out_idx, void* stream) {
+    if (n_prims <= 0 || !points || !radii || !eye_host || !out_idx || !workspace || workspace_bytes < 8)
+        return pf_fail(PF_ERR_ARGS, "pf_start_cell: bad arguments");
+    cudaStream_t st = (cudaStream_t)stream;
+    unsigned long long* best = (unsigned long long*)workspace;
+    cudaMemsetAsync(best, 0xff, 8, st);
+    unsigned grid = (unsigned)std::min<int64_t>((n_prims + 255) / 256, 148 * 8);
+    start_cell_kernel<<<grid, 256, 0, st>>>(points, radii, n_prims, mk(eye_host[0], eye_host[1], eye_host[2]), best);
+    start_cell_finish_kernel<<<1, 1, 0, st>>>(best, out_idx);
+    return pf_check_launch("pf_start_cell");
+}
+
+extern "C" int pf_sh_texel_rgb(const float* points, const float* sh, int64_t n_prims, int32_t n_sites,
+                               const float* eye_host, float* texel_rgb, void* stream) {
+    if (n_prims < 0 || n_sites < 0 || !eye_host || (n_prims > 0 && (!points || !sh || !texel_rgb)))
+        return pf_fail(PF_ERR_ARGS, "pf_sh_texel_rgb: bad arguments");
+    if (n_prims == 0) return PF_OK;
+    sh_texel_rgb_kernel<<<(unsigned)((n_prims + 255) / 256), 256, 0, (cudaStream_t)stream>>>(
+        points, sh, n_prims, n_sites, mk(eye_host[0], eye_host[1], eye_host[2]), texel_rgb);
+    return pf_check_launch("pf_sh_texel_rgb");
+}

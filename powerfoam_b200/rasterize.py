@@ -1,0 +1,341 @@
+"""Tile rasterizer: drop-in for powerfoam/rasterize.py.
+
+``Rasterizer(args, device, attr_dtype)`` keeps the reference's constructor,
+``forward`` (through the ``RasterGradFn`` autograd function), ``benchmark`` and
+``visualize`` signatures, return tuples and error behaviour
+(rasterize.py:23-2285).  Every step runs in libpfoam (hand-written sm_100a
+CUDA) on torch's current stream; there is no CPU path.
+
+Differences from the reference, all deliberate:
+* equal sort keys are ordered by primitive index (the reference leaves them
+  in atomic order), so outputs are deterministic up to float atomics;
+* tile edge ``tile_width`` may be 8 (the reference's constant), 16 or 32;
+* only pinhole cameras (``args.is_pinhole``): the generic-camera cone
+  hierarchy (rasterize.py:202-291, 365-569) is not part of this path.
+"""
+
+from dataclasses import dataclass, field
+
+import torch
+
+from . import _lib
+
+TILE_WIDTH = 8
+TILE_SIZE = TILE_WIDTH * TILE_WIDTH
+
+# Optional instrumentation: when set, called as hook(name, "begin" | "end")
+# around every library call of the forward / backward (bench.py records CUDA
+# events there).  It never changes the work done.
+PROFILE_HOOK = None
+
+
+def _timed_call(name, *args):
+    hook = PROFILE_HOOK
+    if hook is not None:
+        hook(name, "begin")
+    _lib.call(name, *args)
+    if hook is not None:
+        hook(name, "end")
+
+
+@dataclass
+class VisOptions:
+    """rasterize.py:15-20"""
+
+    transmittance_threshold: float = 1e-3
+    max_intersections: int = 1024
+    depth_quantile: float = 0.5
+    bkgd_color: tuple = field(default_factory=lambda: (0.0, 0.0, 0.0))
+
+
+class RasterGradFn(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, rasterizer, *args):
+        return rasterizer._forward(ctx, *args)
+
+    @staticmethod
+    def backward(ctx, *args):
+        return ctx.rasterizer._backward(ctx, *args)
+
+
+def _f32(t, name):
+    if t.dtype != torch.float32:
+        raise ValueError(f"{name} must be float32, got {t.dtype}")
+    return t.contiguous()
+
+
+class TileBins:
+    """Result of binning: per-tile offsets (T+1, int64) and sorted primitive ids."""
+
+    def __init__(self, tile_offsets, tile_prims, n_pairs, prim_visible, sort_keys=None):
+        self.tile_offsets = tile_offsets
+        self.tile_prims = tile_prims
+        self.n_pairs = n_pairs
+        self.prim_visible = prim_visible
+        self.sort_keys = sort_keys
+
+
+class Binner:
+    """Owns the binning workspace and the pair capacity estimate.
+
+    pf_bin never waits on the host; like the reference (offsets[-1].item(),
+    rasterize.py:1714) this wrapper reads the pair count once per call and
+    re-bins with a larger capacity if the estimate was too small."""
+
+    def __init__(self, device):
+        self.device = torch.device(device)
+        self.capacity = 0
+        self.ws = None
+
+    def _ensure(self, n_prims, cap):
+        nbytes = _lib.ctypes.c_size_t(0)
+        _lib.call("pf_bin_workspace_size", n_prims, cap, _lib.ctypes.byref(nbytes))
+        if self.ws is None or self.ws.numel() < nbytes.value:
+            self.ws = torch.empty(max(nbytes.value, 256), dtype=torch.uint8, device=self.device)
+
+    def __call__(self, cam_pf, tile_width, spheres, n_prims, num_tiles, return_keys=False, capacity=None):
+        cap = capacity if capacity is not None else max(self.capacity, 4 * n_prims, 1 << 14)
+        while True:
+            self._ensure(n_prims, cap)
+            tile_offsets = torch.empty(num_tiles + 1, dtype=torch.int64, device=self.device)
+            tile_prims = torch.empty(max(cap, 1), dtype=torch.int32, device=self.device)
+            keys = torch.empty(max(cap, 1), dtype=torch.int64, device=self.device) if return_keys else None
+            visible = torch.empty(n_prims, dtype=torch.uint8, device=self.device)
+            scalars = torch.zeros(2, dtype=torch.int64, device=self.device)  # n_pairs, status
+            status = scalars[1:].view(torch.int32)[:1]
+            _lib.call("pf_bin", _lib.ctypes.byref(cam_pf), tile_width, _lib.ptr(spheres), n_prims,
+                      _lib.ptr(self.ws), self.ws.numel(), cap, _lib.ptr(tile_offsets), _lib.ptr(tile_prims),
+                      _lib.ptr(keys), _lib.ptr(visible), _lib.ptr(scalars[:1]), _lib.ptr(status),
+                      _lib.stream_ptr())
+            n = int(scalars[0].item())
+            if n <= cap:
+                break
+            cap = 1 << (int(n * 1.25) - 1).bit_length()
+        self.capacity = max(self.capacity, cap)
+        return TileBins(tile_offsets, tile_prims[:n], n, visible.bool(), keys[:n] if return_keys else None)
+
+
+class Rasterizer:
+    def __init__(self, args, device, attr_dtype="float", tile_width=TILE_WIDTH):
+        self.device = torch.device(device)
+        self.args = args
+        if attr_dtype == "float":
+            self.tscalar = torch.float32
+        elif attr_dtype == "half":
+            self.tscalar = torch.float16
+        else:
+            raise ValueError(f"Unsupported attribute dtype: {attr_dtype}")
+        self.attr_dtype = attr_dtype
+        self.loss_accumulation = args.render_objective == "surface"
+        self.num_texel_sites = args.num_texel_sites
+        if not getattr(args, "is_pinhole", True):
+            raise NotImplementedError("only pinhole cameras are supported by this rasterizer")
+        if tile_width not in (8, 16, 32):
+            raise ValueError("tile_width must be 8, 16 or 32")
+        self.tile_width = tile_width
+        self.binner = Binner(self.device)
+        self.collect_stats = False
+        self.last_stats = None
+        _lib.load()
+
+    # ------------------------------------------------------------------
+    def num_tiles(self, camera):
+        tw = self.tile_width
+        return (1 + (camera.height - 1) // tw) * (1 + (camera.width - 1) // tw)
+
+    def pack(self, points, radii, normals=None, density=None):
+        """(N,4) spheres (centre, radius) and (N,4) normal+density, as
+        rasterize.py:1619-1620 builds them."""
+        n = points.shape[0]
+        spheres = torch.empty((n, 4), dtype=torch.float32, device=self.device)
+        nsig = torch.empty((n, 4), dtype=torch.float32, device=self.device) if normals is not None else None
+        _lib.call("pf_pack_prims", _lib.ptr(_f32(points, "points")), _lib.ptr(_f32(radii, "radii")),
+                  _lib.ptr(None if normals is None else _f32(normals, "normals")),
+                  _lib.ptr(None if density is None else _f32(density, "density")), n, _lib.ptr(spheres),
+                  _lib.ptr(nsig), _lib.stream_ptr())
+        return spheres, nsig
+
+    def bin(self, camera, spheres, return_keys=False):
+        return self.binner(camera.to_pf(), self.tile_width, spheres, spheres.shape[0], self.num_tiles(camera),
+                           return_keys=return_keys)
+
+    def prefetch_adjacency(self, spheres, adjacency, adjacency_offsets):
+        """(E,4) float16 (c_j - c_i, r_j): rasterize.py:580-606."""
+        adj_diff = torch.empty((adjacency.shape[0], 4), dtype=torch.float16, device=self.device)
+        _lib.call("pf_adjacency_prefetch", _lib.ptr(spheres), _lib.ptr(adjacency), _lib.ptr(adjacency_offsets),
+                  spheres.shape[0], _lib.ptr(adj_diff), _lib.stream_ptr())
+        return adj_diff
+
+    def _inputs(self, camera, spheres, nsig, sites, rgb, height, adjacency, adjacency_offsets, adj_diff, bins,
+                depth_quantiles=None, ray_gt=None, thr=1e-3, attr_half=False):
+        inp = _lib.PfRasterInputs()
+        inp.cam = camera.to_pf()
+        inp.tile_width = self.tile_width
+        inp.n_sites = sites.shape[1]
+        inp.n_prims = spheres.shape[0]
+        inp.spheres = _lib.ptr(spheres)
+        inp.nsigmas = _lib.ptr(nsig)
+        inp.texel_sites = _lib.ptr(sites)
+        inp.texel_rgb = _lib.ptr(rgb)
+        inp.texel_height = _lib.ptr(height)
+        inp.attr_half = int(attr_half)
+        inp.adjacency = _lib.ptr(adjacency)
+        inp.adjacency_offsets = _lib.ptr(adjacency_offsets)
+        inp.adjacency_diff = _lib.ptr(adj_diff)
+        inp.tile_offsets = _lib.ptr(bins.tile_offsets)
+        inp.tile_prims = _lib.ptr(bins.tile_prims) if bins.n_pairs > 0 else _lib.ptr(bins.tile_offsets)
+        inp.depth_quantiles = _lib.ptr(depth_quantiles)
+        inp.n_quantiles = 0 if depth_quantiles is None else depth_quantiles.shape[-1]
+        inp.ray_gt = _lib.ptr(ray_gt)
+        inp.transmittance_threshold = float(thr)
+        return inp
+
+    # ------------------------------------------------------------------
+    def _forward(self, grad_ctx, camera, depth_quantiles, points, radii, density, normals, texel_sites, texel_rgb,
+                 texel_height, adjacency, adjacency_offsets, ray_gt, return_point_err,
+                 transmittance_threshold=1e-3):
+        if self.attr_dtype != "float":
+            raise ValueError("Forward pass only supports float precision")
+        if ray_gt is None and self.loss_accumulation:
+            raise ValueError("Ground truth rays must be provided for surface loss accumulation")
+        if ray_gt is None and return_point_err:
+            raise ValueError("Ground truth rays must be provided to return point error")
+        H, W = camera.height, camera.width
+        dev = self.device
+        n = points.shape[0]
+        spheres, nsig = self.pack(points.detach(), radii.detach(), normals.detach(), density.detach())
+        sites = _f32(texel_sites.detach(), "texel_sites")
+        rgb = _f32(texel_rgb.detach(), "texel_rgb")
+        height = _f32(texel_height.detach(), "texel_height")
+        adjacency = adjacency.to(torch.int32).contiguous()
+        adjacency_offsets = adjacency_offsets.to(torch.int32).contiguous()
+        dq = None if depth_quantiles is None else _f32(depth_quantiles.detach(), "depth_quantiles")
+        gt = None if ray_gt is None else _f32(ray_gt.detach(), "ray_gt")
+
+        bins = self.bin(camera, spheres)
+        adj_diff = self.prefetch_adjacency(spheres, adjacency, adjacency_offsets)
+
+        color = torch.empty((H, W, 3), dtype=torch.float32, device=dev)
+        log_t = torch.empty((H, W), dtype=torch.float32, device=dev)
+        nd = torch.empty((H, W), dtype=torch.float32, device=dev)
+        normal = torch.empty((H, W, 3), dtype=torch.float32, device=dev)
+        contrib = torch.empty(n, dtype=torch.float32, device=dev)
+        qd = torch.empty(dq.shape, dtype=torch.float32, device=dev) if dq is not None else None
+        perr = torch.empty(n, dtype=torch.float32, device=dev) if return_point_err else None
+        err = torch.empty((H, W), dtype=torch.float32, device=dev) if self.loss_accumulation else None
+        early_stop = torch.empty(self.num_tiles(camera), dtype=torch.int32, device=dev)
+        stats = torch.empty(self.num_tiles(camera), dtype=torch.int32, device=dev) if self.collect_stats else None
+        inp = self._inputs(camera, spheres, nsig, sites, rgb, height, adjacency, adjacency_offsets, adj_diff, bins,
+                           dq, gt, transmittance_threshold)
+        _timed_call("pf_raster_forward", _lib.ctypes.byref(inp), int(bool(return_point_err)), _lib.ptr(color),
+                    _lib.ptr(log_t), _lib.ptr(nd), _lib.ptr(normal), _lib.ptr(qd), _lib.ptr(err), _lib.ptr(contrib),
+                    _lib.ptr(perr), _lib.ptr(early_stop), _lib.ptr(stats), _lib.stream_ptr())
+        if self.collect_stats:
+            self.last_stats = dict(bins=bins, early_stop=early_stop, contrib_pairs=stats,
+                                   adjacency_offsets=adjacency_offsets, camera=camera, n_prims=n)
+
+        if grad_ctx is not None:
+            grad_ctx.rasterizer = self
+            grad_ctx.camera = camera
+            grad_ctx.n_inputs = 14 if transmittance_threshold == 1e-3 else 15
+            grad_ctx.thr = transmittance_threshold
+            grad_ctx.bins = bins
+            grad_ctx.save_for_backward(dq, spheres, nsig, sites, rgb, height, adjacency, adjacency_offsets,
+                                       adj_diff, early_stop, log_t)
+        opacity = 1.0 - torch.exp(log_t)
+        return color, opacity, nd, normal, qd, err, contrib, perr, bins.prim_visible
+
+    def forward(self, *args):
+        return RasterGradFn.apply(self, *args)
+
+    def _backward(self, grad_ctx, grad_color_in, grad_opacity_in, grad_normal_distance_in, grad_normal_in,
+                  grad_quantile_depths_in, grad_err_in, grad_contrib_in, grad_point_err_in,
+                  grad_prim_visible_mask_in):
+        del grad_point_err_in, grad_prim_visible_mask_in
+        if self.attr_dtype != "float":
+            raise ValueError("Backward pass only supports float precision")
+        if self.loss_accumulation:
+            raise NotImplementedError()
+        (dq, spheres, nsig, sites, rgb, height, adjacency, adjacency_offsets, adj_diff, early_stop,
+         log_t) = grad_ctx.saved_tensors
+        camera = grad_ctx.camera
+        n = spheres.shape[0]
+        S = sites.shape[1]
+        dev = self.device
+
+        def g(t, shape):
+            return torch.zeros(shape, dtype=torch.float32, device=dev) if t is None else _f32(t, "grad")
+
+        H, W = camera.height, camera.width
+        gc = g(grad_color_in, (H, W, 3))
+        go = g(grad_opacity_in, (H, W))
+        gnd = None if grad_normal_distance_in is None else _f32(grad_normal_distance_in, "grad")
+        gn = None if grad_normal_in is None else _f32(grad_normal_in, "grad")
+        gq = None if (grad_quantile_depths_in is None or dq is None) else _f32(grad_quantile_depths_in, "grad")
+        gcon = None if grad_contrib_in is None else _f32(grad_contrib_in, "grad")
+        out = dict(points=torch.empty((n, 3), dtype=torch.float32, device=dev),
+                   radii=torch.empty(n, dtype=torch.float32, device=dev),
+                   normals=torch.empty((n, 3), dtype=torch.float32, device=dev),
+                   density=torch.empty(n, dtype=torch.float32, device=dev),
+                   sites=torch.empty((n, S, 3), dtype=torch.float32, device=dev),
+                   rgb=torch.empty((n, S, 3), dtype=torch.float32, device=dev),
+                   height=torch.empty((n, S), dtype=torch.float32, device=dev))
+        inp = self._inputs(camera, spheres, nsig, sites, rgb, height, adjacency, adjacency_offsets, adj_diff,
+                           grad_ctx.bins, dq, None, grad_ctx.thr)
+        _timed_call("pf_raster_backward", _lib.ctypes.byref(inp), _lib.ptr(early_stop), _lib.ptr(log_t), _lib.ptr(gc),
+                    _lib.ptr(go), _lib.ptr(gnd), _lib.ptr(gn), _lib.ptr(gq), _lib.ptr(gcon), _lib.ptr(out["points"]),
+                    _lib.ptr(out["radii"]), _lib.ptr(out["normals"]), _lib.ptr(out["density"]),
+                    _lib.ptr(out["sites"]), _lib.ptr(out["rgb"]), _lib.ptr(out["height"]), _lib.stream_ptr())
+        del grad_ctx.rasterizer, grad_ctx.camera, grad_ctx.bins
+        grads = (None, None, None, out["points"], out["radii"], out["density"], out["normals"], out["sites"],
+                 out["rgb"], out["height"], None, None, None, None)
+        return grads + (None,) * (grad_ctx.n_inputs - 14)
+
+    # ------------------------------------------------------------------
+    def benchmark(self, camera, points, radii, density, normals, texel_sites, texel_rgb, texel_height, adjacency,
+                  adjacency_offsets, adjacency_diff, transmittance_threshold=1e-3):
+        """Forward colour only, (dc, dpm)-encoded neighbours, attributes in
+        attr_dtype (rasterize.py:1982-2131)."""
+        H, W = camera.height, camera.width
+        spheres, _ = self.pack(points.float().contiguous(), radii.float().contiguous())
+        nsig = torch.cat([normals, density[:, None]], dim=-1).to(self.tscalar).contiguous()
+        sites = texel_sites.to(self.tscalar).contiguous()
+        rgb = texel_rgb.to(self.tscalar).contiguous()
+        height = texel_height.to(self.tscalar).contiguous()
+        bins = self.bin(camera, spheres)
+        color = torch.empty((H, W, 3), dtype=torch.float32, device=self.device)
+        inp = self._inputs(camera, spheres, nsig, sites, rgb, height, adjacency.to(torch.int32).contiguous(),
+                           adjacency_offsets.to(torch.int32).contiguous(), adjacency_diff.contiguous(), bins,
+                           thr=transmittance_threshold, attr_half=self.attr_dtype == "half")
+        _lib.call("pf_raster_benchmark", _lib.ctypes.byref(inp), _lib.ptr(color), _lib.stream_ptr())
+        return color
+
+    def visualize(self, camera, points, radii, density, normals, texel_sites, texel_rgb, texel_height, adjacency,
+                  adjacency_offsets, vis_options=None):
+        """(color, depth, normal, alpha, intersections), rasterize.py:2133-2285;
+        written to device buffers (no graphics API)."""
+        if vis_options is None:
+            vis_options = VisOptions()
+        H, W = camera.height, camera.width
+        dev = self.device
+        spheres, _ = self.pack(points.float().contiguous(), radii.float().contiguous())
+        nsig = torch.cat([normals, density[:, None]], dim=-1).to(self.tscalar).contiguous()
+        sites = texel_sites.to(self.tscalar).contiguous()
+        rgb = texel_rgb.to(self.tscalar).contiguous()
+        height = texel_height.to(self.tscalar).contiguous()
+        adjacency = adjacency.to(torch.int32).contiguous()
+        adjacency_offsets = adjacency_offsets.to(torch.int32).contiguous()
+        bins = self.bin(camera, spheres)
+        adj_diff = self.prefetch_adjacency(spheres, adjacency, adjacency_offsets)
+        color = torch.empty((H, W, 3), dtype=torch.float32, device=dev)
+        depth = torch.empty((H, W), dtype=torch.float32, device=dev)
+        normal = torch.empty((H, W, 3), dtype=torch.float32, device=dev)
+        alpha = torch.empty((H, W), dtype=torch.float32, device=dev)
+        inter = torch.empty((H, W), dtype=torch.int32, device=dev)
+        inp = self._inputs(camera, spheres, nsig, sites, rgb, height, adjacency, adjacency_offsets, adj_diff, bins,
+                           thr=vis_options.transmittance_threshold, attr_half=self.attr_dtype == "half")
+        b = [float(x) for x in vis_options.bkgd_color]
+        _lib.call("pf_raster_visualize", _lib.ctypes.byref(inp), int(vis_options.max_intersections),
+                  float(vis_options.depth_quantile), b[0], b[1], b[2], _lib.ptr(color), _lib.ptr(depth),
+                  _lib.ptr(normal), _lib.ptr(alpha), _lib.ptr(inter), _lib.stream_ptr())
+        return color, depth, normal, alpha, inter

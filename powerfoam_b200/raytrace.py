@@ -1,0 +1,117 @@
+"""Cell-walk ray tracer: drop-in for powerfoam/raytrace.py.
+
+``RayTracer(args, device, attr_dtype).benchmark(...)`` keeps the reference's
+signature and returns the colour image (raytrace.py:247-309).  ``trace``
+exposes the extensions of the walk kernel: per-ray start cells, a step cap,
+depth / normal / log transmittance and the visited-cell log.
+"""
+
+from dataclasses import dataclass
+
+import torch
+
+from . import _lib
+
+DEFAULT_MAX_STEPS = 1 << 16
+
+
+@dataclass
+class TraceResult:
+    color: torch.Tensor
+    log_t: torch.Tensor
+    depth: torch.Tensor
+    normal: torch.Tensor
+    depth_seg: torch.Tensor
+    depth_sigma: torch.Tensor
+    visit_count: torch.Tensor
+    visits: torch.Tensor = None
+    status: int = 0
+
+
+class RayTracer:
+    def __init__(self, args, device, attr_dtype="float"):
+        self.device = torch.device(device)
+        self.args = args
+        if attr_dtype == "float":
+            self.tscalar = torch.float32
+        elif attr_dtype == "half":
+            self.tscalar = torch.float16
+        else:
+            raise ValueError(f"Unsupported attribute dtype: {attr_dtype}")
+        self.attr_dtype = attr_dtype
+        self.num_texel_sites = args.num_texel_sites
+        _lib.load()
+
+    def _inputs(self, camera, start, spheres, nsig, sites, rgb, height, adjacency, adjacency_offsets,
+                adjacency_diff, thr, max_steps, depth_quantile):
+        inp = _lib.PfTraceInputs()
+        inp.cam = camera.to_pf()
+        inp.n_sites = sites.shape[1]
+        inp.attr_half = int(self.attr_dtype == "half")
+        inp.n_prims = spheres.shape[0]
+        inp.spheres = _lib.ptr(spheres)
+        inp.nsigmas = _lib.ptr(nsig)
+        inp.texel_sites = _lib.ptr(sites)
+        inp.texel_rgb = _lib.ptr(rgb)
+        inp.texel_height = _lib.ptr(height)
+        inp.adjacency = _lib.ptr(adjacency)
+        inp.adjacency_offsets = _lib.ptr(adjacency_offsets)
+        inp.adjacency_diff = _lib.ptr(adjacency_diff)
+        if isinstance(start, torch.Tensor) and start.numel() > 1:
+            inp.start_idx = 0
+            inp.start_cells = _lib.ptr(start)
+        else:
+            inp.start_idx = int(start)
+            inp.start_cells = None
+        inp.transmittance_threshold = float(thr)
+        inp.max_steps = int(max_steps)
+        inp.depth_quantile = float(depth_quantile)
+        return inp
+
+    def _prep(self, points, radii, density, normals, texel_sites, texel_rgb, texel_height, adjacency,
+              adjacency_offsets, adjacency_diff):
+        spheres = torch.cat([points, radii[:, None]], dim=-1).to(torch.float32).contiguous()
+        nsig = torch.cat([normals, density[:, None]], dim=-1).to(self.tscalar).contiguous()
+        return (spheres, nsig, texel_sites.to(self.tscalar).contiguous(), texel_rgb.to(self.tscalar).contiguous(),
+                texel_height.to(self.tscalar).contiguous(), adjacency.to(torch.int32).contiguous(),
+                adjacency_offsets.to(torch.int32).contiguous(), adjacency_diff.contiguous())
+
+    def trace(self, camera, start, points, radii, density, normals, texel_sites, texel_rgb, texel_height, adjacency,
+              adjacency_offsets, adjacency_diff, transmittance_threshold=1e-3, max_steps=DEFAULT_MAX_STEPS,
+              depth_quantile=0.5, visit_cap=0, check_status=True):
+        """Walk every pixel's ray.  ``start`` is one cell index or an (H, W)
+        int32 tensor of per-ray start cells."""
+        H, W = camera.height, camera.width
+        dev = self.device
+        args = self._prep(points, radii, density, normals, texel_sites, texel_rgb, texel_height, adjacency,
+                          adjacency_offsets, adjacency_diff)
+        if isinstance(start, torch.Tensor) and start.numel() > 1:
+            start = start.to(torch.int32).contiguous()
+        r = TraceResult(
+            color=torch.empty((H, W, 3), dtype=torch.float32, device=dev),
+            log_t=torch.empty((H, W), dtype=torch.float32, device=dev),
+            depth=torch.empty((H, W), dtype=torch.float32, device=dev),
+            normal=torch.empty((H, W, 3), dtype=torch.float32, device=dev),
+            depth_seg=torch.empty((H, W), dtype=torch.int32, device=dev),
+            depth_sigma=torch.empty((H, W), dtype=torch.float32, device=dev),
+            visit_count=torch.empty((H, W), dtype=torch.int32, device=dev),
+            visits=torch.empty((H, W, visit_cap), dtype=torch.int32, device=dev) if visit_cap else None,
+        )
+        status = torch.zeros(1, dtype=torch.int32, device=dev)
+        inp = self._inputs(camera, start, *args, transmittance_threshold, max_steps, depth_quantile)
+        _lib.call("pf_trace_forward", _lib.ctypes.byref(inp), _lib.ptr(r.color), _lib.ptr(r.log_t),
+                  _lib.ptr(r.depth), _lib.ptr(r.normal), _lib.ptr(r.depth_seg), _lib.ptr(r.depth_sigma),
+                  _lib.ptr(r.visits), int(visit_cap), _lib.ptr(r.visit_count), _lib.ptr(status), _lib.stream_ptr())
+        if check_status:
+            r.status = int(status.item())
+            if r.status != _lib.PF_OK:
+                raise _lib.PfError(r.status, "cell walk stopped early (step cap or invalid cell index)")
+        return r
+
+    def benchmark(self, camera, start_point_idx, points, radii, density, normals, texel_sites, texel_rgb,
+                  texel_height, adjacency, adjacency_offsets, adjacency_diff, transmittance_threshold=1e-3):
+        """raytrace.py:247-309: colour of every ray walked from start_point_idx."""
+        r = self.trace(camera, start_point_idx, points, radii, density, normals, texel_sites, texel_rgb,
+                       texel_height, adjacency, adjacency_offsets, adjacency_diff, transmittance_threshold,
+                       check_status=False)
+        return r.color

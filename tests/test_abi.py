@@ -1,0 +1,49 @@
+"""The C-ABI library builds, loads and exports every entry point that
+include/pfoam.h declares (no compute calls: this runs without a GPU)."""
+
+import ctypes
+import os
+import re
+
+from tests.conftest import ROOT
+
+
+def declared_symbols():
+    src = open(os.path.join(ROOT, "include", "pfoam.h")).read()
+    return sorted(set(re.findall(r"^PF_API\s+[\w\s\*]+?\b(pf_\w+)\s*\(", src, flags=re.M)))
+
+
+def test_header_declares_entry_points():
+    syms = declared_symbols()
+    assert "pf_raster_forward" in syms and "pf_raster_backward" in syms and "pf_bin" in syms
+    assert len(syms) >= 15
+
+
+def test_library_exports_every_declared_symbol():
+    from powerfoam_b200 import _lib
+
+    lib = _lib.load()
+    for s in declared_symbols():
+        assert hasattr(lib, s), s
+    assert lib.pf_abi_version() == 1
+    # every binding in the Python layer names a declared symbol
+    assert set(_lib.exported_symbols()) <= set(declared_symbols())
+
+
+def test_argument_errors_are_reported_without_a_gpu():
+    from powerfoam_b200 import _lib
+
+    lib = _lib.load()
+    n = ctypes.c_size_t(0)
+    assert lib.pf_bin_workspace_size(-1, 0, ctypes.byref(n)) == _lib.PF_ERR_ARGS
+    assert b"bad arguments" in lib.pf_last_error()
+    assert lib.pf_bin_workspace_size(1000, 5000, ctypes.byref(n)) == 0 and n.value > 0
+    assert lib.pf_raster_forward(None, 0, *([None] * 11)) == _lib.PF_ERR_ARGS
+
+
+def test_oracle_library_loads():
+    from oracle import oracle as orc
+
+    lib = orc.lib()
+    for s in ["orc_bin_f32", "orc_raster_forward_f32", "orc_raster_backward_f64", "orc_trace_forward_f32"]:
+        assert hasattr(lib, s)

@@ -1,0 +1,98 @@
+"""Cell-walk tracer parity: visited-cell sequences bit-exact against the
+reference-source golden vectors and the oracle; colour max-abs 1e-5; step cap
+reported as a status, never a hang."""
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import oracle as orc
+from powerfoam_b200 import _lib
+from powerfoam_b200.adjacency import build_power_adjacency, power_adjacency_diff, start_cell
+from powerfoam_b200.raytrace import RayTracer
+from tests.helpers import max_abs, np_camera, np_scene, orc_cam, packed, to_t, torch_cam
+
+pytestmark = pytest.mark.gpu
+
+
+class Args:
+    num_texel_sites = 8
+
+
+def test_trace_matches_golden(golden):
+    g = golden("trace_small")
+    cam = dict(eye=g["cam_eye"], right=g["cam_right"], up=g["cam_up"], width=int(g["width"]), height=int(g["height"]))
+    t = {k: to_t(g[k]) for k in ["points", "radii", "density", "normals", "texel_sites", "texel_rgb", "texel_height"]}
+    s = start_cell(t["points"], t["radii"], torch.from_numpy(g["cam_eye"]))
+    assert s == int(g["start_idx"])
+    pm = power_adjacency_diff(t["points"], t["radii"], to_t(g["adjacency"]), to_t(g["adjacency_offsets"]))
+    assert np.array_equal(pm.cpu().numpy().view(np.uint16), g["adjacency_diff_pm"])
+    R = RayTracer(Args(), "cuda")
+    r = R.trace(torch_cam(cam), s, t["points"], t["radii"], t["density"], t["normals"], t["texel_sites"],
+                t["texel_rgb"], t["texel_height"], to_t(g["adjacency"]), to_t(g["adjacency_offsets"]), pm,
+                float(g["thr"]), visit_cap=g["visits"].shape[-1])
+    assert np.array_equal(r.visit_count.cpu().numpy(), g["visit_count"])
+    assert np.array_equal(r.visits.cpu().numpy(), g["visits"])
+    assert max_abs(r.color.cpu(), g["color"]) <= 1e-5
+    c = R.benchmark(torch_cam(cam), s, t["points"], t["radii"], t["density"], t["normals"], t["texel_sites"],
+                    t["texel_rgb"], t["texel_height"], to_t(g["adjacency"]), to_t(g["adjacency_offsets"]), pm,
+                    float(g["thr"]))
+    assert max_abs(c.cpu(), g["color"]) <= 1e-5
+
+
+@pytest.mark.parametrize("half", [False, True])
+@pytest.mark.parametrize("seed", [0, 1])
+def test_trace_matches_oracle(seed, half):
+    sc = np_scene(50 + seed, 400, -0.6, 0.6, 0.05, 0.15)
+    cam = np_camera((0.3, 0.2 * seed, 2.2), (0, 0, 0), 40, 30, 55.0)
+    tp = {k: to_t(v) for k, v in sc.items()}
+    adj, off = build_power_adjacency(tp["points"], tp["radii"])
+    adj_np, off_np = adj.cpu().numpy(), off.cpu().numpy()
+    pm = power_adjacency_diff(tp["points"], tp["radii"], adj, off)
+    s = start_cell(tp["points"], tp["radii"], torch.from_numpy(cam["eye"]))
+    assert s == orc.start_cell(sc["points"], sc["radii"], cam["eye"])
+    R = RayTracer(Args(), "cuda", "half" if half else "float")
+    r = R.trace(torch_cam(cam), s, tp["points"], tp["radii"], tp["density"], tp["normals"], tp["texel_sites"],
+                tp["texel_rgb"], tp["texel_height"], adj, off, pm, 1e-3, visit_cap=96)
+    sph, nsig, _ = packed(sc)
+    h = (lambda a: a.astype(np.float16).astype(np.float32)) if half else (lambda a: a)
+    o = orc.trace_forward(orc_cam(cam), sph, h(nsig), h(sc["texel_sites"]), h(sc["texel_rgb"]), h(sc["texel_height"]),
+                          adj_np, off_np, pm.cpu().numpy().view(np.uint16), s, thr=1e-3, visit_cap=96)
+    assert np.array_equal(r.visit_count.cpu().numpy(), o["visit_count"])
+    assert np.array_equal(r.visits.cpu().numpy(), o["visits"])
+    for k in ["color", "log_t", "depth", "normal"]:
+        assert max_abs(getattr(r, k).cpu(), o[k]) <= 1e-5, k
+    assert np.array_equal(r.depth_seg.cpu().numpy(), o["depth_seg"])
+
+
+def test_trace_step_cap_is_reported():
+    sc = np_scene(60, 300, -0.6, 0.6, 0.05, 0.15)
+    cam = np_camera((0.0, 0.0, 2.2), (0, 0, 0), 24, 16, 55.0)
+    tp = {k: to_t(v) for k, v in sc.items()}
+    adj, off = build_power_adjacency(tp["points"], tp["radii"])
+    pm = power_adjacency_diff(tp["points"], tp["radii"], adj, off)
+    s = start_cell(tp["points"], tp["radii"], torch.from_numpy(cam["eye"]))
+    R = RayTracer(Args(), "cuda")
+    args = (torch_cam(cam), s, tp["points"], tp["radii"], tp["density"], tp["normals"], tp["texel_sites"],
+            tp["texel_rgb"], tp["texel_height"], adj, off, pm, 1e-3)
+    with pytest.raises(_lib.PfError) as e:
+        R.trace(*args, max_steps=2)
+    assert e.value.code == _lib.PF_ERR_STEP_CAP
+    r = R.trace(*args, max_steps=2, check_status=False)
+    assert int(r.visit_count.max().item()) <= 2
+
+
+def test_per_ray_start_cells():
+    sc = np_scene(61, 300, -0.6, 0.6, 0.05, 0.15)
+    cam = np_camera((0.1, 0.0, 2.2), (0, 0, 0), 24, 20, 55.0)
+    tp = {k: to_t(v) for k, v in sc.items()}
+    adj, off = build_power_adjacency(tp["points"], tp["radii"])
+    pm = power_adjacency_diff(tp["points"], tp["radii"], adj, off)
+    s = start_cell(tp["points"], tp["radii"], torch.from_numpy(cam["eye"]))
+    R = RayTracer(Args(), "cuda")
+    base = (tp["points"], tp["radii"], tp["density"], tp["normals"], tp["texel_sites"], tp["texel_rgb"],
+            tp["texel_height"], adj, off, pm, 1e-3)
+    a = R.trace(torch_cam(cam), s, *base)
+    cells = torch.full((20, 24), s, dtype=torch.int32, device="cuda")
+    b = R.trace(torch_cam(cam), cells, *base)
+    assert torch.equal(a.color, b.color)
