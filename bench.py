@@ -49,6 +49,8 @@ def parse():
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--tile", type=int, default=8)
+    p.add_argument("--workload", default=WORKLOAD, help="raster1m (the measured configuration) or raster256k "
+                   "(a quarter-size case with the same density per pixel, for profiling)")
     p.add_argument("--cpu-sample-tiles", type=int, default=0, help="tiles composited by the CPU baseline")
     p.add_argument("--no-cpu-baseline", action="store_true")
     return p.parse_args()
@@ -116,11 +118,11 @@ class ClockSampler:
 
 
 # ----------------------------------------------------------------------------
-def build_workload(device, seed_offset=0, tile=8):
+def build_workload(device, seed_offset=0, tile=8, workload=WORKLOAD):
     from powerfoam_b200 import synthetic
     from powerfoam_b200.adjacency import CechBuilder
 
-    cfg = synthetic.CONFIGS[WORKLOAD]
+    cfg = synthetic.CONFIGS[workload]
     scene = synthetic.make_scene(cfg["n"], seed=cfg["seed"], mixture=cfg["mixture"], sigma=cfg["sigma"],
                                  r_range=cfg["r_range"], device=device)
     cam = synthetic.orbit_camera(100 + seed_offset, cfg["width"], cfg["height"], cfg["vfov"], device=device)
@@ -231,7 +233,7 @@ def reference_arm(args, rank, world):
 
     orc.build()
     dev = "cuda" if torch.cuda.is_available() else "cpu"
-    cfg, scene, cam, adj, adj_off, target = build_workload(dev, 0, args.tile)
+    cfg, scene, cam, adj, adj_off, target = build_workload(dev, 0, args.tile, args.workload)
     sample = args.cpu_sample_tiles or 200
     for _ in range(args.warmup):
         cpu_baseline(cfg, scene, cam, adj, adj_off, target, max(sample // 10, 1), args.tile)
@@ -242,7 +244,7 @@ def reference_arm(args, rank, world):
     line = dict(metric=METRIC, value=v, unit=UNIT, n_gpus=world, steps=args.steps, warmup=args.warmup,
                 ms_per_step=1000.0 / v, higher_is_better=True, scaling="weak", vs_baseline=None, dtype="f32",
                 data="synthetic", impl="reference",
-                config=dict(workload=WORKLOAD, prims=cfg["n"], width=cfg["width"], height=cfg["height"],
+                config=dict(workload=args.workload, prims=cfg["n"], width=cfg["width"], height=cfg["height"],
                             tile=args.tile, parallelism="cpu-openmp"),
                 cpu_baseline=cb, e2e=dict(value=v, unit=UNIT, h2d_bytes_per_step=0, d2h_bytes_per_step=0))
     print(json.dumps(line), flush=True)
@@ -264,7 +266,7 @@ def main():
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
     from powerfoam_b200 import rasterize
 
-    cfg, scene, cam, adj, adj_off, target = build_workload(dev, rank, args.tile)
+    cfg, scene, cam, adj, adj_off, target = build_workload(dev, rank, args.tile, args.workload)
     target_dev = target.to(dev)
     R = rasterize.Rasterizer(Args(), dev, tile_width=args.tile)
     step, params = make_step(R, scene, cam, adj, adj_off, target_dev, world)
@@ -348,7 +350,7 @@ def main():
     line = dict(metric=METRIC, value=value, unit=UNIT, n_gpus=world, steps=args.steps, warmup=max(args.warmup, 3),
                 ms_per_step=ms, higher_is_better=True, scaling="weak", vs_baseline=None, dtype="f32",
                 data="synthetic (seeded scene, orbit camera, uniform target)",
-                config=dict(workload=WORKLOAD, prims=cfg["n"], width=cfg["width"], height=cfg["height"],
+                config=dict(workload=args.workload, prims=cfg["n"], width=cfg["width"], height=cfg["height"],
                             tile=args.tile, vfov=cfg["vfov"], pairs=st["pairs"], visited_pairs=st["V"],
                             l2="inputs larger than L2 (256 MB of primitive records), no flush",
                             parallelism=f"view-dp{world}"),

@@ -76,6 +76,11 @@ typedef struct pf_raster_inputs {
     int32_t n_quantiles;
     const float *ray_gt;         /* (H,W,3) or NULL */
     float transmittance_threshold;
+    const int32_t *tile_order;   /* (T) tile processing order (longest lists
+                                    first, from pf_bin) or NULL */
+    void *scratch;               /* >= 256 bytes of device scratch for the
+                                    tile work queue, or NULL (one warp group
+                                    per tile, no queue) */
 } pf_raster_inputs;
 
 /* ---------------------------------------------------------------------- */
@@ -97,10 +102,11 @@ PF_API int pf_pack_prims(const float *points, const float *radii, const float *n
  * ascending primitive index (the reference leaves ties unordered).
  * On overflow (*n_pairs > pair_capacity) the tile lists are emptied and
  * *status is set to PF_ERR_OVERFLOW; *n_pairs always holds the true count. */
-PF_API int pf_bin_workspace_size(int64_t n_prims, int64_t pair_capacity, size_t *bytes);
+PF_API int pf_bin_workspace_size(int64_t n_prims, int64_t pair_capacity, int64_t n_tiles, size_t *bytes);
 PF_API int pf_bin(const pf_camera *cam, int32_t tile_width, const float *spheres, int64_t n_prims, void *workspace,
            size_t workspace_bytes, int64_t pair_capacity, int64_t *tile_offsets, int32_t *tile_prims,
            int64_t *sort_keys /* (capacity) or NULL */, uint8_t *prim_visible /* (N) or NULL */,
+           int32_t *tile_order /* (T) or NULL: tiles by decreasing list length */,
            int64_t *n_pairs /* device scalar */, int32_t *status /* device scalar */, void *stream);
 
 /* ---------------------------------------------------------------------- */

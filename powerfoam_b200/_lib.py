@@ -60,6 +60,8 @@ class PfRasterInputs(ctypes.Structure):
         ("n_quantiles", c_i32),
         ("ray_gt", c_vp),
         ("transmittance_threshold", c_f),
+        ("tile_order", c_vp),
+        ("scratch", c_vp),
     ]
 
 
@@ -89,9 +91,9 @@ class PfTraceInputs(ctypes.Structure):
 _SIGS = {
     "pf_abi_version": [],
     "pf_pack_prims": [c_vp, c_vp, c_vp, c_vp, c_i64, c_vp, c_vp, c_vp],
-    "pf_bin_workspace_size": [c_i64, c_i64, ctypes.POINTER(ctypes.c_size_t)],
+    "pf_bin_workspace_size": [c_i64, c_i64, c_i64, ctypes.POINTER(ctypes.c_size_t)],
     "pf_bin": [ctypes.POINTER(PfCamera), c_i32, c_vp, c_i64, c_vp, ctypes.c_size_t, c_i64, c_vp, c_vp, c_vp, c_vp,
-               c_vp, c_vp, c_vp],
+               c_vp, c_vp, c_vp, c_vp],
     "pf_adjacency_prefetch": [c_vp, c_vp, c_vp, c_i64, c_vp, c_vp],
     "pf_adjacency_power_diff": [c_vp, c_vp, c_vp, c_vp, c_i64, c_vp, c_vp],
     "pf_raster_forward": [ctypes.POINTER(PfRasterInputs), c_i32, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp,

@@ -193,6 +193,17 @@ __global__ void tile_ranges_kernel(const uint32_t* __restrict__ tile_key, const 
     if (i < n && sort_keys) sort_keys[i] = ((int64_t)tile_key[i] << 32) | (int64_t)depth_key[prims[i]];
 }
 
+// keys for the tile processing order: longest lists first, ties by tile index
+__global__ void tile_len_key_kernel(const int64_t* __restrict__ tile_offsets, int64_t T, uint32_t* __restrict__ key,
+                                    uint32_t* __restrict__ idx) {
+    int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= T) return;
+    int64_t len = tile_offsets[t + 1] - tile_offsets[t];
+    if (len > 0xFFFFFF) len = 0xFFFFFF;
+    key[t] = 0xFFFFFFu - (uint32_t)len;
+    idx[t] = (uint32_t)t;
+}
+
 __global__ void pack_prims_kernel(const float* __restrict__ points, const float* __restrict__ radii,
                                   const float* __restrict__ normals, const float* __restrict__ density, int64_t N,
                                   float4* __restrict__ spheres, float4* __restrict__ nsigmas) {
@@ -204,14 +215,14 @@ __global__ void pack_prims_kernel(const float* __restrict__ points, const float*
 
 // ---------------------------------------------------------------------------
 struct BinLayout {
-    size_t counts, dprim, dkey0, idx0, dkey1, idx1, scounts, offsets, spart, pkey0, pprim0, pkey1, pprim1, rhist, rpart,
-        total;
+    size_t counts, dprim, dkey0, idx0, dkey1, idx1, scounts, offsets, spart, pkey0, pprim0, pkey1, pprim1, tk0, tv0,
+        tk1, tv1, rhist, rpart, total;
     size_t bytes;
 };
 
 static size_t align_up(size_t x) { return (x + 255) & ~(size_t)255; }
 
-static BinLayout bin_layout(int64_t N, int64_t cap) {
+static BinLayout bin_layout(int64_t N, int64_t cap, int64_t T) {
     BinLayout L;
     size_t o = 0;
     auto take = [&](size_t b) {
@@ -232,7 +243,13 @@ static BinLayout bin_layout(int64_t N, int64_t cap) {
     L.pprim0 = take(4 * (size_t)cap);
     L.pkey1 = take(4 * (size_t)cap);
     L.pprim1 = take(4 * (size_t)cap);
-    int64_t rb = radix_blocks(cap > N ? cap : N);
+    L.tk0 = take(4 * (size_t)T);
+    L.tv0 = take(4 * (size_t)T);
+    L.tk1 = take(4 * (size_t)T);
+    L.tv1 = take(4 * (size_t)T);
+    int64_t mx = cap > N ? cap : N;
+    mx = mx > T ? mx : T;
+    int64_t rb = radix_blocks(mx);
     L.rhist = take(4 * (size_t)(256 * rb));
     L.rpart = take(4 * (size_t)(scan_blocks(256 * rb) + 1));
     L.total = take(8);
@@ -244,10 +261,10 @@ static BinLayout bin_layout(int64_t N, int64_t cap) {
 
 using namespace pf;
 
-extern "C" int pf_bin_workspace_size(int64_t n_prims, int64_t pair_capacity, size_t* bytes) {
-    if (n_prims < 0 || pair_capacity < 0 || pair_capacity >= (int64_t)1 << 31 || !bytes)
+extern "C" int pf_bin_workspace_size(int64_t n_prims, int64_t pair_capacity, int64_t n_tiles, size_t* bytes) {
+    if (n_prims < 0 || pair_capacity < 0 || pair_capacity >= (int64_t)1 << 31 || n_tiles < 0 || !bytes)
         return pf_fail(PF_ERR_ARGS, "pf_bin_workspace_size: bad arguments");
-    *bytes = bin_layout(n_prims, pair_capacity).bytes;
+    *bytes = bin_layout(n_prims, pair_capacity, n_tiles).bytes;
     return PF_OK;
 }
 
@@ -265,13 +282,14 @@ extern "C" int pf_pack_prims(const float* points, const float* radii, const floa
 
 extern "C" int pf_bin(const pf_camera* cam, int32_t tile_width, const float* spheres, int64_t n_prims,
                       void* workspace, size_t workspace_bytes, int64_t pair_capacity, int64_t* tile_offsets,
-                      int32_t* tile_prims, int64_t* sort_keys, uint8_t* prim_visible, int64_t* n_pairs,
-                      int32_t* status, void* stream) {
+                      int32_t* tile_prims, int64_t* sort_keys, uint8_t* prim_visible, int32_t* tile_order,
+                      int64_t* n_pairs, int32_t* status, void* stream) {
     if (!cam || tile_width <= 0 || n_prims < 0 || pair_capacity < 0 || pair_capacity >= (int64_t)1 << 31 ||
         !tile_offsets || !n_pairs || !status || (n_prims > 0 && !spheres) || (pair_capacity > 0 && !tile_prims))
         return pf_fail(PF_ERR_ARGS, "pf_bin: bad arguments");
     if (cam->width < 2 || cam->height < 2) return pf_fail(PF_ERR_ARGS, "pf_bin: image must be at least 2x2");
-    BinLayout L = bin_layout(n_prims, pair_capacity);
+    const int64_t T_ = (int64_t)(1 + (cam->height - 1) / tile_width) * (1 + (cam->width - 1) / tile_width);
+    BinLayout L = bin_layout(n_prims, pair_capacity, T_);
     if (workspace_bytes < L.bytes || (!workspace && L.bytes)) return pf_fail(PF_ERR_ARGS, "pf_bin: workspace too small");
     cudaStream_t st = (cudaStream_t)stream;
     char* ws = (char*)workspace;
@@ -293,9 +311,18 @@ extern "C" int pf_bin(const pf_camera* cam, int32_t tile_width, const float* sph
     const int64_t tiles_h = 1 + (cam->height - 1) / TW, tiles_w = 1 + (cam->width - 1) / TW;
     const int64_t T = tiles_h * tiles_w;
     if (prim_visible && n_prims) cudaMemsetAsync(prim_visible, 0, (size_t)n_prims, st);
+    auto order = [&]() {
+        if (!tile_order || T == 0) return;
+        uint32_t *tk0 = (uint32_t*)(ws + L.tk0), *tv0 = (uint32_t*)(ws + L.tv0);
+        uint32_t *tk1 = (uint32_t*)(ws + L.tk1), *tv1 = (uint32_t*)(ws + L.tv1);
+        tile_len_key_kernel<<<(unsigned)((T + 255) / 256), 256, 0, st>>>(tile_offsets, T, tk0, tv0);
+        uint32_t* kf = radix_final_key_buffer(tk0, tk1, 24);
+        radix_sort_pairs(tk0, tv0, tk1, tv1, kf, (uint32_t*)tile_order, T, nullptr, 24, rs, st);
+    };
     if (n_prims == 0) {
         cudaMemsetAsync(n_pairs, 0, 8, st);
         cudaMemsetAsync(tile_offsets, 0, 8 * (size_t)(T + 1), st);
+        order();
         return pf_check_launch("pf_bin");
     }
     const unsigned gN = (unsigned)((n_prims + 255) / 256);
@@ -315,5 +342,6 @@ extern "C" int pf_bin(const pf_camera* cam, int32_t tile_width, const float* sph
     tile_ranges_kernel<<<(unsigned)((nthreads + 255) / 256), 256, 0, st>>>(kf, tile_prims, dprim, n_pairs,
                                                                            pair_capacity, T, tile_offsets,
                                                                            sort_keys, status);
+    order();
     return pf_check_launch("pf_bin");
 }

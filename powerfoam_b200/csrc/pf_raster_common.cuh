@@ -1,0 +1,218 @@
+// pf_raster_common.cuh -- parameters, pixel mapping and per-warp staging
+// shared by the rasterizer kernels.
+#pragma once
+#include "pf_common.cuh"
+
+namespace pf {
+
+constexpr int kWarpsPerBlock8 = 4;  // TW = 8: four tiles per 128-thread block
+
+struct RasterParams {
+    Cam cam;
+    int TW, S, Q;
+    int64_t N, T;
+    int tiles_h;
+    const float4* spheres;
+    const float4* nsigmas;
+    const float* sites;   // (N,S,3)
+    const float* rgb;     // (N,S,3)
+    const float* height;  // (N,S)
+    const int32_t* adj;
+    const int32_t* adj_off;
+    const uint2* adj_diff;  // (E) 4 x f16
+    const int64_t* tile_off;
+    const int32_t* tile_prims;
+    const float* dq;   // (H,W,Q)
+    const float* gt;   // (H,W,3)
+    float thr;
+    const int32_t* tile_order;  // processing order of the tiles (NULL: 0..T-1)
+    int* queue;                 // work-queue counter (NULL: one group per tile)
+};
+
+// ---------------------------------------------------------------------------
+// group collectives: G == 1 -> warp vote; G > 1 -> block barrier with reduction
+template <int G>
+PF_D bool group_all(bool p) {
+    if constexpr (G == 1) return __all_sync(0xffffffffu, p);
+    else return __syncthreads_and(p) != 0;
+}
+template <int G>
+PF_D bool group_any(bool p) {
+    if constexpr (G == 1) return __any_sync(0xffffffffu, p);
+    else return __syncthreads_or(p) != 0;
+}
+
+struct PixGeom {
+    v3 d;
+    int64_t px;  // pixel index, valid when !oob
+    bool oob;
+};
+
+PF_D PixGeom pixel_geom(const RasterParams& P, int64_t tile, int idx) {
+    PixGeom g;
+    int ti = (int)(tile % P.tiles_h), tj = (int)(tile / P.tiles_h);
+    int i_in = idx % P.TW, j_in = idx / P.TW;
+    int pi = ti * P.TW + i_in, pj = tj * P.TW + j_in;
+    g.oob = pi >= P.cam.H || pj >= P.cam.W;
+    pi = imin(pi, P.cam.H - 1);
+    pj = imin(pj, P.cam.W - 1);
+    g.d = ray_dir(P.cam, pi, pj);
+    g.px = (int64_t)pi * P.cam.W + pj;
+    return g;
+}
+
+// Per-warp shared staging area.
+struct WarpStage {
+    float4 sph[32];
+    float4 nsg[32];
+    int32_t pid[32];
+    float4 face[32];
+    float ts[3 * kMaxSites];
+    float tr[3 * kMaxSites];
+    float th[kMaxSites];
+};
+
+PF_D void stage_prims(WarpStage& ws, const RasterParams& P, int64_t start, int k0, int total, int lane) {
+    int k = k0 + lane;
+    if (k >= 0 && k < total) {
+        int32_t p = P.tile_prims[start + k];
+        ws.pid[lane] = p;
+        ws.sph[lane] = __ldg(&P.spheres[p]);
+        ws.nsg[lane] = __ldg(&P.nsigmas[p]);
+    }
+    __syncwarp();
+}
+
+PF_D void stage_texels(WarpStage& ws, const RasterParams& P, int32_t prim, int lane) {
+    const int S = P.S;
+    int64_t b3 = (int64_t)prim * S * 3;
+    if (lane < 3 * S) {
+        ws.ts[lane] = __ldg(&P.sites[b3 + lane]);
+        ws.tr[lane] = __ldg(&P.rgb[b3 + lane]);
+    }
+    if (lane < S) ws.th[lane] = __ldg(&P.height[(int64_t)prim * S + lane]);
+    __syncwarp();
+}
+
+// faces e0..e0+31 of the current primitive -> ws.face (n.xyz, num)
+PF_D void stage_faces(WarpStage& ws, const RasterParams& P, int32_t a0, int e0, int n_adj, v3 eye, v3 center,
+                      float cc, float rr, int lane) {
+    int e = e0 + lane;
+    if (e < n_adj) {
+        uint2 raw = __ldg(&P.adj_diff[a0 + e]);
+        v3 diff = mk(h2f((uint16_t)(raw.x & 0xffffu)), h2f((uint16_t)(raw.x >> 16)), h2f((uint16_t)(raw.y & 0xffffu)));
+        float ar = h2f((uint16_t)(raw.y >> 16));
+        Face f = make_face(eye, center, cc, rr, center + diff, ar);
+        ws.face[lane] = make_float4(f.n.x, f.n.y, f.n.z, f.num);
+    }
+    __syncwarp();
+}
+
+// texture.py:10-72 with texel data in shared memory (hit path)
+PF_D PlaneRes plane_fwd_smem(v3 o, v3 d, float t_near, v3 po, v3 pn, float radius, const WarpStage& ws, int S) {
+    PlaneRes r;
+    float _dp;
+    float _t_surf = ray_plane(o, d, po, pn, 0.0f, _dp);
+    float _tq = _dp >= 0.0f ? t_near : fmax_t(t_near, _t_surf);
+    v3 _pt = o + _tq * d;
+    float rr = radius * radius;
+    float hsum = 0.f, _wsum = 0.f;
+#pragma unroll 1
+    for (int i = 0; i < S; i++) {
+        v3 df = _pt - mk(ws.ts[3 * i], ws.ts[3 * i + 1], ws.ts[3 * i + 2]);
+        float dist_sq = dot(df, df) / rr;
+        float w = expf(-kTemp * dist_sq);
+        hsum += w * ws.th[i];
+        _wsum += w;
+    }
+    _wsum = fmax_t(_wsum, 1e-20f);
+    float height = hsum / _wsum;
+    float dp;
+    float t_surf = ray_plane(o, d, po, pn, height, dp);
+    float tq = dp >= 0.0f ? t_near : fmax_t(t_near, t_surf);
+    v3 pt = o + tq * d;
+    v3 rgb_sum = mk(0.f, 0.f, 0.f);
+    float wsum = 0.f;
+#pragma unroll 1
+    for (int i = 0; i < S; i++) {
+        v3 df = pt - mk(ws.ts[3 * i], ws.ts[3 * i + 1], ws.ts[3 * i + 2]);
+        float dist_sq = dot(df, df) / rr;
+        float w = expf(-kTemp * dist_sq);
+        rgb_sum = rgb_sum + w * mk(ws.tr[3 * i], ws.tr[3 * i + 1], ws.tr[3 * i + 2]);
+        wsum += w;
+    }
+    wsum = fmax_t(wsum, 1e-20f);
+    r._t_surf = _t_surf;
+    r._dp = _dp;
+    r.height = height;
+    r._wsum = _wsum;
+    r.t_surf = t_surf;
+    r.dp = dp;
+    r.rgb = rgb_sum / wsum;
+    r.wsum = wsum;
+    return r;
+}
+
+
+inline bool fill_params(const pf_raster_inputs* in, RasterParams& P, bool need_f32, const char** why) {
+    if (!in) {
+        *why = "null inputs";
+        return false;
+    }
+    if (in->cam.width < 2 || in->cam.height < 2) {
+        *why = "image must be at least 2x2";
+        return false;
+    }
+    if (in->n_sites < 0 || in->n_sites > kMaxSites) {
+        *why = "n_sites must be in [0, 8]";
+        return false;
+    }
+    if (in->tile_width <= 0) {
+        *why = "tile_width must be positive";
+        return false;
+    }
+    if (need_f32 && in->attr_half) {
+        *why = "forward/backward take float32 attributes";
+        return false;
+    }
+    if (in->n_quantiles < 0 || (in->n_quantiles > 0 && !in->depth_quantiles)) {
+        *why = "bad quantiles";
+        return false;
+    }
+    if (in->n_prims > 0 && (!in->spheres || !in->nsigmas || !in->adjacency_offsets || !in->texel_sites ||
+                            !in->texel_rgb || !in->texel_height)) {
+        *why = "missing primitive arrays";
+        return false;
+    }
+    if (!in->tile_offsets || !in->tile_prims) {
+        *why = "missing tile lists";
+        return false;
+    }
+    P.cam = load_cam(in->cam);
+    P.TW = in->tile_width;
+    P.S = in->n_sites;
+    P.Q = in->n_quantiles;
+    P.N = in->n_prims;
+    P.tiles_h = 1 + (in->cam.height - 1) / P.TW;
+    int tiles_w = 1 + (in->cam.width - 1) / P.TW;
+    P.T = (int64_t)P.tiles_h * tiles_w;
+    P.spheres = (const float4*)in->spheres;
+    P.nsigmas = (const float4*)in->nsigmas;
+    P.sites = (const float*)in->texel_sites;
+    P.rgb = (const float*)in->texel_rgb;
+    P.height = (const float*)in->texel_height;
+    P.adj = in->adjacency;
+    P.adj_off = in->adjacency_offsets;
+    P.adj_diff = (const uint2*)in->adjacency_diff;
+    P.tile_off = in->tile_offsets;
+    P.tile_prims = in->tile_prims;
+    P.dq = in->depth_quantiles;
+    P.gt = in->ray_gt;
+    P.thr = in->transmittance_threshold;
+    P.tile_order = in->tile_order;
+    P.queue = (int*)in->scratch;
+    return true;
+}
+
+
+}  // namespace pf

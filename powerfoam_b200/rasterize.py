@@ -67,7 +67,8 @@ def _f32(t, name):
 class TileBins:
     """Result of binning: per-tile offsets (T+1, int64) and sorted primitive ids."""
 
-    def __init__(self, tile_offsets, tile_prims, n_pairs, prim_visible, sort_keys=None):
+    def __init__(self, tile_offsets, tile_prims, n_pairs, prim_visible, sort_keys=None, tile_order=None):
+        self.tile_order = tile_order
         self.tile_offsets = tile_offsets
         self.tile_prims = tile_prims
         self.n_pairs = n_pairs
@@ -87,17 +88,18 @@ class Binner:
         self.capacity = 0
         self.ws = None
 
-    def _ensure(self, n_prims, cap):
+    def _ensure(self, n_prims, cap, num_tiles):
         nbytes = _lib.ctypes.c_size_t(0)
-        _lib.call("pf_bin_workspace_size", n_prims, cap, _lib.ctypes.byref(nbytes))
+        _lib.call("pf_bin_workspace_size", n_prims, cap, num_tiles, _lib.ctypes.byref(nbytes))
         if self.ws is None or self.ws.numel() < nbytes.value:
             self.ws = torch.empty(max(nbytes.value, 256), dtype=torch.uint8, device=self.device)
 
     def __call__(self, cam_pf, tile_width, spheres, n_prims, num_tiles, return_keys=False, capacity=None):
         cap = capacity if capacity is not None else max(self.capacity, 4 * n_prims, 1 << 14)
         while True:
-            self._ensure(n_prims, cap)
+            self._ensure(n_prims, cap, num_tiles)
             tile_offsets = torch.empty(num_tiles + 1, dtype=torch.int64, device=self.device)
+            tile_order = torch.empty(num_tiles, dtype=torch.int32, device=self.device)
             tile_prims = torch.empty(max(cap, 1), dtype=torch.int32, device=self.device)
             keys = torch.empty(max(cap, 1), dtype=torch.int64, device=self.device) if return_keys else None
             visible = torch.empty(n_prims, dtype=torch.uint8, device=self.device)
@@ -105,14 +107,15 @@ class Binner:
             status = scalars[1:].view(torch.int32)[:1]
             _lib.call("pf_bin", _lib.ctypes.byref(cam_pf), tile_width, _lib.ptr(spheres), n_prims,
                       _lib.ptr(self.ws), self.ws.numel(), cap, _lib.ptr(tile_offsets), _lib.ptr(tile_prims),
-                      _lib.ptr(keys), _lib.ptr(visible), _lib.ptr(scalars[:1]), _lib.ptr(status),
-                      _lib.stream_ptr())
+                      _lib.ptr(keys), _lib.ptr(visible), _lib.ptr(tile_order), _lib.ptr(scalars[:1]),
+                      _lib.ptr(status), _lib.stream_ptr())
             n = int(scalars[0].item())
             if n <= cap:
                 break
             cap = 1 << (int(n * 1.25) - 1).bit_length()
         self.capacity = max(self.capacity, cap)
-        return TileBins(tile_offsets, tile_prims[:n], n, visible.bool(), keys[:n] if return_keys else None)
+        return TileBins(tile_offsets, tile_prims[:n], n, visible.bool(), keys[:n] if return_keys else None,
+                        tile_order)
 
 
 class Rasterizer:
@@ -136,6 +139,9 @@ class Rasterizer:
         self.binner = Binner(self.device)
         self.collect_stats = False
         self.last_stats = None
+        # device scratch of the compositing kernels' tile work queue; one
+        # Rasterizer serves one stream at a time
+        self.scratch = torch.zeros(64, dtype=torch.int32, device=self.device)
         _lib.load()
 
     # ------------------------------------------------------------------
@@ -188,6 +194,8 @@ class Rasterizer:
         inp.n_quantiles = 0 if depth_quantiles is None else depth_quantiles.shape[-1]
         inp.ray_gt = _lib.ptr(ray_gt)
         inp.transmittance_threshold = float(thr)
+        inp.tile_order = _lib.ptr(bins.tile_order)
+        inp.scratch = _lib.ptr(self.scratch)
         return inp
 
     # ------------------------------------------------------------------

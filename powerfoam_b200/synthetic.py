@@ -123,6 +123,8 @@ CONFIGS = {
     "raster16k": dict(n=16384, seed=0, mixture=0, r_range=(0.01, 0.05), width=256, height=256, vfov=60.0),
     "raster1m": dict(n=1048576, seed=1, mixture=32, sigma=0.15, r_range=(0.002, 0.02), width=1920, height=1080,
                      vfov=50.0),
+    "raster256k": dict(n=262144, seed=1, mixture=32, sigma=0.15, r_range=(0.004, 0.04), width=960, height=540,
+                       vfov=50.0),
     "trace1m": dict(n=1048576, seed=1, mixture=32, sigma=0.15, r_range=(0.002, 0.02), width=1280, height=720,
                     vfov=50.0),
     "batch3m": dict(n=3145728, seed=3, mixture=64, sigma=0.15, r_range=(0.002, 0.02), vfov=50.0),

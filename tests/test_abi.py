@@ -35,9 +35,9 @@ def test_argument_errors_are_reported_without_a_gpu():
 
     lib = _lib.load()
     n = ctypes.c_size_t(0)
-    assert lib.pf_bin_workspace_size(-1, 0, ctypes.byref(n)) == _lib.PF_ERR_ARGS
+    assert lib.pf_bin_workspace_size(-1, 0, 0, ctypes.byref(n)) == _lib.PF_ERR_ARGS
     assert b"bad arguments" in lib.pf_last_error()
-    assert lib.pf_bin_workspace_size(1000, 5000, ctypes.byref(n)) == 0 and n.value > 0
+    assert lib.pf_bin_workspace_size(1000, 5000, 100, ctypes.byref(n)) == 0 and n.value > 0
     assert lib.pf_raster_forward(None, 0, *([None] * 11)) == _lib.PF_ERR_ARGS
 
 

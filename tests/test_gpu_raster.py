@@ -95,14 +95,15 @@ def test_binning_overflow_retry_and_status():
     sp = to_t(sph)
     T = R.num_tiles(c)
     ws_n = ctypes.c_size_t(0)
-    _lib.call("pf_bin_workspace_size", sph.shape[0], 16, ctypes.byref(ws_n))
+    _lib.call("pf_bin_workspace_size", sph.shape[0], 16, T, ctypes.byref(ws_n))
     ws = torch.empty(ws_n.value, dtype=torch.uint8, device="cuda")
     offs_t = torch.full((T + 1,), 7, dtype=torch.int64, device="cuda")
     prims_t = torch.empty(16, dtype=torch.int32, device="cuda")
     npairs = torch.zeros(1, dtype=torch.int64, device="cuda")
     status = torch.zeros(1, dtype=torch.int32, device="cuda")
     _lib.call("pf_bin", ctypes.byref(c.to_pf()), 8, _lib.ptr(sp), sph.shape[0], _lib.ptr(ws), ws.numel(), 16,
-              _lib.ptr(offs_t), _lib.ptr(prims_t), None, None, _lib.ptr(npairs), _lib.ptr(status), _lib.stream_ptr())
+              _lib.ptr(offs_t), _lib.ptr(prims_t), None, None, None, _lib.ptr(npairs), _lib.ptr(status),
+              _lib.stream_ptr())
     assert int(status.item()) == _lib.PF_ERR_OVERFLOW
     assert int(npairs.item()) == keys.shape[0]
     assert int(offs_t.abs().sum().item()) == 0
