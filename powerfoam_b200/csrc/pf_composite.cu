@@ -5,20 +5,20 @@
 //          (plane_intersection_bwd), rendering_math.py:26-147, and the host
 //          side of Rasterizer._backward (:1861-1980).
 //
-// Work decomposition.  A tile of TW x TW pixels belongs to a group of
-// G = TW*TW/64 warps and every lane owns two pixels.  For TW = 8 (G = 1, the
-// reference's tile) warps are persistent: each takes the next tile from a
-// work queue ordered by decreasing list length (longest first, so the last
-// tiles are short), and the reference's block-wide tile_max / tile_sum are
-// single warp votes.  For TW = 16 / 32 a block is the group, takes tiles from
-// the same queue, and the votes are __syncthreads_and / __syncthreads_or.
+// Work decomposition.  A tile of TW x TW pixels belongs to a block of G warps
+// (TW = 8: 2 warps, one pixel per lane; TW = 16: 8 warps, one pixel per lane;
+// TW = 32: 16 warps, two pixels per lane).  Blocks are persistent: each takes
+// the next tile from a work queue ordered by decreasing list length (longest
+// first, so the last tiles are short), and the reference's block-wide
+// tile_max / tile_sum become __syncthreads_and / __syncthreads_or.  A warp
+// whose pixels miss the primitive skips it after the block vote.
 //
 // Per primitive a warp stages the sphere and normal+sigma records of 32
 // primitives at a time, turns the primitive's neighbours into face planes
-// (n, num) one per lane, and stages the texel records once.  Each lane runs
-// ONE copy of the per-pixel code for its two pixels (their states are swapped
-// in registers between the two passes) and the texel loops are rolled: the
-// kernels' hot loops then fit the instruction caches.
+// (n, num) one per lane, and stages the texel records once.  There is ONE copy
+// of the per-pixel code (with two pixels per lane their states are swapped in
+// registers between the two passes) and the texel loops are rolled: the hot
+// loops then fit the instruction caches.
 //
 // Adjoint accumulation.  Each lane adds its pixels' contributions to the
 // primitive's 64 gradient values (centre, radius, normal, sigma, 8 x site,
@@ -39,9 +39,81 @@ namespace pf {
 constexpr int kAccRows = 64;
 constexpr int kFaceSlots = 64;
 
+// Group layout per tile width: TW = 8 and 16 use one pixel per lane (G = 2
+// and 8 warps per tile), TW = 32 two pixels per lane (G = 16).
+template <int TW>
+struct Layout {
+    static constexpr int PPL = TW == 32 ? 2 : 1;
+    static constexpr int G = TW * TW / (32 * PPL);
+    static constexpr int THREADS = 32 * G;
+};
+
+// Early termination across the warps of a tile (forward).  The reference
+// stops a tile before primitive k when every pixel's transmittance is below
+// the threshold (tile_max).  Transmittance never increases, so each warp
+// records the first k at which all of ITS pixels are below (below_at) and the
+// last k it has voted on (prog).  A warp that is not all-below knows the tile
+// cannot stop at k and goes on without waiting; a warp that is all-below at k
+// waits until every other warp has either recorded below_at <= k (stop) or
+// voted on k while not below (go on).  The warp furthest behind never waits,
+// so the protocol always progresses; the wait is nevertheless bounded by a
+// clock limit, after which the kernel reports PF_ERR_CUDA in the status word
+// and carries on compositing.
+struct StopState {
+    int below_at[32];
+    int prog[32];
+};
+
+constexpr long long kWaitLimitCycles = 20000000000ll;  // ~10 s
+
+template <int G>
+PF_D void stop_reset(StopState& ss, int wig, int lane) {
+    if (G > 1 && lane == 0) {
+        ss.below_at[wig] = 0x7fffffff;
+        ss.prog[wig] = -1;
+    }
+}
+
+// returns true when the tile stops before primitive k
+template <int G>
+PF_D bool stop_vote(StopState& ss, int wig, int lane, int k, bool below, int* status) {
+    const bool mine = __all_sync(0xffffffffu, below);
+    if constexpr (G == 1) return mine;
+    int stop = 0;
+    if (lane == 0) {
+        volatile int* vb = ss.below_at;
+        volatile int* vp = ss.prog;
+        if (mine && vb[wig] == 0x7fffffff) vb[wig] = k;
+        __threadfence_block();
+        vp[wig] = k;
+        if (mine) {
+            stop = 1;
+            const long long t0 = clock64();
+            for (int v = 0; v < G && stop; v++) {
+                if (v == wig) continue;
+                for (;;) {
+                    if (vb[v] <= k) break;  // v below at k
+                    if (vp[v] >= k) {
+                        __threadfence_block();
+                        if (vb[v] > k) stop = 0;  // v voted at k, not below
+                        break;
+                    }
+                    if (clock64() - t0 > kWaitLimitCycles) {
+                        if (status) atomicMax(status, PF_ERR_CUDA);
+                        stop = 0;
+                        break;
+                    }
+                    __nanosleep(64);
+                }
+            }
+        }
+    }
+    return __shfl_sync(0xffffffffu, stop, 0) != 0;
+}
+
 // next tile of this group; -1 when the queue is exhausted
 template <int G>
-PF_D int64_t next_tile(const RasterParams& P, int64_t& static_next, int lane) {
+PF_D int64_t next_tile(const RasterParams& P, int64_t& static_next, int lane, StopState* ss) {
     int64_t t;
     if (P.queue) {
         if constexpr (G == 1) {
@@ -51,16 +123,35 @@ PF_D int64_t next_tile(const RasterParams& P, int64_t& static_next, int lane) {
         } else {
             __shared__ int s_t;
             __syncthreads();
+            if (ss) stop_reset<G>(*ss, threadIdx.x >> 5, lane);
             if (threadIdx.x == 0) s_t = atomicAdd(P.queue, 1);
             __syncthreads();
             t = s_t;
         }
     } else {
+        if constexpr (G > 1) {
+            __syncthreads();
+            if (ss) stop_reset<G>(*ss, threadIdx.x >> 5, lane);
+            __syncthreads();
+        }
         t = static_next;
         static_next = P.T;  // one tile per group without a queue
     }
     if (t >= P.T) return -1;
     return P.tile_order ? (int64_t)P.tile_order[t] : t;
+}
+
+// A face can change the running interval only if its exact crossing
+// q = num / dp lies before t_far (dp >= 0) or after t_near (dp < 0); rounding
+// is monotone, so rn(q) < t_far implies q < t_far.  With dp != 0 both tests
+// read t * dp - num >= 0, and fma gives that value's exact sign in one
+// rounding, so the (costly) IEEE division runs only for faces that may clip;
+// dp == +-0 and NaNs always take the division.  Skipped faces would leave
+// t_near, t_far and their ids unchanged, so the result is bit-identical.
+PF_D bool face_may_clip(float dp, float num, float tn, float tf) {
+    float tref = dp >= 0.0f ? tf : tn;
+    float r = fmaf(tref, dp, -num);
+    return !(r < 0.0f) || dp == 0.0f;
 }
 
 // ---------------------------------------------------------------------------
@@ -93,17 +184,22 @@ struct FwdOut {
     int32_t* early_stop;
     int32_t* tile_contrib_pairs;
     int rpe;
+    int* status;
 };
 
-template <int G>
-PF_D void fwd_tile(const RasterParams& P, const FwdOut& out, int64_t tile, int wig, int lane, WarpStage& ws) {
+template <int G, int PPL>
+PF_D void fwd_tile(const RasterParams& P, const FwdOut& out, int64_t tile, int wig, int lane, WarpStage& ws,
+                   StopState& ss) {
     const int TS = P.TW * P.TW;
     const v3 o = P.cam.eye;
     const float HW = (float)(P.cam.H * P.cam.W);
     const bool want_gt = out.rpe || out.err;
     FwdPix a, b;
+    b.g.oob = true;
+    b.hit = false;
+    b.trans = 1.0f;
 #pragma unroll 1
-    for (int s = 0; s < 2; s++) {
+    for (int s = 0; s < PPL; s++) {
         FwdPix& x = a;
         int idx = wig * 32 + lane + s * (TS / 2);
         x.g = pixel_geom(P, tile, idx);
@@ -126,7 +222,7 @@ PF_D void fwd_tile(const RasterParams& P, const FwdOut& out, int64_t tile, int w
             }
             if (want_gt) x.gt = mk(P.gt[3 * x.g.px], P.gt[3 * x.g.px + 1], P.gt[3 * x.g.px + 2]);
         }
-        swap_pix(a, b);
+        if (PPL == 2) swap_pix(a, b);
     }
     // a = pixel idx, b = pixel idx + TS/2
     const int64_t start = P.tile_off[tile];
@@ -139,7 +235,7 @@ PF_D void fwd_tile(const RasterParams& P, const FwdOut& out, int64_t tile, int w
         const int kn = min(32, total - k0);
         for (int kk = 0; kk < kn; kk++) {
             bool below = (a.g.oob ? false : a.trans < P.thr) && (b.g.oob ? false : b.trans < P.thr);
-            if (group_all<G>(below)) {
+            if (stop_vote<G>(ss, wig, lane, k0 + kk, below, out.status)) {
                 es = k0 + kk;
                 stopped = true;
                 break;
@@ -148,8 +244,10 @@ PF_D void fwd_tile(const RasterParams& P, const FwdOut& out, int64_t tile, int w
             const v3 center = mk(s4.x, s4.y, s4.z);
             const float radius = s4.w;
             a.hit = a.g.oob ? false : ray_sphere(o, a.g.d, center, radius, a.tn, a.tf);
-            b.hit = b.g.oob ? false : ray_sphere(o, b.g.d, center, radius, b.tn, b.tf);
-            if (!group_any<G>(a.hit || b.hit)) continue;
+            if (PPL == 2) b.hit = b.g.oob ? false : ray_sphere(o, b.g.d, center, radius, b.tn, b.tf);
+            // The reference skips a primitive no pixel of the tile hits (tile_sum);
+            // the skip changes no output, so each warp decides for its own pixels.
+            if (!__any_sync(0xffffffffu, a.hit || b.hit)) continue;
             const int32_t prim = ws.pid[kk];
             const float4 n4 = ws.nsg[kk];
             const v3 pn = mk(n4.x, n4.y, n4.z);
@@ -166,15 +264,19 @@ PF_D void fwd_tile(const RasterParams& P, const FwdOut& out, int64_t tile, int w
                     const v3 fn = mk(f.x, f.y, f.z);
                     if (a.hit) {
                         float dp = dot(a.g.d, fn);
-                        float t_face = f.w / dp;
-                        a.tf = dp >= 0.0f ? fmin_t(t_face, a.tf) : a.tf;
-                        a.tn = dp < 0.0f ? fmax_t(t_face, a.tn) : a.tn;
+                        if (face_may_clip(dp, f.w, a.tn, a.tf)) {
+                            float t_face = f.w / dp;
+                            a.tf = dp >= 0.0f ? fmin_t(t_face, a.tf) : a.tf;
+                            a.tn = dp < 0.0f ? fmax_t(t_face, a.tn) : a.tn;
+                        }
                     }
-                    if (b.hit) {
+                    if (PPL == 2 && b.hit) {
                         float dp = dot(b.g.d, fn);
-                        float t_face = f.w / dp;
-                        b.tf = dp >= 0.0f ? fmin_t(t_face, b.tf) : b.tf;
-                        b.tn = dp < 0.0f ? fmax_t(t_face, b.tn) : b.tn;
+                        if (face_may_clip(dp, f.w, b.tn, b.tf)) {
+                            float t_face = f.w / dp;
+                            b.tf = dp >= 0.0f ? fmin_t(t_face, b.tf) : b.tf;
+                            b.tn = dp < 0.0f ? fmax_t(t_face, b.tn) : b.tn;
+                        }
                     }
                 }
                 __syncwarp();
@@ -182,7 +284,7 @@ PF_D void fwd_tile(const RasterParams& P, const FwdOut& out, int64_t tile, int w
             stage_texels(ws, P, prim, lane);
             float c_acc = 0.f, e_acc = 0.f;
 #pragma unroll 1
-            for (int s = 0; s < 2; s++) {
+            for (int s = 0; s < PPL; s++) {
                 if (a.hit) {
                     PlaneRes pr = plane_fwd_smem(o, a.g.d, a.tn, center, pn, radius, ws, P.S);
                     float tf = pr.dp >= 0.0f ? fmin_t(pr.t_surf, a.tf) : a.tf;
@@ -217,7 +319,7 @@ PF_D void fwd_tile(const RasterParams& P, const FwdOut& out, int64_t tile, int w
                         a.trans = next_trans;
                     }
                 }
-                swap_pix(a, b);
+                if (PPL == 2) swap_pix(a, b);
             }
             // one atomic per primitive per warp for contrib / point_err
             if (__any_sync(0xffffffffu, c_acc != 0.f || e_acc != 0.f)) {
@@ -233,7 +335,7 @@ PF_D void fwd_tile(const RasterParams& P, const FwdOut& out, int64_t tile, int w
         __syncwarp();
     }
 #pragma unroll 1
-    for (int s = 0; s < 2; s++) {
+    for (int s = 0; s < PPL; s++) {
         if (!a.g.oob) {
             int64_t p = a.g.px;
             out.color[3 * p] = a.rgb.x;
@@ -250,24 +352,23 @@ PF_D void fwd_tile(const RasterParams& P, const FwdOut& out, int64_t tile, int w
                 out.err[p] = a.err + dot(de, de) * expf(a.log_t);
             }
         }
-        swap_pix(a, b);
+        if (PPL == 2) swap_pix(a, b);
     }
     if (lane == 0 && wig == 0) out.early_stop[tile] = es;
     if (out.tile_contrib_pairs && lane == 0) atomicAdd(&out.tile_contrib_pairs[tile], n_contrib_pairs);
 }
 
 template <int TW>
-__global__ void __launch_bounds__(TW == 32 ? 512 : 128) raster_fwd_kernel(RasterParams P, FwdOut out) {
-    constexpr int G = TW * TW / 64;
-    constexpr int WPB = G == 1 ? kWarpsPerBlock8 : G;
-    __shared__ WarpStage stage[WPB];
+__global__ void __launch_bounds__(Layout<TW>::THREADS) raster_fwd_kernel(RasterParams P, FwdOut out) {
+    constexpr int G = Layout<TW>::G;
+    __shared__ WarpStage stage[G];
+    __shared__ StopState ss;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int wig = G == 1 ? 0 : warp;
-    int64_t static_next = G == 1 ? (int64_t)blockIdx.x * WPB + warp : (int64_t)blockIdx.x;
+    int64_t static_next = (int64_t)blockIdx.x;
     for (;;) {
-        int64_t tile = next_tile<G>(P, static_next, lane);
+        int64_t tile = next_tile<G>(P, static_next, lane, &ss);
         if (tile < 0) break;
-        fwd_tile<G>(P, out, tile, wig, lane, stage[warp]);
+        fwd_tile<G, Layout<TW>::PPL>(P, out, tile, warp, lane, stage[warp], ss);
     }
 }
 
@@ -325,6 +426,66 @@ PF_D float* grad_slot(const GradOut& go, int S, int64_t prim, int j) {
     return (r < S) ? go.height + prim * S + r : nullptr;
 }
 
+// Derivative-only arithmetic of the adjoint.  Gradients are compared at a
+// relative tolerance (they are sums over pixels and primitives, and the
+// reference accumulates them with atomics in arbitrary order), so the
+// divisions that only scale derivative values use one reciprocal each.
+// Every DECISION of the adjoint (which surface bounds a segment, whether a
+// texel site passes w / sum(w) >= 1e-3, the sphere-root sign tests) is still
+// taken on the exact operations of the reference.
+
+// rendering_math.py:26-59
+PF_D void ray_sphere_bwd_d(v3 eye, v3 dir, v3 c, float r, v3& dn_dc, v3& df_dc, float& dn_dr, float& df_dr) {
+    v3 oc = eye - c;
+    float qa = dot(dir, dir);
+    float qb = 2.0f * dot(oc, dir);
+    float qc = dot(oc, oc) - r * r;
+    float disc = qb * qb - 4.0f * qa * qc;
+    dn_dc = mk(0.f, 0.f, 0.f);
+    df_dc = mk(0.f, 0.f, 0.f);
+    dn_dr = 0.f;
+    df_dr = 0.f;
+    if (disc < 0.0f) return;
+    float s = sqrtf(disc);
+    float t_far = (-qb + s) / (2.0f * qa);
+    float t_near = (-qb - s) / (2.0f * qa);
+    if (t_near < 0.0f && t_far < 0.0f) return;
+    float inv_qa = 1.0f / qa, inv_s = 1.0f / s;
+    v3 g = (inv_qa * inv_s) * ((2.0f * qa) * oc - qb * dir);
+    v3 dq = inv_qa * dir;
+    df_dc = dq + g;
+    df_dr = 2.0f * r * inv_s;
+    if (t_near >= 0.0f) {
+        dn_dc = dq - g;
+        dn_dr = -df_dr;
+    }
+}
+
+// rendering_math.py:101-125
+PF_D void ray_pface_bwd_d(v3 eye, v3 dir, v3 center, float radius, v3 adj_center, float adj_radius, v3& dc,
+                          float& dr, v3& dac, float& dar) {
+    v3 face_n = adj_center - center;
+    float face_offset = 0.5f * (dot(adj_center, adj_center) - dot(center, center) + radius * radius -
+                                adj_radius * adj_radius);
+    float num = face_offset - dot(eye, face_n);
+    float inv_dp = 1.0f / dot(dir, face_n);
+    v3 q = (num * inv_dp * inv_dp) * dir;
+    dc = inv_dp * (eye - center) + q;
+    dac = inv_dp * (adj_center - eye) - q;
+    dr = radius * inv_dp;
+    dar = -adj_radius * inv_dp;
+}
+
+// rendering_math.py:138-147
+PF_D void ray_plane_bwd_d(v3 eye, v3 dir, v3 p, v3 n, float h, v3& dtdp, v3& dtdn, float& dtdh) {
+    float dp = dot(n, dir);
+    float i1 = 1.0f / (dp + 1e-6f);
+    float i2 = 1.0f / (dp * dp + 1e-6f);
+    dtdp = i1 * n;
+    dtdh = i1;
+    dtdn = i1 * (p - eye) - ((dot(p - eye, n) + h) * i2) * dir;
+}
+
 // texture.py:74-186, accumulating into this lane's column of bs.acc
 PF_D void plane_bwd_acc(v3 o, v3 d, float _t_near, v3 po, v3 pn, float radius, const WarpStage& ws, int S,
                         const PlaneRes& pr, v3 dLdrgb_in, float dLdt_surf_in, BwdStage& bs, int lane, v3& dLdpo_out,
@@ -333,10 +494,12 @@ PF_D void plane_bwd_acc(v3 o, v3 d, float _t_near, v3 po, v3 pn, float radius, c
     float dLdheight_in = 0.f;
     const float height_in = pr.height, weight_sum = pr.wsum, _weight_sum = pr._wsum;
     const float rr = radius * radius;
+    const float inv_rr = 1.0f / rr, inv_ws = 1.0f / weight_sum, inv__ws = 1.0f / _weight_sum;
     float tq = pr.dp >= 0.0f ? _t_near : fmax_t(_t_near, pr.t_surf);
     v3 pt = o + tq * d;
     v3 dLdpt = mk(0.f, 0.f, 0.f);
     float grad_dp_in = dot(dLdrgb_in, pr.rgb);
+    const v3 rgb_scale = inv_ws * dLdrgb_in;
 #pragma unroll 1
     for (int i = 0; i < S; i++) {
         v3 site = mk(ws.ts[3 * i], ws.ts[3 * i + 1], ws.ts[3 * i + 2]);
@@ -344,17 +507,17 @@ PF_D void plane_bwd_acc(v3 o, v3 d, float _t_near, v3 po, v3 pn, float radius, c
         float dist_sq = dot(df, df) / rr;
         float w = expf(-kTemp * dist_sq);
         if (!(w / weight_sum < 1e-3f)) {
-            v3 dwds = ((2.0f * kTemp * w) * (pt - site)) / rr;
-            v3 rgb_grad = (w * dLdrgb_in) / weight_sum;
+            v3 dwds = ((2.0f * kTemp * w) * inv_rr) * df;
+            v3 rgb_grad = w * rgb_scale;
             bs.acc[32 + 3 * i][lane] += rgb_grad.x;
             bs.acc[33 + 3 * i][lane] += rgb_grad.y;
             bs.acc[34 + 3 * i][lane] += rgb_grad.z;
             float grad_dp = dot(dLdrgb_in, mk(ws.tr[3 * i], ws.tr[3 * i + 1], ws.tr[3 * i + 2]));
-            v3 site_grad = ((grad_dp - grad_dp_in) * dwds) / weight_sum;
+            v3 site_grad = ((grad_dp - grad_dp_in) * inv_ws) * dwds;
             bs.acc[8 + 3 * i][lane] += site_grad.x;
             bs.acc[9 + 3 * i][lane] += site_grad.y;
             bs.acc[10 + 3 * i][lane] += site_grad.z;
-            dLdpt = dLdpt + (-site_grad);
+            dLdpt = dLdpt - site_grad;
         }
     }
     float dLdt_query = dot(dLdpt, d);
@@ -364,7 +527,7 @@ PF_D void plane_bwd_acc(v3 o, v3 d, float _t_near, v3 po, v3 pn, float radius, c
     if (fabsf(dLdt_surf) > 0.0f) {
         v3 ga, gb;
         float gc;
-        ray_plane_bwd(o, d, po, pn, height_in, ga, gb, gc);
+        ray_plane_bwd_d(o, d, po, pn, height_in, ga, gb, gc);
         dLdpo = dLdpo + dLdt_surf * ga;
         dLdpn = dLdpn + dLdt_surf * gb;
         dLdheight_in += gc * dLdt_surf;
@@ -373,21 +536,23 @@ PF_D void plane_bwd_acc(v3 o, v3 d, float _t_near, v3 po, v3 pn, float radius, c
     v3 _pt = o + _tq * d;
     v3 dLd_pt = mk(0.f, 0.f, 0.f);
     float _grad_dp_in = dLdheight_in * height_in;
+    if (dLdheight_in != 0.0f) {  // every term of this pass is proportional to dLdheight_in
 #pragma unroll 1
-    for (int i = 0; i < S; i++) {
-        v3 site = mk(ws.ts[3 * i], ws.ts[3 * i + 1], ws.ts[3 * i + 2]);
-        v3 df = _pt - site;
-        float dist_sq = dot(df, df) / rr;
-        float w = expf(-kTemp * dist_sq);
-        if (!(w / weight_sum < 1e-3f)) {
-            v3 dwds = ((2.0f * kTemp * w) * (_pt - site)) / rr;
-            bs.acc[56 + i][lane] += w * dLdheight_in / _weight_sum;
-            float _grad_dp = dLdheight_in * ws.th[i];
-            v3 site_grad = ((_grad_dp - _grad_dp_in) * dwds) / _weight_sum;
-            bs.acc[8 + 3 * i][lane] += site_grad.x;
-            bs.acc[9 + 3 * i][lane] += site_grad.y;
-            bs.acc[10 + 3 * i][lane] += site_grad.z;
-            dLd_pt = dLd_pt + (-site_grad);
+        for (int i = 0; i < S; i++) {
+            v3 site = mk(ws.ts[3 * i], ws.ts[3 * i + 1], ws.ts[3 * i + 2]);
+            v3 df = _pt - site;
+            float dist_sq = dot(df, df) / rr;
+            float w = expf(-kTemp * dist_sq);
+            if (!(w / weight_sum < 1e-3f)) {
+                v3 dwds = ((2.0f * kTemp * w) * inv_rr) * df;
+                bs.acc[56 + i][lane] += w * dLdheight_in * inv__ws;
+                float _grad_dp = dLdheight_in * ws.th[i];
+                v3 site_grad = ((_grad_dp - _grad_dp_in) * inv__ws) * dwds;
+                bs.acc[8 + 3 * i][lane] += site_grad.x;
+                bs.acc[9 + 3 * i][lane] += site_grad.y;
+                bs.acc[10 + 3 * i][lane] += site_grad.z;
+                dLd_pt = dLd_pt - site_grad;
+            }
         }
     }
     float dLd_t_query = dot(dLd_pt, d);
@@ -396,7 +561,7 @@ PF_D void plane_bwd_acc(v3 o, v3 d, float _t_near, v3 po, v3 pn, float radius, c
     if (fabsf(dLd_t_surf) > 0.0f) {
         v3 ga, gb;
         float gc;
-        ray_plane_bwd(o, d, po, pn, 0.0f, ga, gb, gc);
+        ray_plane_bwd_d(o, d, po, pn, 0.0f, ga, gb, gc);
         dLdpo = dLdpo + dLd_t_surf * ga;
         dLdpn = dLdpn + dLd_t_surf * gb;
     }
@@ -416,7 +581,7 @@ struct BwdIn {
     const float* g_contrib;
 };
 
-template <int G>
+template <int G, int PPL>
 PF_D void bwd_tile(const RasterParams& P, const BwdIn& in, const GradOut& go, int64_t tile, int wig, int lane,
                    WarpStage& ws, BwdStage& bs) {
     const int TS = P.TW * P.TW;
@@ -424,8 +589,10 @@ PF_D void bwd_tile(const RasterParams& P, const BwdIn& in, const GradOut& go, in
     const float HW = (float)(P.cam.H * P.cam.W);
     const v3 bkgd = mk(0.f, 0.f, 0.f);
     BwdPix a, b;
+    b.g.oob = true;
+    b.hit = false;
 #pragma unroll 1
-    for (int s = 0; s < 2; s++) {
+    for (int s = 0; s < PPL; s++) {
         int idx = wig * 32 + lane + s * (TS / 2);
         a.g = pixel_geom(P, tile, idx);
         int64_t p = a.g.px;
@@ -449,7 +616,7 @@ PF_D void bwd_tile(const RasterParams& P, const BwdIn& in, const GradOut& go, in
         a.hit = false;
         a.tn = a.tf = 0.f;
         a.tn_id = a.tf_id = -2;
-        swap_pix(a, b);
+        if (PPL == 2) swap_pix(a, b);
     }
     const int64_t start = P.tile_off[tile];
     const int es = in.early_stop[tile];
@@ -462,8 +629,8 @@ PF_D void bwd_tile(const RasterParams& P, const BwdIn& in, const GradOut& go, in
             const v3 center = mk(s4.x, s4.y, s4.z);
             const float radius = s4.w;
             a.hit = a.g.oob ? false : ray_sphere(o, a.g.d, center, radius, a.tn, a.tf);
-            b.hit = b.g.oob ? false : ray_sphere(o, b.g.d, center, radius, b.tn, b.tf);
-            if (!group_any<G>(a.hit || b.hit)) continue;
+            if (PPL == 2) b.hit = b.g.oob ? false : ray_sphere(o, b.g.d, center, radius, b.tn, b.tf);
+            if (!__any_sync(0xffffffffu, a.hit || b.hit)) continue;  // no output changes (see forward)
             const int32_t prim = ws.pid[kk];
             const float4 n4 = ws.nsg[kk];
             const v3 pn = mk(n4.x, n4.y, n4.z);
@@ -492,19 +659,23 @@ PF_D void bwd_tile(const RasterParams& P, const BwdIn& in, const GradOut& go, in
                     const int adj_idx = e0 + q;
                     if (a.hit) {
                         float dp = dot(a.g.d, fn);
-                        float t_face = f.w / dp;
-                        a.tf_id = (dp >= 0.0f && t_face < a.tf) ? adj_idx : a.tf_id;
-                        a.tf = dp >= 0.0f ? fmin_t(t_face, a.tf) : a.tf;
-                        a.tn_id = (dp < 0.0f && t_face > a.tn) ? adj_idx : a.tn_id;
-                        a.tn = dp < 0.0f ? fmax_t(t_face, a.tn) : a.tn;
+                        if (face_may_clip(dp, f.w, a.tn, a.tf)) {
+                            float t_face = f.w / dp;
+                            a.tf_id = (dp >= 0.0f && t_face < a.tf) ? adj_idx : a.tf_id;
+                            a.tf = dp >= 0.0f ? fmin_t(t_face, a.tf) : a.tf;
+                            a.tn_id = (dp < 0.0f && t_face > a.tn) ? adj_idx : a.tn_id;
+                            a.tn = dp < 0.0f ? fmax_t(t_face, a.tn) : a.tn;
+                        }
                     }
-                    if (b.hit) {
+                    if (PPL == 2 && b.hit) {
                         float dp = dot(b.g.d, fn);
-                        float t_face = f.w / dp;
-                        b.tf_id = (dp >= 0.0f && t_face < b.tf) ? adj_idx : b.tf_id;
-                        b.tf = dp >= 0.0f ? fmin_t(t_face, b.tf) : b.tf;
-                        b.tn_id = (dp < 0.0f && t_face > b.tn) ? adj_idx : b.tn_id;
-                        b.tn = dp < 0.0f ? fmax_t(t_face, b.tn) : b.tn;
+                        if (face_may_clip(dp, f.w, b.tn, b.tf)) {
+                            float t_face = f.w / dp;
+                            b.tf_id = (dp >= 0.0f && t_face < b.tf) ? adj_idx : b.tf_id;
+                            b.tf = dp >= 0.0f ? fmin_t(t_face, b.tf) : b.tf;
+                            b.tn_id = (dp < 0.0f && t_face > b.tn) ? adj_idx : b.tn_id;
+                            b.tn = dp < 0.0f ? fmax_t(t_face, b.tn) : b.tn;
+                        }
                     }
                 }
                 __syncwarp();
@@ -514,7 +685,7 @@ PF_D void bwd_tile(const RasterParams& P, const BwdIn& in, const GradOut& go, in
             bool any_contrib = false;
             float g_c0 = 0.f, g_c1 = 0.f, g_c2 = 0.f, g_r = 0.f, g_n0 = 0.f, g_n1 = 0.f, g_n2 = 0.f, g_s = 0.f;
 #pragma unroll 1
-            for (int s = 0; s < 2; s++) {
+            for (int s = 0; s < PPL; s++) {
                 BwdPix& x = a;
                 if (x.hit) {  // oob pixels never hit here
                     const v3 d = x.g.d;
@@ -585,7 +756,7 @@ PF_D void bwd_tile(const RasterParams& P, const BwdIn& in, const GradOut& go, in
                             if (t_id == -1) {
                                 v3 ndc, fdc;
                                 float ndr, fdr;
-                                ray_sphere_bwd(o, d, center, radius, ndc, fdc, ndr, fdr);
+                                ray_sphere_bwd_d(o, d, center, radius, ndc, fdc, ndr, fdr);
                                 dLdcenter = dLdcenter + dLdt * (i == 0 ? ndc : fdc);
                                 dLdradius += dLdt * (i == 0 ? ndr : fdr);
                             } else if (t_id >= 0 && t_id < n_adj) {
@@ -600,7 +771,7 @@ PF_D void bwd_tile(const RasterParams& P, const BwdIn& in, const GradOut& go, in
                                 }
                                 v3 dc, dac;
                                 float dr, dar;
-                                ray_pface_bwd(o, d, center, radius, mk(as.x, as.y, as.z), as.w, dc, dr, dac, dar);
+                                ray_pface_bwd_d(o, d, center, radius, mk(as.x, as.y, as.z), as.w, dc, dr, dac, dar);
                                 dLdcenter = dLdcenter + dLdt * dc;
                                 dLdradius += dLdt * dr;
                                 v3 gac = dLdt * dac;
@@ -628,7 +799,7 @@ PF_D void bwd_tile(const RasterParams& P, const BwdIn& in, const GradOut& go, in
                         g_s += dLdsigma;
                     }
                 }
-                swap_pix(a, b);
+                if (PPL == 2) swap_pix(a, b);
             }
             if (__any_sync(0xffffffffu, any_contrib)) {
                 bs.acc[0][lane] += g_c0;
@@ -674,23 +845,21 @@ PF_D void bwd_tile(const RasterParams& P, const BwdIn& in, const GradOut& go, in
 }
 
 template <int TW>
-__global__ void __launch_bounds__(TW == 32 ? 512 : 128)
+__global__ void __launch_bounds__(Layout<TW>::THREADS)
 raster_bwd_kernel(RasterParams P, BwdIn in, GradOut go) {
-    constexpr int G = TW * TW / 64;
-    constexpr int WPB = G == 1 ? kWarpsPerBlock8 : G;
-    __shared__ WarpStage stage[WPB];
+    constexpr int G = Layout<TW>::G;
+    __shared__ WarpStage stage[G];
     extern __shared__ float4 dyn_smem[];
     BwdStage* bstage = reinterpret_cast<BwdStage*>(dyn_smem);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int wig = G == 1 ? 0 : warp;
     BwdStage& bs = bstage[warp];
     for (int r = 0; r < kAccRows; r++) bs.acc[r][lane] = 0.f;
     __syncwarp();
-    int64_t static_next = G == 1 ? (int64_t)blockIdx.x * WPB + warp : (int64_t)blockIdx.x;
+    int64_t static_next = (int64_t)blockIdx.x;
     for (;;) {
-        int64_t tile = next_tile<G>(P, static_next, lane);
+        int64_t tile = next_tile<G>(P, static_next, lane, nullptr);
         if (tile < 0) break;
-        bwd_tile<G>(P, in, go, tile, wig, lane, stage[warp], bs);
+        bwd_tile<G, Layout<TW>::PPL>(P, in, go, tile, warp, lane, stage[warp], bs);
     }
 }
 
@@ -706,14 +875,12 @@ __global__ void zero_nonfinite_kernel(float* __restrict__ a, int64_t n) {
 // grid: persistent when a queue is available, else one group per tile
 template <int TW, typename K>
 static unsigned composite_grid(const RasterParams& P, K kernel, size_t dyn_smem) {
-    constexpr int G = TW * TW / 64;
-    constexpr int WPB = G == 1 ? kWarpsPerBlock8 : G;
-    const int64_t groups = G == 1 ? (P.T + WPB - 1) / WPB : P.T;
+    const int64_t groups = P.T;
     if (!P.queue) return (unsigned)groups;
     int dev = 0, sms = 148, per_sm = 1;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 32 * WPB, dyn_smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, Layout<TW>::THREADS, dyn_smem);
     int64_t resident = (int64_t)sms * std::max(per_sm, 1);
     return (unsigned)std::max<int64_t>(1, std::min<int64_t>(groups, resident));
 }
@@ -741,30 +908,28 @@ extern "C" int pf_raster_forward(const pf_raster_inputs* in, int32_t return_poin
     if (return_point_err && P.N > 0) cudaMemsetAsync(point_err, 0, sizeof(float) * (size_t)P.N, st);
     if (tile_contrib_pairs && P.T > 0) cudaMemsetAsync(tile_contrib_pairs, 0, sizeof(int32_t) * (size_t)P.T, st);
     if (P.T == 0) return pf_check_launch("pf_raster_forward");
-    if (P.queue) cudaMemsetAsync(P.queue, 0, sizeof(int), st);
+    if (P.queue) cudaMemsetAsync(P.queue, 0, 2 * sizeof(int), st);
     FwdOut out{color, log_t, normal_distance, normal, quantile_depths, err, contrib, point_err, early_stop,
-               tile_contrib_pairs, return_point_err};
+               tile_contrib_pairs, return_point_err, P.queue ? P.queue + 1 : nullptr};
     if (P.TW == 8) {
         unsigned grid = composite_grid<8>(P, raster_fwd_kernel<8>, 0);
-        raster_fwd_kernel<8><<<grid, 32 * kWarpsPerBlock8, 0, st>>>(P, out);
+        raster_fwd_kernel<8><<<grid, Layout<8>::THREADS, 0, st>>>(P, out);
     } else if (P.TW == 16) {
         unsigned grid = composite_grid<16>(P, raster_fwd_kernel<16>, 0);
-        raster_fwd_kernel<16><<<grid, 128, 0, st>>>(P, out);
+        raster_fwd_kernel<16><<<grid, Layout<16>::THREADS, 0, st>>>(P, out);
     } else {
         unsigned grid = composite_grid<32>(P, raster_fwd_kernel<32>, 0);
-        raster_fwd_kernel<32><<<grid, 512, 0, st>>>(P, out);
+        raster_fwd_kernel<32><<<grid, Layout<32>::THREADS, 0, st>>>(P, out);
     }
     return pf_check_launch("pf_raster_forward");
 }
 
 template <int TW>
 static void launch_bwd(const RasterParams& P, const BwdIn& bi, const GradOut& go, cudaStream_t st) {
-    constexpr int G = TW * TW / 64;
-    constexpr int WPB = G == 1 ? kWarpsPerBlock8 : G;
-    const size_t dyn = sizeof(BwdStage) * WPB;
+    const size_t dyn = sizeof(BwdStage) * Layout<TW>::G;
     cudaFuncSetAttribute(raster_bwd_kernel<TW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
     unsigned grid = composite_grid<TW>(P, raster_bwd_kernel<TW>, dyn);
-    raster_bwd_kernel<TW><<<grid, 32 * WPB, dyn, st>>>(P, bi, go);
+    raster_bwd_kernel<TW><<<grid, Layout<TW>::THREADS, dyn, st>>>(P, bi, go);
 }
 
 extern "C" int pf_raster_backward(const pf_raster_inputs* in, const int32_t* early_stop, const float* log_t,
