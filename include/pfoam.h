@@ -109,6 +109,21 @@ PF_API int pf_bin(const pf_camera *cam, int32_t tile_width, const float *spheres
            int32_t *tile_order /* (T) or NULL: tiles by decreasing list length */,
            int64_t *n_pairs /* device scalar */, int32_t *status /* device scalar */, void *stream);
 
+/* Allocation-free binning: pf_bin with its scratch in a static device array
+ * (7 MiB, held by every GPU that loads the library), for callers that cannot
+ * allocate device memory while they render (a host application's frame
+ * callback, code that must not synchronise the device through cudaMalloc).
+ * No counterpart in the reference.  Limits: n_prims <= 65536,
+ * pair_capacity <= 262144, at most 16384 tiles; larger problems return
+ * PF_ERR_ARGS.  The first call on a device caches the array's address: make it
+ * before any stream capture.  All calls share the array, so calls that may
+ * overlap on the GPU race and must be serialised by the caller.  Outputs and
+ * *status as for pf_bin. */
+PF_API int pf_bin_noalloc(const pf_camera *cam, int32_t tile_width, const float *spheres, int64_t n_prims,
+                          int64_t pair_capacity, int64_t *tile_offsets, int32_t *tile_prims, int64_t *sort_keys,
+                          uint8_t *prim_visible, int32_t *tile_order, int64_t *n_pairs, int32_t *status,
+                          void *stream);
+
 /* ---------------------------------------------------------------------- */
 /* Neighbour encodings.
  * pf_adjacency_prefetch: (half(c_j - c_i), half(r_j)); replaces

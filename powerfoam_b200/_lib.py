@@ -94,6 +94,8 @@ _SIGS = {
     "pf_bin_workspace_size": [c_i64, c_i64, c_i64, ctypes.POINTER(ctypes.c_size_t)],
     "pf_bin": [ctypes.POINTER(PfCamera), c_i32, c_vp, c_i64, c_vp, ctypes.c_size_t, c_i64, c_vp, c_vp, c_vp, c_vp,
                c_vp, c_vp, c_vp, c_vp],
+    "pf_bin_noalloc": [ctypes.POINTER(PfCamera), c_i32, c_vp, c_i64, c_i64, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp,
+                       c_vp, c_vp],
     "pf_adjacency_prefetch": [c_vp, c_vp, c_vp, c_i64, c_vp, c_vp],
     "pf_adjacency_power_diff": [c_vp, c_vp, c_vp, c_vp, c_i64, c_vp, c_vp],
     "pf_raster_forward": [ctypes.POINTER(PfRasterInputs), c_i32, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp,

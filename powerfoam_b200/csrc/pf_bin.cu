@@ -9,6 +9,8 @@
 // 8-bit passes), the pairs are then emitted in that order and stably sorted by
 // tile (ceil(log2 T) bits).  Nothing here waits on the host: the pair count
 // stays on the device and a grid sized for the caller's capacity reads it.
+#include <mutex>
+
 #include "pf_common.cuh"
 #include "pf_sort.cuh"
 #include "pf_api.h"
@@ -344,4 +346,80 @@ extern "C" int pf_bin(const pf_camera* cam, int32_t tile_width, const float* sph
                                                                            sort_keys, status);
     order();
     return pf_check_launch("pf_bin");
+}
+
+// ---------------------------------------------------------------------------
+// Allocation-free binning.
+//
+// Some callers cannot allocate device memory at the moment they bin: a render
+// callback running inside another application's frame (a viewer or plugin host
+// that owns the CUDA context and its allocator), or code that must not call
+// cudaMalloc while the device is busy with other work, since that call can
+// synchronise the device.  pf_bin_noalloc serves them: the caller still passes
+// the inputs and every output, and the binning scratch lives in the
+// file-scope array below, so the call allocates nothing.
+//
+// Limits (the array is sized for them; larger problems are rejected with
+// PF_ERR_ARGS): at most kNoAllocMaxPrims primitives, kNoAllocMaxPairs
+// (tile, primitive) pairs of capacity and kNoAllocMaxTiles tiles.  The array
+// (kNoAllocBytes = 7 MiB) is held on every GPU that loads the library, until
+// the process exits.
+//
+// The first call on a device looks up the array's device address (with that
+// device current) and caches it; make that first call before any stream
+// capture.  Every call shares the one array: calls whose work may overlap on
+// the GPU (different streams, or different host threads, without ordering
+// between them) race on it and must be serialised by the caller.  No part of
+// the scratch needs to start at zero: every buffer in it is written before it
+// is read.  The caller's *status word must be zero before the call, as for
+// pf_bin.
+namespace pf {
+constexpr int64_t kNoAllocMaxPrims = 1 << 16;
+constexpr int64_t kNoAllocMaxPairs = 1 << 18;
+constexpr int64_t kNoAllocMaxTiles = 1 << 14;
+constexpr size_t kNoAllocBytes = (size_t)7 << 20;
+constexpr int kNoAllocMaxDevices = 64;
+
+static __device__ __align__(256) unsigned char g_bin_scratch[kNoAllocBytes];
+
+static std::mutex g_scratch_mu;
+static void* g_scratch_ptr[kNoAllocMaxDevices];
+}  // namespace pf
+
+extern "C" int pf_bin_noalloc(const pf_camera* cam, int32_t tile_width, const float* spheres, int64_t n_prims,
+                              int64_t pair_capacity, int64_t* tile_offsets, int32_t* tile_prims, int64_t* sort_keys,
+                              uint8_t* prim_visible, int32_t* tile_order, int64_t* n_pairs, int32_t* status,
+                              void* stream) {
+    if (!cam || tile_width <= 0 || cam->width < 2 || cam->height < 2)
+        return pf_fail(PF_ERR_ARGS, "pf_bin_noalloc: bad camera or tile width");
+    const int64_t T = (int64_t)(1 + (cam->height - 1) / tile_width) * (1 + (cam->width - 1) / tile_width);
+    if (n_prims < 0 || n_prims > kNoAllocMaxPrims)
+        return pf_fail(PF_ERR_ARGS, "pf_bin_noalloc: n_prims exceeds the static scratch limit of 65536 primitives");
+    if (pair_capacity < 0 || pair_capacity > kNoAllocMaxPairs)
+        return pf_fail(PF_ERR_ARGS, "pf_bin_noalloc: pair_capacity exceeds the static scratch limit of 262144 pairs");
+    if (T > kNoAllocMaxTiles)
+        return pf_fail(PF_ERR_ARGS, "pf_bin_noalloc: the image has more than 16384 tiles");
+    size_t need = 0;
+    int rc = pf_bin_workspace_size(n_prims, pair_capacity, T, &need);
+    if (rc != PF_OK) return rc;
+    if (need > kNoAllocBytes) return pf_fail(PF_ERR_ARGS, "pf_bin_noalloc: problem does not fit the static scratch");
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kNoAllocMaxDevices)
+        return pf_fail(PF_ERR_CUDA, "pf_bin_noalloc: no usable current device");
+    void* scratch = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(g_scratch_mu);
+        if (!g_scratch_ptr[dev]) {
+            void* p = nullptr;
+            cudaError_t e = cudaGetSymbolAddress(&p, g_bin_scratch);
+            if (e != cudaSuccess || !p) {
+                cudaGetLastError();
+                return pf_fail(PF_ERR_CUDA, "pf_bin_noalloc: cudaGetSymbolAddress of the static scratch failed");
+            }
+            g_scratch_ptr[dev] = p;
+        }
+        scratch = g_scratch_ptr[dev];
+    }
+    return pf_bin(cam, tile_width, spheres, n_prims, scratch, kNoAllocBytes, pair_capacity, tile_offsets, tile_prims,
+                  sort_keys, prim_visible, tile_order, n_pairs, status, stream);
 }
