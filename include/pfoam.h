@@ -221,6 +221,18 @@ PF_API int pf_trace_forward(const pf_trace_inputs *in, float *color, float *log_
                      int32_t *depth_seg, float *depth_sigma, int32_t *visit_log, int32_t visit_cap,
                      int32_t *visit_count, int32_t *status, void *stream);
 
+/* Adjoint of pf_trace_forward (no counterpart in the reference: its tracer
+ * is forward-only).  Takes the forward's colour, normal, depth_seg and
+ * depth_sigma and the upstream gradients of colour (H,W,3), log
+ * transmittance (H,W), depth (H,W) and normal (H,W,3) (any of the four may
+ * be NULL); writes (zeroes first) the gradients of every primitive attribute
+ * and zeroes non-finite entries.  Attributes must be f32. */
+PF_API int pf_trace_backward(const pf_trace_inputs *in, const float *color, const float *normal,
+                             const int32_t *depth_seg, const float *depth_sigma, const float *grad_color,
+                             const float *grad_log_t, const float *grad_depth, const float *grad_normal,
+                             float *grad_points, float *grad_radii, float *grad_normals, float *grad_density,
+                             float *grad_texel_sites, float *grad_texel_rgb, float *grad_texel_height, void *stream);
+
 /* Start cell of benchmark.py:320-324: argmin_i |p_i - eye|^2 - r_i^2 (first
  * index on ties).  workspace: pf_start_cell_workspace_size bytes. */
 PF_API int pf_start_cell_workspace_size(int64_t n_prims, size_t *bytes);

@@ -120,13 +120,15 @@ def raster_forward(cam, tile_width, spheres, nsigmas, sites, rgbh, adj, adj_off,
     T = tile_offsets.shape[0] - 1
     Q = 0 if depth_q is None else depth_q.shape[-1]
     args = [_c(spheres, F32), _c(nsigmas, F32), _c(sites, F32), _c(rgbh, F32), _c(adj, np.int32),
-            _c(adj_off, np.int32), _c(adj_diff, np.uint16), _c(tile_offsets, np.int64), _c(tile_prims, np.int32)]
+            _c(adj_off, np.int32), None if adj_diff is None else _c(adj_diff, np.uint16), _c(tile_offsets, np.int64),
+            _c(tile_prims, np.int32)]
     dq = None if depth_q is None else _c(depth_q, F32)
     gt = None if ray_gt is None else _c(ray_gt, F32)
-    out = dict(color=np.zeros((H, W, 3), F32), log_t=np.zeros((H, W), F32), normal_distance=np.zeros((H, W), F32),
-               normal=np.zeros((H, W, 3), F32), quantile_depths=-np.ones((H, W, max(Q, 1)), F32),
-               contrib=np.zeros(N, F32), point_err=np.zeros(N, F32), early_stop=np.zeros(T, np.int32),
-               err=np.zeros((H, W), F32) if surface else None)
+    R = np.float64 if prec == "f64" else F32
+    out = dict(color=np.zeros((H, W, 3), R), log_t=np.zeros((H, W), R), normal_distance=np.zeros((H, W), R),
+               normal=np.zeros((H, W, 3), R), quantile_depths=-np.ones((H, W, max(Q, 1)), R),
+               contrib=np.zeros(N, R), point_err=np.zeros(N, R), early_stop=np.zeros(T, np.int32),
+               err=np.zeros((H, W), R) if surface else None)
     rc = _fn("orc_raster_forward", prec)(
         ctypes.byref(cam), ctypes.c_int(tile_width), ctypes.c_int64(N), *[_p(a) for a in args[:4]], ctypes.c_int(S),
         *[_p(a) for a in args[4:]], _p(dq), ctypes.c_int(Q), _p(gt), ctypes.c_float(thr),
@@ -148,11 +150,12 @@ def raster_backward(cam, tile_width, spheres, nsigmas, sites, rgbh, adj, adj_off
     g = dict(spheres=np.zeros((N, 4), F32), nsigmas=np.zeros((N, 4), F32), texel_sites=np.zeros((N, S, 3), F32),
              texel_rgb=np.zeros((N, S, 3), F32), texel_height=np.zeros((N, S), F32))
     args = [_c(spheres, F32), _c(nsigmas, F32), _c(sites, F32), _c(rgbh, F32)]
-    args2 = [_c(adj, np.int32), _c(adj_off, np.int32), _c(adj_diff, np.uint16), _c(tile_offsets, np.int64),
-             _c(tile_prims, np.int32), _c(early_stop, np.int32)]
+    args2 = [_c(adj, np.int32), _c(adj_off, np.int32), None if adj_diff is None else _c(adj_diff, np.uint16),
+             _c(tile_offsets, np.int64), _c(tile_prims, np.int32), _c(early_stop, np.int32)]
     dq = None if depth_q is None else _c(depth_q, F32)
     gq = None if grad_qd is None else _c(grad_qd, F32)
     ins = [_c(log_t, F32), _c(grad_color, F32), _c(grad_log_t, F32), _c(grad_nd, F32), _c(grad_normal, F32)]
+    adj_diff = None if adj_diff is None else _c(adj_diff, np.uint16)
     rc = _fn("orc_raster_backward", prec)(
         ctypes.byref(cam), ctypes.c_int(tile_width), ctypes.c_int64(N), *[_p(a) for a in args], ctypes.c_int(S),
         *[_p(a) for a in args2], _p(dq), ctypes.c_int(Q), *[_p(a) for a in ins], _p(gq),
@@ -197,19 +200,20 @@ def raster_visualize(cam, tile_width, spheres, nsigmas, sites, rgbs, heights, ad
 def trace_forward(cam, spheres, nsigmas, sites, rgbs, heights, adj, adj_off, adj_diff_pm, start_idx=0,
                   start_cells=None, thr=1e-3, max_steps=1 << 16, depth_quantile=0.5, visit_cap=0, prec="f32"):
     H, W = cam.height, cam.width
-    P = H * W
     S = sites.shape[1]
-    out = dict(color=np.zeros((H, W, 3), F32), log_t=np.zeros((H, W), F32), depth=np.zeros((H, W), F32),
-               normal=np.zeros((H, W, 3), F32), depth_seg=np.zeros((H, W), np.int32),
-               depth_sigma=np.zeros((H, W), F32), visit_count=np.zeros((H, W), np.int32),
+    R = np.float64 if prec == "f64" else F32
+    out = dict(color=np.zeros((H, W, 3), R), log_t=np.zeros((H, W), R), depth=np.zeros((H, W), R),
+               normal=np.zeros((H, W, 3), R), depth_seg=np.zeros((H, W), np.int32),
+               depth_sigma=np.zeros((H, W), R), visit_count=np.zeros((H, W), np.int32),
                status=np.zeros((H, W), np.int32))
     vl = np.full((H, W, max(visit_cap, 1)), -1, np.int32) if visit_cap else None
     args = [_c(spheres, F32), _c(nsigmas, F32), _c(sites, F32), _c(rgbs, F32), _c(heights, F32)]
     sc = None if start_cells is None else _c(start_cells, np.int32)
     rc = _fn("orc_trace_forward", prec)(
         ctypes.byref(cam), *[_p(a) for a in args], ctypes.c_int(S), _p(_c(adj, np.int32)),
-        _p(_c(adj_off, np.int32)), _p(_c(adj_diff_pm, np.uint16)), ctypes.c_int32(start_idx), _p(sc),
-        ctypes.c_float(thr), ctypes.c_int(max_steps), ctypes.c_float(depth_quantile), _p(out["color"]),
+        _p(_c(adj_off, np.int32)), _p(None if adj_diff_pm is None else _c(adj_diff_pm, np.uint16)),
+        ctypes.c_int32(start_idx), _p(sc), ctypes.c_float(thr), ctypes.c_int(max_steps),
+        ctypes.c_float(depth_quantile), _p(out["color"]),
         _p(out["log_t"]), _p(out["depth"]), _p(out["normal"]), _p(out["depth_seg"]), _p(out["depth_sigma"]),
         _p(vl), ctypes.c_int(visit_cap), _p(out["visit_count"]), _p(out["status"]))
     out["rc"] = rc
@@ -235,3 +239,28 @@ def sh_texel_rgb(points, sh, eye, S=8):
 
 def num_threads():
     return int(lib().orc_num_threads_f32())
+
+
+def trace_backward(cam, spheres, nsigmas, sites, rgbs, heights, adj, adj_off, adj_diff_pm, fwd, g_color=None,
+                   g_log_t=None, g_depth=None, g_normal=None, start_idx=0, start_cells=None, thr=1e-3,
+                   max_steps=1 << 16, depth_quantile=0.5, prec="f32"):
+    """Exact adjoint of trace_forward (see pf_oracle.c).  ``fwd`` is the dict
+    returned by trace_forward with the same arguments."""
+    N = spheres.shape[0]
+    S = sites.shape[1]
+    R = np.float64 if prec == "f64" else F32
+    g = dict(spheres=np.zeros((N, 4), F32), nsigmas=np.zeros((N, 4), F32), texel_sites=np.zeros((N, S, 3), F32),
+             texel_rgb=np.zeros((N, S, 3), F32), texel_height=np.zeros((N, S), F32))
+    args = [_c(spheres, F32), _c(nsigmas, F32), _c(sites, F32), _c(rgbs, F32), _c(heights, F32)]
+    sc = None if start_cells is None else _c(start_cells, np.int32)
+    opt = lambda a: None if a is None else _c(a, F32)
+    rc = _fn("orc_trace_backward", prec)(
+        ctypes.byref(cam), *[_p(a) for a in args], ctypes.c_int(S), _p(_c(adj, np.int32)), _p(_c(adj_off, np.int32)),
+        _p(None if adj_diff_pm is None else _c(adj_diff_pm, np.uint16)), ctypes.c_int32(start_idx), _p(sc),
+        ctypes.c_float(thr),
+        ctypes.c_int(max_steps), ctypes.c_float(depth_quantile), _p(_c(fwd["color"], R)),
+        _p(_c(fwd["normal"], R)), _p(_c(fwd["depth_seg"], np.int32)), _p(_c(fwd["depth_sigma"], R)),
+        _p(opt(g_color)), _p(opt(g_log_t)), _p(opt(g_depth)), _p(opt(g_normal)), _p(g["spheres"]),
+        _p(g["nsigmas"]), _p(g["texel_sites"]), _p(g["texel_rgb"]), _p(g["texel_height"]))
+    assert rc == 0
+    return g

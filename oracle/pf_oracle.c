@@ -53,6 +53,10 @@ typedef float real;
 
 #define K(x) ((real)(x)) /* a Warp float literal: Python double rounded to float32 */
 
+/* image-space outputs are float32 in the f32 build and float64 in the f64
+ * build (finite-difference checks need the extra digits) */
+typedef real out_t;
+
 /* ------------------------------------------------------------------------ */
 /* status codes (shared meaning with include/pfoam.h)                        */
 #define ORC_OK 0
@@ -565,9 +569,9 @@ static plane_res plane_fwd_local(v3 o, v3 d, real t_near, v3 po, v3 pn, real rad
 }
 
 #ifdef _OPENMP
-#define ATOMIC_ADD(dst, v) do { real _v = (v); _Pragma("omp atomic") (dst) += (float)_v; } while (0)
+#define ATOMIC_ADD(dst, v) do { real _v = (v); _Pragma("omp atomic") (dst) += (__typeof__(dst))_v; } while (0)
 #else
-#define ATOMIC_ADD(dst, v) ((dst) += (float)(v))
+#define ATOMIC_ADD(dst, v) ((dst) += (__typeof__(dst))(v))
 #endif
 
 /* texture.py:74-186 plane_intersection_bwd.  Gradient accumulators are the
@@ -648,6 +652,24 @@ static void plane_bwd(v3 o, v3 d, real _t_near, v3 po, v3 pn, real radius, int h
     *dLdpo_out = dLdpo; *dLdpn_out = dLdpn; *dLd_t_near_out = dLd_t_near;
 }
 
+/* Neighbour e of a primitive as the face clip sees it: centre + half(c_j - c_i)
+ * and half(r_j) from the prefetched encoding (rasterize.py:1054-1058); with
+ * adj_diff == NULL the exact neighbour sphere (used by finite-difference
+ * checks, where the float16 quantisation would make the image piecewise
+ * constant in the primitive positions). */
+static void nbr_sphere(const float *spheres, const int32_t *adj, const uint16_t *adj_diff, int32_t e, v3 center,
+                       v3 *ac, real *ar) {
+    if (adj_diff) {
+        const uint16_t *h = adj_diff + 4 * (int64_t)e;
+        *ac = vadd(center, mk((real)FN(orc_h2f)(h[0]), (real)FN(orc_h2f)(h[1]), (real)FN(orc_h2f)(h[2])));
+        *ar = (real)FN(orc_h2f)(h[3]);
+    } else {
+        const float *t = spheres + 4 * (int64_t)adj[e];
+        *ac = ld3(t);
+        *ar = (real)t[3];
+    }
+}
+
 /* ------------------------------------------------------------------------ */
 /* Rasterizer forward (rasterize.py:892-1146 forward_kernel, host side      */
 /* rasterize.py:1587-1856).  One tile = one Warp block of TW*TW threads; the */
@@ -683,9 +705,9 @@ int FN(orc_raster_forward)(const orc_camera *camera, int TW, int64_t N, const fl
                            const float *nsigmas, const float *sites, const float *rgbh, int S,
                            const int32_t *adj, const int32_t *adj_off, const uint16_t *adj_diff,
                            const int64_t *tile_offsets, const int32_t *tile_prims, const float *depth_q,
-                           int Q, const float *ray_gt, float thr, int return_point_err, float *color,
-                           float *log_t_out, float *nd_out, float *normal_out, float *qdepth_out,
-                           float *err_out, float *contrib, float *point_err, int32_t *early_stop) {
+                           int Q, const float *ray_gt, float thr, int return_point_err, out_t *color,
+                           out_t *log_t_out, out_t *nd_out, out_t *normal_out, out_t *qdepth_out,
+                           out_t *err_out, out_t *contrib, out_t *point_err, int32_t *early_stop) {
     (void)N; (void)adj;
     cam_t cam = cam_load(camera);
     int tiles_h = 1 + (cam.H - 1) / TW, tiles_w = 1 + (cam.W - 1) / TW;
@@ -735,10 +757,9 @@ int FN(orc_raster_forward)(const orc_camera *camera, int TW, int64_t N, const fl
                 real tn = a->tn, tf = a->tf;
                 if (a->hit) {
                     for (int32_t e = a0; e < a1; e++) {
-                        const uint16_t *h = adj_diff + 4 * (int64_t)e;
-                        v3 ac = vadd(center, mk((real)FN(orc_h2f)(h[0]), (real)FN(orc_h2f)(h[1]),
-                                                (real)FN(orc_h2f)(h[2])));
-                        real ar = (real)FN(orc_h2f)(h[3]);
+                        v3 ac;
+                        real ar;
+                        nbr_sphere(spheres, adj, adj_diff, e, center, &ac, &ar);
                         real dp;
                         real t_face = ray_pface(o, a->d, center, radius, ac, ar, &dp);
                         tf = dp >= K(0.0) ? rmin(t_face, tf) : tf;
@@ -772,7 +793,7 @@ int FN(orc_raster_forward)(const orc_camera *camera, int TW, int64_t N, const fl
                     int64_t px = (int64_t)a->pi * cam.W + a->pj;
                     while (a->qi < nq && next_trans < a->q) {
                         real qd = tn + r_log(trans / a->q) / sigma;
-                        qdepth_out[px * Q + a->qi] = (float)qd;
+                        qdepth_out[px * Q + a->qi] = (out_t)qd;
                         a->qi += 1;
                         if (a->qi < nq) a->q = (real)depth_q[px * Q + a->qi];
                     }
@@ -784,17 +805,17 @@ int FN(orc_raster_forward)(const orc_camera *camera, int TW, int64_t N, const fl
             fwd_lane *a = &L[l];
             if (a->oob) continue;
             int64_t px = (int64_t)a->pi * cam.W + a->pj;
-            color[3 * px + 0] = (float)a->rgb.x;
-            color[3 * px + 1] = (float)a->rgb.y;
-            color[3 * px + 2] = (float)a->rgb.z;
-            log_t_out[px] = (float)a->log_t;
-            nd_out[px] = (float)a->nd;
-            normal_out[3 * px + 0] = (float)a->normal.x;
-            normal_out[3 * px + 1] = (float)a->normal.y;
-            normal_out[3 * px + 2] = (float)a->normal.z;
+            color[3 * px + 0] = (out_t)a->rgb.x;
+            color[3 * px + 1] = (out_t)a->rgb.y;
+            color[3 * px + 2] = (out_t)a->rgb.z;
+            log_t_out[px] = (out_t)a->log_t;
+            nd_out[px] = (out_t)a->nd;
+            normal_out[3 * px + 0] = (out_t)a->normal.x;
+            normal_out[3 * px + 1] = (out_t)a->normal.y;
+            normal_out[3 * px + 2] = (out_t)a->normal.z;
             if (err_out) {
                 v3 de = vsub(mk(0, 0, 0), a->gt);
-                err_out[px] = (float)(a->err + dot(de, de) * r_exp(a->log_t));
+                err_out[px] = (out_t)(a->err + dot(de, de) * r_exp(a->log_t));
             }
         }
         free(L);
@@ -890,10 +911,9 @@ int FN(orc_raster_backward)(const orc_camera *camera, int TW, int64_t N, const f
                 int t_far_id = t_far < K(1e-8) ? -2 : -1;
                 if (hit) {
                     for (int32_t e = a0; e < a1; e++) {
-                        const uint16_t *h = adj_diff + 4 * (int64_t)e;
-                        v3 ac = vadd(center, mk((real)FN(orc_h2f)(h[0]), (real)FN(orc_h2f)(h[1]),
-                                                (real)FN(orc_h2f)(h[2])));
-                        real ar = (real)FN(orc_h2f)(h[3]);
+                        v3 ac;
+                        real ar;
+                        nbr_sphere(spheres, adj, adj_diff, e, center, &ac, &ar);
                         real dp;
                         real t_face = ray_pface(o, a->d, center, radius, ac, ar, &dp);
                         int adj_idx = e - a0;
@@ -1195,12 +1215,30 @@ int FN(orc_raster_visualize)(const orc_camera *camera, int TW, const float *sphe
 /* the only state the backward needs besides the forward outputs.            */
 #define NO_CELL 0x7FFFFFFF
 
+/* (c_j - c_i, pm_j - pm_i) of neighbour e: from the float16 encoding of
+ * benchmark.py:296-302, or exactly from the spheres when adj_diff == NULL
+ * (finite-difference checks) */
+static void nbr_pm(const float *spheres, const int32_t *adj, const uint16_t *adj_diff, int32_t prim, int32_t e,
+                   v3 *diff, real *pm) {
+    if (adj_diff) {
+        const uint16_t *h = adj_diff + 4 * (int64_t)e;
+        *diff = mk((real)FN(orc_h2f)(h[0]), (real)FN(orc_h2f)(h[1]), (real)FN(orc_h2f)(h[2]));
+        *pm = (real)FN(orc_h2f)(h[3]);
+    } else {
+        const float *si = spheres + 4 * (int64_t)prim, *sj = spheres + 4 * (int64_t)adj[e];
+        v3 ci = ld3(si), cj = ld3(sj);
+        real ri = (real)si[3], rj = (real)sj[3];
+        *diff = vsub(cj, ci);
+        *pm = K(0.5) * (dot(cj, cj) - rj * rj) - K(0.5) * (dot(ci, ci) - ri * ri);
+    }
+}
+
 int FN(orc_trace_forward)(const orc_camera *camera, const float *spheres, const float *nsigmas,
                           const float *sites, const float *rgbs, const float *heights, int S,
                           const int32_t *adj, const int32_t *adj_off, const uint16_t *adj_diff,
                           int32_t start_idx, const int32_t *start_cells, float thr, int max_steps,
-                          float depth_quantile, float *color, float *log_t_out, float *depth, float *normal,
-                          int32_t *depth_seg, float *depth_sigma, int32_t *visit_log, int visit_cap,
+                          float depth_quantile, out_t *color, out_t *log_t_out, out_t *depth, out_t *normal,
+                          int32_t *depth_seg, out_t *depth_sigma, int32_t *visit_log, int visit_cap,
                           int32_t *visit_count, int32_t *status) {
     cam_t cam = cam_load(camera);
     int64_t P = (int64_t)cam.H * cam.W;
@@ -1234,9 +1272,9 @@ int FN(orc_trace_forward)(const orc_camera *camera, const float *spheres, const 
             int32_t next = NO_CELL;
             real pt_far = K(1e10);
             for (int32_t e = adj_off[prim]; e < adj_off[prim + 1]; e++) {
-                const uint16_t *h = adj_diff + 4 * (int64_t)e;
-                v3 diff = mk((real)FN(orc_h2f)(h[0]), (real)FN(orc_h2f)(h[1]), (real)FN(orc_h2f)(h[2]));
-                real pm = (real)FN(orc_h2f)(h[3]);
+                v3 diff;
+                real pm;
+                nbr_pm(spheres, adj, adj_diff, prim, e, &diff, &pm);
                 real dp;
                 real t_face = ray_pface_diff(o, d, diff, pm, &dp);
                 if (dp >= K(0.0) && t_face < pt_far) { next = adj[e]; pt_far = t_face; }
@@ -1272,18 +1310,18 @@ int FN(orc_trace_forward)(const orc_camera *camera, const float *spheres, const 
                 seg++;
             }
         }
-        color[3 * px + 0] = (float)rgb.x;
-        color[3 * px + 1] = (float)rgb.y;
-        color[3 * px + 2] = (float)rgb.z;
-        if (log_t_out) log_t_out[px] = (float)log_t;
-        if (depth) depth[px] = (float)dout;
+        color[3 * px + 0] = (out_t)rgb.x;
+        color[3 * px + 1] = (out_t)rgb.y;
+        color[3 * px + 2] = (out_t)rgb.z;
+        if (log_t_out) log_t_out[px] = (out_t)log_t;
+        if (depth) depth[px] = (out_t)dout;
         if (normal) {
-            normal[3 * px + 0] = (float)nacc.x;
-            normal[3 * px + 1] = (float)nacc.y;
-            normal[3 * px + 2] = (float)nacc.z;
+            normal[3 * px + 0] = (out_t)nacc.x;
+            normal[3 * px + 1] = (out_t)nacc.y;
+            normal[3 * px + 2] = (out_t)nacc.z;
         }
         if (depth_seg) depth_seg[px] = dseg;
-        if (depth_sigma) depth_sigma[px] = (float)dsig;
+        if (depth_sigma) depth_sigma[px] = (out_t)dsig;
         if (visit_count) visit_count[px] = steps;
         if (status) status[px] = st;
         if (st > worst) worst = st;
@@ -1347,4 +1385,311 @@ int FN(orc_num_threads)(void) {
 #else
     return 1;
 #endif
+}
+
+/* ------------------------------------------------------------------------ */
+/* Ray-tracer adjoint.  The reference tracer (raytrace.py:115-241) has no   */
+/* backward; this is the exact derivative of orc_trace_forward's colour,    */
+/* log transmittance, depth and normal outputs with respect to every        */
+/* primitive attribute.  Per ray the walk is repeated front to back; with   */
+/* the forward's final colour C and normal N,                               */
+/*   dL/d delta_k = gC.(C - C_<=k - c_k T_k+1) + gN.(N - N_<=k - n_k T_k+1)  */
+/*                  + gL + [k < m] gD / sigma_m        (delta = -sigma dt)   */
+/* where m is the segment that produced the depth.  dL/dt_near and          */
+/* dL/dt_far go to the one surface that bounds each end of the segment      */
+/* (sphere, power face or texture plane).  Face derivatives use the exact   */
+/* spheres (the walk itself uses the float16 encoding, as the forward).     */
+/* The texture plane's derivative includes every dependency of the local    */
+/* variant (sites, colours, heights, plane origin and normal, the query     */
+/* depth and the radius through 1/r^2).  Gradients accumulate into the     */
+/* zeroed outputs (float atomics).                                          */
+
+typedef struct {
+    int hit;         /* contributes */
+    real tn, tf, dt; /* final segment */
+    int tn_id, tf_id, pre_tn_id, pre_tf_id; /* -2 none, -1 sphere, k face, n_adj plane */
+    real pre_tn;     /* t_near before the plane (query depth of the texture) */
+    plane_res pr;
+    int32_t next;
+    real sigma;
+    v3 center, pn;
+    real radius;
+} trace_seg;
+
+/* one step of the walk at cell `prim`; mirrors orc_trace_forward */
+static void trace_step(v3 o, v3 d, const float *spheres, const float *nsigmas, const float *sites, const float *rgbs,
+                       const float *heights, int S, const int32_t *adj, const int32_t *adj_off,
+                       const uint16_t *adj_diff, int32_t prim, trace_seg *sg) {
+    const float *sp = spheres + 4 * (int64_t)prim;
+    v3 center = ld3(sp);
+    real radius = (real)sp[3];
+    real tn, tf;
+    int hit = ray_sphere(o, d, center, radius, &tn, &tf);
+    v3 v = vsub(center, o);
+    if (length(v) < K(4.0) * radius) hit = 0;
+    int tn_id = tn < K(1e-8) ? -2 : -1, tf_id = tf < K(1e-8) ? -2 : -1;
+    int32_t next = NO_CELL;
+    real pt_far = K(1e10);
+    int32_t a0 = adj_off[prim], a1 = adj_off[prim + 1];
+    for (int32_t e = a0; e < a1; e++) {
+        v3 diff;
+        real pm;
+        nbr_pm(spheres, adj, adj_diff, prim, e, &diff, &pm);
+        real dp;
+        real t_face = ray_pface_diff(o, d, diff, pm, &dp);
+        if (dp >= K(0.0) && t_face < pt_far) { next = adj[e]; pt_far = t_face; }
+        if (dp >= K(0.0) && t_face < tf) tf_id = e - a0;
+        tf = dp >= K(0.0) ? rmin(t_face, tf) : tf;
+        if (dp < K(0.0) && t_face > tn) tn_id = e - a0;
+        tn = dp < K(0.0) ? rmax(t_face, tn) : tn;
+    }
+    const float *ns = nsigmas + 4 * (int64_t)prim;
+    v3 pn = ld3(ns);
+    real sigma = (real)ns[3];
+    sg->next = next;
+    sg->sigma = sigma;
+    sg->center = center;
+    sg->pn = pn;
+    sg->radius = radius;
+    sg->hit = 0;
+    if (!hit || tn > tf || sigma < K(1e-3)) return;
+    sg->pre_tn = tn;
+    sg->pre_tn_id = tn_id;
+    sg->pre_tf_id = tf_id;
+    plane_res pr = plane_fwd_local(o, d, tn, center, pn, radius, sites + (int64_t)prim * S * 3,
+                                   rgbs + (int64_t)prim * S * 3, heights + (int64_t)prim * S, S);
+    int n_adj = a1 - a0;
+    if (pr.dp >= K(0.0) && pr.t_surf < tf) tf_id = n_adj;
+    tf = pr.dp >= K(0.0) ? rmin(pr.t_surf, tf) : tf;
+    if (pr.dp < K(0.0) && pr.t_surf > tn) tn_id = n_adj;
+    tn = pr.dp < K(0.0) ? rmax(pr.t_surf, tn) : tn;
+    sg->pr = pr;
+    sg->tn = tn;
+    sg->tf = tf;
+    sg->tn_id = tn_id;
+    sg->tf_id = tf_id;
+    sg->dt = tf - tn;
+    sg->hit = sg->dt > K(0.0);
+}
+
+static void add3(float *g, v3 v) {
+    ATOMIC_ADD(g[0], v.x);
+    ATOMIC_ADD(g[1], v.y);
+    ATOMIC_ADD(g[2], v.z);
+}
+
+/* derivative of the local texture plane (rasterize.py:62-137 / raytrace.py:
+ * 42-113) for upstream dL/drgb and dL/dt_surf; returns dL/d(pre-plane
+ * t_near) and accumulates into the primitive's gradients */
+static real plane_local_bwd(v3 o, v3 d, real tn, v3 po, v3 pn, real radius, const float *sites, const float *rgbs,
+                            const float *heights, int S, const plane_res *pr, v3 g_rgb, real g_tsurf, v3 *g_po,
+                            v3 *g_pn, real *g_radius, float *gs, float *gr, float *gh) {
+    real inv_r2 = K(1.0) / (radius * radius);
+    real g_inv_r2 = 0, g_tn = 0;
+    /* colour pass at pt */
+    real tq = pr->dp >= K(0.0) ? tn : rmax(tn, pr->t_surf);
+    v3 pt = vadd(o, smul(tq, d));
+    real V = pr->wsum; /* already clamped */
+    int vclamp = !(pr->wsum > K(1e-20)) ? 0 : 1;
+    v3 g_pt = mk(0, 0, 0);
+    for (int i = 0; i < S; i++) {
+        v3 s = ld3(sites + 3 * i);
+        v3 df = vsub(pt, s);
+        real q2 = dot(df, df);
+        real vi = r_exp(-TEMP * q2 * inv_r2);
+        v3 ci = ld3(rgbs + 3 * i);
+        v3 gci = smul(vi / V, g_rgb);
+        ATOMIC_ADD(gr[3 * i + 0], gci.x);
+        ATOMIC_ADD(gr[3 * i + 1], gci.y);
+        ATOMIC_ADD(gr[3 * i + 2], gci.z);
+        real g_vi = vclamp ? dot(vsub(ci, pr->rgb), g_rgb) / V : dot(ci, g_rgb) / V;
+        /* dv/dpt = v (-2 T inv_r2) (pt - s) */
+        v3 dvdpt = smul(vi * (-K(2.0) * TEMP * inv_r2), df);
+        g_pt = vadd(g_pt, smul(g_vi, dvdpt));
+        v3 gsi = smul(-g_vi, dvdpt);
+        ATOMIC_ADD(gs[3 * i + 0], gsi.x);
+        ATOMIC_ADD(gs[3 * i + 1], gsi.y);
+        ATOMIC_ADD(gs[3 * i + 2], gsi.z);
+        g_inv_r2 += g_vi * vi * (-TEMP * q2);
+    }
+    real g_tq = dot(g_pt, d);
+    real g_tsurf_all = g_tsurf;
+    if (pr->dp >= K(0.0) || tn > pr->t_surf) g_tn += g_tq;
+    else g_tsurf_all += g_tq;
+    /* t_surf = (dot(po - o, pn) + height) / dp */
+    real g_height = 0;
+    if (g_tsurf_all != K(0.0)) {
+        real k = g_tsurf_all / pr->dp;
+        *g_po = vadd(*g_po, smul(k, pn));
+        *g_pn = vadd(*g_pn, smul(k, vsub(vsub(po, o), smul(pr->t_surf, d))));
+        g_height = k;
+    }
+    /* height pass at _pt */
+    real _tq = pr->_dp >= K(0.0) ? tn : rmax(tn, pr->_t_surf);
+    v3 _pt = vadd(o, smul(_tq, d));
+    real W = pr->_wsum;
+    int wclamp = pr->_wsum > K(1e-20);
+    v3 g__pt = mk(0, 0, 0);
+    if (g_height != K(0.0)) {
+        for (int i = 0; i < S; i++) {
+            v3 s = ld3(sites + 3 * i);
+            v3 df = vsub(_pt, s);
+            real q2 = dot(df, df);
+            real wi = r_exp(-TEMP * q2 * inv_r2);
+            real hi = (real)heights[i];
+            ATOMIC_ADD(gh[i], wi / W * g_height);
+            real g_wi = wclamp ? (hi - pr->height) / W * g_height : hi / W * g_height;
+            v3 dwdpt = smul(wi * (-K(2.0) * TEMP * inv_r2), df);
+            g__pt = vadd(g__pt, smul(g_wi, dwdpt));
+            v3 gsi = smul(-g_wi, dwdpt);
+            ATOMIC_ADD(gs[3 * i + 0], gsi.x);
+            ATOMIC_ADD(gs[3 * i + 1], gsi.y);
+            ATOMIC_ADD(gs[3 * i + 2], gsi.z);
+            g_inv_r2 += g_wi * wi * (-TEMP * q2);
+        }
+    }
+    real g__tq = dot(g__pt, d);
+    if (g__tq != K(0.0)) {
+        if (pr->_dp >= K(0.0) || tn > pr->_t_surf) {
+            g_tn += g__tq;
+        } else {
+            real k = g__tq / pr->_dp;
+            *g_po = vadd(*g_po, smul(k, pn));
+            *g_pn = vadd(*g_pn, smul(k, vsub(vsub(po, o), smul(pr->_t_surf, d))));
+        }
+    }
+    *g_radius += g_inv_r2 * (-K(2.0) / (radius * radius * radius));
+    return g_tn;
+}
+
+/* d t / d (centre, radius) of the near (sign -1) or far (+1) sphere root:
+ * t = (-qb -+ s)/2, qb = 2 oc.d, s = sqrt(qb^2 - 4 (|oc|^2 - r^2)), oc = o - c */
+static void sphere_root_grad(v3 o, v3 d, v3 c, real r, int far, v3 *dc, real *dr) {
+    v3 oc = vsub(o, c);
+    real qb = K(2.0) * dot(oc, d);
+    real qc = dot(oc, oc) - r * r;
+    real s = r_sqrt(qb * qb - K(4.0) * qc);
+    /* d disc / dc = -4 qb d + 8 oc */
+    v3 ddisc = vadd(smul(-K(4.0) * qb, d), smul(K(8.0), oc));
+    v3 ds = smul(K(1.0) / (K(2.0) * s), ddisc);
+    real sg = far ? K(1.0) : K(-1.0);
+    *dc = vadd(d, smul(sg * K(0.5), ds));
+    *dr = sg * K(2.0) * r / s;
+}
+
+/* d t / d (c_i, r_i, c_j, r_j) of the power face between i and j */
+static void face_grad(v3 o, v3 d, v3 ci, real ri, v3 cj, real rj, v3 *dci, real *dri, v3 *dcj, real *drj) {
+    v3 n = vsub(cj, ci);
+    real num = K(0.5) * (dot(cj, cj) - rj * rj - dot(ci, ci) + ri * ri) - dot(o, n);
+    real den = dot(d, n);
+    real t = num / den;
+    *dci = smul(K(1.0) / den, vadd(vsub(o, ci), smul(t, d)));
+    *dcj = smul(K(1.0) / den, vsub(vsub(cj, o), smul(t, d)));
+    *dri = ri / den;
+    *drj = -rj / den;
+}
+
+int FN(orc_trace_backward)(const orc_camera *camera, const float *spheres, const float *nsigmas, const float *sites,
+                           const float *rgbs, const float *heights, int S, const int32_t *adj, const int32_t *adj_off,
+                           const uint16_t *adj_diff, int32_t start_idx, const int32_t *start_cells, float thr,
+                           int max_steps, float depth_quantile, const out_t *color, const out_t *normal,
+                           const int32_t *depth_seg, const out_t *depth_sigma, const float *g_color,
+                           const float *g_log_t, const float *g_depth, const float *g_normal, float *g_spheres,
+                           float *g_nsigmas, float *g_sites, float *g_rgb, float *g_height) {
+    cam_t cam = cam_load(camera);
+    int64_t P = (int64_t)cam.H * cam.W;
+    v3 o = cam.eye;
+#pragma omp parallel for schedule(dynamic, 64)
+    for (int64_t px = 0; px < P; px++) {
+        int pi = (int)(px / cam.W), pj = (int)(px % cam.W);
+        v3 rd = get_ray_dir(&cam, (real)pi, (real)pj);
+        v3 d = vdivs(rd, length(rd));
+        v3 gC = g_color ? ld3(g_color + 3 * px) : mk(0, 0, 0);
+        v3 gN = g_normal ? ld3(g_normal + 3 * px) : mk(0, 0, 0);
+        real gL = g_log_t ? (real)g_log_t[px] : 0;
+        real gD = g_depth ? (real)g_depth[px] : 0;
+        int m = depth_seg ? depth_seg[px] : -1;
+        real sig_m = depth_sigma ? (real)depth_sigma[px] : 1;
+        v3 Cf = mk((real)color[3 * px], (real)color[3 * px + 1], (real)color[3 * px + 2]);
+        v3 Nf = normal ? mk((real)normal[3 * px], (real)normal[3 * px + 1], (real)normal[3 * px + 2]) : mk(0, 0, 0);
+        v3 Cacc = mk(0, 0, 0), Nacc = mk(0, 0, 0);
+        real log_t = 0;
+        int32_t prim = start_cells ? start_cells[px] : start_idx;
+        int steps = 0, seg = 0;
+        for (;;) {
+            real trans = r_exp(log_t);
+            if (trans < (real)thr || prim == NO_CELL || steps >= max_steps) break;
+            steps++;
+            trace_seg sg;
+            trace_step(o, d, spheres, nsigmas, sites, rgbs, heights, S, adj, adj_off, adj_diff, prim, &sg);
+            int32_t cur = prim;
+            prim = sg.next;
+            if (!sg.hit) continue;
+            real sigma = sg.sigma, dt = sg.dt;
+            real dlt = -sigma * dt;
+            real e = r_exp(dlt);
+            real alpha = K(1.0) - e;
+            v3 c = sg.pr.rgb;
+            Cacc = vadd(Cacc, smul(trans, smul(alpha, c)));
+            Nacc = vadd(Nacc, smul(alpha * trans, sg.pn));
+            real trans_next = trans * e;
+            real g_delta = dot(gC, vsub(vsub(Cf, Cacc), smul(trans_next, c))) +
+                           dot(gN, vsub(vsub(Nf, Nacc), smul(trans_next, sg.pn))) + gL;
+            if (m >= 0 && seg < m) g_delta += gD / sig_m;
+            real g_sigma = -dt * g_delta;
+            real g_tf = -sigma * g_delta, g_tn = sigma * g_delta;
+            if (seg == m) {
+                g_tn += gD;
+                g_sigma += -gD * r_log(trans / (real)depth_quantile) / (sigma * sigma);
+            }
+            v3 g_c = smul(alpha * trans, gC);
+            v3 g_pn = smul(alpha * trans, gN);
+            v3 g_po = mk(0, 0, 0);
+            real g_r = 0;
+            int n_adj = adj_off[cur + 1] - adj_off[cur];
+            /* the plane bounds at most one end */
+            real g_tsurf = 0;
+            if (sg.tn_id == n_adj) { g_tsurf += g_tn; g_tn = 0; }
+            if (sg.tf_id == n_adj) { g_tsurf += g_tf; g_tf = 0; }
+            real g_pre_tn = plane_local_bwd(o, d, sg.pre_tn, sg.center, sg.pn, sg.radius,
+                                            sites + (int64_t)cur * S * 3, rgbs + (int64_t)cur * S * 3,
+                                            heights + (int64_t)cur * S, S, &sg.pr, g_c, g_tsurf, &g_po, &g_pn, &g_r,
+                                            g_sites + (int64_t)cur * S * 3, g_rgb + (int64_t)cur * S * 3,
+                                            g_height + (int64_t)cur * S);
+            if (sg.tn_id != n_adj) g_tn += g_pre_tn;
+            else g_pre_tn = g_pre_tn; /* query depth is the pre-plane t_near */
+            real g_ends[2] = {sg.tn_id == n_adj ? g_pre_tn : g_tn, g_tf};
+            int ids[2] = {sg.tn_id == n_adj ? sg.pre_tn_id : sg.tn_id, sg.tf_id};
+            v3 g_center = g_po;
+            for (int i = 0; i < 2; i++) {
+                real gt = g_ends[i];
+                int id = ids[i];
+                if (gt == K(0.0)) continue;
+                if (id == -1) {
+                    v3 dc;
+                    real dr;
+                    sphere_root_grad(o, d, sg.center, sg.radius, i == 1, &dc, &dr);
+                    g_center = vadd(g_center, smul(gt, dc));
+                    g_r += gt * dr;
+                } else if (id >= 0 && id < n_adj) {
+                    int32_t nb = adj[adj_off[cur] + id];
+                    const float *ns = spheres + 4 * (int64_t)nb;
+                    v3 dci, dcj;
+                    real dri, drj;
+                    face_grad(o, d, sg.center, sg.radius, ld3(ns), (real)ns[3], &dci, &dri, &dcj, &drj);
+                    g_center = vadd(g_center, smul(gt, dci));
+                    g_r += gt * dri;
+                    add3(g_spheres + 4 * (int64_t)nb, smul(gt, dcj));
+                    ATOMIC_ADD(g_spheres[4 * (int64_t)nb + 3], gt * drj);
+                }
+            }
+            add3(g_spheres + 4 * (int64_t)cur, g_center);
+            ATOMIC_ADD(g_spheres[4 * (int64_t)cur + 3], g_r);
+            add3(g_nsigmas + 4 * (int64_t)cur, g_pn);
+            ATOMIC_ADD(g_nsigmas[4 * (int64_t)cur + 3], g_sigma);
+            log_t += dlt;
+            seg++;
+        }
+    }
+    return ORC_OK;
 }

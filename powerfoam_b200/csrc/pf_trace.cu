@@ -199,6 +199,284 @@ trace_fwd_kernel(TraceParams P, int64_t nthreads, float* __restrict__ color, flo
 }
 
 // ---------------------------------------------------------------------------
+// Adjoint of the walk (no counterpart in the reference, whose tracer is
+// forward-only).  Per ray the walk is repeated front to back; with the
+// forward's final colour C and normal N,
+//   dL/d delta_k = gC.(C - C_<=k - c_k T_k+1) + gN.(N - N_<=k - n_k T_k+1)
+//                  + gL + [k < m] gD / sigma_m          (delta = -sigma dt)
+// where m is the segment that produced the depth.  dL/dt_near and dL/dt_far
+// go to the one surface bounding each end (sphere, power face, texture
+// plane); face derivatives use the exact spheres; the texture plane's
+// derivative covers sites, colours, heights, plane origin and normal, the
+// query depth and the radius (through 1/r^2).
+
+struct TraceSeg {
+    bool hit;
+    float tn, tf, dt, pre_tn, sigma, radius;
+    int tn_id, tf_id, pre_tn_id;
+    int32_t next;
+    v3 center, pn;
+    PlaneRes pr;
+};
+
+PF_D void trace_step(const TraceParams& P, v3 o, v3 d, int32_t prim, TraceSeg& sg) {
+    const float4 s4 = __ldg(&P.spheres[prim]);
+    const v3 center = mk(s4.x, s4.y, s4.z);
+    const float radius = s4.w;
+    float tn, tf;
+    bool hit = ray_sphere(o, d, center, radius, tn, tf);
+    v3 v = center - o;
+    if (length(v) < 4.0f * radius) hit = false;
+    int tn_id = tn < 1e-8f ? -2 : -1, tf_id = tf < 1e-8f ? -2 : -1;
+    int32_t next = kNoCell;
+    float pt_far = 1e10f;
+    const int32_t a0 = __ldg(&P.adj_off[prim]), a1 = __ldg(&P.adj_off[prim + 1]);
+    for (int32_t e = a0; e < a1; e++) {
+        uint2 raw = __ldg(&P.adj_diff[e]);
+        v3 diff = mk(h2f((uint16_t)(raw.x & 0xffffu)), h2f((uint16_t)(raw.x >> 16)), h2f((uint16_t)(raw.y & 0xffffu)));
+        Face f = make_face_pm(o, diff, h2f((uint16_t)(raw.y >> 16)));
+        float dp = dot(d, f.n);
+        float t_face = f.num / dp;
+        if (dp >= 0.0f && t_face < pt_far) {
+            next = __ldg(&P.adj[e]);
+            pt_far = t_face;
+        }
+        if (dp >= 0.0f && t_face < tf) tf_id = e - a0;
+        tf = dp >= 0.0f ? fmin_t(t_face, tf) : tf;
+        if (dp < 0.0f && t_face > tn) tn_id = e - a0;
+        tn = dp < 0.0f ? fmax_t(t_face, tn) : tn;
+    }
+    const float* ns = (const float*)P.nsig + 4 * (int64_t)prim;
+    sg.pn = mk(__ldg(ns), __ldg(ns + 1), __ldg(ns + 2));
+    sg.sigma = __ldg(ns + 3);
+    sg.next = next;
+    sg.center = center;
+    sg.radius = radius;
+    sg.hit = false;
+    if (!hit || tn > tf || sg.sigma < 1e-3f) return;
+    sg.pre_tn = tn;
+    sg.pre_tn_id = tn_id;
+    int64_t b3 = (int64_t)prim * P.S * 3;
+    PlaneRes pr = plane_local<float>(o, d, tn, center, sg.pn, radius, (const float*)P.sites + b3,
+                                     (const float*)P.rgb + b3, (const float*)P.height + (int64_t)prim * P.S, P.S);
+    const int n_adj = a1 - a0;
+    if (pr.dp >= 0.0f && pr.t_surf < tf) tf_id = n_adj;
+    tf = pr.dp >= 0.0f ? fmin_t(pr.t_surf, tf) : tf;
+    if (pr.dp < 0.0f && pr.t_surf > tn) tn_id = n_adj;
+    tn = pr.dp < 0.0f ? fmax_t(pr.t_surf, tn) : tn;
+    sg.pr = pr;
+    sg.tn = tn;
+    sg.tf = tf;
+    sg.tn_id = tn_id;
+    sg.tf_id = tf_id;
+    sg.dt = tf - tn;
+    sg.hit = sg.dt > 0.0f;
+}
+
+struct TraceGrads {
+    float* points;
+    float* radii;
+    float* normals;
+    float* density;
+    float* sites;
+    float* rgb;
+    float* height;
+};
+
+PF_D void atomic_add3(float* g, v3 v) {
+    atomicAdd(g, v.x);
+    atomicAdd(g + 1, v.y);
+    atomicAdd(g + 2, v.z);
+}
+
+// derivative of the local texture plane; returns dL/d(pre-plane t_near)
+PF_D float plane_local_bwd(v3 o, v3 d, float tn, v3 po, v3 pn, float radius, const float* sites, const float* rgbs,
+                           const float* heights, int S, const PlaneRes& pr, v3 g_rgb, float g_tsurf, v3& g_po, v3& g_pn,
+                           float& g_radius, float* gs, float* gr, float* gh) {
+    const float inv_r2 = 1.0f / (radius * radius);
+    float g_inv_r2 = 0.f, g_tn = 0.f;
+    const float tq = pr.dp >= 0.0f ? tn : fmax_t(tn, pr.t_surf);
+    const v3 pt = o + tq * d;
+    const float V = pr.wsum, inv_V = 1.0f / pr.wsum;
+    const bool v_open = pr.wsum > 1e-20f;
+    v3 g_pt = mk(0.f, 0.f, 0.f);
+    for (int i = 0; i < S; i++) {
+        v3 s = mk(sites[3 * i], sites[3 * i + 1], sites[3 * i + 2]);
+        v3 df = pt - s;
+        float q2 = dot(df, df);
+        float vi = expf(-kTemp * q2 * inv_r2);
+        v3 ci = mk(rgbs[3 * i], rgbs[3 * i + 1], rgbs[3 * i + 2]);
+        atomic_add3(gr + 3 * i, (vi * inv_V) * g_rgb);
+        float g_vi = (v_open ? dot(ci - pr.rgb, g_rgb) : dot(ci, g_rgb)) * inv_V;
+        v3 dvdpt = (vi * (-2.0f * kTemp * inv_r2)) * df;
+        g_pt = g_pt + g_vi * dvdpt;
+        atomic_add3(gs + 3 * i, (-g_vi) * dvdpt);
+        g_inv_r2 += g_vi * vi * (-kTemp * q2);
+    }
+    (void)V;
+    float g_tq = dot(g_pt, d);
+    float g_ts = g_tsurf;
+    if (pr.dp >= 0.0f || tn > pr.t_surf) g_tn += g_tq;
+    else g_ts += g_tq;
+    float g_height = 0.f;
+    if (g_ts != 0.0f) {
+        float k = g_ts / pr.dp;
+        g_po = g_po + k * pn;
+        g_pn = g_pn + k * ((po - o) - pr.t_surf * d);
+        g_height = k;
+    }
+    if (g_height != 0.0f) {
+        const float _tq = pr._dp >= 0.0f ? tn : fmax_t(tn, pr._t_surf);
+        const v3 _pt = o + _tq * d;
+        const float inv_W = 1.0f / pr._wsum;
+        const bool w_open = pr._wsum > 1e-20f;
+        v3 g__pt = mk(0.f, 0.f, 0.f);
+        for (int i = 0; i < S; i++) {
+            v3 s = mk(sites[3 * i], sites[3 * i + 1], sites[3 * i + 2]);
+            v3 df = _pt - s;
+            float q2 = dot(df, df);
+            float wi = expf(-kTemp * q2 * inv_r2);
+            float hi = heights[i];
+            atomicAdd(gh + i, wi * inv_W * g_height);
+            float g_wi = (w_open ? (hi - pr.height) : hi) * inv_W * g_height;
+            v3 dwdpt = (wi * (-2.0f * kTemp * inv_r2)) * df;
+            g__pt = g__pt + g_wi * dwdpt;
+            atomic_add3(gs + 3 * i, (-g_wi) * dwdpt);
+            g_inv_r2 += g_wi * wi * (-kTemp * q2);
+        }
+        float g__tq = dot(g__pt, d);
+        if (g__tq != 0.0f) {
+            if (pr._dp >= 0.0f || tn > pr._t_surf) {
+                g_tn += g__tq;
+            } else {
+                float k = g__tq / pr._dp;
+                g_po = g_po + k * pn;
+                g_pn = g_pn + k * ((po - o) - pr._t_surf * d);
+            }
+        }
+    }
+    g_radius += g_inv_r2 * (-2.0f / (radius * radius * radius));
+    return g_tn;
+}
+
+__global__ void __launch_bounds__(128)
+trace_bwd_kernel(TraceParams P, int64_t nthreads, const float* __restrict__ color, const float* __restrict__ normal,
+                 const int32_t* __restrict__ depth_seg, const float* __restrict__ depth_sigma,
+                 const float* __restrict__ g_color, const float* __restrict__ g_log_t,
+                 const float* __restrict__ g_depth, const float* __restrict__ g_normal, TraceGrads G) {
+    int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (tid >= nthreads) return;
+    int pi, pj;
+    if (!trace_pixel(P.cam, tid, pi, pj)) return;
+    const int64_t px = (int64_t)pi * P.cam.W + pj;
+    const v3 o = P.cam.eye;
+    const v3 d = ray_dir(P.cam, pi, pj);
+    const v3 gC = g_color ? mk(g_color[3 * px], g_color[3 * px + 1], g_color[3 * px + 2]) : mk(0.f, 0.f, 0.f);
+    const v3 gN = g_normal ? mk(g_normal[3 * px], g_normal[3 * px + 1], g_normal[3 * px + 2]) : mk(0.f, 0.f, 0.f);
+    const float gL = g_log_t ? g_log_t[px] : 0.f;
+    const float gD = g_depth ? g_depth[px] : 0.f;
+    const int m = depth_seg ? depth_seg[px] : -1;
+    const float sig_m = depth_sigma ? depth_sigma[px] : 1.f;
+    const v3 Cf = mk(color[3 * px], color[3 * px + 1], color[3 * px + 2]);
+    const v3 Nf = normal ? mk(normal[3 * px], normal[3 * px + 1], normal[3 * px + 2]) : mk(0.f, 0.f, 0.f);
+    v3 Cacc = mk(0.f, 0.f, 0.f), Nacc = mk(0.f, 0.f, 0.f);
+    float log_t = 0.f;
+    int32_t prim = P.start_cells ? P.start_cells[px] : P.start_idx;
+    int steps = 0, seg = 0;
+    for (;;) {
+        float trans = expf(log_t);
+        if (trans < P.thr || prim == kNoCell || steps >= P.max_steps || prim < 0 || prim >= P.N) break;
+        steps++;
+        TraceSeg sg;
+        trace_step(P, o, d, prim, sg);
+        const int32_t cur = prim;
+        prim = sg.next;
+        if (!sg.hit) continue;
+        const float sigma = sg.sigma, dt = sg.dt;
+        const float dlt = -sigma * dt;
+        const float e = expf(dlt);
+        const float alpha = 1.0f - e;
+        const v3 c = sg.pr.rgb;
+        Cacc = Cacc + trans * (alpha * c);
+        Nacc = Nacc + (alpha * trans) * sg.pn;
+        const float trans_next = trans * e;
+        float g_delta = dot(gC, (Cf - Cacc) - trans_next * c) + dot(gN, (Nf - Nacc) - trans_next * sg.pn) + gL;
+        if (m >= 0 && seg < m) g_delta += gD / sig_m;
+        float g_sigma = -dt * g_delta;
+        float g_tf = -sigma * g_delta, g_tn = sigma * g_delta;
+        if (seg == m) {
+            g_tn += gD;
+            g_sigma += -gD * logf(trans / P.depth_q) / (sigma * sigma);
+        }
+        const v3 g_c = (alpha * trans) * gC;
+        v3 g_pn = (alpha * trans) * gN;
+        v3 g_po = mk(0.f, 0.f, 0.f);
+        float g_r = 0.f;
+        const int32_t a0 = __ldg(&P.adj_off[cur]);
+        const int n_adj = __ldg(&P.adj_off[cur + 1]) - a0;
+        float g_ts = 0.f;
+        if (sg.tn_id == n_adj) {
+            g_ts += g_tn;
+            g_tn = 0.f;
+        }
+        if (sg.tf_id == n_adj) {
+            g_ts += g_tf;
+            g_tf = 0.f;
+        }
+        const int64_t b3 = (int64_t)cur * P.S * 3;
+        float g_pre_tn = plane_local_bwd(o, d, sg.pre_tn, sg.center, sg.pn, sg.radius, (const float*)P.sites + b3,
+                                         (const float*)P.rgb + b3, (const float*)P.height + (int64_t)cur * P.S, P.S,
+                                         sg.pr, g_c, g_ts, g_po, g_pn, g_r, G.sites + b3, G.rgb + b3,
+                                         G.height + (int64_t)cur * P.S);
+        if (sg.tn_id != n_adj) g_tn += g_pre_tn;
+        const float g_ends[2] = {sg.tn_id == n_adj ? g_pre_tn : g_tn, g_tf};
+        const int ids[2] = {sg.tn_id == n_adj ? sg.pre_tn_id : sg.tn_id, sg.tf_id};
+        v3 g_center = g_po;
+        for (int i = 0; i < 2; i++) {
+            const float gt = g_ends[i];
+            const int id = ids[i];
+            if (gt == 0.0f) continue;
+            if (id == -1) {
+                // t = (-qb -+ s)/2, qb = 2 oc.d, s = sqrt(qb^2 - 4(|oc|^2 - r^2)), oc = o - c
+                v3 oc = o - sg.center;
+                float qb = 2.0f * dot(oc, d);
+                float qc = dot(oc, oc) - sg.radius * sg.radius;
+                float s = sqrtf(qb * qb - 4.0f * qc);
+                v3 ds = (1.0f / (2.0f * s)) * ((-4.0f * qb) * d + 8.0f * oc);
+                float sgn = i == 1 ? 1.0f : -1.0f;
+                g_center = g_center + gt * (d + (sgn * 0.5f) * ds);
+                g_r += gt * (sgn * 2.0f * sg.radius / s);
+            } else if (id >= 0 && id < n_adj) {
+                const int32_t nb = __ldg(&P.adj[a0 + id]);
+                const float4 sj = __ldg(&P.spheres[nb]);
+                const v3 cj = mk(sj.x, sj.y, sj.z), ci = sg.center;
+                v3 n = cj - ci;
+                float num = 0.5f * (dot(cj, cj) - sj.w * sj.w - dot(ci, ci) + sg.radius * sg.radius) - dot(o, n);
+                float inv_den = 1.0f / dot(d, n);
+                float t = num * inv_den;
+                g_center = g_center + (gt * inv_den) * ((o - ci) + t * d);
+                g_r += gt * sg.radius * inv_den;
+                atomic_add3(G.points + 3 * (int64_t)nb, (gt * inv_den) * ((cj - o) - t * d));
+                atomicAdd(G.radii + nb, -gt * sj.w * inv_den);
+            }
+        }
+        atomic_add3(G.points + 3 * (int64_t)cur, g_center);
+        atomicAdd(G.radii + cur, g_r);
+        atomic_add3(G.normals + 3 * (int64_t)cur, g_pn);
+        atomicAdd(G.density + cur, g_sigma);
+        log_t += dlt;
+        seg++;
+    }
+}
+
+__global__ void trace_zero_nonfinite_kernel(float* __restrict__ a, int64_t n) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        float v = a[i];
+        if (!isfinite(v)) a[i] = 0.0f;
+    }
+}
+
+// ---------------------------------------------------------------------------
 // start cell: argmin_i (|p_i - eye|)^2 - r_i^2, first index on ties.  The
 // float is mapped to an order-preserving uint32 and packed above the index,
 // so one 64-bit atomicMin per block finds the first minimum.
@@ -314,6 +592,86 @@ extern "C" int pf_trace_forward(const pf_trace_inputs* in, float* color, float* 
         trace_fwd_kernel<float><<<grid, 128, 0, st>>>(P, n, color, log_t, depth, normal, depth_seg, depth_sigma,
                                                       visit_log, visit_cap, visit_count, status);
     return pf_check_launch("pf_trace_forward");
+}
+
+static bool fill_trace(const pf_trace_inputs* in, TraceParams& P, const char** why) {
+    if (!in) {
+        *why = "null inputs";
+        return false;
+    }
+    if (in->cam.width < 2 || in->cam.height < 2) {
+        *why = "image must be at least 2x2";
+        return false;
+    }
+    if (in->n_sites < 0 || in->n_sites > kMaxSites) {
+        *why = "n_sites must be in [0, 8]";
+        return false;
+    }
+    if (in->max_steps <= 0) {
+        *why = "max_steps must be positive";
+        return false;
+    }
+    if (in->n_prims <= 0) {
+        *why = "no primitives";
+        return false;
+    }
+    if (!in->start_cells && (in->start_idx < 0 || in->start_idx >= in->n_prims) && in->start_idx != kNoCell) {
+        *why = "start_idx out of range";
+        return false;
+    }
+    P.cam = load_cam(in->cam);
+    P.S = in->n_sites;
+    P.N = in->n_prims;
+    P.spheres = (const float4*)in->spheres;
+    P.nsig = in->nsigmas;
+    P.sites = in->texel_sites;
+    P.rgb = in->texel_rgb;
+    P.height = in->texel_height;
+    P.adj = in->adjacency;
+    P.adj_off = in->adjacency_offsets;
+    P.adj_diff = (const uint2*)in->adjacency_diff;
+    P.start_idx = in->start_idx;
+    P.start_cells = in->start_cells;
+    P.thr = in->transmittance_threshold;
+    P.max_steps = in->max_steps;
+    P.depth_q = in->depth_quantile;
+    return true;
+}
+
+extern "C" int pf_trace_backward(const pf_trace_inputs* in, const float* color, const float* normal,
+                                 const int32_t* depth_seg, const float* depth_sigma, const float* grad_color,
+                                 const float* grad_log_t, const float* grad_depth, const float* grad_normal,
+                                 float* grad_points, float* grad_radii, float* grad_normals, float* grad_density,
+                                 float* grad_texel_sites, float* grad_texel_rgb, float* grad_texel_height,
+                                 void* stream) {
+    TraceParams P;
+    const char* why = "";
+    if (!fill_trace(in, P, &why)) return pf_fail(PF_ERR_ARGS, why);
+    if (in->attr_half) return pf_fail(PF_ERR_ARGS, "Backward pass only supports float precision");
+    if (!color || !grad_points || !grad_radii || !grad_normals || !grad_density || !grad_texel_sites ||
+        !grad_texel_rgb || !grad_texel_height || (grad_depth && (!depth_seg || !depth_sigma)) ||
+        (grad_normal && !normal))
+        return pf_fail(PF_ERR_ARGS, "pf_trace_backward: missing argument");
+    cudaStream_t st = (cudaStream_t)stream;
+    const size_t N = (size_t)P.N, S = (size_t)P.S;
+    float* outs[7] = {grad_points, grad_radii, grad_normals, grad_density, grad_texel_sites, grad_texel_rgb,
+                      grad_texel_height};
+    size_t lens[7] = {3 * N, N, 3 * N, N, 3 * N * S, 3 * N * S, N * S};
+    for (int i = 0; i < 7; i++)
+        if (lens[i]) cudaMemsetAsync(outs[i], 0, sizeof(float) * lens[i], st);
+    TraceGrads G{grad_points, grad_radii, grad_normals, grad_density, grad_texel_sites, grad_texel_rgb,
+                 grad_texel_height};
+    int64_t tiles = (int64_t)(1 + (in->cam.height - 1) / 8) * (1 + (in->cam.width - 1) / 8);
+    int64_t n = tiles * 64;
+    trace_bwd_kernel<<<(unsigned)((n + 127) / 128), 128, 0, st>>>(P, n, color, normal, depth_seg, depth_sigma,
+                                                                  grad_color, grad_log_t, grad_depth, grad_normal, G);
+    for (int i = 0; i < 7; i++)
+        if (lens[i]) {
+            int64_t k = (int64_t)lens[i];
+            trace_zero_nonfinite_kernel<<<(unsigned)std::min<int64_t>((k + 255) / 256, 148 * 16), 256, 0, st>>>(
+                outs[i], k);
+        }
+    return pf_check_launch("pf_trace_backward");
 }
 
 extern "C" int pf_start_cell_workspace_size(int64_t n_prims, size_t* bytes) {

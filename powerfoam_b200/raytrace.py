@@ -3,7 +3,9 @@
 ``RayTracer(args, device, attr_dtype).benchmark(...)`` keeps the reference's
 signature and returns the colour image (raytrace.py:247-309).  ``trace``
 exposes the extensions of the walk kernel: per-ray start cells, a step cap,
-depth / normal / log transmittance and the visited-cell log.
+depth / normal / log transmittance and the visited-cell log.  ``forward``
+is differentiable (``RayTraceGradFn``): its adjoint has no counterpart in the
+reference, whose tracer is forward-only.
 """
 
 from dataclasses import dataclass
@@ -26,6 +28,23 @@ class TraceResult:
     visit_count: torch.Tensor
     visits: torch.Tensor = None
     status: int = 0
+
+
+class RayTraceGradFn(torch.autograd.Function):
+    """(color, log_t, depth, normal) of the walk; gradients for points, radii,
+    density, normals, texel_sites, texel_rgb, texel_height."""
+
+    @staticmethod
+    def forward(ctx, tracer, camera, start, points, radii, density, normals, texel_sites, texel_rgb, texel_height,
+                adjacency, adjacency_offsets, adjacency_diff, transmittance_threshold=1e-3, max_steps=None,
+                depth_quantile=0.5):
+        return tracer._forward(ctx, camera, start, points, radii, density, normals, texel_sites, texel_rgb,
+                               texel_height, adjacency, adjacency_offsets, adjacency_diff, transmittance_threshold,
+                               max_steps, depth_quantile)
+
+    @staticmethod
+    def backward(ctx, g_color, g_log_t, g_depth, g_normal):
+        return ctx.tracer._backward(ctx, g_color, g_log_t, g_depth, g_normal)
 
 
 class RayTracer:
@@ -107,6 +126,55 @@ class RayTracer:
             if r.status != _lib.PF_OK:
                 raise _lib.PfError(r.status, "cell walk stopped early (step cap or invalid cell index)")
         return r
+
+    # ------------------------------------------------------------------
+    def forward(self, camera, start, points, radii, density, normals, texel_sites, texel_rgb, texel_height,
+                adjacency, adjacency_offsets, adjacency_diff, transmittance_threshold=1e-3, max_steps=None,
+                depth_quantile=0.5):
+        """Differentiable walk: returns (color, log_t, depth, normal)."""
+        return RayTraceGradFn.apply(self, camera, start, points, radii, density, normals, texel_sites, texel_rgb,
+                                    texel_height, adjacency, adjacency_offsets, adjacency_diff,
+                                    transmittance_threshold, max_steps, depth_quantile)
+
+    def _forward(self, ctx, camera, start, points, radii, density, normals, texel_sites, texel_rgb, texel_height,
+                 adjacency, adjacency_offsets, adjacency_diff, thr, max_steps, depth_quantile):
+        if self.attr_dtype != "float":
+            raise ValueError("Forward pass only supports float precision")
+        max_steps = DEFAULT_MAX_STEPS if max_steps is None else max_steps
+        r = self.trace(camera, start, points.detach(), radii.detach(), density.detach(), normals.detach(),
+                       texel_sites.detach(), texel_rgb.detach(), texel_height.detach(), adjacency, adjacency_offsets,
+                       adjacency_diff, thr, max_steps, depth_quantile)
+        ctx.tracer = self
+        ctx.camera = camera
+        ctx.start = start
+        ctx.cfg = (thr, max_steps, depth_quantile)
+        ctx.save_for_backward(points, radii, density, normals, texel_sites, texel_rgb, texel_height, adjacency,
+                              adjacency_offsets, adjacency_diff, r.color, r.normal, r.depth_seg, r.depth_sigma)
+        return r.color, r.log_t, r.depth, r.normal
+
+    def _backward(self, ctx, g_color, g_log_t, g_depth, g_normal):
+        (points, radii, density, normals, texel_sites, texel_rgb, texel_height, adjacency, adjacency_offsets,
+         adjacency_diff, color, normal, depth_seg, depth_sigma) = ctx.saved_tensors
+        thr, max_steps, depth_quantile = ctx.cfg
+        args = self._prep(points.detach(), radii.detach(), density.detach(), normals.detach(), texel_sites.detach(),
+                          texel_rgb.detach(), texel_height.detach(), adjacency, adjacency_offsets, adjacency_diff)
+        start = ctx.start
+        if isinstance(start, torch.Tensor) and start.numel() > 1:
+            start = start.to(torch.int32).contiguous()
+        inp = self._inputs(ctx.camera, start, *args, thr, max_steps, depth_quantile)
+        n = points.shape[0]
+        S = texel_sites.shape[1]
+        dev = self.device
+        out = [torch.empty(s, dtype=torch.float32, device=dev) for s in ((n, 3), (n,), (n, 3), (n,), (n, S, 3),
+                                                                         (n, S, 3), (n, S))]
+        c = lambda t: None if t is None else t.float().contiguous()
+        _lib.call("pf_trace_backward", _lib.ctypes.byref(inp), _lib.ptr(color), _lib.ptr(normal),
+                  _lib.ptr(depth_seg), _lib.ptr(depth_sigma), _lib.ptr(c(g_color)), _lib.ptr(c(g_log_t)),
+                  _lib.ptr(c(g_depth)), _lib.ptr(c(g_normal)), *[_lib.ptr(t) for t in out], _lib.stream_ptr())
+        del ctx.tracer, ctx.camera, ctx.start
+        g_pts, g_rad, g_nrm, g_den, g_sites, g_rgb, g_h = out
+        return (None, None, None, g_pts, g_rad, g_den, g_nrm, g_sites, g_rgb, g_h, None, None, None, None, None,
+                None)
 
     def benchmark(self, camera, start_point_idx, points, radii, density, normals, texel_sites, texel_rgb,
                   texel_height, adjacency, adjacency_offsets, adjacency_diff, transmittance_threshold=1e-3):
