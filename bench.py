@@ -56,6 +56,21 @@ def parse():
     return p.parse_args()
 
 
+def load_traffic(kernel, workload):
+    """DRAM bytes (read + write) per launch of `kernel` from the committed ncu
+    summary of the same workload, or None."""
+    path = os.path.join(ROOT, "profiles", f"ncu_raster_composite_{workload}.md")
+    try:
+        for line in open(path):
+            if line.startswith("traffic_bytes_per_launch:"):
+                _, name, val = line.split()
+                if name == kernel:
+                    return int(val)
+    except OSError:
+        pass
+    return None
+
+
 def load_peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -358,7 +373,8 @@ def main():
                 e2e=dict(value=world * 1000.0 / e2e_ms, unit=UNIT, h2d_bytes_per_step=target.numel() * 4,
                          d2h_bytes_per_step=4),
                 roofline=dict(bound="hbm", kernel=dominant, achieved=achieved, peak=peak, unit="GB/s",
-                              frac=achieved / peak, peak_source=peak_kind, traffic=None,
+                              frac=achieved / peak, peak_source=peak_kind,
+                              traffic=load_traffic(dominant, args.workload),
                               algorithmic_bytes=dom_bytes, ms=dom_ms, fwd_ms=fwd_ms, bwd_ms=bwd_ms),
                 gpu_launches=None)
     # kernels per step: pack 1, bin 31 (+3 per extra tile-sort pass), prefetch 1, SH 1, forward 1,
