@@ -240,6 +240,64 @@ PF_API int pf_start_cell(const float *points, const float *radii, int64_t n_prim
                   void *workspace, size_t workspace_bytes, int32_t *out_idx, void *stream);
 
 /* ---------------------------------------------------------------------- */
+/* Batched multi-view training step.  No counterpart in the reference, whose
+ * scene renders one view per Rasterizer.forward call (scene.py:314-353).  For
+ * every view: the forward of pf_raster_forward, the L2 loss
+ * sum((color - target)^2), dL/dcolor = 2 (color - target) and the adjoint of
+ * pf_raster_backward, with the gradients of all views summed into one set of
+ * primitive gradients (texel_rgb gradients per view, since the colours are
+ * per view).  One persistent launch takes (view, tile) work items from a
+ * device queue, `chunk` items per pop, in the order `order` selects; each
+ * tile's adjoint runs right after its own forward.  Views are binned
+ * beforehand with pf_bin at the batch's tile width (8, 16 or 32).  Nothing is
+ * allocated and nothing synchronises, so the call can be captured in a CUDA
+ * graph.  Images are bit-identical to pf_raster_forward per view; gradients
+ * equal the sum of the per-view pf_raster_backward results up to the order of
+ * the float additions. */
+#define PF_BATCH_MAX_VIEWS 64
+#define PF_BATCH_ORDER_LONGEST 0 /* all views' tiles by decreasing list length */
+#define PF_BATCH_ORDER_VIEW 1    /* view by view, tiles in index order */
+
+typedef struct pf_batch_scene {
+    int32_t n_sites;
+    int64_t n_prims;
+    const float *spheres;              /* (N,4) */
+    const float *nsigmas;              /* (N,4) */
+    const float *texel_sites;          /* (N,S,3) */
+    const float *texel_height;         /* (N,S) */
+    const int32_t *adjacency;          /* (E) */
+    const int32_t *adjacency_offsets;  /* (N+1) */
+    const uint16_t *adjacency_diff;    /* (E,4) pf_adjacency_prefetch encoding */
+    float transmittance_threshold;
+} pf_batch_scene;
+
+typedef struct pf_batch_view {
+    pf_camera cam;
+    const int64_t *tile_offsets;   /* (T+1) from pf_bin at the batch tile width */
+    const int32_t *tile_prims;
+    const float *texel_rgb;        /* (N,S,3) this view's texel colours */
+    const float *target;           /* (H,W,3) */
+    float *color;                  /* (H,W,3) */
+    float *log_t;                  /* (H,W) */
+    float *normal_distance;        /* (H,W) */
+    float *normal;                 /* (H,W,3) */
+    float *grad_color;             /* (H,W,3) written: 2 (color - target) */
+    float *contrib;                /* (N); views may share one array (summed) */
+    int32_t *early_stop;           /* (T) */
+    int32_t *tile_contrib_pairs;   /* (T) or NULL */
+    float *grad_texel_rgb;         /* (N,S,3); views may share one array (summed) */
+} pf_batch_view;
+
+/* tile_loss holds one float per tile of every view, the views' tiles
+ * concatenated in view order: the loss of view v is the sum of its slice. */
+PF_API int pf_batch_workspace_size(const pf_batch_view *views, int32_t n_views, int32_t tile_width, size_t *bytes);
+PF_API int pf_batch_render(const pf_batch_scene *scene, const pf_batch_view *views, int32_t n_views,
+                           int32_t tile_width, int32_t chunk, int32_t order, void *workspace, size_t workspace_bytes,
+                           float *tile_loss, float *grad_points, float *grad_radii, float *grad_normals,
+                           float *grad_density, float *grad_texel_sites, float *grad_texel_height,
+                           int32_t *status, void *stream);
+
+/* ---------------------------------------------------------------------- */
 /* Texel colour pre-step for the synthetic scenes: degree-3 real SH (16
  * coefficients per channel, constants of powerfoam/sh_utils.py:4-50) at
  * normalize(p - eye), + 0.5, clamped at 0, broadcast to the S sites.
@@ -247,6 +305,13 @@ PF_API int pf_start_cell(const float *points, const float *radii, int64_t n_prim
  * (scene.py:331-335 / benchmark.py:390-399). */
 PF_API int pf_sh_texel_rgb(const float *points, const float *sh /* (N,16,3) */, int64_t n_prims, int32_t n_sites,
                     const float *eye_host, float *texel_rgb, void *stream);
+/* Adjoint of pf_sh_texel_rgb with respect to the coefficients: ADDS
+ * basis(dir) * sum_s dL/dtexel_rgb[s] into grad_sh (N,16,3) wherever the
+ * pre-clamp colour is positive (no gradient reaches the points through the
+ * view direction).  Successive calls for several views accumulate. */
+PF_API int pf_sh_texel_rgb_backward(const float *points, const float *sh, int64_t n_prims, int32_t n_sites,
+                                    const float *eye_host, const float *grad_texel_rgb, float *grad_sh,
+                                    void *stream);
 
 #ifdef __cplusplus
 }

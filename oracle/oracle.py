@@ -237,6 +237,17 @@ def sh_texel_rgb(points, sh, eye, S=8):
     return out
 
 
+def sh_texel_rgb_backward(points, sh, eye, grad_texel_rgb, grad_sh=None):
+    """Adds the coefficient gradient of sh_texel_rgb into grad_sh (N,16,3)."""
+    points = _c(points, F32)
+    N = points.shape[0]
+    g = _c(grad_texel_rgb, F32)
+    out = np.zeros((N, 16, 3), F32) if grad_sh is None else grad_sh
+    lib().orc_sh_texel_rgb_backward_f32(_p(points), _p(_c(sh, F32)), ctypes.c_int64(N), ctypes.c_int(g.shape[1]),
+                                        _p(np.asarray(eye, F32)), _p(g), _p(out))
+    return out
+
+
 def num_threads():
     return int(lib().orc_num_threads_f32())
 

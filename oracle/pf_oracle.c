@@ -1348,33 +1348,58 @@ int32_t FN(orc_start_cell)(const float *points, const float *radii, int64_t N, c
 /* harmonics of degree 3 (16 coefficients per channel, the constants of      */
 /* powerfoam/sh_utils.py:4-50) evaluated at normalize(p - eye), plus 0.5,    */
 /* clamped at 0, broadcast to the S texel sites.  sh is (N,16,3).           */
-void FN(orc_sh_texel_rgb)(const float *points, const float *sh, int64_t N, int S, const float *eye,
-                          float *texel_rgb) {
+static void FN(sh_basis)(v3 dir, real b[16]) {
     const real C0 = K(0.28209479177387814), C1 = K(0.4886025119029199);
     const real C2[5] = {K(1.0925484305920792), K(-1.0925484305920792), K(0.31539156525252005),
                         K(-1.0925484305920792), K(0.5462742152960396)};
     const real C3[7] = {K(-0.5900435899266435), K(2.890611442640554), K(-0.4570457994644658),
                         K(0.3731763325901154), K(-0.4570457994644658), K(1.445305721320277),
                         K(-0.5900435899266435)};
+    real x = dir.x, y = dir.y, z = dir.z;
+    real xx = x * x, yy = y * y, zz = z * z;
+    b[0] = C0;
+    b[1] = -C1 * y; b[2] = C1 * z; b[3] = -C1 * x;
+    b[4] = C2[0] * (x * y); b[5] = C2[1] * (y * z); b[6] = C2[2] * (K(2.0) * zz - xx - yy);
+    b[7] = C2[3] * (x * z); b[8] = C2[4] * (xx - yy);
+    b[9] = C3[0] * y * (K(3.0) * xx - yy); b[10] = C3[1] * (x * y) * z;
+    b[11] = C3[2] * y * (K(4.0) * zz - xx - yy); b[12] = C3[3] * z * (K(2.0) * zz - K(3.0) * xx - K(3.0) * yy);
+    b[13] = C3[4] * x * (K(4.0) * zz - xx - yy); b[14] = C3[5] * z * (xx - yy);
+    b[15] = C3[6] * x * (xx - K(3.0) * yy);
+}
+
+static real FN(sh_raw)(const real b[16], const float *c, int ch) {
+    real acc = 0;
+    for (int k = 0; k < 16; k++) acc += b[k] * (real)c[k * 3 + ch];
+    return acc + K(0.5);
+}
+
+void FN(orc_sh_texel_rgb)(const float *points, const float *sh, int64_t N, int S, const float *eye,
+                          float *texel_rgb) {
     for (int64_t p = 0; p < N; p++) {
-        v3 dir = normalize(vsub(ld3(points + 3 * p), ld3(eye)));
-        real x = dir.x, y = dir.y, z = dir.z;
-        real xx = x * x, yy = y * y, zz = z * z;
         real b[16];
-        b[0] = C0;
-        b[1] = -C1 * y; b[2] = C1 * z; b[3] = -C1 * x;
-        b[4] = C2[0] * (x * y); b[5] = C2[1] * (y * z); b[6] = C2[2] * (K(2.0) * zz - xx - yy);
-        b[7] = C2[3] * (x * z); b[8] = C2[4] * (xx - yy);
-        b[9] = C3[0] * y * (K(3.0) * xx - yy); b[10] = C3[1] * (x * y) * z;
-        b[11] = C3[2] * y * (K(4.0) * zz - xx - yy); b[12] = C3[3] * z * (K(2.0) * zz - K(3.0) * xx - K(3.0) * yy);
-        b[13] = C3[4] * x * (K(4.0) * zz - xx - yy); b[14] = C3[5] * z * (xx - yy);
-        b[15] = C3[6] * x * (xx - K(3.0) * yy);
+        FN(sh_basis)(normalize(vsub(ld3(points + 3 * p), ld3(eye))), b);
         for (int c = 0; c < 3; c++) {
-            real acc = 0;
-            for (int k = 0; k < 16; k++) acc += b[k] * (real)sh[(p * 16 + k) * 3 + c];
-            acc = acc + K(0.5);
+            real acc = FN(sh_raw)(b, sh + p * 48, c);
             acc = acc > K(0.0) ? acc : K(0.0);
             for (int s = 0; s < S; s++) texel_rgb[(p * S + s) * 3 + c] = (float)acc;
+        }
+    }
+}
+
+/* Adjoint of orc_sh_texel_rgb with respect to the coefficients, ADDED into
+ * grad_sh (N,16,3): the colour is broadcast to the S sites (its gradient is
+ * the sum over sites) and the clamp passes it where the pre-clamp value is
+ * positive.  No gradient reaches the points through the view direction. */
+void FN(orc_sh_texel_rgb_backward)(const float *points, const float *sh, int64_t N, int S, const float *eye,
+                                   const float *grad_texel_rgb, float *grad_sh) {
+    for (int64_t p = 0; p < N; p++) {
+        real b[16];
+        FN(sh_basis)(normalize(vsub(ld3(points + 3 * p), ld3(eye))), b);
+        for (int c = 0; c < 3; c++) {
+            if (!(FN(sh_raw)(b, sh + p * 48, c) > K(0.0))) continue;
+            real g = 0;
+            for (int s = 0; s < S; s++) g += (real)grad_texel_rgb[(p * S + s) * 3 + c];
+            for (int k = 0; k < 16; k++) grad_sh[p * 48 + k * 3 + c] += (float)(b[k] * g);
         }
     }
 }

@@ -87,6 +87,44 @@ class PfTraceInputs(ctypes.Structure):
     ]
 
 
+class PfBatchScene(ctypes.Structure):
+    _fields_ = [
+        ("n_sites", c_i32),
+        ("n_prims", c_i64),
+        ("spheres", c_vp),
+        ("nsigmas", c_vp),
+        ("texel_sites", c_vp),
+        ("texel_height", c_vp),
+        ("adjacency", c_vp),
+        ("adjacency_offsets", c_vp),
+        ("adjacency_diff", c_vp),
+        ("transmittance_threshold", c_f),
+    ]
+
+
+class PfBatchView(ctypes.Structure):
+    _fields_ = [
+        ("cam", PfCamera),
+        ("tile_offsets", c_vp),
+        ("tile_prims", c_vp),
+        ("texel_rgb", c_vp),
+        ("target", c_vp),
+        ("color", c_vp),
+        ("log_t", c_vp),
+        ("normal_distance", c_vp),
+        ("normal", c_vp),
+        ("grad_color", c_vp),
+        ("contrib", c_vp),
+        ("early_stop", c_vp),
+        ("tile_contrib_pairs", c_vp),
+        ("grad_texel_rgb", c_vp),
+    ]
+
+
+PF_BATCH_MAX_VIEWS = 64
+PF_BATCH_ORDER_LONGEST = 0
+PF_BATCH_ORDER_VIEW = 1
+
 # name -> argtypes (all return int)
 _SIGS = {
     "pf_abi_version": [],
@@ -112,6 +150,10 @@ _SIGS = {
     "pf_start_cell_workspace_size": [c_i64, ctypes.POINTER(ctypes.c_size_t)],
     "pf_start_cell": [c_vp, c_vp, c_i64, ctypes.POINTER(c_f), c_vp, ctypes.c_size_t, c_vp, c_vp],
     "pf_sh_texel_rgb": [c_vp, c_vp, c_i64, c_i32, ctypes.POINTER(c_f), c_vp, c_vp],
+    "pf_sh_texel_rgb_backward": [c_vp, c_vp, c_i64, c_i32, ctypes.POINTER(c_f), c_vp, c_vp, c_vp],
+    "pf_batch_workspace_size": [ctypes.POINTER(PfBatchView), c_i32, c_i32, ctypes.POINTER(ctypes.c_size_t)],
+    "pf_batch_render": [ctypes.POINTER(PfBatchScene), ctypes.POINTER(PfBatchView), c_i32, c_i32, c_i32, c_i32, c_vp,
+                        ctypes.c_size_t, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp],
     "pf_cech_workspace_size": [c_i64, ctypes.POINTER(ctypes.c_size_t)],
     "pf_cech_adjacency": [c_vp, c_vp, c_i64, c_vp, ctypes.c_size_t, c_i64, c_vp, c_vp, c_vp, c_vp, c_vp],
     "pf_morton_workspace_size": [c_i64, ctypes.POINTER(ctypes.c_size_t)],

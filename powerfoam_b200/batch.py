@@ -1,0 +1,379 @@
+"""Batched multi-view training step: many views of uneven resolution, one
+persistent launch (pf_batch_render), captured with everything around it in
+one CUDA graph, with tile width and work-queue chunking picked by an
+autotuner.
+
+No counterpart in the reference, whose scene renders one view per
+Rasterizer.forward call (powerfoam/scene.py:314-353).  Per view the step is
+the reference's forward + L2 loss + adjoint; the gradients of all views are
+summed.
+
+``BatchStep`` owns every buffer the step touches (static addresses, as graph
+replay needs): packed primitives, the fp16 neighbour table, per-view tile
+lists, images, texel colours and gradients.  The caller updates the bound
+parameter tensors in place between steps.  Texel colours are either given per
+view (``texel_rgb``: a list of (N,S,3) tensors, gradients per view in
+``grad_texel_rgb``) or produced from SH coefficients (``sh``: (N,16,3)) by
+the SH pre-step inside the step, whose adjoint then fills ``grad_sh``.
+
+Sizing without host syncs: the first run bins every view eagerly and reads
+the pair counts once to size the per-view pair buffers (1.25x headroom,
+rounded to a power of two); later runs and graph replays never read them
+back.  ``check()`` reads the device status words (overflow, wait limit) when
+the caller chooses.
+"""
+
+import json
+import os
+import time
+
+import torch
+
+from . import _lib
+
+TILE_WIDTHS = (8, 16, 32)
+CHUNKS = (1, 2, 4, 8)
+ORDERS = {"longest": _lib.PF_BATCH_ORDER_LONGEST, "view": _lib.PF_BATCH_ORDER_VIEW}
+
+
+def _pow2_at_least(n):
+    return 1 << max(int(n) - 1, 1).bit_length()
+
+
+class BatchStep:
+    def __init__(self, device, cameras, tile_width=8, chunk=1, order="longest", transmittance_threshold=1e-3,
+                 headroom=1.25):
+        if not 1 <= len(cameras) <= _lib.PF_BATCH_MAX_VIEWS:
+            raise ValueError(f"1..{_lib.PF_BATCH_MAX_VIEWS} views per batch")
+        if tile_width not in TILE_WIDTHS:
+            raise ValueError("tile_width must be 8, 16 or 32")
+        if order not in ORDERS:
+            raise ValueError(f"order must be one of {sorted(ORDERS)}")
+        self.device = torch.device(device)
+        self.cameras = list(cameras)
+        self.tile_width = tile_width
+        self.chunk = int(chunk)
+        self.order = order
+        self.thr = float(transmittance_threshold)
+        self.headroom = headroom
+        self.graph = None
+        self.bound = False
+        _lib.load()
+        tw = tile_width
+        self.n_tiles = [(1 + (c.height - 1) // tw) * (1 + (c.width - 1) // tw) for c in self.cameras]
+        self.cams_pf = [c.to_pf() for c in self.cameras]
+        self.eyes = [(_lib.c_f * 3)(*[float(x) for x in c.eye.float().cpu().tolist()]) for c in self.cameras]
+
+    # ------------------------------------------------------------------
+    def bind(self, points, radii, density, normals, texel_sites, texel_height, adjacency, adjacency_offsets,
+             targets, texel_rgb=None, sh=None):
+        """Bind the step's inputs (kept by reference: update them in place)."""
+        if (texel_rgb is None) == (sh is None):
+            raise ValueError("give exactly one of texel_rgb (per view) or sh")
+        if len(targets) != len(self.cameras):
+            raise ValueError("one target image per view")
+        dev = self.device
+        f32 = lambda t, name: _check(t, name, torch.float32)
+        self.points = f32(points, "points")
+        self.radii = f32(radii, "radii")
+        self.density = f32(density, "density")
+        self.normals = f32(normals, "normals")
+        self.texel_sites = f32(texel_sites, "texel_sites")
+        self.texel_height = f32(texel_height, "texel_height")
+        self.adjacency = _check(adjacency, "adjacency", torch.int32)
+        self.adjacency_offsets = _check(adjacency_offsets, "adjacency_offsets", torch.int32)
+        self.targets = [f32(t, "target") for t in targets]
+        for t, c in zip(self.targets, self.cameras):
+            if tuple(t.shape) != (c.height, c.width, 3):
+                raise ValueError("target shape must be (H, W, 3) of its view")
+        n = self.points.shape[0]
+        S = self.texel_sites.shape[1]
+        self.n, self.S = n, S
+        V = len(self.cameras)
+        self.sh = None if sh is None else f32(sh, "sh")
+        if texel_rgb is not None:
+            if len(texel_rgb) != V:
+                raise ValueError("one texel_rgb tensor per view")
+            self.texel_rgb = [f32(t, "texel_rgb") for t in texel_rgb]
+        else:
+            self.texel_rgb = [torch.empty((n, S, 3), dtype=torch.float32, device=dev) for _ in range(V)]
+        self.grad_sh = torch.zeros((n, 16, 3), dtype=torch.float32, device=dev) if sh is not None else None
+        self.spheres = torch.empty((n, 4), dtype=torch.float32, device=dev)
+        self.nsigmas = torch.empty((n, 4), dtype=torch.float32, device=dev)
+        self.adj_diff = torch.empty((self.adjacency.shape[0], 4), dtype=torch.float16, device=dev)
+        e = lambda *s, dt=torch.float32: torch.empty(s, dtype=dt, device=dev)
+        self.color = [e(c.height, c.width, 3) for c in self.cameras]
+        self.log_t = [e(c.height, c.width) for c in self.cameras]
+        self.normal_distance = [e(c.height, c.width) for c in self.cameras]
+        self.normal = [e(c.height, c.width, 3) for c in self.cameras]
+        self.grad_color = [e(c.height, c.width, 3) for c in self.cameras]
+        self.contrib = e(n)  # summed over views
+        self.early_stop = [e(T, dt=torch.int32) for T in self.n_tiles]
+        self.tile_contrib_pairs = [e(T, dt=torch.int32) for T in self.n_tiles]
+        self.grad_texel_rgb = [e(n, S, 3) for _ in range(V)]
+        self.grads = {k: torch.empty_like(t) for k, t in (("points", self.points), ("radii", self.radii),
+                                                           ("normals", self.normals), ("density", self.density),
+                                                           ("texel_sites", self.texel_sites),
+                                                           ("texel_height", self.texel_height))}
+        self.tile_loss = e(sum(self.n_tiles))
+        self.loss = e(V)
+        self.status = torch.zeros(1, dtype=torch.int32, device=dev)
+        self.bin_scalars = torch.zeros((V, 2), dtype=torch.int64, device=dev)  # n_pairs, status
+        self.tile_offsets = [e(T + 1, dt=torch.int64) for T in self.n_tiles]
+        self.tile_prims = [None] * V
+        self.capacity = [0] * V
+        self._size_bins()
+        self._build_structs()
+        self.bound = True
+        self.graph = None
+
+    # ------------------------------------------------------------------
+    def _bin_ws(self, cap):
+        nbytes = _lib.ctypes.c_size_t(0)
+        _lib.call("pf_bin_workspace_size", self.n, cap, max(self.n_tiles), _lib.ctypes.byref(nbytes))
+        return nbytes.value
+
+    def _size_bins(self):
+        """Eager binning of every view to size the pair buffers (one host read)."""
+        self._pack()
+        caps = [max(4 * self.n, 1 << 14)] * len(self.cameras)
+        while True:
+            self.bin_ws = torch.empty(max(self._bin_ws(max(caps)), 256), dtype=torch.uint8, device=self.device)
+            self.tile_prims = [torch.empty(max(c, 1), dtype=torch.int32, device=self.device) for c in caps]
+            self.capacity = caps
+            self._bin_all()
+            counts = self.bin_scalars[:, 0].tolist()
+            if all(n <= c for n, c in zip(counts, caps)):
+                break
+            caps = [max(c, _pow2_at_least(n * self.headroom)) for n, c in zip(counts, caps)]
+        self.bin_scalars.zero_()  # statuses are sticky: clear the sizing runs' overflows
+        caps = [_pow2_at_least(max(n, 1) * self.headroom) for n in counts]
+        if caps != self.capacity:
+            self.bin_ws = torch.empty(max(self._bin_ws(max(caps)), 256), dtype=torch.uint8, device=self.device)
+            self.tile_prims = [torch.empty(max(c, 1), dtype=torch.int32, device=self.device) for c in caps]
+            self.capacity = caps
+        ws = _lib.ctypes.c_size_t(0)
+        self._views = (_lib.PfBatchView * len(self.cameras))()
+        self._fill_views()
+        _lib.call("pf_batch_workspace_size", self._views, len(self.cameras), self.tile_width, _lib.ctypes.byref(ws))
+        self.batch_ws = torch.empty(max(ws.value, 256), dtype=torch.uint8, device=self.device)
+
+    def _fill_views(self):
+        for v, c in enumerate(self.cameras):
+            w = self._views[v]
+            w.cam = self.cams_pf[v]
+            w.tile_offsets = _lib.ptr(self.tile_offsets[v])
+            w.tile_prims = _lib.ptr(self.tile_prims[v])
+            w.texel_rgb = _lib.ptr(self.texel_rgb[v])
+            w.target = _lib.ptr(self.targets[v])
+            w.color = _lib.ptr(self.color[v])
+            w.log_t = _lib.ptr(self.log_t[v])
+            w.normal_distance = _lib.ptr(self.normal_distance[v])
+            w.normal = _lib.ptr(self.normal[v])
+            w.grad_color = _lib.ptr(self.grad_color[v])
+            w.contrib = _lib.ptr(self.contrib)
+            w.early_stop = _lib.ptr(self.early_stop[v])
+            w.tile_contrib_pairs = _lib.ptr(self.tile_contrib_pairs[v])
+            w.grad_texel_rgb = _lib.ptr(self.grad_texel_rgb[v])
+
+    def _build_structs(self):
+        self._fill_views()
+        sc = _lib.PfBatchScene()
+        sc.n_sites = self.S
+        sc.n_prims = self.n
+        sc.spheres = _lib.ptr(self.spheres)
+        sc.nsigmas = _lib.ptr(self.nsigmas)
+        sc.texel_sites = _lib.ptr(self.texel_sites)
+        sc.texel_height = _lib.ptr(self.texel_height)
+        sc.adjacency = _lib.ptr(self.adjacency)
+        sc.adjacency_offsets = _lib.ptr(self.adjacency_offsets)
+        sc.adjacency_diff = _lib.ptr(self.adj_diff)
+        sc.transmittance_threshold = self.thr
+        self._scene = sc
+
+    # ------------------------------------------------------------------
+    def _pack(self):
+        st = _lib.stream_ptr()
+        _lib.call("pf_pack_prims", _lib.ptr(self.points), _lib.ptr(self.radii), _lib.ptr(self.normals),
+                  _lib.ptr(self.density), self.n, _lib.ptr(self.spheres), _lib.ptr(self.nsigmas), st)
+
+    def _bin_all(self):
+        st = _lib.stream_ptr()
+        for v in range(len(self.cameras)):
+            sc = self.bin_scalars[v]
+            _lib.call("pf_bin", _lib.ctypes.byref(self.cams_pf[v]), self.tile_width, _lib.ptr(self.spheres), self.n,
+                      _lib.ptr(self.bin_ws), self.bin_ws.numel(), self.capacity[v], _lib.ptr(self.tile_offsets[v]),
+                      _lib.ptr(self.tile_prims[v]), None, None, None, _lib.ptr(sc[:1]),
+                      _lib.ptr(sc[1:].view(torch.int32)[:1]), st)
+
+    def _launch(self):
+        """The whole step, on the current stream, without host syncs."""
+        st = _lib.stream_ptr()
+        self._pack()
+        _lib.call("pf_adjacency_prefetch", _lib.ptr(self.spheres), _lib.ptr(self.adjacency),
+                  _lib.ptr(self.adjacency_offsets), self.n, _lib.ptr(self.adj_diff), st)
+        if self.sh is not None:
+            for v in range(len(self.cameras)):
+                _lib.call("pf_sh_texel_rgb", _lib.ptr(self.points), _lib.ptr(self.sh), self.n, self.S, self.eyes[v],
+                          _lib.ptr(self.texel_rgb[v]), st)
+        self._bin_all()
+        g = self.grads
+        _lib.call("pf_batch_render", _lib.ctypes.byref(self._scene), self._views, len(self.cameras), self.tile_width,
+                  self.chunk, ORDERS[self.order], _lib.ptr(self.batch_ws), self.batch_ws.numel(),
+                  _lib.ptr(self.tile_loss), _lib.ptr(g["points"]), _lib.ptr(g["radii"]), _lib.ptr(g["normals"]),
+                  _lib.ptr(g["density"]), _lib.ptr(g["texel_sites"]), _lib.ptr(g["texel_height"]),
+                  _lib.ptr(self.status), st)
+        if self.sh is not None:
+            self.grad_sh.zero_()
+            for v in range(len(self.cameras)):
+                _lib.call("pf_sh_texel_rgb_backward", _lib.ptr(self.points), _lib.ptr(self.sh), self.n, self.S,
+                          self.eyes[v], _lib.ptr(self.grad_texel_rgb[v]), _lib.ptr(self.grad_sh), st)
+        torch.stack([s.sum() for s in self.tile_loss.split(self.n_tiles)], out=self.loss)
+
+    def run(self):
+        """One step; returns the (V,) per-view loss tensor (device)."""
+        if not self.bound:
+            raise RuntimeError("bind() the inputs first")
+        if self.graph is not None:
+            self.graph.replay()
+        else:
+            self._launch()
+        return self.loss
+
+    def capture(self):
+        """Record the step into a CUDA graph; run() then replays it."""
+        if not self.bound:
+            raise RuntimeError("bind() the inputs first")
+        s = torch.cuda.Stream(device=self.device)
+        s.wait_stream(torch.cuda.current_stream(self.device))
+        with torch.cuda.stream(s):
+            self._launch()  # warm-up outside the graph (kernel attributes, allocator)
+        torch.cuda.current_stream(self.device).wait_stream(s)
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g):
+            self._launch()
+        self.graph = g
+        return g
+
+    def set_schedule(self, chunk=None, order=None):
+        """Change the work-queue chunk / order (drops a captured graph)."""
+        if chunk is not None:
+            self.chunk = int(chunk)
+        if order is not None:
+            if order not in ORDERS:
+                raise ValueError(f"order must be one of {sorted(ORDERS)}")
+            self.order = order
+        self.graph = None
+
+    def check(self):
+        """Raise if any device status word reports a problem (host sync)."""
+        bs = self.bin_scalars.cpu()
+        for v in range(len(self.cameras)):
+            n, st = int(bs[v, 0]), int(bs[v, 1]) & 0xffffffff  # the status is the slot's low int32 word
+            if st != _lib.PF_OK:
+                raise _lib.PfError(st, f"view {v}: {n} pairs exceed the capacity {self.capacity[v]}")
+        s = int(self.status.item())
+        if s != _lib.PF_OK:
+            raise _lib.PfError(s, "batch compositing reported an error")
+
+    def pair_counts(self):
+        return self.bin_scalars[:, 0].tolist()
+
+
+def _check(t, name, dtype):
+    if not t.is_cuda:
+        raise ValueError(f"{name}: only CUDA tensors are supported")
+    if t.dtype != dtype:
+        raise ValueError(f"{name} must be {dtype}, got {t.dtype}")
+    if not t.is_contiguous():
+        raise ValueError(f"{name} must be contiguous (bound tensors are used in place)")
+    return t
+
+
+# ----------------------------------------------------------------------------
+# autotuner
+def default_cache_path():
+    return os.environ.get("PF_AUTOTUNE_CACHE",
+                          os.path.join(os.path.expanduser("~"), ".cache", "powerfoam_b200", "autotune.json"))
+
+
+def tune_key(device, cameras, n_prims, n_sites):
+    """Cache key: GPU name, primitive count, sites and the views' resolutions."""
+    name = torch.cuda.get_device_name(device).replace(" ", "_")
+    res = sorted(f"{c.width}x{c.height}" for c in cameras)
+    counts = {}
+    for r in res:
+        counts[r] = counts.get(r, 0) + 1
+    views = ",".join(f"{k}*{v}" for k, v in sorted(counts.items()))
+    return f"{name}|N={n_prims}|S={n_sites}|views={views}"
+
+
+def time_step(step, iters=3, warmup=1):
+    """Mean device milliseconds of step.run() (CUDA events on the current stream)."""
+    for _ in range(warmup):
+        step.run()
+    st = torch.cuda.current_stream(step.device)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize(step.device)
+    a.record(st)
+    for _ in range(iters):
+        step.run()
+    b.record(st)
+    torch.cuda.synchronize(step.device)
+    return a.elapsed_time(b) / iters
+
+
+def autotune(device, cameras, bind_kwargs, tile_widths=TILE_WIDTHS, chunks=CHUNKS, orders=("longest", "view"),
+             iters=3, warmup=1, cache_path=None, use_cache=True, transmittance_threshold=1e-3, log=None):
+    """Sweep tile width x work-queue chunk x item order over the real step and
+    return (best BatchStep bound and ready, table).  Each candidate is timed
+    with CUDA events over `iters` eager runs after `warmup`.  The winner is
+    cached in a JSON file keyed by tune_key(); a cached entry skips the sweep."""
+    cache_path = cache_path or default_cache_path()
+    n = bind_kwargs["points"].shape[0]
+    S = bind_kwargs["texel_sites"].shape[1]
+    key = tune_key(device, cameras, n, S)
+    cache = {}
+    if os.path.exists(cache_path):
+        try:
+            with open(cache_path) as f:
+                cache = json.load(f)
+        except (OSError, ValueError):
+            cache = {}
+    if use_cache and key in cache:
+        best = cache[key]
+        step = BatchStep(device, cameras, best["tile_width"], best["chunk"], best["order"], transmittance_threshold)
+        step.bind(**bind_kwargs)
+        return step, best.get("table", [])
+    table = []
+    best = None
+    for tw in tile_widths:
+        step = BatchStep(device, cameras, tw, 1, "longest", transmittance_threshold)
+        step.bind(**bind_kwargs)
+        for order in orders:
+            for ch in chunks:
+                step.set_schedule(chunk=ch, order=order)
+                t0 = time.perf_counter()
+                ms = time_step(step, iters=iters, warmup=warmup)
+                row = {"tile_width": tw, "chunk": ch, "order": order, "ms": ms}
+                table.append(row)
+                if log:
+                    log(f"autotune tile={tw} chunk={ch} order={order}: {ms:.3f} ms "
+                        f"({time.perf_counter() - t0:.1f} s)")
+                if best is None or ms < best["ms"]:
+                    best = dict(row)
+        del step
+        torch.cuda.empty_cache()
+    best["table"] = table
+    cache[key] = best
+    try:
+        os.makedirs(os.path.dirname(cache_path), exist_ok=True)
+        tmp = cache_path + ".tmp"
+        with open(tmp, "w") as f:
+            json.dump(cache, f, indent=1, sort_keys=True)
+        os.replace(tmp, cache_path)
+    except OSError:
+        pass
+    step = BatchStep(device, cameras, best["tile_width"], best["chunk"], best["order"], transmittance_threshold)
+    step.bind(**bind_kwargs)
+    return step, table

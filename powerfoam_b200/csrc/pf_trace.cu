@@ -509,19 +509,14 @@ __global__ void start_cell_finish_kernel(const unsigned long long* __restrict__ 
 
 // ---------------------------------------------------------------------------
 // degree-3 real SH colour pre-step (constants of powerfoam/sh_utils.py:4-50)
-__global__ void sh_texel_rgb_kernel(const float* __restrict__ pts, const float* __restrict__ sh, int64_t N, int S,
-                                    v3 eye, float* __restrict__ out) {
-    int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= N) return;
+PF_D void sh_basis(v3 dir, float b[16]) {
     const float C0 = 0.28209479177387814f, C1 = 0.4886025119029199f;
     const float C2[5] = {1.0925484305920792f, -1.0925484305920792f, 0.31539156525252005f, -1.0925484305920792f,
                          0.5462742152960396f};
     const float C3[7] = {-0.5900435899266435f, 2.890611442640554f, -0.4570457994644658f, 0.3731763325901154f,
                          -0.4570457994644658f, 1.445305721320277f, -0.5900435899266435f};
-    v3 dir = normalize(mk(pts[3 * p], pts[3 * p + 1], pts[3 * p + 2]) - eye);
     float x = dir.x, y = dir.y, z = dir.z;
     float xx = x * x, yy = y * y, zz = z * z;
-    float b[16];
     b[0] = C0;
     b[1] = -C1 * y;
     b[2] = C1 * z;
@@ -538,14 +533,46 @@ __global__ void sh_texel_rgb_kernel(const float* __restrict__ pts, const float* 
     b[13] = C3[4] * x * (4.0f * zz - xx - yy);
     b[14] = C3[5] * z * (xx - yy);
     b[15] = C3[6] * x * (xx - 3.0f * yy);
+}
+
+// pre-clamp colour of one channel: sum_k b_k sh[k][ch] + 0.5
+PF_D float sh_raw(const float b[16], const float* c, int ch) {
+    float acc = 0.f;
+#pragma unroll
+    for (int k = 0; k < 16; k++) acc += b[k] * c[k * 3 + ch];
+    return acc + 0.5f;
+}
+
+__global__ void sh_texel_rgb_kernel(const float* __restrict__ pts, const float* __restrict__ sh, int64_t N, int S,
+                                    v3 eye, float* __restrict__ out) {
+    int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= N) return;
+    float b[16];
+    sh_basis(normalize(mk(pts[3 * p], pts[3 * p + 1], pts[3 * p + 2]) - eye), b);
     const float* c = sh + p * 48;
     for (int ch = 0; ch < 3; ch++) {
-        float acc = 0.f;
-#pragma unroll
-        for (int k = 0; k < 16; k++) acc += b[k] * c[k * 3 + ch];
-        acc = acc + 0.5f;
+        float acc = sh_raw(b, c, ch);
         acc = acc > 0.0f ? acc : 0.0f;
         for (int s = 0; s < S; s++) out[(p * S + s) * 3 + ch] = acc;
+    }
+}
+
+// adjoint with respect to the coefficients: the colour is broadcast to the S
+// sites, so its gradient is the sum over sites; the clamp passes it where the
+// pre-clamp value is positive.  Accumulates into grad_sh.
+__global__ void sh_texel_rgb_bwd_kernel(const float* __restrict__ pts, const float* __restrict__ sh, int64_t N,
+                                        int S, v3 eye, const float* __restrict__ g_rgb, float* __restrict__ g_sh) {
+    int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= N) return;
+    float b[16];
+    sh_basis(normalize(mk(pts[3 * p], pts[3 * p + 1], pts[3 * p + 2]) - eye), b);
+    const float* c = sh + p * 48;
+    for (int ch = 0; ch < 3; ch++) {
+        if (!(sh_raw(b, c, ch) > 0.0f)) continue;
+        float g = 0.f;
+        for (int s = 0; s < S; s++) g += g_rgb[(p * S + s) * 3 + ch];
+#pragma unroll
+        for (int k = 0; k < 16; k++) g_sh[p * 48 + k * 3 + ch] += b[k] * g;
     }
 }
 
@@ -701,4 +728,15 @@ extern "C" int pf_sh_texel_rgb(const float* points, const float* sh, int64_t n_p
     sh_texel_rgb_kernel<<<(unsigned)((n_prims + 255) / 256), 256, 0, (cudaStream_t)stream>>>(
         points, sh, n_prims, n_sites, mk(eye_host[0], eye_host[1], eye_host[2]), texel_rgb);
     return pf_check_launch("pf_sh_texel_rgb");
+}
+
+extern "C" int pf_sh_texel_rgb_backward(const float* points, const float* sh, int64_t n_prims, int32_t n_sites,
+                                        const float* eye_host, const float* grad_texel_rgb, float* grad_sh,
+                                        void* stream) {
+    if (n_prims < 0 || n_sites < 0 || !eye_host || (n_prims > 0 && (!points || !sh || !grad_texel_rgb || !grad_sh)))
+        return pf_fail(PF_ERR_ARGS, "pf_sh_texel_rgb_backward: bad arguments");
+    if (n_prims == 0) return PF_OK;
+    sh_texel_rgb_bwd_kernel<<<(unsigned)((n_prims + 255) / 256), 256, 0, (cudaStream_t)stream>>>(
+        points, sh, n_prims, n_sites, mk(eye_host[0], eye_host[1], eye_host[2]), grad_texel_rgb, grad_sh);
+    return pf_check_launch("pf_sh_texel_rgb_backward");
 }

@@ -1,0 +1,206 @@
+"""Batched multi-view step (pf_batch_render through powerfoam_b200.batch):
+per view bit-identical to the single-view rasterizer, gradients equal to the
+sum over views, images and gradients against the CPU oracle, CUDA-graph
+replay, the SH pre-step adjoint and the autotuner's cache.
+
+Tolerances: images, early-stop indices and dL/dcolor bit-exact against the
+single-view kernels (same tile code); images max-abs 1e-5 against the oracle;
+gradients normwise relative 1e-4 against the oracle and 1e-5 against the sum
+of single-view gradients (only the order of the float additions differs)."""
+
+import json
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import oracle as orc
+from powerfoam_b200 import _lib
+from powerfoam_b200.batch import BatchStep, autotune, tune_key
+from powerfoam_b200.rasterize import Rasterizer
+from tests.helpers import assert_close_rel, cech_np, max_abs, np_camera, np_scene, orc_cam, packed, to_t, torch_cam
+
+pytestmark = pytest.mark.gpu
+
+
+class Args:
+    is_pinhole = True
+    render_objective = "volume"
+    num_texel_sites = 8
+
+
+# uneven resolutions, ragged tiles at every width
+VIEW_SPECS = [((0.2, 0.5, 2.3), 61, 37, 55.0), ((-1.6, 0.3, 1.5), 40, 30, 60.0), ((1.2, -0.8, 1.9), 96, 54, 50.0)]
+
+
+def make_case(seed=3, n=500, views=VIEW_SPECS):
+    sc = np_scene(seed, n, -0.6, 0.6, 0.03, 0.15)
+    adj, adj_off = cech_np(sc["points"], sc["radii"])
+    cams = [np_camera(eye, (0, 0, 0), W, H, fov) for eye, W, H, fov in views]
+    rng = np.random.default_rng(seed + 100)
+    rgbs = [rng.uniform(0, 1, sc["texel_rgb"].shape).astype(np.float32) for _ in cams]
+    targets = [rng.uniform(0, 1, (c["height"], c["width"], 3)).astype(np.float32) for c in cams]
+    return sc, adj, adj_off, cams, rgbs, targets
+
+
+def bind_kwargs(sc, adj, adj_off, rgbs, targets):
+    return dict(points=to_t(sc["points"]), radii=to_t(sc["radii"]), density=to_t(sc["density"]),
+                normals=to_t(sc["normals"]), texel_sites=to_t(sc["texel_sites"]),
+                texel_height=to_t(sc["texel_height"]), adjacency=to_t(adj), adjacency_offsets=to_t(adj_off),
+                targets=[to_t(t) for t in targets], texel_rgb=[to_t(r) for r in rgbs])
+
+
+def single_view(sc, adj, adj_off, cam, rgb, target, tw):
+    R = Rasterizer(Args(), "cuda", tile_width=tw)
+    t = {k: to_t(sc[k]).requires_grad_(True) for k in ["points", "radii", "density", "normals", "texel_sites",
+                                                         "texel_height"]}
+    rgb_t = to_t(rgb).requires_grad_(True)
+    out = R.forward(torch_cam(cam), None, t["points"], t["radii"], t["density"], t["normals"], t["texel_sites"],
+                    rgb_t, t["texel_height"], to_t(adj), to_t(adj_off), None, False)
+    loss = ((out[0] - to_t(target)) ** 2).sum()
+    loss.backward()
+    return out, loss, {k: v.grad for k, v in t.items()}, rgb_t.grad, R
+
+
+@pytest.mark.parametrize("tw,chunk,order", [(8, 1, "longest"), (8, 3, "view"), (16, 2, "longest"),
+                                            (32, 1, "longest"), (32, 5, "view")])
+def test_batch_matches_single_view_kernels(tw, chunk, order):
+    sc, adj, adj_off, cams, rgbs, targets = make_case()
+    step = BatchStep("cuda", [torch_cam(c) for c in cams], tile_width=tw, chunk=chunk, order=order)
+    step.bind(**bind_kwargs(sc, adj, adj_off, rgbs, targets))
+    loss = step.run().clone()
+    step.check()
+    gsum = None
+    for v, cam in enumerate(cams):
+        out, l1, grads, g_rgb, R = single_view(sc, adj, adj_off, cam, rgbs[v], targets[v], tw)
+        color, opacity, nd, normal = out[0], out[1], out[2], out[3]
+        assert torch.equal(step.color[v], color.detach())
+        assert torch.equal(step.log_t[v].exp().neg().add(1), opacity.detach())
+        assert torch.equal(step.normal_distance[v], nd.detach())
+        assert torch.equal(step.normal[v], normal.detach())
+        assert torch.equal(step.grad_color[v], 2 * (color.detach() - to_t(targets[v])))
+        assert abs(float(loss[v]) - float(l1.detach())) <= 1e-5 * float(l1.detach())
+        assert_close_rel(step.grad_texel_rgb[v].cpu().numpy(), g_rgb.cpu().numpy(), 1e-5, f"rgb view {v}")
+        gsum = grads if gsum is None else {k: gsum[k] + grads[k] for k in gsum}
+    for k in gsum:
+        assert_close_rel(step.grads[k].cpu().numpy(), gsum[k].cpu().numpy(), 1e-5, k)
+
+
+@pytest.mark.parametrize("tw", [8, 32])
+def test_batch_matches_oracle(tw):
+    sc, adj, adj_off, cams, rgbs, targets = make_case(seed=7)
+    step = BatchStep("cuda", [torch_cam(c) for c in cams], tile_width=tw, chunk=2)
+    step.bind(**bind_kwargs(sc, adj, adj_off, rgbs, targets))
+    step.run()
+    step.check()
+    N, S = sc["points"].shape[0], sc["texel_sites"].shape[1]
+    acc = dict(spheres=np.zeros((N, 4)), nsigmas=np.zeros((N, 4)), texel_sites=np.zeros((N, S, 3)),
+               texel_height=np.zeros((N, S)))
+    for v, cam in enumerate(cams):
+        scv = dict(sc, texel_rgb=rgbs[v])
+        sph, nsig, rgbh = packed(scv)
+        oc = orc_cam(cam)
+        keys, prims, offs, _ = orc.bin(oc, sph, tw)
+        ad = orc.prefetch_adjacency(sph, adj, adj_off)
+        o = orc.raster_forward(oc, tw, sph, nsig, sc["texel_sites"], rgbh, adj, adj_off, ad, offs, prims, None, None,
+                               1e-3, False)
+        assert max_abs(step.color[v].cpu(), o["color"]) <= 1e-5
+        assert max_abs(step.log_t[v].cpu(), o["log_t"]) <= 1e-5
+        assert np.array_equal(step.early_stop[v].cpu().numpy(), o["early_stop"])
+        H, W = cam["height"], cam["width"]
+        g_c = (2 * (o["color"] - targets[v])).astype(np.float32)
+        z = np.zeros((H, W), np.float32)
+        gr = orc.raster_backward(oc, tw, sph, nsig, sc["texel_sites"], rgbh, adj, adj_off, ad, offs, prims,
+                                 o["early_stop"], o["log_t"], g_c, z, z, np.zeros((H, W, 3), np.float32),
+                                 np.zeros(N, np.float32))
+        for k in acc:
+            acc[k] += gr[k]
+        assert_close_rel(step.grad_texel_rgb[v].cpu().numpy(), gr["texel_rgb"], 1e-4, f"rgb view {v}")
+    g = step.grads
+    assert_close_rel(g["points"].cpu().numpy(), acc["spheres"][:, :3], 1e-4, "points")
+    assert_close_rel(g["radii"].cpu().numpy(), acc["spheres"][:, 3], 1e-4, "radii")
+    assert_close_rel(g["normals"].cpu().numpy(), acc["nsigmas"][:, :3], 1e-4, "normals")
+    assert_close_rel(g["density"].cpu().numpy(), acc["nsigmas"][:, 3], 1e-4, "density")
+    assert_close_rel(g["texel_sites"].cpu().numpy(), acc["texel_sites"], 1e-4, "sites")
+    assert_close_rel(g["texel_height"].cpu().numpy(), acc["texel_height"], 1e-4, "height")
+
+
+def test_batch_graph_replay_tracks_in_place_updates():
+    sc, adj, adj_off, cams, rgbs, targets = make_case(seed=11)
+    kw = bind_kwargs(sc, adj, adj_off, rgbs, targets)
+    step = BatchStep("cuda", [torch_cam(c) for c in cams], tile_width=16, chunk=2)
+    step.bind(**kw)
+    step.capture()
+    with torch.no_grad():
+        kw["density"].mul_(1.3)
+        kw["points"].add_(0.01)
+    step.run()
+    torch.cuda.synchronize()
+    step.check()
+    replay = [c.clone() for c in step.color] + [step.grads[k].clone() for k in sorted(step.grads)]
+    ref = BatchStep("cuda", [torch_cam(c) for c in cams], tile_width=16, chunk=2)
+    ref.bind(**kw)
+    ref.run()
+    eager = [c.clone() for c in ref.color] + [ref.grads[k].clone() for k in sorted(ref.grads)]
+    for a, b in zip(replay[:3], eager[:3]):
+        assert torch.equal(a, b)
+    for a, b in zip(replay[3:], eager[3:]):
+        assert_close_rel(a.cpu().numpy(), b.cpu().numpy(), 1e-5, "grad")
+    # the update changed the images
+    base = BatchStep("cuda", [torch_cam(c) for c in cams], tile_width=16, chunk=2)
+    base.bind(**bind_kwargs(sc, adj, adj_off, rgbs, targets))
+    base.run()
+    assert not torch.equal(base.color[0], replay[0])
+
+
+def test_batch_sh_prestep_and_adjoint():
+    sc, adj, adj_off, cams, rgbs, targets = make_case(seed=5)
+    rng = np.random.default_rng(9)
+    sh = (rng.standard_normal((sc["points"].shape[0], 16, 3)) * 0.3).astype(np.float32)
+    kw = bind_kwargs(sc, adj, adj_off, rgbs, targets)
+    kw.pop("texel_rgb")
+    step = BatchStep("cuda", [torch_cam(c) for c in cams], tile_width=8)
+    step.bind(**kw, sh=to_t(sh))
+    step.run()
+    step.check()
+    g_sh = np.zeros_like(sh)
+    for v, cam in enumerate(cams):
+        rgb = orc.sh_texel_rgb(sc["points"], sh, cam["eye"], S=sc["texel_sites"].shape[1])
+        assert max_abs(step.texel_rgb[v].cpu(), rgb) <= 1e-6
+        orc.sh_texel_rgb_backward(sc["points"], sh, cam["eye"], step.grad_texel_rgb[v].cpu().numpy(), g_sh)
+    assert_close_rel(step.grad_sh.cpu().numpy(), g_sh, 1e-5, "sh")
+
+
+def test_batch_argument_errors():
+    sc, adj, adj_off, cams, rgbs, targets = make_case(n=50)
+    with pytest.raises(ValueError):
+        BatchStep("cuda", [torch_cam(c) for c in cams], tile_width=12)
+    step = BatchStep("cuda", [torch_cam(c) for c in cams], tile_width=8)
+    kw = bind_kwargs(sc, adj, adj_off, rgbs, targets)
+    with pytest.raises(ValueError):
+        step.bind(**dict(kw, targets=kw["targets"][:2]))
+    step.bind(**kw)
+    step.set_schedule(chunk=0)
+    with pytest.raises(_lib.PfError):
+        step.run()
+
+
+def test_autotune_sweeps_and_caches(tmp_path):
+    sc, adj, adj_off, cams, rgbs, targets = make_case(seed=13, n=300)
+    tcams = [torch_cam(c) for c in cams]
+    kw = bind_kwargs(sc, adj, adj_off, rgbs, targets)
+    path = str(tmp_path / "tune.json")
+    step, table = autotune("cuda", tcams, kw, tile_widths=(8, 16), chunks=(1, 2), orders=("longest",), iters=1,
+                           warmup=1, cache_path=path)
+    assert len(table) == 4
+    best = min(table, key=lambda r: r["ms"])
+    assert (step.tile_width, step.chunk, step.order) == (best["tile_width"], best["chunk"], best["order"])
+    cache = json.load(open(path))
+    key = tune_key(torch.device("cuda"), tcams, sc["points"].shape[0], sc["texel_sites"].shape[1])
+    assert cache[key]["tile_width"] == best["tile_width"]
+    step2, table2 = autotune("cuda", tcams, kw, tile_widths=(8, 16), chunks=(1, 2), orders=("longest",),
+                             cache_path=path)
+    assert table2 == cache[key]["table"]
+    assert (step2.tile_width, step2.chunk) == (step.tile_width, step.chunk)
+    step2.run()
+    step2.check()
