@@ -49,10 +49,12 @@ def parse():
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--tile", type=int, default=8)
-    p.add_argument("--workload", default=WORKLOAD, help="raster1m (the measured configuration) or raster256k "
-                   "(a quarter-size case with the same density per pixel, for profiling)")
+    p.add_argument("--workload", default=WORKLOAD, help="raster1m (the measured configuration), raster256k "
+                   "(a quarter-size case with the same density per pixel, for profiling), batch3m (32 views of "
+                   "a 3.1M-primitive scene in one graph-captured persistent step) or batch256k (its small case)")
     p.add_argument("--cpu-sample-tiles", type=int, default=0, help="tiles composited by the CPU baseline")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-autotune", action="store_true", help="batch workloads: use --tile, chunk 1")
     return p.parse_args()
 
 
@@ -265,6 +267,179 @@ def reference_arm(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def bin_launches(T, with_order=True):
+    """Kernels one pf_bin call launches: count 1, depth sort 4 radix passes of 5
+    kernels (histogram, 3-kernel scan, scatter), gather 1, scan 3, emit 1, tile
+    sort ceil(log2(T)/8) passes, tile ranges 1; + 16 for the tile order (key
+    kernel and 3 passes)."""
+    bits = max(int(T - 1).bit_length(), 0)
+    return 1 + 20 + 1 + 3 + 1 + 5 * ((bits + 7) // 8) + 1 + (16 if with_order else 0)
+
+
+def batch_main(args, world, rank, local, dev):
+    """Batched multi-view workload: 32 views of sizes drawn from {320x240,
+    640x480, 1280x720, 1920x1080} of a 3,145,728-primitive scene (64-component
+    mixture), one graph-captured step = SH pre-step + binning of every view +
+    the persistent forward/loss/adjoint launch + SH adjoint.  Views are split
+    round-robin over ranks; with N > 1 the gradients are all-reduced (NCCL)."""
+    from powerfoam_b200 import synthetic
+    from powerfoam_b200.adjacency import CechBuilder
+    from powerfoam_b200.batch import autotune
+
+    cfg = synthetic.CONFIGS[args.workload]
+    scene = synthetic.make_scene(cfg["n"], seed=cfg["seed"], mixture=cfg["mixture"], sigma=cfg["sigma"],
+                                 r_range=cfg["r_range"], device=dev)
+    cams_all = synthetic.batch_cameras(cfg["views"], cfg["seed"], cfg["vfov"], device=dev)
+    mine = list(range(rank, len(cams_all), world))
+    cams = [cams_all[v] for v in mine]
+    adj, adj_off = CechBuilder(dev)(scene["points"], scene["radii"])
+    g = torch.Generator().manual_seed(300)
+    targets_host = [torch.rand((c.height, c.width, 3), generator=g) for c in cams_all]
+    targets_host = [targets_host[v].pin_memory() for v in mine]
+    targets = [t.to(dev) for t in targets_host]
+    kw = dict(points=scene["points"], radii=scene["radii"], density=scene["density"], normals=scene["normals"],
+              texel_sites=scene["texel_sites"], texel_height=scene["texel_height"], adjacency=adj,
+              adjacency_offsets=adj_off, targets=targets, sh=scene["sh"])
+    t0 = time.perf_counter()
+    if args.no_autotune:
+        from powerfoam_b200.batch import BatchStep
+
+        step = BatchStep(dev, cams, args.tile, 1, "longest")
+        step.bind(**kw)
+        table = []
+    else:
+        step, table = autotune(dev, cams, kw, chunks=(1, 4), iters=1, warmup=1,
+                               log=(lambda m: print(m, file=sys.stderr, flush=True)) if rank == 0 else None)
+    tune_s = time.perf_counter() - t0
+    step.capture()
+    flat = None
+    if world > 1:
+        names = sorted(step.grads)
+        flat = torch.empty(sum(step.grads[k].numel() for k in names) + step.grad_sh.numel(), device=dev)
+
+    def run():
+        loss = step.run()
+        if world > 1:
+            torch.cat([step.grads[k].reshape(-1) for k in sorted(step.grads)] + [step.grad_sh.reshape(-1)], out=flat)
+            torch.distributed.all_reduce(flat)
+        return loss
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+
+    for _ in range(max(args.warmup, 3)):
+        run()
+    barrier()
+    step.check()
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    barrier()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(args.steps):
+        run()
+    b.record()
+    barrier()
+    clk = clocks.stop()
+    ms = a.elapsed_time(b) / args.steps
+    # end to end: every view's target image from pinned host memory in, the per-view losses out
+    loss_host = torch.empty((args.steps, len(cams)), dtype=torch.float32).pin_memory()
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for i in range(args.steps):
+        for t_dev, t_host in zip(step.targets, targets_host):
+            t_dev.copy_(t_host, non_blocking=True)
+        loss = run()
+        loss_host[i].copy_(loss, non_blocking=True)
+    e1.record()
+    barrier()
+    e2e_ms = e0.elapsed_time(e1) / args.steps
+    if world > 1:
+        t = torch.tensor([ms, e2e_ms], device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms, e2e_ms = (float(x) for x in t.tolist())
+    # live kernel time of the persistent launch (eager runs, events around it)
+    step.kernel_events = []
+    for _ in range(3):
+        step._launch()
+    torch.cuda.synchronize()
+    k_ms = statistics.mean(x.elapsed_time(y) for x, y in step.kernel_events)
+    step.kernel_events = None
+    # the same work as separate per-view calls (SH pre-step, Rasterizer forward, loss, backward), for comparison
+    from powerfoam_b200 import rasterize
+
+    R = rasterize.Rasterizer(Args(), dev, tile_width=step.tile_width)
+    pnames = ["points", "radii", "density", "normals", "texel_sites", "texel_height"]
+    params = {k: scene[k].clone().requires_grad_(True) for k in pnames}
+
+    def per_view_pass():
+        for v, c in enumerate(cams):
+            rgb = synthetic.texel_rgb(scene, c).requires_grad_(True)
+            out = R.forward(c, None, params["points"], params["radii"], params["density"], params["normals"],
+                            params["texel_sites"], rgb, params["texel_height"], adj, adj_off, None, False)
+            ((out[0] - step.targets[v]) ** 2).sum().backward()
+
+    per_view_pass()
+    torch.cuda.synchronize()
+    s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s0.record()
+    per_view_pass()
+    s1.record()
+    torch.cuda.synchronize()
+    sequential_ms = s0.elapsed_time(s1)
+    del R, params
+    alg = 0
+    pairs = 0
+    for v, c in enumerate(cams):
+        class _B:
+            pass
+        bins = _B()
+        bins.tile_offsets = step.tile_offsets[v]
+        n_p = int(step.bin_scalars[v, 0])
+        bins.tile_prims = step.tile_prims[v][:n_p]
+        bins.n_pairs = n_p
+        pairs += n_p
+        st = algorithmic_bytes(dict(bins=bins, early_stop=step.early_stop[v], adjacency_offsets=adj_off,
+                                    contrib_pairs=step.tile_contrib_pairs[v], n_prims=cfg["n"]), c.height, c.width)
+        alg += st["fwd"] + st["bwd"]
+    peak, peak_kind = load_peaks()
+    achieved = alg / (k_ms * 1e-3) / 1e9
+    n_views = len(cams_all)
+    pixels = sum(c.width * c.height for c in cams_all)
+    V = len(cams)
+    # pack 1, neighbour encoding 1, SH pre-step V, binning per view, the batch launch (work list: keys 1
+    # + three 5-kernel radix passes when ordered by length; the persistent kernel 1; 6 + V sanitise), SH adjoint V
+    per_step = 1 + 1 + V + sum(bin_launches(T, with_order=False) for T in step.n_tiles)
+    per_step += 1 + (15 if step.order == "longest" else 0) + 1 + 6 + V + V
+    line = dict(metric="batched multi-view fwd+bwd, views/s", value=n_views * 1000.0 / ms,
+                unit="views/s (32 views per step)", n_gpus=world, steps=args.steps, warmup=max(args.warmup, 3),
+                ms_per_step=ms, higher_is_better=True, scaling="strong", vs_baseline=None, dtype="f32",
+                data="synthetic (seeded scene, orbit cameras, uniform targets)",
+                config=dict(workload=args.workload, prims=cfg["n"], views=n_views, pixels=pixels, pairs=pairs,
+                            tile=step.tile_width, chunk=step.chunk, order=step.order, autotune_s=tune_s,
+                            per_view_calls_ms=sequential_ms,
+                            autotune=table, graph="one CUDA graph per step",
+                            l2="inputs larger than L2 (805 MB of primitive records), no flush",
+                            parallelism=f"view-dp{world}"),
+                clocks=clk,
+                e2e=dict(value=n_views * 1000.0 / e2e_ms, unit="views/s",
+                         h2d_bytes_per_step=sum(t.numel() * 4 for t in targets_host),
+                         d2h_bytes_per_step=4 * len(cams)),
+                roofline=dict(bound="hbm", kernel="pf_batch_render", achieved=achieved, peak=peak, unit="GB/s",
+                              frac=achieved / peak, peak_source=peak_kind, traffic=None, algorithmic_bytes=alg,
+                              ms=k_ms),
+                gpu_launches=args.steps * per_step)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    step.graph = None
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -279,6 +454,9 @@ def main():
         import datetime
 
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
+    if args.workload.startswith("batch"):
+        batch_main(args, world, rank, local, dev)
+        return
     from powerfoam_b200 import rasterize
 
     cfg, scene, cam, adj, adj_off, target = build_workload(dev, rank, args.tile, args.workload)
@@ -377,12 +555,8 @@ def main():
                               traffic=load_traffic(dominant, args.workload),
                               algorithmic_bytes=dom_bytes, ms=dom_ms, fwd_ms=fwd_ms, bwd_ms=bwd_ms),
                 gpu_launches=None)
-    # kernels per step: pack 1, bin 31 (+3 per extra tile-sort pass), prefetch 1, SH 1, forward 1,
-    # backward 1 + 7 sanitise
-    T = st["T"]
-    tile_passes = max(0, (int(T - 1).bit_length() + 7) // 8)
-    bin_k = 1 + 4 * 5 + 1 + 3 + 1 + tile_passes * 5 + 1
-    line["gpu_launches"] = args.steps * (1 + bin_k + 1 + 1 + 1 + 1 + 7)
+    # kernels per step: pack 1, binning with tile order, prefetch 1, SH 1, forward 1, backward 1 + 7 sanitise
+    line["gpu_launches"] = args.steps * (1 + bin_launches(st["T"]) + 1 + 1 + 1 + 1 + 7)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(cfg, scene, cam, adj, adj_off, target, args.cpu_sample_tiles or 200,
                                             args.tile)

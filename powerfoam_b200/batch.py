@@ -58,6 +58,7 @@ class BatchStep:
         self.headroom = headroom
         self.graph = None
         self.bound = False
+        self.kernel_events = None  # a list: eager runs append (start, end) events around pf_batch_render
         _lib.load()
         tw = tile_width
         self.n_tiles = [(1 + (c.height - 1) // tw) * (1 + (c.width - 1) // tw) for c in self.cameras]
@@ -218,11 +219,17 @@ class BatchStep:
                           _lib.ptr(self.texel_rgb[v]), st)
         self._bin_all()
         g = self.grads
+        if self.kernel_events is not None:
+            ev = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+            ev[0].record()
         _lib.call("pf_batch_render", _lib.ctypes.byref(self._scene), self._views, len(self.cameras), self.tile_width,
                   self.chunk, ORDERS[self.order], _lib.ptr(self.batch_ws), self.batch_ws.numel(),
                   _lib.ptr(self.tile_loss), _lib.ptr(g["points"]), _lib.ptr(g["radii"]), _lib.ptr(g["normals"]),
                   _lib.ptr(g["density"]), _lib.ptr(g["texel_sites"]), _lib.ptr(g["texel_height"]),
                   _lib.ptr(self.status), st)
+        if self.kernel_events is not None:
+            ev[1].record()
+            self.kernel_events.append(ev)
         if self.sh is not None:
             self.grad_sh.zero_()
             for v in range(len(self.cameras)):
@@ -324,11 +331,15 @@ def time_step(step, iters=3, warmup=1):
 
 
 def autotune(device, cameras, bind_kwargs, tile_widths=TILE_WIDTHS, chunks=CHUNKS, orders=("longest", "view"),
-             iters=3, warmup=1, cache_path=None, use_cache=True, transmittance_threshold=1e-3, log=None):
+             iters=3, warmup=1, cache_path=None, use_cache=True, transmittance_threshold=1e-3, log=None,
+             prune=1.3):
     """Sweep tile width x work-queue chunk x item order over the real step and
     return (best BatchStep bound and ready, table).  Each candidate is timed
-    with CUDA events over `iters` eager runs after `warmup`.  The winner is
-    cached in a JSON file keyed by tune_key(); a cached entry skips the sweep."""
+    with CUDA events over `iters` eager runs after `warmup`.  Tile widths are
+    swept in the given order; once a width's best time exceeds `prune` x the
+    best so far, the remaining widths are skipped (step time grows
+    monotonically with the width on these workloads).  The winner is cached in
+    a JSON file keyed by tune_key(); a cached entry skips the sweep."""
     cache_path = cache_path or default_cache_path()
     n = bind_kwargs["points"].shape[0]
     S = bind_kwargs["texel_sites"].shape[1]
@@ -364,6 +375,11 @@ def autotune(device, cameras, bind_kwargs, tile_widths=TILE_WIDTHS, chunks=CHUNK
                     best = dict(row)
         del step
         torch.cuda.empty_cache()
+        width_best = min(r["ms"] for r in table if r["tile_width"] == tw)
+        if prune and width_best > prune * best["ms"]:
+            if log:
+                log(f"autotune: tile {tw} is {width_best / best['ms']:.2f}x the best; larger widths skipped")
+            break
     best["table"] = table
     cache[key] = best
     try:

@@ -103,6 +103,18 @@ def orbit_camera(seed, width, height, vfov_deg, distance=3.0, device="cuda", azi
     return look_at(eye, (0.0, 0.0, 0.0), width, height, vfov_deg, device=device)
 
 
+BATCH_RESOLUTIONS = ((320, 240), (640, 480), (1280, 720), (1920, 1080))
+
+
+def batch_cameras(n_views, seed, vfov_deg=50.0, distance=3.0, device="cuda", resolutions=BATCH_RESOLUTIONS):
+    """n_views orbit cameras, each resolution drawn uniformly from
+    `resolutions` (seeded)."""
+    g = torch.Generator().manual_seed(seed)
+    idx = torch.randint(0, len(resolutions), (n_views,), generator=g).tolist()
+    return [orbit_camera(seed * 1000 + v, *resolutions[i], vfov_deg, distance, device=device)
+            for v, i in enumerate(idx)]
+
+
 def front_camera(width, height, vfov_deg, distance=3.0, device="cuda"):
     return look_at((0.0, 0.0, distance), (0.0, 0.0, 0.0), width, height, vfov_deg, device=device)
 
@@ -127,7 +139,8 @@ CONFIGS = {
                        vfov=50.0),
     "trace1m": dict(n=1048576, seed=1, mixture=32, sigma=0.15, r_range=(0.002, 0.02), width=1280, height=720,
                     vfov=50.0),
-    "batch3m": dict(n=3145728, seed=3, mixture=64, sigma=0.15, r_range=(0.002, 0.02), vfov=50.0),
+    "batch3m": dict(n=3145728, seed=3, mixture=64, sigma=0.15, r_range=(0.002, 0.02), vfov=50.0, views=32),
+    "batch256k": dict(n=262144, seed=3, mixture=64, sigma=0.15, r_range=(0.004, 0.04), vfov=50.0, views=8),
     "trace6m": dict(n=6291456, seed=4, mixture=64, sigma=0.1, r_range=(0.001, 0.01), width=2048, height=1536,
                     vfov=50.0),
 }
