@@ -233,11 +233,82 @@ PF_API int pf_trace_backward(const pf_trace_inputs *in, const float *color, cons
                              float *grad_points, float *grad_radii, float *grad_normals, float *grad_density,
                              float *grad_texel_sites, float *grad_texel_rgb, float *grad_texel_height, void *stream);
 
+/* Training labels of the ray-proposal network (no counterpart in the
+ * reference): the walk of pf_trace_forward (f32 attributes) writing, per
+ * pixel ray, the colour and the first cell after whose compositing the
+ * transmittance is below label_threshold: the t at which the ray enters it
+ * (label_t), the cell (label_cell) and the cells walked before it
+ * (label_step), all -1 when the transmittance never falls below the
+ * threshold. */
+PF_API int pf_trace_labels(const pf_trace_inputs *in, float label_threshold, float *color, float *label_t,
+                           int32_t *label_cell, int32_t *label_step, int32_t *visit_count, int32_t *status,
+                           void *stream);
+
 /* Start cell of benchmark.py:320-324: argmin_i |p_i - eye|^2 - r_i^2 (first
  * index on ties).  workspace: pf_start_cell_workspace_size bytes. */
 PF_API int pf_start_cell_workspace_size(int64_t n_prims, size_t *bytes);
 PF_API int pf_start_cell(const float *points, const float *radii, int64_t n_prims, const float *eye_host,
                   void *workspace, size_t workspace_bytes, int32_t *out_idx, void *stream);
+
+/* ---------------------------------------------------------------------- */
+/* Point location in the power diagram: the cell containing x is
+ * argmin_i |x - p_i|^2 - r_i^2 (the start-cell rule of benchmark.py:320-324
+ * applied to any point; lowest index on ties).  pf_locator_build buckets the
+ * primitives in a uniform grid kept in the caller's workspace
+ * (pf_locator_workspace_size bytes); queries scan grid shells until no
+ * unscanned primitive can win.  A query cut short by the shell cap raises
+ * PF_ERR_SEED in *status.  No counterpart in the reference (its start cell
+ * is a brute-force argmin for the camera eye only). */
+PF_API int pf_locator_workspace_size(int64_t n_prims, size_t *bytes);
+PF_API int pf_locator_build(const float *points, const float *radii, int64_t n_prims, void *workspace,
+                            size_t workspace_bytes, void *stream);
+PF_API int pf_locate_cells(const float *points, const float *radii, int64_t n_prims, const void *workspace,
+                           const float *queries /* (n,3) */, int64_t n_queries, int32_t *cells, int32_t *status,
+                           void *stream);
+/* Proposal-seeded start cells for every pixel ray of `cam`: where
+ * confidence >= conf_threshold and t_entry > 0 the cell containing
+ * eye + t_entry * dir (the ray's walk then skips the cells before it), else
+ * default_start.  *n_seeded (optional) accumulates the seeded rays. */
+PF_API int pf_seed_start_cells(const float *points, const float *radii, int64_t n_prims, const void *workspace,
+                               const pf_camera *cam, const float *t_entry, const float *confidence,
+                               float conf_threshold, int32_t default_start, int32_t *start_cells,
+                               int32_t *n_seeded, void *stream);
+
+/* ---------------------------------------------------------------------- */
+/* Ray-proposal network (no counterpart in the reference): 6-frequency
+ * positional encoding of (origin / 3, unit direction) -> 3 x 64 ReLU -> (entry
+ * distance, confidence), BF16 tcgen05 GEMMs with FP32 accumulation in tensor
+ * memory.  Parameters: pf_mlp_param_count() FP32 values, four row-major
+ * (out x 80) matrices (64, 64, 64 and 16 rows; input column 78 of layer 1 and
+ * 64 of layers 2-4 carry the bias, other pad columns and rows 2..15 of layer
+ * 4 are zero); the kernels read a BF16 image of pf_mlp_image_bytes() bytes
+ * that pf_mlp_pack (or pf_mlp_adam) writes.
+ * pf_mlp_forward: rays (n,6) = origin, unit direction, or every pixel ray of
+ *   `cam` when rays is NULL; writes t_entry (world units) and confidence.
+ * pf_mlp_train_step: one minibatch of `batch` rays drawn (hashed with *step
+ *   and seed) from rays (n,8) = origin, direction, label t (< 0: no hit), pad;
+ *   loss = asymmetric squared error of t / 6 (overshoot_weight on
+ *   over-estimates) + cross-entropy of the confidence against "seed is safe"
+ *   (hit and t_pred - margin <= t); ADDS the mean-loss gradient into grad and
+ *   the loss sums into loss[0..1] (may be NULL).
+ * pf_mlp_adam: Adam on the master weights, clears grad, writes the image and
+ *   advances *step (done: a device word, zero before the first call).
+ * pf_mlp_gemm_selftest: D (128 x 80 f32) = A (128 x 128) B^T (B 80 x 128),
+ *   BF16 row-major inputs, through the tensor-core path with mode 0: both
+ *   K-major, 1: B MN-major, 2: both MN-major (the three operand arrangements
+ *   the network uses). */
+PF_API int pf_mlp_param_count(void);
+PF_API int pf_mlp_image_bytes(void);
+PF_API int pf_mlp_pack(const float *weights, uint8_t *image, void *stream);
+PF_API int pf_mlp_forward(const uint8_t *image, const float *rays, int64_t n_rays, const pf_camera *cam,
+                          float *t_entry, float *confidence, int32_t *status, void *stream);
+PF_API int pf_mlp_train_step(const uint8_t *image, const float *rays, int64_t n_rays, int32_t batch,
+                             const int32_t *step, uint32_t seed, float overshoot_weight, float margin, float *grad,
+                             float *loss, int32_t *status, void *stream);
+PF_API int pf_mlp_adam(float *weights, float *m, float *v, float *grad, uint8_t *image, int32_t *step,
+                       uint32_t *done, float lr, float beta1, float beta2, float eps, void *stream);
+PF_API int pf_mlp_gemm_selftest(const uint16_t *a, const uint16_t *b, int32_t mode, float *d, int32_t *status,
+                                void *stream);
 
 /* ---------------------------------------------------------------------- */
 /* Batched multi-view training step.  No counterpart in the reference, whose

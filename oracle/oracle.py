@@ -221,6 +221,28 @@ def trace_forward(cam, spheres, nsigmas, sites, rgbs, heights, adj, adj_off, adj
     return out
 
 
+def trace_labels(cam, spheres, nsigmas, sites, rgbs, heights, adj, adj_off, adj_diff_pm, start_idx=0,
+                 start_cells=None, thr=1e-3, max_steps=1 << 16, label_thr=0.99):
+    """Proposal-network labels of every camera ray: entry t / cell / step of
+    the first cell after which the transmittance is below label_thr (-1 when
+    never), with the colour and the number of cells walked."""
+    H, W = cam.height, cam.width
+    S = sites.shape[1]
+    out = dict(color=np.zeros((H, W, 3), F32), label_t=np.zeros((H, W), F32),
+               label_cell=np.zeros((H, W), np.int32), label_step=np.zeros((H, W), np.int32),
+               visit_count=np.zeros((H, W), np.int32), status=np.zeros((H, W), np.int32))
+    args = [_c(spheres, F32), _c(nsigmas, F32), _c(sites, F32), _c(rgbs, F32), _c(heights, F32)]
+    sc = None if start_cells is None else _c(start_cells, np.int32)
+    rc = lib().orc_trace_labels_f32(
+        ctypes.byref(cam), *[_p(a) for a in args], ctypes.c_int(S), _p(_c(adj, np.int32)),
+        _p(_c(adj_off, np.int32)), _p(_c(adj_diff_pm, np.uint16)), ctypes.c_int32(start_idx), _p(sc),
+        ctypes.c_float(thr), ctypes.c_int(max_steps), ctypes.c_float(label_thr), _p(out["color"]),
+        _p(out["label_t"]), _p(out["label_cell"]), _p(out["label_step"]), _p(out["visit_count"]),
+        _p(out["status"]))
+    out["rc"] = rc
+    return out
+
+
 def start_cell(points, radii, eye):
     f = lib().orc_start_cell_f32
     f.restype = ctypes.c_int32

@@ -1233,13 +1233,19 @@ static void nbr_pm(const float *spheres, const int32_t *adj, const uint16_t *adj
     }
 }
 
-int FN(orc_trace_forward)(const orc_camera *camera, const float *spheres, const float *nsigmas,
+/* The walk of orc_trace_forward.  With label outputs it also records, per
+ * ray, the first cell after whose compositing the transmittance is below
+ * label_thr: the t at which the ray enters that cell (label_t), the cell
+ * (label_cell) and the number of cells walked before it (label_step); -1 in
+ * all three when the transmittance never falls below label_thr. */
+static int FN(trace_walk)(const orc_camera *camera, const float *spheres, const float *nsigmas,
                           const float *sites, const float *rgbs, const float *heights, int S,
                           const int32_t *adj, const int32_t *adj_off, const uint16_t *adj_diff,
                           int32_t start_idx, const int32_t *start_cells, float thr, int max_steps,
                           float depth_quantile, out_t *color, out_t *log_t_out, out_t *depth, out_t *normal,
                           int32_t *depth_seg, out_t *depth_sigma, int32_t *visit_log, int visit_cap,
-                          int32_t *visit_count, int32_t *status) {
+                          int32_t *visit_count, int32_t *status, float label_thr, out_t *label_t,
+                          int32_t *label_cell, int32_t *label_step) {
     cam_t cam = cam_load(camera);
     int64_t P = (int64_t)cam.H * cam.W;
     v3 o = cam.eye;
@@ -1256,11 +1262,15 @@ int FN(orc_trace_forward)(const orc_camera *camera, const float *spheres, const 
         int steps = 0, st = ORC_OK, seg = 0;
         int32_t dseg = -1;
         real dout = 0, dsig = 0;
+        real lab_t = -1;
+        int32_t lab_cell = -1, lab_step = -1;
         for (;;) {
             real trans = r_exp(log_t);
             if (trans < (real)thr || prim == NO_CELL) break;
             if (steps >= max_steps) { st = ORC_ERR_STEP_CAP; break; }
             if (visit_log && steps < visit_cap) visit_log[px * visit_cap + steps] = prim;
+            const real cell_entry = pt_near;
+            const int32_t cell = prim;
             steps++;
             const float *sp = spheres + 4 * (int64_t)prim;
             v3 center = ld3(sp);
@@ -1307,9 +1317,17 @@ int FN(orc_trace_forward)(const orc_camera *camera, const float *spheres, const 
                     dseg = seg;
                     dsig = sigma;
                 }
+                if (lab_cell < 0 && r_exp(log_t) < (real)label_thr) {
+                    lab_t = cell_entry;
+                    lab_cell = cell;
+                    lab_step = steps - 1;
+                }
                 seg++;
             }
         }
+        if (label_t) label_t[px] = (out_t)lab_t;
+        if (label_cell) label_cell[px] = lab_cell;
+        if (label_step) label_step[px] = lab_step;
         color[3 * px + 0] = (out_t)rgb.x;
         color[3 * px + 1] = (out_t)rgb.y;
         color[3 * px + 2] = (out_t)rgb.z;
@@ -1327,6 +1345,32 @@ int FN(orc_trace_forward)(const orc_camera *camera, const float *spheres, const 
         if (st > worst) worst = st;
     }
     return worst;
+}
+
+int FN(orc_trace_forward)(const orc_camera *camera, const float *spheres, const float *nsigmas,
+                          const float *sites, const float *rgbs, const float *heights, int S,
+                          const int32_t *adj, const int32_t *adj_off, const uint16_t *adj_diff,
+                          int32_t start_idx, const int32_t *start_cells, float thr, int max_steps,
+                          float depth_quantile, out_t *color, out_t *log_t_out, out_t *depth, out_t *normal,
+                          int32_t *depth_seg, out_t *depth_sigma, int32_t *visit_log, int visit_cap,
+                          int32_t *visit_count, int32_t *status) {
+    return FN(trace_walk)(camera, spheres, nsigmas, sites, rgbs, heights, S, adj, adj_off, adj_diff, start_idx,
+                          start_cells, thr, max_steps, depth_quantile, color, log_t_out, depth, normal, depth_seg,
+                          depth_sigma, visit_log, visit_cap, visit_count, status, 0.0f, NULL, NULL, NULL);
+}
+
+/* Training labels of the ray-proposal network (no counterpart in the
+ * reference): the walk of orc_trace_forward with the label outputs of
+ * trace_walk; colour is written too (the image the labels belong to). */
+int FN(orc_trace_labels)(const orc_camera *camera, const float *spheres, const float *nsigmas,
+                         const float *sites, const float *rgbs, const float *heights, int S,
+                         const int32_t *adj, const int32_t *adj_off, const uint16_t *adj_diff,
+                         int32_t start_idx, const int32_t *start_cells, float thr, int max_steps,
+                         float label_thr, out_t *color, out_t *label_t, int32_t *label_cell, int32_t *label_step,
+                         int32_t *visit_count, int32_t *status) {
+    return FN(trace_walk)(camera, spheres, nsigmas, sites, rgbs, heights, S, adj, adj_off, adj_diff, start_idx,
+                          start_cells, thr, max_steps, 0.5f, color, NULL, NULL, NULL, NULL, NULL, NULL, 0,
+                          visit_count, status, label_thr, label_t, label_cell, label_step);
 }
 
 /* start cell of benchmark.py:320-324: argmin_i |p_i - eye|^2 - r_i^2 with the

@@ -154,6 +154,19 @@ _SIGS = {
     "pf_batch_workspace_size": [ctypes.POINTER(PfBatchView), c_i32, c_i32, ctypes.POINTER(ctypes.c_size_t)],
     "pf_batch_render": [ctypes.POINTER(PfBatchScene), ctypes.POINTER(PfBatchView), c_i32, c_i32, c_i32, c_i32, c_vp,
                         ctypes.c_size_t, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp],
+    "pf_trace_labels": [ctypes.POINTER(PfTraceInputs), c_f, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp],
+    "pf_locator_workspace_size": [c_i64, ctypes.POINTER(ctypes.c_size_t)],
+    "pf_locator_build": [c_vp, c_vp, c_i64, c_vp, ctypes.c_size_t, c_vp],
+    "pf_locate_cells": [c_vp, c_vp, c_i64, c_vp, c_vp, c_i64, c_vp, c_vp, c_vp],
+    "pf_seed_start_cells": [c_vp, c_vp, c_i64, c_vp, ctypes.POINTER(PfCamera), c_vp, c_vp, c_f, c_i32, c_vp, c_vp,
+                            c_vp],
+    "pf_mlp_param_count": [],
+    "pf_mlp_image_bytes": [],
+    "pf_mlp_pack": [c_vp, c_vp, c_vp],
+    "pf_mlp_forward": [c_vp, c_vp, c_i64, ctypes.POINTER(PfCamera), c_vp, c_vp, c_vp, c_vp],
+    "pf_mlp_train_step": [c_vp, c_vp, c_i64, c_i32, c_vp, ctypes.c_uint32, c_f, c_f, c_vp, c_vp, c_vp, c_vp],
+    "pf_mlp_adam": [c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_f, c_f, c_f, c_f, c_vp],
+    "pf_mlp_gemm_selftest": [c_vp, c_vp, c_i32, c_vp, c_vp, c_vp],
     "pf_cech_workspace_size": [c_i64, ctypes.POINTER(ctypes.c_size_t)],
     "pf_cech_adjacency": [c_vp, c_vp, c_i64, c_vp, ctypes.c_size_t, c_i64, c_vp, c_vp, c_vp, c_vp, c_vp],
     "pf_morton_workspace_size": [c_i64, ctypes.POINTER(ctypes.c_size_t)],

@@ -277,6 +277,141 @@ __global__ void gather_u32_kernel(const uint32_t* __restrict__ src, const uint32
     if (i < N) dst[i] = src[perm[i]];
 }
 
+// ---------------------------------------------------------------------------
+// Cell location: the power cell containing a point x is the primitive that
+// minimises |x - p_i|^2 - r_i^2 (the cell of benchmark.py:320-324 for an
+// arbitrary point).  Primitives are bucketed in a uniform grid of about four
+// per cell; a query scans shells of grid cells around x's cell and stops once
+// every unscanned primitive lies at least s * h away, i.e. its power distance
+// is at least (s h)^2 - rmax^2 >= the best found.  Ties go to the lower index.
+constexpr int kLocateMaxShell = 48;
+
+__global__ void locate_grid_kernel(const float* __restrict__ bkeys, int64_t N, int max_cells_log2,
+                                   CechGrid* __restrict__ g, float* __restrict__ rmax_out) {
+    const int* k = (const int*)bkeys;
+    float lo[3], hi[3];
+    for (int i = 0; i < 3; i++) {
+        lo[i] = from_key(k[i]);
+        hi[i] = from_key(k[3 + i]);
+    }
+    *rmax_out = from_key(k[6]);
+    double vol = 1.0;
+    for (int i = 0; i < 3; i++) vol *= fmax((double)(hi[i] - lo[i]), 1e-6);
+    float h = (float)cbrt(vol * 4.0 / (double)(N > 0 ? N : 1));
+    h = fmaxf(h, 1e-6f);
+    g->nx = g->ny = g->nz = 1;
+    for (int it = 0; it < 256; it++) {
+        double nx = floor((double)(hi[0] - lo[0]) / h) + 1, ny = floor((double)(hi[1] - lo[1]) / h) + 1,
+               nz = floor((double)(hi[2] - lo[2]) / h) + 1;
+        if (!(nx * ny * nz < 1e30)) break;
+        if (nx * ny * nz < (double)(1ll << max_cells_log2)) {
+            g->nx = (int)nx;
+            g->ny = (int)ny;
+            g->nz = (int)nz;
+            break;
+        }
+        h *= 1.25f;
+    }
+    if (g->nx == 1 && g->ny == 1 && g->nz == 1) h = INFINITY;
+    g->lo_x = lo[0];
+    g->lo_y = lo[1];
+    g->lo_z = lo[2];
+    g->inv_h = 1.0f / h;
+}
+
+struct Locator {
+    const float* pts;
+    const float* radii;
+    const CechGrid* grid;
+    const int32_t* cell_start;
+    const uint32_t* sorted;
+    const float* rmax;
+};
+
+// returns the containing cell, or -1; *exact = false when the shell cap cut
+// the search short
+PF_D int32_t locate_point(const Locator& L, v3 x, bool* exact) {
+    const CechGrid g = *L.grid;
+    const float rmax = *L.rmax;
+    const float h = 1.0f / g.inv_h;
+    const int cx = cell_coord(x.x, g.lo_x, g.inv_h, g.nx);
+    const int cy = cell_coord(x.y, g.lo_y, g.inv_h, g.ny);
+    const int cz = cell_coord(x.z, g.lo_z, g.inv_h, g.nz);
+    const int smax = imax(imax(g.nx, g.ny), g.nz);
+    float best = INFINITY;
+    int32_t best_i = -1;
+    *exact = false;
+    for (int s = 0; s <= kLocateMaxShell; s++) {
+        for (int dz = -s; dz <= s; dz++) {
+            const int z = cz + dz;
+            if (z < 0 || z >= g.nz) continue;
+            for (int dy = -s; dy <= s; dy++) {
+                const int y = cy + dy;
+                if (y < 0 || y >= g.ny) continue;
+                const bool face = (dz == -s || dz == s || dy == -s || dy == s);
+                const int step = (face || s == 0) ? 1 : 2 * s;
+                for (int dx = -s; dx <= s; dx += step) {
+                    const int xx = cx + dx;
+                    if (xx < 0 || xx >= g.nx) continue;
+                    const int64_t c = ((int64_t)z * g.ny + y) * g.nx + xx;
+                    for (int32_t q = L.cell_start[c]; q < L.cell_start[c + 1]; q++) {
+                        const int32_t j = (int32_t)L.sorted[q];
+                        v3 dv = x - mk(L.pts[3 * j], L.pts[3 * j + 1], L.pts[3 * j + 2]);
+                        const float rj = L.radii[j];
+                        const float pd = dot(dv, dv) - rj * rj;
+                        if (pd < best || (pd == best && j < best_i)) {
+                            best = pd;
+                            best_i = j;
+                        }
+                    }
+                }
+            }
+        }
+        const float reach = (float)s * h;
+        if ((best_i >= 0 && reach * reach - rmax * rmax >= best) || s >= smax) {
+            *exact = true;
+            break;
+        }
+    }
+    return best_i;
+}
+
+__global__ void locate_kernel(Locator L, const float* __restrict__ q, int64_t n, int32_t* __restrict__ out,
+                              int32_t* __restrict__ status) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    bool exact;
+    out[i] = locate_point(L, mk(q[3 * i], q[3 * i + 1], q[3 * i + 2]), &exact);
+    if (!exact && status) atomicMax(status, PF_ERR_SEED);
+}
+
+// start cell of every pixel ray: the cell containing eye + t d where the
+// proposal is confident (conf >= conf_thr, t > 0), else the default start
+__global__ void seed_kernel(Locator L, Cam cam, const float* __restrict__ t_entry, const float* __restrict__ conf,
+                            float conf_thr, int32_t default_start, int32_t* __restrict__ start_cells,
+                            int32_t* __restrict__ n_seeded) {
+    const int64_t px = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t n = (int64_t)cam.W * cam.H;
+    bool seeded = false;
+    if (px < n) {
+        int32_t cell = default_start;
+        const float t = t_entry[px];
+        if (conf[px] >= conf_thr && t > 0.0f) {
+            const int pi = (int)(px / cam.W), pj = (int)(px % cam.W);
+            const v3 d = ray_dir(cam, pi, pj);
+            bool exact;
+            const int32_t c = locate_point(L, cam.eye + t * d, &exact);
+            if (c >= 0 && exact) {
+                cell = c;
+                seeded = true;
+            }
+        }
+        start_cells[px] = cell;
+    }
+    const unsigned b = __ballot_sync(0xffffffffu, seeded);
+    if ((threadIdx.x & 31) == 0 && b && n_seeded) atomicAdd(n_seeded, __popc(b));
+}
+
 static size_t align_up(size_t x) { return (x + 255) & ~(size_t)255; }
 
 struct CechLayout {
@@ -357,6 +492,80 @@ extern "C" int pf_cech_adjacency(const float* points, const float* radii, int64_
     offsets_i32_kernel<<<(unsigned)((N + 1 + 255) / 256), 256, 0, st>>>(off64, N, n_edges, edge_capacity,
                                                                         adjacency_offsets, status);
     return pf_check_launch("pf_cech_adjacency");
+}
+
+// The locator keeps, in its workspace, the grid, the primitive ids sorted by
+// grid cell and the per-cell ranges (the Čech layout without the edge lists).
+static Locator locator_view(const float* points, const float* radii, int64_t N, char* ws) {
+    CechLayout L = cech_layout(N);
+    uint32_t* key0 = (uint32_t*)(ws + L.key0);
+    uint32_t* key1 = (uint32_t*)(ws + L.key1);
+    uint32_t* kf = radix_final_key_buffer(key0, key1, kMaxCellsLog2);
+    Locator loc;
+    loc.pts = points;
+    loc.radii = radii;
+    loc.grid = (const CechGrid*)(ws + L.grid);
+    loc.cell_start = (const int32_t*)(ws + L.cell_start);
+    loc.sorted = kf == key0 ? (const uint32_t*)(ws + L.idx0) : (const uint32_t*)(ws + L.idx1);
+    loc.rmax = (const float*)(ws + L.bounds + 32);
+    return loc;
+}
+
+extern "C" int pf_locator_workspace_size(int64_t n_prims, size_t* bytes) {
+    return pf_cech_workspace_size(n_prims, bytes);
+}
+
+extern "C" int pf_locator_build(const float* points, const float* radii, int64_t n_prims, void* workspace,
+                                size_t workspace_bytes, void* stream) {
+    if (n_prims <= 0 || n_prims >= ((int64_t)1 << 31) || !points || !radii)
+        return pf_fail(PF_ERR_ARGS, "pf_locator_build: bad arguments");
+    CechLayout L = cech_layout(n_prims);
+    if (!workspace || workspace_bytes < L.bytes) return pf_fail(PF_ERR_ARGS, "pf_locator_build: workspace too small");
+    cudaStream_t st = (cudaStream_t)stream;
+    char* ws = (char*)workspace;
+    float* bounds = (float*)(ws + L.bounds);
+    CechGrid* grid = (CechGrid*)(ws + L.grid);
+    uint32_t *key0 = (uint32_t*)(ws + L.key0), *idx0 = (uint32_t*)(ws + L.idx0);
+    uint32_t *key1 = (uint32_t*)(ws + L.key1), *idx1 = (uint32_t*)(ws + L.idx1);
+    int32_t* cell_start = (int32_t*)(ws + L.cell_start);
+    RadixScratch rs{(uint32_t*)(ws + L.rhist), (uint32_t*)(ws + L.rpart)};
+    const int64_t N = n_prims;
+    const unsigned gN = (unsigned)((N + 255) / 256);
+    bounds_init_kernel<<<1, 1, 0, st>>>(bounds);
+    bounds_kernel<<<(unsigned)std::min<int64_t>(gN, 148 * 8), 256, 0, st>>>(points, radii, N, bounds);
+    locate_grid_kernel<<<1, 1, 0, st>>>(bounds, N, kMaxCellsLog2, grid, bounds + 8);
+    cell_key_kernel<<<gN, 256, 0, st>>>(points, N, grid, key0, idx0);
+    uint32_t* kf = radix_final_key_buffer(key0, key1, kMaxCellsLog2);
+    uint32_t* vf = kf == key0 ? idx0 : idx1;
+    radix_sort_pairs(key0, idx0, key1, idx1, kf, vf, N, nullptr, kMaxCellsLog2, rs, st);
+    cell_ranges_kernel<<<(unsigned)((N + 1 + 255) / 256), 256, 0, st>>>(kf, N, grid, cell_start);
+    return pf_check_launch("pf_locator_build");
+}
+
+extern "C" int pf_locate_cells(const float* points, const float* radii, int64_t n_prims, const void* workspace,
+                               const float* queries, int64_t n_queries, int32_t* cells, int32_t* status,
+                               void* stream) {
+    if (n_prims <= 0 || !points || !radii || !workspace || n_queries < 0 || (n_queries > 0 && (!queries || !cells)))
+        return pf_fail(PF_ERR_ARGS, "pf_locate_cells: bad arguments");
+    if (n_queries == 0) return PF_OK;
+    Locator loc = locator_view(points, radii, n_prims, (char*)workspace);
+    locate_kernel<<<(unsigned)((n_queries + 127) / 128), 128, 0, (cudaStream_t)stream>>>(loc, queries, n_queries,
+                                                                                        cells, status);
+    return pf_check_launch("pf_locate_cells");
+}
+
+extern "C" int pf_seed_start_cells(const float* points, const float* radii, int64_t n_prims, const void* workspace,
+                                   const pf_camera* cam, const float* t_entry, const float* confidence,
+                                   float conf_threshold, int32_t default_start, int32_t* start_cells,
+                                   int32_t* n_seeded, void* stream) {
+    if (n_prims <= 0 || !points || !radii || !workspace || !cam || !t_entry || !confidence || !start_cells ||
+        cam->width < 2 || cam->height < 2 || default_start < 0 || default_start >= n_prims)
+        return pf_fail(PF_ERR_ARGS, "pf_seed_start_cells: bad arguments");
+    Locator loc = locator_view(points, radii, n_prims, (char*)workspace);
+    const int64_t n = (int64_t)cam->width * cam->height;
+    seed_kernel<<<(unsigned)((n + 127) / 128), 128, 0, (cudaStream_t)stream>>>(
+        loc, load_cam(*cam), t_entry, confidence, conf_threshold, default_start, start_cells, n_seeded);
+    return pf_check_launch("pf_seed_start_cells");
 }
 
 extern "C" int pf_morton_workspace_size(int64_t n_prims, size_t* bytes) {

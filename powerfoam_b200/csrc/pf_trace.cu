@@ -94,12 +94,22 @@ PF_D bool trace_pixel(const Cam& cam, int64_t tid, int& pi, int& pj) {
     return pi < cam.H && pj < cam.W;
 }
 
-template <typename A>
+// Labels of the ray-proposal network (no counterpart in the reference): the
+// first cell after whose compositing the transmittance is below `thr`, the t
+// at which the ray enters it and the number of cells walked before it.
+struct LabelOut {
+    float thr;
+    float* t;
+    int32_t* cell;
+    int32_t* step;
+};
+
+template <typename A, bool LABELS = false>
 __global__ void __launch_bounds__(128)
 trace_fwd_kernel(TraceParams P, int64_t nthreads, float* __restrict__ color, float* __restrict__ log_t_out,
                  float* __restrict__ depth, float* __restrict__ normal, int32_t* __restrict__ depth_seg,
                  float* __restrict__ depth_sigma, int32_t* __restrict__ visit_log, int visit_cap,
-                 int32_t* __restrict__ visit_count, int32_t* __restrict__ status) {
+                 int32_t* __restrict__ visit_count, int32_t* __restrict__ status, LabelOut lab = LabelOut{}) {
     int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (tid >= nthreads) return;
     int pi, pj;
@@ -115,6 +125,8 @@ trace_fwd_kernel(TraceParams P, int64_t nthreads, float* __restrict__ color, flo
     int steps = 0, seg = 0, st = PF_OK;
     int32_t dseg = -1;
     float dout = 0.f, dsig = 0.f;
+    float lab_t = -1.0f;
+    int32_t lab_cell = -1, lab_step = -1;
     for (;;) {
         float trans = expf(log_t);
         if (trans < P.thr || prim == kNoCell) break;
@@ -127,6 +139,8 @@ trace_fwd_kernel(TraceParams P, int64_t nthreads, float* __restrict__ color, flo
             break;
         }
         if (visit_log && steps < visit_cap) visit_log[px * visit_cap + steps] = prim;
+        const float cell_entry = pt_near;
+        const int32_t cell = prim;
         steps++;
         const float4 s4 = __ldg(&P.spheres[prim]);
         const v3 center = mk(s4.x, s4.y, s4.z);
@@ -177,8 +191,18 @@ trace_fwd_kernel(TraceParams P, int64_t nthreads, float* __restrict__ color, flo
                 dseg = seg;
                 dsig = sigma;
             }
+            if (LABELS && lab_cell < 0 && expf(log_t) < lab.thr) {
+                lab_t = cell_entry;
+                lab_cell = cell;
+                lab_step = steps - 1;
+            }
             seg++;
         }
+    }
+    if (LABELS) {
+        lab.t[px] = lab_t;
+        lab.cell[px] = lab_cell;
+        lab.step[px] = lab_step;
     }
     color[3 * px] = rgb.x;
     color[3 * px + 1] = rgb.y;
@@ -619,6 +643,26 @@ extern "C" int pf_trace_forward(const pf_trace_inputs* in, float* color, float* 
         trace_fwd_kernel<float><<<grid, 128, 0, st>>>(P, n, color, log_t, depth, normal, depth_seg, depth_sigma,
                                                       visit_log, visit_cap, visit_count, status);
     return pf_check_launch("pf_trace_forward");
+}
+
+static bool fill_trace(const pf_trace_inputs* in, TraceParams& P, const char** why);
+
+extern "C" int pf_trace_labels(const pf_trace_inputs* in, float label_threshold, float* color, float* label_t,
+                               int32_t* label_cell, int32_t* label_step, int32_t* visit_count, int32_t* status,
+                               void* stream) {
+    TraceParams P;
+    const char* why = "";
+    if (!fill_trace(in, P, &why)) return pf_fail(PF_ERR_ARGS, why);
+    if (in->attr_half) return pf_fail(PF_ERR_ARGS, "pf_trace_labels: attributes must be f32");
+    if (!color || !label_t || !label_cell || !label_step)
+        return pf_fail(PF_ERR_ARGS, "pf_trace_labels: missing output");
+    const int64_t tiles = (int64_t)(1 + (P.cam.H - 1) / 8) * (1 + (P.cam.W - 1) / 8);
+    const int64_t n = tiles * 64;
+    const unsigned grid = (unsigned)((n + 127) / 128);
+    LabelOut lab{label_threshold, label_t, label_cell, label_step};
+    trace_fwd_kernel<float, true><<<grid, 128, 0, (cudaStream_t)stream>>>(
+        P, n, color, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, 0, visit_count, status, lab);
+    return pf_check_launch("pf_trace_labels");
 }
 
 static bool fill_trace(const pf_trace_inputs* in, TraceParams& P, const char** why) {

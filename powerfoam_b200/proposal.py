@@ -1,0 +1,233 @@
+"""Ray-proposal network and the proposal-seeded cell walk.
+
+No counterpart in the reference (its tracer, powerfoam/raytrace.py:115-309,
+always walks from the camera's cell).  ``ProposalNet`` holds the network of
+pf_mlp.cu (positional encoding -> 3 x 64 ReLU -> entry distance and
+confidence; BF16 tensor-core GEMMs, FP32 accumulation and FP32 master
+weights with Adam), trains it with the library's own forward/backward/Adam
+kernels on rays labelled by the plain tracer (``make_training_rays``), and
+``SeededTracer`` starts each confident ray's walk at the power cell that
+contains its predicted entry point, falling back to the plain walk below the
+confidence threshold.
+"""
+
+import math
+
+import torch
+
+from . import _lib
+from .raytrace import DEFAULT_MAX_STEPS
+
+LABEL_TRANSMITTANCE = 0.99
+
+
+class ProposalNet:
+    def __init__(self, device, seed=0):
+        self.device = torch.device(device)
+        lib = _lib.load()
+        self.n_params = lib.pf_mlp_param_count()
+        self.image_bytes = lib.pf_mlp_image_bytes()
+        dev = self.device
+        self.weights = init_weights(seed).to(dev)
+        self.m = torch.zeros_like(self.weights)
+        self.v = torch.zeros_like(self.weights)
+        self.grad = torch.zeros_like(self.weights)
+        self.image = torch.zeros(self.image_bytes, dtype=torch.uint8, device=dev)
+        self.step = torch.zeros(1, dtype=torch.int32, device=dev)
+        self.done = torch.zeros(1, dtype=torch.int32, device=dev)
+        self.loss = torch.zeros(2, dtype=torch.float32, device=dev)
+        self.status = torch.zeros(1, dtype=torch.int32, device=dev)
+        self.pack()
+
+    def pack(self):
+        """BF16 image of the current master weights."""
+        _lib.call("pf_mlp_pack", _lib.ptr(self.weights), _lib.ptr(self.image), _lib.stream_ptr())
+
+    def load_weights(self, w):
+        with torch.no_grad():
+            self.weights.copy_(torch.as_tensor(w, dtype=torch.float32))
+        self.pack()
+
+    # ------------------------------------------------------------------
+    def forward(self, rays=None, camera=None):
+        """(t_entry, confidence) for rays (n, 6) = origin, unit direction, or
+        for every pixel ray of `camera` ((H, W) each)."""
+        if (rays is None) == (camera is None):
+            raise ValueError("give rays or a camera")
+        if rays is not None:
+            rays = rays.to(torch.float32).contiguous()
+            n = rays.shape[0]
+            shape = (n,)
+            cam = None
+        else:
+            n = camera.width * camera.height
+            shape = (camera.height, camera.width)
+            cam = _lib.ctypes.byref(camera.to_pf())
+        t = torch.empty(shape, dtype=torch.float32, device=self.device)
+        c = torch.empty(shape, dtype=torch.float32, device=self.device)
+        _lib.call("pf_mlp_forward", _lib.ptr(self.image), _lib.ptr(rays), n, cam, _lib.ptr(t), _lib.ptr(c),
+                  _lib.ptr(self.status), _lib.stream_ptr())
+        return t, c
+
+    def train_step(self, rays8, batch, seed=0, overshoot_weight=10.0, margin=0.02, lr=1e-3, record_loss=True):
+        """One Adam step on a minibatch drawn from rays8 (n, 8) (no host sync)."""
+        st = _lib.stream_ptr()
+        if record_loss:
+            self.loss.zero_()
+        _lib.call("pf_mlp_train_step", _lib.ptr(self.image), _lib.ptr(rays8), rays8.shape[0], int(batch),
+                  _lib.ptr(self.step), int(seed) & 0xFFFFFFFF, float(overshoot_weight), float(margin),
+                  _lib.ptr(self.grad), _lib.ptr(self.loss) if record_loss else None, _lib.ptr(self.status), st)
+        _lib.call("pf_mlp_adam", _lib.ptr(self.weights), _lib.ptr(self.m), _lib.ptr(self.v), _lib.ptr(self.grad),
+                  _lib.ptr(self.image), _lib.ptr(self.step), _lib.ptr(self.done), float(lr), 0.9, 0.999, 1e-8, st)
+
+    def train(self, rays8, steps=5000, batch=65536, lr=1e-3, seed=0, overshoot_weight=10.0, margin=0.02,
+              graph_steps=50, log=None):
+        """Train for `steps` Adam steps; chunks of graph_steps steps are
+        replayed from one CUDA graph.  Returns the per-chunk mean losses
+        (entry-distance term, confidence term) of each chunk's last step."""
+        rays8 = rays8.to(torch.float32).contiguous()
+        history = []
+        kw = dict(seed=seed, overshoot_weight=overshoot_weight, margin=margin, lr=lr)
+
+        def chunk(n):
+            for i in range(n):
+                self.train_step(rays8, batch, record_loss=(i == n - 1), **kw)
+
+        done = 0
+        g = None
+        if graph_steps and steps >= 2 * graph_steps:
+            s = torch.cuda.Stream(device=self.device)
+            s.wait_stream(torch.cuda.current_stream(self.device))
+            with torch.cuda.stream(s):
+                chunk(graph_steps)  # warm-up (kernel attributes) outside the graph
+            torch.cuda.current_stream(self.device).wait_stream(s)
+            done += graph_steps
+            history.append([x / batch for x in self.loss.tolist()])
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(g):
+                chunk(graph_steps)
+        while done < steps:
+            n = min(graph_steps or steps, steps - done)
+            if g is not None and n == graph_steps:
+                g.replay()
+            else:
+                chunk(n)
+            done += n
+            history.append([x / batch for x in self.loss.tolist()])
+            if log:
+                log(f"proposal step {done}: loss_t {history[-1][0]:.5f} loss_conf {history[-1][1]:.4f}")
+        self.check()
+        return history
+
+    def check(self):
+        s = int(self.status.item())
+        if s != _lib.PF_OK:
+            raise _lib.PfError(s, "proposal network kernel reported an error")
+
+
+def init_weights(seed=0):
+    """Uniform fan-in initialisation of the data columns (CPU, seeded); the
+    bias and pad columns and the unused output rows start at zero."""
+    g = torch.Generator().manual_seed(seed)
+    blocks = []
+    for li, out in enumerate((64, 64, 64, 16)):
+        fan_in = 78 if li == 0 else 64
+        bound = math.sqrt(6.0 / fan_in) if li < 3 else math.sqrt(1.0 / fan_in)
+        w = torch.zeros(out, 80)
+        rows = out if li < 3 else 2
+        w[:rows, :fan_in] = (torch.rand(rows, fan_in, generator=g) * 2 - 1) * bound
+        blocks.append(w.reshape(-1))
+    return torch.cat(blocks).float()
+
+
+# ----------------------------------------------------------------------------
+def trace_labels(tracer, camera, start, scene_args, label_transmittance=LABEL_TRANSMITTANCE,
+                 max_steps=DEFAULT_MAX_STEPS):
+    """pf_trace_labels over every pixel ray of `camera`: dict of colour, label
+    t / cell / step and the number of cells walked."""
+    args = tracer._prep(*scene_args)
+    inp = tracer._inputs(camera, start, *args, 1e-3, max_steps, 0.5)
+    H, W = camera.height, camera.width
+    dev = tracer.device
+    out = dict(color=torch.empty((H, W, 3), dtype=torch.float32, device=dev),
+               label_t=torch.empty((H, W), dtype=torch.float32, device=dev),
+               label_cell=torch.empty((H, W), dtype=torch.int32, device=dev),
+               label_step=torch.empty((H, W), dtype=torch.int32, device=dev),
+               visit_count=torch.empty((H, W), dtype=torch.int32, device=dev))
+    status = torch.zeros(1, dtype=torch.int32, device=dev)
+    _lib.call("pf_trace_labels", _lib.ctypes.byref(inp), float(label_transmittance), _lib.ptr(out["color"]),
+              _lib.ptr(out["label_t"]), _lib.ptr(out["label_cell"]), _lib.ptr(out["label_step"]),
+              _lib.ptr(out["visit_count"]), _lib.ptr(status), _lib.stream_ptr())
+    out["status"] = status
+    return out
+
+
+def camera_rays(camera):
+    """(H*W, 6) origin and unit direction of every pixel ray (row-major)."""
+    H, W = camera.height, camera.width
+    d = camera.ray_directions().float()
+    o = camera.eye.float()[None, None, :].expand(H, W, 3)
+    return torch.cat([o, d], dim=-1).reshape(-1, 6)
+
+
+def make_training_rays(tracer, cameras, scene_args, start_cells, label_transmittance=LABEL_TRANSMITTANCE):
+    """(n, 8) training rays (origin, direction, label t or -1, 0) from the
+    plain walk of every pixel of every camera."""
+    parts = []
+    for cam, start in zip(cameras, start_cells):
+        lab = trace_labels(tracer, cam, start, scene_args, label_transmittance)
+        r = camera_rays(cam)
+        t = lab["label_t"].reshape(-1, 1)
+        parts.append(torch.cat([r, t, torch.zeros_like(t)], dim=-1))
+    return torch.cat(parts, 0).contiguous()
+
+
+class CellLocator:
+    """Power-cell point location over fixed primitives (pf_locator_build)."""
+
+    def __init__(self, points, radii):
+        self.points = points.float().contiguous()
+        self.radii = radii.float().contiguous()
+        n = self.points.shape[0]
+        nbytes = _lib.ctypes.c_size_t(0)
+        _lib.call("pf_locator_workspace_size", n, _lib.ctypes.byref(nbytes))
+        self.ws = torch.empty(max(nbytes.value, 256), dtype=torch.uint8, device=self.points.device)
+        _lib.call("pf_locator_build", _lib.ptr(self.points), _lib.ptr(self.radii), n, _lib.ptr(self.ws),
+                  self.ws.numel(), _lib.stream_ptr())
+
+    def locate(self, queries, status=None):
+        q = queries.float().contiguous()
+        out = torch.empty(q.shape[0], dtype=torch.int32, device=q.device)
+        st = status if status is not None else torch.zeros(1, dtype=torch.int32, device=q.device)
+        _lib.call("pf_locate_cells", _lib.ptr(self.points), _lib.ptr(self.radii), self.points.shape[0],
+                  _lib.ptr(self.ws), _lib.ptr(q), q.shape[0], _lib.ptr(out), _lib.ptr(st), _lib.stream_ptr())
+        return out
+
+    def seed(self, camera, t_entry, confidence, conf_threshold, default_start, n_seeded=None):
+        H, W = camera.height, camera.width
+        start = torch.empty((H, W), dtype=torch.int32, device=self.points.device)
+        _lib.call("pf_seed_start_cells", _lib.ptr(self.points), _lib.ptr(self.radii), self.points.shape[0],
+                  _lib.ptr(self.ws), _lib.ctypes.byref(camera.to_pf()), _lib.ptr(t_entry), _lib.ptr(confidence),
+                  float(conf_threshold), int(default_start), _lib.ptr(start), _lib.ptr(n_seeded), _lib.stream_ptr())
+        return start
+
+
+class SeededTracer:
+    """Proposal-seeded cell walk: network forward over the pixel rays, start
+    cells from the locator where the confidence reaches the threshold, then
+    the tracer's walk from those cells (plain start cell elsewhere)."""
+
+    def __init__(self, tracer, net, points, radii, conf_threshold=0.9):
+        self.tracer = tracer
+        self.net = net
+        self.conf_threshold = conf_threshold
+        self.locator = CellLocator(points, radii)
+        self.n_seeded = torch.zeros(1, dtype=torch.int32, device=tracer.device)
+
+    def start_cells(self, camera, default_start):
+        t, c = self.net.forward(camera=camera)
+        return self.locator.seed(camera, t, c, self.conf_threshold, default_start, self.n_seeded)
+
+    def render(self, camera, default_start, scene_args, **kw):
+        start = self.start_cells(camera, default_start)
+        return self.tracer.trace(camera, start, *scene_args, check_status=False, **kw)
