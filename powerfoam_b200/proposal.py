@@ -37,6 +37,7 @@ class ProposalNet:
         self.done = torch.zeros(1, dtype=torch.int32, device=dev)
         self.loss = torch.zeros(2, dtype=torch.float32, device=dev)
         self.status = torch.zeros(1, dtype=torch.int32, device=dev)
+        self.margin = 0.02  # seed back-off the confidence head was trained for
         self.pack()
 
     def pack(self):
@@ -86,6 +87,7 @@ class ProposalNet:
         replayed from one CUDA graph.  Returns the per-chunk mean losses
         (entry-distance term, confidence term) of each chunk's last step."""
         rays8 = rays8.to(torch.float32).contiguous()
+        self.margin = float(margin)
         history = []
         kw = dict(seed=seed, overshoot_weight=overshoot_weight, margin=margin, lr=lr)
 
@@ -118,6 +120,19 @@ class ProposalNet:
                 log(f"proposal step {done}: loss_t {history[-1][0]:.5f} loss_conf {history[-1][1]:.4f}")
         self.check()
         return history
+
+    def calibrate(self, rays8, max_unsafe=0, floor=0.9):
+        """Confidence threshold from held-out labelled rays (n, 8): the plain
+        walk judges each seed, and the threshold sits just above the
+        confidence of the (max_unsafe + 1)-th most confident seed that would
+        have started past its first significant cell (never below `floor`)."""
+        rays8 = rays8.to(torch.float32).contiguous()
+        t, c = self.forward(rays=rays8[:, :6].contiguous())
+        lab = rays8[:, 6]
+        unsafe = (lab >= 0) & (t - self.margin > lab)
+        cu = torch.sort(c[unsafe], descending=True).values
+        thr = float(cu[max_unsafe]) if cu.numel() > max_unsafe else 0.0
+        return max(floor, math.nextafter(thr, 2.0))
 
     def check(self):
         s = int(self.status.item())
@@ -225,7 +240,10 @@ class SeededTracer:
         self.n_seeded = torch.zeros(1, dtype=torch.int32, device=tracer.device)
 
     def start_cells(self, camera, default_start):
+        """The confidence predicts that t - margin lies before the first
+        significant cell, so the seed point is backed off by the margin."""
         t, c = self.net.forward(camera=camera)
+        t.sub_(self.net.margin)
         return self.locator.seed(camera, t, c, self.conf_threshold, default_start, self.n_seeded)
 
     def render(self, camera, default_start, scene_args, **kw):
