@@ -37,6 +37,8 @@ sys.path.insert(0, ROOT)
 import numpy as np  # noqa: E402
 import torch  # noqa: E402
 
+from powerfoam_b200.multiview import GradReducer, allreduce_, max_over_ranks, shard_views  # noqa: E402
+
 METRIC = "fwd+bwd ms/iter, FPS @1M prims 1080p; proposal vs plain trace @≥50dB PSNR"
 UNIT = "frames/s (fwd+bwd iterations/s)"
 WORKLOAD = "raster1m"
@@ -171,9 +173,7 @@ def make_step(R, scene, cam, adj, adj_off, target_dev, world):
         loss = ((out[0] - t) ** 2).sum()
         loss.backward()
         if world > 1:
-            grads = [params[k].grad.reshape(-1) for k in names] + [rgb.grad.reshape(-1)]
-            flat = torch.cat(grads)
-            torch.distributed.all_reduce(flat)
+            allreduce_([params[k].grad for k in names] + [rgb.grad])
         return loss
 
     return step, params
@@ -290,7 +290,7 @@ def batch_main(args, world, rank, local, dev):
     scene = synthetic.make_scene(cfg["n"], seed=cfg["seed"], mixture=cfg["mixture"], sigma=cfg["sigma"],
                                  r_range=cfg["r_range"], device=dev)
     cams_all = synthetic.batch_cameras(cfg["views"], cfg["seed"], cfg["vfov"], device=dev)
-    mine = list(range(rank, len(cams_all), world))
+    mine = shard_views(len(cams_all), rank, world)
     cams = [cams_all[v] for v in mine]
     adj, adj_off = CechBuilder(dev)(scene["points"], scene["radii"])
     g = torch.Generator().manual_seed(300)
@@ -312,16 +312,12 @@ def batch_main(args, world, rank, local, dev):
                                log=(lambda m: print(m, file=sys.stderr, flush=True)) if rank == 0 else None)
     tune_s = time.perf_counter() - t0
     step.capture()
-    flat = None
-    if world > 1:
-        names = sorted(step.grads)
-        flat = torch.empty(sum(step.grads[k].numel() for k in names) + step.grad_sh.numel(), device=dev)
+    reducer = GradReducer([step.grads[k] for k in sorted(step.grads)] + [step.grad_sh]) if world > 1 else None
 
     def run():
         loss = step.run()
-        if world > 1:
-            torch.cat([step.grads[k].reshape(-1) for k in sorted(step.grads)] + [step.grad_sh.reshape(-1)], out=flat)
-            torch.distributed.all_reduce(flat)
+        if reducer is not None:
+            reducer()
         return loss
 
     def barrier():
@@ -359,9 +355,7 @@ def batch_main(args, world, rank, local, dev):
     barrier()
     e2e_ms = e0.elapsed_time(e1) / args.steps
     if world > 1:
-        t = torch.tensor([ms, e2e_ms], device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms, e2e_ms = (float(x) for x in t.tolist())
+        ms, e2e_ms = max_over_ranks(ms, dev), max_over_ranks(e2e_ms, dev)
     # live kernel time of the persistent launch (eager runs, events around it)
     step.kernel_events = []
     for _ in range(3):
@@ -501,9 +495,7 @@ def main():
     clk = clocks.stop()
     ms = start.elapsed_time(end) / args.steps
     if world > 1:
-        t = torch.tensor([ms], device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms = float(t.item())
+        ms = max_over_ranks(ms, dev)
     value = world * 1000.0 / ms
     fwd_ms = statistics.mean(a.elapsed_time(b) for a, b in events["pf_raster_forward"])
     bwd_ms = statistics.mean(a.elapsed_time(b) for a, b in events["pf_raster_backward"])
@@ -524,9 +516,7 @@ def main():
     barrier()
     e2e_ms = e0.elapsed_time(e1) / args.steps
     if world > 1:
-        t = torch.tensor([e2e_ms], device=dev)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+        e2e_ms = max_over_ranks(e2e_ms, dev)
 
     # statistics of one step for the roofline (outside the timed regions)
     R.collect_stats = True
