@@ -23,6 +23,7 @@ of a random sample of tiles), scaled to frames/s.
 """
 
 import argparse
+import math
 import json
 import os
 import statistics
@@ -53,10 +54,13 @@ def parse():
     p.add_argument("--tile", type=int, default=8)
     p.add_argument("--workload", default=WORKLOAD, help="raster1m (the measured configuration), raster256k "
                    "(a quarter-size case with the same density per pixel, for profiling), batch3m (32 views of "
-                   "a 3.1M-primitive scene in one graph-captured persistent step) or batch256k (its small case)")
+                   "a 3.1M-primitive scene in one graph-captured persistent step), batch256k (its small case) or "
+                   "proposal (proposal-seeded vs plain cell walk)")
     p.add_argument("--cpu-sample-tiles", type=int, default=0, help="tiles composited by the CPU baseline")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-autotune", action="store_true", help="batch workloads: use --tile, chunk 1")
+    p.add_argument("--proposal-prims", type=int, default=0,
+                   help="proposal workload: primitive count (default 6,291,456; radii scale with the spacing)")
     return p.parse_args()
 
 
@@ -434,6 +438,97 @@ def batch_main(args, world, rank, local, dev):
         torch.distributed.destroy_process_group()
 
 
+def proposal_main(args, dev):
+    """Proposal-seeded vs plain cell walk (one GPU): the 64-cluster scene of
+    the tracer configuration (σ 0.1, r log-uniform in [0.001, 0.01], 10 %
+    background) with its power-diagram adjacency, the network trained for 5000
+    Adam steps of 65,536 rays on 2M rays labelled by the plain walk (2048
+    random 32x32 views, first cell with transmittance < 0.999), its confidence
+    gate calibrated on 256 held-out views, then one 2048x1536 frame from a
+    held-out view.  Reported: plain and seeded frame times (the seeded time
+    includes the network forward and the cell location), PSNR of the seeded
+    frame against the plain one, and the same for seeding from the plain
+    walk's own labels (the bound a perfect proposal reaches)."""
+    from powerfoam_b200 import synthetic
+    from powerfoam_b200.adjacency import build_power_adjacency, power_adjacency_diff, start_cell
+    from powerfoam_b200.proposal import ProposalNet, SeededTracer, make_training_rays, trace_labels
+    from powerfoam_b200.raytrace import RayTracer
+
+    cfg = dict(synthetic.CONFIGS["trace6m"])
+    if args.proposal_prims:
+        s = (cfg["n"] / args.proposal_prims) ** (1 / 3)
+        cfg["n"] = args.proposal_prims
+        cfg["r_range"] = tuple(r * s for r in cfg["r_range"])
+    log = lambda m: print(m, file=sys.stderr, flush=True)  # noqa: E731
+    sc = synthetic.make_scene(cfg["n"], seed=cfg["seed"], mixture=cfg["mixture"], sigma=cfg["sigma"],
+                              r_range=cfg["r_range"], device=dev)
+    t0 = time.perf_counter()
+    adj, off = build_power_adjacency(sc["points"], sc["radii"])
+    log(f"power adjacency {time.perf_counter() - t0:.1f} s, {adj.shape[0]} edges")
+    pm = power_adjacency_diff(sc["points"], sc["radii"], adj, off)
+    ev = synthetic.orbit_camera(4242, cfg["width"], cfg["height"], cfg["vfov"], device=dev)
+    rgb = synthetic.texel_rgb(sc, ev)
+    scene_args = (sc["points"], sc["radii"], sc["density"], sc["normals"], sc["texel_sites"], rgb,
+                  sc["texel_height"], adj, off, pm)
+    tr = RayTracer(Args(), dev)
+
+    def labelled(seed0, k):
+        cams = [synthetic.orbit_camera(seed0 + i, 32, 32, cfg["vfov"], device=dev) for i in range(k)]
+        return make_training_rays(tr, cams, scene_args, [start_cell(sc["points"], sc["radii"], c.eye) for c in cams],
+                                  label_transmittance=0.999)
+
+    t0 = time.perf_counter()
+    rays8, val = labelled(10000, 2048), labelled(50000, 256)
+    label_s = time.perf_counter() - t0
+    net = ProposalNet(dev, seed=1)
+    t0 = time.perf_counter()
+    hist = net.train(rays8, steps=5000, batch=65536, lr=1e-3, overshoot_weight=100.0, margin=0.1, graph_steps=100)
+    torch.cuda.synchronize()
+    train_s = time.perf_counter() - t0
+    seeded = SeededTracer(tr, net, sc["points"], sc["radii"], conf_threshold=net.calibrate(val))
+    st = start_cell(sc["points"], sc["radii"], ev.eye)
+
+    def timed(fn):
+        for _ in range(max(args.warmup, 3)):
+            fn()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(args.steps):
+            r = fn()
+        b.record()
+        torch.cuda.synchronize()
+        return r, a.elapsed_time(b) / args.steps
+
+    def psnr(a, b):
+        mse = float(((a.double() - b.double()) ** 2).mean())
+        return 10 * math.log10(1.0 / max(mse, 1e-20))
+
+    plain, plain_ms = timed(lambda: tr.trace(ev, st, *scene_args, check_status=False))
+    seeded.n_seeded.zero_()
+    seed_r, seed_ms = timed(lambda: seeded.render(ev, st, scene_args))
+    n_seeded = int(seeded.n_seeded.item()) // (args.steps + max(args.warmup, 3))
+    lab = trace_labels(tr, ev, st, scene_args, label_transmittance=0.999)
+    hit = lab["label_cell"] >= 0
+    one = torch.ones_like(lab["label_t"])
+    t_lab = torch.where(hit, lab["label_t"] - net.margin, -one).contiguous()
+    conf_lab = torch.where(hit, one, 0 * one).contiguous()
+    ideal_r, ideal_ms = timed(lambda: tr.trace(ev, seeded.locator.seed(ev, t_lab, conf_lab, 0.5, st), *scene_args,
+                                                check_status=False))
+    H, W = cfg["height"], cfg["width"]
+    line = dict(metric=METRIC, value=plain_ms / seed_ms, unit="x (plain / proposal-seeded frame time)", n_gpus=1,
+                steps=args.steps, warmup=max(args.warmup, 3), ms_per_step=seed_ms, higher_is_better=True,
+                scaling="weak", vs_baseline=None, dtype="f32 walk, bf16 network", data="synthetic",
+                config=dict(workload="proposal", prims=cfg["n"], width=W, height=H, plain_ms=plain_ms,
+                            seeded_ms=seed_ms, psnr_db=psnr(seed_r.color, plain.color), seeded_rays=n_seeded,
+                            rays=H * W, threshold=seeded.conf_threshold, cells_plain=int(plain.visit_count.sum()),
+                            cells_seeded=int(seed_r.visit_count.sum()), label_seed_ms=ideal_ms,
+                            label_seed_psnr_db=psnr(ideal_r.color, plain.color),
+                            label_seed_cells=int(ideal_r.visit_count.sum()), label_s=label_s, train_s=train_s,
+                            train_rays=int(rays8.shape[0]), loss_first=hist[0], loss_last=hist[-1]))
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -448,6 +543,9 @@ def main():
         import datetime
 
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
+    if args.workload == "proposal":
+        proposal_main(args, dev)
+        return
     if args.workload.startswith("batch"):
         batch_main(args, world, rank, local, dev)
         return
