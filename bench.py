@@ -109,6 +109,12 @@ class ClockSampler:
             self.t.start()
         except Exception:  # noqa: BLE001
             self.proc = None
+            return
+        # nvidia-smi's start-up (driver queries) must not fall inside the timed
+        # region: wait for its first two samples (bounded)
+        t0 = time.time()
+        while len(self.lines) < 2 and time.time() - t0 < 10.0 and self.proc.poll() is None:
+            time.sleep(0.05)
 
     def _read(self):
         for line in self.proc.stdout:

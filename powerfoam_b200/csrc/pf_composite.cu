@@ -49,7 +49,7 @@ __global__ void __launch_bounds__(Layout<TW>::THREADS) raster_fwd_kernel(RasterP
 }
 
 template <int TW>
-__global__ void __launch_bounds__(Layout<TW>::THREADS)
+__global__ void __launch_bounds__(Layout<TW>::THREADS, Layout<TW>::BWD_MIN_BLOCKS)
 raster_bwd_kernel(RasterParams P, BwdIn in, GradOut go) {
     constexpr int G = Layout<TW>::G;
     __shared__ WarpStage stage[G];

@@ -12,7 +12,7 @@ namespace pf {
 
 
 constexpr int kAccRows = 64;
-constexpr int kFaceSlots = 64;
+constexpr int kFaceSlots = 16;
 
 // Group layout per tile width: TW = 8 and 16 use one pixel per lane (G = 2
 // and 8 warps per tile), TW = 32 two pixels per lane (G = 16).
@@ -21,6 +21,8 @@ struct Layout {
     static constexpr int PPL = TW == 32 ? 2 : 1;
     static constexpr int G = TW * TW / (32 * PPL);
     static constexpr int THREADS = 32 * G;
+    // resident blocks per SM the adjoint is compiled for (register budget)
+    static constexpr int BWD_MIN_BLOCKS = TW == 8 ? 10 : 1;
 };
 
 // Early termination across the warps of a tile (forward).  The reference
@@ -354,7 +356,6 @@ PF_D void swap_pix(BwdPix& a, BwdPix& b) {
 
 struct BwdStage {
     float acc[kAccRows][32];     // per-lane gradient columns of the current primitive
-    float wc[2 * kMaxSites][32]; // per-lane texel weights of the recomputed forward
     float4 face_acc[kFaceSlots]; // neighbour sphere gradients per neighbour slot
     float4 nbr_sph[kFaceSlots];  // exact neighbour spheres (face adjoint)
     int32_t nbr_id[kFaceSlots];
@@ -448,57 +449,6 @@ PF_D void ray_plane_bwd_d(v3 eye, v3 dir, v3 p, v3 n, float h, v3& dtdp, v3& dtd
     dtdn = i1 * (p - eye) - ((dot(p - eye, n) + h) * i2) * dir;
 }
 
-// texture.py:10-72 (as plane_fwd_smem) for the adjoint: also stores the 2 x S
-// texel weights in this lane's column of bs.wc.  plane_intersection_bwd
-// evaluates the very same weights (same query points, same expressions), so
-// reading them back is exact.
-PF_D PlaneRes plane_fwd_cache(v3 o, v3 d, float t_near, v3 po, v3 pn, float radius, const WarpStage& ws, int S,
-                              BwdStage& bs, int lane) {
-    PlaneRes r;
-    float _dp;
-    float _t_surf = ray_plane(o, d, po, pn, 0.0f, _dp);
-    float _tq = _dp >= 0.0f ? t_near : fmax_t(t_near, _t_surf);
-    v3 _pt = o + _tq * d;
-    float rr = radius * radius;
-    float hsum = 0.f, _wsum = 0.f;
-#pragma unroll 1
-    for (int i = 0; i < S; i++) {
-        v3 df = _pt - mk(ws.ts[3 * i], ws.ts[3 * i + 1], ws.ts[3 * i + 2]);
-        float dist_sq = dot(df, df) / rr;
-        float w = expf(-kTemp * dist_sq);
-        bs.wc[kMaxSites + i][lane] = w;
-        hsum += w * ws.th[i];
-        _wsum += w;
-    }
-    _wsum = fmax_t(_wsum, 1e-20f);
-    float height = hsum / _wsum;
-    float dp;
-    float t_surf = ray_plane(o, d, po, pn, height, dp);
-    float tq = dp >= 0.0f ? t_near : fmax_t(t_near, t_surf);
-    v3 pt = o + tq * d;
-    v3 rgb_sum = mk(0.f, 0.f, 0.f);
-    float wsum = 0.f;
-#pragma unroll 1
-    for (int i = 0; i < S; i++) {
-        v3 df = pt - mk(ws.ts[3 * i], ws.ts[3 * i + 1], ws.ts[3 * i + 2]);
-        float dist_sq = dot(df, df) / rr;
-        float w = expf(-kTemp * dist_sq);
-        bs.wc[i][lane] = w;
-        rgb_sum = rgb_sum + w * mk(ws.tr[3 * i], ws.tr[3 * i + 1], ws.tr[3 * i + 2]);
-        wsum += w;
-    }
-    wsum = fmax_t(wsum, 1e-20f);
-    r._t_surf = _t_surf;
-    r._dp = _dp;
-    r.height = height;
-    r._wsum = _wsum;
-    r.t_surf = t_surf;
-    r.dp = dp;
-    r.rgb = rgb_sum / wsum;
-    r.wsum = wsum;
-    return r;
-}
-
 // texture.py:74-186, accumulating into this lane's column of bs.acc
 PF_D void plane_bwd_acc(v3 o, v3 d, float _t_near, v3 po, v3 pn, float radius, const WarpStage& ws, int S,
                         const PlaneRes& pr, v3 dLdrgb_in, float dLdt_surf_in, BwdStage& bs, int lane, v3& dLdpo_out,
@@ -517,7 +467,7 @@ PF_D void plane_bwd_acc(v3 o, v3 d, float _t_near, v3 po, v3 pn, float radius, c
     for (int i = 0; i < S; i++) {
         v3 site = mk(ws.ts[3 * i], ws.ts[3 * i + 1], ws.ts[3 * i + 2]);
         v3 df = pt - site;
-        float w = bs.wc[i][lane];  // texture.py:116-117, computed by plane_fwd_cache
+        float w = expf(-kTemp * (dot(df, df) / rr));  // texture.py:116-117 (as the forward)
         if (!(w / weight_sum < 1e-3f)) {
             v3 dwds = ((2.0f * kTemp * w) * inv_rr) * df;
             v3 rgb_grad = w * rgb_scale;
@@ -553,7 +503,7 @@ PF_D void plane_bwd_acc(v3 o, v3 d, float _t_near, v3 po, v3 pn, float radius, c
         for (int i = 0; i < S; i++) {
             v3 site = mk(ws.ts[3 * i], ws.ts[3 * i + 1], ws.ts[3 * i + 2]);
             v3 df = _pt - site;
-            float w = bs.wc[kMaxSites + i][lane];  // texture.py:156-157
+            float w = expf(-kTemp * (dot(df, df) / rr));  // texture.py:156-157
             if (!(w / weight_sum < 1e-3f)) {
                 v3 dwds = ((2.0f * kTemp * w) * inv_rr) * df;
                 bs.acc[56 + i][lane] += w * dLdheight_in * inv__ws;
@@ -704,7 +654,7 @@ PF_D void bwd_tile(const RasterParams& P, const BwdIn& in, const GradOut& go, in
                     int t_near_id = x.tn_id, t_far_id = x.tf_id;
                     const float _t_near = t_near;
                     const int _t_near_id = t_near_id, _t_far_id = t_far_id;
-                    PlaneRes pr = plane_fwd_cache(o, d, t_near, center, pn, radius, ws, P.S, bs, lane);
+                    PlaneRes pr = plane_fwd_smem(o, d, t_near, center, pn, radius, ws, P.S);
                     t_far_id = (pr.dp >= 0.0f && pr.t_surf < t_far) ? n_adj : t_far_id;
                     t_far = pr.dp >= 0.0f ? fmin_t(pr.t_surf, t_far) : t_far;
                     t_near_id = (pr.dp < 0.0f && pr.t_surf > t_near) ? n_adj : t_near_id;
