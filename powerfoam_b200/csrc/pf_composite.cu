@@ -39,14 +39,25 @@ __global__ void __launch_bounds__(Layout<TW>::THREADS) raster_fwd_kernel(RasterP
     constexpr int G = Layout<TW>::G;
     __shared__ WarpStage stage[G];
     __shared__ StopState ss;
+    extern __shared__ float4 fwd_dyn[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     int64_t static_next = (int64_t)blockIdx.x;
     for (;;) {
         int64_t tile = next_tile<G>(P, static_next, lane, &ss);
         if (tile < 0) break;
-        fwd_tile<G, Layout<TW>::PPL>(P, out, tile, warp, lane, stage[warp], ss);
+        if constexpr (Layout<TW>::PPL == 1)
+            fwd_tile_c<G>(P, out, tile, warp, lane, stage[warp], reinterpret_cast<FwdCStage*>(fwd_dyn)[warp], ss);
+        else
+            fwd_tile<G, Layout<TW>::PPL>(P, out, tile, warp, lane, stage[warp], ss);
     }
 }
+
+// dynamic shared memory of the forward: the pair-compaction stage per warp
+template <int TW>
+constexpr size_t fwd_dyn_bytes() {
+    return Layout<TW>::PPL == 1 ? sizeof(FwdCStage) * Layout<TW>::G : 0;
+}
+
 
 template <int TW>
 __global__ void __launch_bounds__(Layout<TW>::THREADS, Layout<TW>::BWD_MIN_BLOCKS)
@@ -89,6 +100,19 @@ static unsigned composite_grid(const RasterParams& P, K kernel, size_t dyn_smem)
     return (unsigned)std::max<int64_t>(1, std::min<int64_t>(groups, resident));
 }
 
+template <int TW>
+static int launch_fwd(const RasterParams& P, const FwdOut& out, cudaStream_t st) {
+    const size_t dyn = fwd_dyn_bytes<TW>();
+    if (dyn > 0) {
+        cudaError_t e = cudaFuncSetAttribute(raster_fwd_kernel<TW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)dyn);
+        if (e != cudaSuccess) return pf_fail(PF_ERR_CUDA, cudaGetErrorString(e));
+    }
+    unsigned grid = composite_grid<TW>(P, raster_fwd_kernel<TW>, dyn);
+    raster_fwd_kernel<TW><<<grid, Layout<TW>::THREADS, dyn, st>>>(P, out);
+    return PF_OK;
+}
+
 }  // namespace pf
 
 using namespace pf;
@@ -115,16 +139,11 @@ extern "C" int pf_raster_forward(const pf_raster_inputs* in, int32_t return_poin
     if (P.queue) cudaMemsetAsync(P.queue, 0, 2 * sizeof(int), st);
     FwdOut out{color, log_t, normal_distance, normal, quantile_depths, err, contrib, point_err, early_stop,
                tile_contrib_pairs, return_point_err, P.queue ? P.queue + 1 : nullptr};
-    if (P.TW == 8) {
-        unsigned grid = composite_grid<8>(P, raster_fwd_kernel<8>, 0);
-        raster_fwd_kernel<8><<<grid, Layout<8>::THREADS, 0, st>>>(P, out);
-    } else if (P.TW == 16) {
-        unsigned grid = composite_grid<16>(P, raster_fwd_kernel<16>, 0);
-        raster_fwd_kernel<16><<<grid, Layout<16>::THREADS, 0, st>>>(P, out);
-    } else {
-        unsigned grid = composite_grid<32>(P, raster_fwd_kernel<32>, 0);
-        raster_fwd_kernel<32><<<grid, Layout<32>::THREADS, 0, st>>>(P, out);
-    }
+    int rc;
+    if (P.TW == 8) rc = launch_fwd<8>(P, out, st);
+    else if (P.TW == 16) rc = launch_fwd<16>(P, out, st);
+    else rc = launch_fwd<32>(P, out, st);
+    if (rc != PF_OK) return rc;
     return pf_check_launch("pf_raster_forward");
 }
 

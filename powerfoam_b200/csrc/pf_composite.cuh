@@ -211,7 +211,10 @@ PF_D void fwd_tile(const RasterParams& P, const FwdOut& out, int64_t tile, int w
         stage_prims(ws, P, start, k0, total, lane);
         const int kn = min(32, total - k0);
         for (int kk = 0; kk < kn; kk++) {
-            bool below = (a.g.oob ? false : a.trans < P.thr) && (b.g.oob ? false : b.trans < P.thr);
+            // an out-of-image pixel blocks the stop (rasterize.py:984-990: its
+            // transmittance stays 1); a lane without a second pixel does not
+            const bool below = (a.g.oob ? false : a.trans < P.thr) &&
+                               (PPL == 1 ? true : (b.g.oob ? false : b.trans < P.thr));
             if (stop_vote<G>(ss, wig, lane, k0 + kk, below, out.status)) {
                 es = k0 + kk;
                 stopped = true;
@@ -330,6 +333,294 @@ PF_D void fwd_tile(const RasterParams& P, const FwdOut& out, int64_t tile, int w
             }
         }
         if (PPL == 2) swap_pix(a, b);
+    }
+    if (lane == 0 && wig == 0) out.early_stop[tile] = es;
+    if (out.tile_contrib_pairs && lane == 0) atomicAdd(&out.tile_contrib_pairs[tile], n_contrib_pairs);
+}
+
+// ---------------------------------------------------------------------------
+// Forward with (primitive, pixel) hit pairs packed onto the lanes (one pixel
+// per lane layouts).  Per batch of 32 staged primitives every lane tests its
+// pixel against all of them (hit masks by ballot); the pairs that hit, in
+// primitive order, are dealt 32 per round to the lanes, which clip the segment
+// by the primitive's faces and evaluate the texture (the costly part, now on
+// every lane instead of the ~45 % whose pixel a primitive covers) and leave
+// (dt, rgb, t_near) in a two-round ring; after each round every lane
+// composites, in primitive order, the pairs of its own pixel for the
+// primitives completed so far, with the early-termination vote before each
+// primitive exactly as the one-primitive-at-a-time loop.  Each pair is
+// evaluated with the same functions on the same operands, so the images are
+// bit-identical to fwd_tile's.  Face planes of a sub-batch of primitives
+// (<= kFaceCap faces) are staged once; a primitive with more faces than that
+// builds them from global memory per pair.
+constexpr int kFaceCap = 256;
+
+struct FwdCStage {
+    float4 face[kFaceCap];
+    float4 rec[64];     // per pair: dt, rgb
+    float rec_tn[64];   // per pair: segment start (quantile depths)
+    float4 dir[32];     // ray direction of each lane's pixel
+    uint32_t mask[32];  // hit mask of each staged primitive
+    int pair_off[33];
+    int face_off[33];
+};
+
+PF_D int warp_incl_scan(int v, int lane) {
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        int y = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= o) v += y;
+    }
+    return v;
+}
+
+// position of the n-th (0-based) set bit of m (n < popc(m))
+PF_D int nth_set_bit(uint32_t m, int n) {
+    int pos = 0;
+#pragma unroll
+    for (int w = 16; w > 0; w >>= 1) {
+        const uint32_t low = m & ((1u << w) - 1u);
+        const int c = __popc(low);
+        if (n >= c) {
+            n -= c;
+            m >>= w;
+            pos += w;
+        } else {
+            m = low;
+        }
+    }
+    return pos;
+}
+
+// largest j in [0, n) with off[j] <= x (off non-decreasing, off[0] = 0)
+PF_D int seg_search(const int* off, int n, int x) {
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (off[mid] <= x) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+template <int G>
+PF_D void fwd_tile_c(const RasterParams& P, const FwdOut& out, int64_t tile, int wig, int lane, WarpStage& ws,
+                     FwdCStage& cs, StopState& ss) {
+    const v3 o = P.cam.eye;
+    const float HW = (float)(P.cam.H * P.cam.W);
+    const bool want_gt = out.rpe || out.err;
+    FwdPix a;
+    a.g = pixel_geom(P, tile, wig * 32 + lane);
+    a.log_t = 0.f;
+    a.trans = 1.0f;
+    a.nd = 0.f;
+    a.err = 0.f;
+    a.rgb = mk(0.f, 0.f, 0.f);
+    a.nrm = mk(0.f, 0.f, 0.f);
+    a.gt = mk(0.f, 0.f, 0.f);
+    a.qi = 0;
+    a.q = 0.f;
+    if (!a.g.oob) {
+        if (P.Q > 0) {
+            a.q = P.dq[a.g.px * P.Q];
+            for (int q = 0; q < P.Q; q++) out.qd[a.g.px * P.Q + q] = -1.0f;
+        }
+        if (want_gt) a.gt = mk(P.gt[3 * a.g.px], P.gt[3 * a.g.px + 1], P.gt[3 * a.g.px + 2]);
+    }
+    cs.dir[lane] = make_float4(a.g.d.x, a.g.d.y, a.g.d.z, 0.f);
+    const uint32_t lt_mask = (1u << lane) - 1u;
+    const int64_t start = P.tile_off[tile];
+    const int total = (int)(P.tile_off[tile + 1] - start);
+    int es = total;
+    int n_contrib_pairs = 0;
+    bool stopped = false;
+    for (int k0 = 0; k0 < total && !stopped; k0 += 32) {
+        stage_prims(ws, P, start, k0, total, lane);
+        const int kn = min(32, total - k0);
+        for (int kk = 0; kk < kn; kk++) {
+            const float4 s4 = ws.sph[kk];
+            float tn, tf;
+            const bool hit = a.g.oob ? false : ray_sphere(o, a.g.d, mk(s4.x, s4.y, s4.z), s4.w, tn, tf);
+            const uint32_t m = __ballot_sync(0xffffffffu, hit);
+            if (lane == 0) cs.mask[kk] = m;
+        }
+        __syncwarp();
+        int kb = 0;
+        while (kb < kn && !stopped) {
+            // sub-batch [kb, kb + nsub): primitives whose faces fit the staging area
+            const int kl = kb + lane;
+            int deg = 0;
+            if (kl < kn && cs.mask[kl] != 0u) {
+                const int32_t pr = ws.pid[kl];
+                deg = __ldg(&P.adj_off[pr + 1]) - __ldg(&P.adj_off[pr]);
+            }
+            const int incl = warp_incl_scan(deg, lane);
+            const uint32_t fits = __ballot_sync(0xffffffffu, kl < kn && incl <= kFaceCap);
+            const int cnt = __popc(fits);  // a prefix of the lanes
+            const bool big = cnt == 0;     // the first primitive alone exceeds the staging area
+            const int nsub = big ? 1 : cnt;
+            const int np = (lane < nsub) ? __popc(cs.mask[kl]) : 0;
+            const int pincl = warp_incl_scan(np, lane);
+            if (lane < nsub) {
+                cs.face_off[lane] = big ? 0 : incl - deg;
+                cs.pair_off[lane] = pincl - np;
+            }
+            if (lane == nsub - 1) {
+                cs.face_off[nsub] = big ? 0 : incl;
+                cs.pair_off[nsub] = pincl;
+            }
+            __syncwarp();
+            const int n_faces = cs.face_off[nsub];
+            const int n_pairs = cs.pair_off[nsub];
+            for (int i = lane; i < n_faces; i += 32) {
+                const int j = seg_search(cs.face_off, nsub, i);
+                const int kk = kb + j;
+                const int32_t pr = ws.pid[kk];
+                const float4 s4 = ws.sph[kk];
+                const v3 center = mk(s4.x, s4.y, s4.z);
+                const int32_t a0 = __ldg(&P.adj_off[pr]);
+                const uint2 raw = __ldg(&P.adj_diff[a0 + (i - cs.face_off[j])]);
+                const v3 diff = mk(h2f((uint16_t)(raw.x & 0xffffu)), h2f((uint16_t)(raw.x >> 16)),
+                                   h2f((uint16_t)(raw.y & 0xffffu)));
+                const Face f = make_face(o, center, dot(center, center), s4.w * s4.w, center + diff,
+                                         h2f((uint16_t)(raw.y >> 16)));
+                cs.face[i] = make_float4(f.n.x, f.n.y, f.n.z, f.num);
+            }
+            __syncwarp();
+            int next = 0;  // next primitive of the sub-batch to composite
+            for (int base = 0; next < nsub; base += 32) {
+                const int j = base + lane;
+                if (j < n_pairs) {
+                    const int r = seg_search(cs.pair_off, nsub, j);
+                    const int kk = kb + r;
+                    const int p = nth_set_bit(cs.mask[kk], j - cs.pair_off[r]);
+                    const float4 d4 = cs.dir[p];
+                    const v3 d = mk(d4.x, d4.y, d4.z);
+                    const float4 s4 = ws.sph[kk];
+                    const v3 center = mk(s4.x, s4.y, s4.z);
+                    const float radius = s4.w;
+                    const int32_t prim = ws.pid[kk];
+                    float tn, tf;
+                    ray_sphere(o, d, center, radius, tn, tf);
+                    if (!big) {
+                        const int f1 = cs.face_off[r + 1];
+#pragma unroll 2
+                        for (int q = cs.face_off[r]; q < f1; q++) {
+                            const float4 f = cs.face[q];
+                            const float dp = dot(d, mk(f.x, f.y, f.z));
+                            if (face_may_clip(dp, f.w, tn, tf)) {
+                                const float t_face = f.w / dp;
+                                tf = dp >= 0.0f ? fmin_t(t_face, tf) : tf;
+                                tn = dp < 0.0f ? fmax_t(t_face, tn) : tn;
+                            }
+                        }
+                    } else {
+                        const int32_t a0 = __ldg(&P.adj_off[prim]);
+                        const int32_t a1 = __ldg(&P.adj_off[prim + 1]);
+                        const float cc = dot(center, center), rr = radius * radius;
+                        for (int32_t e = a0; e < a1; e++) {
+                            const uint2 raw = __ldg(&P.adj_diff[e]);
+                            const v3 diff = mk(h2f((uint16_t)(raw.x & 0xffffu)), h2f((uint16_t)(raw.x >> 16)),
+                                               h2f((uint16_t)(raw.y & 0xffffu)));
+                            const Face f = make_face(o, center, cc, rr, center + diff, h2f((uint16_t)(raw.y >> 16)));
+                            const float dp = dot(d, f.n);
+                            if (face_may_clip(dp, f.num, tn, tf)) {
+                                const float t_face = f.num / dp;
+                                tf = dp >= 0.0f ? fmin_t(t_face, tf) : tf;
+                                tn = dp < 0.0f ? fmax_t(t_face, tn) : tn;
+                            }
+                        }
+                    }
+                    const float4 n4 = ws.nsg[kk];
+                    const PlaneRes pr =
+                        plane_fwd_tex(o, d, tn, center, mk(n4.x, n4.y, n4.z), radius, global_texels(P, prim), P.S);
+                    const float tf2 = pr.dp >= 0.0f ? fmin_t(pr.t_surf, tf) : tf;
+                    const float tn2 = pr.dp < 0.0f ? fmax_t(pr.t_surf, tn) : tn;
+                    cs.rec[j & 63] = make_float4(tf2 - tn2, pr.rgb.x, pr.rgb.y, pr.rgb.z);
+                    cs.rec_tn[j & 63] = tn2;
+                }
+                __syncwarp();
+                const int done = min(base + 32, n_pairs);
+                while (next < nsub && cs.pair_off[next + 1] <= done) {
+                    const int kk = kb + next;
+                    const bool below = a.g.oob ? false : a.trans < P.thr;
+                    if (stop_vote<G>(ss, wig, lane, k0 + kk, below, out.status)) {
+                        es = k0 + kk;
+                        stopped = true;
+                        break;
+                    }
+                    const uint32_t m = cs.mask[kk];
+                    float c_acc = 0.f, e_acc = 0.f;
+                    if ((m >> lane) & 1u) {
+                        const int slot = (cs.pair_off[next] + __popc(m & lt_mask)) & 63;
+                        const float4 rc = cs.rec[slot];
+                        const float dt = rc.x;
+                        if (dt > 0.0f) {
+                            const v3 prgb = mk(rc.y, rc.z, rc.w);
+                            const float tn = cs.rec_tn[slot];
+                            const float4 n4 = ws.nsg[kk];
+                            const v3 pn = mk(n4.x, n4.y, n4.z);
+                            const float sigma = n4.w;
+                            float dlt = -sigma * dt;
+                            float alpha = 1.0f - expf(dlt);
+                            float trans = a.trans;
+                            if (out.err) {
+                                v3 de = prgb - a.gt;
+                                a.err += dot(de, de) * alpha * trans;
+                            }
+                            a.rgb = a.rgb + trans * (alpha * prgb);
+                            a.log_t += dlt;
+                            c_acc += alpha * trans / HW;
+                            if (out.rpe) {
+                                v3 df = prgb - a.gt;
+                                float l1 = fabsf(df.x) + fabsf(df.y) + fabsf(df.z);
+                                e_acc += alpha * trans * l1 / HW;
+                            }
+                            float ndv = dot(pn, a.g.d);
+                            if (ndv > 0.0f) a.nd += ndv * ndv * alpha * trans;
+                            a.nrm = a.nrm + (alpha * trans) * pn;
+                            float next_trans = expf(a.log_t);
+                            while (a.qi < P.Q && next_trans < a.q) {
+                                float qd = tn + logf(trans / a.q) / sigma;
+                                out.qd[a.g.px * P.Q + a.qi] = qd;
+                                a.qi += 1;
+                                if (a.qi < P.Q) a.q = P.dq[a.g.px * P.Q + a.qi];
+                            }
+                            a.trans = next_trans;
+                        }
+                    }
+                    if (__any_sync(0xffffffffu, c_acc != 0.f || e_acc != 0.f)) {
+                        n_contrib_pairs++;
+                        float csum = warp_sum(c_acc);
+                        float esum = out.rpe ? warp_sum(e_acc) : 0.f;
+                        if (lane == 0) {
+                            atomicAdd(&out.contrib[ws.pid[kk]], csum);
+                            if (out.rpe) atomicAdd(&out.point_err[ws.pid[kk]], esum);
+                        }
+                    }
+                    next++;
+                }
+                if (stopped) break;
+            }
+            __syncwarp();
+            kb += nsub;
+        }
+        __syncwarp();
+    }
+    if (!a.g.oob) {
+        const int64_t p = a.g.px;
+        out.color[3 * p] = a.rgb.x;
+        out.color[3 * p + 1] = a.rgb.y;
+        out.color[3 * p + 2] = a.rgb.z;
+        out.log_t[p] = a.log_t;
+        out.nd[p] = a.nd;
+        out.normal[3 * p] = a.nrm.x;
+        out.normal[3 * p + 1] = a.nrm.y;
+        out.normal[3 * p + 2] = a.nrm.z;
+        if (out.err) {
+            v3 de = mk(0.f, 0.f, 0.f) - a.gt;
+            out.err[p] = a.err + dot(de, de) * expf(a.log_t);
+        }
     }
     if (lane == 0 && wig == 0) out.early_stop[tile] = es;
     if (out.tile_contrib_pairs && lane == 0) atomicAdd(&out.tile_contrib_pairs[tile], n_contrib_pairs);

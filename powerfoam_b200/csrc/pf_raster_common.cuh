@@ -108,8 +108,32 @@ PF_D void stage_faces(WarpStage& ws, const RasterParams& P, int32_t a0, int e0, 
     __syncwarp();
 }
 
-// texture.py:10-72 with texel data in shared memory (hit path)
-PF_D PlaneRes plane_fwd_smem(v3 o, v3 d, float t_near, v3 po, v3 pn, float radius, const WarpStage& ws, int S) {
+// texel records of one primitive, from the warp's shared staging area or
+// straight from global memory (read-only path)
+struct SmemTexels {
+    const WarpStage& ws;
+    PF_D v3 site(int i) const { return mk(ws.ts[3 * i], ws.ts[3 * i + 1], ws.ts[3 * i + 2]); }
+    PF_D v3 rgb(int i) const { return mk(ws.tr[3 * i], ws.tr[3 * i + 1], ws.tr[3 * i + 2]); }
+    PF_D float height(int i) const { return ws.th[i]; }
+};
+
+struct GlobalTexels {
+    const float* s;  // (S,3) of the primitive
+    const float* c;  // (S,3)
+    const float* h;  // (S)
+    PF_D v3 site(int i) const { return mk(__ldg(s + 3 * i), __ldg(s + 3 * i + 1), __ldg(s + 3 * i + 2)); }
+    PF_D v3 rgb(int i) const { return mk(__ldg(c + 3 * i), __ldg(c + 3 * i + 1), __ldg(c + 3 * i + 2)); }
+    PF_D float height(int i) const { return __ldg(h + i); }
+};
+
+PF_D GlobalTexels global_texels(const RasterParams& P, int32_t prim) {
+    const int64_t b3 = (int64_t)prim * P.S * 3;
+    return GlobalTexels{P.sites + b3, P.rgb + b3, P.height + (int64_t)prim * P.S};
+}
+
+// texture.py:10-72 (hit path); one copy of the arithmetic for every texel source
+template <typename TX>
+PF_D PlaneRes plane_fwd_tex(v3 o, v3 d, float t_near, v3 po, v3 pn, float radius, const TX& tx, int S) {
     PlaneRes r;
     float _dp;
     float _t_surf = ray_plane(o, d, po, pn, 0.0f, _dp);
@@ -119,10 +143,10 @@ PF_D PlaneRes plane_fwd_smem(v3 o, v3 d, float t_near, v3 po, v3 pn, float radiu
     float hsum = 0.f, _wsum = 0.f;
 #pragma unroll 1
     for (int i = 0; i < S; i++) {
-        v3 df = _pt - mk(ws.ts[3 * i], ws.ts[3 * i + 1], ws.ts[3 * i + 2]);
+        v3 df = _pt - tx.site(i);
         float dist_sq = dot(df, df) / rr;
         float w = expf(-kTemp * dist_sq);
-        hsum += w * ws.th[i];
+        hsum += w * tx.height(i);
         _wsum += w;
     }
     _wsum = fmax_t(_wsum, 1e-20f);
@@ -135,10 +159,10 @@ PF_D PlaneRes plane_fwd_smem(v3 o, v3 d, float t_near, v3 po, v3 pn, float radiu
     float wsum = 0.f;
 #pragma unroll 1
     for (int i = 0; i < S; i++) {
-        v3 df = pt - mk(ws.ts[3 * i], ws.ts[3 * i + 1], ws.ts[3 * i + 2]);
+        v3 df = pt - tx.site(i);
         float dist_sq = dot(df, df) / rr;
         float w = expf(-kTemp * dist_sq);
-        rgb_sum = rgb_sum + w * mk(ws.tr[3 * i], ws.tr[3 * i + 1], ws.tr[3 * i + 2]);
+        rgb_sum = rgb_sum + w * tx.rgb(i);
         wsum += w;
     }
     wsum = fmax_t(wsum, 1e-20f);
@@ -151,6 +175,10 @@ PF_D PlaneRes plane_fwd_smem(v3 o, v3 d, float t_near, v3 po, v3 pn, float radiu
     r.rgb = rgb_sum / wsum;
     r.wsum = wsum;
     return r;
+}
+
+PF_D PlaneRes plane_fwd_smem(v3 o, v3 d, float t_near, v3 po, v3 pn, float radius, const WarpStage& ws, int S) {
+    return plane_fwd_tex(o, d, t_near, po, pn, radius, SmemTexels{ws}, S);
 }
 
 

@@ -366,6 +366,12 @@ def main():
     if "raster_edge" in which:
         sc = edge_scene(2)
         raster_case("raster_edge", sc, look_at_camera((0.0, 0.0, 2.5), (0, 0, 0), 40, 24, 55.0), 2)
+    if "raster_dense" in which:
+        # opaque enough that whole tiles fall below the transmittance threshold
+        # (early termination); 24x24 so no tile is ragged
+        sc = make_scene(5, 700, -1.0, 1.0, 0.12, 0.3)
+        sc["density"] = (sc["density"] * 300.0).astype(F32)
+        raster_case("raster_dense", sc, look_at_camera((0.2, 0.3, 2.2), (0, 0, 0), 24, 24, 40.0), 5)
     if "bin_large" in which:
         sc = make_scene(3, 3000, -1.0, 1.0, 0.01, 0.08)
         binning_case("bin_large", sc, look_at_camera((1.0, 0.5, 2.6), (0, 0, 0), 96, 64, 50.0))

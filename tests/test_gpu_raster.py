@@ -51,7 +51,7 @@ def oracle_forward(sc, cam, adj, adj_off, dq=None, gt=None, rpe=False, tw=8, thr
     return o, (keys, prims, offs, ad)
 
 
-@pytest.mark.parametrize("case", ["raster_small", "raster_edge"])
+@pytest.mark.parametrize("case", ["raster_small", "raster_edge", "raster_dense"])
 def test_binning_matches_golden(golden, case):
     g = golden(case)
     sc, cam, adj, adj_off = golden_inputs(g)
@@ -124,7 +124,7 @@ def test_binning_empty_and_all_culled():
     assert int(b.tile_offsets.abs().sum().item()) == 0
 
 
-@pytest.mark.parametrize("case", ["raster_small", "raster_edge"])
+@pytest.mark.parametrize("case", ["raster_small", "raster_edge", "raster_dense"])
 def test_forward_backward_match_golden(golden, case):
     g = golden(case)
     sc, cam, adj, adj_off = golden_inputs(g)
@@ -191,6 +191,41 @@ def test_forward_backward_match_oracle(seed, tw):
     assert_close_rel(t["texel_height"].grad.cpu().numpy(), gr["texel_height"], 1e-4, "height")
 
 
+@pytest.mark.parametrize("tw", [8, 16, 32])
+def test_dense_early_termination_matches_oracle(tw):
+    """Opaque scene: whole tiles fall below the transmittance threshold, so
+    the barrier-free stop vote decides where every tile ends; early-stop
+    indices must equal the oracle's (48x40 leaves ragged tiles at 16 and 32,
+    which never stop)."""
+    sc = np_scene(77, 700, -1.0, 1.0, 0.12, 0.3)
+    sc["density"] = (sc["density"] * 300.0).astype(np.float32)
+    cam = np_camera((0.2, 0.3, 2.2), (0, 0, 0), 48, 40, 40.0)
+    adj, adj_off = cech_np(sc["points"], sc["radii"])
+    R = Rasterizer(Args(), "cuda", "float", tile_width=tw)
+    R.collect_stats = True
+    t = {k: to_t(v).requires_grad_(True) for k, v in sc.items()}
+    out = R.forward(torch_cam(cam), None, t["points"], t["radii"], t["density"], t["normals"], t["texel_sites"],
+                    t["texel_rgb"], t["texel_height"], to_t(adj), to_t(adj_off), None, False)
+    o, (keys, prims, offs, ad) = oracle_forward(sc, cam, adj, adj_off, tw=tw)
+    es = R.last_stats["early_stop"].cpu().numpy()
+    assert np.array_equal(es, o["early_stop"])
+    assert (o["early_stop"] < np.diff(offs)).sum() >= (2 if tw < 32 else 1)
+    assert max_abs(out[0].detach().cpu(), o["color"]) <= 1e-5
+    assert max_abs(out[1].detach().cpu(), 1 - np.exp(o["log_t"])) <= 1e-5
+    loss = (out[0] * to_t(np.random.default_rng(3).standard_normal(o["color"].shape).astype(np.float32))).sum()
+    loss.backward()
+    sph, nsig, rgbh = packed(sc)
+    H, W = cam["height"], cam["width"]
+    g_c = np.random.default_rng(3).standard_normal(o["color"].shape).astype(np.float32)
+    z = np.zeros((H, W), np.float32)
+    gr = orc.raster_backward(orc_cam(cam), tw, sph, nsig, sc["texel_sites"], rgbh, adj, adj_off, ad, offs, prims,
+                             o["early_stop"], o["log_t"], g_c, z, z, np.zeros((H, W, 3), np.float32),
+                             np.zeros(sc["points"].shape[0], np.float32))
+    assert_close_rel(t["points"].grad.cpu().numpy(), gr["spheres"][:, :3], 1e-4, "points")
+    assert_close_rel(t["density"].grad.cpu().numpy(), gr["nsigmas"][:, 3], 1e-4, "density")
+    assert_close_rel(t["texel_rgb"].grad.cpu().numpy(), gr["texel_rgb"], 1e-4, "rgb")
+
+
 def test_surface_objective_forward_and_errors():
     sc = np_scene(21, 300, -0.6, 0.6, 0.03, 0.15)
     cam = np_camera((0.0, 0.2, 2.2), (0, 0, 0), 48, 40, 55.0)
@@ -221,7 +256,7 @@ def test_surface_objective_forward_and_errors():
         Rasterizer(Args(), "cuda", attr_dtype="half").forward(*args, None, False)
 
 
-@pytest.mark.parametrize("case", ["raster_small", "raster_edge"])
+@pytest.mark.parametrize("case", ["raster_small", "raster_edge", "raster_dense"])
 def test_benchmark_and_visualize_match_golden(golden, case):
     g = golden(case)
     sc, cam, adj, adj_off = golden_inputs(g)
