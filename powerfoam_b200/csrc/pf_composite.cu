@@ -37,7 +37,9 @@ namespace pf {
 template <int TW>
 __global__ void __launch_bounds__(Layout<TW>::THREADS) raster_fwd_kernel(RasterParams P, FwdOut out) {
     constexpr int G = Layout<TW>::G;
-    __shared__ WarpStage stage[G];
+    // the two-pixels-per-lane layout stages per warp here; the compacted
+    // one-pixel-per-lane path keeps its staging in dynamic shared memory
+    __shared__ WarpStage stage[Layout<TW>::PPL == 1 ? 1 : G];
     __shared__ StopState ss;
     extern __shared__ float4 fwd_dyn[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -46,7 +48,7 @@ __global__ void __launch_bounds__(Layout<TW>::THREADS) raster_fwd_kernel(RasterP
         int64_t tile = next_tile<G>(P, static_next, lane, &ss);
         if (tile < 0) break;
         if constexpr (Layout<TW>::PPL == 1)
-            fwd_tile_c<G>(P, out, tile, warp, lane, stage[warp], reinterpret_cast<FwdCStage*>(fwd_dyn)[warp], ss);
+            fwd_tile_c<G>(P, out, tile, warp, lane, reinterpret_cast<FwdCStage*>(fwd_dyn)[warp], ss);
         else
             fwd_tile<G, Layout<TW>::PPL>(P, out, tile, warp, lane, stage[warp], ss);
     }

@@ -356,6 +356,9 @@ PF_D void fwd_tile(const RasterParams& P, const FwdOut& out, int64_t tile, int w
 constexpr int kFaceCap = 256;
 
 struct FwdCStage {
+    float4 sph[32];     // staged primitives (as WarpStage)
+    float4 nsg[32];
+    int32_t pid[32];
     float4 face[kFaceCap];
     float4 rec[64];     // per pair: dt, rgb
     float rec_tn[64];   // per pair: segment start (quantile depths)
@@ -404,8 +407,8 @@ PF_D int seg_search(const int* off, int n, int x) {
 }
 
 template <int G>
-PF_D void fwd_tile_c(const RasterParams& P, const FwdOut& out, int64_t tile, int wig, int lane, WarpStage& ws,
-                     FwdCStage& cs, StopState& ss) {
+PF_D void fwd_tile_c(const RasterParams& P, const FwdOut& out, int64_t tile, int wig, int lane, FwdCStage& cs,
+                     StopState& ss) {
     const v3 o = P.cam.eye;
     const float HW = (float)(P.cam.H * P.cam.W);
     const bool want_gt = out.rpe || out.err;
@@ -435,10 +438,19 @@ PF_D void fwd_tile_c(const RasterParams& P, const FwdOut& out, int64_t tile, int
     int n_contrib_pairs = 0;
     bool stopped = false;
     for (int k0 = 0; k0 < total && !stopped; k0 += 32) {
-        stage_prims(ws, P, start, k0, total, lane);
+        {
+            const int k = k0 + lane;
+            if (k < total) {
+                const int32_t p = P.tile_prims[start + k];
+                cs.pid[lane] = p;
+                cs.sph[lane] = __ldg(&P.spheres[p]);
+                cs.nsg[lane] = __ldg(&P.nsigmas[p]);
+            }
+            __syncwarp();
+        }
         const int kn = min(32, total - k0);
         for (int kk = 0; kk < kn; kk++) {
-            const float4 s4 = ws.sph[kk];
+            const float4 s4 = cs.sph[kk];
             float tn, tf;
             const bool hit = a.g.oob ? false : ray_sphere(o, a.g.d, mk(s4.x, s4.y, s4.z), s4.w, tn, tf);
             const uint32_t m = __ballot_sync(0xffffffffu, hit);
@@ -451,7 +463,7 @@ PF_D void fwd_tile_c(const RasterParams& P, const FwdOut& out, int64_t tile, int
             const int kl = kb + lane;
             int deg = 0;
             if (kl < kn && cs.mask[kl] != 0u) {
-                const int32_t pr = ws.pid[kl];
+                const int32_t pr = cs.pid[kl];
                 deg = __ldg(&P.adj_off[pr + 1]) - __ldg(&P.adj_off[pr]);
             }
             const int incl = warp_incl_scan(deg, lane);
@@ -475,8 +487,8 @@ PF_D void fwd_tile_c(const RasterParams& P, const FwdOut& out, int64_t tile, int
             for (int i = lane; i < n_faces; i += 32) {
                 const int j = seg_search(cs.face_off, nsub, i);
                 const int kk = kb + j;
-                const int32_t pr = ws.pid[kk];
-                const float4 s4 = ws.sph[kk];
+                const int32_t pr = cs.pid[kk];
+                const float4 s4 = cs.sph[kk];
                 const v3 center = mk(s4.x, s4.y, s4.z);
                 const int32_t a0 = __ldg(&P.adj_off[pr]);
                 const uint2 raw = __ldg(&P.adj_diff[a0 + (i - cs.face_off[j])]);
@@ -496,10 +508,10 @@ PF_D void fwd_tile_c(const RasterParams& P, const FwdOut& out, int64_t tile, int
                     const int p = nth_set_bit(cs.mask[kk], j - cs.pair_off[r]);
                     const float4 d4 = cs.dir[p];
                     const v3 d = mk(d4.x, d4.y, d4.z);
-                    const float4 s4 = ws.sph[kk];
+                    const float4 s4 = cs.sph[kk];
                     const v3 center = mk(s4.x, s4.y, s4.z);
                     const float radius = s4.w;
-                    const int32_t prim = ws.pid[kk];
+                    const int32_t prim = cs.pid[kk];
                     float tn, tf;
                     ray_sphere(o, d, center, radius, tn, tf);
                     if (!big) {
@@ -531,7 +543,7 @@ PF_D void fwd_tile_c(const RasterParams& P, const FwdOut& out, int64_t tile, int
                             }
                         }
                     }
-                    const float4 n4 = ws.nsg[kk];
+                    const float4 n4 = cs.nsg[kk];
                     const PlaneRes pr =
                         plane_fwd_tex(o, d, tn, center, mk(n4.x, n4.y, n4.z), radius, global_texels(P, prim), P.S);
                     const float tf2 = pr.dp >= 0.0f ? fmin_t(pr.t_surf, tf) : tf;
@@ -558,7 +570,7 @@ PF_D void fwd_tile_c(const RasterParams& P, const FwdOut& out, int64_t tile, int
                         if (dt > 0.0f) {
                             const v3 prgb = mk(rc.y, rc.z, rc.w);
                             const float tn = cs.rec_tn[slot];
-                            const float4 n4 = ws.nsg[kk];
+                            const float4 n4 = cs.nsg[kk];
                             const v3 pn = mk(n4.x, n4.y, n4.z);
                             const float sigma = n4.w;
                             float dlt = -sigma * dt;
@@ -594,8 +606,8 @@ PF_D void fwd_tile_c(const RasterParams& P, const FwdOut& out, int64_t tile, int
                         float csum = warp_sum(c_acc);
                         float esum = out.rpe ? warp_sum(e_acc) : 0.f;
                         if (lane == 0) {
-                            atomicAdd(&out.contrib[ws.pid[kk]], csum);
-                            if (out.rpe) atomicAdd(&out.point_err[ws.pid[kk]], esum);
+                            atomicAdd(&out.contrib[cs.pid[kk]], csum);
+                            if (out.rpe) atomicAdd(&out.point_err[cs.pid[kk]], esum);
                         }
                     }
                     next++;

@@ -131,7 +131,18 @@ PF_D GlobalTexels global_texels(const RasterParams& P, int32_t prim) {
     return GlobalTexels{P.sites + b3, P.rgb + b3, P.height + (int64_t)prim * P.S};
 }
 
-// texture.py:10-72 (hit path); one copy of the arithmetic for every texel source
+// texture.py:10-72 (hit path); one copy of the arithmetic for every texel
+// source.  Texels read from global memory unroll the site loops by 2 so two
+// sites' loads are in flight together (the sums keep their order).
+template <typename TX>
+struct TexUnroll {
+    static constexpr int value = 1;
+};
+template <>
+struct TexUnroll<GlobalTexels> {
+    static constexpr int value = 2;
+};
+
 template <typename TX>
 PF_D PlaneRes plane_fwd_tex(v3 o, v3 d, float t_near, v3 po, v3 pn, float radius, const TX& tx, int S) {
     PlaneRes r;
@@ -141,7 +152,7 @@ PF_D PlaneRes plane_fwd_tex(v3 o, v3 d, float t_near, v3 po, v3 pn, float radius
     v3 _pt = o + _tq * d;
     float rr = radius * radius;
     float hsum = 0.f, _wsum = 0.f;
-#pragma unroll 1
+#pragma unroll TexUnroll<TX>::value
     for (int i = 0; i < S; i++) {
         v3 df = _pt - tx.site(i);
         float dist_sq = dot(df, df) / rr;
@@ -157,7 +168,7 @@ PF_D PlaneRes plane_fwd_tex(v3 o, v3 d, float t_near, v3 po, v3 pn, float radius
     v3 pt = o + tq * d;
     v3 rgb_sum = mk(0.f, 0.f, 0.f);
     float wsum = 0.f;
-#pragma unroll 1
+#pragma unroll TexUnroll<TX>::value
     for (int i = 0; i < S; i++) {
         v3 df = pt - tx.site(i);
         float dist_sq = dot(df, df) / rr;
