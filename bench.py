@@ -54,8 +54,8 @@ def parse():
     p.add_argument("--tile", type=int, default=8)
     p.add_argument("--workload", default=WORKLOAD, help="raster1m (the measured configuration), raster256k "
                    "(a quarter-size case with the same density per pixel, for profiling), batch3m (32 views of "
-                   "a 3.1M-primitive scene in one graph-captured persistent step), batch256k (its small case) or "
-                   "proposal (proposal-seeded vs plain cell walk)")
+                   "a 3.1M-primitive scene in one graph-captured persistent step), batch256k (its small case), "
+                   "trace1m (tracer forward + adjoint) or proposal (proposal-seeded vs plain cell walk)")
     p.add_argument("--cpu-sample-tiles", type=int, default=0, help="tiles composited by the CPU baseline")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-autotune", action="store_true", help="batch workloads: use --tile, chunk 1")
@@ -418,13 +418,14 @@ def batch_main(args, world, rank, local, dev):
     # pack 1, neighbour encoding 1, SH pre-step V, binning per view, the batch launch (work list: keys 1
     # + three 5-kernel radix passes when ordered by length; the persistent kernel 1; 6 + V sanitise), SH adjoint V
     per_step = 1 + 1 + V + sum(bin_launches(T, with_order=False) for T in step.n_tiles)
-    per_step += 1 + (15 if step.order == "longest" else 0) + 1 + 6 + V + V
+    per_step += 1 + (15 if step.order == "longest" else 0) + (2 if step.split else 1) + 6 + V + V
     line = dict(metric="batched multi-view fwd+bwd, views/s", value=n_views * 1000.0 / ms,
                 unit="views/s (32 views per step)", n_gpus=world, steps=args.steps, warmup=max(args.warmup, 3),
                 ms_per_step=ms, higher_is_better=True, scaling="strong", vs_baseline=None, dtype="f32",
                 data="synthetic (seeded scene, orbit cameras, uniform targets)",
                 config=dict(workload=args.workload, prims=cfg["n"], views=n_views, pixels=pixels, pairs=pairs,
-                            tile=step.tile_width, chunk=step.chunk, order=step.order, autotune_s=tune_s,
+                            tile=step.tile_width, chunk=step.chunk, order=step.order, split=step.split,
+                            autotune_s=tune_s,
                             per_view_calls_ms=sequential_ms,
                             autotune=table, graph="one CUDA graph per step",
                             l2="inputs larger than L2 (805 MB of primitive records), no flush",
@@ -535,6 +536,85 @@ def proposal_main(args, dev):
     print(json.dumps(line), flush=True)
 
 
+def trace_main(args, dev):
+    """Tracer forward + adjoint (config 2): the 1,048,576-primitive scene of
+    the rasterizer workload with its power-diagram adjacency (Qhull on the
+    host, once), one 1280x720 camera on the radius-3 orbit at a seeded
+    azimuth / elevation, walks from the camera's cell; one step = the walk
+    (colour, log transmittance, depth, normal), an L2 loss against a seeded
+    uniform target and the hand-written adjoint to every primitive gradient."""
+    from powerfoam_b200 import synthetic
+    from powerfoam_b200.adjacency import build_power_adjacency, power_adjacency_diff, start_cell
+    from powerfoam_b200.raytrace import RayTracer
+
+    cfg = synthetic.CONFIGS["trace1m"]
+    sc = synthetic.make_scene(cfg["n"], seed=cfg["seed"], mixture=cfg["mixture"], sigma=cfg["sigma"],
+                              r_range=cfg["r_range"], device=dev)
+    t0 = time.perf_counter()
+    adj, off = build_power_adjacency(sc["points"], sc["radii"])
+    adj_s = time.perf_counter() - t0
+    pm = power_adjacency_diff(sc["points"], sc["radii"], adj, off)
+    cam = synthetic.orbit_camera(2, cfg["width"], cfg["height"], cfg["vfov"], device=dev)
+    rgb = synthetic.texel_rgb(sc, cam)
+    st = start_cell(sc["points"], sc["radii"], cam.eye)
+    tr = RayTracer(Args(), dev)
+    names = ["points", "radii", "density", "normals", "texel_sites", "texel_height"]
+    params = {k: sc[k].clone().requires_grad_(True) for k in names}
+    rgb_p = rgb.clone().requires_grad_(True)
+    g = torch.Generator().manual_seed(202)
+    target_host = torch.rand((cfg["height"], cfg["width"], 3), generator=g).pin_memory()
+    target = target_host.to(dev)
+
+    def step(t=None):
+        for p in list(params.values()) + [rgb_p]:
+            p.grad = None
+        color, log_t, depth, normal = tr.forward(cam, st, params["points"], params["radii"], params["density"],
+                                                 params["normals"], params["texel_sites"], rgb_p,
+                                                 params["texel_height"], adj, off, pm)
+        loss = ((color - (target if t is None else t)) ** 2).sum()
+        loss.backward()
+        return loss
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(int(os.environ.get("LOCAL_RANK", "0")))
+    clocks.start()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    a.record()
+    for _ in range(args.steps):
+        step()
+    b.record()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = a.elapsed_time(b) / args.steps
+    t_dev = torch.empty_like(target)
+    loss_host = torch.empty(args.steps, dtype=torch.float32).pin_memory()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    for i in range(args.steps):
+        t_dev.copy_(target_host, non_blocking=True)
+        loss_host[i].copy_(step(t_dev).detach(), non_blocking=True)
+    e1.record()
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1) / args.steps
+    r = tr.trace(cam, st, sc["points"], sc["radii"], sc["density"], sc["normals"], sc["texel_sites"], rgb,
+                 sc["texel_height"], adj, off, pm)
+    steps_total = int(r.visit_count.sum())
+    deg = (off[1:] - off[:-1]).float().mean().item()
+    line = dict(metric="tracer fwd+bwd ms/iter @1M prims 720p", value=1000.0 / ms, unit="frames/s (fwd+bwd)",
+                n_gpus=1, steps=args.steps, warmup=max(args.warmup, 3), ms_per_step=ms, higher_is_better=True,
+                scaling="weak", vs_baseline=None, dtype="f32", data="synthetic",
+                config=dict(workload="trace1m", prims=cfg["n"], width=cfg["width"], height=cfg["height"],
+                            cells_walked=steps_total, mean_degree=deg, adjacency_s=adj_s,
+                            l2="inputs larger than L2, no flush"),
+                clocks=clk, e2e=dict(value=1000.0 / e2e_ms, unit="frames/s", h2d_bytes_per_step=target.numel() * 4,
+                                     d2h_bytes_per_step=4))
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -551,6 +631,9 @@ def main():
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
     if args.workload == "proposal":
         proposal_main(args, dev)
+        return
+    if args.workload == "trace1m":
+        trace_main(args, dev)
         return
     if args.workload.startswith("batch"):
         batch_main(args, world, rank, local, dev)

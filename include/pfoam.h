@@ -317,9 +317,11 @@ PF_API int pf_mlp_gemm_selftest(const uint16_t *a, const uint16_t *b, int32_t mo
  * sum((color - target)^2), dL/dcolor = 2 (color - target) and the adjoint of
  * pf_raster_backward, with the gradients of all views summed into one set of
  * primitive gradients (texel_rgb gradients per view, since the colours are
- * per view).  One persistent launch takes (view, tile) work items from a
- * device queue, `chunk` items per pop, in the order `order` selects; each
- * tile's adjoint runs right after its own forward.  Views are binned
+ * per view).  A persistent launch takes (view, tile) work items from a
+ * device queue, `chunk` items per pop, in the order `order` selects; fused
+ * (split = 0), each tile's adjoint runs right after its own forward in the
+ * same launch; split (split = 1), one persistent launch runs every tile's
+ * forward and loss gradient, then a second every tile's adjoint.  Views are binned
  * beforehand with pf_bin at the batch's tile width (8, 16 or 32).  Nothing is
  * allocated and nothing synchronises, so the call can be captured in a CUDA
  * graph.  Images are bit-identical to pf_raster_forward per view; gradients
@@ -363,7 +365,9 @@ typedef struct pf_batch_view {
  * concatenated in view order: the loss of view v is the sum of its slice. */
 PF_API int pf_batch_workspace_size(const pf_batch_view *views, int32_t n_views, int32_t tile_width, size_t *bytes);
 PF_API int pf_batch_render(const pf_batch_scene *scene, const pf_batch_view *views, int32_t n_views,
-                           int32_t tile_width, int32_t chunk, int32_t order, void *workspace, size_t workspace_bytes,
+                           int32_t tile_width, int32_t chunk, int32_t order,
+                           int32_t split /* 0: one fused launch; 1: a forward launch, then an adjoint launch */,
+                           void *workspace, size_t workspace_bytes,
                            float *tile_loss, float *grad_points, float *grad_radii, float *grad_normals,
                            float *grad_density, float *grad_texel_sites, float *grad_texel_height,
                            int32_t *status, void *stream);

@@ -152,8 +152,8 @@ _SIGS = {
     "pf_sh_texel_rgb": [c_vp, c_vp, c_i64, c_i32, ctypes.POINTER(c_f), c_vp, c_vp],
     "pf_sh_texel_rgb_backward": [c_vp, c_vp, c_i64, c_i32, ctypes.POINTER(c_f), c_vp, c_vp, c_vp],
     "pf_batch_workspace_size": [ctypes.POINTER(PfBatchView), c_i32, c_i32, ctypes.POINTER(ctypes.c_size_t)],
-    "pf_batch_render": [ctypes.POINTER(PfBatchScene), ctypes.POINTER(PfBatchView), c_i32, c_i32, c_i32, c_i32, c_vp,
-                        ctypes.c_size_t, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp],
+    "pf_batch_render": [ctypes.POINTER(PfBatchScene), ctypes.POINTER(PfBatchView), c_i32, c_i32, c_i32, c_i32, c_i32,
+                        c_vp, ctypes.c_size_t, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp],
     "pf_trace_labels": [ctypes.POINTER(PfTraceInputs), c_f, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp],
     "pf_locator_workspace_size": [c_i64, ctypes.POINTER(ctypes.c_size_t)],
     "pf_locator_build": [c_vp, c_vp, c_i64, c_vp, ctypes.c_size_t, c_vp],

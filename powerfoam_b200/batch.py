@@ -42,7 +42,7 @@ def _pow2_at_least(n):
 
 class BatchStep:
     def __init__(self, device, cameras, tile_width=8, chunk=1, order="longest", transmittance_threshold=1e-3,
-                 headroom=1.25):
+                 headroom=1.25, split=False):
         if not 1 <= len(cameras) <= _lib.PF_BATCH_MAX_VIEWS:
             raise ValueError(f"1..{_lib.PF_BATCH_MAX_VIEWS} views per batch")
         if tile_width not in TILE_WIDTHS:
@@ -54,6 +54,7 @@ class BatchStep:
         self.tile_width = tile_width
         self.chunk = int(chunk)
         self.order = order
+        self.split = bool(split)
         self.thr = float(transmittance_threshold)
         self.headroom = headroom
         self.graph = None
@@ -223,7 +224,7 @@ class BatchStep:
             ev = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
             ev[0].record()
         _lib.call("pf_batch_render", _lib.ctypes.byref(self._scene), self._views, len(self.cameras), self.tile_width,
-                  self.chunk, ORDERS[self.order], _lib.ptr(self.batch_ws), self.batch_ws.numel(),
+                  self.chunk, ORDERS[self.order], int(self.split), _lib.ptr(self.batch_ws), self.batch_ws.numel(),
                   _lib.ptr(self.tile_loss), _lib.ptr(g["points"]), _lib.ptr(g["radii"]), _lib.ptr(g["normals"]),
                   _lib.ptr(g["density"]), _lib.ptr(g["texel_sites"]), _lib.ptr(g["texel_height"]),
                   _lib.ptr(self.status), st)
@@ -262,10 +263,13 @@ class BatchStep:
         self.graph = g
         return g
 
-    def set_schedule(self, chunk=None, order=None):
-        """Change the work-queue chunk / order (drops a captured graph)."""
+    def set_schedule(self, chunk=None, order=None, split=None):
+        """Change the work-queue chunk / order / fused-or-split schedule (drops
+        a captured graph)."""
         if chunk is not None:
             self.chunk = int(chunk)
+        if split is not None:
+            self.split = bool(split)
         if order is not None:
             if order not in ORDERS:
                 raise ValueError(f"order must be one of {sorted(ORDERS)}")
@@ -331,15 +335,16 @@ def time_step(step, iters=3, warmup=1):
 
 
 def autotune(device, cameras, bind_kwargs, tile_widths=TILE_WIDTHS, chunks=CHUNKS, orders=("longest", "view"),
-             iters=3, warmup=1, cache_path=None, use_cache=True, transmittance_threshold=1e-3, log=None,
-             prune=1.3):
-    """Sweep tile width x work-queue chunk x item order over the real step and
-    return (best BatchStep bound and ready, table).  Each candidate is timed
-    with CUDA events over `iters` eager runs after `warmup`.  Tile widths are
-    swept in the given order; once a width's best time exceeds `prune` x the
-    best so far, the remaining widths are skipped (step time grows
-    monotonically with the width on these workloads).  The winner is cached in
-    a JSON file keyed by tune_key(); a cached entry skips the sweep."""
+             splits=(False, True), iters=3, warmup=1, cache_path=None, use_cache=True, transmittance_threshold=1e-3,
+             log=None, prune=1.3):
+    """Sweep tile width x work-queue chunk x item order x fused / split
+    schedule over the real step and return (best BatchStep bound and ready,
+    table).  Each candidate is timed with CUDA events over `iters` eager runs
+    after `warmup`.  Tile widths are swept in the given order; once a width's
+    best time exceeds `prune` x the best so far, the remaining widths are
+    skipped (step time grows monotonically with the width on these
+    workloads).  The winner is cached in a JSON file keyed by tune_key(); a
+    cached entry skips the sweep."""
     cache_path = cache_path or default_cache_path()
     n = bind_kwargs["points"].shape[0]
     S = bind_kwargs["texel_sites"].shape[1]
@@ -351,28 +356,34 @@ def autotune(device, cameras, bind_kwargs, tile_widths=TILE_WIDTHS, chunks=CHUNK
                 cache = json.load(f)
         except (OSError, ValueError):
             cache = {}
+
+    def make(best):
+        step = BatchStep(device, cameras, best["tile_width"], best["chunk"], best["order"], transmittance_threshold,
+                         split=best.get("split", False))
+        step.bind(**bind_kwargs)
+        return step
+
     if use_cache and key in cache:
         best = cache[key]
-        step = BatchStep(device, cameras, best["tile_width"], best["chunk"], best["order"], transmittance_threshold)
-        step.bind(**bind_kwargs)
-        return step, best.get("table", [])
+        return make(best), best.get("table", [])
     table = []
     best = None
     for tw in tile_widths:
         step = BatchStep(device, cameras, tw, 1, "longest", transmittance_threshold)
         step.bind(**bind_kwargs)
-        for order in orders:
-            for ch in chunks:
-                step.set_schedule(chunk=ch, order=order)
-                t0 = time.perf_counter()
-                ms = time_step(step, iters=iters, warmup=warmup)
-                row = {"tile_width": tw, "chunk": ch, "order": order, "ms": ms}
-                table.append(row)
-                if log:
-                    log(f"autotune tile={tw} chunk={ch} order={order}: {ms:.3f} ms "
-                        f"({time.perf_counter() - t0:.1f} s)")
-                if best is None or ms < best["ms"]:
-                    best = dict(row)
+        for split in splits:
+            for order in orders:
+                for ch in chunks:
+                    step.set_schedule(chunk=ch, order=order, split=split)
+                    t0 = time.perf_counter()
+                    ms = time_step(step, iters=iters, warmup=warmup)
+                    row = {"tile_width": tw, "chunk": ch, "order": order, "split": bool(split), "ms": ms}
+                    table.append(row)
+                    if log:
+                        log(f"autotune tile={tw} chunk={ch} order={order} split={bool(split)}: {ms:.3f} ms "
+                            f"({time.perf_counter() - t0:.1f} s)")
+                    if best is None or ms < best["ms"]:
+                        best = dict(row)
         del step
         torch.cuda.empty_cache()
         width_best = min(r["ms"] for r in table if r["tile_width"] == tw)
@@ -390,6 +401,4 @@ def autotune(device, cameras, bind_kwargs, tile_widths=TILE_WIDTHS, chunks=CHUNK
         os.replace(tmp, cache_path)
     except OSError:
         pass
-    step = BatchStep(device, cameras, best["tile_width"], best["chunk"], best["order"], transmittance_threshold)
-    step.bind(**bind_kwargs)
-    return step, table
+    return make(best), table

@@ -58,6 +58,11 @@ struct BatchParams {
     BatchView views[kMaxViews];
 };
 
+union BatchStage {
+    FwdCStage fwd;
+    BwdStage bwd;
+};
+
 struct BatchShared {
     RasterParams P;
     FwdOut out;
@@ -89,22 +94,45 @@ PF_D void load_view(const BatchParams& B, int v, BatchShared& sh) {
     sh.tile_loss = B.tile_loss + V.item_base;
 }
 
-template <int TW>
-__global__ void __launch_bounds__(Layout<TW>::THREADS) batch_step_kernel(const __grid_constant__ BatchParams B) {
+// Phases of one work item: the fused schedule runs the tile's forward, its L2
+// gradient and its adjoint back to back in one launch; the split schedule runs
+// one persistent launch of forwards (+ L2 gradients) over all items, then one
+// of adjoints, each kernel at its own occupancy.
+enum BatchPhase { kFused = 0, kFwdOnly = 1, kBwdOnly = 2 };
+
+template <int TW, int PH>
+struct BatchKernel {
+    static constexpr int MIN_BLOCKS = PH == kFwdOnly ? 1 : Layout<TW>::BWD_MIN_BLOCKS;
+    static constexpr size_t STAGE = PH == kFused    ? sizeof(BatchStage)
+                                    : PH == kBwdOnly ? sizeof(BwdStage)
+                                    : (Layout<TW>::PPL == 1 ? sizeof(FwdCStage) : 0);
+};
+
+template <int TW, int PH>
+__global__ void __launch_bounds__(Layout<TW>::THREADS, BatchKernel<TW, PH>::MIN_BLOCKS)
+batch_step_kernel(const __grid_constant__ BatchParams B) {
     constexpr int G = Layout<TW>::G, PPL = Layout<TW>::PPL;
     constexpr int TS = TW * TW;
+    constexpr bool FWD = PH != kBwdOnly, BWD = PH != kFwdOnly;
     __shared__ WarpStage stage[G];
     __shared__ StopState ss;
     __shared__ BatchShared sh;
     extern __shared__ float4 dyn_smem[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    BwdStage& bs = reinterpret_cast<BwdStage*>(dyn_smem)[warp];
-    for (int r = 0; r < kAccRows; r++) bs.acc[r][lane] = 0.f;
+    // per-warp area: the forward's pair compaction stage (one-pixel-per-lane
+    // layouts) and the adjoint's gradient table, in turn when fused
+    BwdStage& bs = *reinterpret_cast<BwdStage*>(reinterpret_cast<char*>(dyn_smem) + warp * BatchKernel<TW, PH>::STAGE);
+    FwdCStage& fs = *reinterpret_cast<FwdCStage*>(reinterpret_cast<char*>(dyn_smem) + warp * BatchKernel<TW, PH>::STAGE);
+    int* queue = B.queue + (PH == kBwdOnly ? 1 : 0);
+    if (PH == kBwdOnly) {
+        for (int r = 0; r < kAccRows; r++) bs.acc[r][lane] = 0.f;
+        __syncwarp();
+    }
     stop_reset<G>(ss, warp, lane);
     int view = -1;
     for (;;) {
         __syncthreads();
-        if (threadIdx.x == 0) sh.next = atomicAdd(B.queue, B.chunk);
+        if (threadIdx.x == 0) sh.next = atomicAdd(queue, B.chunk);
         __syncthreads();
         const int64_t c0 = sh.next;
         if (c0 >= B.n_items) break;
@@ -119,33 +147,42 @@ __global__ void __launch_bounds__(Layout<TW>::THREADS) batch_step_kernel(const _
                 __syncthreads();
                 view = v;
             }
-            fwd_tile<G, PPL>(sh.P, sh.out, tile, warp, lane, stage[warp], ss);
-            // dL/dcolor of this thread's own pixels (written by it in fwd_tile)
-            float l = 0.f;
+            if constexpr (FWD) {
+                if constexpr (PPL == 1) fwd_tile_c<G>(sh.P, sh.out, tile, warp, lane, fs, ss);
+                else fwd_tile<G, PPL>(sh.P, sh.out, tile, warp, lane, stage[warp], ss);
+                // dL/dcolor of this thread's own pixels (written by it in the forward)
+                float l = 0.f;
 #pragma unroll 1
-            for (int s = 0; s < PPL; s++) {
-                PixGeom g = pixel_geom(sh.P, tile, warp * 32 + lane + s * (TS / 2));
-                if (!g.oob) {
-                    const int64_t p = g.px;
-                    float d0 = sh.out.color[3 * p] - __ldg(&sh.target[3 * p]);
-                    float d1 = sh.out.color[3 * p + 1] - __ldg(&sh.target[3 * p + 1]);
-                    float d2 = sh.out.color[3 * p + 2] - __ldg(&sh.target[3 * p + 2]);
-                    sh.g_color[3 * p] = 2.0f * d0;
-                    sh.g_color[3 * p + 1] = 2.0f * d1;
-                    sh.g_color[3 * p + 2] = 2.0f * d2;
-                    l += d0 * d0 + d1 * d1 + d2 * d2;
+                for (int s = 0; s < PPL; s++) {
+                    PixGeom g = pixel_geom(sh.P, tile, warp * 32 + lane + s * (TS / 2));
+                    if (!g.oob) {
+                        const int64_t p = g.px;
+                        float d0 = sh.out.color[3 * p] - __ldg(&sh.target[3 * p]);
+                        float d1 = sh.out.color[3 * p + 1] - __ldg(&sh.target[3 * p + 1]);
+                        float d2 = sh.out.color[3 * p + 2] - __ldg(&sh.target[3 * p + 2]);
+                        sh.g_color[3 * p] = 2.0f * d0;
+                        sh.g_color[3 * p + 1] = 2.0f * d1;
+                        sh.g_color[3 * p + 2] = 2.0f * d2;
+                        l += d0 * d0 + d1 * d1 + d2 * d2;
+                    }
                 }
+                l = warp_sum(l);
+                if (lane == 0) sh.loss[warp] = l;
+                __syncthreads();  // early_stop, log_t and g_color of the whole tile are written
+                if (threadIdx.x == 0) {
+                    float t = 0.f;
+                    for (int w = 0; w < G; w++) t += sh.loss[w];
+                    sh.tile_loss[tile] = t;
+                }
+                stop_reset<G>(ss, warp, lane);  // ready for the next tile's forward
             }
-            l = warp_sum(l);
-            if (lane == 0) sh.loss[warp] = l;
-            __syncthreads();  // early_stop, log_t and g_color of the whole tile are written
-            if (threadIdx.x == 0) {
-                float t = 0.f;
-                for (int w = 0; w < G; w++) t += sh.loss[w];
-                sh.tile_loss[tile] = t;
+            if constexpr (BWD) {
+                if constexpr (PH == kFused) {
+                    for (int r = 0; r < kAccRows; r++) bs.acc[r][lane] = 0.f;  // the forward used this area
+                    __syncwarp();
+                }
+                bwd_tile<G, PPL>(sh.P, sh.in, sh.go, tile, warp, lane, stage[warp], bs);
             }
-            stop_reset<G>(ss, warp, lane);  // ready for the next tile's forward
-            bwd_tile<G, PPL>(sh.P, sh.in, sh.go, tile, warp, lane, stage[warp], bs);
         }
     }
 }
@@ -197,21 +234,30 @@ inline BatchLayout batch_layout(int64_t n_items) {
     return L;
 }
 
-template <int TW>
-static int launch_batch(const BatchParams& B, cudaStream_t st) {
-    const size_t dyn = sizeof(BwdStage) * Layout<TW>::G;
-    cudaError_t e = cudaFuncSetAttribute(batch_step_kernel<TW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
+template <int TW, int PH>
+static int launch_phase(const BatchParams& B, cudaStream_t st) {
+    const size_t dyn = BatchKernel<TW, PH>::STAGE * Layout<TW>::G;
+    cudaError_t e =
+        cudaFuncSetAttribute(batch_step_kernel<TW, PH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
     if (e != cudaSuccess) return pf_fail(PF_ERR_CUDA, cudaGetErrorString(e));
     int dev = 0, sms = 148, per_sm = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_step_kernel<TW>, Layout<TW>::THREADS, dyn);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_step_kernel<TW, PH>, Layout<TW>::THREADS, dyn);
     if (per_sm < 1) return pf_fail(PF_ERR_CUDA, "pf_batch_render: kernel does not fit on an SM");
     const int64_t items_per_pop = std::max(B.chunk, 1);
     const int64_t pops = (B.n_items + items_per_pop - 1) / items_per_pop;
     const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>((int64_t)sms * per_sm, pops));
-    batch_step_kernel<TW><<<grid, Layout<TW>::THREADS, dyn, st>>>(B);
+    batch_step_kernel<TW, PH><<<grid, Layout<TW>::THREADS, dyn, st>>>(B);
     return PF_OK;
+}
+
+template <int TW>
+static int launch_batch(const BatchParams& B, bool split, cudaStream_t st) {
+    if (!split) return launch_phase<TW, kFused>(B, st);
+    int rc = launch_phase<TW, kFwdOnly>(B, st);
+    if (rc != PF_OK) return rc;
+    return launch_phase<TW, kBwdOnly>(B, st);
 }
 
 static int batch_params(const pf_batch_scene* sc, const pf_batch_view* views, int32_t n_views, int32_t tile_width,
@@ -313,7 +359,7 @@ extern "C" int pf_batch_workspace_size(const pf_batch_view* views, int32_t n_vie
 }
 
 extern "C" int pf_batch_render(const pf_batch_scene* scene, const pf_batch_view* views, int32_t n_views,
-                               int32_t tile_width, int32_t chunk, int32_t order, void* workspace,
+                               int32_t tile_width, int32_t chunk, int32_t order, int32_t split, void* workspace,
                                size_t workspace_bytes, float* tile_loss, float* grad_points, float* grad_radii,
                                float* grad_normals, float* grad_density, float* grad_texel_sites,
                                float* grad_texel_height, int32_t* status, void* stream) {
@@ -349,7 +395,7 @@ extern "C" int pf_batch_render(const pf_batch_scene* scene, const pf_batch_view*
     B.queue = (int*)(ws + L.queue);
     B.status = (int*)status;
     B.tile_loss = tile_loss;
-    cudaMemsetAsync(B.queue, 0, sizeof(int), st);
+    cudaMemsetAsync(B.queue, 0, 2 * sizeof(int), st);
     // work list
     uint32_t* k0 = (uint32_t*)(ws + L.k0);
     uint32_t* v0 = (uint32_t*)(ws + L.v0);
@@ -367,9 +413,9 @@ extern "C" int pf_batch_render(const pf_batch_scene* scene, const pf_batch_view*
     }
     int rc = PF_OK;
     if (B.n_items > 0) {
-        if (tile_width == 8) rc = launch_batch<8>(B, st);
-        else if (tile_width == 16) rc = launch_batch<16>(B, st);
-        else rc = launch_batch<32>(B, st);
+        if (tile_width == 8) rc = launch_batch<8>(B, split != 0, st);
+        else if (tile_width == 16) rc = launch_batch<16>(B, split != 0, st);
+        else rc = launch_batch<32>(B, split != 0, st);
     }
     if (rc != PF_OK) return rc;
     auto sanitize = [&](float* a, size_t n) {

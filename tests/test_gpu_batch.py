@@ -62,11 +62,12 @@ def single_view(sc, adj, adj_off, cam, rgb, target, tw):
     return out, loss, {k: v.grad for k, v in t.items()}, rgb_t.grad, R
 
 
-@pytest.mark.parametrize("tw,chunk,order", [(8, 1, "longest"), (8, 3, "view"), (16, 2, "longest"),
-                                            (32, 1, "longest"), (32, 5, "view")])
-def test_batch_matches_single_view_kernels(tw, chunk, order):
+@pytest.mark.parametrize("tw,chunk,order,split", [(8, 1, "longest", False), (8, 3, "view", True),
+                                                  (16, 2, "longest", False), (16, 1, "view", True),
+                                                  (32, 1, "longest", False), (32, 5, "view", True)])
+def test_batch_matches_single_view_kernels(tw, chunk, order, split):
     sc, adj, adj_off, cams, rgbs, targets = make_case()
-    step = BatchStep("cuda", [torch_cam(c) for c in cams], tile_width=tw, chunk=chunk, order=order)
+    step = BatchStep("cuda", [torch_cam(c) for c in cams], tile_width=tw, chunk=chunk, order=order, split=split)
     step.bind(**bind_kwargs(sc, adj, adj_off, rgbs, targets))
     loss = step.run().clone()
     step.check()
@@ -191,15 +192,16 @@ def test_autotune_sweeps_and_caches(tmp_path):
     kw = bind_kwargs(sc, adj, adj_off, rgbs, targets)
     path = str(tmp_path / "tune.json")
     step, table = autotune("cuda", tcams, kw, tile_widths=(8, 16), chunks=(1, 2), orders=("longest",), iters=1,
-                           warmup=1, cache_path=path)
-    assert len(table) == 4
+                           warmup=1, cache_path=path, prune=0)
+    assert len(table) == 8
     best = min(table, key=lambda r: r["ms"])
-    assert (step.tile_width, step.chunk, step.order) == (best["tile_width"], best["chunk"], best["order"])
+    assert (step.tile_width, step.chunk, step.order, step.split) == (best["tile_width"], best["chunk"],
+                                                                     best["order"], best["split"])
     cache = json.load(open(path))
     key = tune_key(torch.device("cuda"), tcams, sc["points"].shape[0], sc["texel_sites"].shape[1])
     assert cache[key]["tile_width"] == best["tile_width"]
     step2, table2 = autotune("cuda", tcams, kw, tile_widths=(8, 16), chunks=(1, 2), orders=("longest",),
-                             cache_path=path)
+                             cache_path=path, prune=0)
     assert table2 == cache[key]["table"]
     assert (step2.tile_width, step2.chunk) == (step.tile_width, step.chunk)
     step2.run()
