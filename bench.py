@@ -55,7 +55,8 @@ def parse():
     p.add_argument("--workload", default=WORKLOAD, help="raster1m (the measured configuration), raster256k "
                    "(a quarter-size case with the same density per pixel, for profiling), batch3m (32 views of "
                    "a 3.1M-primitive scene in one graph-captured persistent step), batch256k (its small case), "
-                   "trace1m (tracer forward + adjoint) or proposal (proposal-seeded vs plain cell walk)")
+                   "trace1m (tracer forward + adjoint), interpen3m (interpenetration loss forward + adjoint) or proposal "
+                   "(proposal-seeded vs plain cell walk)")
     p.add_argument("--cpu-sample-tiles", type=int, default=0, help="tiles composited by the CPU baseline")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-autotune", action="store_true", help="batch workloads: use --tile, chunk 1")
@@ -615,6 +616,105 @@ def trace_main(args, dev):
     print(json.dumps(line), flush=True)
 
 
+def interpen_main(args, dev):
+    """Interpenetration loss forward + adjoint: the 3,145,728-primitive scene
+    of the batched workload with its Čech adjacency (built on the GPU, once);
+    one step = areas of every sphere, their sum (the trainer's loss term,
+    train.py:277) and the adjoint to points and radii through the autograd
+    mirror."""
+    from oracle import oracle as orc
+    from powerfoam_b200 import synthetic
+    from powerfoam_b200.adjacency import CechBuilder
+    from powerfoam_b200.geometry import InterpenetrationFunction
+
+    cfg = synthetic.CONFIGS["batch3m"]
+    sc = synthetic.make_scene(cfg["n"], seed=cfg["seed"], mixture=cfg["mixture"], sigma=cfg["sigma"],
+                              r_range=cfg["r_range"], device=dev)
+    adj, off = CechBuilder(dev)(sc["points"], sc["radii"])
+    n, e = cfg["n"], adj.numel()
+    pts = sc["points"].clone().requires_grad_(True)
+    radii = sc["radii"].clone().requires_grad_(True)
+    events = {"fwd": [], "bwd": []}
+
+    def step(record=False):
+        pts.grad = None
+        radii.grad = None
+        if record:
+            a0, a1, b1 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+            a0.record()
+        loss = InterpenetrationFunction.apply(pts, radii, adj, off).sum()
+        if record:
+            a1.record()
+        loss.backward()
+        if record:
+            b1.record()
+            events["fwd"].append((a0, a1))
+            events["bwd"].append((a1, b1))
+        return loss
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(int(os.environ.get("LOCAL_RANK", "0")))
+    clocks.start()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    a.record()
+    for _ in range(args.steps):
+        step()
+    b.record()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = a.elapsed_time(b) / args.steps
+    for _ in range(args.steps):
+        step(record=True)
+    torch.cuda.synchronize()
+    fwd_ms = statistics.mean(x.elapsed_time(y) for x, y in events["fwd"])
+    bwd_ms = statistics.mean(x.elapsed_time(y) for x, y in events["bwd"])
+    loss_host = torch.empty(args.steps, dtype=torch.float32).pin_memory()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    for i in range(args.steps):
+        loss_host[i].copy_(step().detach(), non_blocking=True)
+    e1.record()
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1) / args.steps
+    # unique bytes a launch must move: spheres, offsets, lists, areas (or
+    # dL/dareas) and, for the adjoint, the (N,4) gradient written once
+    fwd_bytes = 16 * n + 4 * (n + 1) + 4 * e + 4 * n
+    bwd_bytes = fwd_bytes + 16 * n
+    peak, peak_kind = load_peaks()
+    dom = "bwd" if bwd_ms >= fwd_ms else "fwd"
+    dom_ms, dom_bytes = (bwd_ms, bwd_bytes) if dom == "bwd" else (fwd_ms, fwd_bytes)
+    achieved = dom_bytes / (dom_ms * 1e-3) / 1e9
+    line = dict(metric="interpenetration loss fwd+bwd @3.1M prims", value=1000.0 / ms, unit="iterations/s",
+                n_gpus=1, steps=args.steps, warmup=max(args.warmup, 3), ms_per_step=ms, higher_is_better=True,
+                scaling="weak", vs_baseline=None, dtype="f32", data="synthetic (seeded scene, GPU Čech lists)",
+                config=dict(workload="interpen3m", prims=n, pairs=e, mean_degree=e / n,
+                            l2="inputs larger than L2 (50 MB spheres + lists), no flush"),
+                clocks=clk,
+                e2e=dict(value=1000.0 / e2e_ms, unit="iterations/s", h2d_bytes_per_step=0, d2h_bytes_per_step=4,
+                         note="the scene is training state resident on the device; the loss is read back"),
+                roofline=dict(bound="hbm", kernel="pf_interpenetration" + ("_backward" if dom == "bwd" else ""),
+                              achieved=achieved, peak=peak, unit="GB/s", frac=achieved / peak,
+                              peak_source=peak_kind, traffic=None, algorithmic_bytes=dom_bytes, ms=dom_ms,
+                              fwd_ms=fwd_ms, bwd_ms=bwd_ms),
+                gpu_launches=args.steps * 2)
+    if not args.no_cpu_baseline:
+        sph = torch.cat([sc["points"], sc["radii"][:, None]], -1).cpu().numpy()
+        a_np, o_np = adj.cpu().numpy(), off.cpu().numpy()
+        m = min(n, 1 << 19)
+        t0 = time.perf_counter()
+        orc.interpenetration(sph, a_np, o_np, rows=m)
+        orc.interpenetration_backward(sph, a_np, o_np, np.ones(n, np.float32), rows=m)
+        dt = time.perf_counter() - t0
+        line["cpu_baseline"] = dict(value=(m / n) / dt, unit="iterations/s", cores=1, kind="port",
+                                    sample=f"the lists of the first {m} spheres, forward + adjoint (oracle, one "
+                                           "thread), scaled by the sphere share")
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -634,6 +734,9 @@ def main():
         return
     if args.workload == "trace1m":
         trace_main(args, dev)
+        return
+    if args.workload == "interpen3m":
+        interpen_main(args, dev)
         return
     if args.workload.startswith("batch"):
         batch_main(args, world, rank, local, dev)

@@ -149,6 +149,25 @@ PF_API int pf_cech_adjacency(const float *points, const float *radii, int64_t n_
                              int32_t *adjacency_offsets /* (N+1) */, int64_t *n_edges /* device */,
                              int32_t *status /* device */, void *stream);
 
+/* Interpenetration penalty.  Replaces interpenetration_kernel and
+ * InterpenetrationFunction (powerfoam/geometry.py:88-189).  spheres (N,4) =
+ * (centre, radius), 16-byte aligned; for each i, areas[i] = sum over its list,
+ * in list order, of (r_i + r_j - d)^2 where d = |c_i - c_j| < r_i + r_j
+ * (bit-identical to the reference's loop, with pow(x, 2) as x * x).  The
+ * backward writes dL/dspheres (N,4, zeroed first, 16-byte aligned) given
+ * dL/dareas (N): per overlapping entry g = 2 (r_i + r_j - d) dL/dareas_i to
+ * both radii and, when d > 0, -g (c_i - c_j) / d to c_i and its negative to
+ * c_j (Warp's generated adjoint; summed in no fixed order).  n_edges is
+ * the length of adjacency.  A neighbour index outside [0, N), or offsets that
+ * decrease or leave [0, n_edges], are skipped (clamped) and set PF_ERR_ARGS
+ * in *status (device, may be NULL); the reference has no such check. */
+PF_API int pf_interpenetration(const float *spheres, const int32_t *adjacency, const int32_t *adjacency_offsets,
+                               int64_t n_prims, int64_t n_edges, float *areas, int32_t *status, void *stream);
+PF_API int pf_interpenetration_backward(const float *spheres, const int32_t *adjacency,
+                                        const int32_t *adjacency_offsets, int64_t n_prims, int64_t n_edges,
+                                        const float *grad_areas, float *grad_spheres, int32_t *status,
+                                        void *stream);
+
 /* Morton order of the primitives (stable on equal codes).  Replaces
  * morton_sort (powerfoam/geometry.py:7-85, Warp radix_sort_pairs). */
 PF_API int pf_morton_workspace_size(int64_t n_prims, size_t *bytes);

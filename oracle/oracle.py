@@ -270,6 +270,31 @@ def sh_texel_rgb_backward(points, sh, eye, grad_texel_rgb, grad_sh=None):
     return out
 
 
+def interpenetration(spheres, adj, adj_off, prec="f32", rows=None):
+    """areas (N,) of interpenetration_kernel (geometry.py:88-117); with
+    ``rows`` only the first rows are evaluated (the rest stay 0)."""
+    sph = _c(spheres, F32)
+    N = sph.shape[0]
+    R = np.float64 if prec == "f64" else F32
+    out = np.zeros(N, R)
+    getattr(lib(), f"orc_interpenetration_{prec}")(_p(sph), _p(_c(adj, np.int32)), _p(_c(adj_off, np.int32)),
+                                                   ctypes.c_int64(N if rows is None else rows), _p(out))
+    return out
+
+
+def interpenetration_backward(spheres, adj, adj_off, grad_areas, prec="f32", rows=None):
+    """dL/dspheres (N,4) given dL/dareas (geometry.py:158-189); with ``rows``
+    only the lists of the first rows are replayed."""
+    sph = _c(spheres, F32)
+    N = sph.shape[0]
+    R = np.float64 if prec == "f64" else F32
+    out = np.zeros((N, 4), R)
+    getattr(lib(), f"orc_interpenetration_backward_{prec}")(_p(sph), _p(_c(adj, np.int32)), _p(_c(adj_off, np.int32)),
+                                                            ctypes.c_int64(N if rows is None else rows),
+                                                            _p(_c(grad_areas, F32)), _p(out))
+    return out
+
+
 def num_threads():
     return int(lib().orc_num_threads_f32())
 

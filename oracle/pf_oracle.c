@@ -1448,6 +1448,71 @@ void FN(orc_sh_texel_rgb_backward)(const float *points, const float *sh, int64_t
     }
 }
 
+/* ------------------------------------------------------------------------ */
+/* Interpenetration penalty (powerfoam/geometry.py:88-117): for sphere i,    */
+/* areas_i = sum over its list, in list order from 0, of (s - d)^2 for the    */
+/* entries with d < s, where d = |c_i - c_j| and s = r_i + r_j.  pow(x, 2.0)  */
+/* is taken as x * x.                                                         */
+void FN(orc_interpenetration)(const float *spheres, const int32_t *adj, const int32_t *adj_off, int64_t N,
+                              out_t *areas) {
+    for (int64_t i = 0; i < N; i++) {
+        v3 c = ld3(spheres + 4 * i);
+        real r = (real)spheres[4 * i + 3];
+        real acc = K(0.0);
+        for (int32_t e = adj_off[i]; e < adj_off[i + 1]; e++) {
+            const float *q = spheres + 4 * (int64_t)adj[e];
+            real d = length(vsub(c, ld3(q)));
+            real s = r + (real)q[3];
+            if (d < s) {
+                real x = s - d;
+                acc += x * x;
+            }
+        }
+        areas[i] = acc;
+    }
+}
+
+/* Adjoint of orc_interpenetration as Warp's generated adjoint of the same  */
+/* kernel computes it (InterpenetrationFunction.backward, geometry.py:158-  */
+/* 189): the list is replayed in reverse; per overlapping entry              */
+/* g = (2 (s - d)) dL/dareas_i reaches r_i and r_j; when d > 0 the centre    */
+/* share a = (v / d) (-g), v = c_i - c_j, is added to c_i and subtracted     */
+/* from c_j (length's adjoint is zero at d = 0).  The neighbour's share is   */
+/* added at once, the own share once after the list.  grad_spheres (N,4) is  */
+/* added into.                                                               */
+void FN(orc_interpenetration_backward)(const float *spheres, const int32_t *adj, const int32_t *adj_off, int64_t N,
+                                       const float *grad_areas, out_t *grad_spheres) {
+    for (int64_t i = 0; i < N; i++) {
+        v3 c = ld3(spheres + 4 * i);
+        real r = (real)spheres[4 * i + 3];
+        real ga = (real)grad_areas[i];
+        v3 gc = mk(K(0.0), K(0.0), K(0.0));
+        real gr = K(0.0);
+        for (int32_t e = adj_off[i + 1] - 1; e >= adj_off[i]; e--) {
+            int64_t j = adj[e];
+            const float *q = spheres + 4 * j;
+            v3 v = vsub(c, ld3(q));
+            real d = length(v);
+            real s = r + (real)q[3];
+            if (!(d < s)) continue;
+            real g = (K(2.0) * (s - d)) * ga;
+            gr += g;
+            grad_spheres[4 * j + 3] += g;
+            if (d > K(0.0)) {
+                v3 a = mk((v.x / d) * -g, (v.y / d) * -g, (v.z / d) * -g);
+                gc = vadd(gc, a);
+                grad_spheres[4 * j + 0] -= a.x;
+                grad_spheres[4 * j + 1] -= a.y;
+                grad_spheres[4 * j + 2] -= a.z;
+            }
+        }
+        grad_spheres[4 * i + 0] += gc.x;
+        grad_spheres[4 * i + 1] += gc.y;
+        grad_spheres[4 * i + 2] += gc.z;
+        grad_spheres[4 * i + 3] += gr;
+    }
+}
+
 int FN(orc_num_threads)(void) {
 #ifdef _OPENMP
     return omp_get_max_threads();

@@ -171,6 +171,8 @@ _SIGS = {
     "pf_cech_adjacency": [c_vp, c_vp, c_i64, c_vp, ctypes.c_size_t, c_i64, c_vp, c_vp, c_vp, c_vp, c_vp],
     "pf_morton_workspace_size": [c_i64, ctypes.POINTER(ctypes.c_size_t)],
     "pf_morton_sort": [c_vp, c_i64, c_vp, ctypes.c_size_t, c_vp, c_vp],
+    "pf_interpenetration": [c_vp, c_vp, c_vp, c_i64, c_i64, c_vp, c_vp, c_vp],
+    "pf_interpenetration_backward": [c_vp, c_vp, c_vp, c_i64, c_i64, c_vp, c_vp, c_vp, c_vp],
 }
 
 _lib = None

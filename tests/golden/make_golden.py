@@ -1,6 +1,6 @@
 """Generate golden vectors by executing the reference's own kernel source.
 
-Imports powerfoam/rasterize.py and powerfoam/raytrace.py from the reference
+Imports powerfoam/rasterize.py, raytrace.py and geometry.py from the reference
 checkout (default /root/reference, or $PF_REFERENCE) with warp replaced by
 tests/golden/warp_shim.py, runs the kernels on small seeded scenes, and writes
 tests/golden/*.npz.  Run from the repository root:
@@ -28,12 +28,13 @@ sys.path.insert(0, REF)
 import torch  # noqa: E402
 
 import powerfoam.camera as rcam  # noqa: E402
+import powerfoam.geometry as rgeo  # noqa: E402
 import powerfoam.rasterize as rras  # noqa: E402
 import powerfoam.raytrace as rtrace  # noqa: E402
 import powerfoam.rendering_math as rmath  # noqa: E402
 import powerfoam.texture as rtex  # noqa: E402
 
-for m in (rcam, rras, rtrace, rmath, rtex):
+for m in (rcam, rgeo, rras, rtrace, rmath, rtex):
     warp_shim.patch_module_builtins(m)
 warp_shim.patch_camera_module(rcam, wp)
 
@@ -335,6 +336,34 @@ def trace_case(name, scene, cam, thr=1e-2):
     print(f"{name}: N={spheres.shape[0]} E={adj.shape[0]} start={start} maxlen={maxlen} {time.time() - t0:.1f}s")
 
 
+def interpen_case(name, seed):
+    """interpenetration_kernel (geometry.py:88-117) on overlapping spheres.
+    The lists are the Čech lists (the reference's caller, scene.py:476-482)
+    plus, on every fifth sphere, two far spheres that do not overlap (the
+    d >= r_i + r_j branch), a self entry (d = 0), a pair of spheres with one
+    centre (d = 0 between two spheres) and a sphere with an empty list."""
+    sc = make_scene(seed, 200, -0.5, 0.5, 0.04, 0.16)
+    pts, radii = sc["points"], sc["radii"]
+    pts[1] = pts[0]
+    pts[199] = np.array([3.0, 3.0, 3.0], F32)
+    adj, off = cech_adjacency(pts, radii)
+    rng = np.random.default_rng(seed + 1)
+    lists = [adj[off[i]:off[i + 1]].tolist() for i in range(pts.shape[0])]
+    for i in range(0, 195, 5):
+        far = np.argsort(np.linalg.norm(pts[:195] - pts[i], axis=1))[-2:]
+        lists[i] += far.tolist()
+    lists[7].append(7)
+    assert 1 in lists[0] and not lists[199]
+    adj = np.array([j for l in lists for j in l], np.int32)
+    off = np.concatenate([[0], np.cumsum([len(l) for l in lists])]).astype(np.int32)
+    spheres = np.concatenate([pts, radii[:, None]], -1).astype(F32)
+    areas = np.zeros(pts.shape[0], F32)
+    wp.launch(rgeo.interpenetration_kernel, dim=pts.shape[0], inputs=[spheres, adj, off, areas])
+    np.savez_compressed(os.path.join(HERE, f"{name}.npz"), spheres=spheres, adjacency=adj, adjacency_offsets=off,
+                        areas=areas)
+    print(name, "pairs", adj.shape[0], "overlapping", int((areas > 0).sum()))
+
+
 def edge_scene(seed):
     """Primitives that exercise culling and the tile-range arithmetic: behind
     the camera, closer than 4r, straddling the image border, one covering many
@@ -359,7 +388,7 @@ def edge_scene(seed):
 
 
 def main():
-    which = sys.argv[1:] or ["raster_small", "raster_edge", "bin_large", "trace_small"]
+    which = sys.argv[1:] or ["raster_small", "raster_edge", "raster_dense", "bin_large", "interpen_small", "trace_small"]
     if "raster_small" in which:
         sc = make_scene(1, 120, -0.6, 0.6, 0.05, 0.2)
         raster_case("raster_small", sc, look_at_camera((0.3, 0.4, 2.0), (0, 0, 0), 36, 28, 60.0), 1)
@@ -375,6 +404,8 @@ def main():
     if "bin_large" in which:
         sc = make_scene(3, 3000, -1.0, 1.0, 0.01, 0.08)
         binning_case("bin_large", sc, look_at_camera((1.0, 0.5, 2.6), (0, 0, 0), 96, 64, 50.0))
+    if "interpen_small" in which:
+        interpen_case("interpen_small", 6)
     if "trace_small" in which:
         sc = make_scene(4, 150, -0.6, 0.6, 0.08, 0.2)
         trace_case("trace_small", sc, look_at_camera((0.2, 0.3, 2.2), (0, 0, 0), 24, 20, 60.0))
