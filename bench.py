@@ -55,8 +55,8 @@ def parse():
     p.add_argument("--workload", default=WORKLOAD, help="raster1m (the measured configuration), raster256k "
                    "(a quarter-size case with the same density per pixel, for profiling), batch3m (32 views of "
                    "a 3.1M-primitive scene in one graph-captured persistent step), batch256k (its small case), "
-                   "trace1m (tracer forward + adjoint), interpen3m (interpenetration loss forward + adjoint) or proposal "
-                   "(proposal-seeded vs plain cell walk)")
+                   "trace1m (tracer forward + adjoint), interpen3m (interpenetration loss forward + adjoint), power1m "
+                   "(power-diagram adjacency build) or proposal (proposal-seeded vs plain cell walk)")
     p.add_argument("--cpu-sample-tiles", type=int, default=0, help="tiles composited by the CPU baseline")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-autotune", action="store_true", help="batch workloads: use --tile, chunk 1")
@@ -715,6 +715,72 @@ def interpen_main(args, dev):
     print(json.dumps(line), flush=True)
 
 
+def power_main(args, dev):
+    """Power-diagram adjacency of the 1,048,576-primitive rasterizer scene on
+    the GPU (pf_power_adjacency; one step = one full build: grid, cells,
+    symmetric CSR lists), against the reference's construction (lifted 4-D
+    hull by scipy's Qhull on one host core, benchmark.py:25-83) on a bounded
+    subset."""
+    from powerfoam_b200 import synthetic
+    from powerfoam_b200.adjacency import PowerBuilder, build_power_adjacency
+
+    cfg = synthetic.CONFIGS["raster1m"]
+    sc = synthetic.make_scene(cfg["n"], seed=cfg["seed"], mixture=cfg["mixture"], sigma=cfg["sigma"],
+                              r_range=cfg["r_range"], device=dev)
+    pts, radii = sc["points"], sc["radii"]
+    b = PowerBuilder(dev)
+    for _ in range(max(args.warmup, 3)):
+        adj, off = b(pts, radii)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(int(os.environ.get("LOCAL_RANK", "0")))
+    clocks.start()
+    times = []
+    for _ in range(args.steps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        adj, off = b(pts, radii)
+        e1.record()
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1))
+    clk = clocks.stop()
+    ms = statistics.mean(times)
+    # end to end: host points and radii in, host lists out
+    pts_h, radii_h = pts.cpu().pin_memory(), radii.cpu().pin_memory()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    for _ in range(args.steps):
+        a_d, o_d = b(pts_h.to(dev, non_blocking=True), radii_h.to(dev, non_blocking=True))
+        a_h, o_h = a_d.cpu(), o_d.cpu()
+    e1.record()
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1) / args.steps
+    n, e = cfg["n"], adj.numel()
+    line = dict(metric="power-diagram adjacency build @1M prims", value=1000.0 / ms, unit="builds/s", n_gpus=1,
+                steps=args.steps, warmup=max(args.warmup, 3), ms_per_step=ms, higher_is_better=True, scaling="weak",
+                vs_baseline=None, dtype="f64", data="synthetic (seeded raster1m scene)",
+                config=dict(workload="power1m", prims=n, directed_edges=e, mean_degree=e / n,
+                            l2="compute-bound build; inputs 16 MB, no flush"),
+                clocks=clk,
+                e2e=dict(value=1000.0 / e2e_ms, unit="builds/s", h2d_bytes_per_step=16 * n,
+                         d2h_bytes_per_step=4 * (e + n + 1)),
+                # per build: grid (bounds init, bounds, grid, cell keys, 3 radix passes of 5 kernels, cell
+                # ranges), cell weights 2, cells, symmetrize, count, scan 3, write, offsets
+                gpu_launches=args.steps * (4 + 15 + 1 + 2 + 1 + 1 + 1 + 3 + 1 + 1))
+    if not args.no_cpu_baseline:
+        m = 1 << 17
+        sub = torch.randperm(n, generator=torch.Generator().manual_seed(0))[:m]
+        p_s, r_s = pts.cpu()[sub], radii.cpu()[sub]
+        t0 = time.perf_counter()
+        build_power_adjacency(p_s, r_s)
+        dt = time.perf_counter() - t0
+        line["cpu_baseline"] = dict(value=(m / n) / dt, unit="builds/s", cores=1, kind="reference",
+                                    sample=f"the reference's hull construction (scipy Qhull) on {m} of the {n} "
+                                           "primitives, scaled by the point share (Qhull is superlinear, so this "
+                                           "overstates its full-size rate)")
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -737,6 +803,9 @@ def main():
         return
     if args.workload == "interpen3m":
         interpen_main(args, dev)
+        return
+    if args.workload == "power1m":
+        power_main(args, dev)
         return
     if args.workload.startswith("batch"):
         batch_main(args, world, rank, local, dev)

@@ -33,6 +33,7 @@ extern "C" {
 #define PF_ERR_ARGS 3      /* invalid argument */
 #define PF_ERR_CUDA 4      /* CUDA launch / runtime error */
 #define PF_ERR_SEED 5      /* a proposal seed landed outside every cell */
+#define PF_ERR_CELL 6      /* a power cell exceeded its plane / neighbour capacity */
 
 #define PF_ABI_VERSION 1
 
@@ -167,6 +168,22 @@ PF_API int pf_interpenetration_backward(const float *spheres, const int32_t *adj
                                         const int32_t *adjacency_offsets, int64_t n_prims, int64_t n_edges,
                                         const float *grad_areas, float *grad_spheres, int32_t *status,
                                         void *stream);
+
+/* Power-diagram (weighted Delaunay) adjacency on the GPU.  Replaces
+ * build_power_adjacency (benchmark.py:25-83: lifted 4-D convex hull by Qhull
+ * on the host, lower facets, tetrahedron edges, optional alpha_complex filter
+ * |c_i - c_j| < r_i + r_j) by clipping each site's power cell with its
+ * neighbours' radical planes in double precision.  The lists hold the
+ * reference's neighbour sets, ascending and without the repeats its
+ * torch.unique over unordered pairs leaves.  A cell with more than 96
+ * neighbours or 128 live planes sets PF_ERR_CELL in *status; *n_edges and
+ * edge overflow behave as in pf_cech_adjacency.  Exact duplicate sites (same
+ * centre and radius) both keep their cells, where the hull keeps one. */
+PF_API int pf_power_workspace_size(int64_t n_prims, size_t *bytes);
+PF_API int pf_power_adjacency(const float *points, const float *radii, int64_t n_prims, int32_t alpha_complex,
+                              void *workspace, size_t workspace_bytes, int64_t edge_capacity,
+                              int32_t *adjacency /* (capacity) */, int32_t *adjacency_offsets /* (N+1) */,
+                              int64_t *n_edges /* device */, int32_t *status /* device */, void *stream);
 
 /* Morton order of the primitives (stable on equal codes).  Replaces
  * morton_sort (powerfoam/geometry.py:7-85, Warp radix_sort_pairs). */

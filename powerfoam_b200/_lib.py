@@ -20,6 +20,7 @@ PF_ERR_STEP_CAP = 2
 PF_ERR_ARGS = 3
 PF_ERR_CUDA = 4
 PF_ERR_SEED = 5
+PF_ERR_CELL = 6
 
 _ERR_NAMES = {
     PF_ERR_OVERFLOW: "PF_ERR_OVERFLOW",
@@ -27,6 +28,7 @@ _ERR_NAMES = {
     PF_ERR_ARGS: "PF_ERR_ARGS",
     PF_ERR_CUDA: "PF_ERR_CUDA",
     PF_ERR_SEED: "PF_ERR_SEED",
+    PF_ERR_CELL: "PF_ERR_CELL",
 }
 
 c_f = ctypes.c_float
@@ -171,6 +173,9 @@ _SIGS = {
     "pf_cech_adjacency": [c_vp, c_vp, c_i64, c_vp, ctypes.c_size_t, c_i64, c_vp, c_vp, c_vp, c_vp, c_vp],
     "pf_morton_workspace_size": [c_i64, ctypes.POINTER(ctypes.c_size_t)],
     "pf_morton_sort": [c_vp, c_i64, c_vp, ctypes.c_size_t, c_vp, c_vp],
+    "pf_power_workspace_size": [c_i64, c_vp],
+    "pf_power_adjacency": [c_vp, c_vp, c_i64, ctypes.c_int32, c_vp, ctypes.c_size_t, c_i64, c_vp, c_vp, c_vp, c_vp,
+                           c_vp],
     "pf_interpenetration": [c_vp, c_vp, c_vp, c_i64, c_i64, c_vp, c_vp, c_vp],
     "pf_interpenetration_backward": [c_vp, c_vp, c_vp, c_i64, c_i64, c_vp, c_vp, c_vp, c_vp],
 }

@@ -7,6 +7,8 @@
 * ``build_power_adjacency`` -- weighted-Delaunay edges through the lower hull
   of the lifted points (benchmark.py:25-83), via scipy's Qhull on the host, as
   the reference does; meant for small scenes.
+* ``power_adjacency`` / ``PowerBuilder`` -- the same edges on the GPU by
+  clipping power cells (pf_power_adjacency).
 """
 
 import numpy as np
@@ -42,7 +44,9 @@ def build_power_adjacency(points, radii, alpha_complex=False):
     to 4-D, keep the facets of the convex hull whose normal points down in the
     lifted coordinate, take the tetrahedra's edges; with ``alpha_complex`` keep
     only edges whose balls overlap.  Returns (adjacency int32 (E), offsets int32
-    (N+1)) grouped by source vertex (neighbours ascending)."""
+    (N+1)) grouped by source vertex, neighbours ascending and without the
+    repeats the reference's lists carry (it runs torch.unique over unordered
+    pairs, so an edge two tetrahedra name in opposite orders appears twice)."""
     from scipy.spatial import ConvexHull
 
     p = points.detach().cpu().double()
@@ -99,6 +103,51 @@ class CechBuilder:
             cap = min(1 << (int(e * 1.25) - 1).bit_length(), (1 << 31) - 1)
         self.capacity = max(self.capacity, cap)
         return adj[:e], off
+
+
+class PowerBuilder:
+    """GPU power-diagram adjacency (pf_power_adjacency): the neighbour sets of
+    build_power_adjacency (benchmark.py:25-83) without the host hull, lists
+    ascending.  Like CechBuilder it reads the edge count once to size the
+    output; a cell beyond the kernel's capacity raises PF_ERR_CELL."""
+
+    def __init__(self, device):
+        self.device = torch.device(device)
+        self.ws = None
+        self.capacity = 0
+
+    def __call__(self, points, radii, alpha_complex=False):
+        points = points.float().contiguous()
+        radii = radii.float().contiguous()
+        n = points.shape[0]
+        nbytes = _lib.ctypes.c_size_t(0)
+        _lib.call("pf_power_workspace_size", n, _lib.ctypes.byref(nbytes))
+        if self.ws is None or self.ws.numel() < nbytes.value:
+            self.ws = torch.empty(nbytes.value, dtype=torch.uint8, device=self.device)
+        cap = max(self.capacity, 20 * n, 1 << 16)
+        while True:
+            adj = torch.empty(cap, dtype=torch.int32, device=self.device)
+            off = torch.empty(n + 1, dtype=torch.int32, device=self.device)
+            scalars = torch.zeros(2, dtype=torch.int64, device=self.device)
+            status = scalars[1:].view(torch.int32)[:1]
+            _lib.call("pf_power_adjacency", _lib.ptr(points), _lib.ptr(radii), n, int(bool(alpha_complex)),
+                      _lib.ptr(self.ws), self.ws.numel(), cap, _lib.ptr(adj), _lib.ptr(off), _lib.ptr(scalars[:1]),
+                      _lib.ptr(status), _lib.stream_ptr())
+            e, st = (int(v) for v in torch.stack([scalars[0], status[0].long()]).tolist())
+            if st == _lib.PF_ERR_CELL:
+                raise _lib.PfError(st, "a power cell exceeded the kernel's plane / neighbour capacity")
+            if e <= cap:
+                break
+            if e >= (1 << 31) - 1:
+                raise _lib.PfError(_lib.PF_ERR_OVERFLOW, f"{e} adjacency entries exceed int32 offsets")
+            cap = min(1 << (int(e * 1.25) - 1).bit_length(), (1 << 31) - 1)
+        self.capacity = max(self.capacity, cap)
+        return adj[:e], off
+
+
+def power_adjacency(points, radii, alpha_complex=False):
+    """build_power_adjacency on the GPU (the same neighbour sets)."""
+    return PowerBuilder(points.device)(points, radii, alpha_complex)
 
 
 def cech_adjacency(points, radii):

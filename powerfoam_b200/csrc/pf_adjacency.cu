@@ -20,13 +20,10 @@
 #include "pf_common.cuh"
 #include "pf_sort.cuh"
 #include "pf_api.h"
+#include "pf_power.cuh"
 
 namespace pf {
 
-struct CechGrid {
-    float lo_x, lo_y, lo_z, inv_h;
-    int nx, ny, nz;
-};
 
 __global__ void bounds_kernel(const float* __restrict__ pts, const float* __restrict__ radii, int64_t N,
                               float* __restrict__ out /* lo3, hi3, rmax */) {
@@ -281,13 +278,13 @@ __global__ void gather_u32_kernel(const uint32_t* __restrict__ src, const uint32
 // Cell location: the power cell containing a point x is the primitive that
 // minimises |x - p_i|^2 - r_i^2 (the cell of benchmark.py:320-324 for an
 // arbitrary point).  Primitives are bucketed in a uniform grid of about four
-// per cell; a query scans shells of grid cells around x's cell and stops once
+// per cell (pts_per_cell); a query scans shells of grid cells around x's cell and stops once
 // every unscanned primitive lies at least s * h away, i.e. its power distance
 // is at least (s h)^2 - rmax^2 >= the best found.  Ties go to the lower index.
 constexpr int kLocateMaxShell = 48;
 
 __global__ void locate_grid_kernel(const float* __restrict__ bkeys, int64_t N, int max_cells_log2,
-                                   CechGrid* __restrict__ g, float* __restrict__ rmax_out) {
+                                   CechGrid* __restrict__ g, float* __restrict__ rmax_out, float pts_per_cell) {
     const int* k = (const int*)bkeys;
     float lo[3], hi[3];
     for (int i = 0; i < 3; i++) {
@@ -297,7 +294,7 @@ __global__ void locate_grid_kernel(const float* __restrict__ bkeys, int64_t N, i
     *rmax_out = from_key(k[6]);
     double vol = 1.0;
     for (int i = 0; i < 3; i++) vol *= fmax((double)(hi[i] - lo[i]), 1e-6);
-    float h = (float)cbrt(vol * 4.0 / (double)(N > 0 ? N : 1));
+    float h = (float)cbrt(vol * (double)pts_per_cell / (double)(N > 0 ? N : 1));
     h = fmaxf(h, 1e-6f);
     g->nx = g->ny = g->nz = 1;
     for (int it = 0; it < 256; it++) {
@@ -412,6 +409,124 @@ __global__ void seed_kernel(Locator L, Cam cam, const float* __restrict__ t_entr
     if ((threadIdx.x & 31) == 0 && b && n_seeded) atomicAdd(n_seeded, __popc(b));
 }
 
+// ---------------------------------------------------------------------------
+// Power-diagram adjacency (replaces build_power_adjacency, benchmark.py:25-83):
+// every site clips its own power cell (pf_power.cuh) into a fixed slab of
+// neighbours; edges seen from one side only are added to the other side (the
+// hull's edges are undirected), the optional alpha_complex filter keeps the
+// pairs whose balls overlap, and the lists are counted, scanned and written
+// as CSR, ascending per site.
+
+// per grid cell, the largest squared radius of its sites (non-negative
+// floats order as their bit patterns)
+__global__ void cell_weight_kernel(const float* __restrict__ pts, const float* __restrict__ radii, int64_t N,
+                                   const CechGrid* __restrict__ gp, float* __restrict__ cell_w) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    const CechGrid g = *gp;
+    const int cx = cell_coord(pts[3 * i], g.lo_x, g.inv_h, g.nx);
+    const int cy = cell_coord(pts[3 * i + 1], g.lo_y, g.inv_h, g.ny);
+    const int cz = cell_coord(pts[3 * i + 2], g.lo_z, g.inv_h, g.nz);
+    const float w = radii[i] * radii[i];
+    atomicMax((int*)cell_w + ((int64_t)cz * g.ny + cy) * g.nx + cx, __float_as_int(w));
+}
+
+// per block of kPcSuper^3 grid cells, the largest cell weight (-1 bits: no site)
+__global__ void super_weight_kernel(const CechGrid* __restrict__ gp, const int32_t* __restrict__ cell_start,
+                                    const float* __restrict__ cell_w, int* __restrict__ super_w) {
+    const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const CechGrid g = *gp;
+    if (c >= (int64_t)g.nx * g.ny * g.nz || cell_start[c] == cell_start[c + 1]) return;
+    const int x = (int)(c % g.nx), y = (int)((c / g.nx) % g.ny), z = (int)(c / ((int64_t)g.nx * g.ny));
+    const int snx = (g.nx + kPcSuper - 1) / kPcSuper, sny = (g.ny + kPcSuper - 1) / kPcSuper;
+    atomicMax(super_w + ((int64_t)(z / kPcSuper) * sny + y / kPcSuper) * snx + x / kPcSuper,
+              __float_as_int(cell_w[c]));
+}
+
+__global__ void __launch_bounds__(64) power_cell_kernel(PowerScene S, int64_t N, int32_t* __restrict__ slab,
+                                                        int32_t* __restrict__ counts, int32_t* __restrict__ status) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    PowerCell C;
+    bool full = false;
+    counts[i] = power_site(S, i, C, slab + i * kPowerSlab, &full);
+    if (full && status) atomicMax(status, PF_ERR_CELL);
+}
+
+PF_D bool slab_has(const int32_t* a, int n, int32_t v) {
+    int lo = 0, hi = n;
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (a[mid] < v) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo < n && a[lo] == v;
+}
+
+// an edge i -> j that j's list lacks goes to j's extra slots
+__global__ void power_symmetrize_kernel(const int32_t* __restrict__ slab, const int32_t* __restrict__ counts, int64_t N,
+                                        int32_t* __restrict__ extra, int32_t* __restrict__ extra_n,
+                                        int32_t* __restrict__ status) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    const int32_t* a = slab + i * kPowerSlab;
+    for (int k = 0; k < counts[i]; k++) {
+        const int32_t j = a[k];
+        if (slab_has(slab + (int64_t)j * kPowerSlab, counts[j], (int32_t)i)) continue;
+        const int slot = atomicAdd(extra_n + j, 1);
+        if (slot < kPowerExtra) extra[(int64_t)j * kPowerExtra + slot] = (int32_t)i;
+        else if (status) atomicMax(status, PF_ERR_CELL);
+    }
+}
+
+// alpha_complex filter (benchmark.py:62-68): |p_i - p_j| < r_i + r_j
+PF_D bool power_keep(const float* pts, const float* radii, int64_t i, int64_t j, bool alpha) {
+    if (!alpha) return true;
+    double d2 = 0.0;
+    for (int k = 0; k < 3; k++) {
+        const double e = (double)pts[3 * i + k] - (double)pts[3 * j + k];
+        d2 += e * e;
+    }
+    return sqrt(d2) < (double)radii[i] + (double)radii[j];
+}
+
+// WRITE = false: the length of each final list; true: the lists
+template <bool WRITE>
+__global__ void power_emit_kernel(const float* __restrict__ pts, const float* __restrict__ radii,
+                                  const int32_t* __restrict__ slab, const int32_t* __restrict__ counts,
+                                  const int32_t* __restrict__ extra, const int32_t* __restrict__ extra_n, int64_t N,
+                                  int alpha, int32_t* __restrict__ out_counts, const int64_t* __restrict__ offsets,
+                                  const int64_t* __restrict__ total, int64_t capacity, int32_t* __restrict__ adj) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    if (WRITE && *total > capacity) return;
+    const int32_t* a = slab + i * kPowerSlab;
+    const int na = counts[i];
+    const int nx = min(extra_n[i], kPowerExtra);
+    int32_t ex[kPowerExtra];
+    for (int k = 0; k < nx; k++) ex[k] = extra[i * kPowerExtra + k];
+    for (int u = 1; u < nx; u++) {
+        const int32_t v = ex[u];
+        int w = u - 1;
+        while (w >= 0 && ex[w] > v) {
+            ex[w + 1] = ex[w];
+            w--;
+        }
+        ex[w + 1] = v;
+    }
+    const int64_t pos = WRITE ? offsets[i] : 0;
+    int n = 0, ia = 0, ix = 0;
+    while (ia < na || ix < nx) {
+        int32_t v;
+        if (ix >= nx || (ia < na && a[ia] < ex[ix])) v = a[ia++];
+        else v = ex[ix++];
+        if (!power_keep(pts, radii, i, v, alpha != 0)) continue;
+        if (WRITE) adj[pos + n] = v;
+        n++;
+    }
+    if (!WRITE) out_counts[i] = n;
+}
+
 static size_t align_up(size_t x) { return (x + 255) & ~(size_t)255; }
 
 struct CechLayout {
@@ -515,30 +630,36 @@ extern "C" int pf_locator_workspace_size(int64_t n_prims, size_t* bytes) {
     return pf_cech_workspace_size(n_prims, bytes);
 }
 
-extern "C" int pf_locator_build(const float* points, const float* radii, int64_t n_prims, void* workspace,
-                                size_t workspace_bytes, void* stream) {
-    if (n_prims <= 0 || n_prims >= ((int64_t)1 << 31) || !points || !radii)
-        return pf_fail(PF_ERR_ARGS, "pf_locator_build: bad arguments");
-    CechLayout L = cech_layout(n_prims);
-    if (!workspace || workspace_bytes < L.bytes) return pf_fail(PF_ERR_ARGS, "pf_locator_build: workspace too small");
-    cudaStream_t st = (cudaStream_t)stream;
-    char* ws = (char*)workspace;
+// grid over the bounds with about pts_per_cell primitives per cell, the ids
+// sorted by cell and the per-cell ranges (the locator's and the power
+// build's)
+static void build_point_grid(const float* points, const float* radii, int64_t N, char* ws, float pts_per_cell,
+                             cudaStream_t st) {
+    const CechLayout L = cech_layout(N);
     float* bounds = (float*)(ws + L.bounds);
     CechGrid* grid = (CechGrid*)(ws + L.grid);
     uint32_t *key0 = (uint32_t*)(ws + L.key0), *idx0 = (uint32_t*)(ws + L.idx0);
     uint32_t *key1 = (uint32_t*)(ws + L.key1), *idx1 = (uint32_t*)(ws + L.idx1);
     int32_t* cell_start = (int32_t*)(ws + L.cell_start);
     RadixScratch rs{(uint32_t*)(ws + L.rhist), (uint32_t*)(ws + L.rpart)};
-    const int64_t N = n_prims;
     const unsigned gN = (unsigned)((N + 255) / 256);
     bounds_init_kernel<<<1, 1, 0, st>>>(bounds);
     bounds_kernel<<<(unsigned)std::min<int64_t>(gN, 148 * 8), 256, 0, st>>>(points, radii, N, bounds);
-    locate_grid_kernel<<<1, 1, 0, st>>>(bounds, N, kMaxCellsLog2, grid, bounds + 8);
+    locate_grid_kernel<<<1, 1, 0, st>>>(bounds, N, kMaxCellsLog2, grid, bounds + 8, pts_per_cell);
     cell_key_kernel<<<gN, 256, 0, st>>>(points, N, grid, key0, idx0);
     uint32_t* kf = radix_final_key_buffer(key0, key1, kMaxCellsLog2);
     uint32_t* vf = kf == key0 ? idx0 : idx1;
     radix_sort_pairs(key0, idx0, key1, idx1, kf, vf, N, nullptr, kMaxCellsLog2, rs, st);
     cell_ranges_kernel<<<(unsigned)((N + 1 + 255) / 256), 256, 0, st>>>(kf, N, grid, cell_start);
+}
+
+extern "C" int pf_locator_build(const float* points, const float* radii, int64_t n_prims, void* workspace,
+                                size_t workspace_bytes, void* stream) {
+    if (n_prims <= 0 || n_prims >= ((int64_t)1 << 31) || !points || !radii)
+        return pf_fail(PF_ERR_ARGS, "pf_locator_build: bad arguments");
+    CechLayout L = cech_layout(n_prims);
+    if (!workspace || workspace_bytes < L.bytes) return pf_fail(PF_ERR_ARGS, "pf_locator_build: workspace too small");
+    build_point_grid(points, radii, n_prims, (char*)workspace, 4.0f, (cudaStream_t)stream);
     return pf_check_launch("pf_locator_build");
 }
 
@@ -609,4 +730,79 @@ extern "C" int pf_morton_sort(const float* points, int64_t n_prims, void* worksp
     gather_u32_kernel<<<gN, 256, 0, st>>>(hi, idx0, N, hi_s);
     radix_sort_pairs(hi_s, idx0, k1, idx1, hi_s, (uint32_t*)permutation, N, nullptr, 32, rs, st);
     return pf_check_launch("pf_morton_sort");
+}
+
+struct PowerLayout {
+    size_t slab, counts, extra, extra_n, cell_w, super_w, bytes;
+};
+
+static PowerLayout power_layout(int64_t N) {
+    PowerLayout P;
+    size_t o = cech_layout(N).bytes;
+    auto take = [&](size_t b) {
+        size_t r = o;
+        o = align_up(o + b);
+        return r;
+    };
+    P.slab = take(4 * (size_t)kPowerSlab * (size_t)N);
+    P.counts = take(4 * (size_t)N);
+    P.extra = take(4 * (size_t)kPowerExtra * (size_t)N);
+    P.extra_n = take(4 * (size_t)N);
+    P.cell_w = take(4 * ((size_t)1 << kMaxCellsLog2));
+    P.super_w = take(4 * ((size_t)1 << kMaxCellsLog2));
+    P.bytes = o;
+    return P;
+}
+
+extern "C" int pf_power_workspace_size(int64_t n_prims, size_t* bytes) {
+    if (!bytes || n_prims < 0 || n_prims >= ((int64_t)1 << 31))
+        return pf_fail(PF_ERR_ARGS, "pf_power_workspace_size: bad arguments");
+    *bytes = power_layout(n_prims).bytes;
+    return PF_OK;
+}
+
+extern "C" int pf_power_adjacency(const float* points, const float* radii, int64_t n_prims, int32_t alpha_complex,
+                                  void* workspace, size_t workspace_bytes, int64_t edge_capacity, int32_t* adjacency,
+                                  int32_t* adjacency_offsets, int64_t* n_edges, int32_t* status, void* stream) {
+    if (n_prims <= 0 || n_prims >= ((int64_t)1 << 31) || !points || !radii || !adjacency_offsets || !n_edges ||
+        !status || edge_capacity < 0 || edge_capacity >= ((int64_t)1 << 31) || (edge_capacity > 0 && !adjacency))
+        return pf_fail(PF_ERR_ARGS, "pf_power_adjacency: bad arguments");
+    const PowerLayout P = power_layout(n_prims);
+    if (!workspace || workspace_bytes < P.bytes) return pf_fail(PF_ERR_ARGS, "pf_power_adjacency: workspace too small");
+    cudaStream_t st = (cudaStream_t)stream;
+    char* ws = (char*)workspace;
+    const CechLayout L = cech_layout(n_prims);
+    const int64_t N = n_prims;
+    build_point_grid(points, radii, N, ws, kPowerPtsPerCell, st);
+    const Locator loc = locator_view(points, radii, N, ws);
+    float* cell_w = (float*)(ws + P.cell_w);
+    int* super_w = (int*)(ws + P.super_w);
+    int32_t* slab = (int32_t*)(ws + P.slab);
+    int32_t* counts = (int32_t*)(ws + P.counts);
+    int32_t* extra = (int32_t*)(ws + P.extra);
+    int32_t* extra_n = (int32_t*)(ws + P.extra_n);
+    int32_t* out_counts = (int32_t*)(ws + L.counts);
+    int64_t* off64 = (int64_t*)(ws + L.off64);
+    int64_t* spart = (int64_t*)(ws + L.spart);
+    const size_t grid_bytes = 4 * ((size_t)1 << kMaxCellsLog2);
+    if (cudaMemsetAsync(cell_w, 0, grid_bytes, st) != cudaSuccess ||
+        cudaMemsetAsync(super_w, 0xff, grid_bytes, st) != cudaSuccess ||
+        cudaMemsetAsync(extra_n, 0, 4 * (size_t)N, st) != cudaSuccess)
+        return pf_check_launch("pf_power_adjacency");
+    const unsigned gN = (unsigned)((N + 255) / 256);
+    cell_weight_kernel<<<gN, 256, 0, st>>>(points, radii, N, loc.grid, cell_w);
+    super_weight_kernel<<<(unsigned)(((int64_t)1 << kMaxCellsLog2) / 256), 256, 0, st>>>(loc.grid, loc.cell_start,
+                                                                                          cell_w, super_w);
+    PowerScene S{points, radii, loc.grid, loc.cell_start, loc.sorted, (const float*)(ws + L.bounds), cell_w,
+                 (const float*)super_w};
+    power_cell_kernel<<<(unsigned)((N + 63) / 64), 64, 0, st>>>(S, N, slab, counts, status);
+    power_symmetrize_kernel<<<gN, 256, 0, st>>>(slab, counts, N, extra, extra_n, status);
+    power_emit_kernel<false><<<gN, 256, 0, st>>>(points, radii, slab, counts, extra, extra_n, N, alpha_complex,
+                                                 out_counts, nullptr, nullptr, 0, nullptr);
+    exclusive_scan<int32_t, int64_t>(out_counts, off64, N, spart, n_edges, st);
+    power_emit_kernel<true><<<gN, 256, 0, st>>>(points, radii, slab, counts, extra, extra_n, N, alpha_complex, nullptr,
+                                                off64, n_edges, edge_capacity, adjacency);
+    offsets_i32_kernel<<<(unsigned)((N + 1 + 255) / 256), 256, 0, st>>>(off64, N, n_edges, edge_capacity,
+                                                                        adjacency_offsets, status);
+    return pf_check_launch("pf_power_adjacency");
 }
