@@ -458,7 +458,7 @@ def proposal_main(args, dev):
     frame against the plain one, and the same for seeding from the plain
     walk's own labels (the bound a perfect proposal reaches)."""
     from powerfoam_b200 import synthetic
-    from powerfoam_b200.adjacency import build_power_adjacency, power_adjacency_diff, start_cell
+    from powerfoam_b200.adjacency import power_adjacency, power_adjacency_diff, start_cell
     from powerfoam_b200.proposal import ProposalNet, SeededTracer, make_training_rays, trace_labels
     from powerfoam_b200.raytrace import RayTracer
 
@@ -471,7 +471,7 @@ def proposal_main(args, dev):
     sc = synthetic.make_scene(cfg["n"], seed=cfg["seed"], mixture=cfg["mixture"], sigma=cfg["sigma"],
                               r_range=cfg["r_range"], device=dev)
     t0 = time.perf_counter()
-    adj, off = build_power_adjacency(sc["points"], sc["radii"])
+    adj, off = power_adjacency(sc["points"], sc["radii"])
     log(f"power adjacency {time.perf_counter() - t0:.1f} s, {adj.shape[0]} edges")
     pm = power_adjacency_diff(sc["points"], sc["radii"], adj, off)
     ev = synthetic.orbit_camera(4242, cfg["width"], cfg["height"], cfg["vfov"], device=dev)
@@ -539,20 +539,21 @@ def proposal_main(args, dev):
 
 def trace_main(args, dev):
     """Tracer forward + adjoint (config 2): the 1,048,576-primitive scene of
-    the rasterizer workload with its power-diagram adjacency (Qhull on the
-    host, once), one 1280x720 camera on the radius-3 orbit at a seeded
+    the rasterizer workload with its power-diagram adjacency (built on the
+    GPU once, the neighbour sets of the reference's hull construction), one 1280x720 camera on the radius-3 orbit at a seeded
     azimuth / elevation, walks from the camera's cell; one step = the walk
     (colour, log transmittance, depth, normal), an L2 loss against a seeded
     uniform target and the hand-written adjoint to every primitive gradient."""
     from powerfoam_b200 import synthetic
-    from powerfoam_b200.adjacency import build_power_adjacency, power_adjacency_diff, start_cell
+    from powerfoam_b200.adjacency import power_adjacency, power_adjacency_diff, start_cell
     from powerfoam_b200.raytrace import RayTracer
 
     cfg = synthetic.CONFIGS["trace1m"]
     sc = synthetic.make_scene(cfg["n"], seed=cfg["seed"], mixture=cfg["mixture"], sigma=cfg["sigma"],
                               r_range=cfg["r_range"], device=dev)
     t0 = time.perf_counter()
-    adj, off = build_power_adjacency(sc["points"], sc["radii"])
+    adj, off = power_adjacency(sc["points"], sc["radii"])
+    torch.cuda.synchronize()
     adj_s = time.perf_counter() - t0
     pm = power_adjacency_diff(sc["points"], sc["radii"], adj, off)
     cam = synthetic.orbit_camera(2, cfg["width"], cfg["height"], cfg["vfov"], device=dev)

@@ -38,9 +38,9 @@
 
 namespace pf {
 
-constexpr int kPcPlanes = 128;              // live planes of one cell (plane ids fit a byte)
+constexpr int kPcPlanes = 255;              // live planes of one cell (plane ids fit a byte)
 constexpr int kPcTris = 2 * kPcPlanes - 4;  // vertices of a cell with kPcPlanes faces
-constexpr int kPowerSlab = 96;              // neighbours written per site
+constexpr int kPowerSlab = 192;             // neighbours written per site
 constexpr int kPowerExtra = 4;              // one-sided edges added to a site's list
 constexpr int kPcWarm = 32;                 // warm-start planes
 constexpr int kPcSuper = 8;                 // grid cells per block edge in the coarse walk
@@ -73,7 +73,7 @@ struct PowerCell {
     double v[kPcTris][3];
     double vn2[kPcTris];
     uint8_t out[kPcTris];
-    uint8_t ol[kPcTris];  // triangles beyond the clipping plane
+    uint16_t ol[kPcTris];  // triangles beyond the clipping plane
     uint8_t bnd[kPcTris * 3][2];
     double wkey[kPcWarm];  // warm-start candidates, nearest plane first
     int32_t wid[kPcWarm];
@@ -173,7 +173,7 @@ static __host__ __device__ __noinline__ bool pc_clip(PowerCell& C, double nx, do
     for (int t = 0; t < C.nt; t++) {
         const bool o = nx * C.v[t][0] + ny * C.v[t][1] + nz * C.v[t][2] > c;
         C.out[t] = o;
-        if (o) C.ol[n_out++] = (uint8_t)t;
+        if (o) C.ol[n_out++] = (uint16_t)t;
     }
     if (n_out == 0) return false;
     if (n_out == C.nt) {
