@@ -111,9 +111,44 @@ def power_adjacency_diff(points, radii, adj, adj_off):
     return out
 
 
+def _cam_args(cam, ray_maps, name, prec):
+    """(function, leading camera arguments): the generic-camera variant takes
+    the ray maps (H,W,6) after the camera."""
+    if ray_maps is None:
+        return _fn(name, prec), [ctypes.byref(cam)]
+    rm = _c(ray_maps, F32)
+    return _fn(name + "_generic", prec), [ctypes.byref(cam), _p(rm), rm]
+
+
+def bin_generic(cam, ray_maps, spheres, tile_width=8, prec="f32"):
+    """Generic-camera binning through the cone hierarchy: sorted (key, prim)
+    pairs, per-tile offsets, per-prim tile counts and the cones (n, 4)."""
+    spheres = _c(spheres, F32)
+    rm = _c(ray_maps, F32)
+    N = spheres.shape[0]
+    T = (1 + (cam.height - 1) // tile_width) * (1 + (cam.width - 1) // tile_width)
+    n = ctypes.c_int64(0)
+    nc = ctypes.c_int64(0)
+    counts = np.zeros(N, np.int32)
+    offs = np.zeros(T + 1, np.int64)
+    R = np.float64 if prec == "f64" else F32
+    f = _fn("orc_bin_generic", prec)
+    f(ctypes.byref(cam), _p(rm), _p(spheres), ctypes.c_int64(N), ctypes.c_int(tile_width), ctypes.c_int64(0), None,
+      None, _p(offs), _p(counts), ctypes.byref(n), None, ctypes.byref(nc))
+    keys = np.zeros(max(n.value, 1), np.int64)
+    prims = np.zeros(max(n.value, 1), np.int32)
+    cones = np.zeros((nc.value, 4), R)
+    rc = f(ctypes.byref(cam), _p(rm), _p(spheres), ctypes.c_int64(N), ctypes.c_int(tile_width),
+           ctypes.c_int64(n.value), _p(keys), _p(prims), _p(offs), _p(counts), ctypes.byref(n), _p(cones),
+           ctypes.byref(nc))
+    assert rc == 0
+    return keys[: n.value], prims[: n.value], offs, counts, cones
+
+
 def raster_forward(cam, tile_width, spheres, nsigmas, sites, rgbh, adj, adj_off, adj_diff, tile_offsets,
                    tile_prims, depth_q=None, ray_gt=None, thr=1e-3, return_point_err=False, surface=False,
-                   prec="f32"):
+                   prec="f32", ray_maps=None):
+    """ray_maps (H,W,6): per-pixel origin and direction (generic camera)."""
     N = spheres.shape[0]
     S = sites.shape[1]
     H, W = cam.height, cam.width
@@ -129,8 +164,9 @@ def raster_forward(cam, tile_width, spheres, nsigmas, sites, rgbh, adj, adj_off,
                normal=np.zeros((H, W, 3), R), quantile_depths=-np.ones((H, W, max(Q, 1)), R),
                contrib=np.zeros(N, R), point_err=np.zeros(N, R), early_stop=np.zeros(T, np.int32),
                err=np.zeros((H, W), R) if surface else None)
-    rc = _fn("orc_raster_forward", prec)(
-        ctypes.byref(cam), ctypes.c_int(tile_width), ctypes.c_int64(N), *[_p(a) for a in args[:4]], ctypes.c_int(S),
+    fn, lead = _cam_args(cam, ray_maps, "orc_raster_forward", prec)
+    rc = fn(
+        *lead[:2], ctypes.c_int(tile_width), ctypes.c_int64(N), *[_p(a) for a in args[:4]], ctypes.c_int(S),
         *[_p(a) for a in args[4:]], _p(dq), ctypes.c_int(Q), _p(gt), ctypes.c_float(thr),
         ctypes.c_int(int(return_point_err)), _p(out["color"]), _p(out["log_t"]), _p(out["normal_distance"]),
         _p(out["normal"]), _p(out["quantile_depths"]), _p(out["err"]), _p(out["contrib"]), _p(out["point_err"]),
@@ -143,7 +179,7 @@ def raster_forward(cam, tile_width, spheres, nsigmas, sites, rgbh, adj, adj_off,
 
 def raster_backward(cam, tile_width, spheres, nsigmas, sites, rgbh, adj, adj_off, adj_diff, tile_offsets,
                     tile_prims, early_stop, log_t, grad_color, grad_log_t, grad_nd, grad_normal, grad_contrib,
-                    depth_q=None, grad_qd=None, prec="f32"):
+                    depth_q=None, grad_qd=None, prec="f32", ray_maps=None):
     N = spheres.shape[0]
     S = sites.shape[1]
     Q = 0 if depth_q is None else depth_q.shape[-1]
@@ -156,8 +192,9 @@ def raster_backward(cam, tile_width, spheres, nsigmas, sites, rgbh, adj, adj_off
     gq = None if grad_qd is None else _c(grad_qd, F32)
     ins = [_c(log_t, F32), _c(grad_color, F32), _c(grad_log_t, F32), _c(grad_nd, F32), _c(grad_normal, F32)]
     adj_diff = None if adj_diff is None else _c(adj_diff, np.uint16)
-    rc = _fn("orc_raster_backward", prec)(
-        ctypes.byref(cam), ctypes.c_int(tile_width), ctypes.c_int64(N), *[_p(a) for a in args], ctypes.c_int(S),
+    fn, lead = _cam_args(cam, ray_maps, "orc_raster_backward", prec)
+    rc = fn(
+        *lead[:2], ctypes.c_int(tile_width), ctypes.c_int64(N), *[_p(a) for a in args], ctypes.c_int(S),
         *[_p(a) for a in args2], _p(dq), ctypes.c_int(Q), *[_p(a) for a in ins], _p(gq),
         _p(_c(grad_contrib, F32)), _p(g["spheres"]), _p(g["nsigmas"]), _p(g["texel_sites"]), _p(g["texel_rgb"]),
         _p(g["texel_height"]))

@@ -353,6 +353,207 @@ int FN(orc_bin)(const orc_camera *camera, const float *spheres, int64_t N, int T
     return total > cap ? ORC_ERR_OVERFLOW : ORC_OK;
 }
 
+/* ------------------------------------------------------------------------ */
+/* Generic-camera binning (rasterize.py:202-291, 365-569, 1518-1585): a     */
+/* hierarchy of ray cones over the ray map, leaves of 2x2 pixels, each level */
+/* merging 2x2 children up to one root; a primitive descends from the root  */
+/* into every child cone its sphere meets (camera.py:28-44) and is emitted   */
+/* into the tiles of the tile level.                                          */
+
+#define ORC_LEAF 2
+#define ORC_MAX_LEVELS 32
+
+typedef struct {
+    int n_levels, tile_level;
+    int off[ORC_MAX_LEVELS], dh[ORC_MAX_LEVELS], dw[ORC_MAX_LEVELS];
+    int64_t total;
+} cone_dims;
+
+static int cone_layout(int H, int W, int TW, cone_dims *cd) {
+    int dh = (H + ORC_LEAF - 1) / ORC_LEAF, dw = (W + ORC_LEAF - 1) / ORC_LEAF;
+    cd->n_levels = 0;
+    cd->total = 0;
+    for (;;) {
+        if (cd->n_levels == ORC_MAX_LEVELS) return ORC_ERR_ARGS;
+        cd->off[cd->n_levels] = (int)cd->total;
+        cd->dh[cd->n_levels] = dh;
+        cd->dw[cd->n_levels] = dw;
+        cd->n_levels++;
+        cd->total += (int64_t)dh * dw;
+        if (dh == 1 && dw == 1) break;
+        dh = (dh + 1) / 2;
+        dw = (dw + 1) / 2;
+    }
+    cd->tile_level = 0;
+    for (int sz = ORC_LEAF; sz < TW; sz *= 2) cd->tile_level++;
+    return ORC_OK;
+}
+
+/* compute_leaf_cones_kernel (rasterize.py:473-515) and merge_cones_kernel
+ * (:517-569); cones (total, 4): axis, cos of the half angle (2: empty). */
+static void build_cones(const cam_t *cam, const float *ray_maps, const cone_dims *cd, real *cones) {
+    const int lw = cd->dw[0];
+    const int64_t n_leaf = (int64_t)cd->dh[0] * lw;
+    for (int64_t t = 0; t < n_leaf; t++) {
+        int a = (int)(t / lw), b = (int)(t % lw);
+        v3 axis_sum = mk(0, 0, 0), rays[4];
+        int valid = 0;
+        for (int di = 0; di < ORC_LEAF; di++)
+            for (int dj = 0; dj < ORC_LEAF; dj++) {
+                int pi = imin(a * ORC_LEAF + di, cam->H - 1), pj = imin(b * ORC_LEAF + dj, cam->W - 1);
+                v3 ray = ld3(ray_maps + 6 * ((int64_t)pi * cam->W + pj) + 3);
+                real len = length(ray);
+                if (len > K(1.0e-6)) {
+                    v3 rn = vdivs(ray, len);
+                    rays[valid++] = rn;
+                    axis_sum = vadd(axis_sum, rn);
+                }
+            }
+        real *c = cones + 4 * t;
+        if (valid == 0) { c[0] = c[1] = c[2] = 0; c[3] = K(2.0); continue; }
+        v3 axis = normalize(axis_sum);
+        real ch = K(1.0);
+        for (int i = 0; i < valid; i++) ch = rmin(ch, dot(axis, rays[i]));
+        c[0] = axis.x; c[1] = axis.y; c[2] = axis.z; c[3] = ch;
+    }
+    for (int l = 1; l < cd->n_levels; l++) {
+        const int pdw = cd->dw[l], cdh = cd->dh[l - 1], cdw = cd->dw[l - 1];
+        const int64_t n = (int64_t)cd->dh[l] * pdw;
+        for (int64_t t = 0; t < n; t++) {
+            int a = (int)(t / pdw), b = (int)(t % pdw);
+            v3 axis_sum = mk(0, 0, 0), axes[4];
+            real chs[4];
+            int valid = 0;
+            for (int di = 0; di < 2; di++)
+                for (int dj = 0; dj < 2; dj++) {
+                    int ca = 2 * a + di, cb = 2 * b + dj;
+                    if (ca < cdh && cb < cdw) {
+                        const real *cc = cones + 4 * ((int64_t)cd->off[l - 1] + (int64_t)ca * cdw + cb);
+                        if (cc[3] <= K(1.0)) {
+                            axes[valid] = mk(cc[0], cc[1], cc[2]);
+                            chs[valid] = cc[3];
+                            axis_sum = vadd(axis_sum, axes[valid]);
+                            valid++;
+                        }
+                    }
+                }
+            real *c = cones + 4 * ((int64_t)cd->off[l] + t);
+            if (valid == 0) { c[0] = c[1] = c[2] = 0; c[3] = K(2.0); continue; }
+            v3 axis = normalize(axis_sum);
+            real ch = K(1.0);
+            for (int i = 0; i < valid; i++) {
+                real dv = dot(axis, axes[i]);
+                real sin_angle = r_sqrt(rmax(K(1.0) - dv * dv, K(0.0)));
+                real sin_child = r_sqrt(rmax(K(1.0) - chs[i] * chs[i], K(0.0)));
+                real extent = dv * chs[i] - sin_angle * sin_child;
+                ch = rmin(ch, extent);
+            }
+            c[0] = axis.x; c[1] = axis.y; c[2] = axis.z; c[3] = ch;
+        }
+    }
+}
+
+/* camera.py:28-44 */
+static int sphere_cone(v3 center, real radius, v3 eye, v3 axis, real cos_half) {
+    v3 v = vsub(center, eye);
+    real dist = length(v);
+    real cos_alpha = dot(v, axis) / dist;
+    real sin_half = r_sqrt(K(1.0) - cos_half * cos_half);
+    real sin_beta = radius / dist;
+    real cos_beta = r_sqrt(K(1.0) - sin_beta * sin_beta);
+    real threshold = cos_half * cos_beta - sin_half * sin_beta;
+    return cos_alpha > threshold;
+}
+
+/* count / write_visible_generic_kernel traversal (rasterize.py:202-291,
+ * 365-464): emits every tile-level cone the sphere reaches. */
+static int prim_tiles_generic(const cam_t *cam, const cone_dims *cd, const real *cones, int TW, v3 center,
+                              real radius, emit_fn emit, void *ctx) {
+    int tiles_h = 1 + (cam->H - 1) / TW;
+    v3 v = vsub(center, cam->eye);
+    v3 forward = cross(cam->up, cam->right);
+    if (length(v) < K(4.0) * radius || dot(v, forward) < K(0.1)) return 0;
+    int st_l[4 * ORC_MAX_LEVELS], st_a[4 * ORC_MAX_LEVELS], st_b[4 * ORC_MAX_LEVELS];
+    int n = 1;
+    st_l[0] = cd->n_levels - 1; st_a[0] = 0; st_b[0] = 0;
+    while (n > 0) {
+        n--;
+        int level = st_l[n], a = st_a[n], b = st_b[n];
+        const real *c = cones + 4 * ((int64_t)cd->off[level] + (int64_t)a * cd->dw[level] + b);
+        if (c[3] > K(1.0)) continue;
+        if (!sphere_cone(center, radius, cam->eye, mk(c[0], c[1], c[2]), c[3])) continue;
+        if (level == cd->tile_level) {
+            emit(ctx, a + b * tiles_h);
+            continue;
+        }
+        int cl = level - 1;
+        for (int di = 0; di < 2; di++)
+            for (int dj = 0; dj < 2; dj++) {
+                int ca = 2 * a + di, cb = 2 * b + dj;
+                if (ca < cd->dh[cl] && cb < cd->dw[cl]) {
+                    st_l[n] = cl; st_a[n] = ca; st_b[n] = cb;
+                    n++;
+                }
+            }
+    }
+    return 1;
+}
+
+/* Binning with a generic camera; as orc_bin otherwise.  cones_out (total x
+ * 4, optional) receives the cone hierarchy; *n_cones its node count. */
+int FN(orc_bin_generic)(const orc_camera *camera, const float *ray_maps, const float *spheres, int64_t N, int TW,
+                        int64_t cap, int64_t *keys_out, int32_t *prims_out, int64_t *tile_offsets,
+                        int32_t *prim_counts, int64_t *n_pairs, out_t *cones_out, int64_t *n_cones) {
+    if (TW <= 0 || !ray_maps) return ORC_ERR_ARGS;
+    cam_t cam = cam_load(camera);
+    cone_dims cd;
+    if (cone_layout(cam.H, cam.W, TW, &cd) != ORC_OK) return ORC_ERR_ARGS;
+    if (n_cones) *n_cones = cd.total;
+    real *cones = (real *)malloc(sizeof(real) * 4 * (size_t)cd.total);
+    build_cones(&cam, ray_maps, &cd, cones);
+    if (cones_out)
+        for (int64_t k = 0; k < 4 * cd.total; k++) cones_out[k] = (out_t)cones[k];
+    int tiles_h = 1 + (cam.H - 1) / TW, tiles_w = 1 + (cam.W - 1) / TW;
+    int64_t T = (int64_t)tiles_h * tiles_w;
+    int64_t total = 0;
+    for (int64_t p = 0; p < N; p++) {
+        int64_t c = 0;
+        const float *s = spheres + 4 * p;
+        prim_tiles_generic(&cam, &cd, cones, TW, ld3(s), (real)s[3], count_emit, &c);
+        if (prim_counts) prim_counts[p] = (int32_t)c;
+        total += c;
+    }
+    *n_pairs = total;
+    pair_t *pairs = (pair_t *)malloc(sizeof(pair_t) * (size_t)(total > 0 ? total : 1));
+    int64_t *tk = (int64_t *)malloc(sizeof(int64_t) * (size_t)(total > 0 ? total : 1));
+    int32_t *tp = (int32_t *)malloc(sizeof(int32_t) * (size_t)(total > 0 ? total : 1));
+    int64_t pos = 0;
+    for (int64_t p = 0; p < N; p++) {
+        const float *s = spheres + 4 * p;
+        v3 c = ld3(s);
+        real r = (real)s[3];
+        v3 v = vsub(c, cam.eye);
+        float pd = (float)(dot(v, v) - r * r);
+        write_ctx w;
+        w.pos = &pos; w.cap = total; w.keys = tk; w.prims = tp; w.prim = (int32_t)p;
+        memcpy(&w.depth_bits, &pd, 4);
+        prim_tiles_generic(&cam, &cd, cones, TW, c, r, write_emit, &w);
+    }
+    for (int64_t k = 0; k < total; k++) {
+        pairs[k].key = tk[k]; pairs[k].ord = k; pairs[k].prim = tp[k];
+    }
+    qsort(pairs, (size_t)total, sizeof(pair_t), pair_cmp);
+    for (int64_t t = 0; t <= T; t++) tile_offsets[t] = 0;
+    for (int64_t k = 0; k < total; k++) {
+        int64_t t = pairs[k].key >> 32;
+        tile_offsets[t + 1]++;
+        if (k < cap) { keys_out[k] = pairs[k].key; prims_out[k] = pairs[k].prim; }
+    }
+    for (int64_t t = 0; t < T; t++) tile_offsets[t + 1] += tile_offsets[t];
+    free(pairs); free(tk); free(tp); free(cones);
+    return total > cap ? ORC_ERR_OVERFLOW : ORC_OK;
+}
+
 /* rasterize.py:580-606 prefetch_adjacency_kernel: (half(c_j - c_i), half(r_j)) */
 void FN(orc_prefetch_adjacency)(const float *spheres, const int32_t *adj, const int32_t *adj_off,
                                 int64_t N, uint16_t *adj_diff) {
@@ -678,7 +879,7 @@ static void nbr_sphere(const float *spheres, const int32_t *adj, const uint16_t 
 /* as the reference does (zeros; quantile depths -1).                        */
 
 typedef struct {
-    v3 d;
+    v3 o, d;
     int oob, pi, pj;
     real log_t, nd, err;
     v3 rgb, normal;
@@ -689,38 +890,49 @@ typedef struct {
     real tn, tf;
 } fwd_lane;
 
-static void lane_setup(const cam_t *cam, int TW, int tiles_h, int64_t tile, int l, v3 *d, int *oob, int *pi, int *pj) {
+/* The ray of lane l: the pinhole ray from the eye, or with ray_maps (H,W,6)
+ * (the generic camera, rasterize.py:940-954) the pixel's own origin and its
+ * direction divided by its length. */
+static void lane_setup(const cam_t *cam, const float *ray_maps, int TW, int tiles_h, int64_t tile, int l, v3 *o,
+                       v3 *d, int *oob, int *pi, int *pj) {
     int ti = (int)(tile % tiles_h), tj = (int)(tile / tiles_h);
     int i_in = l % TW, j_in = l / TW;
     int pix_i = ti * TW + i_in, pix_j = tj * TW + j_in;
     *oob = pix_i >= cam->H || pix_j >= cam->W;
     pix_i = imin(pix_i, cam->H - 1);
     pix_j = imin(pix_j, cam->W - 1);
-    v3 rd = get_ray_dir(cam, (real)pix_i, (real)pix_j);
-    *d = vdivs(rd, length(rd));
+    if (ray_maps) {
+        const float *m = ray_maps + 6 * ((int64_t)pix_i * cam->W + pix_j);
+        *o = ld3(m);
+        v3 rd = ld3(m + 3);
+        *d = vdivs(rd, length(rd));
+    } else {
+        v3 rd = get_ray_dir(cam, (real)pix_i, (real)pix_j);
+        *d = vdivs(rd, length(rd));
+        *o = cam->eye;
+    }
     *pi = pix_i; *pj = pix_j;
 }
 
-int FN(orc_raster_forward)(const orc_camera *camera, int TW, int64_t N, const float *spheres,
-                           const float *nsigmas, const float *sites, const float *rgbh, int S,
-                           const int32_t *adj, const int32_t *adj_off, const uint16_t *adj_diff,
-                           const int64_t *tile_offsets, const int32_t *tile_prims, const float *depth_q,
-                           int Q, const float *ray_gt, float thr, int return_point_err, out_t *color,
-                           out_t *log_t_out, out_t *nd_out, out_t *normal_out, out_t *qdepth_out,
-                           out_t *err_out, out_t *contrib, out_t *point_err, int32_t *early_stop) {
+static int FN(raster_forward)(const orc_camera *camera, const float *ray_maps, int TW, int64_t N,
+                              const float *spheres, const float *nsigmas, const float *sites, const float *rgbh,
+                              int S, const int32_t *adj, const int32_t *adj_off, const uint16_t *adj_diff,
+                              const int64_t *tile_offsets, const int32_t *tile_prims, const float *depth_q, int Q,
+                              const float *ray_gt, float thr, int return_point_err, out_t *color, out_t *log_t_out,
+                              out_t *nd_out, out_t *normal_out, out_t *qdepth_out, out_t *err_out, out_t *contrib,
+                              out_t *point_err, int32_t *early_stop) {
     (void)N; (void)adj;
     cam_t cam = cam_load(camera);
     int tiles_h = 1 + (cam.H - 1) / TW, tiles_w = 1 + (cam.W - 1) / TW;
     int64_t T = (int64_t)tiles_h * tiles_w;
     int TS = TW * TW;
     real HW = (real)(cam.H * cam.W);
-    v3 o = cam.eye;
 #pragma omp parallel for schedule(dynamic, 1)
     for (int64_t tile = 0; tile < T; tile++) {
         fwd_lane *L = (fwd_lane *)calloc((size_t)TS, sizeof(fwd_lane));
         for (int l = 0; l < TS; l++) {
             fwd_lane *a = &L[l];
-            lane_setup(&cam, TW, tiles_h, tile, l, &a->d, &a->oob, &a->pi, &a->pj);
+            lane_setup(&cam, ray_maps, TW, tiles_h, tile, l, &a->o, &a->d, &a->oob, &a->pi, &a->pj);
             a->log_t = 0; a->nd = 0; a->rgb = mk(0, 0, 0); a->normal = mk(0, 0, 0);
             int64_t px = (int64_t)a->pi * cam.W + a->pj;
             if (depth_q) { a->qi = 0; a->q = (real)depth_q[px * Q + 0]; } else { a->qi = 0; a->q = 0; }
@@ -745,7 +957,7 @@ int FN(orc_raster_forward)(const orc_camera *camera, int TW, int64_t N, const fl
             real sigma = (real)ns[3];
             int any = 0;
             for (int l = 0; l < TS; l++) {
-                L[l].hit = ray_sphere(o, L[l].d, center, radius, &L[l].tn, &L[l].tf);
+                L[l].hit = ray_sphere(L[l].o, L[l].d, center, radius, &L[l].tn, &L[l].tf);
                 any += L[l].hit;
             }
             if (any == 0) continue;
@@ -761,12 +973,12 @@ int FN(orc_raster_forward)(const orc_camera *camera, int TW, int64_t N, const fl
                         real ar;
                         nbr_sphere(spheres, adj, adj_diff, e, center, &ac, &ar);
                         real dp;
-                        real t_face = ray_pface(o, a->d, center, radius, ac, ar, &dp);
+                        real t_face = ray_pface(a->o, a->d, center, radius, ac, ar, &dp);
                         tf = dp >= K(0.0) ? rmin(t_face, tf) : tf;
                         tn = dp < K(0.0) ? rmax(t_face, tn) : tn;
                     }
                 }
-                plane_res pr = plane_fwd(o, a->d, tn, center, pn, radius, !a->oob && a->hit, ps, pv, S);
+                plane_res pr = plane_fwd(a->o, a->d, tn, center, pn, radius, !a->oob && a->hit, ps, pv, S);
                 tf = pr.dp >= K(0.0) ? rmin(pr.t_surf, tf) : tf;
                 tn = pr.dp < K(0.0) ? rmax(pr.t_surf, tn) : tn;
                 real dt = tf - tn;
@@ -824,6 +1036,32 @@ int FN(orc_raster_forward)(const orc_camera *camera, int TW, int64_t N, const fl
 }
 
 /* ------------------------------------------------------------------------ */
+int FN(orc_raster_forward)(const orc_camera *camera, int TW, int64_t N, const float *spheres,
+                           const float *nsigmas, const float *sites, const float *rgbh, int S,
+                           const int32_t *adj, const int32_t *adj_off, const uint16_t *adj_diff,
+                           const int64_t *tile_offsets, const int32_t *tile_prims, const float *depth_q,
+                           int Q, const float *ray_gt, float thr, int return_point_err, out_t *color,
+                           out_t *log_t_out, out_t *nd_out, out_t *normal_out, out_t *qdepth_out,
+                           out_t *err_out, out_t *contrib, out_t *point_err, int32_t *early_stop) {
+    return FN(raster_forward)(camera, NULL, TW, N, spheres, nsigmas, sites, rgbh, S, adj, adj_off, adj_diff,
+                              tile_offsets, tile_prims, depth_q, Q, ray_gt, thr, return_point_err, color, log_t_out,
+                              nd_out, normal_out, qdepth_out, err_out, contrib, point_err, early_stop);
+}
+
+/* The same with a generic camera: per-pixel rays from ray_maps (H,W,6). */
+int FN(orc_raster_forward_generic)(const orc_camera *camera, const float *ray_maps, int TW, int64_t N,
+                                   const float *spheres, const float *nsigmas, const float *sites, const float *rgbh,
+                                   int S, const int32_t *adj, const int32_t *adj_off, const uint16_t *adj_diff,
+                                   const int64_t *tile_offsets, const int32_t *tile_prims, const float *depth_q,
+                                   int Q, const float *ray_gt, float thr, int return_point_err, out_t *color,
+                                   out_t *log_t_out, out_t *nd_out, out_t *normal_out, out_t *qdepth_out,
+                                   out_t *err_out, out_t *contrib, out_t *point_err, int32_t *early_stop) {
+    return FN(raster_forward)(camera, ray_maps, TW, N, spheres, nsigmas, sites, rgbh, S, adj, adj_off, adj_diff,
+                              tile_offsets, tile_prims, depth_q, Q, ray_gt, thr, return_point_err, color, log_t_out,
+                              nd_out, normal_out, qdepth_out, err_out, contrib, point_err, early_stop);
+}
+
+/* ------------------------------------------------------------------------ */
 /* Rasterizer backward (rasterize.py:1150-1514 backward_kernel; host side   */
 /* rasterize.py:1861-1980).  log_t_grad is dL/dlog_t = -dL/dopacity*exp(log_t)*/
 /* (computed by the caller as the reference's host code does).  Gradient    */
@@ -831,7 +1069,7 @@ int FN(orc_raster_forward)(const orc_camera *camera, int TW, int64_t N, const fl
 /* at the end, as rasterize.py:1954-1958 does.                               */
 
 typedef struct {
-    v3 d;
+    v3 o, d;
     int oob, pi, pj;
     real log_t, dLdlog_t;
     v3 g_rgb, g_n;
@@ -847,28 +1085,26 @@ static void zero_nonfinite(float *a, int64_t n) {
         if (!isfinite(a[i])) a[i] = 0.0f;
 }
 
-int FN(orc_raster_backward)(const orc_camera *camera, int TW, int64_t N, const float *spheres,
-                            const float *nsigmas, const float *sites, const float *rgbh, int S,
-                            const int32_t *adj, const int32_t *adj_off, const uint16_t *adj_diff,
-                            const int64_t *tile_offsets, const int32_t *tile_prims,
-                            const int32_t *early_stop, const float *depth_q, int Q,
-                            const float *log_t_in, const float *color_grad, const float *log_t_grad,
-                            const float *nd_grad, const float *normal_grad, const float *qdepth_grad,
-                            const float *contrib_grad, float *spheres_g, float *nsigmas_g, float *sites_g,
-                            float *rgb_g, float *height_g) {
+static int FN(raster_backward)(const orc_camera *camera, const float *ray_maps, int TW, int64_t N,
+                               const float *spheres, const float *nsigmas, const float *sites, const float *rgbh,
+                               int S, const int32_t *adj, const int32_t *adj_off, const uint16_t *adj_diff,
+                               const int64_t *tile_offsets, const int32_t *tile_prims, const int32_t *early_stop,
+                               const float *depth_q, int Q, const float *log_t_in, const float *color_grad,
+                               const float *log_t_grad, const float *nd_grad, const float *normal_grad,
+                               const float *qdepth_grad, const float *contrib_grad, float *spheres_g,
+                               float *nsigmas_g, float *sites_g, float *rgb_g, float *height_g) {
     cam_t cam = cam_load(camera);
     int tiles_h = 1 + (cam.H - 1) / TW, tiles_w = 1 + (cam.W - 1) / TW;
     int64_t T = (int64_t)tiles_h * tiles_w;
     int TS = TW * TW;
     real HW = (real)(cam.H * cam.W);
-    v3 o = cam.eye;
     v3 bkgd = mk(0, 0, 0);
 #pragma omp parallel for schedule(dynamic, 1)
     for (int64_t tile = 0; tile < T; tile++) {
         bwd_lane *L = (bwd_lane *)calloc((size_t)TS, sizeof(bwd_lane));
         for (int l = 0; l < TS; l++) {
             bwd_lane *a = &L[l];
-            lane_setup(&cam, TW, tiles_h, tile, l, &a->d, &a->oob, &a->pi, &a->pj);
+            lane_setup(&cam, ray_maps, TW, tiles_h, tile, l, &a->o, &a->d, &a->oob, &a->pi, &a->pj);
             int64_t px = (int64_t)a->pi * cam.W + a->pj;
             a->log_t = (real)log_t_in[px];
             if (depth_q) { a->qi = Q - 1; a->q = (real)depth_q[px * Q + Q - 1]; } else { a->qi = -1; a->q = K(1.0); }
@@ -892,7 +1128,7 @@ int FN(orc_raster_backward)(const orc_camera *camera, int TW, int64_t N, const f
             real sigma = (real)ns[3];
             int any = 0;
             for (int l = 0; l < TS; l++) {
-                L[l].hit = ray_sphere(o, L[l].d, center, radius, &L[l].tn, &L[l].tf);
+                L[l].hit = ray_sphere(L[l].o, L[l].d, center, radius, &L[l].tn, &L[l].tf);
                 any += L[l].hit;
             }
             if (any == 0) continue;
@@ -915,7 +1151,7 @@ int FN(orc_raster_backward)(const orc_camera *camera, int TW, int64_t N, const f
                         real ar;
                         nbr_sphere(spheres, adj, adj_diff, e, center, &ac, &ar);
                         real dp;
-                        real t_face = ray_pface(o, a->d, center, radius, ac, ar, &dp);
+                        real t_face = ray_pface(a->o, a->d, center, radius, ac, ar, &dp);
                         int adj_idx = e - a0;
                         t_far_id = (dp >= K(0.0) && t_face < t_far) ? adj_idx : t_far_id;
                         t_far = dp >= K(0.0) ? rmin(t_face, t_far) : t_far;
@@ -925,7 +1161,7 @@ int FN(orc_raster_backward)(const orc_camera *camera, int TW, int64_t N, const f
                 }
                 real _t_near = t_near;
                 int _t_near_id = t_near_id, _t_far_id = t_far_id;
-                plane_res pr = plane_fwd(o, a->d, t_near, center, pn, radius, !a->oob && hit, ps, pv, S);
+                plane_res pr = plane_fwd(a->o, a->d, t_near, center, pn, radius, !a->oob && hit, ps, pv, S);
                 t_far_id = (pr.dp >= K(0.0) && pr.t_surf < t_far) ? n_adj : t_far_id;
                 t_far = pr.dp >= K(0.0) ? rmin(pr.t_surf, t_far) : t_far;
                 t_near_id = (pr.dp < K(0.0) && pr.t_surf > t_near) ? n_adj : t_near_id;
@@ -976,7 +1212,7 @@ int FN(orc_raster_backward)(const orc_camera *camera, int TW, int64_t N, const f
                 else dLdt_surf = K(0.0);
                 v3 _dc, _dn;
                 real dLd_t_near;
-                plane_bwd(o, a->d, _t_near, center, pn, radius, contributes, ps, pv, pr._dp, pr._t_surf,
+                plane_bwd(a->o, a->d, _t_near, center, pn, radius, contributes, ps, pv, pr._dp, pr._t_surf,
                           pr.height, pr._wsum, pr.dp, pr.t_surf, pr.rgb, pr.wsum, dLdcolor, dLdt_surf, S, gs,
                           gr, gh, &_dc, &_dn, &dLd_t_near);
                 dLdcenter = vadd(dLdcenter, _dc);
@@ -989,7 +1225,7 @@ int FN(orc_raster_backward)(const orc_camera *camera, int TW, int64_t N, const f
                         if (t_id == -1) {
                             v3 ndc, fdc;
                             real ndr, fdr;
-                            ray_sphere_bwd(o, a->d, center, radius, &ndc, &fdc, &ndr, &fdr);
+                            ray_sphere_bwd(a->o, a->d, center, radius, &ndc, &fdc, &ndr, &fdr);
                             if (i == 0) {
                                 dLdcenter = vadd(dLdcenter, smul(dLdt, ndc));
                                 dLdradius += dLdt * ndr;
@@ -1002,7 +1238,7 @@ int FN(orc_raster_backward)(const orc_camera *camera, int TW, int64_t N, const f
                             const float *as = spheres + 4 * (int64_t)adjacent;
                             v3 dc, dac;
                             real dr, dar;
-                            ray_pface_bwd(o, a->d, center, radius, ld3(as), (real)as[3], &dc, &dr, &dac, &dar);
+                            ray_pface_bwd(a->o, a->d, center, radius, ld3(as), (real)as[3], &dc, &dr, &dac, &dar);
                             dLdcenter = vadd(dLdcenter, smul(dLdt, dc));
                             dLdradius += dLdt * dr;
                             v3 g = smul(dLdt, dac);
@@ -1038,6 +1274,37 @@ int FN(orc_raster_backward)(const orc_camera *camera, int TW, int64_t N, const f
 /* thread early-out, (dc, dpm)-encoded neighbour faces with break, local     */
 /* plane with separate sites/rgb/height arrays (which hold float32 values,   */
 /* already rounded to float16 by the caller for attr_dtype "half").          */
+int FN(orc_raster_backward)(const orc_camera *camera, int TW, int64_t N, const float *spheres,
+                            const float *nsigmas, const float *sites, const float *rgbh, int S,
+                            const int32_t *adj, const int32_t *adj_off, const uint16_t *adj_diff,
+                            const int64_t *tile_offsets, const int32_t *tile_prims,
+                            const int32_t *early_stop, const float *depth_q, int Q,
+                            const float *log_t_in, const float *color_grad, const float *log_t_grad,
+                            const float *nd_grad, const float *normal_grad, const float *qdepth_grad,
+                            const float *contrib_grad, float *spheres_g, float *nsigmas_g, float *sites_g,
+                            float *rgb_g, float *height_g) {
+    return FN(raster_backward)(camera, NULL, TW, N, spheres, nsigmas, sites, rgbh, S, adj, adj_off, adj_diff,
+                               tile_offsets, tile_prims, early_stop, depth_q, Q, log_t_in, color_grad, log_t_grad,
+                               nd_grad, normal_grad, qdepth_grad, contrib_grad, spheres_g, nsigmas_g, sites_g,
+                               rgb_g, height_g);
+}
+
+/* The same with a generic camera: per-pixel rays from ray_maps (H,W,6). */
+int FN(orc_raster_backward_generic)(const orc_camera *camera, const float *ray_maps, int TW, int64_t N,
+                                    const float *spheres, const float *nsigmas, const float *sites,
+                                    const float *rgbh, int S, const int32_t *adj, const int32_t *adj_off,
+                                    const uint16_t *adj_diff, const int64_t *tile_offsets,
+                                    const int32_t *tile_prims, const int32_t *early_stop, const float *depth_q,
+                                    int Q, const float *log_t_in, const float *color_grad, const float *log_t_grad,
+                                    const float *nd_grad, const float *normal_grad, const float *qdepth_grad,
+                                    const float *contrib_grad, float *spheres_g, float *nsigmas_g, float *sites_g,
+                                    float *rgb_g, float *height_g) {
+    return FN(raster_backward)(camera, ray_maps, TW, N, spheres, nsigmas, sites, rgbh, S, adj, adj_off, adj_diff,
+                               tile_offsets, tile_prims, early_stop, depth_q, Q, log_t_in, color_grad, log_t_grad,
+                               nd_grad, normal_grad, qdepth_grad, contrib_grad, spheres_g, nsigmas_g, sites_g,
+                               rgb_g, height_g);
+}
+
 int FN(orc_raster_benchmark)(const orc_camera *camera, int TW, const float *spheres, const float *nsigmas,
                              const float *sites, const float *rgbs, const float *heights, int S,
                              const int32_t *adj_off, const uint16_t *adj_diff, const int64_t *tile_offsets,
@@ -1052,7 +1319,8 @@ int FN(orc_raster_benchmark)(const orc_camera *camera, int TW, const float *sphe
         for (int l = 0; l < TS; l++) {
             v3 d;
             int oob, pi, pj;
-            lane_setup(&cam, TW, tiles_h, tile, l, &d, &oob, &pi, &pj);
+            v3 o_unused;
+            lane_setup(&cam, NULL, TW, tiles_h, tile, l, &o_unused, &d, &oob, &pi, &pj);
             v3 rgb = mk(0, 0, 0);
             real log_t = 0;
             int64_t start = tile_offsets[tile], end = tile_offsets[tile + 1];
@@ -1123,7 +1391,8 @@ int FN(orc_raster_visualize)(const orc_camera *camera, int TW, const float *sphe
         for (int l = 0; l < TS; l++) {
             v3 d;
             int oob, pi, pj;
-            lane_setup(&cam, TW, tiles_h, tile, l, &d, &oob, &pi, &pj);
+            v3 o_unused;
+            lane_setup(&cam, NULL, TW, tiles_h, tile, l, &o_unused, &d, &oob, &pi, &pj);
             v3 rgb = mk(0, 0, 0), nacc = mk(0, 0, 0);
             real dq_out = 0;
             int dq_found = 0;

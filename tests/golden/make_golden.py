@@ -260,6 +260,142 @@ def raster_case(name, scene, cam, seed, Q=3, thr=1e-3, bench_thr=1e-2):
           f"fwd {t1 - t0:.1f}s bwd {t2 - t1:.1f}s bench+vis {t3 - t2:.1f}s")
 
 
+class ArgsGeneric(Args):
+    is_pinhole = False
+
+
+def run_cones(R, wcam, H, W):
+    """Rasterizer._precompute_cones (rasterize.py:1518-1585) with the
+    reference's cone kernels."""
+    leaf = rras.LEAF_SIZE
+    dh, dw = (H + leaf - 1) // leaf, (W + leaf - 1) // leaf
+    offs, dhs, dws, total = [], [], [], 0
+    while True:
+        offs.append(total)
+        dhs.append(dh)
+        dws.append(dw)
+        total += dh * dw
+        if dh == 1 and dw == 1:
+            break
+        dh, dw = (dh + 1) // 2, (dw + 1) // 2
+    tile_level, sz = 0, leaf
+    while sz < TILE_WIDTH:
+        tile_level += 1
+        sz *= 2
+    cones = np.zeros((total, 4), F32)
+    wp.launch(R.compute_leaf_cones_kernel, dim=dhs[0] * dws[0], inputs=[wcam, cones, dws[0]])
+    for l in range(1, len(offs)):
+        wp.launch(R.merge_cones_kernel, dim=dhs[l] * dws[l],
+                  inputs=[cones, offs[l], offs[l - 1], dws[l], dhs[l - 1], dws[l - 1]])
+    return (cones, np.array(offs, np.int32), np.array(dhs, np.int32), np.array(dws, np.int32), len(offs),
+            tile_level)
+
+
+def run_binning_generic(R, wcam, spheres, cone_args):
+    """The generic-camera branch of rasterize.py:1681-1768."""
+    N = spheres.shape[0]
+    H, W = int(wcam.height), int(wcam.width)
+    T = (1 + (H - 1) // TILE_WIDTH) * (1 + (W - 1) // TILE_WIDTH)
+    counts = np.zeros(T + 1, np.int32)
+    wp.launch(R.count_visible_kernel, dim=N, inputs=[wcam, spheres, *cone_args, counts])
+    offsets = np.cumsum(counts.astype(np.int64))
+    n = int(offsets[-1])
+    prims = np.zeros(n, np.int32)
+    keys = np.zeros(n, np.int64)
+    wc = np.zeros(T, np.int32)
+    wp.launch(R.write_visible_kernel, dim=N, inputs=[wcam, spheres, *cone_args, offsets, prims, keys, wc])
+    perm = np.argsort(keys, kind="stable")
+    return keys[perm], prims[perm], offsets, T
+
+
+def fisheye_ray_maps(cam, fov_deg, scale=1.7, shift=0.02):
+    """A generic camera: equidistant fisheye directions (length `scale`, so the
+    kernels' normalisation is exercised) from per-pixel origins spread along
+    the image axes by up to `shift`."""
+    H, W = cam["height"], cam["width"]
+    r_hat = cam["right"] / np.linalg.norm(cam["right"])
+    u_hat = cam["up"] / np.linalg.norm(cam["up"])
+    f = np.cross(cam["up"], cam["right"])
+    f = f / np.linalg.norm(f)
+    jj, ii = np.meshgrid(np.arange(W), np.arange(H))
+    x = 2.0 * jj / (W - 1) - 1.0
+    y = 1.0 - 2.0 * ii / (H - 1)
+    rad = np.sqrt(x * x + y * y)
+    th = rad * np.deg2rad(fov_deg) / 2.0
+    s = np.where(rad > 0, np.sin(th) / np.maximum(rad, 1e-12), 0.0)
+    d = (np.cos(th)[..., None] * f + (s * x)[..., None] * r_hat + (s * y)[..., None] * u_hat) * scale
+    o = cam["eye"] + shift * (x[..., None] * r_hat + y[..., None] * u_hat)
+    return np.concatenate([o, d], -1).astype(F32)
+
+
+def generic_case(name, scene, cam, ray_maps, seed, Q=3, thr=1e-3):
+    """Binning through the cone hierarchy and the forward / adjoint with
+    per-pixel rays (is_pinhole=False)."""
+    t0 = time.time()
+    R = rras.Rasterizer(ArgsGeneric(), "cpu", "float")
+    wcam = warp_camera(cam)
+    wcam.ray_maps = ray_maps
+    N = scene["points"].shape[0]
+    H, W = cam["height"], cam["width"]
+    spheres = np.concatenate([scene["points"], scene["radii"][:, None]], -1).astype(F32)
+    nsig = np.concatenate([scene["normals"], scene["density"][:, None]], -1).astype(F32)
+    rgbh = np.concatenate([scene["texel_rgb"], scene["texel_height"][..., None]], -1).astype(F32)
+    adj, adj_off = cech_adjacency(scene["points"], scene["radii"])
+    cone_args = run_cones(R, wcam, H, W)
+    keys, prims, offsets, T = run_binning_generic(R, wcam, spheres, cone_args)
+    adj_diff = np.zeros((adj.shape[0], 4), np.float16)
+    wp.launch(R.prefetch_adjacency_kernel, dim=N, inputs=[spheres, adj, adj_off, adj_diff, N])
+    rng = np.random.default_rng(seed + 1000)
+    dq = np.sort(rng.uniform(0.05, 0.95, (H, W, Q)).astype(F32), axis=-1)[..., ::-1].copy()
+    gt = rng.uniform(0, 1, (H, W, 3)).astype(F32)
+    color = np.zeros((H, W, 3), F32)
+    log_t = np.zeros((H, W), F32)
+    nd = np.zeros((H, W), F32)
+    normal = np.zeros((H, W, 3), F32)
+    qd = -np.ones((H, W, Q), F32)
+    contrib = np.zeros(N, F32)
+    perr = np.zeros(N, F32)
+    es = np.zeros(T, np.int32)
+    TS = TILE_WIDTH * TILE_WIDTH
+    wp.launch(R.forward_kernel, dim=T * TS, block_dim=TS, cooperative=True, inputs=[
+        wcam, dq, True, spheres, nsig, scene["texel_sites"], rgbh, adj, adj_off, adj_diff, prims,
+        offsets, es, gt, F32(thr), True, color, log_t, nd, normal, qd, None, contrib, perr])
+    t1 = time.time()
+    g_color = rng.standard_normal((H, W, 3)).astype(F32)
+    g_opac = rng.standard_normal((H, W)).astype(F32)
+    g_nd = rng.standard_normal((H, W)).astype(F32)
+    g_normal = rng.standard_normal((H, W, 3)).astype(F32)
+    g_qd = rng.standard_normal((H, W, Q)).astype(F32)
+    g_contrib = (rng.standard_normal(N) * 100).astype(F32)
+    g_logt = (-g_opac * np.exp(log_t)).astype(F32)
+    sg = np.zeros((N, 4), F32)
+    ng = np.zeros((N, 4), F32)
+    tsg = np.zeros((N, 8, 3), F32)
+    trg = np.zeros((N, 8, 3), F32)
+    thg = np.zeros((N, 8), F32)
+    wp.launch(R.backward_kernel, dim=T * TS, block_dim=TS, cooperative=True, inputs=[
+        wcam, dq, True, spheres, nsig, scene["texel_sites"], rgbh, adj, adj_off, adj_diff, prims,
+        offsets, es, gt, color, log_t, g_color, g_logt, g_nd, g_normal, g_qd, None, g_contrib,
+        sg, ng, tsg, trg, thg])
+    for a in (sg, ng, tsg, trg, thg):
+        a[~np.isfinite(a)] = 0
+    t2 = time.time()
+    cones, lo, ldh, ldw, nl, tl = cone_args
+    out = dict(cam_eye=cam["eye"], cam_right=cam["right"], cam_up=cam["up"], width=W, height=H,
+               tile_width=TILE_WIDTH, thr=F32(thr), ray_maps=ray_maps, cones=cones, level_offsets=lo,
+               level_dims_h=ldh, level_dims_w=ldw, num_levels=nl, tile_level=tl, **scene,
+               adjacency=adj, adjacency_offsets=adj_off, sort_keys=keys, tile_prims=prims,
+               tile_offsets=offsets, adjacency_diff=adj_diff.view(np.uint16), depth_quantiles=dq, ray_gt=gt,
+               color=color, log_t=log_t, normal_distance=nd, normal=normal, quantile_depths=qd,
+               contrib=contrib, point_err=perr, early_stop=es, grad_color=g_color,
+               grad_opacity=g_opac, grad_normal_distance=g_nd, grad_normal=g_normal,
+               grad_quantile_depths=g_qd, grad_contrib=g_contrib, grad_log_t=g_logt,
+               spheres_grad=sg, nsigmas_grad=ng, texel_sites_grad=tsg, texel_rgb_grad=trg,
+               texel_height_grad=thg)
+    np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **out)
+    print(f"{name}: N={N} {W}x{H} pairs={keys.shape[0]} levels={nl} fwd {t1 - t0:.1f}s bwd {t2 - t1:.1f}s")
+
+
 def binning_case(name, scene, cam):
     R = rras.Rasterizer(Args(), "cpu", "float")
     wcam = warp_camera(cam)
@@ -388,7 +524,7 @@ def edge_scene(seed):
 
 
 def main():
-    which = sys.argv[1:] or ["raster_small", "raster_edge", "raster_dense", "bin_large", "interpen_small", "trace_small"]
+    which = sys.argv[1:] or ["raster_small", "raster_edge", "raster_dense", "bin_large", "interpen_small", "raster_generic", "trace_small"]
     if "raster_small" in which:
         sc = make_scene(1, 120, -0.6, 0.6, 0.05, 0.2)
         raster_case("raster_small", sc, look_at_camera((0.3, 0.4, 2.0), (0, 0, 0), 36, 28, 60.0), 1)
@@ -406,6 +542,11 @@ def main():
         binning_case("bin_large", sc, look_at_camera((1.0, 0.5, 2.6), (0, 0, 0), 96, 64, 50.0))
     if "interpen_small" in which:
         interpen_case("interpen_small", 6)
+    if "raster_generic" in which:
+        # per-pixel rays of a wide fisheye; 40x28 so the last tiles are ragged
+        sc = make_scene(8, 220, -0.9, 0.9, 0.06, 0.22)
+        cam = look_at_camera((0.3, -0.2, 2.1), (0, 0, 0), 40, 28, 60.0)
+        generic_case("raster_generic", sc, cam, fisheye_ray_maps(cam, 80.0), 8)
     if "trace_small" in which:
         sc = make_scene(4, 150, -0.6, 0.6, 0.08, 0.2)
         trace_case("trace_small", sc, look_at_camera((0.2, 0.3, 2.2), (0, 0, 0), 24, 20, 60.0))

@@ -326,6 +326,9 @@ def install():
     wp.tile_sum = tile_sum
     wp.tile_load = tile_load
     wp.math = types.SimpleNamespace(norm_l1=norm_l1)
+    # fixed-size local matrices (the generic binning's traversal stacks, the
+    # cone builders' scratch): zero-initialised numpy arrays of that type
+    wp.mat = lambda shape, dtype: np.zeros(shape, dtype=np.int32 if dtype in (_int32, _uint32, _int64) else F32)
     wp.launch = launch
     wp.cw_div = lambda a, b: a / b
     wp.Bvh = None

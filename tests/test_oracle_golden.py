@@ -100,3 +100,38 @@ def test_f16_rounding_matches_numpy():
     x = np.concatenate([rng.standard_normal(2000) * 10 ** rng.uniform(-9, 5, 2000),
                         [0.0, -0.0, 65504.0, 65520.0, 1e-8, 6.1e-5, np.inf, -np.inf]]).astype(np.float32)
     assert np.array_equal(orc.f2h(x), x.astype(np.float16).view(np.uint16))
+
+
+# ---------------------------------------------------------------------------
+# generic camera (is_pinhole=False): cone-hierarchy binning and per-pixel rays
+
+
+def test_generic_binning_and_cones_bit_exact(golden):
+    g = golden("raster_generic")
+    sph, _, _ = packed(g)
+    keys, prims, offs, _, cones = orc.bin_generic(_cam(g), g["ray_maps"], sph, 8)
+    assert np.array_equal(cones.view(np.uint32), g["cones"].view(np.uint32))
+    assert np.array_equal(keys, g["sort_keys"])
+    assert np.array_equal(prims, g["tile_prims"])
+    assert np.array_equal(offs, g["tile_offsets"])
+
+
+def test_generic_forward_and_backward(golden):
+    g = golden("raster_generic")
+    sph, nsig, rgbh = packed(g)
+    o = orc.raster_forward(_cam(g), 8, sph, nsig, g["texel_sites"], rgbh, g["adjacency"], g["adjacency_offsets"],
+                           g["adjacency_diff"], g["tile_offsets"], g["tile_prims"], g["depth_quantiles"], g["ray_gt"],
+                           float(g["thr"]), True, ray_maps=g["ray_maps"])
+    assert np.array_equal(o["early_stop"], g["early_stop"])
+    for k in ["color", "normal_distance", "normal", "quantile_depths", "log_t"]:
+        assert max_abs(o[k], g[k]) <= 1e-5, k
+    for k in ["contrib", "point_err"]:
+        assert_close_rel(o[k], g[k], 1e-5, k)
+    gr = orc.raster_backward(_cam(g), 8, sph, nsig, g["texel_sites"], rgbh, g["adjacency"], g["adjacency_offsets"],
+                             g["adjacency_diff"], g["tile_offsets"], g["tile_prims"], g["early_stop"], g["log_t"],
+                             g["grad_color"], g["grad_log_t"], g["grad_normal_distance"], g["grad_normal"],
+                             g["grad_contrib"], g["depth_quantiles"], g["grad_quantile_depths"],
+                             ray_maps=g["ray_maps"])
+    for a, b in [("spheres", "spheres_grad"), ("nsigmas", "nsigmas_grad"), ("texel_sites", "texel_sites_grad"),
+                 ("texel_rgb", "texel_rgb_grad"), ("texel_height", "texel_height_grad")]:
+        assert_close_rel(gr[a], g[b], 1e-4, a)
