@@ -82,6 +82,13 @@ typedef struct pf_raster_inputs {
     void *scratch;               /* >= 256 bytes of device scratch for the
                                     tile work queue, or NULL (one warp group
                                     per tile, no queue) */
+    const float *ray_maps;       /* (H,W,6) f32 per-pixel ray origin and
+                                    direction of a generic camera
+                                    (TorchCamera.ray_maps, is_pinhole=False;
+                                    rasterize.py:944-954) for the forward and
+                                    backward, or NULL for the pinhole rays;
+                                    the benchmark and viewer paths are
+                                    pinhole only, as in the reference */
 } pf_raster_inputs;
 
 /* ---------------------------------------------------------------------- */
@@ -124,6 +131,22 @@ PF_API int pf_bin_noalloc(const pf_camera *cam, int32_t tile_width, const float 
                           int64_t pair_capacity, int64_t *tile_offsets, int32_t *tile_prims, int64_t *sort_keys,
                           uint8_t *prim_visible, int32_t *tile_order, int64_t *n_pairs, int32_t *status,
                           void *stream);
+
+/* Binning for a generic camera (TorchCamera.ray_maps with is_pinhole=False).
+ * Replaces _precompute_cones, compute_leaf_cones_kernel, merge_cones_kernel
+ * and count/write_visible_generic_kernel (rasterize.py:202-291, 365-569,
+ * 1518-1585): ray cones over 2x2-pixel leaves merged level by level to one
+ * root, each primitive descending into every cone its sphere meets
+ * (camera.py:28-44) down to the level whose cones are the tiles.  ray_maps
+ * is (H,W,6) f32 (origin, direction); tile_width must be a power of two
+ * (8, 16 or 32 for the compositing kernels).  Outputs, ordering and *status
+ * as for pf_bin; the workspace also holds the cones. */
+PF_API int pf_bin_generic_workspace_size(int64_t n_prims, int64_t pair_capacity, int32_t width, int32_t height,
+                                         int32_t tile_width, size_t *bytes);
+PF_API int pf_bin_generic(const pf_camera *cam, const float *ray_maps, int32_t tile_width, const float *spheres,
+                          int64_t n_prims, void *workspace, size_t workspace_bytes, int64_t pair_capacity,
+                          int64_t *tile_offsets, int32_t *tile_prims, int64_t *sort_keys, uint8_t *prim_visible,
+                          int32_t *tile_order, int64_t *n_pairs, int32_t *status, void *stream);
 
 /* ---------------------------------------------------------------------- */
 /* Neighbour encodings.

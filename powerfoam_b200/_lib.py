@@ -64,6 +64,7 @@ class PfRasterInputs(ctypes.Structure):
         ("transmittance_threshold", c_f),
         ("tile_order", c_vp),
         ("scratch", c_vp),
+        ("ray_maps", c_vp),
     ]
 
 
@@ -134,6 +135,9 @@ _SIGS = {
     "pf_bin_workspace_size": [c_i64, c_i64, c_i64, ctypes.POINTER(ctypes.c_size_t)],
     "pf_bin": [ctypes.POINTER(PfCamera), c_i32, c_vp, c_i64, c_vp, ctypes.c_size_t, c_i64, c_vp, c_vp, c_vp, c_vp,
                c_vp, c_vp, c_vp, c_vp],
+    "pf_bin_generic_workspace_size": [c_i64, c_i64, c_i32, c_i32, c_i32, c_vp],
+    "pf_bin_generic": [ctypes.POINTER(PfCamera), c_vp, c_i32, c_vp, c_i64, c_vp, ctypes.c_size_t, c_i64, c_vp, c_vp,
+                       c_vp, c_vp, c_vp, c_vp, c_vp, c_vp],
     "pf_bin_noalloc": [ctypes.POINTER(PfCamera), c_i32, c_vp, c_i64, c_i64, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp,
                        c_vp, c_vp],
     "pf_adjacency_prefetch": [c_vp, c_vp, c_vp, c_i64, c_vp, c_vp],

@@ -1,4 +1,4 @@
-"""Pinhole camera of the rendering path.
+"""Camera of the rendering path (pinhole, or generic through ray maps).
 
 TorchCamera keeps the fields and helpers of the reference's TorchCamera
 (powerfoam/camera.py:181-305): ``eye``, ``right``, ``up`` with
@@ -49,6 +49,13 @@ class TorchCamera:
         x = 2.0 * j / (float(self.width) - 1.0) - 1.0
         y = 1.0 - 2.0 * i / (float(self.height) - 1.0)
         return x[:, None] * self.right[None, :] + y[:, None] * self.up[None, :] + forward[None, :]
+
+    def build_pinhole_ray_maps(self):
+        """(H, W, 6) origins and unit directions of the pinhole rays, the ray
+        maps the reference builds when none are given (camera.py:198-215)."""
+        d = self.ray_directions().reshape(-1, 3)
+        o = self.eye[None, :].expand(d.shape[0], 3)
+        return torch.cat([o, d], dim=-1).view(self.height, self.width, 6)
 
     def ray_directions(self):
         """(H, W, 3) unit ray directions."""

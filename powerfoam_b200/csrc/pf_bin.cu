@@ -118,9 +118,167 @@ PF_D bool prim_tile_range(const Cam& cam, int TW, v3 center, float radius, TileR
     return true;
 }
 
+// ---------------------------------------------------------------------------
+// Generic cameras (rasterize.py:202-291, 365-569, 1518-1585): a hierarchy of
+// ray cones over the ray map -- leaves of 2x2 pixels, each level merging 2x2
+// children, up to one root -- and a per-primitive descent into every child
+// cone the sphere meets (camera.py:28-44); the cones of the tile level are
+// the tiles.  Level sizes are host-known; the cones live in the workspace.
+constexpr int kConeLeaf = 2;
+constexpr int kConeMaxLevels = 24;
+constexpr int kConeStack = 4 * kConeMaxLevels;
+
+struct ConeTree {
+    const float4* cones;
+    int n_levels, tile_level;
+    int off[kConeMaxLevels], dh[kConeMaxLevels], dw[kConeMaxLevels];
+};
+
+// level sizes of an H x W image and the level whose cones are TW x TW tiles;
+// false if the image needs more levels or TW is not a power of two >= 2
+static bool cone_layout(int H, int W, int TW, ConeTree& ct, int64_t* total) {
+    if (TW < kConeLeaf || (TW & (TW - 1))) return false;
+    int dh = (H + kConeLeaf - 1) / kConeLeaf, dw = (W + kConeLeaf - 1) / kConeLeaf;
+    int64_t t = 0;
+    ct.n_levels = 0;
+    for (;;) {
+        if (ct.n_levels == kConeMaxLevels) return false;
+        ct.off[ct.n_levels] = (int)t;
+        ct.dh[ct.n_levels] = dh;
+        ct.dw[ct.n_levels] = dw;
+        ct.n_levels++;
+        t += (int64_t)dh * dw;
+        if (dh == 1 && dw == 1) break;
+        dh = (dh + 1) / 2;
+        dw = (dw + 1) / 2;
+    }
+    ct.tile_level = 0;
+    for (int sz = kConeLeaf; sz < TW; sz *= 2) ct.tile_level++;
+    *total = t;
+    return true;
+}
+
+// compute_leaf_cones_kernel (rasterize.py:473-515): axis = normalised sum of
+// the unit rays of the 2x2 pixels, cos half angle = min dot (2: no ray)
+__global__ void cone_leaf_kernel(const float* __restrict__ ray_maps, int H, int W, int leaf_w, int64_t n,
+                                 float4* __restrict__ cones) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const int a = (int)(t / leaf_w), b = (int)(t % leaf_w);
+    v3 sum = mk(0.f, 0.f, 0.f), rays[4];
+    int valid = 0;
+    for (int di = 0; di < kConeLeaf; di++)
+        for (int dj = 0; dj < kConeLeaf; dj++) {
+            const int pi = imin(a * kConeLeaf + di, H - 1), pj = imin(b * kConeLeaf + dj, W - 1);
+            const float* m = ray_maps + 6 * ((int64_t)pi * W + pj) + 3;
+            const v3 ray = mk(m[0], m[1], m[2]);
+            const float len = length(ray);
+            if (len > 1.0e-6f) {
+                const v3 rn = ray / len;
+                rays[valid++] = rn;
+                sum = sum + rn;
+            }
+        }
+    if (valid == 0) {
+        cones[t] = make_float4(0.f, 0.f, 0.f, 2.0f);
+        return;
+    }
+    const v3 axis = normalize(sum);
+    float ch = 1.0f;
+    for (int i = 0; i < valid; i++) ch = fmin_t(ch, dot(axis, rays[i]));
+    cones[t] = make_float4(axis.x, axis.y, axis.z, ch);
+}
+
+// merge_cones_kernel (rasterize.py:517-569)
+__global__ void cone_merge_kernel(float4* __restrict__ cones, int parent_off, int child_off, int parent_w,
+                                  int child_h, int child_w, int64_t n) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const int a = (int)(t / parent_w), b = (int)(t % parent_w);
+    v3 sum = mk(0.f, 0.f, 0.f), axes[4];
+    float chs[4];
+    int valid = 0;
+    for (int di = 0; di < 2; di++)
+        for (int dj = 0; dj < 2; dj++) {
+            const int ca = 2 * a + di, cb = 2 * b + dj;
+            if (ca < child_h && cb < child_w) {
+                const float4 c = cones[child_off + (int64_t)ca * child_w + cb];
+                if (c.w <= 1.0f) {
+                    axes[valid] = mk(c.x, c.y, c.z);
+                    chs[valid] = c.w;
+                    sum = sum + axes[valid];
+                    valid++;
+                }
+            }
+        }
+    if (valid == 0) {
+        cones[parent_off + t] = make_float4(0.f, 0.f, 0.f, 2.0f);
+        return;
+    }
+    const v3 axis = normalize(sum);
+    float ch = 1.0f;
+    for (int i = 0; i < valid; i++) {
+        const float dv = dot(axis, axes[i]);
+        const float sin_angle = sqrtf(fmax_t(1.0f - dv * dv, 0.0f));
+        const float sin_child = sqrtf(fmax_t(1.0f - chs[i] * chs[i], 0.0f));
+        ch = fmin_t(ch, dv * chs[i] - sin_angle * sin_child);
+    }
+    cones[parent_off + t] = make_float4(axis.x, axis.y, axis.z, ch);
+}
+
+// camera.py:28-44
+PF_D bool sphere_cone(v3 center, float radius, v3 eye, v3 axis, float cos_half) {
+    const v3 v = center - eye;
+    const float dist = length(v);
+    const float cos_alpha = dot(v, axis) / dist;
+    const float sin_half = sqrtf(1.0f - cos_half * cos_half);
+    const float sin_beta = radius / dist;
+    const float cos_beta = sqrtf(1.0f - sin_beta * sin_beta);
+    const float threshold = cos_half * cos_beta - sin_half * sin_beta;
+    return cos_alpha > threshold;
+}
+
+// the generic kernels' cull and descent (rasterize.py:214-291): calls
+// emit(tile) for every tile-level cone the sphere reaches; false if culled
+template <typename Emit>
+PF_D bool cone_tiles(const Cam& cam, const ConeTree& ct, int tiles_h, v3 c, float r, Emit emit) {
+    const v3 v = c - cam.eye;
+    const v3 forward = cross(cam.up, cam.right);
+    if (length(v) < 4.0f * r || dot(v, forward) < 0.1f) return false;
+    int st_l[kConeStack], st_a[kConeStack], st_b[kConeStack];
+    int n = 1;
+    st_l[0] = ct.n_levels - 1;
+    st_a[0] = 0;
+    st_b[0] = 0;
+    while (n > 0) {
+        n--;
+        const int level = st_l[n], a = st_a[n], b = st_b[n];
+        const float4 cn = ct.cones[ct.off[level] + (int64_t)a * ct.dw[level] + b];
+        if (cn.w > 1.0f) continue;
+        if (!sphere_cone(c, r, cam.eye, mk(cn.x, cn.y, cn.z), cn.w)) continue;
+        if (level == ct.tile_level) {
+            emit(a + b * tiles_h);
+            continue;
+        }
+        const int cl = level - 1;
+        for (int di = 0; di < 2; di++)
+            for (int dj = 0; dj < 2; dj++) {
+                const int ca = 2 * a + di, cb = 2 * b + dj;
+                if (ca < ct.dh[cl] && cb < ct.dw[cl]) {  // at most 1 + 3 (levels - 1) entries
+                    st_l[n] = cl;
+                    st_a[n] = ca;
+                    st_b[n] = cb;
+                    n++;
+                }
+            }
+    }
+    return true;
+}
+
+template <bool GEN>
 __global__ void bin_count_kernel(pf_camera camera, int TW, const float4* __restrict__ spheres, int64_t N,
                                  int32_t* __restrict__ counts, uint32_t* __restrict__ depth_key,
-                                 uint32_t* __restrict__ depth_by_prim, uint32_t* __restrict__ idx) {
+                                 uint32_t* __restrict__ depth_by_prim, uint32_t* __restrict__ idx, ConeTree ct) {
     int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= N) return;
     Cam cam = load_cam(camera);
@@ -132,11 +290,15 @@ __global__ void bin_count_kernel(pf_camera camera, int TW, const float4* __restr
     depth_by_prim[p] = __float_as_uint(pow_dist);
     idx[p] = (uint32_t)p;
     int n = 0;
-    TileRange tr;
-    if (prim_tile_range(cam, TW, c, s.w, tr)) {
-        for (int ti = tr.ti0; ti <= tr.ti1; ti++)
-            for (int tj = tr.tj0; tj <= tr.tj1; tj++)
-                if (tile_obb(ti, tj, cam, TW, tr.o)) n++;
+    if constexpr (GEN) {
+        cone_tiles(cam, ct, 1 + (cam.H - 1) / TW, c, s.w, [&](int) { n++; });
+    } else {
+        TileRange tr;
+        if (prim_tile_range(cam, TW, c, s.w, tr)) {
+            for (int ti = tr.ti0; ti <= tr.ti1; ti++)
+                for (int tj = tr.tj0; tj <= tr.tj1; tj++)
+                    if (tile_obb(ti, tj, cam, TW, tr.o)) n++;
+        }
     }
     counts[p] = n;
 }
@@ -147,11 +309,12 @@ __global__ void gather_counts_kernel(const uint32_t* __restrict__ order, const i
     if (k < N) sorted_counts[k] = counts[order[k]];
 }
 
+template <bool GEN>
 __global__ void bin_emit_kernel(pf_camera camera, int TW, const float4* __restrict__ spheres, int64_t N,
                                 const uint32_t* __restrict__ order, const int32_t* __restrict__ sorted_counts,
                                 const int64_t* __restrict__ offsets, const int64_t* __restrict__ total,
                                 int64_t capacity, uint32_t* __restrict__ tile_key, uint32_t* __restrict__ pair_prim,
-                                uint8_t* __restrict__ prim_visible) {
+                                uint8_t* __restrict__ prim_visible, ConeTree ct) {
     int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= N) return;
     if (*total > capacity) return;
@@ -163,6 +326,18 @@ __global__ void bin_emit_kernel(pf_camera camera, int TW, const float4* __restri
     float4 s = spheres[p];
     v3 c = mk(s.x, s.y, s.z);
     int64_t pos = offsets[k];
+    if constexpr (GEN) {
+        // the descent finds the same tiles as the counting pass did
+        const int64_t end = pos + sorted_counts[k];
+        cone_tiles(cam, ct, tiles_h, c, s.w, [&](int tile) {
+            if (pos < end) {
+                tile_key[pos] = (uint32_t)tile;
+                pair_prim[pos] = p;
+                pos++;
+            }
+        });
+        return;
+    }
     TileRange tr;
     if (!prim_tile_range(cam, TW, c, s.w, tr)) return;
     for (int ti = tr.ti0; ti <= tr.ti1; ti++)
@@ -282,10 +457,11 @@ extern "C" int pf_pack_prims(const float* points, const float* radii, const floa
     return pf_check_launch("pf_pack_prims");
 }
 
-extern "C" int pf_bin(const pf_camera* cam, int32_t tile_width, const float* spheres, int64_t n_prims,
-                      void* workspace, size_t workspace_bytes, int64_t pair_capacity, int64_t* tile_offsets,
-                      int32_t* tile_prims, int64_t* sort_keys, uint8_t* prim_visible, int32_t* tile_order,
-                      int64_t* n_pairs, int32_t* status, void* stream) {
+// the pinhole binning (ct == NULL) or the generic one over a built cone tree
+static int bin_impl(const pf_camera* cam, int32_t tile_width, const float* spheres, int64_t n_prims,
+                    void* workspace, size_t workspace_bytes, int64_t pair_capacity, int64_t* tile_offsets,
+                    int32_t* tile_prims, int64_t* sort_keys, uint8_t* prim_visible, int32_t* tile_order,
+                    int64_t* n_pairs, int32_t* status, void* stream, const ConeTree* ct) {
     if (!cam || tile_width <= 0 || n_prims < 0 || pair_capacity < 0 || pair_capacity >= (int64_t)1 << 31 ||
         !tile_offsets || !n_pairs || !status || (n_prims > 0 && !spheres) || (pair_capacity > 0 && !tile_prims))
         return pf_fail(PF_ERR_ARGS, "pf_bin: bad arguments");
@@ -294,6 +470,7 @@ extern "C" int pf_bin(const pf_camera* cam, int32_t tile_width, const float* sph
     BinLayout L = bin_layout(n_prims, pair_capacity, T_);
     if (workspace_bytes < L.bytes || (!workspace && L.bytes)) return pf_fail(PF_ERR_ARGS, "pf_bin: workspace too small");
     cudaStream_t st = (cudaStream_t)stream;
+    const ConeTree no_cones{};
     char* ws = (char*)workspace;
     int32_t* counts = (int32_t*)(ws + L.counts);
     uint32_t* dprim = (uint32_t*)(ws + L.dprim);
@@ -328,13 +505,22 @@ extern "C" int pf_bin(const pf_camera* cam, int32_t tile_width, const float* sph
         return pf_check_launch("pf_bin");
     }
     const unsigned gN = (unsigned)((n_prims + 255) / 256);
-    bin_count_kernel<<<gN, 256, 0, st>>>(*cam, TW, (const float4*)spheres, n_prims, counts, dkey0, dprim, idx0);
+    if (ct)
+        bin_count_kernel<true><<<gN, 256, 0, st>>>(*cam, TW, (const float4*)spheres, n_prims, counts, dkey0, dprim,
+                                                   idx0, *ct);
+    else
+        bin_count_kernel<false><<<gN, 256, 0, st>>>(*cam, TW, (const float4*)spheres, n_prims, counts, dkey0, dprim,
+                                                    idx0, no_cones);
     // stable sort of primitives by depth bits: 4 passes, result back in (dkey0, idx0)
     radix_sort_pairs(dkey0, idx0, dkey1, idx1, dkey0, idx0, n_prims, nullptr, 32, rs, st);
     gather_counts_kernel<<<gN, 256, 0, st>>>(idx0, counts, n_prims, scounts);
     exclusive_scan<int32_t, int64_t>(scounts, offsets, n_prims, spart, n_pairs, st);
-    bin_emit_kernel<<<gN, 256, 0, st>>>(*cam, TW, (const float4*)spheres, n_prims, idx0, scounts, offsets, n_pairs,
-                                        pair_capacity, pkey0, pprim0, prim_visible);
+    if (ct)
+        bin_emit_kernel<true><<<gN, 256, 0, st>>>(*cam, TW, (const float4*)spheres, n_prims, idx0, scounts, offsets,
+                                                  n_pairs, pair_capacity, pkey0, pprim0, prim_visible, *ct);
+    else
+        bin_emit_kernel<false><<<gN, 256, 0, st>>>(*cam, TW, (const float4*)spheres, n_prims, idx0, scounts, offsets,
+                                                   n_pairs, pair_capacity, pkey0, pprim0, prim_visible, no_cones);
     // stable sort of the pairs by tile
     int bits = 0;
     while (((int64_t)1 << bits) < T) bits++;
@@ -346,6 +532,58 @@ extern "C" int pf_bin(const pf_camera* cam, int32_t tile_width, const float* sph
                                                                            sort_keys, status);
     order();
     return pf_check_launch("pf_bin");
+}
+
+extern "C" int pf_bin(const pf_camera* cam, int32_t tile_width, const float* spheres, int64_t n_prims,
+                      void* workspace, size_t workspace_bytes, int64_t pair_capacity, int64_t* tile_offsets,
+                      int32_t* tile_prims, int64_t* sort_keys, uint8_t* prim_visible, int32_t* tile_order,
+                      int64_t* n_pairs, int32_t* status, void* stream) {
+    return bin_impl(cam, tile_width, spheres, n_prims, workspace, workspace_bytes, pair_capacity, tile_offsets,
+                    tile_prims, sort_keys, prim_visible, tile_order, n_pairs, status, stream, nullptr);
+}
+
+extern "C" int pf_bin_generic_workspace_size(int64_t n_prims, int64_t pair_capacity, int32_t width, int32_t height,
+                                             int32_t tile_width, size_t* bytes) {
+    ConeTree ct{};
+    int64_t n_cones = 0;
+    if (!bytes || width < 2 || height < 2 || !cone_layout(height, width, tile_width, ct, &n_cones))
+        return pf_fail(PF_ERR_ARGS, "pf_bin_generic_workspace_size: bad arguments (tile_width must be 2, 4, 8, ...)");
+    const int64_t T = (int64_t)(1 + (height - 1) / tile_width) * (1 + (width - 1) / tile_width);
+    size_t b = 0;
+    int rc = pf_bin_workspace_size(n_prims, pair_capacity, T, &b);
+    if (rc != PF_OK) return rc;
+    *bytes = align_up(b) + align_up(16 * (size_t)n_cones);
+    return PF_OK;
+}
+
+extern "C" int pf_bin_generic(const pf_camera* cam, const float* ray_maps, int32_t tile_width, const float* spheres,
+                              int64_t n_prims, void* workspace, size_t workspace_bytes, int64_t pair_capacity,
+                              int64_t* tile_offsets, int32_t* tile_prims, int64_t* sort_keys, uint8_t* prim_visible,
+                              int32_t* tile_order, int64_t* n_pairs, int32_t* status, void* stream) {
+    ConeTree ct{};
+    int64_t n_cones = 0;
+    if (!cam || !ray_maps || cam->width < 2 || cam->height < 2 ||
+        !cone_layout(cam->height, cam->width, tile_width, ct, &n_cones))
+        return pf_fail(PF_ERR_ARGS, "pf_bin_generic: bad camera, ray maps or tile width (2, 4, 8, ...)");
+    size_t need = 0;
+    int rc = pf_bin_generic_workspace_size(n_prims, pair_capacity, cam->width, cam->height, tile_width, &need);
+    if (rc != PF_OK) return rc;
+    if (!workspace || workspace_bytes < need) return pf_fail(PF_ERR_ARGS, "pf_bin_generic: workspace too small");
+    const int64_t T = (int64_t)(1 + (cam->height - 1) / tile_width) * (1 + (cam->width - 1) / tile_width);
+    const size_t bin_bytes = align_up(bin_layout(n_prims, pair_capacity, T).bytes);
+    float4* cones = (float4*)((char*)workspace + bin_bytes);
+    ct.cones = cones;
+    cudaStream_t st = (cudaStream_t)stream;
+    const int64_t n_leaf = (int64_t)ct.dh[0] * ct.dw[0];
+    cone_leaf_kernel<<<(unsigned)((n_leaf + 255) / 256), 256, 0, st>>>(ray_maps, cam->height, cam->width, ct.dw[0],
+                                                                       n_leaf, cones);
+    for (int l = 1; l < ct.n_levels; l++) {
+        const int64_t n = (int64_t)ct.dh[l] * ct.dw[l];
+        cone_merge_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(cones, ct.off[l], ct.off[l - 1], ct.dw[l],
+                                                                       ct.dh[l - 1], ct.dw[l - 1], n);
+    }
+    return bin_impl(cam, tile_width, spheres, n_prims, workspace, bin_bytes, pair_capacity, tile_offsets, tile_prims,
+                    sort_keys, prim_visible, tile_order, n_pairs, status, stream, &ct);
 }
 
 // ---------------------------------------------------------------------------

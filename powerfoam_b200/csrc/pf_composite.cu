@@ -34,12 +34,15 @@
 
 namespace pf {
 
-template <int TW>
+// GEN: a generic camera (per-pixel rays from ray maps); it takes the
+// one-pixel-per-lane (or two-per-lane) path, not the pair-compacted one
+template <int TW, bool GEN = false>
 __global__ void __launch_bounds__(Layout<TW>::THREADS) raster_fwd_kernel(RasterParams P, FwdOut out) {
     constexpr int G = Layout<TW>::G;
-    // the two-pixels-per-lane layout stages per warp here; the compacted
-    // one-pixel-per-lane path keeps its staging in dynamic shared memory
-    __shared__ WarpStage stage[Layout<TW>::PPL == 1 ? 1 : G];
+    constexpr bool COMPACT = Layout<TW>::PPL == 1 && !GEN;
+    // the per-pixel layouts stage per warp here; the compacted one keeps its
+    // staging in dynamic shared memory
+    __shared__ WarpStage stage[COMPACT ? 1 : G];
     __shared__ StopState ss;
     extern __shared__ float4 fwd_dyn[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -47,21 +50,21 @@ __global__ void __launch_bounds__(Layout<TW>::THREADS) raster_fwd_kernel(RasterP
     for (;;) {
         int64_t tile = next_tile<G>(P, static_next, lane, &ss);
         if (tile < 0) break;
-        if constexpr (Layout<TW>::PPL == 1)
+        if constexpr (COMPACT)
             fwd_tile_c<G>(P, out, tile, warp, lane, reinterpret_cast<FwdCStage*>(fwd_dyn)[warp], ss);
         else
-            fwd_tile<G, Layout<TW>::PPL>(P, out, tile, warp, lane, stage[warp], ss);
+            fwd_tile<G, Layout<TW>::PPL, GEN>(P, out, tile, warp, lane, stage[warp], ss);
     }
 }
 
 // dynamic shared memory of the forward: the pair-compaction stage per warp
-template <int TW>
+template <int TW, bool GEN = false>
 constexpr size_t fwd_dyn_bytes() {
-    return Layout<TW>::PPL == 1 ? sizeof(FwdCStage) * Layout<TW>::G : 0;
+    return (Layout<TW>::PPL == 1 && !GEN) ? sizeof(FwdCStage) * Layout<TW>::G : 0;
 }
 
 
-template <int TW>
+template <int TW, bool GEN = false>
 __global__ void __launch_bounds__(Layout<TW>::THREADS, Layout<TW>::BWD_MIN_BLOCKS)
 raster_bwd_kernel(RasterParams P, BwdIn in, GradOut go) {
     constexpr int G = Layout<TW>::G;
@@ -76,7 +79,7 @@ raster_bwd_kernel(RasterParams P, BwdIn in, GradOut go) {
     for (;;) {
         int64_t tile = next_tile<G>(P, static_next, lane, nullptr);
         if (tile < 0) break;
-        bwd_tile<G, Layout<TW>::PPL>(P, in, go, tile, warp, lane, stage[warp], bs);
+        bwd_tile<G, Layout<TW>::PPL, GEN>(P, in, go, tile, warp, lane, stage[warp], bs);
     }
 }
 
@@ -102,17 +105,22 @@ static unsigned composite_grid(const RasterParams& P, K kernel, size_t dyn_smem)
     return (unsigned)std::max<int64_t>(1, std::min<int64_t>(groups, resident));
 }
 
-template <int TW>
-static int launch_fwd(const RasterParams& P, const FwdOut& out, cudaStream_t st) {
-    const size_t dyn = fwd_dyn_bytes<TW>();
+template <int TW, bool GEN>
+static int launch_fwd_t(const RasterParams& P, const FwdOut& out, cudaStream_t st) {
+    const size_t dyn = fwd_dyn_bytes<TW, GEN>();
     if (dyn > 0) {
-        cudaError_t e = cudaFuncSetAttribute(raster_fwd_kernel<TW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        cudaError_t e = cudaFuncSetAttribute(raster_fwd_kernel<TW, GEN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)dyn);
         if (e != cudaSuccess) return pf_fail(PF_ERR_CUDA, cudaGetErrorString(e));
     }
-    unsigned grid = composite_grid<TW>(P, raster_fwd_kernel<TW>, dyn);
-    raster_fwd_kernel<TW><<<grid, Layout<TW>::THREADS, dyn, st>>>(P, out);
+    unsigned grid = composite_grid<TW>(P, raster_fwd_kernel<TW, GEN>, dyn);
+    raster_fwd_kernel<TW, GEN><<<grid, Layout<TW>::THREADS, dyn, st>>>(P, out);
     return PF_OK;
+}
+
+template <int TW>
+static int launch_fwd(const RasterParams& P, const FwdOut& out, cudaStream_t st) {
+    return P.ray_maps ? launch_fwd_t<TW, true>(P, out, st) : launch_fwd_t<TW, false>(P, out, st);
 }
 
 }  // namespace pf
@@ -149,12 +157,20 @@ extern "C" int pf_raster_forward(const pf_raster_inputs* in, int32_t return_poin
     return pf_check_launch("pf_raster_forward");
 }
 
+template <int TW, bool GEN>
+static void launch_bwd_t(const RasterParams& P, const BwdIn& bi, const GradOut& go, cudaStream_t st) {
+    const size_t dyn = sizeof(BwdStage) * Layout<TW>::G;
+    cudaFuncSetAttribute(raster_bwd_kernel<TW, GEN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
+    unsigned grid = composite_grid<TW>(P, raster_bwd_kernel<TW, GEN>, dyn);
+    raster_bwd_kernel<TW, GEN><<<grid, Layout<TW>::THREADS, dyn, st>>>(P, bi, go);
+}
+
 template <int TW>
 static void launch_bwd(const RasterParams& P, const BwdIn& bi, const GradOut& go, cudaStream_t st) {
-    const size_t dyn = sizeof(BwdStage) * Layout<TW>::G;
-    cudaFuncSetAttribute(raster_bwd_kernel<TW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
-    unsigned grid = composite_grid<TW>(P, raster_bwd_kernel<TW>, dyn);
-    raster_bwd_kernel<TW><<<grid, Layout<TW>::THREADS, dyn, st>>>(P, bi, go);
+    if (P.ray_maps)
+        launch_bwd_t<TW, true>(P, bi, go, st);
+    else
+        launch_bwd_t<TW, false>(P, bi, go, st);
 }
 
 extern "C" int pf_raster_backward(const pf_raster_inputs* in, const int32_t* early_stop, const float* log_t,

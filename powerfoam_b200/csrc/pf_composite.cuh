@@ -135,6 +135,7 @@ PF_D bool face_may_clip(float dp, float num, float tn, float tf) {
 // forward
 struct FwdPix {
     PixGeom g;
+    v3 o;  // ray origin (generic cameras)
     float log_t, trans, nd, err;
     v3 rgb, nrm, gt;
     int qi;
@@ -147,6 +148,26 @@ PF_D void swap_pix(FwdPix& a, FwdPix& b) {
     FwdPix t = a;
     a = b;
     b = t;
+}
+
+// The origin of pixel x's ray: the eye, or with a generic camera its own.
+template <bool GEN, typename X>
+PF_D v3 ray_org(const X& x, v3 eye) {
+    if constexpr (GEN)
+        return x.o;
+    else
+        return eye;
+}
+
+// Face numerator for pixel x.  The staged value is face_offset - eye . n for
+// a pinhole camera; a generic camera stages face_offset alone (eye = 0) and
+// subtracts its own origin here, as rendering_math.py:71-80 does per ray.
+template <bool GEN, typename X>
+PF_D float face_num(const float4& f, v3 fn, const X& x) {
+    if constexpr (GEN)
+        return f.w - dot(x.o, fn);
+    else
+        return f.w;
 }
 
 struct FwdOut {
@@ -164,7 +185,7 @@ struct FwdOut {
     int* status;
 };
 
-template <int G, int PPL>
+template <int G, int PPL, bool GEN = false>
 PF_D void fwd_tile(const RasterParams& P, const FwdOut& out, int64_t tile, int wig, int lane, WarpStage& ws,
                    StopState& ss) {
     const int TS = P.TW * P.TW;
@@ -180,6 +201,7 @@ PF_D void fwd_tile(const RasterParams& P, const FwdOut& out, int64_t tile, int w
         FwdPix& x = a;
         int idx = wig * 32 + lane + s * (TS / 2);
         x.g = pixel_geom(P, tile, idx);
+        if constexpr (GEN) pixel_ray_map(P, x.g, x.o);
         x.log_t = 0.f;
         x.trans = 1.0f;
         x.nd = 0.f;
@@ -223,8 +245,8 @@ PF_D void fwd_tile(const RasterParams& P, const FwdOut& out, int64_t tile, int w
             const float4 s4 = ws.sph[kk];
             const v3 center = mk(s4.x, s4.y, s4.z);
             const float radius = s4.w;
-            a.hit = a.g.oob ? false : ray_sphere(o, a.g.d, center, radius, a.tn, a.tf);
-            if (PPL == 2) b.hit = b.g.oob ? false : ray_sphere(o, b.g.d, center, radius, b.tn, b.tf);
+            a.hit = a.g.oob ? false : ray_sphere(ray_org<GEN>(a, o), a.g.d, center, radius, a.tn, a.tf);
+            if (PPL == 2) b.hit = b.g.oob ? false : ray_sphere(ray_org<GEN>(b, o), b.g.d, center, radius, b.tn, b.tf);
             // The reference skips a primitive no pixel of the tile hits (tile_sum);
             // the skip changes no output, so each warp decides for its own pixels.
             if (!__any_sync(0xffffffffu, a.hit || b.hit)) continue;
@@ -236,7 +258,7 @@ PF_D void fwd_tile(const RasterParams& P, const FwdOut& out, int64_t tile, int w
             const int n_adj = __ldg(&P.adj_off[prim + 1]) - a0;
             const float cc = dot(center, center), rr = radius * radius;
             for (int e0 = 0; e0 < n_adj; e0 += 32) {
-                stage_faces(ws, P, a0, e0, n_adj, o, center, cc, rr, lane);
+                stage_faces(ws, P, a0, e0, n_adj, GEN ? mk(0.f, 0.f, 0.f) : o, center, cc, rr, lane);
                 const int en = min(32, n_adj - e0);
 #pragma unroll 2
                 for (int q = 0; q < en; q++) {
@@ -244,16 +266,18 @@ PF_D void fwd_tile(const RasterParams& P, const FwdOut& out, int64_t tile, int w
                     const v3 fn = mk(f.x, f.y, f.z);
                     if (a.hit) {
                         float dp = dot(a.g.d, fn);
-                        if (face_may_clip(dp, f.w, a.tn, a.tf)) {
-                            float t_face = f.w / dp;
+                        const float num = face_num<GEN>(f, fn, a);
+                        if (face_may_clip(dp, num, a.tn, a.tf)) {
+                            float t_face = num / dp;
                             a.tf = dp >= 0.0f ? fmin_t(t_face, a.tf) : a.tf;
                             a.tn = dp < 0.0f ? fmax_t(t_face, a.tn) : a.tn;
                         }
                     }
                     if (PPL == 2 && b.hit) {
                         float dp = dot(b.g.d, fn);
-                        if (face_may_clip(dp, f.w, b.tn, b.tf)) {
-                            float t_face = f.w / dp;
+                        const float num = face_num<GEN>(f, fn, b);
+                        if (face_may_clip(dp, num, b.tn, b.tf)) {
+                            float t_face = num / dp;
                             b.tf = dp >= 0.0f ? fmin_t(t_face, b.tf) : b.tf;
                             b.tn = dp < 0.0f ? fmax_t(t_face, b.tn) : b.tn;
                         }
@@ -266,7 +290,7 @@ PF_D void fwd_tile(const RasterParams& P, const FwdOut& out, int64_t tile, int w
 #pragma unroll 1
             for (int s = 0; s < PPL; s++) {
                 if (a.hit) {
-                    PlaneRes pr = plane_fwd_smem(o, a.g.d, a.tn, center, pn, radius, ws, P.S);
+                    PlaneRes pr = plane_fwd_smem(ray_org<GEN>(a, o), a.g.d, a.tn, center, pn, radius, ws, P.S);
                     float tf = pr.dp >= 0.0f ? fmin_t(pr.t_surf, a.tf) : a.tf;
                     float tn = pr.dp < 0.0f ? fmax_t(pr.t_surf, a.tn) : a.tn;
                     float dt = tf - tn;
@@ -642,6 +666,7 @@ PF_D void fwd_tile_c(const RasterParams& P, const FwdOut& out, int64_t tile, int
 // adjoint
 struct BwdPix {
     PixGeom g;
+    v3 o;  // ray origin (generic cameras)
     float log_t, dLdlog_t, g_nd;
     v3 g_rgb, g_n;
     int qi;
@@ -845,7 +870,7 @@ struct BwdIn {
     const float* g_contrib;
 };
 
-template <int G, int PPL>
+template <int G, int PPL, bool GEN = false>
 PF_D void bwd_tile(const RasterParams& P, const BwdIn& in, const GradOut& go, int64_t tile, int wig, int lane,
                    WarpStage& ws, BwdStage& bs) {
     const int TS = P.TW * P.TW;
@@ -859,6 +884,7 @@ PF_D void bwd_tile(const RasterParams& P, const BwdIn& in, const GradOut& go, in
     for (int s = 0; s < PPL; s++) {
         int idx = wig * 32 + lane + s * (TS / 2);
         a.g = pixel_geom(P, tile, idx);
+        if constexpr (GEN) pixel_ray_map(P, a.g, a.o);
         int64_t p = a.g.px;
         a.log_t = in.log_t[p];
         if (P.Q > 0) {
@@ -892,8 +918,8 @@ PF_D void bwd_tile(const RasterParams& P, const BwdIn& in, const GradOut& go, in
             const float4 s4 = ws.sph[kk];
             const v3 center = mk(s4.x, s4.y, s4.z);
             const float radius = s4.w;
-            a.hit = a.g.oob ? false : ray_sphere(o, a.g.d, center, radius, a.tn, a.tf);
-            if (PPL == 2) b.hit = b.g.oob ? false : ray_sphere(o, b.g.d, center, radius, b.tn, b.tf);
+            a.hit = a.g.oob ? false : ray_sphere(ray_org<GEN>(a, o), a.g.d, center, radius, a.tn, a.tf);
+            if (PPL == 2) b.hit = b.g.oob ? false : ray_sphere(ray_org<GEN>(b, o), b.g.d, center, radius, b.tn, b.tf);
             if (!__any_sync(0xffffffffu, a.hit || b.hit)) continue;  // no output changes (see forward)
             const int32_t prim = ws.pid[kk];
             const float4 n4 = ws.nsg[kk];
@@ -914,7 +940,7 @@ PF_D void bwd_tile(const RasterParams& P, const BwdIn& in, const GradOut& go, in
                 bs.face_acc[e] = make_float4(0.f, 0.f, 0.f, 0.f);
             }
             for (int e0 = 0; e0 < n_adj; e0 += 32) {
-                stage_faces(ws, P, a0, e0, n_adj, o, center, cc, rr, lane);
+                stage_faces(ws, P, a0, e0, n_adj, GEN ? mk(0.f, 0.f, 0.f) : o, center, cc, rr, lane);
                 const int en = min(32, n_adj - e0);
 #pragma unroll 2
                 for (int q = 0; q < en; q++) {
@@ -923,8 +949,9 @@ PF_D void bwd_tile(const RasterParams& P, const BwdIn& in, const GradOut& go, in
                     const int adj_idx = e0 + q;
                     if (a.hit) {
                         float dp = dot(a.g.d, fn);
-                        if (face_may_clip(dp, f.w, a.tn, a.tf)) {
-                            float t_face = f.w / dp;
+                        const float num = face_num<GEN>(f, fn, a);
+                        if (face_may_clip(dp, num, a.tn, a.tf)) {
+                            float t_face = num / dp;
                             a.tf_id = (dp >= 0.0f && t_face < a.tf) ? adj_idx : a.tf_id;
                             a.tf = dp >= 0.0f ? fmin_t(t_face, a.tf) : a.tf;
                             a.tn_id = (dp < 0.0f && t_face > a.tn) ? adj_idx : a.tn_id;
@@ -933,8 +960,9 @@ PF_D void bwd_tile(const RasterParams& P, const BwdIn& in, const GradOut& go, in
                     }
                     if (PPL == 2 && b.hit) {
                         float dp = dot(b.g.d, fn);
-                        if (face_may_clip(dp, f.w, b.tn, b.tf)) {
-                            float t_face = f.w / dp;
+                        const float num = face_num<GEN>(f, fn, b);
+                        if (face_may_clip(dp, num, b.tn, b.tf)) {
+                            float t_face = num / dp;
                             b.tf_id = (dp >= 0.0f && t_face < b.tf) ? adj_idx : b.tf_id;
                             b.tf = dp >= 0.0f ? fmin_t(t_face, b.tf) : b.tf;
                             b.tn_id = (dp < 0.0f && t_face > b.tn) ? adj_idx : b.tn_id;
@@ -957,7 +985,8 @@ PF_D void bwd_tile(const RasterParams& P, const BwdIn& in, const GradOut& go, in
                     int t_near_id = x.tn_id, t_far_id = x.tf_id;
                     const float _t_near = t_near;
                     const int _t_near_id = t_near_id, _t_far_id = t_far_id;
-                    PlaneRes pr = plane_fwd_smem(o, d, t_near, center, pn, radius, ws, P.S);
+                    const v3 xo = ray_org<GEN>(x, o);
+                    PlaneRes pr = plane_fwd_smem(xo, d, t_near, center, pn, radius, ws, P.S);
                     t_far_id = (pr.dp >= 0.0f && pr.t_surf < t_far) ? n_adj : t_far_id;
                     t_far = pr.dp >= 0.0f ? fmin_t(pr.t_surf, t_far) : t_far;
                     t_near_id = (pr.dp < 0.0f && pr.t_surf > t_near) ? n_adj : t_near_id;
@@ -1008,7 +1037,7 @@ PF_D void bwd_tile(const RasterParams& P, const BwdIn& in, const GradOut& go, in
                         else dLdt_surf = 0.0f;
                         v3 _dc, _dn;
                         float dLd_t_near;
-                        plane_bwd_acc(o, d, _t_near, center, pn, radius, ws, P.S, pr, dLdcolor, dLdt_surf, bs, lane,
+                        plane_bwd_acc(xo, d, _t_near, center, pn, radius, ws, P.S, pr, dLdcolor, dLdt_surf, bs, lane,
                                       _dc, _dn, dLd_t_near);
                         dLdcenter = dLdcenter + _dc;
                         dLdnormal = dLdnormal + _dn;
@@ -1020,7 +1049,7 @@ PF_D void bwd_tile(const RasterParams& P, const BwdIn& in, const GradOut& go, in
                             if (t_id == -1) {
                                 v3 ndc, fdc;
                                 float ndr, fdr;
-                                ray_sphere_bwd_d(o, d, center, radius, ndc, fdc, ndr, fdr);
+                                ray_sphere_bwd_d(xo, d, center, radius, ndc, fdc, ndr, fdr);
                                 dLdcenter = dLdcenter + dLdt * (i == 0 ? ndc : fdc);
                                 dLdradius += dLdt * (i == 0 ? ndr : fdr);
                             } else if (t_id >= 0 && t_id < n_adj) {
@@ -1035,7 +1064,7 @@ PF_D void bwd_tile(const RasterParams& P, const BwdIn& in, const GradOut& go, in
                                 }
                                 v3 dc, dac;
                                 float dr, dar;
-                                ray_pface_bwd_d(o, d, center, radius, mk(as.x, as.y, as.z), as.w, dc, dr, dac, dar);
+                                ray_pface_bwd_d(xo, d, center, radius, mk(as.x, as.y, as.z), as.w, dc, dr, dac, dar);
                                 dLdcenter = dLdcenter + dLdt * dc;
                                 dLdradius += dLdt * dr;
                                 v3 gac = dLdt * dac;

@@ -27,6 +27,7 @@ struct RasterParams {
     float thr;
     const int32_t* tile_order;  // processing order of the tiles (NULL: 0..T-1)
     int* queue;                 // work-queue counter (NULL: one group per tile)
+    const float* ray_maps;      // (H,W,6) per-pixel origin, direction (generic camera) or NULL
 };
 
 // ---------------------------------------------------------------------------
@@ -59,6 +60,15 @@ PF_D PixGeom pixel_geom(const RasterParams& P, int64_t tile, int idx) {
     g.d = ray_dir(P.cam, pi, pj);
     g.px = (int64_t)pi * P.cam.W + pj;
     return g;
+}
+
+// A generic camera's ray (rasterize.py:944-954): the pixel's own origin and
+// its direction divided by its length.
+PF_D void pixel_ray_map(const RasterParams& P, PixGeom& g, v3& o) {
+    const float* m = P.ray_maps + 6 * g.px;
+    o = mk(m[0], m[1], m[2]);
+    const v3 rd = mk(m[3], m[4], m[5]);
+    g.d = rd / length(rd);
 }
 
 // Per-warp shared staging area.
@@ -250,6 +260,7 @@ inline bool fill_params(const pf_raster_inputs* in, RasterParams& P, bool need_f
     P.thr = in->transmittance_threshold;
     P.tile_order = in->tile_order;
     P.queue = (int*)in->scratch;
+    P.ray_maps = in->ray_maps;
     return true;
 }
 

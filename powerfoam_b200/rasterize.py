@@ -9,9 +9,14 @@ CUDA) on torch's current stream; there is no CPU path.
 Differences from the reference, all deliberate:
 * equal sort keys are ordered by primitive index (the reference leaves them
   in atomic order), so outputs are deterministic up to float atomics;
-* tile edge ``tile_width`` may be 8 (the reference's constant), 16 or 32;
-* only pinhole cameras (``args.is_pinhole``): the generic-camera cone
-  hierarchy (rasterize.py:202-291, 365-569) is not part of this path.
+* tile edge ``tile_width`` may be 8 (the reference's constant), 16 or 32.
+
+Generic cameras (``args.is_pinhole`` False) follow the reference: binning
+through the ray-cone hierarchy built from ``camera.ray_maps``
+(rasterize.py:202-291, 365-569, 1518-1585; pinhole ray maps are built when
+the camera has none, as TorchCamera.to_warp does) and per-pixel ray origins
+and directions in the forward and backward; ``benchmark`` and ``visualize``
+composite pinhole rays over those bins, as the reference's kernels do.
 """
 
 from dataclasses import dataclass, field
@@ -94,10 +99,22 @@ class Binner:
         if self.ws is None or self.ws.numel() < nbytes.value:
             self.ws = torch.empty(max(nbytes.value, 256), dtype=torch.uint8, device=self.device)
 
-    def __call__(self, cam_pf, tile_width, spheres, n_prims, num_tiles, return_keys=False, capacity=None):
+    def _ensure_generic(self, n_prims, cap, cam_pf, tile_width):
+        nbytes = _lib.ctypes.c_size_t(0)
+        _lib.call("pf_bin_generic_workspace_size", n_prims, cap, cam_pf.width, cam_pf.height, tile_width,
+                  _lib.ctypes.byref(nbytes))
+        if self.ws is None or self.ws.numel() < nbytes.value:
+            self.ws = torch.empty(max(nbytes.value, 256), dtype=torch.uint8, device=self.device)
+
+    def __call__(self, cam_pf, tile_width, spheres, n_prims, num_tiles, return_keys=False, capacity=None,
+                 ray_maps=None):
+        """ray_maps (H,W,6) f32: bin a generic camera through its ray cones."""
         cap = capacity if capacity is not None else max(self.capacity, 4 * n_prims, 1 << 14)
         while True:
-            self._ensure(n_prims, cap, num_tiles)
+            if ray_maps is None:
+                self._ensure(n_prims, cap, num_tiles)
+            else:
+                self._ensure_generic(n_prims, cap, cam_pf, tile_width)
             tile_offsets = torch.empty(num_tiles + 1, dtype=torch.int64, device=self.device)
             tile_order = torch.empty(num_tiles, dtype=torch.int32, device=self.device)
             tile_prims = torch.empty(max(cap, 1), dtype=torch.int32, device=self.device)
@@ -105,10 +122,14 @@ class Binner:
             visible = torch.empty(n_prims, dtype=torch.uint8, device=self.device)
             scalars = torch.zeros(2, dtype=torch.int64, device=self.device)  # n_pairs, status
             status = scalars[1:].view(torch.int32)[:1]
-            _lib.call("pf_bin", _lib.ctypes.byref(cam_pf), tile_width, _lib.ptr(spheres), n_prims,
-                      _lib.ptr(self.ws), self.ws.numel(), cap, _lib.ptr(tile_offsets), _lib.ptr(tile_prims),
-                      _lib.ptr(keys), _lib.ptr(visible), _lib.ptr(tile_order), _lib.ptr(scalars[:1]),
-                      _lib.ptr(status), _lib.stream_ptr())
+            outs = (_lib.ptr(self.ws), self.ws.numel(), cap, _lib.ptr(tile_offsets), _lib.ptr(tile_prims),
+                    _lib.ptr(keys), _lib.ptr(visible), _lib.ptr(tile_order), _lib.ptr(scalars[:1]), _lib.ptr(status),
+                    _lib.stream_ptr())
+            if ray_maps is None:
+                _lib.call("pf_bin", _lib.ctypes.byref(cam_pf), tile_width, _lib.ptr(spheres), n_prims, *outs)
+            else:
+                _lib.call("pf_bin_generic", _lib.ctypes.byref(cam_pf), _lib.ptr(ray_maps), tile_width,
+                          _lib.ptr(spheres), n_prims, *outs)
             n = int(scalars[0].item())
             if n <= cap:
                 break
@@ -131,8 +152,7 @@ class Rasterizer:
         self.attr_dtype = attr_dtype
         self.loss_accumulation = args.render_objective == "surface"
         self.num_texel_sites = args.num_texel_sites
-        if not getattr(args, "is_pinhole", True):
-            raise NotImplementedError("only pinhole cameras are supported by this rasterizer")
+        self.generic = not getattr(args, "is_pinhole", True)
         if tile_width not in (8, 16, 32):
             raise ValueError("tile_width must be 8, 16 or 32")
         self.tile_width = tile_width
@@ -161,9 +181,23 @@ class Rasterizer:
                   _lib.ptr(nsig), _lib.stream_ptr())
         return spheres, nsig
 
-    def bin(self, camera, spheres, return_keys=False):
+    def ray_maps(self, camera):
+        """The (H,W,6) f32 ray maps of a generic camera (pinhole ones if it
+        has none, as the reference's TorchCamera.to_warp builds), else None."""
+        if not self.generic:
+            return None
+        rm = camera.ray_maps if camera.ray_maps is not None else camera.build_pinhole_ray_maps()
+        if rm.shape != (camera.height, camera.width, 6):
+            raise ValueError("ray_maps must have shape (height, width, 6)")
+        if not rm.is_cuda:
+            raise ValueError("Only CUDA tensors are supported as inputs")
+        return rm.detach().to(torch.float32).contiguous()
+
+    def bin(self, camera, spheres, return_keys=False, ray_maps=None):
+        if self.generic and ray_maps is None:
+            ray_maps = self.ray_maps(camera)
         return self.binner(camera.to_pf(), self.tile_width, spheres, spheres.shape[0], self.num_tiles(camera),
-                           return_keys=return_keys)
+                           return_keys=return_keys, ray_maps=ray_maps)
 
     def prefetch_adjacency(self, spheres, adjacency, adjacency_offsets):
         """(E,4) float16 (c_j - c_i, r_j): rasterize.py:580-606."""
@@ -173,8 +207,9 @@ class Rasterizer:
         return adj_diff
 
     def _inputs(self, camera, spheres, nsig, sites, rgb, height, adjacency, adjacency_offsets, adj_diff, bins,
-                depth_quantiles=None, ray_gt=None, thr=1e-3, attr_half=False):
+                depth_quantiles=None, ray_gt=None, thr=1e-3, attr_half=False, ray_maps=None):
         inp = _lib.PfRasterInputs()
+        inp.ray_maps = _lib.ptr(ray_maps)
         inp.cam = camera.to_pf()
         inp.tile_width = self.tile_width
         inp.n_sites = sites.shape[1]
@@ -220,7 +255,8 @@ class Rasterizer:
         dq = None if depth_quantiles is None else _f32(depth_quantiles.detach(), "depth_quantiles")
         gt = None if ray_gt is None else _f32(ray_gt.detach(), "ray_gt")
 
-        bins = self.bin(camera, spheres)
+        ray_maps = self.ray_maps(camera)
+        bins = self.bin(camera, spheres, ray_maps=ray_maps)
         adj_diff = self.prefetch_adjacency(spheres, adjacency, adjacency_offsets)
 
         color = torch.empty((H, W, 3), dtype=torch.float32, device=dev)
@@ -234,7 +270,7 @@ class Rasterizer:
         early_stop = torch.empty(self.num_tiles(camera), dtype=torch.int32, device=dev)
         stats = torch.empty(self.num_tiles(camera), dtype=torch.int32, device=dev) if self.collect_stats else None
         inp = self._inputs(camera, spheres, nsig, sites, rgb, height, adjacency, adjacency_offsets, adj_diff, bins,
-                           dq, gt, transmittance_threshold)
+                           dq, gt, transmittance_threshold, ray_maps=ray_maps)
         _timed_call("pf_raster_forward", _lib.ctypes.byref(inp), int(bool(return_point_err)), _lib.ptr(color),
                     _lib.ptr(log_t), _lib.ptr(nd), _lib.ptr(normal), _lib.ptr(qd), _lib.ptr(err), _lib.ptr(contrib),
                     _lib.ptr(perr), _lib.ptr(early_stop), _lib.ptr(stats), _lib.stream_ptr())
@@ -248,6 +284,7 @@ class Rasterizer:
             grad_ctx.n_inputs = 14 if transmittance_threshold == 1e-3 else 15
             grad_ctx.thr = transmittance_threshold
             grad_ctx.bins = bins
+            grad_ctx.ray_maps = ray_maps
             grad_ctx.save_for_backward(dq, spheres, nsig, sites, rgb, height, adjacency, adjacency_offsets,
                                        adj_diff, early_stop, log_t)
         opacity = 1.0 - torch.exp(log_t)
@@ -289,7 +326,7 @@ class Rasterizer:
                    rgb=torch.empty((n, S, 3), dtype=torch.float32, device=dev),
                    height=torch.empty((n, S), dtype=torch.float32, device=dev))
         inp = self._inputs(camera, spheres, nsig, sites, rgb, height, adjacency, adjacency_offsets, adj_diff,
-                           grad_ctx.bins, dq, None, grad_ctx.thr)
+                           grad_ctx.bins, dq, None, grad_ctx.thr, ray_maps=grad_ctx.ray_maps)
         _timed_call("pf_raster_backward", _lib.ctypes.byref(inp), _lib.ptr(early_stop), _lib.ptr(log_t), _lib.ptr(gc),
                     _lib.ptr(go), _lib.ptr(gnd), _lib.ptr(gn), _lib.ptr(gq), _lib.ptr(gcon), _lib.ptr(out["points"]),
                     _lib.ptr(out["radii"]), _lib.ptr(out["normals"]), _lib.ptr(out["density"]),
