@@ -56,7 +56,8 @@ def parse():
                    "(a quarter-size case with the same density per pixel, for profiling), batch3m (32 views of "
                    "a 3.1M-primitive scene in one graph-captured persistent step), batch256k (its small case), "
                    "trace1m (tracer forward + adjoint), interpen3m (interpenetration loss forward + adjoint), power1m "
-                   "(power-diagram adjacency build) or proposal (proposal-seeded vs plain cell walk)")
+                   "(power-diagram adjacency build), fisheye1m (raster1m through a generic fisheye camera) or proposal "
+                   "(proposal-seeded vs plain cell walk)")
     p.add_argument("--cpu-sample-tiles", type=int, default=0, help="tiles composited by the CPU baseline")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-autotune", action="store_true", help="batch workloads: use --tile, chunk 1")
@@ -166,6 +167,10 @@ class Args:
     is_pinhole = True
     render_objective = "volume"
     num_texel_sites = 8
+
+
+class ArgsGeneric(Args):
+    is_pinhole = False
 
 
 def make_step(R, scene, cam, adj, adj_off, target_dev, world):
@@ -813,9 +818,17 @@ def main():
         return
     from powerfoam_b200 import rasterize
 
-    cfg, scene, cam, adj, adj_off, target = build_workload(dev, rank, args.tile, args.workload)
+    fisheye = args.workload == "fisheye1m"
+    cfg, scene, cam, adj, adj_off, target = build_workload(dev, rank, args.tile,
+                                                           "raster1m" if fisheye else args.workload)
     target_dev = target.to(dev)
-    R = rasterize.Rasterizer(Args(), dev, tile_width=args.tile)
+    if fisheye:
+        # the same scene and view through a 150-degree equidistant fisheye (generic camera)
+        from powerfoam_b200 import synthetic
+
+        cam.ray_maps = synthetic.fisheye_ray_maps(cam, 150.0)
+        args.no_cpu_baseline = True
+    R = rasterize.Rasterizer(ArgsGeneric() if fisheye else Args(), dev, tile_width=args.tile)
     step, params = make_step(R, scene, cam, adj, adj_off, target_dev, world)
 
     def barrier():
@@ -907,6 +920,12 @@ def main():
                 gpu_launches=None)
     # kernels per step: pack 1, binning with tile order, prefetch 1, SH 1, forward 1, backward 1 + 7 sanitise
     line["gpu_launches"] = args.steps * (1 + bin_launches(st["T"]) + 1 + 1 + 1 + 1 + 7)
+    if fisheye:  # the cone hierarchy: one leaf launch and one per merged level
+        dh, dw, levels = (cfg["height"] + 1) // 2, (cfg["width"] + 1) // 2, 1
+        while dh > 1 or dw > 1:
+            dh, dw, levels = (dh + 1) // 2, (dw + 1) // 2, levels + 1
+        line["gpu_launches"] += args.steps * levels
+        line["config"]["camera"] = "generic: 150-degree equidistant fisheye ray maps"
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(cfg, scene, cam, adj, adj_off, target, args.cpu_sample_tiles or 200,
                                             args.tile)

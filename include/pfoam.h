@@ -208,6 +208,23 @@ PF_API int pf_power_adjacency(const float *points, const float *radii, int64_t n
                               int32_t *adjacency /* (capacity) */, int32_t *adjacency_offsets /* (N+1) */,
                               int64_t *n_edges /* device */, int32_t *status /* device */, void *stream);
 
+/* Steiner points (get_steiner_points, benchmark.py:93-180), the two steps
+ * of a round that are not plumbing.  pf_steiner_knn: with a locator built
+ * over the primitives (pf_locator_build), for each sample its k <= 32
+ * nearest centres (scipy cKDTree.query in the reference; float64 distances
+ * rounded to float32), the smallest dist - r over them -> sample_radius and
+ * the primitive attaining it (first in distance order) -> closest.
+ * pf_steiner_select: _greedy_min_overlap_fps (:93-134) from sample `seed`:
+ * repeatedly select the sample with the smallest largest-overlap
+ * (r_i + r_j - |p_i - p_j|) / (r_i + r_j) with the selected ones while it is
+ * <= threshold; selected (n) gets 0/1, *n_selected (device, optional) the
+ * count; scratch is n floats.  One block of 1024 threads. */
+PF_API int pf_steiner_knn(const float *points, const float *radii, int64_t n_prims, const void *workspace,
+                          const float *samples, int64_t n_samples, int32_t k, float *sample_radius,
+                          int32_t *closest, int32_t *status, void *stream);
+PF_API int pf_steiner_select(const float *samples, const float *radii, int64_t n, int64_t seed, float threshold,
+                             float *scratch, uint8_t *selected, int32_t *n_selected, void *stream);
+
 /* Morton order of the primitives (stable on equal codes).  Replaces
  * morton_sort (powerfoam/geometry.py:7-85, Warp radix_sort_pairs). */
 PF_API int pf_morton_workspace_size(int64_t n_prims, size_t *bytes);

@@ -527,6 +527,191 @@ __global__ void power_emit_kernel(const float* __restrict__ pts, const float* __
     if (!WRITE) out_counts[i] = n;
 }
 
+// ---------------------------------------------------------------------------
+// Steiner points (benchmark.py:93-180).  Each round of get_steiner_points
+// draws random samples, finds for each its 32 nearest primitive centres
+// (scipy's cKDTree in the reference), takes the smallest dist - r over them
+// as the sample's radius and the primitive that attains it, keeps samples
+// whose radius is 2..6 times that primitive's, and thins them with a greedy
+// minimum-overlap selection.  The nearest-neighbour query and the selection
+// run here; distances are float64 rounded to float32, as the tree's are.
+
+constexpr int kSteinerK = 32;
+
+// k nearest centres of q (ascending distance), exact: grid shells until the
+// shells scanned cover the k-th distance
+__global__ void steiner_knn_kernel(Locator L, const float* __restrict__ queries, int64_t nq, int k,
+                                   float* __restrict__ radius_out, int32_t* __restrict__ closest_out,
+                                   int32_t* __restrict__ status) {
+    const int64_t qi = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (qi >= nq) return;
+    const CechGrid g = *L.grid;
+    const double q[3] = {(double)queries[3 * qi], (double)queries[3 * qi + 1], (double)queries[3 * qi + 2]};
+    const double h = 1.0 / (double)g.inv_h;
+    const double glo[3] = {(double)g.lo_x, (double)g.lo_y, (double)g.lo_z};
+    const int gn[3] = {g.nx, g.ny, g.nz};
+    const int cc[3] = {cell_coord(queries[3 * qi], g.lo_x, g.inv_h, g.nx),
+                       cell_coord(queries[3 * qi + 1], g.lo_y, g.inv_h, g.ny),
+                       cell_coord(queries[3 * qi + 2], g.lo_z, g.inv_h, g.nz)};
+    double bd[kSteinerK];
+    int32_t bi[kSteinerK];
+    int nb = 0;
+    const int smax = imax(imax(g.nx, g.ny), g.nz);
+    for (int s = 0; s <= smax; s++) {
+        for (int dz = -s; dz <= s; dz++) {
+            const int z = cc[2] + dz;
+            if (z < 0 || z >= g.nz) continue;
+            for (int dy = -s; dy <= s; dy++) {
+                const int y = cc[1] + dy;
+                if (y < 0 || y >= g.ny) continue;
+                const bool face = (dz == -s || dz == s || dy == -s || dy == s);
+                const int step = (face || s == 0) ? 1 : 2 * s;
+                for (int dx = -s; dx <= s; dx += step) {
+                    const int x = cc[0] + dx;
+                    if (x < 0 || x >= g.nx) continue;
+                    const int64_t c = ((int64_t)z * g.ny + y) * g.nx + x;
+                    for (int32_t p = L.cell_start[c]; p < L.cell_start[c + 1]; p++) {
+                        const int32_t j = (int32_t)L.sorted[p];
+                        const double d0 = (double)L.pts[3 * j] - q[0], d1 = (double)L.pts[3 * j + 1] - q[1],
+                                     d2 = (double)L.pts[3 * j + 2] - q[2];
+                        const double d = sqrt(d0 * d0 + d1 * d1 + d2 * d2);
+                        if (nb == k && !(d < bd[k - 1] || (d == bd[k - 1] && j < bi[k - 1]))) continue;
+                        int w = nb < k ? nb++ : k - 1;
+                        while (w > 0 && (bd[w - 1] > d || (bd[w - 1] == d && bi[w - 1] > j))) {
+                            bd[w] = bd[w - 1];
+                            bi[w] = bi[w - 1];
+                            w--;
+                        }
+                        bd[w] = d;
+                        bi[w] = j;
+                    }
+                }
+            }
+        }
+        if (nb == k) {
+            double reach = INFINITY;
+            for (int a = 0; a < 3; a++) {
+                if (cc[a] - s > 0) reach = fmin(reach, q[a] - (glo[a] + (cc[a] - s) * h));
+                if (cc[a] + s < gn[a] - 1) reach = fmin(reach, glo[a] + (cc[a] + s + 1) * h - q[a]);
+            }
+            if (reach > bd[k - 1]) break;
+        }
+    }
+    if (nb < k) {  // fewer primitives than neighbours asked for
+        if (status) atomicMax(status, PF_ERR_ARGS);
+        radius_out[qi] = NAN;
+        closest_out[qi] = -1;
+        return;
+    }
+    // (dists - all_radii[idxs]).min(dim=1), float32 as the reference
+    float best = (float)bd[0] - L.radii[bi[0]];
+    int32_t arg = bi[0];
+    for (int a = 1; a < k; a++) {
+        const float v = (float)bd[a] - L.radii[bi[a]];
+        if (v < best) {
+            best = v;
+            arg = bi[a];
+        }
+    }
+    radius_out[qi] = best;
+    closest_out[qi] = arg;
+}
+
+constexpr int kSelectThreads = 1024;
+
+PF_D float steiner_overlap(const float* p, const float* r, int64_t i, int64_t j) {
+    const float sum_r = r[i] + r[j];
+    const float dx = p[3 * i] - p[3 * j], dy = p[3 * i + 1] - p[3 * j + 1], dz = p[3 * i + 2] - p[3 * j + 2];
+    const float dist = sqrtf(dx * dx + dy * dy + dz * dz);
+    return (sum_r - dist) / sum_r;
+}
+
+// _greedy_min_overlap_fps (benchmark.py:93-134) in one block: starting from
+// `seed`, repeatedly select the sample whose largest overlap with the
+// selected ones is smallest (first index on ties) while it is <= threshold.
+// max_overlap is n floats of scratch.  At most n rounds.
+__global__ void __launch_bounds__(kSelectThreads)
+    steiner_select_kernel(const float* __restrict__ pts, const float* __restrict__ radii, int64_t n, int64_t seed,
+                          float threshold, float* __restrict__ max_overlap, uint8_t* __restrict__ selected,
+                          int32_t* __restrict__ n_selected) {
+    __shared__ float sv[kSelectThreads / 32];
+    __shared__ int64_t si[kSelectThreads / 32];
+    __shared__ int64_t pick;
+    __shared__ float pick_v;
+    const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+    for (int64_t i = t; i < n; i += blockDim.x) {
+        selected[i] = 0;
+        max_overlap[i] = steiner_overlap(pts, radii, i, seed);
+    }
+    __syncthreads();
+    if (t == 0) {
+        selected[seed] = 1;
+        max_overlap[seed] = INFINITY;
+    }
+    int32_t count = 1;
+    __syncthreads();
+    for (int64_t round = 0; round < n; round++) {
+        // block argmin, first index on ties; NaN compares as the reference's
+        // torch.min: it wins (min propagates NaN)
+        float bv = INFINITY;
+        int64_t bidx = -1;
+        for (int64_t i = t; i < n; i += blockDim.x) {
+            const float v = max_overlap[i];
+            if (bidx < 0 || v < bv || (v != v && bv == bv)) {
+                bv = v;
+                bidx = i;
+            }
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            const float ov = __shfl_down_sync(0xffffffffu, bv, o);
+            const int64_t oi = __shfl_down_sync(0xffffffffu, bidx, o);
+            const bool take = oi >= 0 && (bidx < 0 || (ov != ov && (bv == bv || oi < bidx)) ||
+                                          (!(bv != bv) && (ov < bv || (ov == bv && oi < bidx))));
+            if (take) {
+                bv = ov;
+                bidx = oi;
+            }
+        }
+        if (lane == 0) {
+            sv[w] = bv;
+            si[w] = bidx;
+        }
+        __syncthreads();
+        if (t == 0) {
+            float v = sv[0];
+            int64_t ix = si[0];
+            for (int k = 1; k < (int)(blockDim.x / 32); k++) {
+                const float ov = sv[k];
+                const int64_t oi = si[k];
+                const bool take = oi >= 0 && (ix < 0 || (ov != ov && (v == v || oi < ix)) ||
+                                              (!(v != v) && (ov < v || (ov == v && oi < ix))));
+                if (take) {
+                    v = ov;
+                    ix = oi;
+                }
+            }
+            pick = ix;
+            pick_v = v;
+        }
+        __syncthreads();
+        const int64_t j = pick;
+        if (j < 0 || pick_v > threshold) break;
+        if (t == 0) {
+            selected[j] = 1;
+            max_overlap[j] = INFINITY;
+        }
+        count++;
+        __syncthreads();
+        for (int64_t i = t; i < n; i += blockDim.x) {
+            const float nv = steiner_overlap(pts, radii, i, j);
+            const float cur = max_overlap[i];
+            max_overlap[i] = (cur != cur || nv != nv) ? NAN : fmaxf(cur, nv);  // torch.maximum propagates NaN
+        }
+        __syncthreads();
+    }
+    if (t == 0 && n_selected) *n_selected = count;
+}
+
 static size_t align_up(size_t x) { return (x + 255) & ~(size_t)255; }
 
 struct CechLayout {
@@ -805,4 +990,32 @@ extern "C" int pf_power_adjacency(const float* points, const float* radii, int64
     offsets_i32_kernel<<<(unsigned)((N + 1 + 255) / 256), 256, 0, st>>>(off64, N, n_edges, edge_capacity,
                                                                         adjacency_offsets, status);
     return pf_check_launch("pf_power_adjacency");
+}
+
+extern "C" int pf_steiner_knn(const float* points, const float* radii, int64_t n_prims, const void* workspace,
+                              const float* samples, int64_t n_samples, int32_t k, float* sample_radius,
+                              int32_t* closest, int32_t* status, void* stream) {
+    if (n_prims <= 0 || !points || !radii || !workspace || n_samples < 0 || k < 1 || k > kSteinerK ||
+        (n_samples > 0 && (!samples || !sample_radius || !closest)))
+        return pf_fail(PF_ERR_ARGS, "pf_steiner_knn: bad arguments (k must be in [1, 32])");
+    if (n_samples == 0) return PF_OK;
+    Locator loc = locator_view(points, radii, n_prims, (char*)workspace);
+    steiner_knn_kernel<<<(unsigned)((n_samples + 127) / 128), 128, 0, (cudaStream_t)stream>>>(
+        loc, samples, n_samples, k, sample_radius, closest, status);
+    return pf_check_launch("pf_steiner_knn");
+}
+
+extern "C" int pf_steiner_select(const float* samples, const float* radii, int64_t n, int64_t seed, float threshold,
+                                 float* scratch, uint8_t* selected, int32_t* n_selected, void* stream) {
+    if (n < 0 || (n > 0 && (!samples || !radii || !scratch || !selected || seed < 0 || seed >= n)))
+        return pf_fail(PF_ERR_ARGS, "pf_steiner_select: bad arguments");
+    cudaStream_t st = (cudaStream_t)stream;
+    if (n == 0) {
+        if (n_selected && cudaMemsetAsync(n_selected, 0, 4, st) != cudaSuccess)
+            return pf_check_launch("pf_steiner_select");
+        return PF_OK;
+    }
+    steiner_select_kernel<<<1, kSelectThreads, 0, st>>>(samples, radii, n, seed, threshold, scratch, selected,
+                                                         n_selected);
+    return pf_check_launch("pf_steiner_select");
 }

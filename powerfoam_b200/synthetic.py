@@ -103,6 +103,29 @@ def orbit_camera(seed, width, height, vfov_deg, distance=3.0, device="cuda", azi
     return look_at(eye, (0.0, 0.0, 0.0), width, height, vfov_deg, device=device)
 
 
+def fisheye_ray_maps(cam, fov_deg):
+    """(H, W, 6) ray maps of an equidistant fisheye with the camera's eye,
+    axes and image size: a generic camera (per-pixel rays) for the
+    is_pinhole=False path.  The diagonal field of view is fov_deg."""
+    H, W = cam.height, cam.width
+    dev = cam.eye.device
+    r_hat = cam.right / torch.linalg.norm(cam.right)
+    u_hat = cam.up / torch.linalg.norm(cam.up)
+    f = torch.cross(cam.up, cam.right, dim=-1)
+    f = f / torch.linalg.norm(f)
+    i = torch.arange(H, dtype=torch.float32, device=dev)
+    j = torch.arange(W, dtype=torch.float32, device=dev)
+    ii, jj = torch.meshgrid(i, j, indexing="ij")
+    x = (2.0 * jj / (W - 1) - 1.0) * (W / math.hypot(W, H))
+    y = (1.0 - 2.0 * ii / (H - 1)) * (H / math.hypot(W, H))
+    rad = torch.sqrt(x * x + y * y)
+    th = rad * math.radians(fov_deg) / 2.0
+    s = torch.where(rad > 0, torch.sin(th) / rad.clamp_min(1e-12), torch.zeros_like(rad))
+    d = torch.cos(th)[..., None] * f + (s * x)[..., None] * r_hat + (s * y)[..., None] * u_hat
+    o = cam.eye.expand(H, W, 3)
+    return torch.cat([o, d], dim=-1).float().contiguous()
+
+
 BATCH_RESOLUTIONS = ((320, 240), (640, 480), (1280, 720), (1920, 1080))
 
 

@@ -1,6 +1,7 @@
 """Generate golden vectors by executing the reference's own kernel source.
 
-Imports powerfoam/rasterize.py, raytrace.py and geometry.py from the reference
+Imports powerfoam/rasterize.py, raytrace.py and geometry.py (and functions of
+benchmark.py) from the reference
 checkout (default /root/reference, or $PF_REFERENCE) with warp replaced by
 tests/golden/warp_shim.py, runs the kernels on small seeded scenes, and writes
 tests/golden/*.npz.  Run from the repository root:
@@ -500,6 +501,54 @@ def interpen_case(name, seed):
     print(name, "pairs", adj.shape[0], "overlapping", int((areas > 0).sum()))
 
 
+def steiner_case(name, seed, n=4000):
+    """get_steiner_points (benchmark.py:137-180) with its helpers, executed
+    from benchmark.py's own source on a small seeded scene (cKDTree on the
+    host).  The random draws are recorded: per round the samples
+    (points_mean + 0.5 * points_std * randn, evaluated as the function does)
+    and the greedy selection's first pick."""
+    from scipy.spatial import cKDTree
+
+    src = open(os.path.join(REF, "benchmark.py")).read()
+    tree = ast.parse(src)
+    keep = {"inverse_softplus", "_greedy_min_overlap_fps", "get_steiner_points"}
+    fns = [nd for nd in tree.body if isinstance(nd, ast.FunctionDef) and nd.name in keep]
+    rec = dict(randn=[], randint=[])
+
+    class TorchRec(types.ModuleType):
+        def __getattr__(self, k):
+            return getattr(torch, k)
+
+    trec = TorchRec("torch_rec")
+
+    def randn(*a, **k):
+        v = torch.randn(*a, **k)
+        rec["randn"].append(v.clone())
+        return v
+
+    def randint(*a, **k):
+        v = torch.randint(*a, **k)
+        rec["randint"].append(int(v.item()))
+        return v
+
+    trec.randn = randn
+    trec.randint = randint
+    ns = {"torch": trec, "cKDTree": cKDTree}
+    exec(compile(ast.Module(body=fns, type_ignores=[]), "benchmark.py", "exec"), ns)
+    sc = make_scene(seed, n, -1.0, 1.0, 0.01, 0.05)
+    pts = torch.from_numpy(sc["points"])
+    radii = torch.from_numpy(sc["radii"])
+    torch.manual_seed(seed)
+    sp, sr = ns["get_steiner_points"](pts, radii, None)
+    mean = pts.mean(dim=0, keepdim=True)
+    std = pts.std(dim=0, keepdim=True)
+    samples = [(mean + 0.5 * std * r).numpy() for r in rec["randn"]]
+    np.savez_compressed(os.path.join(HERE, f"{name}.npz"), points=sc["points"], radii=sc["radii"],
+                        samples=np.stack(samples), seeds=np.array(rec["randint"], np.int64),
+                        steiner_points=sp.numpy(), steiner_radii=sr.numpy())
+    print(name, "steiner points", sp.shape[0], "rounds", len(samples))
+
+
 def edge_scene(seed):
     """Primitives that exercise culling and the tile-range arithmetic: behind
     the camera, closer than 4r, straddling the image border, one covering many
@@ -524,7 +573,8 @@ def edge_scene(seed):
 
 
 def main():
-    which = sys.argv[1:] or ["raster_small", "raster_edge", "raster_dense", "bin_large", "interpen_small", "raster_generic", "trace_small"]
+    which = sys.argv[1:] or ["raster_small", "raster_edge", "raster_dense", "bin_large", "interpen_small", "raster_generic", "steiner_small",
+                           "trace_small"]
     if "raster_small" in which:
         sc = make_scene(1, 120, -0.6, 0.6, 0.05, 0.2)
         raster_case("raster_small", sc, look_at_camera((0.3, 0.4, 2.0), (0, 0, 0), 36, 28, 60.0), 1)
@@ -547,6 +597,8 @@ def main():
         sc = make_scene(8, 220, -0.9, 0.9, 0.06, 0.22)
         cam = look_at_camera((0.3, -0.2, 2.1), (0, 0, 0), 40, 28, 60.0)
         generic_case("raster_generic", sc, cam, fisheye_ray_maps(cam, 80.0), 8)
+    if "steiner_small" in which:
+        steiner_case("steiner_small", 9)
     if "trace_small" in which:
         sc = make_scene(4, 150, -0.6, 0.6, 0.08, 0.2)
         trace_case("trace_small", sc, look_at_camera((0.2, 0.3, 2.2), (0, 0, 0), 24, 20, 60.0))
