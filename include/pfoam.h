@@ -225,6 +225,26 @@ PF_API int pf_steiner_knn(const float *points, const float *radii, int64_t n_pri
 PF_API int pf_steiner_select(const float *samples, const float *radii, int64_t n, int64_t seed, float threshold,
                              float *scratch, uint8_t *selected, int32_t *n_selected, void *stream);
 
+/* Spherical-Voronoi texel colour.  Replaces spherical_voronoi_fwd_kernel /
+ * spherical_voronoi_bwd_kernel (powerfoam/color_fn.py:54-184): per point,
+ * colour = max(sum_i w_i val_i / sum_i w_i + 0.5, 0) with
+ * w_i = exp(-temp_i |normalize(p - origin) - axis_i|) over sv_dof sites, or
+ * 0.5 grey (weight sum 0) when the direction is outside the camera cone
+ * (dot(d, forward) < fov_cos_cutoff).  att_sites / att_values are
+ * (sv_dof, N, 3), att_temps (sv_dof, N); f32, or f16 with attr_half = 1
+ * (then value_out / weights_sum_out are f16 too).  The backward zeroes and
+ * fills the site gradients, skipping sites with w / sum w < 1e-3; the
+ * points get no gradient (the reference's is disabled). */
+PF_API int pf_sv_forward(const float *points, const float *camera_origin /* host, 3 */,
+                         const float *camera_forward /* host, 3 */, float fov_cos_cutoff, const void *att_sites,
+                         const void *att_values, const void *att_temps, int64_t n_points, int32_t sv_dof,
+                         int32_t attr_half, void *value_out, void *weights_sum_out, void *stream);
+PF_API int pf_sv_backward(const float *points, const float *camera_origin, const float *camera_forward,
+                          float fov_cos_cutoff, const void *att_sites, const void *att_values, const void *att_temps,
+                          const void *weights_sum, const void *values, const void *grad_values, int64_t n_points,
+                          int32_t sv_dof, int32_t attr_half, void *grad_att_sites, void *grad_att_values,
+                          void *grad_att_temps, void *stream);
+
 /* Morton order of the primitives (stable on equal codes).  Replaces
  * morton_sort (powerfoam/geometry.py:7-85, Warp radix_sort_pairs). */
 PF_API int pf_morton_workspace_size(int64_t n_prims, size_t *bytes);

@@ -332,6 +332,37 @@ def interpenetration_backward(spheres, adj, adj_off, grad_areas, prec="f32", row
     return out
 
 
+def sv_forward(points, origin, forward, cutoff, sites, values, temps, prec="f32"):
+    """Spherical-Voronoi colour and weight sum (color_fn.py:54-101)."""
+    pts = _c(points, F32)
+    N = pts.shape[0]
+    dof = sites.shape[0]
+    R = np.float64 if prec == "f64" else F32
+    v = np.zeros((N, 3), R)
+    w = np.zeros(N, R)
+    getattr(lib(), f"orc_sv_forward_{prec}")(_p(pts), _p(np.asarray(origin, F32)), _p(np.asarray(forward, F32)),
+                                             ctypes.c_float(cutoff), _p(_c(sites, F32)), _p(_c(values, F32)),
+                                             _p(_c(temps, F32)), ctypes.c_int64(N), ctypes.c_int(dof), _p(v), _p(w))
+    return v, w
+
+
+def sv_backward(points, origin, forward, cutoff, sites, values, temps, wsum, value, grad_value, prec="f32"):
+    """Site gradients of sv_forward (color_fn.py:105-182)."""
+    pts = _c(points, F32)
+    N = pts.shape[0]
+    dof = sites.shape[0]
+    R = np.float64 if prec == "f64" else F32
+    gs = np.zeros((dof, N, 3), R)
+    gv = np.zeros((dof, N, 3), R)
+    gt = np.zeros((dof, N), R)
+    getattr(lib(), f"orc_sv_backward_{prec}")(_p(pts), _p(np.asarray(origin, F32)), _p(np.asarray(forward, F32)),
+                                              ctypes.c_float(cutoff), _p(_c(sites, F32)), _p(_c(values, F32)),
+                                              _p(_c(temps, F32)), _p(_c(wsum, F32)), _p(_c(value, F32)),
+                                              _p(_c(grad_value, F32)), ctypes.c_int64(N), ctypes.c_int(dof), _p(gs),
+                                              _p(gv), _p(gt))
+    return gs, gv, gt
+
+
 def num_threads():
     return int(lib().orc_num_threads_f32())
 

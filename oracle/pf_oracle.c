@@ -1782,6 +1782,75 @@ void FN(orc_interpenetration_backward)(const float *spheres, const int32_t *adj,
     }
 }
 
+/* ------------------------------------------------------------------------ */
+/* Spherical-Voronoi texel colour (powerfoam/color_fn.py:54-184), float32    */
+/* attributes: sites / values (dof, N, 3), temps (dof, N).                   */
+void FN(orc_sv_forward)(const float *points, const float *origin, const float *forward, float cutoff,
+                        const float *sites, const float *values, const float *temps, int64_t N, int dof,
+                        out_t *value_out, out_t *wsum_out) {
+    v3 o = ld3(origin), fw = ld3(forward);
+    for (int64_t t = 0; t < N; t++) {
+        v3 dir = normalize(vsub(ld3(points + 3 * t), o));
+        if (dot(dir, fw) < (real)cutoff) {
+            value_out[3 * t] = value_out[3 * t + 1] = value_out[3 * t + 2] = K(0.5);
+            wsum_out[t] = 0;
+            continue;
+        }
+        real ws = K(0.0);
+        v3 vs = mk(0, 0, 0);
+        for (int i = 0; i < dof; i++) {
+            int64_t e = (int64_t)i * N + t;
+            v3 axis = ld3(sites + 3 * e), val = ld3(values + 3 * e);
+            real temp = (real)temps[e];
+            real dist = length(vsub(dir, axis));
+            real w = r_exp(-temp * dist);
+            ws += w;
+            vs = vadd(vs, smul(w, val));
+        }
+        wsum_out[t] = (out_t)ws;
+        v3 v = vadd(vdivs(vs, ws), mk(K(0.5), K(0.5), K(0.5)));
+        value_out[3 * t] = (out_t)rmax(v.x, K(0.0));
+        value_out[3 * t + 1] = (out_t)rmax(v.y, K(0.0));
+        value_out[3 * t + 2] = (out_t)rmax(v.z, K(0.0));
+    }
+}
+
+/* the adjoint (color_fn.py:105-182); gradients written where the site's
+ * normalised weight is >= 1e-3, left untouched elsewhere */
+void FN(orc_sv_backward)(const float *points, const float *origin, const float *forward, float cutoff,
+                         const float *sites, const float *values, const float *temps, const float *wsum_in,
+                         const float *value_in, const float *grad_value, int64_t N, int dof, out_t *g_sites,
+                         out_t *g_values, out_t *g_temps) {
+    v3 o = ld3(origin), fw = ld3(forward);
+    for (int64_t t = 0; t < N; t++) {
+        v3 dir = normalize(vsub(ld3(points + 3 * t), o));
+        if (dot(dir, fw) < (real)cutoff) continue;
+        real ws = (real)wsum_in[t];
+        v3 value = ld3(value_in + 3 * t), g = ld3(grad_value + 3 * t);
+        if (value.x <= K(0.0)) g.x = 0;
+        if (value.y <= K(0.0)) g.y = 0;
+        if (value.z <= K(0.0)) g.z = 0;
+        value = vsub(value, mk(K(0.5), K(0.5), K(0.5)));
+        real dp_out = dot(g, value);
+        for (int i = 0; i < dof; i++) {
+            int64_t e = (int64_t)i * N + t;
+            v3 axis = ld3(sites + 3 * e), val = ld3(values + 3 * e);
+            real temp = (real)temps[e];
+            real dist = length(vsub(dir, axis));
+            real w = r_exp(-temp * dist);
+            if (w / ws < K(1e-3)) continue;
+            v3 dval = vdivs(smul(w, g), ws);
+            g_values[3 * e] = (out_t)dval.x; g_values[3 * e + 1] = (out_t)dval.y; g_values[3 * e + 2] = (out_t)dval.z;
+            v3 dwds = vdivs(smul(temp * w, vsub(dir, axis)), dist);
+            real dwdt = -dist * w;
+            real dp = dot(g, val);
+            v3 daxis = vdivs(smul(dp - dp_out, dwds), ws);
+            g_sites[3 * e] = (out_t)daxis.x; g_sites[3 * e + 1] = (out_t)daxis.y; g_sites[3 * e + 2] = (out_t)daxis.z;
+            g_temps[e] = (out_t)(dwdt * (dp - dp_out) / ws);
+        }
+    }
+}
+
 int FN(orc_num_threads)(void) {
 #ifdef _OPENMP
     return omp_get_max_threads();

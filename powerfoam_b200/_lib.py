@@ -178,6 +178,9 @@ _SIGS = {
     "pf_morton_workspace_size": [c_i64, ctypes.POINTER(ctypes.c_size_t)],
     "pf_morton_sort": [c_vp, c_i64, c_vp, ctypes.c_size_t, c_vp, c_vp],
     "pf_power_workspace_size": [c_i64, c_vp],
+    "pf_sv_forward": [c_vp, c_vp, c_vp, ctypes.c_float, c_vp, c_vp, c_vp, c_i64, c_i32, c_i32, c_vp, c_vp, c_vp],
+    "pf_sv_backward": [c_vp, c_vp, c_vp, ctypes.c_float, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_i64, c_i32, c_i32,
+                       c_vp, c_vp, c_vp, c_vp],
     "pf_steiner_knn": [c_vp, c_vp, c_i64, c_vp, c_vp, c_i64, c_i32, c_vp, c_vp, c_vp, c_vp],
     "pf_steiner_select": [c_vp, c_vp, c_i64, c_i64, ctypes.c_float, c_vp, c_vp, c_vp, c_vp],
     "pf_power_adjacency": [c_vp, c_vp, c_i64, ctypes.c_int32, c_vp, ctypes.c_size_t, c_i64, c_vp, c_vp, c_vp, c_vp,

@@ -19,7 +19,7 @@ LIB_PATH = os.path.join(LIB_DIR, "libpfoam.so")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
 SOURCES = ["pf_api.cu", "pf_bin.cu", "pf_composite.cu", "pf_batch.cu", "pf_raster.cu", "pf_trace.cu", "pf_adjacency.cu", "pf_interpen.cu",
-           "pf_mlp.cu"]
+           "pf_color.cu", "pf_mlp.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-fmad=false", "-prec-div=true", "-prec-sqrt=true",
          "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden", "--expt-relaxed-constexpr"]

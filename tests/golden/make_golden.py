@@ -1,7 +1,7 @@
 """Generate golden vectors by executing the reference's own kernel source.
 
-Imports powerfoam/rasterize.py, raytrace.py and geometry.py (and functions of
-benchmark.py) from the reference
+Imports powerfoam/rasterize.py, raytrace.py, geometry.py and color_fn.py (and
+functions of benchmark.py) from the reference
 checkout (default /root/reference, or $PF_REFERENCE) with warp replaced by
 tests/golden/warp_shim.py, runs the kernels on small seeded scenes, and writes
 tests/golden/*.npz.  Run from the repository root:
@@ -549,6 +549,48 @@ def steiner_case(name, seed, n=4000):
     print(name, "steiner points", sp.shape[0], "rounds", len(samples))
 
 
+def sv_case(name, seed, n=3000, dof=6):
+    """spherical_voronoi_fwd_kernel / _bwd_kernel (color_fn.py:54-184) from
+    the reference's own source, float32 attributes; a camera whose cone
+    leaves some points out."""
+    import powerfoam.color_fn as rcol
+
+    warp_shim.patch_module_builtins(rcol)
+
+    class SvArgs:
+        sv_dof = dof
+
+    sv = rcol.SphericalVoronoi(SvArgs(), "cpu", "float")
+    rng = np.random.default_rng(seed)
+    pts = rng.uniform(-1, 1, (n, 3)).astype(F32)
+    cam = look_at_camera((0.2, 0.1, 0.3), (0, 0, -1.0), 64, 48, 70.0)  # inside the cloud
+    origin = cam["eye"].astype(F32)
+    fwd = np.cross(cam["up"], cam["right"]).astype(F32)
+    fwd = (fwd / np.linalg.norm(fwd)).astype(F32)
+    cutoff = F32(np.cos(np.arctan(np.hypot(np.linalg.norm(cam["right"]), np.linalg.norm(cam["up"])))
+                        + np.radians(10.0)))
+    ax = rng.standard_normal((dof, n, 3))
+    sites = (ax / np.linalg.norm(ax, axis=-1, keepdims=True)).astype(F32)
+    values = (rng.standard_normal((dof, n, 3)) * 0.4).astype(F32)
+    temps = rng.uniform(1.0, 12.0, (dof, n)).astype(F32)
+    vout = np.zeros((n, 3), F32)
+    wout = np.zeros(n, F32)
+    wp.launch(sv.spherical_voronoi_fwd_kernel, dim=n,
+              inputs=[pts, origin, fwd, cutoff, sites, values, temps, n, vout, wout])
+    g = rng.standard_normal((n, 3)).astype(F32)
+    gp = np.zeros((n, 3), F32)
+    gs = np.zeros((dof, n, 3), F32)
+    gv = np.zeros((dof, n, 3), F32)
+    gt = np.zeros((dof, n), F32)
+    wp.launch(sv.spherical_voronoi_bwd_kernel, dim=n,
+              inputs=[pts, origin, fwd, cutoff, sites, values, temps, wout, vout, g, n, gp, gs, gv, gt])
+    np.savez_compressed(os.path.join(HERE, f"{name}.npz"), points=pts, origin=origin, forward=fwd,
+                        cutoff=np.float32(cutoff), sites=sites, values=values, temps=temps, value=vout, wsum=wout,
+                        grad_value=g, grad_sites=gs, grad_values=gv, grad_temps=gt, cam_eye=cam["eye"],
+                        cam_right=cam["right"], cam_up=cam["up"], width=cam["width"], height=cam["height"])
+    print(name, "outside the cone", int((wout == 0).sum()), "of", n)
+
+
 def edge_scene(seed):
     """Primitives that exercise culling and the tile-range arithmetic: behind
     the camera, closer than 4r, straddling the image border, one covering many
@@ -574,7 +616,7 @@ def edge_scene(seed):
 
 def main():
     which = sys.argv[1:] or ["raster_small", "raster_edge", "raster_dense", "bin_large", "interpen_small", "raster_generic", "steiner_small",
-                           "trace_small"]
+                           "sv_small", "trace_small"]
     if "raster_small" in which:
         sc = make_scene(1, 120, -0.6, 0.6, 0.05, 0.2)
         raster_case("raster_small", sc, look_at_camera((0.3, 0.4, 2.0), (0, 0, 0), 36, 28, 60.0), 1)
@@ -599,6 +641,8 @@ def main():
         generic_case("raster_generic", sc, cam, fisheye_ray_maps(cam, 80.0), 8)
     if "steiner_small" in which:
         steiner_case("steiner_small", 9)
+    if "sv_small" in which:
+        sv_case("sv_small", 10)
     if "trace_small" in which:
         sc = make_scene(4, 150, -0.6, 0.6, 0.08, 0.2)
         trace_case("trace_small", sc, look_at_camera((0.2, 0.3, 2.2), (0, 0, 0), 24, 20, 60.0))

@@ -329,6 +329,9 @@ def install():
     # fixed-size local matrices (the generic binning's traversal stacks, the
     # cone builders' scratch): zero-initialised numpy arrays of that type
     wp.mat = lambda shape, dtype: np.zeros(shape, dtype=np.int32 if dtype in (_int32, _uint32, _int64) else F32)
+    wp.identity = lambda n, dtype: np.eye(n, dtype=F32)
+    wp.outer = lambda a, b: np.outer(np.asarray(a, F32), np.asarray(b, F32)).astype(F32)
+    wp.array2d = _array
     wp.launch = launch
     wp.cw_div = lambda a, b: a / b
     wp.Bvh = None

@@ -135,3 +135,19 @@ def test_generic_forward_and_backward(golden):
     for a, b in [("spheres", "spheres_grad"), ("nsigmas", "nsigmas_grad"), ("texel_sites", "texel_sites_grad"),
                  ("texel_rgb", "texel_rgb_grad"), ("texel_height", "texel_height_grad")]:
         assert_close_rel(gr[a], g[b], 1e-4, a)
+
+
+# ---------------------------------------------------------------------------
+# spherical-Voronoi texel colour (color_fn.py:54-184)
+
+
+def test_spherical_voronoi_forward_and_backward(golden):
+    g = golden("sv_small")
+    args = (g["points"], g["origin"], g["forward"], float(g["cutoff"]), g["sites"], g["values"], g["temps"])
+    v, w = orc.sv_forward(*args)
+    assert max_abs(v, g["value"]) <= 1e-6
+    assert_close_rel(w, g["wsum"], 1e-6, "weight sum")
+    assert np.array_equal(w == 0, g["wsum"] == 0)  # the same points fall outside the cone
+    gs, gv, gt = orc.sv_backward(*args, g["wsum"], g["value"], g["grad_value"])
+    for a, k in [(gs, "grad_sites"), (gv, "grad_values"), (gt, "grad_temps")]:
+        assert_close_rel(a, g[k], 1e-5, k)
