@@ -56,7 +56,8 @@ def parse():
                    "(a quarter-size case with the same density per pixel, for profiling), batch3m (32 views of "
                    "a 3.1M-primitive scene in one graph-captured persistent step), batch256k (its small case), "
                    "trace1m (tracer forward + adjoint), interpen3m (interpenetration loss forward + adjoint), power1m "
-                   "(power-diagram adjacency build), fisheye1m (raster1m through a generic fisheye camera) or proposal "
+                   "(power-diagram adjacency build), fisheye1m (raster1m through a generic fisheye camera), color1m "
+                   "(spherical-Voronoi texel colour forward + adjoint) or proposal "
                    "(proposal-seeded vs plain cell walk)")
     p.add_argument("--cpu-sample-tiles", type=int, default=0, help="tiles composited by the CPU baseline")
     p.add_argument("--no-cpu-baseline", action="store_true")
@@ -787,6 +788,102 @@ def power_main(args, dev):
     print(json.dumps(line), flush=True)
 
 
+def color_main(args, dev):
+    """Spherical-Voronoi texel colour forward + adjoint (color_fn.py) for the
+    texel sites of the 1,048,576-primitive scene: 8 sites per primitive
+    (8,388,608 points), sv_dof 8, float32 attributes, seeded; one step =
+    colours of every texel, an L2 loss and the site gradients."""
+    from powerfoam_b200 import synthetic
+    from powerfoam_b200.color_fn import SphericalVoronoi
+
+    cfg = synthetic.CONFIGS["raster1m"]
+    sc = synthetic.make_scene(cfg["n"], seed=cfg["seed"], mixture=cfg["mixture"], sigma=cfg["sigma"],
+                              r_range=cfg["r_range"], device=dev)
+    cam = synthetic.orbit_camera(100, cfg["width"], cfg["height"], cfg["vfov"], device=dev)
+    pts = sc["texel_sites"].reshape(-1, 3).contiguous()
+    n, dof = pts.shape[0], 8
+    g = torch.Generator(device=dev).manual_seed(7)
+    ax = torch.randn(dof, n, 3, device=dev, generator=g)
+    sites = (ax / ax.norm(dim=-1, keepdim=True)).requires_grad_(True)
+    values = (0.3 * torch.randn(dof, n, 3, device=dev, generator=g)).requires_grad_(True)
+    temps = (1.0 + 9.0 * torch.rand(dof, n, device=dev, generator=g)).requires_grad_(True)
+    target = torch.rand(n, 3, device=dev, generator=g)
+
+    class SvArgs:
+        sv_dof = dof
+
+    sv = SphericalVoronoi(SvArgs(), dev)
+    events = {"fwd": [], "bwd": []}
+
+    def step(record=False):
+        for t in (sites, values, temps):
+            t.grad = None
+        if record:
+            a0, a1, b1 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+            a0.record()
+        col = sv.forward(pts, cam, sites, values, temps)
+        if record:
+            a1.record()
+        loss = ((col - target) ** 2).sum()
+        loss.backward()
+        if record:
+            b1.record()
+            events["fwd"].append((a0, a1))
+            events["bwd"].append((a1, b1))
+        return loss
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(int(os.environ.get("LOCAL_RANK", "0")))
+    clocks.start()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    a.record()
+    for _ in range(args.steps):
+        step()
+    b.record()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = a.elapsed_time(b) / args.steps
+    for _ in range(args.steps):
+        step(record=True)
+    torch.cuda.synchronize()
+    fwd_ms = statistics.mean(x.elapsed_time(y) for x, y in events["fwd"])
+    bwd_ms = statistics.mean(x.elapsed_time(y) for x, y in events["bwd"])
+    # unique bytes: points 12, per site axis 12 + value 12 + temperature 4; forward writes colour 12 + weight
+    # sum 4; the adjoint also reads those and the colour gradient (12) and writes the 28 B of site gradients
+    fwd_bytes = n * (12 + dof * 28 + 16)
+    bwd_bytes = n * (12 + dof * 28 + 28) + n * dof * 28
+    peak, peak_kind = load_peaks()
+    dom_ms, dom_bytes, kern = ((bwd_ms, bwd_bytes, "pf_sv_backward") if bwd_ms >= fwd_ms
+                               else (fwd_ms, fwd_bytes, "pf_sv_forward"))
+    achieved = dom_bytes / (dom_ms * 1e-3) / 1e9
+    loss_host = torch.empty(args.steps, dtype=torch.float32).pin_memory()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    for i in range(args.steps):
+        loss_host[i].copy_(step().detach(), non_blocking=True)
+    e1.record()
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1) / args.steps
+    line = dict(metric="spherical-Voronoi texel colour fwd+bwd @8.4M texels", value=1000.0 / ms,
+                unit="iterations/s", n_gpus=1, steps=args.steps, warmup=max(args.warmup, 3), ms_per_step=ms,
+                higher_is_better=True, scaling="weak", vs_baseline=None, dtype="f32",
+                data="synthetic (texel sites of the seeded raster1m scene, seeded sites / values / temperatures)",
+                config=dict(workload="color1m", points=n, sv_dof=dof,
+                            l2="inputs larger than L2 (1.9 GB of site attributes), no flush"),
+                clocks=clk,
+                e2e=dict(value=1000.0 / e2e_ms, unit="iterations/s", h2d_bytes_per_step=0, d2h_bytes_per_step=4,
+                         note="attributes are training state resident on the device; the loss is read back"),
+                roofline=dict(bound="hbm", kernel=kern, achieved=achieved, peak=peak, unit="GB/s",
+                              frac=achieved / peak, peak_source=peak_kind, traffic=None, algorithmic_bytes=dom_bytes,
+                              ms=dom_ms, fwd_ms=fwd_ms, bwd_ms=bwd_ms),
+                gpu_launches=args.steps * 2)
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -812,6 +909,9 @@ def main():
         return
     if args.workload == "power1m":
         power_main(args, dev)
+        return
+    if args.workload == "color1m":
+        color_main(args, dev)
         return
     if args.workload.startswith("batch"):
         batch_main(args, world, rank, local, dev)

@@ -232,9 +232,9 @@ PF_API int pf_steiner_select(const float *samples, const float *radii, int64_t n
  * 0.5 grey (weight sum 0) when the direction is outside the camera cone
  * (dot(d, forward) < fov_cos_cutoff).  att_sites / att_values are
  * (sv_dof, N, 3), att_temps (sv_dof, N); f32, or f16 with attr_half = 1
- * (then value_out / weights_sum_out are f16 too).  The backward zeroes and
- * fills the site gradients, skipping sites with w / sum w < 1e-3; the
- * points get no gradient (the reference's is disabled). */
+ * (then value_out / weights_sum_out are f16 too).  The backward writes every
+ * site gradient: zero where w / sum w < 1e-3 or outside the cone; the points
+ * get no gradient (the reference's is disabled). */
 PF_API int pf_sv_forward(const float *points, const float *camera_origin /* host, 3 */,
                          const float *camera_forward /* host, 3 */, float fov_cos_cutoff, const void *att_sites,
                          const void *att_values, const void *att_temps, int64_t n_points, int32_t sv_dof,

@@ -5,14 +5,16 @@
 // texel point p with view direction d = normalize(p - eye):
 //     w_i = exp(-temp_i |d - axis_i|),  colour = max(sum w_i val_i / sum w_i + 0.5, 0)
 // over its sv_dof sites, or 0.5 grey with weight sum 0 outside the camera
-// cone (d . forward < fov_cos_cutoff).  The adjoint gives the site axes,
-// values and temperatures their gradients, skipping sites whose normalised
-// weight is below 1e-3 (their gradients stay zero, as the reference's zeroed
-// outputs); the points receive none (the reference's point gradient is
-// disabled).  Float32 arithmetic in the reference's order; attributes may be
-// float32 or float16 (then read and written rounded as the reference's half
-// kernels do).  One thread per point: the kernels stream 12 * sv_dof * 2 + 4
-// bytes (f32) per point and are HBM-bound.
+// cone (d . forward < fov_cos_cutoff).  The adjoint writes every site's
+// gradients: zero for sites whose normalised weight is below 1e-3 and for
+// points outside the cone (the reference leaves its zero-initialised outputs
+// there), the derivatives elsewhere; the points receive none (the
+// reference's point gradient is disabled).  Float32 arithmetic in the
+// reference's order; attributes may be float32 or float16 (then read and
+// written rounded as the reference's half kernels do).  One thread per
+// point; the site arrays are (sv_dof, N, ...), so a warp reads contiguous
+// 384-byte runs.  The kernels stream 28 bytes per site (f32) and are
+// HBM-bound.
 
 #include <cstdint>
 
@@ -97,7 +99,17 @@ __global__ void sv_backward_kernel(const float* __restrict__ points, SvArgs a, c
     const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= a.n) return;
     v3 dir;
-    if (!sv_direction(points, t, a, dir)) return;
+    if (!sv_direction(points, t, a, dir)) {  // no gradient outside the camera cone
+        for (int i = 0; i < a.dof; i++) {
+            const int64_t e = (int64_t)i * a.n + t;
+            for (int k = 0; k < 3; k++) {
+                st_attr(g_sites, 3 * e + k, 0.0f);
+                st_attr(g_values, 3 * e + k, 0.0f);
+            }
+            st_attr(g_temps, e, 0.0f);
+        }
+        return;
+    }
     const float ws = ld_attr(wsum_in, t);
     v3 value = mk(ld_attr(value_in, 3 * t), ld_attr(value_in, 3 * t + 1), ld_attr(value_in, 3 * t + 2));
     v3 g = mk(ld_attr(grad_value, 3 * t), ld_attr(grad_value, 3 * t + 1), ld_attr(grad_value, 3 * t + 2));
@@ -113,7 +125,14 @@ __global__ void sv_backward_kernel(const float* __restrict__ points, SvArgs a, c
         const float temp = ld_attr(temps, e);
         const float dist = length(dir - axis);
         const float w = expf(-temp * dist);
-        if (w / ws < 1e-3f) continue;
+        if (w / ws < 1e-3f) {  // a negligible site: zero gradient
+            for (int k = 0; k < 3; k++) {
+                st_attr(g_sites, 3 * e + k, 0.0f);
+                st_attr(g_values, 3 * e + k, 0.0f);
+            }
+            st_attr(g_temps, e, 0.0f);
+            continue;
+        }
         const v3 dval = (w * g) / ws;
         st_attr(g_values, 3 * e, dval.x);
         st_attr(g_values, 3 * e + 1, dval.y);
@@ -178,11 +197,6 @@ extern "C" int pf_sv_backward(const float* points, const float* camera_origin, c
         return pf_fail(PF_ERR_ARGS, "pf_sv_backward: bad arguments");
     if (n_points == 0) return PF_OK;
     cudaStream_t st = (cudaStream_t)stream;
-    const size_t es = attr_half ? 2 : 4, m = (size_t)sv_dof * (size_t)n_points;
-    if (cudaMemsetAsync(grad_att_sites, 0, 3 * m * es, st) != cudaSuccess ||
-        cudaMemsetAsync(grad_att_values, 0, 3 * m * es, st) != cudaSuccess ||
-        cudaMemsetAsync(grad_att_temps, 0, m * es, st) != cudaSuccess)
-        return pf_check_launch("pf_sv_backward");
     const unsigned g = (unsigned)((n_points + 255) / 256);
     if (attr_half)
         sv_backward_kernel<__half><<<g, 256, 0, st>>>(
