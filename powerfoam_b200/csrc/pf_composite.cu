@@ -34,12 +34,11 @@
 
 namespace pf {
 
-// GEN: a generic camera (per-pixel rays from ray maps); it takes the
-// one-pixel-per-lane (or two-per-lane) path, not the pair-compacted one
+// GEN: a generic camera (per-pixel rays from ray maps)
 template <int TW, bool GEN = false>
 __global__ void __launch_bounds__(Layout<TW>::THREADS) raster_fwd_kernel(RasterParams P, FwdOut out) {
     constexpr int G = Layout<TW>::G;
-    constexpr bool COMPACT = Layout<TW>::PPL == 1 && !GEN;
+    constexpr bool COMPACT = Layout<TW>::PPL == 1;
     // the per-pixel layouts stage per warp here; the compacted one keeps its
     // staging in dynamic shared memory
     __shared__ WarpStage stage[COMPACT ? 1 : G];
@@ -51,7 +50,9 @@ __global__ void __launch_bounds__(Layout<TW>::THREADS) raster_fwd_kernel(RasterP
         int64_t tile = next_tile<G>(P, static_next, lane, &ss);
         if (tile < 0) break;
         if constexpr (COMPACT)
-            fwd_tile_c<G>(P, out, tile, warp, lane, reinterpret_cast<FwdCStage*>(fwd_dyn)[warp], ss);
+            // generic cameras keep the pixels' ray origins after the stages
+            fwd_tile_c<G, GEN>(P, out, tile, warp, lane, reinterpret_cast<FwdCStage*>(fwd_dyn)[warp], ss,
+                               reinterpret_cast<float4*>(reinterpret_cast<FwdCStage*>(fwd_dyn) + G) + 32 * warp);
         else
             fwd_tile<G, Layout<TW>::PPL, GEN>(P, out, tile, warp, lane, stage[warp], ss);
     }
@@ -60,7 +61,7 @@ __global__ void __launch_bounds__(Layout<TW>::THREADS) raster_fwd_kernel(RasterP
 // dynamic shared memory of the forward: the pair-compaction stage per warp
 template <int TW, bool GEN = false>
 constexpr size_t fwd_dyn_bytes() {
-    return (Layout<TW>::PPL == 1 && !GEN) ? sizeof(FwdCStage) * Layout<TW>::G : 0;
+    return Layout<TW>::PPL == 1 ? (sizeof(FwdCStage) + (GEN ? 32 * sizeof(float4) : 0)) * Layout<TW>::G : 0;
 }
 
 

@@ -430,14 +430,18 @@ PF_D int seg_search(const int* off, int n, int x) {
     return lo;
 }
 
-template <int G>
+// GEN: per-pixel rays of a generic camera; `org` (32 per warp, shared) then
+// holds the pixels' ray origins, and faces are staged with the ray-independent
+// face_offset, each pair subtracting its own origin's dot product.
+template <int G, bool GEN = false>
 PF_D void fwd_tile_c(const RasterParams& P, const FwdOut& out, int64_t tile, int wig, int lane, FwdCStage& cs,
-                     StopState& ss) {
+                     StopState& ss, float4* org = nullptr) {
     const v3 o = P.cam.eye;
     const float HW = (float)(P.cam.H * P.cam.W);
     const bool want_gt = out.rpe || out.err;
     FwdPix a;
     a.g = pixel_geom(P, tile, wig * 32 + lane);
+    if constexpr (GEN) pixel_ray_map(P, a.g, a.o);
     a.log_t = 0.f;
     a.trans = 1.0f;
     a.nd = 0.f;
@@ -455,6 +459,7 @@ PF_D void fwd_tile_c(const RasterParams& P, const FwdOut& out, int64_t tile, int
         if (want_gt) a.gt = mk(P.gt[3 * a.g.px], P.gt[3 * a.g.px + 1], P.gt[3 * a.g.px + 2]);
     }
     cs.dir[lane] = make_float4(a.g.d.x, a.g.d.y, a.g.d.z, 0.f);
+    if constexpr (GEN) org[lane] = make_float4(a.o.x, a.o.y, a.o.z, 0.f);
     const uint32_t lt_mask = (1u << lane) - 1u;
     const int64_t start = P.tile_off[tile];
     const int total = (int)(P.tile_off[tile + 1] - start);
@@ -476,7 +481,7 @@ PF_D void fwd_tile_c(const RasterParams& P, const FwdOut& out, int64_t tile, int
         for (int kk = 0; kk < kn; kk++) {
             const float4 s4 = cs.sph[kk];
             float tn, tf;
-            const bool hit = a.g.oob ? false : ray_sphere(o, a.g.d, mk(s4.x, s4.y, s4.z), s4.w, tn, tf);
+            const bool hit = a.g.oob ? false : ray_sphere(ray_org<GEN>(a, o), a.g.d, mk(s4.x, s4.y, s4.z), s4.w, tn, tf);
             const uint32_t m = __ballot_sync(0xffffffffu, hit);
             if (lane == 0) cs.mask[kk] = m;
         }
@@ -518,8 +523,8 @@ PF_D void fwd_tile_c(const RasterParams& P, const FwdOut& out, int64_t tile, int
                 const uint2 raw = __ldg(&P.adj_diff[a0 + (i - cs.face_off[j])]);
                 const v3 diff = mk(h2f((uint16_t)(raw.x & 0xffffu)), h2f((uint16_t)(raw.x >> 16)),
                                    h2f((uint16_t)(raw.y & 0xffffu)));
-                const Face f = make_face(o, center, dot(center, center), s4.w * s4.w, center + diff,
-                                         h2f((uint16_t)(raw.y >> 16)));
+                const Face f = make_face(GEN ? mk(0.f, 0.f, 0.f) : o, center, dot(center, center), s4.w * s4.w,
+                                         center + diff, h2f((uint16_t)(raw.y >> 16)));
                 cs.face[i] = make_float4(f.n.x, f.n.y, f.n.z, f.num);
             }
             __syncwarp();
@@ -532,20 +537,24 @@ PF_D void fwd_tile_c(const RasterParams& P, const FwdOut& out, int64_t tile, int
                     const int p = nth_set_bit(cs.mask[kk], j - cs.pair_off[r]);
                     const float4 d4 = cs.dir[p];
                     const v3 d = mk(d4.x, d4.y, d4.z);
+                    v3 po = o;  // the pair's ray origin
+                    if constexpr (GEN) po = mk(org[p].x, org[p].y, org[p].z);
                     const float4 s4 = cs.sph[kk];
                     const v3 center = mk(s4.x, s4.y, s4.z);
                     const float radius = s4.w;
                     const int32_t prim = cs.pid[kk];
                     float tn, tf;
-                    ray_sphere(o, d, center, radius, tn, tf);
+                    ray_sphere(po, d, center, radius, tn, tf);
                     if (!big) {
                         const int f1 = cs.face_off[r + 1];
 #pragma unroll 2
                         for (int q = cs.face_off[r]; q < f1; q++) {
                             const float4 f = cs.face[q];
-                            const float dp = dot(d, mk(f.x, f.y, f.z));
-                            if (face_may_clip(dp, f.w, tn, tf)) {
-                                const float t_face = f.w / dp;
+                            const v3 fn = mk(f.x, f.y, f.z);
+                            const float dp = dot(d, fn);
+                            const float num = GEN ? f.w - dot(po, fn) : f.w;
+                            if (face_may_clip(dp, num, tn, tf)) {
+                                const float t_face = num / dp;
                                 tf = dp >= 0.0f ? fmin_t(t_face, tf) : tf;
                                 tn = dp < 0.0f ? fmax_t(t_face, tn) : tn;
                             }
@@ -558,7 +567,7 @@ PF_D void fwd_tile_c(const RasterParams& P, const FwdOut& out, int64_t tile, int
                             const uint2 raw = __ldg(&P.adj_diff[e]);
                             const v3 diff = mk(h2f((uint16_t)(raw.x & 0xffffu)), h2f((uint16_t)(raw.x >> 16)),
                                                h2f((uint16_t)(raw.y & 0xffffu)));
-                            const Face f = make_face(o, center, cc, rr, center + diff, h2f((uint16_t)(raw.y >> 16)));
+                            const Face f = make_face(po, center, cc, rr, center + diff, h2f((uint16_t)(raw.y >> 16)));
                             const float dp = dot(d, f.n);
                             if (face_may_clip(dp, f.num, tn, tf)) {
                                 const float t_face = f.num / dp;
@@ -569,7 +578,7 @@ PF_D void fwd_tile_c(const RasterParams& P, const FwdOut& out, int64_t tile, int
                     }
                     const float4 n4 = cs.nsg[kk];
                     const PlaneRes pr =
-                        plane_fwd_tex(o, d, tn, center, mk(n4.x, n4.y, n4.z), radius, global_texels(P, prim), P.S);
+                        plane_fwd_tex(po, d, tn, center, mk(n4.x, n4.y, n4.z), radius, global_texels(P, prim), P.S);
                     const float tf2 = pr.dp >= 0.0f ? fmin_t(pr.t_surf, tf) : tf;
                     const float tn2 = pr.dp < 0.0f ? fmax_t(pr.t_surf, tn) : tn;
                     cs.rec[j & 63] = make_float4(tf2 - tn2, pr.rgb.x, pr.rgb.y, pr.rgb.z);
