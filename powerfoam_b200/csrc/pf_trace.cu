@@ -234,16 +234,19 @@ trace_fwd_kernel(TraceParams P, int64_t nthreads, float* __restrict__ color, flo
 // derivative covers sites, colours, heights, plane origin and normal, the
 // query depth and the radius (through 1/r^2).
 
-struct TraceSeg {
+// One step of the walk without the texture plane: the cell's sphere and power
+// faces bound the segment [tn, tf] (ids: -1 sphere, -2 behind the eye, else
+// the face index), `next` is the cell across the nearest exit face.  `hit`
+// is false for a cell the ray misses, an empty interval or density < 1e-3.
+struct WalkStep {
     bool hit;
-    float tn, tf, dt, pre_tn, sigma, radius;
-    int tn_id, tf_id, pre_tn_id;
+    float tn, tf, sigma;
+    int tn_id, tf_id;
     int32_t next;
-    v3 center, pn;
-    PlaneRes pr;
 };
 
-PF_D void trace_step(const TraceParams& P, v3 o, v3 d, int32_t prim, TraceSeg& sg) {
+PF_D WalkStep walk_step(const TraceParams& P, v3 o, v3 d, int32_t prim) {
+    WalkStep w;
     const float4 s4 = __ldg(&P.spheres[prim]);
     const v3 center = mk(s4.x, s4.y, s4.z);
     const float radius = s4.w;
@@ -270,31 +273,14 @@ PF_D void trace_step(const TraceParams& P, v3 o, v3 d, int32_t prim, TraceSeg& s
         if (dp < 0.0f && t_face > tn) tn_id = e - a0;
         tn = dp < 0.0f ? fmax_t(t_face, tn) : tn;
     }
-    const float* ns = (const float*)P.nsig + 4 * (int64_t)prim;
-    sg.pn = mk(__ldg(ns), __ldg(ns + 1), __ldg(ns + 2));
-    sg.sigma = __ldg(ns + 3);
-    sg.next = next;
-    sg.center = center;
-    sg.radius = radius;
-    sg.hit = false;
-    if (!hit || tn > tf || sg.sigma < 1e-3f) return;
-    sg.pre_tn = tn;
-    sg.pre_tn_id = tn_id;
-    int64_t b3 = (int64_t)prim * P.S * 3;
-    PlaneRes pr = plane_local<float>(o, d, tn, center, sg.pn, radius, (const float*)P.sites + b3,
-                                     (const float*)P.rgb + b3, (const float*)P.height + (int64_t)prim * P.S, P.S);
-    const int n_adj = a1 - a0;
-    if (pr.dp >= 0.0f && pr.t_surf < tf) tf_id = n_adj;
-    tf = pr.dp >= 0.0f ? fmin_t(pr.t_surf, tf) : tf;
-    if (pr.dp < 0.0f && pr.t_surf > tn) tn_id = n_adj;
-    tn = pr.dp < 0.0f ? fmax_t(pr.t_surf, tn) : tn;
-    sg.pr = pr;
-    sg.tn = tn;
-    sg.tf = tf;
-    sg.tn_id = tn_id;
-    sg.tf_id = tf_id;
-    sg.dt = tf - tn;
-    sg.hit = sg.dt > 0.0f;
+    w.sigma = __ldg((const float*)P.nsig + 4 * (int64_t)prim + 3);
+    w.next = next;
+    w.tn = tn;
+    w.tf = tf;
+    w.tn_id = tn_id;
+    w.tf_id = tf_id;
+    w.hit = hit && !(tn > tf) && !(w.sigma < 1e-3f);
+    return w;
 }
 
 struct TraceGrads {
@@ -383,113 +369,278 @@ PF_D float plane_local_bwd(v3 o, v3 d, float tn, v3 po, v3 pn, float radius, con
     return g_tn;
 }
 
+// The adjoint kernel runs each warp's 32 rays in rounds.  Walk: every live
+// lane steps its ray until it holds kTrQueue hit cells (sphere and faces
+// give a non-empty interval) or the ray ends; only the face loop runs here.
+// Texture planes: the warp's queued hits, compacted, are spread over all 32
+// lanes.  Prefix: each lane folds its own hits in walk order into the
+// transmittance and the colour / normal accumulated so far (the exact float
+// sequence of the forward), dropping the hits after the ray's transmittance
+// fell below the threshold.  Gradients: the compacted hits again over all
+// lanes.  Only about one walked cell in five is a hit, so the texture and
+// gradient work, which dominate, run on full warps instead of on the few
+// lanes whose cell is a hit.
+constexpr int kTrQueue = 4;    // queued hits per lane and round
+constexpr int kTrItem = 23;    // words per queued hit (odd: conflict-free strides)
+constexpr int kTrWarps = 4;    // warps per 128-thread block
+// queued hit words
+enum : int {
+    kQCell = 0, kQTn = 1, kQTf = 2, kQIds = 3, kQSigma = 4,
+    kQPr = 5,       // PlaneRes: _t_surf _dp height _wsum t_surf dp wsum rgb.x rgb.y rgb.z (5..14)
+    kQTrans = 15, kQC = 16, kQN = 19, kQSeg = 22
+};
+
+PF_D void q_store_pr(float* q, const PlaneRes& r) {
+    q[kQPr] = r._t_surf;
+    q[kQPr + 1] = r._dp;
+    q[kQPr + 2] = r.height;
+    q[kQPr + 3] = r._wsum;
+    q[kQPr + 4] = r.t_surf;
+    q[kQPr + 5] = r.dp;
+    q[kQPr + 6] = r.wsum;
+    q[kQPr + 7] = r.rgb.x;
+    q[kQPr + 8] = r.rgb.y;
+    q[kQPr + 9] = r.rgb.z;
+}
+
+PF_D PlaneRes q_load_pr(const float* q) {
+    PlaneRes r;
+    r._t_surf = q[kQPr];
+    r._dp = q[kQPr + 1];
+    r.height = q[kQPr + 2];
+    r._wsum = q[kQPr + 3];
+    r.t_surf = q[kQPr + 4];
+    r.dp = q[kQPr + 5];
+    r.wsum = q[kQPr + 6];
+    r.rgb = mk(q[kQPr + 7], q[kQPr + 8], q[kQPr + 9]);
+    return r;
+}
+
+PF_D int warp_incl_scan(int v, int lane) {
+    for (int s = 1; s < 32; s <<= 1) {
+        const int t = __shfl_up_sync(0xffffffffu, v, s);
+        if (lane >= s) v += t;
+    }
+    return v;
+}
+
+constexpr size_t trace_bwd_smem() {
+    return sizeof(float) * kTrWarps * 32 * (kTrQueue * kTrItem + 4) + sizeof(int) * kTrWarps * 32 * kTrQueue;
+}
+
 __global__ void __launch_bounds__(128)
 trace_bwd_kernel(TraceParams P, int64_t nthreads, const float* __restrict__ color, const float* __restrict__ normal,
                  const int32_t* __restrict__ depth_seg, const float* __restrict__ depth_sigma,
                  const float* __restrict__ g_color, const float* __restrict__ g_log_t,
                  const float* __restrict__ g_depth, const float* __restrict__ g_normal, TraceGrads G) {
-    int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (tid >= nthreads) return;
-    int pi, pj;
-    if (!trace_pixel(P.cam, tid, pi, pj)) return;
+    extern __shared__ float tr_smem[];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    float* Q = tr_smem + (size_t)w * 32 * kTrQueue * kTrItem;                      // queued hits
+    float* R = tr_smem + (size_t)kTrWarps * 32 * kTrQueue * kTrItem + w * 32 * 4;   // per lane: d, px
+    int* I = (int*)(tr_smem + (size_t)kTrWarps * 32 * (kTrQueue * kTrItem + 4)) + w * 32 * kTrQueue;
+    const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    int pi = 0, pj = 0;
+    bool alive = tid < nthreads && trace_pixel(P.cam, tid, pi, pj);
     const int64_t px = (int64_t)pi * P.cam.W + pj;
     const v3 o = P.cam.eye;
     const v3 d = ray_dir(P.cam, pi, pj);
-    const v3 gC = g_color ? mk(g_color[3 * px], g_color[3 * px + 1], g_color[3 * px + 2]) : mk(0.f, 0.f, 0.f);
-    const v3 gN = g_normal ? mk(g_normal[3 * px], g_normal[3 * px + 1], g_normal[3 * px + 2]) : mk(0.f, 0.f, 0.f);
-    const float gL = g_log_t ? g_log_t[px] : 0.f;
-    const float gD = g_depth ? g_depth[px] : 0.f;
-    const int m = depth_seg ? depth_seg[px] : -1;
-    const float sig_m = depth_sigma ? depth_sigma[px] : 1.f;
-    const v3 Cf = mk(color[3 * px], color[3 * px + 1], color[3 * px + 2]);
-    const v3 Nf = normal ? mk(normal[3 * px], normal[3 * px + 1], normal[3 * px + 2]) : mk(0.f, 0.f, 0.f);
+    R[lane * 4] = d.x;
+    R[lane * 4 + 1] = d.y;
+    R[lane * 4 + 2] = d.z;
+    R[lane * 4 + 3] = __int_as_float((int)px);
     v3 Cacc = mk(0.f, 0.f, 0.f), Nacc = mk(0.f, 0.f, 0.f);
     float log_t = 0.f;
-    int32_t prim = P.start_cells ? P.start_cells[px] : P.start_idx;
+    int32_t prim = alive ? (P.start_cells ? P.start_cells[px] : P.start_idx) : kNoCell;
     int steps = 0, seg = 0;
     for (;;) {
-        float trans = expf(log_t);
-        if (trans < P.thr || prim == kNoCell || steps >= P.max_steps || prim < 0 || prim >= P.N) break;
-        steps++;
-        TraceSeg sg;
-        trace_step(P, o, d, prim, sg);
-        const int32_t cur = prim;
-        prim = sg.next;
-        if (!sg.hit) continue;
-        const float sigma = sg.sigma, dt = sg.dt;
-        const float dlt = -sigma * dt;
-        const float e = expf(dlt);
-        const float alpha = 1.0f - e;
-        const v3 c = sg.pr.rgb;
-        Cacc = Cacc + trans * (alpha * c);
-        Nacc = Nacc + (alpha * trans) * sg.pn;
-        const float trans_next = trans * e;
-        float g_delta = dot(gC, (Cf - Cacc) - trans_next * c) + dot(gN, (Nf - Nacc) - trans_next * sg.pn) + gL;
-        if (m >= 0 && seg < m) g_delta += gD / sig_m;
-        float g_sigma = -dt * g_delta;
-        float g_tf = -sigma * g_delta, g_tn = sigma * g_delta;
-        if (seg == m) {
-            g_tn += gD;
-            g_sigma += -gD * logf(trans / P.depth_q) / (sigma * sigma);
-        }
-        const v3 g_c = (alpha * trans) * gC;
-        v3 g_pn = (alpha * trans) * gN;
-        v3 g_po = mk(0.f, 0.f, 0.f);
-        float g_r = 0.f;
-        const int32_t a0 = __ldg(&P.adj_off[cur]);
-        const int n_adj = __ldg(&P.adj_off[cur + 1]) - a0;
-        float g_ts = 0.f;
-        if (sg.tn_id == n_adj) {
-            g_ts += g_tn;
-            g_tn = 0.f;
-        }
-        if (sg.tf_id == n_adj) {
-            g_ts += g_tf;
-            g_tf = 0.f;
-        }
-        const int64_t b3 = (int64_t)cur * P.S * 3;
-        float g_pre_tn = plane_local_bwd(o, d, sg.pre_tn, sg.center, sg.pn, sg.radius, (const float*)P.sites + b3,
-                                         (const float*)P.rgb + b3, (const float*)P.height + (int64_t)cur * P.S, P.S,
-                                         sg.pr, g_c, g_ts, g_po, g_pn, g_r, G.sites + b3, G.rgb + b3,
-                                         G.height + (int64_t)cur * P.S);
-        if (sg.tn_id != n_adj) g_tn += g_pre_tn;
-        const float g_ends[2] = {sg.tn_id == n_adj ? g_pre_tn : g_tn, g_tf};
-        const int ids[2] = {sg.tn_id == n_adj ? sg.pre_tn_id : sg.tn_id, sg.tf_id};
-        v3 g_center = g_po;
-        for (int i = 0; i < 2; i++) {
-            const float gt = g_ends[i];
-            const int id = ids[i];
-            if (gt == 0.0f) continue;
-            if (id == -1) {
-                // t = (-qb -+ s)/2, qb = 2 oc.d, s = sqrt(qb^2 - 4(|oc|^2 - r^2)), oc = o - c
-                v3 oc = o - sg.center;
-                float qb = 2.0f * dot(oc, d);
-                float qc = dot(oc, oc) - sg.radius * sg.radius;
-                float s = sqrtf(qb * qb - 4.0f * qc);
-                v3 ds = (1.0f / (2.0f * s)) * ((-4.0f * qb) * d + 8.0f * oc);
-                float sgn = i == 1 ? 1.0f : -1.0f;
-                g_center = g_center + gt * (d + (sgn * 0.5f) * ds);
-                g_r += gt * (sgn * 2.0f * sg.radius / s);
-            } else if (id >= 0 && id < n_adj) {
-                const int32_t nb = __ldg(&P.adj[a0 + id]);
-                const float4 sj = __ldg(&P.spheres[nb]);
-                const v3 cj = mk(sj.x, sj.y, sj.z), ci = sg.center;
-                v3 n = cj - ci;
-                float num = 0.5f * (dot(cj, cj) - sj.w * sj.w - dot(ci, ci) + sg.radius * sg.radius) - dot(o, n);
-                float inv_den = 1.0f / dot(d, n);
-                float t = num * inv_den;
-                g_center = g_center + (gt * inv_den) * ((o - ci) + t * d);
-                g_r += gt * sg.radius * inv_den;
-                atomic_add3(G.points + 3 * (int64_t)nb, (gt * inv_den) * ((cj - o) - t * d));
-                atomicAdd(G.radii + nb, -gt * sj.w * inv_den);
+        // walk until kTrQueue hits are queued or the ray ends
+        int cnt = 0;
+        while (alive && cnt < kTrQueue) {
+            if (expf(log_t) < P.thr || prim == kNoCell || steps >= P.max_steps || prim < 0 || prim >= P.N) {
+                alive = false;
+                break;
             }
+            steps++;
+            const WalkStep ws = walk_step(P, o, d, prim);
+            if (ws.hit) {
+                float* q = Q + (lane * kTrQueue + cnt) * kTrItem;
+                q[kQCell] = __int_as_float(prim);
+                q[kQTn] = ws.tn;
+                q[kQTf] = ws.tf;
+                q[kQIds] = __uint_as_float(((unsigned)ws.tn_id & 0xffffu) | ((unsigned)ws.tf_id << 16));  // |id| < 2^15
+                q[kQSigma] = ws.sigma;
+                cnt++;
+            }
+            prim = ws.next;
         }
-        atomic_add3(G.points + 3 * (int64_t)cur, g_center);
-        atomicAdd(G.radii + cur, g_r);
-        atomic_add3(G.normals + 3 * (int64_t)cur, g_pn);
-        atomicAdd(G.density + cur, g_sigma);
-        log_t += dlt;
-        seg++;
+        const int incl = warp_incl_scan(cnt, lane);
+        const int total = __shfl_sync(0xffffffffu, incl, 31);
+        if (total == 0) break;  // a live lane leaves the walk only with a full queue
+        for (int k = 0; k < cnt; k++) I[incl - cnt + k] = lane * kTrQueue + k;
+        __syncwarp();
+        // texture planes of the queued hits, all lanes
+        for (int j = lane; j < total; j += 32) {
+            const int slot = I[j];
+            float* q = Q + slot * kTrItem;
+            const float* rr = R + (slot / kTrQueue) * 4;
+            const v3 dq = mk(rr[0], rr[1], rr[2]);
+            const int32_t cell = __float_as_int(q[kQCell]);
+            const float4 s4 = __ldg(&P.spheres[cell]);
+            const float* ns = (const float*)P.nsig + 4 * (int64_t)cell;
+            const v3 pn = mk(__ldg(ns), __ldg(ns + 1), __ldg(ns + 2));
+            const int64_t b3 = (int64_t)cell * P.S * 3;
+            q_store_pr(q, plane_local<float>(o, dq, q[kQTn], mk(s4.x, s4.y, s4.z), pn, s4.w,
+                                             (const float*)P.sites + b3, (const float*)P.rgb + b3,
+                                             (const float*)P.height + (int64_t)cell * P.S, P.S));
+        }
+        __syncwarp();
+        // transmittance and accumulated colour / normal, per ray in walk order
+        bool opaque = false;  // queued hits past the transmittance threshold are dropped
+        for (int k = 0; k < cnt; k++) {
+            float* q = Q + (lane * kTrQueue + k) * kTrItem;
+            q[kQSeg] = __int_as_float(-1);
+            const float trans = expf(log_t);
+            if (opaque || trans < P.thr) {
+                opaque = true;
+                alive = false;
+                continue;
+            }
+            float tn = q[kQTn], tf = q[kQTf];
+            const float t_surf = q[kQPr + 4], dp = q[kQPr + 5];
+            tf = dp >= 0.0f ? fmin_t(t_surf, tf) : tf;
+            tn = dp < 0.0f ? fmax_t(t_surf, tn) : tn;
+            const float dt = tf - tn;
+            if (!(dt > 0.0f)) continue;
+            const int32_t cell = __float_as_int(q[kQCell]);
+            const float* ns = (const float*)P.nsig + 4 * (int64_t)cell;
+            const v3 pn = mk(__ldg(ns), __ldg(ns + 1), __ldg(ns + 2));
+            const float sigma = q[kQSigma];
+            const float dlt = -sigma * dt;
+            const float alpha = 1.0f - expf(dlt);
+            Cacc = Cacc + trans * (alpha * mk(q[kQPr + 7], q[kQPr + 8], q[kQPr + 9]));
+            Nacc = Nacc + (alpha * trans) * pn;
+            q[kQTrans] = trans;
+            q[kQC] = Cacc.x;
+            q[kQC + 1] = Cacc.y;
+            q[kQC + 2] = Cacc.z;
+            q[kQN] = Nacc.x;
+            q[kQN + 1] = Nacc.y;
+            q[kQN + 2] = Nacc.z;
+            q[kQSeg] = __int_as_float(seg);
+            log_t += dlt;
+            seg++;
+        }
+        __syncwarp();
+        // gradients of the queued segments, all lanes
+        for (int j = lane; j < total; j += 32) {
+            const int slot = I[j];
+            const float* q = Q + slot * kTrItem;
+            const int sg_idx = __float_as_int(q[kQSeg]);
+            if (sg_idx < 0) continue;
+            const float* rr = R + (slot / kTrQueue) * 4;
+            const v3 dq = mk(rr[0], rr[1], rr[2]);
+            const int64_t qpx = (int64_t)__float_as_int(rr[3]);
+            const int32_t cur = __float_as_int(q[kQCell]);
+            const PlaneRes pr = q_load_pr(q);
+            const float4 s4 = __ldg(&P.spheres[cur]);
+            const v3 center = mk(s4.x, s4.y, s4.z);
+            const float radius = s4.w;
+            const float* ns = (const float*)P.nsig + 4 * (int64_t)cur;
+            const v3 pn = mk(__ldg(ns), __ldg(ns + 1), __ldg(ns + 2));
+            const int32_t a0 = __ldg(&P.adj_off[cur]);
+            const int n_adj = __ldg(&P.adj_off[cur + 1]) - a0;
+            const int ids = __float_as_int(q[kQIds]);
+            const int pre_tn_id = (int)(int16_t)(ids & 0xffff);
+            int tn_id = pre_tn_id, tf_id = ids >> 16;
+            const float pre_tn = q[kQTn];
+            float tn = pre_tn, tf = q[kQTf];
+            if (pr.dp >= 0.0f && pr.t_surf < tf) tf_id = n_adj;
+            tf = pr.dp >= 0.0f ? fmin_t(pr.t_surf, tf) : tf;
+            if (pr.dp < 0.0f && pr.t_surf > tn) tn_id = n_adj;
+            tn = pr.dp < 0.0f ? fmax_t(pr.t_surf, tn) : tn;
+            const float sigma = q[kQSigma], dt = tf - tn;
+            const float trans = q[kQTrans];
+            const v3 Cq = mk(q[kQC], q[kQC + 1], q[kQC + 2]);
+            const v3 Nq = mk(q[kQN], q[kQN + 1], q[kQN + 2]);
+            const v3 gC = g_color ? mk(g_color[3 * qpx], g_color[3 * qpx + 1], g_color[3 * qpx + 2])
+                                  : mk(0.f, 0.f, 0.f);
+            const v3 gN = g_normal ? mk(g_normal[3 * qpx], g_normal[3 * qpx + 1], g_normal[3 * qpx + 2])
+                                   : mk(0.f, 0.f, 0.f);
+            const float gL = g_log_t ? g_log_t[qpx] : 0.f;
+            const float gD = g_depth ? g_depth[qpx] : 0.f;
+            const int m = depth_seg ? depth_seg[qpx] : -1;
+            const float sig_m = depth_sigma ? depth_sigma[qpx] : 1.f;
+            const v3 Cf = mk(color[3 * qpx], color[3 * qpx + 1], color[3 * qpx + 2]);
+            const v3 Nf = normal ? mk(normal[3 * qpx], normal[3 * qpx + 1], normal[3 * qpx + 2]) : mk(0.f, 0.f, 0.f);
+            const float dlt = -sigma * dt;
+            const float e = expf(dlt);
+            const float alpha = 1.0f - e;
+            const v3 c = pr.rgb;
+            const float trans_next = trans * e;
+            float g_delta = dot(gC, (Cf - Cq) - trans_next * c) + dot(gN, (Nf - Nq) - trans_next * pn) + gL;
+            if (m >= 0 && sg_idx < m) g_delta += gD / sig_m;
+            float g_sigma = -dt * g_delta;
+            float g_tf = -sigma * g_delta, g_tn = sigma * g_delta;
+            if (sg_idx == m) {
+                g_tn += gD;
+                g_sigma += -gD * logf(trans / P.depth_q) / (sigma * sigma);
+            }
+            const v3 g_c = (alpha * trans) * gC;
+            v3 g_pn = (alpha * trans) * gN;
+            v3 g_po = mk(0.f, 0.f, 0.f);
+            float g_r = 0.f;
+            float g_ts = 0.f;
+            if (tn_id == n_adj) {
+                g_ts += g_tn;
+                g_tn = 0.f;
+            }
+            if (tf_id == n_adj) {
+                g_ts += g_tf;
+                g_tf = 0.f;
+            }
+            const int64_t b3 = (int64_t)cur * P.S * 3;
+            float g_pre_tn = plane_local_bwd(o, dq, pre_tn, center, pn, radius, (const float*)P.sites + b3,
+                                             (const float*)P.rgb + b3, (const float*)P.height + (int64_t)cur * P.S,
+                                             P.S, pr, g_c, g_ts, g_po, g_pn, g_r, G.sites + b3, G.rgb + b3,
+                                             G.height + (int64_t)cur * P.S);
+            if (tn_id != n_adj) g_tn += g_pre_tn;
+            const float g_ends[2] = {tn_id == n_adj ? g_pre_tn : g_tn, g_tf};
+            const int end_ids[2] = {tn_id == n_adj ? pre_tn_id : tn_id, tf_id};
+            v3 g_center = g_po;
+            for (int i = 0; i < 2; i++) {
+                const float gt = g_ends[i];
+                const int id = end_ids[i];
+                if (gt == 0.0f) continue;
+                if (id == -1) {
+                    // t = (-qb -+ s)/2, qb = 2 oc.d, s = sqrt(qb^2 - 4(|oc|^2 - r^2)), oc = o - c
+                    v3 oc = o - center;
+                    float qb = 2.0f * dot(oc, dq);
+                    float qc = dot(oc, oc) - radius * radius;
+                    float s = sqrtf(qb * qb - 4.0f * qc);
+                    v3 ds = (1.0f / (2.0f * s)) * ((-4.0f * qb) * dq + 8.0f * oc);
+                    float sgn = i == 1 ? 1.0f : -1.0f;
+                    g_center = g_center + gt * (dq + (sgn * 0.5f) * ds);
+                    g_r += gt * (sgn * 2.0f * radius / s);
+                } else if (id >= 0 && id < n_adj) {
+                    const int32_t nb = __ldg(&P.adj[a0 + id]);
+                    const float4 sj = __ldg(&P.spheres[nb]);
+                    const v3 cj = mk(sj.x, sj.y, sj.z), ci = center;
+                    v3 n = cj - ci;
+                    float num = 0.5f * (dot(cj, cj) - sj.w * sj.w - dot(ci, ci) + radius * radius) - dot(o, n);
+                    float inv_den = 1.0f / dot(dq, n);
+                    float t = num * inv_den;
+                    g_center = g_center + (gt * inv_den) * ((o - ci) + t * dq);
+                    g_r += gt * radius * inv_den;
+                    atomic_add3(G.points + 3 * (int64_t)nb, (gt * inv_den) * ((cj - o) - t * dq));
+                    atomicAdd(G.radii + nb, -gt * sj.w * inv_den);
+                }
+            }
+            atomic_add3(G.points + 3 * (int64_t)cur, g_center);
+            atomicAdd(G.radii + cur, g_r);
+            atomic_add3(G.normals + 3 * (int64_t)cur, g_pn);
+            atomicAdd(G.density + cur, g_sigma);
+        }
+        __syncwarp();
     }
 }
 
@@ -734,8 +885,11 @@ extern "C" int pf_trace_backward(const pf_trace_inputs* in, const float* color, 
                  grad_texel_height};
     int64_t tiles = (int64_t)(1 + (in->cam.height - 1) / 8) * (1 + (in->cam.width - 1) / 8);
     int64_t n = tiles * 64;
-    trace_bwd_kernel<<<(unsigned)((n + 127) / 128), 128, 0, st>>>(P, n, color, normal, depth_seg, depth_sigma,
-                                                                  grad_color, grad_log_t, grad_depth, grad_normal, G);
+    constexpr size_t smem = trace_bwd_smem();  // above the 48 KB default: opt in (per device, so every call)
+    cudaFuncSetAttribute(trace_bwd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    trace_bwd_kernel<<<(unsigned)((n + 127) / 128), 128, smem, st>>>(P, n, color, normal, depth_seg, depth_sigma,
+                                                                    grad_color, grad_log_t, grad_depth, grad_normal,
+                                                                    G);
     for (int i = 0; i < 7; i++)
         if (lens[i]) {
             int64_t k = (int64_t)lens[i];

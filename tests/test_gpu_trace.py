@@ -98,10 +98,12 @@ def test_per_ray_start_cells():
     assert torch.equal(a.color, b.color)
 
 
-@pytest.mark.parametrize("seed", [0, 1])
-def test_trace_adjoint_matches_oracle(seed):
+@pytest.mark.parametrize("seed,thr,W,H", [(0, 1e-3, 32, 24), (1, 1e-3, 32, 24), (2, 0.3, 29, 21), (3, 0.6, 37, 19)])
+def test_trace_adjoint_matches_oracle(seed, thr, W, H):
+    """Ragged images (lanes without a pixel in the adjoint's warps) and high
+    transmittance thresholds (rays ending between queued hits)."""
     sc = np_scene(80 + seed, 300, -0.6, 0.6, 0.05, 0.15, height_scale=0.2)
-    cam = np_camera((0.3, 0.2 * seed, 2.2), (0, 0, 0), 32, 24, 55.0)
+    cam = np_camera((0.3, 0.2 * seed, 2.2), (0, 0, 0), W, H, 55.0)
     tp = {k: to_t(v).requires_grad_(True) for k, v in sc.items()}
     adj, off = build_power_adjacency(tp["points"].detach(), tp["radii"].detach())
     pm = power_adjacency_diff(tp["points"].detach(), tp["radii"].detach(), adj, off)
@@ -109,23 +111,23 @@ def test_trace_adjoint_matches_oracle(seed):
     R = RayTracer(Args(), "cuda")
     color, log_t, depth, normal = R.forward(torch_cam(cam), s, tp["points"], tp["radii"], tp["density"],
                                             tp["normals"], tp["texel_sites"], tp["texel_rgb"], tp["texel_height"],
-                                            adj, off, pm, 1e-3)
+                                            adj, off, pm, thr)
     rng = np.random.default_rng(seed)
-    wC = rng.standard_normal((24, 32, 3)).astype(np.float32)
-    wL = rng.standard_normal((24, 32)).astype(np.float32)
-    wD = rng.standard_normal((24, 32)).astype(np.float32)
-    wN = rng.standard_normal((24, 32, 3)).astype(np.float32)
+    wC = rng.standard_normal((H, W, 3)).astype(np.float32)
+    wL = rng.standard_normal((H, W)).astype(np.float32)
+    wD = rng.standard_normal((H, W)).astype(np.float32)
+    wN = rng.standard_normal((H, W, 3)).astype(np.float32)
     loss = ((color * to_t(wC)).sum() + (log_t * to_t(wL)).sum() + (depth * to_t(wD)).sum()
             + (normal * to_t(wN)).sum())
     loss.backward()
     sph, nsig, _ = packed(sc)
     adj_np, off_np, pm_np = adj.cpu().numpy(), off.cpu().numpy(), pm.cpu().numpy().view(np.uint16)
     f = orc.trace_forward(orc_cam(cam), sph, nsig, sc["texel_sites"], sc["texel_rgb"], sc["texel_height"], adj_np,
-                          off_np, pm_np, s, thr=1e-3)
+                          off_np, pm_np, s, thr=thr)
     for k, v in [("color", color), ("log_t", log_t), ("depth", depth), ("normal", normal)]:
         assert max_abs(v.detach().cpu(), f[k]) <= 1e-5, k
     g = orc.trace_backward(orc_cam(cam), sph, nsig, sc["texel_sites"], sc["texel_rgb"], sc["texel_height"], adj_np,
-                           off_np, pm_np, f, wC, wL, wD, wN, s, thr=1e-3)
+                           off_np, pm_np, f, wC, wL, wD, wN, s, thr=thr)
     from tests.helpers import assert_close_rel
     assert_close_rel(tp["points"].grad.cpu().numpy(), g["spheres"][:, :3], 1e-4, "points")
     assert_close_rel(tp["radii"].grad.cpu().numpy(), g["spheres"][:, 3], 1e-4, "radii")
