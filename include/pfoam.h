@@ -322,12 +322,20 @@ PF_API int pf_trace_forward(const pf_trace_inputs *in, float *color, float *log_
  * depth_sigma and the upstream gradients of colour (H,W,3), log
  * transmittance (H,W), depth (H,W) and normal (H,W,3) (any of the four may
  * be NULL); writes (zeroes first) the gradients of every primitive attribute
- * and zeroes non-finite entries.  Attributes must be f32. */
+ * and zeroes non-finite entries.  Attributes must be f32.  The walk is
+ * repeated (transmittance recomputed, nothing kept from the forward); up to
+ * segments_per_ray segments of each ray are recorded in the workspace
+ * (256-byte aligned, pf_trace_backward_workspace_size bytes, about
+ * 48 * segments_per_ray + 60 bytes per pixel) for the gradient launch, and
+ * rays with more are finished by a launch that walks them on from there.
+ * Any segments_per_ray in [0, 65535] gives the same gradients. */
+PF_API int pf_trace_backward_workspace_size(const pf_trace_inputs *in, int32_t segments_per_ray, size_t *bytes);
 PF_API int pf_trace_backward(const pf_trace_inputs *in, const float *color, const float *normal,
                              const int32_t *depth_seg, const float *depth_sigma, const float *grad_color,
                              const float *grad_log_t, const float *grad_depth, const float *grad_normal,
                              float *grad_points, float *grad_radii, float *grad_normals, float *grad_density,
-                             float *grad_texel_sites, float *grad_texel_rgb, float *grad_texel_height, void *stream);
+                             float *grad_texel_sites, float *grad_texel_rgb, float *grad_texel_height,
+                             int32_t segments_per_ray, void *workspace, size_t workspace_bytes, void *stream);
 
 /* Training labels of the ray-proposal network (no counterpart in the
  * reference): the walk of pf_trace_forward (f32 attributes) writing, per

@@ -369,18 +369,272 @@ PF_D float plane_local_bwd(v3 o, v3 d, float tn, v3 po, v3 pn, float radius, con
     return g_tn;
 }
 
-// The adjoint kernel runs each warp's 32 rays in rounds.  Walk: every live
-// lane steps its ray until it holds kTrQueue hit cells (sphere and faces
-// give a non-empty interval) or the ray ends; only the face loop runs here.
-// Texture planes: the warp's queued hits, compacted, are spread over all 32
-// lanes.  Prefix: each lane folds its own hits in walk order into the
-// transmittance and the colour / normal accumulated so far (the exact float
-// sequence of the forward), dropping the hits after the ray's transmittance
-// fell below the threshold.  Gradients: the compacted hits again over all
-// lanes.  Only about one walked cell in five is a hit, so the texture and
-// gradient work, which dominate, run on full warps instead of on the few
-// lanes whose cell is a hit.
-constexpr int kTrQueue = 4;    // queued hits per lane and round
+// A segment of the walk: the cell, the interval its sphere and faces bound
+// before the texture plane (ids as in WalkStep), the transmittance before
+// it, the colour and normal accumulated up to and including it, and its
+// index among the ray's segments.
+struct SegRec {
+    int32_t cell;
+    float tn, tf;
+    uint32_t ids;  // tn_id in the low, tf_id in the high 16 bits (|id| < 2^15)
+    float trans;
+    v3 C, N;
+    int32_t seg;
+};
+
+PF_D uint32_t pack_ids(int tn_id, int tf_id) { return ((uint32_t)tn_id & 0xffffu) | ((uint32_t)tf_id << 16); }
+
+// Per-pixel inputs of the adjoint: the forward's colour / normal / depth
+// segment and the loss gradients (any may be null where the reference's
+// interface allows it).
+struct TraceAdjIn {
+    const float* color;
+    const float* normal;
+    const int32_t* depth_seg;
+    const float* depth_sigma;
+    const float* g_color;
+    const float* g_log_t;
+    const float* g_depth;
+    const float* g_normal;
+};
+
+// Gradients of one segment into every primitive attribute it depends on.
+// `pr` is the texture plane of the segment's cell at the pre-plane t_near.
+PF_D void segment_adjoint(const TraceParams& P, const TraceAdjIn& A, const TraceGrads& G, v3 o, v3 d, int64_t px,
+                          const SegRec& r, const PlaneRes& pr) {
+    const int32_t cur = r.cell;
+    const float4 s4 = __ldg(&P.spheres[cur]);
+    const v3 center = mk(s4.x, s4.y, s4.z);
+    const float radius = s4.w;
+    const float* ns = (const float*)P.nsig + 4 * (int64_t)cur;
+    const v3 pn = mk(__ldg(ns), __ldg(ns + 1), __ldg(ns + 2));
+    const float sigma = __ldg(ns + 3);
+    const int32_t a0 = __ldg(&P.adj_off[cur]);
+    const int n_adj = __ldg(&P.adj_off[cur + 1]) - a0;
+    const int pre_tn_id = (int)(int16_t)(r.ids & 0xffffu);
+    int tn_id = pre_tn_id, tf_id = (int)r.ids >> 16;
+    float tn = r.tn, tf = r.tf;
+    if (pr.dp >= 0.0f && pr.t_surf < tf) tf_id = n_adj;
+    tf = pr.dp >= 0.0f ? fmin_t(pr.t_surf, tf) : tf;
+    if (pr.dp < 0.0f && pr.t_surf > tn) tn_id = n_adj;
+    tn = pr.dp < 0.0f ? fmax_t(pr.t_surf, tn) : tn;
+    const float dt = tf - tn;
+    const float trans = r.trans;
+    const v3 gC = A.g_color ? mk(A.g_color[3 * px], A.g_color[3 * px + 1], A.g_color[3 * px + 2]) : mk(0.f, 0.f, 0.f);
+    const v3 gN =
+        A.g_normal ? mk(A.g_normal[3 * px], A.g_normal[3 * px + 1], A.g_normal[3 * px + 2]) : mk(0.f, 0.f, 0.f);
+    const float gL = A.g_log_t ? A.g_log_t[px] : 0.f;
+    const float gD = A.g_depth ? A.g_depth[px] : 0.f;
+    const int m = A.depth_seg ? A.depth_seg[px] : -1;
+    const float sig_m = A.depth_sigma ? A.depth_sigma[px] : 1.f;
+    const v3 Cf = mk(A.color[3 * px], A.color[3 * px + 1], A.color[3 * px + 2]);
+    const v3 Nf = A.normal ? mk(A.normal[3 * px], A.normal[3 * px + 1], A.normal[3 * px + 2]) : mk(0.f, 0.f, 0.f);
+    const float dlt = -sigma * dt;
+    const float e = expf(dlt);
+    const float alpha = 1.0f - e;
+    const v3 c = pr.rgb;
+    const float trans_next = trans * e;
+    float g_delta = dot(gC, (Cf - r.C) - trans_next * c) + dot(gN, (Nf - r.N) - trans_next * pn) + gL;
+    if (m >= 0 && r.seg < m) g_delta += gD / sig_m;
+    float g_sigma = -dt * g_delta;
+    float g_tf = -sigma * g_delta, g_tn = sigma * g_delta;
+    if (r.seg == m) {
+        g_tn += gD;
+        g_sigma += -gD * logf(trans / P.depth_q) / (sigma * sigma);
+    }
+    const v3 g_c = (alpha * trans) * gC;
+    v3 g_pn = (alpha * trans) * gN;
+    v3 g_po = mk(0.f, 0.f, 0.f);
+    float g_r = 0.f;
+    float g_ts = 0.f;
+    if (tn_id == n_adj) {
+        g_ts += g_tn;
+        g_tn = 0.f;
+    }
+    if (tf_id == n_adj) {
+        g_ts += g_tf;
+        g_tf = 0.f;
+    }
+    const int64_t b3 = (int64_t)cur * P.S * 3;
+    float g_pre_tn = plane_local_bwd(o, d, r.tn, center, pn, radius, (const float*)P.sites + b3,
+                                     (const float*)P.rgb + b3, (const float*)P.height + (int64_t)cur * P.S, P.S, pr,
+                                     g_c, g_ts, g_po, g_pn, g_r, G.sites + b3, G.rgb + b3,
+                                     G.height + (int64_t)cur * P.S);
+    if (tn_id != n_adj) g_tn += g_pre_tn;
+    const float g_ends[2] = {tn_id == n_adj ? g_pre_tn : g_tn, g_tf};
+    const int end_ids[2] = {tn_id == n_adj ? pre_tn_id : tn_id, tf_id};
+    v3 g_center = g_po;
+    for (int i = 0; i < 2; i++) {
+        const float gt = g_ends[i];
+        const int id = end_ids[i];
+        if (gt == 0.0f) continue;
+        if (id == -1) {
+            // t = (-qb -+ s)/2, qb = 2 oc.d, s = sqrt(qb^2 - 4(|oc|^2 - r^2)), oc = o - c
+            v3 oc = o - center;
+            float qb = 2.0f * dot(oc, d);
+            float qc = dot(oc, oc) - radius * radius;
+            float s = sqrtf(qb * qb - 4.0f * qc);
+            v3 ds = (1.0f / (2.0f * s)) * ((-4.0f * qb) * d + 8.0f * oc);
+            float sgn = i == 1 ? 1.0f : -1.0f;
+            g_center = g_center + gt * (d + (sgn * 0.5f) * ds);
+            g_r += gt * (sgn * 2.0f * radius / s);
+        } else if (id >= 0 && id < n_adj) {
+            const int32_t nb = __ldg(&P.adj[a0 + id]);
+            const float4 sj = __ldg(&P.spheres[nb]);
+            const v3 cj = mk(sj.x, sj.y, sj.z), ci = center;
+            v3 n = cj - ci;
+            float num = 0.5f * (dot(cj, cj) - sj.w * sj.w - dot(ci, ci) + radius * radius) - dot(o, n);
+            float inv_den = 1.0f / dot(d, n);
+            float t = num * inv_den;
+            g_center = g_center + (gt * inv_den) * ((o - ci) + t * d);
+            g_r += gt * radius * inv_den;
+            atomic_add3(G.points + 3 * (int64_t)nb, (gt * inv_den) * ((cj - o) - t * d));
+            atomicAdd(G.radii + nb, -gt * sj.w * inv_den);
+        }
+    }
+    atomic_add3(G.points + 3 * (int64_t)cur, g_center);
+    atomicAdd(G.radii + cur, g_r);
+    atomic_add3(G.normals + 3 * (int64_t)cur, g_pn);
+    atomicAdd(G.density + cur, g_sigma);
+}
+
+PF_D PlaneRes cell_plane(const TraceParams& P, v3 o, v3 d, int32_t cell, float t_near) {
+    const float4 s4 = __ldg(&P.spheres[cell]);
+    const float* ns = (const float*)P.nsig + 4 * (int64_t)cell;
+    const int64_t b3 = (int64_t)cell * P.S * 3;
+    return plane_local<float>(o, d, t_near, mk(s4.x, s4.y, s4.z), mk(__ldg(ns), __ldg(ns + 1), __ldg(ns + 2)), s4.w,
+                              (const float*)P.sites + b3, (const float*)P.rgb + b3,
+                              (const float*)P.height + (int64_t)cell * P.S, P.S);
+}
+
+// The adjoint runs in three launches over the rays of the trace (thread
+// index = pixel slot in the 8 x 8 tile order):
+//  1. trace_bwd_walk_kernel repeats the walk of the forward (the same float
+//     sequence for transmittance, colour and normal) and records up to
+//     `kb` segments per ray in the workspace; a ray with more stops there
+//     and leaves its walk state (cell, steps, log T, segment index,
+//     accumulated colour / normal) on an overflow list.
+//  2. trace_bwd_segment_kernel: one thread per recorded segment (grid y =
+//     slot), texture plane recomputed, gradients by atomics.
+//  3. trace_bwd_resume_kernel finishes the overflow rays from their saved
+//     state (empty list: every warp returns at once).
+// Launches 1 and 2 carry no per-ray loop around the gradient work, so the
+// walk runs at the forward's register count and occupancy and the gradient
+// work on full warps (only about one walked cell in five is a segment).
+struct SegWs {
+    int64_t n;       // ray slots
+    int kb;          // recorded segments per ray
+    int32_t* count;  // [n] recorded segments
+    float4* rec;     // [kb][n][3]
+    int32_t* n_over; // overflow rays
+    int32_t* over;   // [n] their slots
+    float4* state;   // [n][3] their walk state
+};
+
+PF_D void store_rec(float4* p, const SegRec& r) {
+    p[0] = make_float4(__int_as_float(r.cell), r.tn, r.tf, __uint_as_float(r.ids));
+    p[1] = make_float4(r.trans, r.C.x, r.C.y, r.C.z);
+    p[2] = make_float4(r.N.x, r.N.y, r.N.z, __int_as_float(r.seg));
+}
+
+PF_D SegRec load_rec(const float4* p) {
+    const float4 a = p[0], b = p[1], c = p[2];
+    SegRec r;
+    r.cell = __float_as_int(a.x);
+    r.tn = a.y;
+    r.tf = a.z;
+    r.ids = __float_as_uint(a.w);
+    r.trans = b.x;
+    r.C = mk(b.y, b.z, b.w);
+    r.N = mk(c.x, c.y, c.z);
+    r.seg = __float_as_int(c.w);
+    return r;
+}
+
+__global__ void __launch_bounds__(128)
+trace_bwd_walk_kernel(TraceParams P, SegWs W) {
+    const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (tid >= W.n) return;
+    int pi, pj;
+    if (!trace_pixel(P.cam, tid, pi, pj)) {
+        W.count[tid] = 0;
+        return;
+    }
+    const int64_t px = (int64_t)pi * P.cam.W + pj;
+    const v3 o = P.cam.eye;
+    const v3 d = ray_dir(P.cam, pi, pj);
+    v3 Cacc = mk(0.f, 0.f, 0.f), Nacc = mk(0.f, 0.f, 0.f);
+    float log_t = 0.f;
+    int32_t prim = P.start_cells ? P.start_cells[px] : P.start_idx;
+    int steps = 0, seg = 0, nrec = 0;
+    for (;;) {
+        const float trans = expf(log_t);
+        if (trans < P.thr || prim == kNoCell || steps >= P.max_steps || prim < 0 || prim >= P.N) break;
+        if (nrec == W.kb) {  // the rest of this ray goes to the resume launch
+            const int32_t k = atomicAdd(W.n_over, 1);
+            W.over[k] = (int32_t)tid;
+            W.state[3 * (int64_t)k] = make_float4(__int_as_float(prim), __int_as_float(steps), log_t,
+                                                   __int_as_float(seg));
+            W.state[3 * (int64_t)k + 1] = make_float4(Cacc.x, Cacc.y, Cacc.z, Nacc.x);
+            W.state[3 * (int64_t)k + 2] = make_float4(Nacc.y, Nacc.z, 0.f, 0.f);
+            break;
+        }
+        steps++;
+        const WalkStep ws = walk_step(P, o, d, prim);
+        const int32_t cur = prim;
+        prim = ws.next;
+        if (!ws.hit) continue;
+        const PlaneRes pr = cell_plane(P, o, d, cur, ws.tn);
+        const float tf = pr.dp >= 0.0f ? fmin_t(pr.t_surf, ws.tf) : ws.tf;
+        const float tn = pr.dp < 0.0f ? fmax_t(pr.t_surf, ws.tn) : ws.tn;
+        const float dt = tf - tn;
+        if (!(dt > 0.0f)) continue;
+        const float* ns = (const float*)P.nsig + 4 * (int64_t)cur;
+        const v3 pn = mk(__ldg(ns), __ldg(ns + 1), __ldg(ns + 2));
+        const float dlt = -ws.sigma * dt;
+        const float alpha = 1.0f - expf(dlt);
+        Cacc = Cacc + trans * (alpha * pr.rgb);
+        Nacc = Nacc + (alpha * trans) * pn;
+        SegRec r;
+        r.cell = cur;
+        r.tn = ws.tn;
+        r.tf = ws.tf;
+        r.ids = pack_ids(ws.tn_id, ws.tf_id);
+        r.trans = trans;
+        r.C = Cacc;
+        r.N = Nacc;
+        r.seg = seg;
+        store_rec(W.rec + 3 * ((int64_t)nrec * W.n + tid), r);
+        nrec++;
+        log_t += dlt;
+        seg++;
+    }
+    W.count[tid] = nrec;
+}
+
+__global__ void __launch_bounds__(128)
+trace_bwd_segment_kernel(TraceParams P, SegWs W, TraceAdjIn A, TraceGrads G) {
+    const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int k = blockIdx.y;
+    if (tid >= W.n || k >= W.count[tid]) return;
+    int pi, pj;
+    trace_pixel(P.cam, tid, pi, pj);
+    const int64_t px = (int64_t)pi * P.cam.W + pj;
+    const v3 o = P.cam.eye;
+    const v3 d = ray_dir(P.cam, pi, pj);
+    const SegRec r = load_rec(W.rec + 3 * ((int64_t)k * W.n + tid));
+    segment_adjoint(P, A, G, o, d, px, r, cell_plane(P, o, d, r.cell, r.tn));
+}
+
+// Resume launch: each warp takes 32 overflow rays and runs them in rounds.
+// Walk: every live lane steps its ray until it holds kTrQueue hit cells
+// (sphere and faces give a non-empty interval) or the ray ends.  Texture
+// planes: the warp's queued hits, compacted, over all 32 lanes.  Prefix:
+// each lane folds its own hits in walk order into the transmittance and
+// the accumulated colour / normal, dropping hits after the transmittance
+// fell below the threshold.  Gradients: the compacted segments over all
+// lanes.
+constexpr int kTrQueue = 3;    // queued hits per lane and round
 constexpr int kTrItem = 23;    // words per queued hit (odd: conflict-free strides)
 constexpr int kTrWarps = 4;    // warps per 128-thread block
 // queued hit words
@@ -424,23 +678,37 @@ PF_D int warp_incl_scan(int v, int lane) {
     return v;
 }
 
-constexpr size_t trace_bwd_smem() {
+constexpr size_t trace_resume_smem() {
     return sizeof(float) * kTrWarps * 32 * (kTrQueue * kTrItem + 4) + sizeof(int) * kTrWarps * 32 * kTrQueue;
 }
 
 __global__ void __launch_bounds__(128)
-trace_bwd_kernel(TraceParams P, int64_t nthreads, const float* __restrict__ color, const float* __restrict__ normal,
-                 const int32_t* __restrict__ depth_seg, const float* __restrict__ depth_sigma,
-                 const float* __restrict__ g_color, const float* __restrict__ g_log_t,
-                 const float* __restrict__ g_depth, const float* __restrict__ g_normal, TraceGrads G) {
+trace_bwd_resume_kernel(TraceParams P, SegWs W, TraceAdjIn A, TraceGrads G) {
     extern __shared__ float tr_smem[];
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int64_t first = ((int64_t)blockIdx.x * kTrWarps + w) * 32;  // warp-uniform
+    const int n_over = *W.n_over;
+    if (first >= n_over) return;
     float* Q = tr_smem + (size_t)w * 32 * kTrQueue * kTrItem;                      // queued hits
     float* R = tr_smem + (size_t)kTrWarps * 32 * kTrQueue * kTrItem + w * 32 * 4;   // per lane: d, px
     int* I = (int*)(tr_smem + (size_t)kTrWarps * 32 * (kTrQueue * kTrItem + 4)) + w * 32 * kTrQueue;
-    const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t pos = first + lane;
+    bool alive = pos < n_over;
     int pi = 0, pj = 0;
-    bool alive = tid < nthreads && trace_pixel(P.cam, tid, pi, pj);
+    v3 Cacc = mk(0.f, 0.f, 0.f), Nacc = mk(0.f, 0.f, 0.f);
+    float log_t = 0.f;
+    int32_t prim = kNoCell;
+    int steps = 0, seg = 0;
+    if (alive) {
+        trace_pixel(P.cam, W.over[pos], pi, pj);
+        const float4 a = W.state[3 * pos], b = W.state[3 * pos + 1], c = W.state[3 * pos + 2];
+        prim = __float_as_int(a.x);
+        steps = __float_as_int(a.y);
+        log_t = a.z;
+        seg = __float_as_int(a.w);
+        Cacc = mk(b.x, b.y, b.z);
+        Nacc = mk(b.w, c.x, c.y);
+    }
     const int64_t px = (int64_t)pi * P.cam.W + pj;
     const v3 o = P.cam.eye;
     const v3 d = ray_dir(P.cam, pi, pj);
@@ -448,10 +716,6 @@ trace_bwd_kernel(TraceParams P, int64_t nthreads, const float* __restrict__ colo
     R[lane * 4 + 1] = d.y;
     R[lane * 4 + 2] = d.z;
     R[lane * 4 + 3] = __int_as_float((int)px);
-    v3 Cacc = mk(0.f, 0.f, 0.f), Nacc = mk(0.f, 0.f, 0.f);
-    float log_t = 0.f;
-    int32_t prim = alive ? (P.start_cells ? P.start_cells[px] : P.start_idx) : kNoCell;
-    int steps = 0, seg = 0;
     for (;;) {
         // walk until kTrQueue hits are queued or the ray ends
         int cnt = 0;
@@ -467,7 +731,7 @@ trace_bwd_kernel(TraceParams P, int64_t nthreads, const float* __restrict__ colo
                 q[kQCell] = __int_as_float(prim);
                 q[kQTn] = ws.tn;
                 q[kQTf] = ws.tf;
-                q[kQIds] = __uint_as_float(((unsigned)ws.tn_id & 0xffffu) | ((unsigned)ws.tf_id << 16));  // |id| < 2^15
+                q[kQIds] = __uint_as_float(pack_ids(ws.tn_id, ws.tf_id));
                 q[kQSigma] = ws.sigma;
                 cnt++;
             }
@@ -483,15 +747,7 @@ trace_bwd_kernel(TraceParams P, int64_t nthreads, const float* __restrict__ colo
             const int slot = I[j];
             float* q = Q + slot * kTrItem;
             const float* rr = R + (slot / kTrQueue) * 4;
-            const v3 dq = mk(rr[0], rr[1], rr[2]);
-            const int32_t cell = __float_as_int(q[kQCell]);
-            const float4 s4 = __ldg(&P.spheres[cell]);
-            const float* ns = (const float*)P.nsig + 4 * (int64_t)cell;
-            const v3 pn = mk(__ldg(ns), __ldg(ns + 1), __ldg(ns + 2));
-            const int64_t b3 = (int64_t)cell * P.S * 3;
-            q_store_pr(q, plane_local<float>(o, dq, q[kQTn], mk(s4.x, s4.y, s4.z), pn, s4.w,
-                                             (const float*)P.sites + b3, (const float*)P.rgb + b3,
-                                             (const float*)P.height + (int64_t)cell * P.S, P.S));
+            q_store_pr(q, cell_plane(P, o, mk(rr[0], rr[1], rr[2]), __float_as_int(q[kQCell]), q[kQTn]));
         }
         __syncwarp();
         // transmittance and accumulated colour / normal, per ray in walk order
@@ -514,8 +770,7 @@ trace_bwd_kernel(TraceParams P, int64_t nthreads, const float* __restrict__ colo
             const int32_t cell = __float_as_int(q[kQCell]);
             const float* ns = (const float*)P.nsig + 4 * (int64_t)cell;
             const v3 pn = mk(__ldg(ns), __ldg(ns + 1), __ldg(ns + 2));
-            const float sigma = q[kQSigma];
-            const float dlt = -sigma * dt;
+            const float dlt = -q[kQSigma] * dt;
             const float alpha = 1.0f - expf(dlt);
             Cacc = Cacc + trans * (alpha * mk(q[kQPr + 7], q[kQPr + 8], q[kQPr + 9]));
             Nacc = Nacc + (alpha * trans) * pn;
@@ -535,110 +790,18 @@ trace_bwd_kernel(TraceParams P, int64_t nthreads, const float* __restrict__ colo
         for (int j = lane; j < total; j += 32) {
             const int slot = I[j];
             const float* q = Q + slot * kTrItem;
-            const int sg_idx = __float_as_int(q[kQSeg]);
-            if (sg_idx < 0) continue;
+            SegRec r;
+            r.seg = __float_as_int(q[kQSeg]);
+            if (r.seg < 0) continue;
             const float* rr = R + (slot / kTrQueue) * 4;
-            const v3 dq = mk(rr[0], rr[1], rr[2]);
-            const int64_t qpx = (int64_t)__float_as_int(rr[3]);
-            const int32_t cur = __float_as_int(q[kQCell]);
-            const PlaneRes pr = q_load_pr(q);
-            const float4 s4 = __ldg(&P.spheres[cur]);
-            const v3 center = mk(s4.x, s4.y, s4.z);
-            const float radius = s4.w;
-            const float* ns = (const float*)P.nsig + 4 * (int64_t)cur;
-            const v3 pn = mk(__ldg(ns), __ldg(ns + 1), __ldg(ns + 2));
-            const int32_t a0 = __ldg(&P.adj_off[cur]);
-            const int n_adj = __ldg(&P.adj_off[cur + 1]) - a0;
-            const int ids = __float_as_int(q[kQIds]);
-            const int pre_tn_id = (int)(int16_t)(ids & 0xffff);
-            int tn_id = pre_tn_id, tf_id = ids >> 16;
-            const float pre_tn = q[kQTn];
-            float tn = pre_tn, tf = q[kQTf];
-            if (pr.dp >= 0.0f && pr.t_surf < tf) tf_id = n_adj;
-            tf = pr.dp >= 0.0f ? fmin_t(pr.t_surf, tf) : tf;
-            if (pr.dp < 0.0f && pr.t_surf > tn) tn_id = n_adj;
-            tn = pr.dp < 0.0f ? fmax_t(pr.t_surf, tn) : tn;
-            const float sigma = q[kQSigma], dt = tf - tn;
-            const float trans = q[kQTrans];
-            const v3 Cq = mk(q[kQC], q[kQC + 1], q[kQC + 2]);
-            const v3 Nq = mk(q[kQN], q[kQN + 1], q[kQN + 2]);
-            const v3 gC = g_color ? mk(g_color[3 * qpx], g_color[3 * qpx + 1], g_color[3 * qpx + 2])
-                                  : mk(0.f, 0.f, 0.f);
-            const v3 gN = g_normal ? mk(g_normal[3 * qpx], g_normal[3 * qpx + 1], g_normal[3 * qpx + 2])
-                                   : mk(0.f, 0.f, 0.f);
-            const float gL = g_log_t ? g_log_t[qpx] : 0.f;
-            const float gD = g_depth ? g_depth[qpx] : 0.f;
-            const int m = depth_seg ? depth_seg[qpx] : -1;
-            const float sig_m = depth_sigma ? depth_sigma[qpx] : 1.f;
-            const v3 Cf = mk(color[3 * qpx], color[3 * qpx + 1], color[3 * qpx + 2]);
-            const v3 Nf = normal ? mk(normal[3 * qpx], normal[3 * qpx + 1], normal[3 * qpx + 2]) : mk(0.f, 0.f, 0.f);
-            const float dlt = -sigma * dt;
-            const float e = expf(dlt);
-            const float alpha = 1.0f - e;
-            const v3 c = pr.rgb;
-            const float trans_next = trans * e;
-            float g_delta = dot(gC, (Cf - Cq) - trans_next * c) + dot(gN, (Nf - Nq) - trans_next * pn) + gL;
-            if (m >= 0 && sg_idx < m) g_delta += gD / sig_m;
-            float g_sigma = -dt * g_delta;
-            float g_tf = -sigma * g_delta, g_tn = sigma * g_delta;
-            if (sg_idx == m) {
-                g_tn += gD;
-                g_sigma += -gD * logf(trans / P.depth_q) / (sigma * sigma);
-            }
-            const v3 g_c = (alpha * trans) * gC;
-            v3 g_pn = (alpha * trans) * gN;
-            v3 g_po = mk(0.f, 0.f, 0.f);
-            float g_r = 0.f;
-            float g_ts = 0.f;
-            if (tn_id == n_adj) {
-                g_ts += g_tn;
-                g_tn = 0.f;
-            }
-            if (tf_id == n_adj) {
-                g_ts += g_tf;
-                g_tf = 0.f;
-            }
-            const int64_t b3 = (int64_t)cur * P.S * 3;
-            float g_pre_tn = plane_local_bwd(o, dq, pre_tn, center, pn, radius, (const float*)P.sites + b3,
-                                             (const float*)P.rgb + b3, (const float*)P.height + (int64_t)cur * P.S,
-                                             P.S, pr, g_c, g_ts, g_po, g_pn, g_r, G.sites + b3, G.rgb + b3,
-                                             G.height + (int64_t)cur * P.S);
-            if (tn_id != n_adj) g_tn += g_pre_tn;
-            const float g_ends[2] = {tn_id == n_adj ? g_pre_tn : g_tn, g_tf};
-            const int end_ids[2] = {tn_id == n_adj ? pre_tn_id : tn_id, tf_id};
-            v3 g_center = g_po;
-            for (int i = 0; i < 2; i++) {
-                const float gt = g_ends[i];
-                const int id = end_ids[i];
-                if (gt == 0.0f) continue;
-                if (id == -1) {
-                    // t = (-qb -+ s)/2, qb = 2 oc.d, s = sqrt(qb^2 - 4(|oc|^2 - r^2)), oc = o - c
-                    v3 oc = o - center;
-                    float qb = 2.0f * dot(oc, dq);
-                    float qc = dot(oc, oc) - radius * radius;
-                    float s = sqrtf(qb * qb - 4.0f * qc);
-                    v3 ds = (1.0f / (2.0f * s)) * ((-4.0f * qb) * dq + 8.0f * oc);
-                    float sgn = i == 1 ? 1.0f : -1.0f;
-                    g_center = g_center + gt * (dq + (sgn * 0.5f) * ds);
-                    g_r += gt * (sgn * 2.0f * radius / s);
-                } else if (id >= 0 && id < n_adj) {
-                    const int32_t nb = __ldg(&P.adj[a0 + id]);
-                    const float4 sj = __ldg(&P.spheres[nb]);
-                    const v3 cj = mk(sj.x, sj.y, sj.z), ci = center;
-                    v3 n = cj - ci;
-                    float num = 0.5f * (dot(cj, cj) - sj.w * sj.w - dot(ci, ci) + radius * radius) - dot(o, n);
-                    float inv_den = 1.0f / dot(dq, n);
-                    float t = num * inv_den;
-                    g_center = g_center + (gt * inv_den) * ((o - ci) + t * dq);
-                    g_r += gt * radius * inv_den;
-                    atomic_add3(G.points + 3 * (int64_t)nb, (gt * inv_den) * ((cj - o) - t * dq));
-                    atomicAdd(G.radii + nb, -gt * sj.w * inv_den);
-                }
-            }
-            atomic_add3(G.points + 3 * (int64_t)cur, g_center);
-            atomicAdd(G.radii + cur, g_r);
-            atomic_add3(G.normals + 3 * (int64_t)cur, g_pn);
-            atomicAdd(G.density + cur, g_sigma);
+            r.cell = __float_as_int(q[kQCell]);
+            r.tn = q[kQTn];
+            r.tf = q[kQTf];
+            r.ids = __float_as_uint(q[kQIds]);
+            r.trans = q[kQTrans];
+            r.C = mk(q[kQC], q[kQC + 1], q[kQC + 2]);
+            r.N = mk(q[kQN], q[kQN + 1], q[kQN + 2]);
+            segment_adjoint(P, A, G, o, mk(rr[0], rr[1], rr[2]), (int64_t)__float_as_int(rr[3]), r, q_load_pr(q));
         }
         __syncwarp();
     }
@@ -860,12 +1023,38 @@ static bool fill_trace(const pf_trace_inputs* in, TraceParams& P, const char** w
     return true;
 }
 
+// Workspace of the adjoint for `kb` recorded segments per ray: counts,
+// records (48 B per segment slot), overflow list and states.
+static size_t seg_ws_layout(int64_t n, int kb, size_t off[5]) {
+    auto up = [](size_t x) { return (x + 255) & ~(size_t)255; };
+    size_t o = 0;
+    off[0] = o;  o = up(o + sizeof(int32_t) * n);                 // count
+    off[1] = o;  o = up(o + sizeof(float4) * 3 * n * (size_t)kb); // records
+    off[2] = o;  o = up(o + sizeof(int32_t));                     // n_over
+    off[3] = o;  o = up(o + sizeof(int32_t) * n);                 // over
+    off[4] = o;  o = up(o + sizeof(float4) * 3 * n);              // state
+    return o;
+}
+
+static int64_t trace_slots(const pf_trace_inputs* in) {
+    return (int64_t)(1 + (in->cam.height - 1) / 8) * (1 + (in->cam.width - 1) / 8) * 64;
+}
+
+extern "C" int pf_trace_backward_workspace_size(const pf_trace_inputs* in, int32_t segments_per_ray, size_t* bytes) {
+    if (!in || !bytes || segments_per_ray < 0 || segments_per_ray > 65535 || in->cam.width <= 0 ||
+        in->cam.height <= 0)
+        return pf_fail(PF_ERR_ARGS, "pf_trace_backward_workspace_size: bad arguments");
+    size_t off[5];
+    *bytes = seg_ws_layout(trace_slots(in), segments_per_ray, off);
+    return PF_OK;
+}
+
 extern "C" int pf_trace_backward(const pf_trace_inputs* in, const float* color, const float* normal,
                                  const int32_t* depth_seg, const float* depth_sigma, const float* grad_color,
                                  const float* grad_log_t, const float* grad_depth, const float* grad_normal,
                                  float* grad_points, float* grad_radii, float* grad_normals, float* grad_density,
                                  float* grad_texel_sites, float* grad_texel_rgb, float* grad_texel_height,
-                                 void* stream) {
+                                 int32_t segments_per_ray, void* workspace, size_t workspace_bytes, void* stream) {
     TraceParams P;
     const char* why = "";
     if (!fill_trace(in, P, &why)) return pf_fail(PF_ERR_ARGS, why);
@@ -874,6 +1063,10 @@ extern "C" int pf_trace_backward(const pf_trace_inputs* in, const float* color, 
         !grad_texel_rgb || !grad_texel_height || (grad_depth && (!depth_seg || !depth_sigma)) ||
         (grad_normal && !normal))
         return pf_fail(PF_ERR_ARGS, "pf_trace_backward: missing argument");
+    size_t need = 0;
+    if (pf_trace_backward_workspace_size(in, segments_per_ray, &need) != PF_OK) return PF_ERR_ARGS;
+    if (!workspace || workspace_bytes < need || ((uintptr_t)workspace & 255))
+        return pf_fail(PF_ERR_ARGS, "pf_trace_backward: workspace missing, too small or not 256-byte aligned");
     cudaStream_t st = (cudaStream_t)stream;
     const size_t N = (size_t)P.N, S = (size_t)P.S;
     float* outs[7] = {grad_points, grad_radii, grad_normals, grad_density, grad_texel_sites, grad_texel_rgb,
@@ -883,13 +1076,19 @@ extern "C" int pf_trace_backward(const pf_trace_inputs* in, const float* color, 
         if (lens[i]) cudaMemsetAsync(outs[i], 0, sizeof(float) * lens[i], st);
     TraceGrads G{grad_points, grad_radii, grad_normals, grad_density, grad_texel_sites, grad_texel_rgb,
                  grad_texel_height};
-    int64_t tiles = (int64_t)(1 + (in->cam.height - 1) / 8) * (1 + (in->cam.width - 1) / 8);
-    int64_t n = tiles * 64;
-    constexpr size_t smem = trace_bwd_smem();  // above the 48 KB default: opt in (per device, so every call)
-    cudaFuncSetAttribute(trace_bwd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    trace_bwd_kernel<<<(unsigned)((n + 127) / 128), 128, smem, st>>>(P, n, color, normal, depth_seg, depth_sigma,
-                                                                    grad_color, grad_log_t, grad_depth, grad_normal,
-                                                                    G);
+    TraceAdjIn A{color, normal, depth_seg, depth_sigma, grad_color, grad_log_t, grad_depth, grad_normal};
+    const int64_t n = trace_slots(in);
+    size_t off[5];
+    seg_ws_layout(n, segments_per_ray, off);
+    char* ws = (char*)workspace;
+    SegWs W{n, segments_per_ray, (int32_t*)(ws + off[0]), (float4*)(ws + off[1]), (int32_t*)(ws + off[2]),
+            (int32_t*)(ws + off[3]), (float4*)(ws + off[4])};
+    cudaMemsetAsync(W.n_over, 0, sizeof(int32_t), st);
+    const unsigned blocks = (unsigned)((n + 127) / 128);
+    trace_bwd_walk_kernel<<<blocks, 128, 0, st>>>(P, W);
+    if (segments_per_ray > 0) trace_bwd_segment_kernel<<<dim3(blocks, segments_per_ray), 128, 0, st>>>(P, W, A, G);
+    static_assert(trace_resume_smem() <= 48 * 1024, "resume queue above the default shared-memory limit");
+    trace_bwd_resume_kernel<<<blocks, 128, trace_resume_smem(), st>>>(P, W, A, G);
     for (int i = 0; i < 7; i++)
         if (lens[i]) {
             int64_t k = (int64_t)lens[i];

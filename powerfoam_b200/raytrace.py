@@ -15,6 +15,8 @@ import torch
 from . import _lib
 
 DEFAULT_MAX_STEPS = 1 << 16
+# bound on the adjoint's segment records when segments_per_ray is left to the tracer
+RECORD_BYTES = 4 << 30
 
 
 @dataclass
@@ -59,6 +61,11 @@ class RayTracer:
             raise ValueError(f"Unsupported attribute dtype: {attr_dtype}")
         self.attr_dtype = attr_dtype
         self.num_texel_sites = args.num_texel_sites
+        # segments per ray the adjoint records for its gradient launch (rays
+        # with more are walked on by its slower resume launch; any value
+        # gives the same gradients), 48 bytes per pixel each; None: 96,
+        # lowered so the records stay within RECORD_BYTES
+        self.segments_per_ray = None
         _lib.load()
 
     def _inputs(self, camera, start, spheres, nsig, sites, rgb, height, adjacency, adjacency_offsets,
@@ -168,9 +175,19 @@ class RayTracer:
         out = [torch.empty(s, dtype=torch.float32, device=dev) for s in ((n, 3), (n,), (n, 3), (n,), (n, S, 3),
                                                                          (n, S, 3), (n, S))]
         c = lambda t: None if t is None else t.float().contiguous()
+        kb = self.segments_per_ray
+        if kb is None:
+            slots = ((int(ctx.camera.height) + 7) // 8) * ((int(ctx.camera.width) + 7) // 8) * 64
+            kb = max(1, min(96, RECORD_BYTES // (48 * slots)))
+        kb = int(kb)
+        nbytes = _lib.ctypes.c_size_t(0)
+        _lib.call("pf_trace_backward_workspace_size", _lib.ctypes.byref(inp), kb, _lib.ctypes.byref(nbytes))
+        ws = torch.empty(nbytes.value + 256, dtype=torch.uint8, device=dev)
+        ws_ptr = (ws.data_ptr() + 255) & ~255
         _lib.call("pf_trace_backward", _lib.ctypes.byref(inp), _lib.ptr(color), _lib.ptr(normal),
                   _lib.ptr(depth_seg), _lib.ptr(depth_sigma), _lib.ptr(c(g_color)), _lib.ptr(c(g_log_t)),
-                  _lib.ptr(c(g_depth)), _lib.ptr(c(g_normal)), *[_lib.ptr(t) for t in out], _lib.stream_ptr())
+                  _lib.ptr(c(g_depth)), _lib.ptr(c(g_normal)), *[_lib.ptr(t) for t in out], kb, ws_ptr,
+                  nbytes.value, _lib.stream_ptr())
         del ctx.tracer, ctx.camera, ctx.start
         g_pts, g_rad, g_nrm, g_den, g_sites, g_rgb, g_h = out
         return (None, None, None, g_pts, g_rad, g_den, g_nrm, g_sites, g_rgb, g_h, None, None, None, None, None,

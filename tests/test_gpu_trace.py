@@ -102,6 +102,18 @@ def test_per_ray_start_cells():
 def test_trace_adjoint_matches_oracle(seed, thr, W, H):
     """Ragged images (lanes without a pixel in the adjoint's warps) and high
     transmittance thresholds (rays ending between queued hits)."""
+    _adjoint_case(seed, thr, W, H, 32)
+
+
+@pytest.mark.parametrize("kb", [0, 1, 3])
+@pytest.mark.parametrize("seed,thr", [(0, 1e-3), (2, 0.3)])
+def test_trace_adjoint_overflow(seed, thr, kb):
+    """Few recorded segments per ray: most rays overflow and are finished by
+    the resume launch from their saved walk state (kb = 0: all of them)."""
+    _adjoint_case(seed, thr, 29, 21, kb)
+
+
+def _adjoint_case(seed, thr, W, H, kb):
     sc = np_scene(80 + seed, 300, -0.6, 0.6, 0.05, 0.15, height_scale=0.2)
     cam = np_camera((0.3, 0.2 * seed, 2.2), (0, 0, 0), W, H, 55.0)
     tp = {k: to_t(v).requires_grad_(True) for k, v in sc.items()}
@@ -109,6 +121,7 @@ def test_trace_adjoint_matches_oracle(seed, thr, W, H):
     pm = power_adjacency_diff(tp["points"].detach(), tp["radii"].detach(), adj, off)
     s = start_cell(tp["points"].detach(), tp["radii"].detach(), torch.from_numpy(cam["eye"]))
     R = RayTracer(Args(), "cuda")
+    R.segments_per_ray = kb
     color, log_t, depth, normal = R.forward(torch_cam(cam), s, tp["points"], tp["radii"], tp["density"],
                                             tp["normals"], tp["texel_sites"], tp["texel_rgb"], tp["texel_height"],
                                             adj, off, pm, thr)
