@@ -291,6 +291,7 @@ struct TraceGrads {
     float* sites;
     float* rgb;
     float* height;
+    bool vec4;  // S % 4 == 0 and the texel gradient arrays 16-byte aligned: float4 atomics
 };
 
 PF_D void atomic_add3(float* g, v3 v) {
@@ -353,6 +354,125 @@ PF_D float plane_local_bwd(v3 o, v3 d, float tn, v3 po, v3 pn, float radius, con
             g__pt = g__pt + g_wi * dwdpt;
             atomic_add3(gs + 3 * i, (-g_wi) * dwdpt);
             g_inv_r2 += g_wi * wi * (-kTemp * q2);
+        }
+        float g__tq = dot(g__pt, d);
+        if (g__tq != 0.0f) {
+            if (pr._dp >= 0.0f || tn > pr._t_surf) {
+                g_tn += g__tq;
+            } else {
+                float k = g__tq / pr._dp;
+                g_po = g_po + k * pn;
+                g_pn = g_pn + k * ((po - o) - pr._t_surf * d);
+            }
+        }
+    }
+    g_radius += g_inv_r2 * (-2.0f / (radius * radius * radius));
+    return g_tn;
+}
+
+PF_D void red4(float* p, const float* v) { atomicAdd((float4*)p, make_float4(v[0], v[1], v[2], v[3])); }
+
+// plane_local_bwd for S a multiple of 4 with 16-byte aligned gradient rows:
+// the texel gradients leave as float4 atomics, four sites at a time, and a
+// site's colour and height terms are summed before its atomic (the colour
+// terms are recomputed when the height term is live, i.e. when the plane
+// bounds the segment or holds the colour query point).  Every other value
+// is computed in plane_local_bwd's order.
+PF_D float plane_local_bwd4(v3 o, v3 d, float tn, v3 po, v3 pn, float radius, const float* sites, const float* rgbs,
+                            const float* heights, int S, const PlaneRes& pr, v3 g_rgb, float g_tsurf, v3& g_po,
+                            v3& g_pn, float& g_radius, float* gs, float* gr, float* gh) {
+    const float inv_r2 = 1.0f / (radius * radius);
+    float g_inv_r2 = 0.f, g_tn = 0.f;
+    const float tq = pr.dp >= 0.0f ? tn : fmax_t(tn, pr.t_surf);
+    const v3 pt = o + tq * d;
+    const float inv_V = 1.0f / pr.wsum;
+    const bool v_open = pr.wsum > 1e-20f;
+    const bool on_plane = !(pr.dp >= 0.0f || tn > pr.t_surf);
+    const bool height_live = g_tsurf != 0.0f || on_plane;
+    v3 g_pt = mk(0.f, 0.f, 0.f);
+    for (int g = 0; g < S; g += 4) {
+        float rg[12], sg[12];
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            const int i = g + u;
+            v3 s = mk(sites[3 * i], sites[3 * i + 1], sites[3 * i + 2]);
+            v3 df = pt - s;
+            float q2 = dot(df, df);
+            float vi = expf(-kTemp * q2 * inv_r2);
+            v3 ci = mk(rgbs[3 * i], rgbs[3 * i + 1], rgbs[3 * i + 2]);
+            const v3 a = (vi * inv_V) * g_rgb;
+            rg[3 * u] = a.x;
+            rg[3 * u + 1] = a.y;
+            rg[3 * u + 2] = a.z;
+            float g_vi = (v_open ? dot(ci - pr.rgb, g_rgb) : dot(ci, g_rgb)) * inv_V;
+            v3 dvdpt = (vi * (-2.0f * kTemp * inv_r2)) * df;
+            g_pt = g_pt + g_vi * dvdpt;
+            const v3 b = (-g_vi) * dvdpt;
+            sg[3 * u] = b.x;
+            sg[3 * u + 1] = b.y;
+            sg[3 * u + 2] = b.z;
+            g_inv_r2 += g_vi * vi * (-kTemp * q2);
+        }
+        red4(gr + 3 * g, rg);
+        red4(gr + 3 * g + 4, rg + 4);
+        red4(gr + 3 * g + 8, rg + 8);
+        if (!height_live) {
+            red4(gs + 3 * g, sg);
+            red4(gs + 3 * g + 4, sg + 4);
+            red4(gs + 3 * g + 8, sg + 8);
+        }
+    }
+    float g_tq = dot(g_pt, d);
+    float g_ts = g_tsurf;
+    if (!on_plane) g_tn += g_tq;
+    else g_ts += g_tq;
+    float g_height = 0.f;
+    if (g_ts != 0.0f) {
+        float k = g_ts / pr.dp;
+        g_po = g_po + k * pn;
+        g_pn = g_pn + k * ((po - o) - pr.t_surf * d);
+        g_height = k;
+    }
+    if (height_live) {
+        const float _tq = pr._dp >= 0.0f ? tn : fmax_t(tn, pr._t_surf);
+        const v3 _pt = o + _tq * d;
+        const float inv_W = 1.0f / pr._wsum;
+        const bool w_open = pr._wsum > 1e-20f;
+        const bool h_on = g_height != 0.0f;
+        v3 g__pt = mk(0.f, 0.f, 0.f);
+        for (int g = 0; g < S; g += 4) {
+            float sg[12], hg[4];
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                const int i = g + u;
+                v3 s = mk(sites[3 * i], sites[3 * i + 1], sites[3 * i + 2]);
+                v3 df = pt - s;
+                float q2 = dot(df, df);
+                float vi = expf(-kTemp * q2 * inv_r2);
+                v3 ci = mk(rgbs[3 * i], rgbs[3 * i + 1], rgbs[3 * i + 2]);
+                float g_vi = (v_open ? dot(ci - pr.rgb, g_rgb) : dot(ci, g_rgb)) * inv_V;
+                v3 b = (-g_vi) * ((vi * (-2.0f * kTemp * inv_r2)) * df);
+                hg[u] = 0.f;
+                if (h_on) {
+                    v3 dfw = _pt - s;
+                    float q2w = dot(dfw, dfw);
+                    float wi = expf(-kTemp * q2w * inv_r2);
+                    float hi = heights[i];
+                    hg[u] = wi * inv_W * g_height;
+                    float g_wi = (w_open ? (hi - pr.height) : hi) * inv_W * g_height;
+                    v3 dwdpt = (wi * (-2.0f * kTemp * inv_r2)) * dfw;
+                    g__pt = g__pt + g_wi * dwdpt;
+                    b = b + (-g_wi) * dwdpt;
+                    g_inv_r2 += g_wi * wi * (-kTemp * q2w);
+                }
+                sg[3 * u] = b.x;
+                sg[3 * u + 1] = b.y;
+                sg[3 * u + 2] = b.z;
+            }
+            red4(gs + 3 * g, sg);
+            red4(gs + 3 * g + 4, sg + 4);
+            red4(gs + 3 * g + 8, sg + 8);
+            if (h_on) red4(gh + g, hg);
         }
         float g__tq = dot(g__pt, d);
         if (g__tq != 0.0f) {
@@ -456,10 +576,14 @@ PF_D void segment_adjoint(const TraceParams& P, const TraceAdjIn& A, const Trace
         g_tf = 0.f;
     }
     const int64_t b3 = (int64_t)cur * P.S * 3;
-    float g_pre_tn = plane_local_bwd(o, d, r.tn, center, pn, radius, (const float*)P.sites + b3,
-                                     (const float*)P.rgb + b3, (const float*)P.height + (int64_t)cur * P.S, P.S, pr,
-                                     g_c, g_ts, g_po, g_pn, g_r, G.sites + b3, G.rgb + b3,
-                                     G.height + (int64_t)cur * P.S);
+    const float* ts = (const float*)P.sites + b3;
+    const float* tr = (const float*)P.rgb + b3;
+    const float* th = (const float*)P.height + (int64_t)cur * P.S;
+    float g_pre_tn =
+        G.vec4 ? plane_local_bwd4(o, d, r.tn, center, pn, radius, ts, tr, th, P.S, pr, g_c, g_ts, g_po, g_pn, g_r,
+                                  G.sites + b3, G.rgb + b3, G.height + (int64_t)cur * P.S)
+               : plane_local_bwd(o, d, r.tn, center, pn, radius, ts, tr, th, P.S, pr, g_c, g_ts, g_po, g_pn, g_r,
+                                 G.sites + b3, G.rgb + b3, G.height + (int64_t)cur * P.S);
     if (tn_id != n_adj) g_tn += g_pre_tn;
     const float g_ends[2] = {tn_id == n_adj ? g_pre_tn : g_tn, g_tf};
     const int end_ids[2] = {tn_id == n_adj ? pre_tn_id : tn_id, tf_id};
@@ -1074,8 +1198,10 @@ extern "C" int pf_trace_backward(const pf_trace_inputs* in, const float* color, 
     size_t lens[7] = {3 * N, N, 3 * N, N, 3 * N * S, 3 * N * S, N * S};
     for (int i = 0; i < 7; i++)
         if (lens[i]) cudaMemsetAsync(outs[i], 0, sizeof(float) * lens[i], st);
-    TraceGrads G{grad_points, grad_radii, grad_normals, grad_density, grad_texel_sites, grad_texel_rgb,
-                 grad_texel_height};
+    const bool vec4 = (P.S % 4) == 0 && ((uintptr_t)grad_texel_sites % 16) == 0 &&
+                      ((uintptr_t)grad_texel_rgb % 16) == 0 && ((uintptr_t)grad_texel_height % 16) == 0;
+    TraceGrads G{grad_points,      grad_radii,     grad_normals,      grad_density,
+                 grad_texel_sites, grad_texel_rgb, grad_texel_height, vec4};
     TraceAdjIn A{color, normal, depth_seg, depth_sigma, grad_color, grad_log_t, grad_depth, grad_normal};
     const int64_t n = trace_slots(in);
     size_t off[5];

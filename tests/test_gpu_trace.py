@@ -113,8 +113,14 @@ def test_trace_adjoint_overflow(seed, thr, kb):
     _adjoint_case(seed, thr, 29, 21, kb)
 
 
-def _adjoint_case(seed, thr, W, H, kb):
-    sc = np_scene(80 + seed, 300, -0.6, 0.6, 0.05, 0.15, height_scale=0.2)
+@pytest.mark.parametrize("S", [4, 6])
+def test_trace_adjoint_texel_counts(S):
+    """Texel counts with (4) and without (6) the float4 gradient atomics."""
+    _adjoint_case(5, 1e-3, 29, 21, None, S)
+
+
+def _adjoint_case(seed, thr, W, H, kb, S=8):
+    sc = np_scene(80 + seed, 300, -0.6, 0.6, 0.05, 0.15, S=S, height_scale=0.2)
     cam = np_camera((0.3, 0.2 * seed, 2.2), (0, 0, 0), W, H, 55.0)
     tp = {k: to_t(v).requires_grad_(True) for k, v in sc.items()}
     adj, off = build_power_adjacency(tp["points"].detach(), tp["radii"].detach())
