@@ -119,16 +119,28 @@ def test_trace_adjoint_texel_counts(S):
     _adjoint_case(5, 1e-3, 29, 21, None, S)
 
 
-def _adjoint_case(seed, thr, W, H, kb, S=8):
+@pytest.mark.parametrize("kb", [None, 2])
+def test_trace_adjoint_per_ray_start_cells(kb):
+    """Per-ray start cells (the seeded tracer's input): half the rays start in
+    the camera's cell, the others in seeded cells anywhere in the scene."""
+    _adjoint_case(6, 1e-3, 29, 21, kb, per_ray_start=True)
+
+
+def _adjoint_case(seed, thr, W, H, kb, S=8, per_ray_start=False):
     sc = np_scene(80 + seed, 300, -0.6, 0.6, 0.05, 0.15, S=S, height_scale=0.2)
     cam = np_camera((0.3, 0.2 * seed, 2.2), (0, 0, 0), W, H, 55.0)
     tp = {k: to_t(v).requires_grad_(True) for k, v in sc.items()}
     adj, off = build_power_adjacency(tp["points"].detach(), tp["radii"].detach())
     pm = power_adjacency_diff(tp["points"].detach(), tp["radii"].detach(), adj, off)
     s = start_cell(tp["points"].detach(), tp["radii"].detach(), torch.from_numpy(cam["eye"]))
+    cells = None
+    if per_ray_start:
+        cells = np.random.default_rng(100 + seed).integers(0, 300, (H, W)).astype(np.int32)
+        cells[: H // 2] = int(s)
     R = RayTracer(Args(), "cuda")
     R.segments_per_ray = kb
-    color, log_t, depth, normal = R.forward(torch_cam(cam), s, tp["points"], tp["radii"], tp["density"],
+    start = s if cells is None else to_t(cells)
+    color, log_t, depth, normal = R.forward(torch_cam(cam), start, tp["points"], tp["radii"], tp["density"],
                                             tp["normals"], tp["texel_sites"], tp["texel_rgb"], tp["texel_height"],
                                             adj, off, pm, thr)
     rng = np.random.default_rng(seed)
@@ -142,11 +154,12 @@ def _adjoint_case(seed, thr, W, H, kb, S=8):
     sph, nsig, _ = packed(sc)
     adj_np, off_np, pm_np = adj.cpu().numpy(), off.cpu().numpy(), pm.cpu().numpy().view(np.uint16)
     f = orc.trace_forward(orc_cam(cam), sph, nsig, sc["texel_sites"], sc["texel_rgb"], sc["texel_height"], adj_np,
-                          off_np, pm_np, s, thr=thr)
+                          off_np, pm_np, s if cells is None else 0, start_cells=cells, thr=thr)
     for k, v in [("color", color), ("log_t", log_t), ("depth", depth), ("normal", normal)]:
         assert max_abs(v.detach().cpu(), f[k]) <= 1e-5, k
     g = orc.trace_backward(orc_cam(cam), sph, nsig, sc["texel_sites"], sc["texel_rgb"], sc["texel_height"], adj_np,
-                           off_np, pm_np, f, wC, wL, wD, wN, s, thr=thr)
+                           off_np, pm_np, f, wC, wL, wD, wN, s if cells is None else 0, start_cells=cells,
+                           thr=thr)
     from tests.helpers import assert_close_rel
     assert_close_rel(tp["points"].grad.cpu().numpy(), g["spheres"][:, :3], 1e-4, "points")
     assert_close_rel(tp["radii"].grad.cpu().numpy(), g["spheres"][:, 3], 1e-4, "radii")
