@@ -180,13 +180,15 @@ def make_step(R, scene, cam, adj, adj_off, target_dev, world):
     names = ["points", "radii", "density", "normals", "texel_sites", "texel_height"]
     params = {k: scene[k].clone().requires_grad_(True) for k in names}
 
-    def step(target=None):
+    def step(target=None, ready=None):
         t = target_dev if target is None else target
         for p in params.values():
             p.grad = None
         rgb = synthetic.texel_rgb(scene, cam).requires_grad_(True)
         out = R.forward(cam, None, params["points"], params["radii"], params["density"], params["normals"],
                         params["texel_sites"], rgb, params["texel_height"], adj, adj_off, None, False)
+        if ready is not None:  # the target's upload, issued on a copy stream, is needed from here on
+            torch.cuda.current_stream().wait_event(ready)
         loss = ((out[0] - t) ** 2).sum()
         loss.backward()
         if world > 1:
@@ -573,12 +575,14 @@ def trace_main(args, dev):
     target_host = torch.rand((cfg["height"], cfg["width"], 3), generator=g).pin_memory()
     target = target_host.to(dev)
 
-    def step(t=None):
+    def step(t=None, ready=None):
         for p in list(params.values()) + [rgb_p]:
             p.grad = None
         color, log_t, depth, normal = tr.forward(cam, st, params["points"], params["radii"], params["density"],
                                                  params["normals"], params["texel_sites"], rgb_p,
                                                  params["texel_height"], adj, off, pm)
+        if ready is not None:  # the target's upload on the copy stream
+            torch.cuda.current_stream().wait_event(ready)
         loss = ((color - (target if t is None else t)) ** 2).sum()
         loss.backward()
         return loss
@@ -597,14 +601,24 @@ def trace_main(args, dev):
     torch.cuda.synchronize()
     clk = clocks.stop()
     ms = a.elapsed_time(b) / args.steps
-    t_dev = torch.empty_like(target)
+    # targets uploaded on a copy stream into two buffers, as in the rasterizer workload
+    t_dev = [torch.empty_like(target) for _ in range(2)]
+    copy_stream = torch.cuda.Stream()
+    ready = [torch.cuda.Event() for _ in range(2)]
+    consumed = [torch.cuda.Event() for _ in range(2)]
     loss_host = torch.empty(args.steps, dtype=torch.float32).pin_memory()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
     e0.record()
     for i in range(args.steps):
-        t_dev.copy_(target_host, non_blocking=True)
-        loss_host[i].copy_(step(t_dev).detach(), non_blocking=True)
+        b = i % 2
+        copy_stream.wait_event(e0 if i < 2 else consumed[b])
+        with torch.cuda.stream(copy_stream):
+            t_dev[b].copy_(target_host, non_blocking=True)
+            ready[b].record(copy_stream)
+        loss = step(t_dev[b], ready[b])
+        consumed[b].record()
+        loss_host[i].copy_(loss.detach(), non_blocking=True)
     e1.record()
     torch.cuda.synchronize()
     e2e_ms = e0.elapsed_time(e1) / args.steps
@@ -973,17 +987,29 @@ def main():
     fwd_ms = statistics.mean(a.elapsed_time(b) for a, b in events["pf_raster_forward"])
     bwd_ms = statistics.mean(a.elapsed_time(b) for a, b in events["pf_raster_backward"])
 
-    # end to end through the public API: host target image in, loss out
+    # end to end through the public API: host target image in, loss out.  Each
+    # step's target is uploaded from pinned memory on a copy stream into one of
+    # two buffers (a training loop's prefetch), overlapping binning and the
+    # forward; the loss waits for it, and a buffer is refilled only after the
+    # loss that read it.
     target_host = target.pin_memory()
     loss_host = torch.empty(args.steps, dtype=torch.float32).pin_memory()
-    t_dev = torch.empty_like(target_dev)
+    t_dev = [torch.empty_like(target_dev) for _ in range(2)]
+    copy_stream = torch.cuda.Stream()
+    ready = [torch.cuda.Event() for _ in range(2)]
+    consumed = [torch.cuda.Event() for _ in range(2)]
     barrier()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record()
     for i in range(args.steps):
-        t_dev.copy_(target_host, non_blocking=True)
-        loss = step(t_dev)
+        b = i % 2
+        copy_stream.wait_event(e0 if i < 2 else consumed[b])
+        with torch.cuda.stream(copy_stream):
+            t_dev[b].copy_(target_host, non_blocking=True)
+            ready[b].record(copy_stream)
+        loss = step(t_dev[b], ready[b])
+        consumed[b].record()
         loss_host[i].copy_(loss.detach(), non_blocking=True)
     e1.record()
     barrier()
