@@ -6,6 +6,7 @@
 // cells.  The walk is bounded by max_steps; a ray that reaches the cap stops
 // and raises PF_ERR_STEP_CAP in the status word instead of looping forever.
 #include <algorithm>
+#include <type_traits>
 
 #include "pf_common.cuh"
 #include "pf_api.h"
@@ -24,6 +25,7 @@ struct TraceParams {
     const int32_t* adj;
     const int32_t* adj_off;
     const uint2* adj_diff;
+    bool tex4;  // f32 texels, S % 4 == 0, 16-byte aligned rows: texels read as float4 groups
     int32_t start_idx;
     const int32_t* start_cells;
     float thr;
@@ -70,6 +72,67 @@ PF_D PlaneRes plane_local(v3 o, v3 d, float t_near, v3 po, v3 pn, float radius, 
         float w = expf(-kTemp * dist_sq);
         rgb_sum = rgb_sum + w * mk(ldT(rgbs, 3 * i), ldT(rgbs, 3 * i + 1), ldT(rgbs, 3 * i + 2));
         wsum += w;
+    }
+    wsum = fmax_t(wsum, 1e-20f);
+    r._t_surf = _t_surf;
+    r._dp = _dp;
+    r.height = height;
+    r._wsum = _wsum;
+    r.t_surf = t_surf;
+    r.dp = dp;
+    r.rgb = rgb_sum / wsum;
+    r.wsum = wsum;
+    return r;
+}
+
+PF_D float4 ldg4(const float* p) { return __ldg(reinterpret_cast<const float4*>(p)); }
+
+// plane_local for f32 texels with S % 4 == 0 and 16-byte aligned rows: the
+// same arithmetic in the same order, texels fetched four sites at a time.
+PF_D PlaneRes plane_local4(v3 o, v3 d, float t_near, v3 po, v3 pn, float radius, const float* sites,
+                           const float* rgbs, const float* heights, int S) {
+    PlaneRes r;
+    float _dp;
+    float _t_surf = ray_plane(o, d, po, pn, 0.0f, _dp);
+    float _tq = _dp >= 0.0f ? t_near : fmax_t(t_near, _t_surf);
+    v3 _pt = o + _tq * d;
+    float inv_r2 = 1.0f / (radius * radius);
+    float hsum = 0.f, _wsum = 0.f;
+    for (int g = 0; g < S; g += 4) {
+        const float4 a = ldg4(sites + 3 * g), b = ldg4(sites + 3 * g + 4), c = ldg4(sites + 3 * g + 8);
+        const float4 h = ldg4(heights + g);
+        const float sx[12] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w, c.x, c.y, c.z, c.w};
+        const float hh[4] = {h.x, h.y, h.z, h.w};
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            v3 df = _pt - mk(sx[3 * u], sx[3 * u + 1], sx[3 * u + 2]);
+            float dist_sq = dot(df, df) * inv_r2;
+            float w = expf(-kTemp * dist_sq);
+            hsum += w * hh[u];
+            _wsum += w;
+        }
+    }
+    _wsum = fmax_t(_wsum, 1e-20f);
+    float height = hsum / _wsum;
+    float dp;
+    float t_surf = ray_plane(o, d, po, pn, height, dp);
+    float tq = dp >= 0.0f ? t_near : fmax_t(t_near, t_surf);
+    v3 pt = o + tq * d;
+    v3 rgb_sum = mk(0.f, 0.f, 0.f);
+    float wsum = 0.f;
+    for (int g = 0; g < S; g += 4) {
+        const float4 a = ldg4(sites + 3 * g), b = ldg4(sites + 3 * g + 4), c = ldg4(sites + 3 * g + 8);
+        const float4 e = ldg4(rgbs + 3 * g), f = ldg4(rgbs + 3 * g + 4), k = ldg4(rgbs + 3 * g + 8);
+        const float sx[12] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w, c.x, c.y, c.z, c.w};
+        const float cx[12] = {e.x, e.y, e.z, e.w, f.x, f.y, f.z, f.w, k.x, k.y, k.z, k.w};
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            v3 df = pt - mk(sx[3 * u], sx[3 * u + 1], sx[3 * u + 2]);
+            float dist_sq = dot(df, df) * inv_r2;
+            float w = expf(-kTemp * dist_sq);
+            rgb_sum = rgb_sum + w * mk(cx[3 * u], cx[3 * u + 1], cx[3 * u + 2]);
+            wsum += w;
+        }
     }
     wsum = fmax_t(wsum, 1e-20f);
     r._t_surf = _t_surf;
@@ -173,8 +236,18 @@ trace_fwd_kernel(TraceParams P, int64_t nthreads, float* __restrict__ color, flo
             continue;
         }
         int64_t b3 = (int64_t)prim * P.S * 3;
-        PlaneRes pr = plane_local<A>(o, d, tn, center, pn, radius, (const A*)P.sites + b3, (const A*)P.rgb + b3,
-                                     (const A*)P.height + (int64_t)prim * P.S, P.S);
+        PlaneRes pr;
+        if constexpr (std::is_same<A, float>::value) {
+            if (P.tex4)
+                pr = plane_local4(o, d, tn, center, pn, radius, (const float*)P.sites + b3, (const float*)P.rgb + b3,
+                                  (const float*)P.height + (int64_t)prim * P.S, P.S);
+            else
+                pr = plane_local<A>(o, d, tn, center, pn, radius, (const A*)P.sites + b3, (const A*)P.rgb + b3,
+                                    (const A*)P.height + (int64_t)prim * P.S, P.S);
+        } else {
+            pr = plane_local<A>(o, d, tn, center, pn, radius, (const A*)P.sites + b3, (const A*)P.rgb + b3,
+                                (const A*)P.height + (int64_t)prim * P.S, P.S);
+        }
         tf = pr.dp >= 0.0f ? fmin_t(pr.t_surf, tf) : tf;
         tn = pr.dp < 0.0f ? fmax_t(pr.t_surf, tn) : tn;
         prim = next;
@@ -372,7 +445,8 @@ PF_D float plane_local_bwd(v3 o, v3 d, float tn, v3 po, v3 pn, float radius, con
 
 PF_D void red4(float* p, const float* v) { atomicAdd((float4*)p, make_float4(v[0], v[1], v[2], v[3])); }
 
-// plane_local_bwd for S a multiple of 4 with 16-byte aligned gradient rows:
+// plane_local_bwd for S a multiple of 4 with 16-byte aligned texel and gradient rows (texels read as
+// float4 groups):
 // the texel gradients leave as float4 atomics, four sites at a time, and a
 // site's colour and height terms are summed before its atomic (the colour
 // terms are recomputed when the height term is live, i.e. when the plane
@@ -392,14 +466,17 @@ PF_D float plane_local_bwd4(v3 o, v3 d, float tn, v3 po, v3 pn, float radius, co
     v3 g_pt = mk(0.f, 0.f, 0.f);
     for (int g = 0; g < S; g += 4) {
         float rg[12], sg[12];
+        const float4 a0 = ldg4(sites + 3 * g), a1 = ldg4(sites + 3 * g + 4), a2 = ldg4(sites + 3 * g + 8);
+        const float4 c0 = ldg4(rgbs + 3 * g), c1 = ldg4(rgbs + 3 * g + 4), c2 = ldg4(rgbs + 3 * g + 8);
+        const float sx[12] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w, a2.x, a2.y, a2.z, a2.w};
+        const float cx[12] = {c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c1.z, c1.w, c2.x, c2.y, c2.z, c2.w};
 #pragma unroll
         for (int u = 0; u < 4; u++) {
-            const int i = g + u;
-            v3 s = mk(sites[3 * i], sites[3 * i + 1], sites[3 * i + 2]);
+            v3 s = mk(sx[3 * u], sx[3 * u + 1], sx[3 * u + 2]);
             v3 df = pt - s;
             float q2 = dot(df, df);
             float vi = expf(-kTemp * q2 * inv_r2);
-            v3 ci = mk(rgbs[3 * i], rgbs[3 * i + 1], rgbs[3 * i + 2]);
+            v3 ci = mk(cx[3 * u], cx[3 * u + 1], cx[3 * u + 2]);
             const v3 a = (vi * inv_V) * g_rgb;
             rg[3 * u] = a.x;
             rg[3 * u + 1] = a.y;
@@ -442,14 +519,19 @@ PF_D float plane_local_bwd4(v3 o, v3 d, float tn, v3 po, v3 pn, float radius, co
         v3 g__pt = mk(0.f, 0.f, 0.f);
         for (int g = 0; g < S; g += 4) {
             float sg[12], hg[4];
+            const float4 a0 = ldg4(sites + 3 * g), a1 = ldg4(sites + 3 * g + 4), a2 = ldg4(sites + 3 * g + 8);
+            const float4 c0 = ldg4(rgbs + 3 * g), c1 = ldg4(rgbs + 3 * g + 4), c2 = ldg4(rgbs + 3 * g + 8);
+            const float4 h4 = ldg4(heights + g);
+            const float sx[12] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w, a2.x, a2.y, a2.z, a2.w};
+            const float cx[12] = {c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c1.z, c1.w, c2.x, c2.y, c2.z, c2.w};
+            const float hx[4] = {h4.x, h4.y, h4.z, h4.w};
 #pragma unroll
             for (int u = 0; u < 4; u++) {
-                const int i = g + u;
-                v3 s = mk(sites[3 * i], sites[3 * i + 1], sites[3 * i + 2]);
+                v3 s = mk(sx[3 * u], sx[3 * u + 1], sx[3 * u + 2]);
                 v3 df = pt - s;
                 float q2 = dot(df, df);
                 float vi = expf(-kTemp * q2 * inv_r2);
-                v3 ci = mk(rgbs[3 * i], rgbs[3 * i + 1], rgbs[3 * i + 2]);
+                v3 ci = mk(cx[3 * u], cx[3 * u + 1], cx[3 * u + 2]);
                 float g_vi = (v_open ? dot(ci - pr.rgb, g_rgb) : dot(ci, g_rgb)) * inv_V;
                 v3 b = (-g_vi) * ((vi * (-2.0f * kTemp * inv_r2)) * df);
                 hg[u] = 0.f;
@@ -457,7 +539,7 @@ PF_D float plane_local_bwd4(v3 o, v3 d, float tn, v3 po, v3 pn, float radius, co
                     v3 dfw = _pt - s;
                     float q2w = dot(dfw, dfw);
                     float wi = expf(-kTemp * q2w * inv_r2);
-                    float hi = heights[i];
+                    float hi = hx[u];
                     hg[u] = wi * inv_W * g_height;
                     float g_wi = (w_open ? (hi - pr.height) : hi) * inv_W * g_height;
                     v3 dwdpt = (wi * (-2.0f * kTemp * inv_r2)) * dfw;
@@ -580,7 +662,7 @@ PF_D void segment_adjoint(const TraceParams& P, const TraceAdjIn& A, const Trace
     const float* tr = (const float*)P.rgb + b3;
     const float* th = (const float*)P.height + (int64_t)cur * P.S;
     float g_pre_tn =
-        G.vec4 ? plane_local_bwd4(o, d, r.tn, center, pn, radius, ts, tr, th, P.S, pr, g_c, g_ts, g_po, g_pn, g_r,
+        G.vec4 && P.tex4 ? plane_local_bwd4(o, d, r.tn, center, pn, radius, ts, tr, th, P.S, pr, g_c, g_ts, g_po, g_pn, g_r,
                                   G.sites + b3, G.rgb + b3, G.height + (int64_t)cur * P.S)
                : plane_local_bwd(o, d, r.tn, center, pn, radius, ts, tr, th, P.S, pr, g_c, g_ts, g_po, g_pn, g_r,
                                  G.sites + b3, G.rgb + b3, G.height + (int64_t)cur * P.S);
@@ -626,9 +708,12 @@ PF_D PlaneRes cell_plane(const TraceParams& P, v3 o, v3 d, int32_t cell, float t
     const float4 s4 = __ldg(&P.spheres[cell]);
     const float* ns = (const float*)P.nsig + 4 * (int64_t)cell;
     const int64_t b3 = (int64_t)cell * P.S * 3;
-    return plane_local<float>(o, d, t_near, mk(s4.x, s4.y, s4.z), mk(__ldg(ns), __ldg(ns + 1), __ldg(ns + 2)), s4.w,
-                              (const float*)P.sites + b3, (const float*)P.rgb + b3,
-                              (const float*)P.height + (int64_t)cell * P.S, P.S);
+    const v3 c = mk(s4.x, s4.y, s4.z), pn = mk(__ldg(ns), __ldg(ns + 1), __ldg(ns + 2));
+    const float* ts = (const float*)P.sites + b3;
+    const float* tr = (const float*)P.rgb + b3;
+    const float* th = (const float*)P.height + (int64_t)cell * P.S;
+    return P.tex4 ? plane_local4(o, d, t_near, c, pn, s4.w, ts, tr, th, P.S)
+                  : plane_local<float>(o, d, t_near, c, pn, s4.w, ts, tr, th, P.S);
 }
 
 // The adjoint runs in three launches over the rays of the trace (thread
@@ -1065,6 +1150,8 @@ extern "C" int pf_trace_forward(const pf_trace_inputs* in, float* color, float* 
     P.adj = in->adjacency;
     P.adj_off = in->adjacency_offsets;
     P.adj_diff = (const uint2*)in->adjacency_diff;
+    P.tex4 = !in->attr_half && in->n_sites % 4 == 0 && ((uintptr_t)in->texel_sites % 16) == 0 &&
+             ((uintptr_t)in->texel_rgb % 16) == 0 && ((uintptr_t)in->texel_height % 16) == 0;
     P.start_idx = in->start_idx;
     P.start_cells = in->start_cells;
     P.thr = in->transmittance_threshold;
@@ -1139,6 +1226,8 @@ static bool fill_trace(const pf_trace_inputs* in, TraceParams& P, const char** w
     P.adj = in->adjacency;
     P.adj_off = in->adjacency_offsets;
     P.adj_diff = (const uint2*)in->adjacency_diff;
+    P.tex4 = !in->attr_half && in->n_sites % 4 == 0 && ((uintptr_t)in->texel_sites % 16) == 0 &&
+             ((uintptr_t)in->texel_rgb % 16) == 0 && ((uintptr_t)in->texel_height % 16) == 0;
     P.start_idx = in->start_idx;
     P.start_cells = in->start_cells;
     P.thr = in->transmittance_threshold;
