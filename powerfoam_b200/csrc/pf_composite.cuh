@@ -691,8 +691,8 @@ PF_D void swap_pix(BwdPix& a, BwdPix& b) {
     b = t;
 }
 
-struct BwdStage {
-    float acc[kAccRows][32];     // per-lane gradient columns of the current primitive
+struct __align__(16) BwdStage {
+    float acc[kAccRows][32];     // per-lane gradient columns of the current primitive (rows 16-byte aligned)
     float4 face_acc[kFaceSlots]; // neighbour sphere gradients per neighbour slot
     float4 nbr_sph[kFaceSlots];  // exact neighbour spheres (face adjoint)
     int32_t nbr_id[kFaceSlots];
@@ -1113,16 +1113,23 @@ PF_D void bwd_tile(const RasterParams& P, const BwdIn& in, const GradOut& go, in
                 bs.acc[6][lane] += g_n2;
                 bs.acc[7][lane] += g_s;
                 __syncwarp();
-                // sum rows 2l, 2l+1 over the 32 columns (rotated: conflict-free), zero them
+                // sum rows 2l, 2l+1 over the 32 columns, four at a time (128-bit
+                // accesses rotated by lane: each 8-lane phase hits distinct banks),
+                // zero them
 #pragma unroll
                 for (int h = 0; h < 2; h++) {
                     const int row = 2 * lane + h;
+                    float4* r4 = reinterpret_cast<float4*>(bs.acc[row]);
                     float sum = 0.f;
-#pragma unroll 8
-                    for (int c = 0; c < 32; c++) {
-                        const int col = (c + lane) & 31;
-                        sum += bs.acc[row][col];
-                        bs.acc[row][col] = 0.f;
+#pragma unroll
+                    for (int c = 0; c < 8; c++) {
+                        const int cc = (c + lane) & 7;
+                        const float4 v = r4[cc];
+                        sum += v.x;
+                        sum += v.y;
+                        sum += v.z;
+                        sum += v.w;
+                        r4[cc] = make_float4(0.f, 0.f, 0.f, 0.f);
                     }
                     if (sum != 0.0f) {
                         float* dst = grad_slot(go, P.S, prim, row);
