@@ -633,7 +633,10 @@ def trace_main(args, dev):
                             cells_walked=steps_total, mean_degree=deg, adjacency_s=adj_s,
                             l2="inputs larger than L2, no flush"),
                 clocks=clk, e2e=dict(value=1000.0 / e2e_ms, unit="frames/s", h2d_bytes_per_step=target.numel() * 4,
-                                     d2h_bytes_per_step=4))
+                                     d2h_bytes_per_step=4),
+                # per step: the walk (pf_trace_forward), then the adjoint's walk, segment and resume launches
+                # and seven gradient sanitising launches (pf_trace_backward)
+                gpu_launches=args.steps * (1 + 3 + 7))
     print(json.dumps(line), flush=True)
 
 
