@@ -637,7 +637,35 @@ def trace_main(args, dev):
                 # per step: the walk (pf_trace_forward), then the adjoint's walk, segment and resume launches
                 # and seven gradient sanitising launches (pf_trace_backward)
                 gpu_launches=args.steps * (1 + 3 + 7))
+    if not args.no_cpu_baseline:
+        line["cpu_baseline"] = trace_cpu_baseline(sc, rgb, adj, off, pm, cam, st, cfg)
     print(json.dumps(line), flush=True)
+
+
+def trace_cpu_baseline(sc, rgb, adj, off, pm, cam, start, cfg, w=None, h=None):
+    """The oracle's tracer (CPU restatement, OpenMP over rays) forward + L2
+    adjoint of the same view and frustum at w x h rays (default: the whole
+    image, about 6 s on 16 host threads), scaled to the full image by ray
+    count."""
+    from oracle import oracle as orc
+
+    w, h = w or cfg["width"], h or cfg["height"]
+    orc.build()
+    n = lambda t: t.detach().cpu().numpy()  # noqa: E731
+    sph = np.concatenate([n(sc["points"]), n(sc["radii"])[:, None]], -1).astype(np.float32)
+    nsig = np.concatenate([n(sc["normals"]), n(sc["density"])[:, None]], -1).astype(np.float32)
+    oc = orc.camera(n(cam.eye), n(cam.right), n(cam.up), w, h)
+    args = (oc, sph, nsig, n(sc["texel_sites"]), n(rgb), n(sc["texel_height"]), n(adj), n(off),
+            n(pm).view(np.uint16))
+    t0 = time.perf_counter()
+    f = orc.trace_forward(*args, int(start), thr=1e-3)
+    g_c = (2.0 * (f["color"] - np.random.default_rng(202).uniform(0, 1, f["color"].shape))).astype(np.float32)
+    orc.trace_backward(*args, f, g_c, None, None, None, int(start), thr=1e-3)
+    t_sample = time.perf_counter() - t0
+    t = t_sample * (cfg["width"] * cfg["height"]) / (w * h)
+    return dict(value=1.0 / t, unit="frames/s (fwd+bwd)", cores=orc.num_threads(), kind="port",
+                sample=(f"oracle walk + adjoint of the same view at {w}x{h} rays ({t_sample:.2f}s), "
+                        f"scaled to {cfg['width']}x{cfg['height']}"))
 
 
 def interpen_main(args, dev):
