@@ -201,3 +201,38 @@ def test_trace_adjoint_paths_agree_at_scale():
         for a, b in zip(grads[0], other):
             assert torch.isfinite(b).all()
             assert ((a - b).norm() / a.norm().clamp_min(1e-30)).item() <= 1e-5
+
+
+def test_trace_backward_workspace_checks():
+    """The adjoint's C entry rejects a missing, short or misaligned workspace
+    and an out-of-range segment count before launching anything."""
+    sc = np_scene(90, 200, -0.6, 0.6, 0.05, 0.15)
+    cam = np_camera((0.2, 0.1, 2.2), (0, 0, 0), 16, 12, 55.0)
+    tp = {k: to_t(v) for k, v in sc.items()}
+    adj, off = build_power_adjacency(tp["points"], tp["radii"])
+    pm = power_adjacency_diff(tp["points"], tp["radii"], adj, off)
+    s = start_cell(tp["points"], tp["radii"], torch.from_numpy(cam["eye"]))
+    R = RayTracer(Args(), "cuda")
+    args = R._prep(tp["points"], tp["radii"], tp["density"], tp["normals"], tp["texel_sites"], tp["texel_rgb"],
+                   tp["texel_height"], adj, off, pm)
+    inp = R._inputs(torch_cam(cam), s, *args, 1e-3, 1 << 16, 0.5)
+    nbytes = _lib.ctypes.c_size_t(0)
+    _lib.call("pf_trace_backward_workspace_size", _lib.ctypes.byref(inp), 8, _lib.ctypes.byref(nbytes))
+    assert nbytes.value >= 8 * 48 * 16 * 12
+    for kb in (-1, 65536):
+        with pytest.raises(_lib.PfError):
+            _lib.call("pf_trace_backward_workspace_size", _lib.ctypes.byref(inp), kb, _lib.ctypes.byref(nbytes))
+    _lib.call("pf_trace_backward_workspace_size", _lib.ctypes.byref(inp), 8, _lib.ctypes.byref(nbytes))
+    n, S = tp["points"].shape[0], tp["texel_sites"].shape[1]
+    color = torch.zeros((12, 16, 3), device="cuda")
+    g = torch.zeros_like(color)
+    out = [torch.zeros(sh, device="cuda") for sh in ((n, 3), (n,), (n, 3), (n,), (n, S, 3), (n, S, 3), (n, S))]
+    ws = torch.empty(nbytes.value + 512, dtype=torch.uint8, device="cuda")
+    base = (ws.data_ptr() + 255) & ~255
+    for ptr, size in ((None, nbytes.value), (base, nbytes.value - 1), (base + 16, nbytes.value)):
+        with pytest.raises(_lib.PfError):
+            _lib.call("pf_trace_backward", _lib.ctypes.byref(inp), _lib.ptr(color), None, None, None, _lib.ptr(g),
+                      None, None, None, *[_lib.ptr(t) for t in out], 8, ptr, size, _lib.stream_ptr())
+    _lib.call("pf_trace_backward", _lib.ctypes.byref(inp), _lib.ptr(color), None, None, None, _lib.ptr(g), None,
+              None, None, *[_lib.ptr(t) for t in out], 8, base, nbytes.value, _lib.stream_ptr())
+    torch.cuda.synchronize()
