@@ -576,13 +576,18 @@ PF_D void fwd_tile_c(const RasterParams& P, const FwdOut& out, int64_t tile, int
                             }
                         }
                     }
-                    const float4 n4 = cs.nsg[kk];
-                    const PlaneRes pr =
-                        plane_fwd_tex(po, d, tn, center, mk(n4.x, n4.y, n4.z), radius, global_texels(P, prim), P.S);
-                    const float tf2 = pr.dp >= 0.0f ? fmin_t(pr.t_surf, tf) : tf;
-                    const float tn2 = pr.dp < 0.0f ? fmax_t(pr.t_surf, tn) : tn;
-                    cs.rec[j & 63] = make_float4(tf2 - tn2, pr.rgb.x, pr.rgb.y, pr.rgb.z);
-                    cs.rec_tn[j & 63] = tn2;
+                    if (tn < tf) {  // else the plane, which only shrinks [tn, tf], leaves dt <= 0 (or NaN)
+                        const float4 n4 = cs.nsg[kk];
+                        const PlaneRes pr = plane_fwd_tex(po, d, tn, center, mk(n4.x, n4.y, n4.z), radius,
+                                                          global_texels(P, prim), P.S);
+                        const float tf2 = pr.dp >= 0.0f ? fmin_t(pr.t_surf, tf) : tf;
+                        const float tn2 = pr.dp < 0.0f ? fmax_t(pr.t_surf, tn) : tn;
+                        cs.rec[j & 63] = make_float4(tf2 - tn2, pr.rgb.x, pr.rgb.y, pr.rgb.z);
+                        cs.rec_tn[j & 63] = tn2;
+                    } else {
+                        cs.rec[j & 63] = make_float4(-1.0f, 0.f, 0.f, 0.f);
+                        cs.rec_tn[j & 63] = tn;
+                    }
                 }
                 __syncwarp();
                 const int done = min(base + 32, n_pairs);
