@@ -946,13 +946,6 @@ PF_D void bwd_tile(const RasterParams& P, const BwdIn& in, const GradOut& go, in
             a.tf_id = a.tf < 1e-8f ? -2 : -1;
             b.tn_id = b.tn < 1e-8f ? -2 : -1;
             b.tf_id = b.tf < 1e-8f ? -2 : -1;
-            // neighbour slots used by the face adjoint
-            for (int e = lane; e < min(n_adj, kFaceSlots); e += 32) {
-                int32_t nb = __ldg(&P.adj[a0 + e]);
-                bs.nbr_id[e] = nb;
-                bs.nbr_sph[e] = __ldg(&P.spheres[nb]);
-                bs.face_acc[e] = make_float4(0.f, 0.f, 0.f, 0.f);
-            }
             for (int e0 = 0; e0 < n_adj; e0 += 32) {
                 stage_faces(ws, P, a0, e0, n_adj, GEN ? mk(0.f, 0.f, 0.f) : o, center, cc, rr, lane);
                 const int en = min(32, n_adj - e0);
@@ -991,6 +984,14 @@ PF_D void bwd_tile(const RasterParams& P, const BwdIn& in, const GradOut& go, in
             // with no such lane left the primitive is done (28 % of the hit
             // primitives at 1M primitives, 1080p).
             if (!__any_sync(0xffffffffu, (a.hit && a.tn < a.tf) || (PPL == 2 && b.hit && b.tn < b.tf))) continue;
+            // neighbour slots used by the face adjoint (read across lanes after
+            // stage_texels' barrier)
+            for (int e = lane; e < min(n_adj, kFaceSlots); e += 32) {
+                int32_t nb = __ldg(&P.adj[a0 + e]);
+                bs.nbr_id[e] = nb;
+                bs.nbr_sph[e] = __ldg(&P.spheres[nb]);
+                bs.face_acc[e] = make_float4(0.f, 0.f, 0.f, 0.f);
+            }
             stage_texels(ws, P, prim, lane);
             const float cg = in.g_contrib ? __ldg(&in.g_contrib[prim]) : 0.f;
             bool any_contrib = false;
