@@ -47,3 +47,24 @@ def test_oracle_library_loads():
     lib = orc.lib()
     for s in ["orc_bin_f32", "orc_raster_forward_f32", "orc_raster_backward_f64", "orc_trace_forward_f32"]:
         assert hasattr(lib, s)
+
+
+def test_trace_backward_workspace_size_without_a_gpu():
+    """The tracer adjoint's workspace: 48-byte records per pixel slot (8 x 8
+    tiles) and segment slot plus counts, overflow list and states; segment
+    counts outside [0, 65535] are rejected."""
+    from powerfoam_b200 import _lib
+
+    lib = _lib.load()
+    inp = _lib.PfTraceInputs()
+    inp.cam.width, inp.cam.height = 30, 17  # 4 x 3 tiles: 768 slots
+    n = ctypes.c_size_t(0)
+    _lib.call("pf_trace_backward_workspace_size", ctypes.byref(inp), 0, ctypes.byref(n))
+    base = n.value
+    assert base >= 768 * (4 + 4 + 48)
+    _lib.call("pf_trace_backward_workspace_size", ctypes.byref(inp), 10, ctypes.byref(n))
+    assert n.value - base >= 768 * 10 * 48 and n.value % 256 == 0
+    for kb in (-1, 65536):
+        assert lib.pf_trace_backward_workspace_size(ctypes.byref(inp), kb, ctypes.byref(n)) == _lib.PF_ERR_ARGS
+    inp.cam.width = 0
+    assert lib.pf_trace_backward_workspace_size(ctypes.byref(inp), 4, ctypes.byref(n)) == _lib.PF_ERR_ARGS
