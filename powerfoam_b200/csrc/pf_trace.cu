@@ -445,13 +445,12 @@ PF_D float plane_local_bwd(v3 o, v3 d, float tn, v3 po, v3 pn, float radius, con
 
 PF_D void red4(float* p, const float* v) { atomicAdd((float4*)p, make_float4(v[0], v[1], v[2], v[3])); }
 
-// plane_local_bwd for S a multiple of 4 with 16-byte aligned texel and gradient rows (texels read as
-// float4 groups):
-// the texel gradients leave as float4 atomics, four sites at a time, and a
-// site's colour and height terms are summed before its atomic (the colour
-// terms are recomputed when the height term is live, i.e. when the plane
-// bounds the segment or holds the colour query point).  Every other value
-// is computed in plane_local_bwd's order.
+// plane_local_bwd for S a multiple of 4 with 16-byte aligned texel and
+// gradient rows: texels are read and their gradients leave as float4 groups
+// of four sites, and a site's colour and height terms are summed before its
+// atomic (the colour terms are recomputed when the height term is live, i.e.
+// when the plane bounds the segment or holds the colour query point).  Every
+// other value is computed in plane_local_bwd's order.
 PF_D float plane_local_bwd4(v3 o, v3 d, float tn, v3 po, v3 pn, float radius, const float* sites, const float* rgbs,
                             const float* heights, int S, const PlaneRes& pr, v3 g_rgb, float g_tsurf, v3& g_po,
                             v3& g_pn, float& g_radius, float* gs, float* gr, float* gh) {
