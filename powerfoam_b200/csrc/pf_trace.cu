@@ -722,8 +722,9 @@ PF_D PlaneRes cell_plane(const TraceParams& P, v3 o, v3 d, int32_t cell, float t
 //     `kb` segments per ray in the workspace; a ray with more stops there
 //     and leaves its walk state (cell, steps, log T, segment index,
 //     accumulated colour / normal) on an overflow list.
-//  2. trace_bwd_segment_kernel: one thread per recorded segment (grid y =
-//     slot), texture plane recomputed, gradients by atomics.
+//  2. trace_bwd_segment_kernel: the recorded segments, every lane of a warp
+//     on one segment index at a time, texture plane recomputed, gradients
+//     by atomics.
 //  3. trace_bwd_resume_kernel finishes the overflow rays from their saved
 //     state (empty list: every warp returns at once).
 // Launches 1 and 2 carry no per-ray loop around the gradient work, so the
@@ -820,18 +821,27 @@ trace_bwd_walk_kernel(TraceParams P, SegWs W) {
     W.count[tid] = nrec;
 }
 
+// Grid y = kSegStride: the thread of ray slot `tid` takes its segments
+// blockIdx.y, blockIdx.y + kSegStride, ... below its count, so the lanes of
+// a warp work on one segment index at a time (as with one block per index)
+// without a block launched for every index up to kb.
+constexpr int kSegStride = 8;
+
 __global__ void __launch_bounds__(128)
 trace_bwd_segment_kernel(TraceParams P, SegWs W, TraceAdjIn A, TraceGrads G) {
     const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const int k = blockIdx.y;
-    if (tid >= W.n || k >= W.count[tid]) return;
+    if (tid >= W.n) return;
+    const int count = W.count[tid];
+    if ((int)blockIdx.y >= count) return;
     int pi, pj;
     trace_pixel(P.cam, tid, pi, pj);
     const int64_t px = (int64_t)pi * P.cam.W + pj;
     const v3 o = P.cam.eye;
     const v3 d = ray_dir(P.cam, pi, pj);
-    const SegRec r = load_rec(W.rec + 3 * ((int64_t)k * W.n + tid));
-    segment_adjoint(P, A, G, o, d, px, r, cell_plane(P, o, d, r.cell, r.tn));
+    for (int k = blockIdx.y; k < count; k += gridDim.y) {
+        const SegRec r = load_rec(W.rec + 3 * ((int64_t)k * W.n + tid));
+        segment_adjoint(P, A, G, o, d, px, r, cell_plane(P, o, d, r.cell, r.tn));
+    }
 }
 
 // Resume launch: each warp takes 32 overflow rays and runs them in rounds.
@@ -1300,7 +1310,8 @@ extern "C" int pf_trace_backward(const pf_trace_inputs* in, const float* color, 
     cudaMemsetAsync(W.n_over, 0, sizeof(int32_t), st);
     const unsigned blocks = (unsigned)((n + 127) / 128);
     trace_bwd_walk_kernel<<<blocks, 128, 0, st>>>(P, W);
-    if (segments_per_ray > 0) trace_bwd_segment_kernel<<<dim3(blocks, segments_per_ray), 128, 0, st>>>(P, W, A, G);
+    if (segments_per_ray > 0)
+        trace_bwd_segment_kernel<<<dim3(blocks, std::min(segments_per_ray, kSegStride)), 128, 0, st>>>(P, W, A, G);
     static_assert(trace_resume_smem() <= 48 * 1024, "resume queue above the default shared-memory limit");
     trace_bwd_resume_kernel<<<blocks, 128, trace_resume_smem(), st>>>(P, W, A, G);
     for (int i = 0; i < 7; i++)
