@@ -152,16 +152,8 @@ class ClockSampler:
 # ----------------------------------------------------------------------------
 def build_workload(device, seed_offset=0, tile=8, workload=WORKLOAD):
     from powerfoam_b200 import synthetic
-    from powerfoam_b200.adjacency import CechBuilder
 
-    cfg = synthetic.CONFIGS[workload]
-    scene = synthetic.make_scene(cfg["n"], seed=cfg["seed"], mixture=cfg["mixture"], sigma=cfg["sigma"],
-                                 r_range=cfg["r_range"], device=device)
-    cam = synthetic.orbit_camera(100 + seed_offset, cfg["width"], cfg["height"], cfg["vfov"], device=device)
-    adj, adj_off = CechBuilder(device)(scene["points"], scene["radii"])
-    g = torch.Generator().manual_seed(200 + seed_offset)
-    target = torch.rand((cfg["height"], cfg["width"], 3), generator=g)
-    return cfg, scene, cam, adj, adj_off, target
+    return synthetic.raster_workload(workload, device, view=seed_offset)
 
 
 class Args:
@@ -774,7 +766,8 @@ def power_main(args, dev):
     hull by scipy's Qhull on one host core, benchmark.py:25-83) on a bounded
     subset."""
     from powerfoam_b200 import synthetic
-    from powerfoam_b200.adjacency import PowerBuilder, build_power_adjacency
+    from oracle.power_hull import build_power_adjacency
+    from powerfoam_b200.adjacency import PowerBuilder
 
     cfg = synthetic.CONFIGS["raster1m"]
     sc = synthetic.make_scene(cfg["n"], seed=cfg["seed"], mixture=cfg["mixture"], sigma=cfg["sigma"],

@@ -34,8 +34,9 @@ extern "C" {
 #define PF_ERR_CUDA 4      /* CUDA launch / runtime error */
 #define PF_ERR_SEED 5      /* a proposal seed landed outside every cell */
 #define PF_ERR_CELL 6      /* a power cell exceeded its plane / neighbour capacity */
+#define PF_ERR_NONFINITE 7 /* a primitive attribute is NaN or infinite */
 
-#define PF_ABI_VERSION 1
+#define PF_ABI_VERSION 2
 
 #if defined(__GNUC__)
 #define PF_API __attribute__((visibility("default")))
@@ -97,9 +98,12 @@ PF_API const char *pf_last_error(void);
 
 /* Pack per-primitive attributes into the float4 layouts the kernels read:
  * spheres = (points, radii), nsigmas = (normals, density).
- * Replaces the torch.cat calls of rasterize.py:1619-1620. */
+ * Replaces the torch.cat calls of rasterize.py:1619-1620.  status (device,
+ * may be NULL) is raised to PF_ERR_NONFINITE (atomic max, never lowered) when
+ * any packed value is NaN or infinite; the reference has no such check (its
+ * adjoint only zeroes non-finite gradients, rasterize.py:1954-1958). */
 PF_API int pf_pack_prims(const float *points, const float *radii, const float *normals, const float *density,
-                  int64_t n_prims, float *spheres, float *nsigmas, void *stream);
+                  int64_t n_prims, float *spheres, float *nsigmas, int32_t *status, void *stream);
 
 /* ---------------------------------------------------------------------- */
 /* Binning.  Replaces rasterize.py:1671-1768: count_visible_pinhole_kernel

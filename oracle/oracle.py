@@ -258,6 +258,33 @@ def trace_forward(cam, spheres, nsigmas, sites, rgbs, heights, adj, adj_off, adj
     return out
 
 
+def trace_forward_pixels(cam, spheres, nsigmas, sites, rgbs, heights, adj, adj_off, adj_diff_pm, pixels,
+                         start_idx=0, start_cells=None, thr=1e-3, max_steps=1 << 16, depth_quantile=0.5,
+                         visit_cap=0, prec="f32"):
+    """trace_forward for the camera pixels listed in ``pixels`` (row-major
+    indices); every output is indexed like ``pixels``."""
+    pixels = _c(pixels, np.int64)
+    n = pixels.shape[0]
+    S = sites.shape[1]
+    R = np.float64 if prec == "f64" else F32
+    out = dict(color=np.zeros((n, 3), R), log_t=np.zeros(n, R), depth=np.zeros(n, R), normal=np.zeros((n, 3), R),
+               depth_seg=np.zeros(n, np.int32), depth_sigma=np.zeros(n, R), visit_count=np.zeros(n, np.int32),
+               status=np.zeros(n, np.int32))
+    vl = np.full((n, max(visit_cap, 1)), -1, np.int32) if visit_cap else None
+    args = [_c(spheres, F32), _c(nsigmas, F32), _c(sites, F32), _c(rgbs, F32), _c(heights, F32)]
+    sc = None if start_cells is None else _c(start_cells, np.int32)
+    rc = _fn("orc_trace_forward_pixels", prec)(
+        ctypes.byref(cam), *[_p(a) for a in args], ctypes.c_int(S), _p(_c(adj, np.int32)),
+        _p(_c(adj_off, np.int32)), _p(None if adj_diff_pm is None else _c(adj_diff_pm, np.uint16)),
+        ctypes.c_int32(start_idx), _p(sc), ctypes.c_float(thr), ctypes.c_int(max_steps),
+        ctypes.c_float(depth_quantile), _p(pixels), ctypes.c_int64(n), _p(out["color"]), _p(out["log_t"]),
+        _p(out["depth"]), _p(out["normal"]), _p(out["depth_seg"]), _p(out["depth_sigma"]), _p(vl),
+        ctypes.c_int(visit_cap), _p(out["visit_count"]), _p(out["status"]))
+    out["rc"] = rc
+    out["visits"] = vl
+    return out
+
+
 def trace_labels(cam, spheres, nsigmas, sites, rgbs, heights, adj, adj_off, adj_diff_pm, start_idx=0,
                  start_cells=None, thr=1e-3, max_steps=1 << 16, label_thr=0.99):
     """Proposal-network labels of every camera ray: entry t / cell / step of
@@ -390,3 +417,18 @@ def trace_backward(cam, spheres, nsigmas, sites, rgbs, heights, adj, adj_off, ad
         _p(g["nsigmas"]), _p(g["texel_sites"]), _p(g["texel_rgb"]), _p(g["texel_height"]))
     assert rc == 0
     return g
+
+
+def cech_adjacency(points, radii):
+    """Čech adjacency of bvh.py:7-69 / build_cech_complex (bvh.py:96-123):
+    (adjacency int32 (E), offsets int32 (N+1)), lists ascending."""
+    pts = _c(points, F32)
+    rad = _c(radii, F32)
+    N = pts.shape[0]
+    off = np.zeros(N + 1, np.int32)
+    ne = ctypes.c_int64(0)
+    f = lib().orc_cech_adjacency_f32
+    assert f(_p(pts), _p(rad), ctypes.c_int64(N), _p(off), None, ctypes.byref(ne)) == 0
+    adj = np.zeros(max(ne.value, 1), np.int32)
+    assert f(_p(pts), _p(rad), ctypes.c_int64(N), _p(off), _p(adj), ctypes.byref(ne)) == 0
+    return adj[: ne.value], off

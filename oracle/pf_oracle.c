@@ -1514,19 +1514,28 @@ static int FN(trace_walk)(const orc_camera *camera, const float *spheres, const 
                           float depth_quantile, out_t *color, out_t *log_t_out, out_t *depth, out_t *normal,
                           int32_t *depth_seg, out_t *depth_sigma, int32_t *visit_log, int visit_cap,
                           int32_t *visit_count, int32_t *status, float label_thr, out_t *label_t,
-                          int32_t *label_cell, int32_t *label_step) {
+                          int32_t *label_cell, int32_t *label_step, const int64_t *pixels, int64_t n_pixels) {
     cam_t cam = cam_load(camera);
-    int64_t P = (int64_t)cam.H * cam.W;
+    const int64_t HW = (int64_t)cam.H * cam.W;
+    int64_t P = pixels ? n_pixels : HW;
     v3 o = cam.eye;
     int worst = ORC_OK;
 #pragma omp parallel for schedule(dynamic, 64) reduction(max : worst)
     for (int64_t px = 0; px < P; px++) {
-        int pi = (int)(px / cam.W), pj = (int)(px % cam.W);
+        /* px indexes the outputs; ray is the camera pixel traced (a subset of
+         * the pixels when a list is given) */
+        const int64_t ray = pixels ? pixels[px] : px;
+        if (ray < 0 || ray >= HW) {
+            if (status) status[px] = ORC_ERR_ARGS;
+            if (ORC_ERR_ARGS > worst) worst = ORC_ERR_ARGS;
+            continue;
+        }
+        int pi = (int)(ray / cam.W), pj = (int)(ray % cam.W);
         v3 rd = get_ray_dir(&cam, (real)pi, (real)pj);
         v3 d = vdivs(rd, length(rd));
         v3 rgb = mk(0, 0, 0), nacc = mk(0, 0, 0);
         real log_t = 0;
-        int32_t prim = start_cells ? start_cells[px] : start_idx;
+        int32_t prim = start_cells ? start_cells[ray] : start_idx;
         real pt_near = 0;
         int steps = 0, st = ORC_OK, seg = 0;
         int32_t dseg = -1;
@@ -1625,7 +1634,26 @@ int FN(orc_trace_forward)(const orc_camera *camera, const float *spheres, const 
                           int32_t *visit_count, int32_t *status) {
     return FN(trace_walk)(camera, spheres, nsigmas, sites, rgbs, heights, S, adj, adj_off, adj_diff, start_idx,
                           start_cells, thr, max_steps, depth_quantile, color, log_t_out, depth, normal, depth_seg,
-                          depth_sigma, visit_log, visit_cap, visit_count, status, 0.0f, NULL, NULL, NULL);
+                          depth_sigma, visit_log, visit_cap, visit_count, status, 0.0f, NULL, NULL, NULL, NULL, 0);
+}
+
+/* orc_trace_forward on a list of camera pixels (row-major indices): output
+ * i (and visit_log row i) belongs to pixel pixels[i]; start_cells, when
+ * given, is still indexed by camera pixel.  Test infrastructure for
+ * comparing walks of sampled rays of a large frame. */
+int FN(orc_trace_forward_pixels)(const orc_camera *camera, const float *spheres, const float *nsigmas,
+                                 const float *sites, const float *rgbs, const float *heights, int S,
+                                 const int32_t *adj, const int32_t *adj_off, const uint16_t *adj_diff,
+                                 int32_t start_idx, const int32_t *start_cells, float thr, int max_steps,
+                                 float depth_quantile, const int64_t *pixels, int64_t n_pixels, out_t *color,
+                                 out_t *log_t_out, out_t *depth, out_t *normal, int32_t *depth_seg,
+                                 out_t *depth_sigma, int32_t *visit_log, int visit_cap, int32_t *visit_count,
+                                 int32_t *status) {
+    if (!pixels || n_pixels < 0) return ORC_ERR_ARGS;
+    return FN(trace_walk)(camera, spheres, nsigmas, sites, rgbs, heights, S, adj, adj_off, adj_diff, start_idx,
+                          start_cells, thr, max_steps, depth_quantile, color, log_t_out, depth, normal, depth_seg,
+                          depth_sigma, visit_log, visit_cap, visit_count, status, 0.0f, NULL, NULL, NULL, pixels,
+                          n_pixels);
 }
 
 /* Training labels of the ray-proposal network (no counterpart in the
@@ -1639,7 +1667,7 @@ int FN(orc_trace_labels)(const orc_camera *camera, const float *spheres, const f
                          int32_t *visit_count, int32_t *status) {
     return FN(trace_walk)(camera, spheres, nsigmas, sites, rgbs, heights, S, adj, adj_off, adj_diff, start_idx,
                           start_cells, thr, max_steps, 0.5f, color, NULL, NULL, NULL, NULL, NULL, NULL, 0,
-                          visit_count, status, label_thr, label_t, label_cell, label_step);
+                          visit_count, status, label_thr, label_t, label_cell, label_step, NULL, 0);
 }
 
 /* start cell of benchmark.py:320-324: argmin_i |p_i - eye|^2 - r_i^2 with the
@@ -2165,3 +2193,148 @@ int FN(orc_trace_backward)(const orc_camera *camera, const float *spheres, const
     }
     return ORC_OK;
 }
+
+/* ------------------------------------------------------------------------ */
+/* Čech adjacency (powerfoam/bvh.py:7-69 predicate, build_cech_complex       */
+/* bvh.py:96-123): j is a neighbour of i (j != i) when the AABBs of the two   */
+/* balls overlap (the BVH query) and |c_i - c_j| < r_i + r_j, with c and r    */
+/* recomputed from the AABB as the reference's bvh_query does.  Lists are     */
+/* ascending.  Candidates come from a uniform grid of cell edge >= 2 max r,   */
+/* so every overlapping pair lies in adjacent cells; the grid only prunes, it  */
+/* never decides.  Two calls: adjacency NULL -> counts only (offsets filled,  */
+/* *n_edges set); then with adjacency of *n_edges entries.                   */
+#ifndef PF_F64
+typedef struct { float lo[3], hi[3], c[3], r; } cech_ball;
+
+static cech_ball cech_make(const float *pts, const float *radii, int64_t i) {
+    cech_ball b;
+    float r = radii[i];
+    for (int k = 0; k < 3; k++) {
+        float p = pts[3 * i + k];
+        b.lo[k] = p - r;
+        b.hi[k] = p + r;
+    }
+    for (int k = 0; k < 3; k++) b.c[k] = 0.5f * (b.lo[k] + b.hi[k]);
+    b.r = 0.5f * (b.hi[0] - b.lo[0]);
+    return b;
+}
+
+static int cech_overlap(const cech_ball *a, const cech_ball *b) {
+    for (int k = 0; k < 3; k++)
+        if (!(a->lo[k] <= b->hi[k] && a->hi[k] >= b->lo[k])) return 0;
+    float dx = a->c[0] - b->c[0], dy = a->c[1] - b->c[1], dz = a->c[2] - b->c[2];
+    float d = sqrtf((dx * dx + dy * dy) + dz * dz);
+    return d < a->r + b->r;
+}
+
+static int cmp_i32(const void *a, const void *b) {
+    int32_t x = *(const int32_t *)a, y = *(const int32_t *)b;
+    return (x > y) - (x < y);
+}
+
+int orc_cech_adjacency_f32(const float *pts, const float *radii, int64_t N, int32_t *offsets, int32_t *adjacency,
+                           int64_t *n_edges) {
+    if (N <= 0) {
+        offsets[0] = 0;
+        *n_edges = 0;
+        return ORC_OK;
+    }
+    float lo[3] = {pts[0], pts[1], pts[2]}, hi[3] = {pts[0], pts[1], pts[2]}, rmax = 0.0f;
+    for (int64_t i = 0; i < N; i++) {
+        for (int k = 0; k < 3; k++) {
+            float v = pts[3 * i + k];
+            lo[k] = v < lo[k] ? v : lo[k];
+            hi[k] = v > hi[k] ? v : hi[k];
+        }
+        rmax = radii[i] > rmax ? radii[i] : rmax;
+    }
+    double h = 2.0 * (double)rmax * 1.0001 + 1e-12;
+    int n[3];
+    for (;;) {
+        int ok = 1;
+        for (int k = 0; k < 3; k++) {
+            double c = floor(((double)hi[k] - (double)lo[k]) / h) + 1.0;
+            n[k] = c > 1024.0 ? 1025 : (int)c;
+            if (n[k] > 1024) ok = 0;
+        }
+        if (ok && (int64_t)n[0] * n[1] * n[2] <= (int64_t)1 << 26) break;
+        h *= 1.5;
+    }
+    int64_t ncell = (int64_t)n[0] * n[1] * n[2];
+    int64_t *cell_of = (int64_t *)malloc(sizeof(int64_t) * N);
+    int64_t *start = (int64_t *)calloc(ncell + 1, sizeof(int64_t));
+    int64_t *sorted = (int64_t *)malloc(sizeof(int64_t) * N);
+    if (!cell_of || !start || !sorted) {
+        free(cell_of);
+        free(start);
+        free(sorted);
+        return ORC_ERR_ARGS;
+    }
+    for (int64_t i = 0; i < N; i++) {
+        int64_t cc[3];
+        for (int k = 0; k < 3; k++) {
+            int64_t c = (int64_t)floor(((double)pts[3 * i + k] - (double)lo[k]) / h);
+            cc[k] = c < 0 ? 0 : (c >= n[k] ? n[k] - 1 : c);
+        }
+        cell_of[i] = (cc[2] * n[1] + cc[1]) * n[0] + cc[0];
+        start[cell_of[i] + 1]++;
+    }
+    for (int64_t c = 0; c < ncell; c++) start[c + 1] += start[c];
+    {
+        int64_t *fill = (int64_t *)malloc(sizeof(int64_t) * (ncell + 1));
+        memcpy(fill, start, sizeof(int64_t) * (ncell + 1));
+        for (int64_t i = 0; i < N; i++) sorted[fill[cell_of[i]]++] = i;
+        free(fill);
+    }
+    int32_t *counts = adjacency ? NULL : offsets; /* pass 1 counts into offsets[1..N] */
+    int bad = 0;
+#pragma omp parallel for schedule(dynamic, 256) reduction(| : bad)
+    for (int64_t i = 0; i < N; i++) {
+        cech_ball bi = cech_make(pts, radii, i);
+        int64_t ci = cell_of[i];
+        int64_t cx = ci % n[0], cy = (ci / n[0]) % n[1], cz = ci / ((int64_t)n[0] * n[1]);
+        int64_t pos = adjacency ? offsets[i] : 0;
+        int32_t cnt = 0;
+        for (int64_t z = cz - 1; z <= cz + 1; z++) {
+            if (z < 0 || z >= n[2]) continue;
+            for (int64_t y = cy - 1; y <= cy + 1; y++) {
+                if (y < 0 || y >= n[1]) continue;
+                for (int64_t x = cx - 1; x <= cx + 1; x++) {
+                    if (x < 0 || x >= n[0]) continue;
+                    int64_t c = (z * n[1] + y) * n[0] + x;
+                    for (int64_t s = start[c]; s < start[c + 1]; s++) {
+                        int64_t j = sorted[s];
+                        if (j == i) continue;
+                        cech_ball bj = cech_make(pts, radii, j);
+                        if (cech_overlap(&bi, &bj)) {
+                            if (adjacency) adjacency[pos + cnt] = (int32_t)j;
+                            cnt++;
+                        }
+                    }
+                }
+            }
+        }
+        if (adjacency) {
+            if (cnt != offsets[i + 1] - offsets[i]) bad = 1;
+            qsort(adjacency + pos, (size_t)cnt, sizeof(int32_t), cmp_i32);
+        } else {
+            counts[i + 1] = cnt;
+        }
+    }
+    if (!adjacency) {
+        offsets[0] = 0;
+        int64_t total = 0;
+        for (int64_t i = 0; i < N; i++) {
+            total += offsets[i + 1];
+            offsets[i + 1] = (int32_t)total;
+        }
+        *n_edges = total;
+    } else {
+        *n_edges = offsets[N];
+    }
+    free(cell_of);
+    free(start);
+    free(sorted);
+    return bad ? ORC_ERR_ARGS : ORC_OK;
+}
+#endif

@@ -21,6 +21,7 @@ PF_ERR_ARGS = 3
 PF_ERR_CUDA = 4
 PF_ERR_SEED = 5
 PF_ERR_CELL = 6
+PF_ERR_NONFINITE = 7
 
 _ERR_NAMES = {
     PF_ERR_OVERFLOW: "PF_ERR_OVERFLOW",
@@ -29,6 +30,7 @@ _ERR_NAMES = {
     PF_ERR_CUDA: "PF_ERR_CUDA",
     PF_ERR_SEED: "PF_ERR_SEED",
     PF_ERR_CELL: "PF_ERR_CELL",
+    PF_ERR_NONFINITE: "PF_ERR_NONFINITE",
 }
 
 c_f = ctypes.c_float
@@ -131,7 +133,7 @@ PF_BATCH_ORDER_VIEW = 1
 # name -> argtypes (all return int)
 _SIGS = {
     "pf_abi_version": [],
-    "pf_pack_prims": [c_vp, c_vp, c_vp, c_vp, c_i64, c_vp, c_vp, c_vp],
+    "pf_pack_prims": [c_vp, c_vp, c_vp, c_vp, c_i64, c_vp, c_vp, c_vp, c_vp],
     "pf_bin_workspace_size": [c_i64, c_i64, c_i64, ctypes.POINTER(ctypes.c_size_t)],
     "pf_bin": [ctypes.POINTER(PfCamera), c_i32, c_vp, c_i64, c_vp, ctypes.c_size_t, c_i64, c_vp, c_vp, c_vp, c_vp,
                c_vp, c_vp, c_vp, c_vp],

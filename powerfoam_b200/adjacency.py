@@ -4,14 +4,11 @@
   benchmark.py:296-302, on the GPU.
 * ``start_cell`` -- argmin_i |p_i - eye|^2 - r_i^2, benchmark.py:320-324, on
   the GPU.
-* ``build_power_adjacency`` -- weighted-Delaunay edges through the lower hull
-  of the lifted points (benchmark.py:25-83), via scipy's Qhull on the host, as
-  the reference does; meant for small scenes.
-* ``power_adjacency`` / ``PowerBuilder`` -- the same edges on the GPU by
-  clipping power cells (pf_power_adjacency).
+* ``power_adjacency`` / ``PowerBuilder`` -- the weighted-Delaunay edges of
+  build_power_adjacency (benchmark.py:25-83) on the GPU by clipping power
+  cells (pf_power_adjacency).
 """
 
-import numpy as np
 import torch
 
 from . import _lib
@@ -37,36 +34,6 @@ def start_cell(points, radii, eye, as_tensor=False):
     _lib.call("pf_start_cell", _lib.ptr(points), _lib.ptr(radii), points.shape[0], e, _lib.ptr(ws), ws.numel(),
               _lib.ptr(out), _lib.stream_ptr())
     return out if as_tensor else int(out.item())
-
-
-def build_power_adjacency(points, radii, alpha_complex=False):
-    """Weighted Delaunay adjacency (benchmark.py:25-83): lift (p, |p|^2 - r^2)
-    to 4-D, keep the facets of the convex hull whose normal points down in the
-    lifted coordinate, take the tetrahedra's edges; with ``alpha_complex`` keep
-    only edges whose balls overlap.  Returns (adjacency int32 (E), offsets int32
-    (N+1)) grouped by source vertex, neighbours ascending and without the
-    repeats the reference's lists carry (it runs torch.unique over unordered
-    pairs, so an edge two tetrahedra name in opposite orders appears twice)."""
-    from scipy.spatial import ConvexHull
-
-    p = points.detach().cpu().double()
-    r = radii.detach().cpu().double()
-    lifted = torch.cat([p, (p.norm(dim=-1) ** 2 - r**2)[:, None]], dim=-1).numpy()
-    hull = ConvexHull(lifted)
-    simp = hull.simplices[hull.equations[:, 3] < 0]
-    pairs = np.concatenate([simp[:, [a, b]] for a, b in ((0, 1), (1, 2), (2, 0), (0, 3), (1, 3), (2, 3))], 0)
-    pairs = np.unique(np.sort(pairs, axis=1), axis=0)
-    if alpha_complex:
-        d = np.linalg.norm(p.numpy()[pairs[:, 0]] - p.numpy()[pairs[:, 1]], axis=-1)
-        pairs = pairs[d < (r.numpy()[pairs[:, 0]] + r.numpy()[pairs[:, 1]])]
-    directed = np.concatenate([pairs, pairs[:, ::-1]], 0)
-    order = np.lexsort((directed[:, 1], directed[:, 0]))
-    directed = directed[order]
-    n = points.shape[0]
-    counts = np.bincount(directed[:, 0], minlength=n)
-    offsets = np.concatenate([[0], np.cumsum(counts)]).astype(np.int32)
-    dev = points.device
-    return (torch.from_numpy(directed[:, 1].astype(np.int32)).to(dev), torch.from_numpy(offsets).to(dev))
 
 
 class CechBuilder:

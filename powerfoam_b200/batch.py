@@ -197,7 +197,8 @@ class BatchStep:
     def _pack(self):
         st = _lib.stream_ptr()
         _lib.call("pf_pack_prims", _lib.ptr(self.points), _lib.ptr(self.radii), _lib.ptr(self.normals),
-                  _lib.ptr(self.density), self.n, _lib.ptr(self.spheres), _lib.ptr(self.nsigmas), st)
+                  _lib.ptr(self.density), self.n, _lib.ptr(self.spheres), _lib.ptr(self.nsigmas),
+                  _lib.ptr(self.status), st)
 
     def _bin_all(self):
         st = _lib.stream_ptr()
@@ -285,7 +286,8 @@ class BatchStep:
                 raise _lib.PfError(st, f"view {v}: {n} pairs exceed the capacity {self.capacity[v]}")
         s = int(self.status.item())
         if s != _lib.PF_OK:
-            raise _lib.PfError(s, "batch compositing reported an error")
+            raise _lib.PfError(s, "batch step reported an error (a non-finite primitive attribute, or a "
+                                  "compositing wait limit)")
 
     def pair_counts(self):
         return self.bin_scalars[:, 0].tolist()

@@ -7,7 +7,7 @@ normalize(cross(up, right)).  The open3d export of the reference is not part
 of the rendering path and is not provided.
 """
 
-from dataclasses import dataclass
+from dataclasses import dataclass, field
 
 import math
 
@@ -25,10 +25,17 @@ class TorchCamera:
     height: int
     ray_maps: torch.Tensor = None
     fov_cos_cutoff: float = None
+    _pf: tuple = field(default=None, repr=False, compare=False)
 
     def to_pf(self):
-        """The C-ABI pf_camera struct."""
-        return _lib.make_camera(self.eye, self.right, self.up, self.width, self.height)
+        """The C-ABI pf_camera struct.  Kept while eye / right / up are the
+        same tensors at the same version, so that repeated calls (and CUDA
+        graph capture, where a device-to-host read is not allowed) do not
+        read device tensors back."""
+        key = (self.width, self.height) + tuple((id(t), t._version) for t in (self.eye, self.right, self.up))
+        if self._pf is None or self._pf[0] != key:
+            self._pf = (key, _lib.make_camera(self.eye, self.right, self.up, self.width, self.height))
+        return self._pf[1]
 
     def to_device(self, device):
         dev = torch.device(device)

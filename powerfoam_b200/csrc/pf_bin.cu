@@ -383,11 +383,22 @@ __global__ void tile_len_key_kernel(const int64_t* __restrict__ tile_offsets, in
 
 __global__ void pack_prims_kernel(const float* __restrict__ points, const float* __restrict__ radii,
                                   const float* __restrict__ normals, const float* __restrict__ density, int64_t N,
-                                  float4* __restrict__ spheres, float4* __restrict__ nsigmas) {
+                                  float4* __restrict__ spheres, float4* __restrict__ nsigmas,
+                                  int32_t* __restrict__ status) {
     int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= N) return;
-    if (spheres) spheres[p] = make_float4(points[3 * p], points[3 * p + 1], points[3 * p + 2], radii[p]);
-    if (nsigmas) nsigmas[p] = make_float4(normals[3 * p], normals[3 * p + 1], normals[3 * p + 2], density[p]);
+    bool finite = true;
+    if (spheres) {
+        float4 s = make_float4(points[3 * p], points[3 * p + 1], points[3 * p + 2], radii[p]);
+        spheres[p] = s;
+        finite = isfinite(s.x) && isfinite(s.y) && isfinite(s.z) && isfinite(s.w);
+    }
+    if (nsigmas) {
+        float4 n = make_float4(normals[3 * p], normals[3 * p + 1], normals[3 * p + 2], density[p]);
+        nsigmas[p] = n;
+        finite = finite && isfinite(n.x) && isfinite(n.y) && isfinite(n.z) && isfinite(n.w);
+    }
+    if (status && !finite) atomicMax(status, PF_ERR_NONFINITE);
 }
 
 // ---------------------------------------------------------------------------
@@ -446,14 +457,14 @@ extern "C" int pf_bin_workspace_size(int64_t n_prims, int64_t pair_capacity, int
 }
 
 extern "C" int pf_pack_prims(const float* points, const float* radii, const float* normals, const float* density,
-                             int64_t n_prims, float* spheres, float* nsigmas, void* stream) {
+                             int64_t n_prims, float* spheres, float* nsigmas, int32_t* status, void* stream) {
     if (n_prims < 0) return pf_fail(PF_ERR_ARGS, "pf_pack_prims: n_prims < 0");
     if (n_prims == 0) return PF_OK;
     if ((spheres && (!points || !radii)) || (nsigmas && (!normals || !density)))
         return pf_fail(PF_ERR_ARGS, "pf_pack_prims: missing input");
     cudaStream_t st = (cudaStream_t)stream;
     pack_prims_kernel<<<(unsigned)((n_prims + 255) / 256), 256, 0, st>>>(points, radii, normals, density, n_prims,
-                                                                        (float4*)spheres, (float4*)nsigmas);
+                                                                        (float4*)spheres, (float4*)nsigmas, status);
     return pf_check_launch("pf_pack_prims");
 }
 

@@ -70,7 +70,11 @@ def _f32(t, name):
 
 
 class TileBins:
-    """Result of binning: per-tile offsets (T+1, int64) and sorted primitive ids."""
+    """Result of binning: per-tile offsets (T+1, int64) and sorted primitive
+    ids.  ``n_pairs`` is an int after a synchronous binning and a device
+    scalar (int64) after a sync-free one, whose ``tile_prims`` / ``sort_keys``
+    then keep the buffer's full capacity (only the first n_pairs entries are
+    meaningful; the kernels read the lists through ``tile_offsets``)."""
 
     def __init__(self, tile_offsets, tile_prims, n_pairs, prim_visible, sort_keys=None, tile_order=None):
         self.tile_order = tile_order
@@ -84,13 +88,20 @@ class TileBins:
 class Binner:
     """Owns the binning workspace and the pair capacity estimate.
 
-    pf_bin never waits on the host; like the reference (offsets[-1].item(),
-    rasterize.py:1714) this wrapper reads the pair count once per call and
-    re-bins with a larger capacity if the estimate was too small."""
+    Synchronous (``sync=True``, the reference's behaviour: offsets[-1].item(),
+    rasterize.py:1714): one host read of the pair count and the status word
+    per call, re-binning with a larger capacity when the estimate was too
+    small, and PfError(PF_ERR_NONFINITE) when the status reports a NaN or
+    infinite attribute.  Sync-free (``sync=False``): the first call sizes the
+    pair buffer with one read (1.25x headroom, a power of two); later calls
+    read nothing back, so they can be captured in a CUDA graph; an overflow
+    then empties the tile lists and raises PF_ERR_OVERFLOW in the caller's
+    persistent ``status`` word, which the caller checks when it chooses."""
 
-    def __init__(self, device):
+    def __init__(self, device, headroom=1.25):
         self.device = torch.device(device)
         self.capacity = 0
+        self.headroom = headroom
         self.ws = None
 
     def _ensure(self, n_prims, cap, num_tiles):
@@ -106,42 +117,68 @@ class Binner:
         if self.ws is None or self.ws.numel() < nbytes.value:
             self.ws = torch.empty(max(nbytes.value, 256), dtype=torch.uint8, device=self.device)
 
+    def _launch(self, cam_pf, tile_width, spheres, n_prims, num_tiles, cap, return_keys, ray_maps, status):
+        if ray_maps is None:
+            self._ensure(n_prims, cap, num_tiles)
+        else:
+            self._ensure_generic(n_prims, cap, cam_pf, tile_width)
+        tile_offsets = torch.empty(num_tiles + 1, dtype=torch.int64, device=self.device)
+        tile_order = torch.empty(num_tiles, dtype=torch.int32, device=self.device)
+        tile_prims = torch.empty(max(cap, 1), dtype=torch.int32, device=self.device)
+        keys = torch.empty(max(cap, 1), dtype=torch.int64, device=self.device) if return_keys else None
+        visible = torch.empty(n_prims, dtype=torch.uint8, device=self.device)
+        n_pairs = torch.zeros(1, dtype=torch.int64, device=self.device)
+        outs = (_lib.ptr(self.ws), self.ws.numel(), cap, _lib.ptr(tile_offsets), _lib.ptr(tile_prims), _lib.ptr(keys),
+                _lib.ptr(visible), _lib.ptr(tile_order), _lib.ptr(n_pairs), _lib.ptr(status), _lib.stream_ptr())
+        if ray_maps is None:
+            _lib.call("pf_bin", _lib.ctypes.byref(cam_pf), tile_width, _lib.ptr(spheres), n_prims, *outs)
+        else:
+            _lib.call("pf_bin_generic", _lib.ctypes.byref(cam_pf), _lib.ptr(ray_maps), tile_width,
+                      _lib.ptr(spheres), n_prims, *outs)
+        return tile_offsets, tile_order, tile_prims, keys, visible, n_pairs
+
     def __call__(self, cam_pf, tile_width, spheres, n_prims, num_tiles, return_keys=False, capacity=None,
-                 ray_maps=None):
-        """ray_maps (H,W,6) f32: bin a generic camera through its ray cones."""
+                 ray_maps=None, status=None, sync=True):
+        """ray_maps (H,W,6) f32: bin a generic camera through its ray cones.
+        status: device int32 word the kernels raise (pf_pack_prims' non-finite
+        flag may already be in it); a fresh one when None."""
+        own_status = status is None
+        if own_status:
+            status = torch.zeros(1, dtype=torch.int32, device=self.device)
+        if not sync and self.capacity > 0 and capacity is None:
+            t_off, t_ord, t_prims, keys, vis, n_pairs = self._launch(cam_pf, tile_width, spheres, n_prims, num_tiles,
+                                                                     self.capacity, return_keys, ray_maps, status)
+            return TileBins(t_off, t_prims, n_pairs[0], vis.bool(), keys, t_ord)
         cap = capacity if capacity is not None else max(self.capacity, 4 * n_prims, 1 << 14)
         while True:
-            if ray_maps is None:
-                self._ensure(n_prims, cap, num_tiles)
-            else:
-                self._ensure_generic(n_prims, cap, cam_pf, tile_width)
-            tile_offsets = torch.empty(num_tiles + 1, dtype=torch.int64, device=self.device)
-            tile_order = torch.empty(num_tiles, dtype=torch.int32, device=self.device)
-            tile_prims = torch.empty(max(cap, 1), dtype=torch.int32, device=self.device)
-            keys = torch.empty(max(cap, 1), dtype=torch.int64, device=self.device) if return_keys else None
-            visible = torch.empty(n_prims, dtype=torch.uint8, device=self.device)
-            scalars = torch.zeros(2, dtype=torch.int64, device=self.device)  # n_pairs, status
-            status = scalars[1:].view(torch.int32)[:1]
-            outs = (_lib.ptr(self.ws), self.ws.numel(), cap, _lib.ptr(tile_offsets), _lib.ptr(tile_prims),
-                    _lib.ptr(keys), _lib.ptr(visible), _lib.ptr(tile_order), _lib.ptr(scalars[:1]), _lib.ptr(status),
-                    _lib.stream_ptr())
-            if ray_maps is None:
-                _lib.call("pf_bin", _lib.ctypes.byref(cam_pf), tile_width, _lib.ptr(spheres), n_prims, *outs)
-            else:
-                _lib.call("pf_bin_generic", _lib.ctypes.byref(cam_pf), _lib.ptr(ray_maps), tile_width,
-                          _lib.ptr(spheres), n_prims, *outs)
-            n = int(scalars[0].item())
+            t_off, t_ord, t_prims, keys, vis, n_pairs = self._launch(cam_pf, tile_width, spheres, n_prims, num_tiles,
+                                                                     cap, return_keys, ray_maps, status)
+            n, st = (int(v) for v in torch.stack([n_pairs[0], status[0].long()]).tolist())
+            if st == _lib.PF_ERR_NONFINITE:
+                raise _lib.PfError(st, "a primitive attribute is NaN or infinite")
             if n <= cap:
                 break
-            cap = 1 << (int(n * 1.25) - 1).bit_length()
+            cap = 1 << (int(n * self.headroom) - 1).bit_length()
+            status.zero_()
         self.capacity = max(self.capacity, cap)
-        return TileBins(tile_offsets, tile_prims[:n], n, visible.bool(), keys[:n] if return_keys else None,
-                        tile_order)
+        if not sync:  # sized: later calls read nothing back
+            self.capacity = max(self.capacity, 1 << (int(max(n, 1) * self.headroom) - 1).bit_length())
+        return TileBins(t_off, t_prims[:n], n, vis.bool(), keys[:n] if return_keys else None, t_ord)
 
 
 class Rasterizer:
-    def __init__(self, args, device, attr_dtype="float", tile_width=TILE_WIDTH):
+    """``host_sync`` (default True) keeps the reference's one host read per
+    call (the pair count, rasterize.py:1714), here together with the status
+    word, so overflow is handled and non-finite attributes raise at once.
+    With ``host_sync=False`` only the first call reads back (to size the pair
+    buffer); later forward / backward calls never wait on the host and can be
+    captured in a CUDA graph, and overflow (PF_ERR_OVERFLOW) or non-finite
+    attributes (PF_ERR_NONFINITE) accumulate in the device word ``status``,
+    raised by ``check()``."""
+
+    def __init__(self, args, device, attr_dtype="float", tile_width=TILE_WIDTH, host_sync=True):
         self.device = torch.device(device)
+        self.host_sync = bool(host_sync)
         self.args = args
         if attr_dtype == "float":
             self.tscalar = torch.float32
@@ -162,23 +199,39 @@ class Rasterizer:
         # device scratch of the compositing kernels' tile work queue; one
         # Rasterizer serves one stream at a time
         self.scratch = torch.zeros(64, dtype=torch.int32, device=self.device)
+        # persistent device status word of the sync-free mode (see class docstring)
+        self.status = torch.zeros(1, dtype=torch.int32, device=self.device)
         _lib.load()
+
+    def check(self):
+        """Raise PfError if a sync-free call reported overflow or non-finite
+        attributes since the last check (one host read); clears the word."""
+        st = int(self.status.item())
+        if st != _lib.PF_OK:
+            self.status.zero_()
+            raise _lib.PfError(st, "a sync-free rasterizer call overflowed its pair buffer (re-run it: the "
+                                   "capacity is re-sized) or met a non-finite attribute")
+        return True
+
+    def _call_status(self):
+        return torch.zeros(1, dtype=torch.int32, device=self.device) if self.host_sync else self.status
 
     # ------------------------------------------------------------------
     def num_tiles(self, camera):
         tw = self.tile_width
         return (1 + (camera.height - 1) // tw) * (1 + (camera.width - 1) // tw)
 
-    def pack(self, points, radii, normals=None, density=None):
+    def pack(self, points, radii, normals=None, density=None, status=None):
         """(N,4) spheres (centre, radius) and (N,4) normal+density, as
-        rasterize.py:1619-1620 builds them."""
+        rasterize.py:1619-1620 builds them; a NaN or infinite value raises
+        PF_ERR_NONFINITE in ``status`` (device int32, optional)."""
         n = points.shape[0]
         spheres = torch.empty((n, 4), dtype=torch.float32, device=self.device)
         nsig = torch.empty((n, 4), dtype=torch.float32, device=self.device) if normals is not None else None
         _lib.call("pf_pack_prims", _lib.ptr(_f32(points, "points")), _lib.ptr(_f32(radii, "radii")),
                   _lib.ptr(None if normals is None else _f32(normals, "normals")),
                   _lib.ptr(None if density is None else _f32(density, "density")), n, _lib.ptr(spheres),
-                  _lib.ptr(nsig), _lib.stream_ptr())
+                  _lib.ptr(nsig), _lib.ptr(status), _lib.stream_ptr())
         return spheres, nsig
 
     def ray_maps(self, camera):
@@ -193,11 +246,11 @@ class Rasterizer:
             raise ValueError("Only CUDA tensors are supported as inputs")
         return rm.detach().to(torch.float32).contiguous()
 
-    def bin(self, camera, spheres, return_keys=False, ray_maps=None):
+    def bin(self, camera, spheres, return_keys=False, ray_maps=None, status=None):
         if self.generic and ray_maps is None:
             ray_maps = self.ray_maps(camera)
         return self.binner(camera.to_pf(), self.tile_width, spheres, spheres.shape[0], self.num_tiles(camera),
-                           return_keys=return_keys, ray_maps=ray_maps)
+                           return_keys=return_keys, ray_maps=ray_maps, status=status, sync=self.host_sync)
 
     def prefetch_adjacency(self, spheres, adjacency, adjacency_offsets):
         """(E,4) float16 (c_j - c_i, r_j): rasterize.py:580-606."""
@@ -224,7 +277,7 @@ class Rasterizer:
         inp.adjacency_offsets = _lib.ptr(adjacency_offsets)
         inp.adjacency_diff = _lib.ptr(adj_diff)
         inp.tile_offsets = _lib.ptr(bins.tile_offsets)
-        inp.tile_prims = _lib.ptr(bins.tile_prims) if bins.n_pairs > 0 else _lib.ptr(bins.tile_offsets)
+        inp.tile_prims = _lib.ptr(bins.tile_prims) if bins.tile_prims.numel() > 0 else _lib.ptr(bins.tile_offsets)
         inp.depth_quantiles = _lib.ptr(depth_quantiles)
         inp.n_quantiles = 0 if depth_quantiles is None else depth_quantiles.shape[-1]
         inp.ray_gt = _lib.ptr(ray_gt)
@@ -246,7 +299,8 @@ class Rasterizer:
         H, W = camera.height, camera.width
         dev = self.device
         n = points.shape[0]
-        spheres, nsig = self.pack(points.detach(), radii.detach(), normals.detach(), density.detach())
+        status = self._call_status()
+        spheres, nsig = self.pack(points.detach(), radii.detach(), normals.detach(), density.detach(), status)
         sites = _f32(texel_sites.detach(), "texel_sites")
         rgb = _f32(texel_rgb.detach(), "texel_rgb")
         height = _f32(texel_height.detach(), "texel_height")
@@ -256,7 +310,7 @@ class Rasterizer:
         gt = None if ray_gt is None else _f32(ray_gt.detach(), "ray_gt")
 
         ray_maps = self.ray_maps(camera)
-        bins = self.bin(camera, spheres, ray_maps=ray_maps)
+        bins = self.bin(camera, spheres, ray_maps=ray_maps, status=status)
         adj_diff = self.prefetch_adjacency(spheres, adjacency, adjacency_offsets)
 
         color = torch.empty((H, W, 3), dtype=torch.float32, device=dev)
@@ -342,12 +396,13 @@ class Rasterizer:
         """Forward colour only, (dc, dpm)-encoded neighbours, attributes in
         attr_dtype (rasterize.py:1982-2131)."""
         H, W = camera.height, camera.width
-        spheres, _ = self.pack(points.float().contiguous(), radii.float().contiguous())
+        status = self._call_status()
+        spheres, _ = self.pack(points.float().contiguous(), radii.float().contiguous(), status=status)
         nsig = torch.cat([normals, density[:, None]], dim=-1).to(self.tscalar).contiguous()
         sites = texel_sites.to(self.tscalar).contiguous()
         rgb = texel_rgb.to(self.tscalar).contiguous()
         height = texel_height.to(self.tscalar).contiguous()
-        bins = self.bin(camera, spheres)
+        bins = self.bin(camera, spheres, status=status)
         color = torch.empty((H, W, 3), dtype=torch.float32, device=self.device)
         inp = self._inputs(camera, spheres, nsig, sites, rgb, height, adjacency.to(torch.int32).contiguous(),
                            adjacency_offsets.to(torch.int32).contiguous(), adjacency_diff.contiguous(), bins,
@@ -363,14 +418,15 @@ class Rasterizer:
             vis_options = VisOptions()
         H, W = camera.height, camera.width
         dev = self.device
-        spheres, _ = self.pack(points.float().contiguous(), radii.float().contiguous())
+        status = self._call_status()
+        spheres, _ = self.pack(points.float().contiguous(), radii.float().contiguous(), status=status)
         nsig = torch.cat([normals, density[:, None]], dim=-1).to(self.tscalar).contiguous()
         sites = texel_sites.to(self.tscalar).contiguous()
         rgb = texel_rgb.to(self.tscalar).contiguous()
         height = texel_height.to(self.tscalar).contiguous()
         adjacency = adjacency.to(torch.int32).contiguous()
         adjacency_offsets = adjacency_offsets.to(torch.int32).contiguous()
-        bins = self.bin(camera, spheres)
+        bins = self.bin(camera, spheres, status=status)
         adj_diff = self.prefetch_adjacency(spheres, adjacency, adjacency_offsets)
         color = torch.empty((H, W, 3), dtype=torch.float32, device=dev)
         depth = torch.empty((H, W), dtype=torch.float32, device=dev)

@@ -167,3 +167,38 @@ CONFIGS = {
     "trace6m": dict(n=6291456, seed=4, mixture=64, sigma=0.1, r_range=(0.001, 0.01), width=2048, height=1536,
                     vfov=50.0),
 }
+
+
+def raster_workload(name="raster1m", device="cuda", view=0):
+    """The rasterizer workload ``name`` of CONFIGS: scene, the orbit camera
+    of view ``view`` (seed 100 + view), its Čech adjacency (built on the
+    device) and the seeded uniform target image (host, seed 200 + view).
+    Returns (cfg, scene, camera, adjacency, adjacency_offsets, target)."""
+    from .adjacency import CechBuilder
+
+    cfg = CONFIGS[name]
+    scene = make_scene(cfg["n"], seed=cfg["seed"], mixture=cfg["mixture"], sigma=cfg.get("sigma", 0.15),
+                       r_range=cfg["r_range"], device=device)
+    cam = orbit_camera(100 + view, cfg["width"], cfg["height"], cfg["vfov"], device=device)
+    adj, adj_off = CechBuilder(device)(scene["points"], scene["radii"])
+    g = torch.Generator().manual_seed(200 + view)
+    target = torch.rand((cfg["height"], cfg["width"], 3), generator=g)
+    return cfg, scene, cam, adj, adj_off, target
+
+
+def trace_workload(name="trace1m", device="cuda"):
+    """The tracer workload: scene, its power-diagram adjacency (built on the
+    device), the (c_j - c_i, pm_j - pm_i) neighbour encoding, the orbit
+    camera (seed 2) and the camera's start cell (benchmark.py:320-324).
+    Returns (cfg, scene, camera, adjacency, adjacency_offsets, adj_diff_pm,
+    start)."""
+    from .adjacency import power_adjacency, power_adjacency_diff, start_cell
+
+    cfg = CONFIGS[name]
+    sc = make_scene(cfg["n"], seed=cfg["seed"], mixture=cfg["mixture"], sigma=cfg["sigma"], r_range=cfg["r_range"],
+                    device=device)
+    adj, off = power_adjacency(sc["points"], sc["radii"])
+    pm = power_adjacency_diff(sc["points"], sc["radii"], adj, off)
+    cam = orbit_camera(2, cfg["width"], cfg["height"], cfg["vfov"], device=device)
+    st = start_cell(sc["points"], sc["radii"], cam.eye)
+    return cfg, sc, cam, adj, off, pm, st

@@ -1,12 +1,12 @@
 """Generate golden vectors by executing the reference's own kernel source.
 
 Imports powerfoam/rasterize.py, raytrace.py, geometry.py and color_fn.py (and
-functions of benchmark.py) from the reference
-checkout (default /root/reference, or $PF_REFERENCE) with warp replaced by
-tests/golden/warp_shim.py, runs the kernels on small seeded scenes, and writes
-tests/golden/*.npz.  Run from the repository root:
+functions of benchmark.py) from the reference checkout named by
+$PF_REFERENCE (required) with warp replaced by tests/golden/warp_shim.py, runs
+the kernels on small seeded scenes, and writes tests/golden/*.npz.  Run from
+the repository root:
 
-    python tests/golden/make_golden.py
+    PF_REFERENCE=<path of the powerfoam checkout> python tests/golden/make_golden.py
 
 The fixtures are committed; tests read only the .npz files.
 """
@@ -20,7 +20,9 @@ import types
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = os.environ.get("PF_REFERENCE", "/root/reference")
+REF = os.environ.get("PF_REFERENCE")
+if not REF or not os.path.isdir(os.path.join(REF, "powerfoam")):
+    sys.exit("set PF_REFERENCE to the reference checkout (the directory holding powerfoam/ and benchmark.py)")
 sys.path.insert(0, HERE)
 import warp_shim  # noqa: E402
 

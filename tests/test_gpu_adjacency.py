@@ -63,7 +63,8 @@ def _power_case(seed, n, mode):
                                                (2, 5000, "mix", False), (3, 20000, "mix", True),
                                                (4, 3000, "hidden", False), (5, 6, "uniform", False)])
 def test_power_adjacency_matches_hull(seed, n, mode, alpha):
-    from powerfoam_b200.adjacency import PowerBuilder, build_power_adjacency
+    from oracle.power_hull import build_power_adjacency
+    from powerfoam_b200.adjacency import PowerBuilder
 
     pts, radii = _power_case(seed, n, mode)
     a_ref, o_ref = build_power_adjacency(torch.from_numpy(pts), torch.from_numpy(radii), alpha_complex=alpha)
@@ -78,7 +79,8 @@ def test_power_adjacency_synthetic_scene_matches_hull():
     """A 200,000-primitive mixture scene of the benchmark recipe (clusters,
     uniform background, radii spread tenfold)."""
     from powerfoam_b200 import synthetic
-    from powerfoam_b200.adjacency import build_power_adjacency, power_adjacency
+    from oracle.power_hull import build_power_adjacency
+    from powerfoam_b200.adjacency import power_adjacency
 
     n = 200000
     s = (1048576 / n) ** (1 / 3)
@@ -115,7 +117,8 @@ def test_power_adjacency_golden_trace_scene(golden):
 
 def test_power_adjacency_capacity_growth_and_reuse():
     from powerfoam_b200 import _lib
-    from powerfoam_b200.adjacency import PowerBuilder, build_power_adjacency
+    from oracle.power_hull import build_power_adjacency
+    from powerfoam_b200.adjacency import PowerBuilder
 
     pts, radii = _power_case(6, 1500, "uniform")
     a_ref, o_ref = build_power_adjacency(torch.from_numpy(pts), torch.from_numpy(radii))

@@ -14,7 +14,8 @@ import torch
 from oracle import mlp_oracle as mo
 from oracle import oracle as orc
 from powerfoam_b200 import _lib
-from powerfoam_b200.adjacency import build_power_adjacency, power_adjacency_diff, start_cell
+from oracle.power_hull import build_power_adjacency
+from powerfoam_b200.adjacency import power_adjacency_diff, start_cell
 from powerfoam_b200.proposal import (CellLocator, ProposalNet, SeededTracer, camera_rays, make_training_rays,
                                      trace_labels)
 from powerfoam_b200.raytrace import RayTracer

@@ -301,3 +301,104 @@ def test_nonfinite_gradients_are_zeroed():
     (out[0].sum() * 1e38 * 1e38).backward()
     for k in ["points", "radii", "density", "normals", "texel_sites", "texel_rgb", "texel_height"]:
         assert torch.isfinite(t[k].grad).all(), k
+
+
+def _params(sc):
+    return {k: to_t(v).requires_grad_(True) for k, v in sc.items()}
+
+
+def _render_grads(R, cam, t, adj, adj_off, w):
+    out = R.forward(cam, None, t["points"], t["radii"], t["density"], t["normals"], t["texel_sites"], t["texel_rgb"],
+                    t["texel_height"], adj, adj_off, None, False)
+    loss = (out[0] * w[0]).sum() + (out[1] * w[1]).sum() + (out[3] * w[2]).sum()
+    names = ["points", "radii", "density", "normals", "texel_sites", "texel_rgb", "texel_height"]
+    grads = torch.autograd.grad(loss, [t[k] for k in names])
+    return (out[0], out[1], out[2], out[3]), dict(zip(names, grads))
+
+
+def test_sync_free_forward_backward_graph_replay():
+    """host_sync=False: after the sizing call nothing is read back, so the
+    whole forward + adjoint is captured in one CUDA graph; replays (also
+    after the inputs are updated in place) give the eager images bit for bit
+    and the eager gradients up to the order of float atomics."""
+    sc = np_scene(61, 900, -0.6, 0.6, 0.03, 0.15)
+    cam = torch_cam(np_camera((0.2, 0.3, 2.2), (0, 0, 0), 96, 72, 55.0))
+    adj, adj_off = (to_t(a) for a in cech_np(sc["points"], sc["radii"]))
+    rng = np.random.default_rng(9)
+    w = [to_t(rng.standard_normal(s).astype(np.float32)) for s in ((72, 96, 3), (72, 96), (72, 96, 3))]
+    R = Rasterizer(Args(), "cuda", host_sync=False)
+    t = _params(sc)
+    side = torch.cuda.Stream()
+    side.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(side):
+        for _ in range(3):
+            _render_grads(R, cam, t, adj, adj_off, w)
+    torch.cuda.current_stream().wait_stream(side)
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        imgs, grads = _render_grads(R, cam, t, adj, adj_off, w)
+    for step in range(2):
+        if step == 1:
+            with torch.no_grad():
+                t["points"].add_(to_t(rng.normal(0, 2e-3, sc["points"].shape).astype(np.float32)))
+                t["density"].mul_(1.1)
+        g.replay()
+        torch.cuda.synchronize()
+        ref_imgs, ref_grads = _render_grads(Rasterizer(Args(), "cuda"), cam, t, adj, adj_off, w)
+        for a, b in zip(imgs, ref_imgs):
+            assert torch.equal(a, b)
+        for k in ref_grads:
+            assert_close_rel(grads[k].cpu().numpy(), ref_grads[k].cpu().numpy(), 1e-5, k)
+    assert R.check()
+
+
+def test_sync_free_overflow_is_reported_by_check():
+    sc = np_scene(62, 800, -0.8, 0.8, 0.05, 0.2)
+    cam = torch_cam(np_camera((0.0, 0.2, 2.4), (0, 0, 0), 64, 48, 55.0))
+    adj, adj_off = (to_t(a) for a in cech_np(sc["points"], sc["radii"]))
+    R = Rasterizer(Args(), "cuda", host_sync=False)
+    t = {k: to_t(v) for k, v in sc.items()}
+    args = (cam, None, t["points"], t["radii"], t["density"], t["normals"], t["texel_sites"], t["texel_rgb"],
+            t["texel_height"], adj, adj_off, None, False)
+    ref = R.forward(*args)[0]
+    assert R.check()
+    R.binner.capacity = 64  # far too small: the lists are emptied and the status word raised
+    out = R.forward(*args)[0]
+    assert float(out.abs().max()) == 0.0
+    with pytest.raises(_lib.PfError) as e:
+        R.check()
+    assert e.value.code == _lib.PF_ERR_OVERFLOW
+    R.binner.capacity = 0  # re-size on the next call
+    assert torch.equal(R.forward(*args)[0], ref)
+    assert R.check()
+
+
+@pytest.mark.parametrize("field", ["radii", "points", "density", "normals"])
+def test_nonfinite_attribute_raises(field):
+    """A NaN / infinite primitive attribute is reported as PF_ERR_NONFINITE:
+    at once with the default host read, by check() in the sync-free mode.
+    Every loop of the kernels is bounded by integer list lengths, so the
+    non-finite primitive only makes its own pixels non-finite."""
+    sc = np_scene(63, 300, -0.6, 0.6, 0.03, 0.15)
+    bad = {k: v.copy() for k, v in sc.items()}
+    bad[field].reshape(bad[field].shape[0], -1)[17, 0] = np.nan if field != "density" else np.inf
+    cam = torch_cam(np_camera((0.0, 0.2, 2.2), (0, 0, 0), 40, 30, 55.0))
+    adj, adj_off = (to_t(a) for a in cech_np(sc["points"], sc["radii"]))
+
+    def args(s):
+        t = {k: to_t(v) for k, v in s.items()}
+        return (cam, None, t["points"], t["radii"], t["density"], t["normals"], t["texel_sites"], t["texel_rgb"],
+                t["texel_height"], adj, adj_off, None, False)
+
+    with pytest.raises(_lib.PfError) as e:
+        Rasterizer(Args(), "cuda").forward(*args(bad))
+    assert e.value.code == _lib.PF_ERR_NONFINITE
+    R = Rasterizer(Args(), "cuda", host_sync=False)
+    R.forward(*args(sc))  # the sizing call
+    assert R.check()
+    R.forward(*args(bad))
+    with pytest.raises(_lib.PfError) as e:
+        R.check()
+    assert e.value.code == _lib.PF_ERR_NONFINITE
+    R.forward(*args(sc))
+    assert R.check()

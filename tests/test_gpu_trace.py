@@ -8,7 +8,8 @@ import torch
 
 from oracle import oracle as orc
 from powerfoam_b200 import _lib
-from powerfoam_b200.adjacency import build_power_adjacency, power_adjacency_diff, start_cell
+from oracle.power_hull import build_power_adjacency
+from powerfoam_b200.adjacency import power_adjacency_diff, start_cell
 from powerfoam_b200.raytrace import RayTracer
 from tests.helpers import max_abs, np_camera, np_scene, orc_cam, packed, to_t, torch_cam
 

@@ -19,7 +19,7 @@ F32 = np.float32
 def _power_adj(sc):
     import torch
 
-    from powerfoam_b200.adjacency import build_power_adjacency
+    from oracle.power_hull import build_power_adjacency
 
     a, o = build_power_adjacency(torch.from_numpy(sc["points"]), torch.from_numpy(sc["radii"]))
     return a.numpy(), o.numpy()
