@@ -17,9 +17,10 @@ view of the same scene and the per-primitive gradients are summed across ranks
 with one NCCL all-reduce per step (data-parallel over views): weak scaling.
 
 --impl reference times the reference algorithm on the host cores: the CPU
-restatement of the reference kernels (oracle/, OpenMP), on a bounded sample of
-the same frame (binning of every primitive plus compositing forward + adjoint
-of a random sample of tiles), scaled to frames/s.
+restatement of the reference kernels (oracle/, OpenMP; the reference's Warp
+kernels are not importable here), inputs built on the host, each step 1/16 of
+the frame's work (binning of every 16th primitive, forward + adjoint of every
+16th tile), frames/s = frames of work done / time.
 """
 
 import argparse
@@ -38,7 +39,7 @@ sys.path.insert(0, ROOT)
 import numpy as np  # noqa: E402
 import torch  # noqa: E402
 
-from powerfoam_b200.multiview import GradReducer, allreduce_, max_over_ranks, shard_views  # noqa: E402
+from powerfoam_b200.multiview import GradBuffer, max_over_ranks, raster_fields, shard_views  # noqa: E402
 
 METRIC = "fwd+bwd ms/iter, FPS @1M prims 1080p; proposal vs plain trace @≥50dB PSNR"
 UNIT = "frames/s (fwd+bwd iterations/s)"
@@ -59,7 +60,7 @@ def parse():
                    "(power-diagram adjacency build), fisheye1m (raster1m through a generic fisheye camera), color1m "
                    "(spherical-Voronoi texel colour forward + adjoint) or proposal "
                    "(proposal-seeded vs plain cell walk)")
-    p.add_argument("--cpu-sample-tiles", type=int, default=0, help="tiles composited by the CPU baseline")
+    p.add_argument("--cpu-slices", type=int, default=4, help="slices (1/16 of a frame each) the CPU baseline times")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-autotune", action="store_true", help="batch workloads: use --tile, chunk 1")
     p.add_argument("--proposal-prims", type=int, default=0,
@@ -67,19 +68,17 @@ def parse():
     return p.parse_args()
 
 
-def load_traffic(kernel, workload):
-    """DRAM bytes (read + write) per launch of `kernel` from the committed ncu
-    summary of the same workload, or None."""
-    path = os.path.join(ROOT, "profiles", f"ncu_raster_composite_{workload}.md")
-    try:
-        for line in open(path):
-            if line.startswith("traffic_bytes_per_launch:"):
-                _, name, val = line.split()
-                if name == kernel:
-                    return int(val)
-    except OSError:
-        pass
-    return None
+# DRAM bytes (read + write) per launch of the dominant kernel from one ncu
+# capture of the same command (dram__bytes_read.sum + dram__bytes_write.sum),
+# with the summary that records it; None where no capture of the current
+# kernel exists.
+TRAFFIC = {
+    ("raster1m", "pf_raster_backward"): None,
+}
+
+
+def capture_traffic(kernel, workload):
+    return TRAFFIC.get((workload, kernel))
 
 
 def load_peaks():
@@ -171,6 +170,9 @@ def make_step(R, scene, cam, adj, adj_off, target_dev, world):
 
     names = ["points", "radii", "density", "normals", "texel_sites", "texel_height"]
     params = {k: scene[k].clone().requires_grad_(True) for k in names}
+    if world > 1:  # the adjoint writes into one flat buffer, all-reduced in place
+        R.grad_buffer = GradBuffer(raster_fields(scene["points"].shape[0], scene["texel_sites"].shape[1]),
+                                   scene["points"].device, world=world)
 
     def step(target=None, ready=None):
         t = target_dev if target is None else target
@@ -184,7 +186,7 @@ def make_step(R, scene, cam, adj, adj_off, target_dev, world):
         loss = ((out[0] - t) ** 2).sum()
         loss.backward()
         if world > 1:
-            allreduce_([params[k].grad for k in names] + [rgb.grad])
+            R.grad_buffer.allreduce()
         return loss
 
     return step, params
@@ -215,66 +217,115 @@ def algorithmic_bytes(stats, H, W):
     return dict(fwd=fwd, bwd=bwd, V=V, U=U, deg=deg, pairs=bins.n_pairs, T=T)
 
 
-def cpu_baseline(cfg, scene, cam, adj, adj_off, target, sample_tiles, tile=8):
-    """The oracle (CPU restatement, OpenMP) on a bounded sample of the frame:
-    binning of every primitive + forward/adjoint compositing of a random
-    sample of tiles; returns frames/s scaled to the whole frame."""
-    from oracle import oracle as orc
-    from powerfoam_b200 import synthetic
+def cpu_model():
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
 
-    rgb = synthetic.texel_rgb(scene, cam).cpu().numpy()
-    sc = {k: v.cpu().numpy() for k, v in scene.items()}
-    adj_np, off_np = adj.cpu().numpy(), adj_off.cpu().numpy()
-    oc = orc.camera(cam.eye.cpu().numpy(), cam.right.cpu().numpy(), cam.up.cpu().numpy(), cam.width, cam.height)
-    sph = np.concatenate([sc["points"], sc["radii"][:, None]], -1).astype(np.float32)
-    nsig = np.concatenate([sc["normals"], sc["density"][:, None]], -1).astype(np.float32)
-    rgbh = np.concatenate([rgb, sc["texel_height"][..., None]], -1).astype(np.float32)
-    t0 = time.perf_counter()
-    keys, prims, offs, _ = orc.bin(oc, sph, tile)
-    ad = orc.prefetch_adjacency(sph, adj_np, off_np)
-    t_bin = time.perf_counter() - t0
-    T = offs.shape[0] - 1
-    rng = np.random.default_rng(0)
-    sample = np.sort(rng.choice(T, size=min(sample_tiles, T), replace=False))
-    new_prims = np.concatenate([prims[offs[t]:offs[t + 1]] for t in sample]) if len(sample) else prims[:0]
-    lens = np.zeros(T, np.int64)
-    lens[sample] = offs[sample + 1] - offs[sample]
-    new_offs = np.concatenate([[0], np.cumsum(lens)]).astype(np.int64)
-    t1 = time.perf_counter()
-    o = orc.raster_forward(oc, tile, sph, nsig, sc["texel_sites"], rgbh, adj_np, off_np, ad, new_offs, new_prims)
-    g_c = (2 * (o["color"] - target.numpy())).astype(np.float32)
-    z = np.zeros_like(o["log_t"])
-    orc.raster_backward(oc, tile, sph, nsig, sc["texel_sites"], rgbh, adj_np, off_np, ad, new_offs, new_prims,
-                        o["early_stop"], o["log_t"], g_c, z, z, np.zeros_like(o["normal"]),
-                        np.zeros(sph.shape[0], np.float32))
-    t_comp = time.perf_counter() - t1
-    t_frame = t_bin + t_comp * T / max(len(sample), 1)
-    return dict(value=1.0 / t_frame, unit=UNIT, cores=orc.num_threads(), kind="port",
-                sample=(f"oracle binning of all {sph.shape[0]} prims ({t_bin:.2f}s) + forward/adjoint of "
-                        f"{len(sample)}/{T} random tiles ({t_comp:.2f}s), scaled to the full frame"))
+
+class OracleFrame:
+    """The raster workload on the host, for the CPU baseline and the reference
+    arm: scene, camera, texel colours (SH pre-step), Čech adjacency and target
+    built on the CPU by the oracle (no GPU library loaded), and the oracle's
+    binning + forward + adjoint timed in slices.  Slice k of S holds 1/S of a
+    frame's work: the binning of every S-th primitive (k, k + S, ...) and the
+    forward + adjoint of every S-th tile with its full list; S consecutive
+    slices time one whole frame, every part of it once."""
+
+    def __init__(self, workload, tile=8):
+        from oracle import oracle as orc
+        from powerfoam_b200 import synthetic
+
+        self.orc = orc
+        orc.build()
+        cfg = synthetic.CONFIGS[workload]
+        sc = synthetic.make_scene(cfg["n"], seed=cfg["seed"], mixture=cfg["mixture"], sigma=cfg.get("sigma", 0.15),
+                                  r_range=cfg["r_range"], device="cpu")
+        cam = synthetic.orbit_camera(100, cfg["width"], cfg["height"], cfg["vfov"], device="cpu")
+        self.cfg, self.tile = cfg, tile
+        n = {k: v.numpy() for k, v in sc.items()}
+        eye = cam.eye.numpy()
+        rgb = orc.sh_texel_rgb(n["points"], n["sh"], eye)
+        self.sites = n["texel_sites"]
+        self.sph = np.concatenate([n["points"], n["radii"][:, None]], -1).astype(np.float32)
+        self.nsig = np.concatenate([n["normals"], n["density"][:, None]], -1).astype(np.float32)
+        self.rgbh = np.concatenate([rgb, n["texel_height"][..., None]], -1).astype(np.float32)
+        self.adj, self.adj_off = orc.cech_adjacency(n["points"], n["radii"])
+        self.oc = orc.camera(eye, cam.right.numpy(), cam.up.numpy(), cam.width, cam.height)
+        g = torch.Generator().manual_seed(200)
+        self.target = torch.rand((cfg["height"], cfg["width"], 3), generator=g).numpy()
+        # the frame's tile lists (the slices composite them); each slice re-bins its primitives in its timing
+        keys, self.prims, self.offs, _ = orc.bin(self.oc, self.sph, tile)
+        self.ad = orc.prefetch_adjacency(self.sph, self.adj, self.adj_off)
+        self.T = self.offs.shape[0] - 1
+        self.zeros = (np.zeros((cfg["height"], cfg["width"]), np.float32),
+                      np.zeros((cfg["height"], cfg["width"], 3), np.float32), np.zeros(self.sph.shape[0], np.float32))
+
+    def run_slice(self, k, S):
+        """Seconds of slice k of S (binning of primitives k::S, neighbour
+        records of their lists, forward + adjoint of tiles k::S)."""
+        orc = self.orc
+        tiles = np.arange(k, self.T, S)
+        lens = np.zeros(self.T, np.int64)
+        lens[tiles] = self.offs[tiles + 1] - self.offs[tiles]
+        offs = np.concatenate([[0], np.cumsum(lens)]).astype(np.int64)
+        prims = np.concatenate([self.prims[self.offs[t]:self.offs[t + 1]] for t in tiles]).astype(np.int32)
+        sph_k = np.ascontiguousarray(self.sph[k::S])
+        z, zn, zc = self.zeros
+        t0 = time.perf_counter()
+        orc.bin(self.oc, sph_k, self.tile)
+        o = orc.raster_forward(self.oc, self.tile, self.sph, self.nsig, self.sites, self.rgbh, self.adj, self.adj_off,
+                               self.ad, offs, prims)
+        g_c = (2 * (o["color"] - self.target)).astype(np.float32)
+        orc.raster_backward(self.oc, self.tile, self.sph, self.nsig, self.sites, self.rgbh, self.adj, self.adj_off,
+                            self.ad, offs, prims, o["early_stop"], o["log_t"], g_c, z, z, zn, zc)
+        return time.perf_counter() - t0
+
+
+CPU_SLICES = 16
+
+
+def cpu_baseline_line(frame, n_slices):
+    """frames/s of the oracle over n_slices consecutive slices (1/CPU_SLICES
+    of a frame each)."""
+    t = sum(frame.run_slice(k % CPU_SLICES, CPU_SLICES) for k in range(n_slices))
+    frac = n_slices / CPU_SLICES
+    return dict(value=frac / t, unit=UNIT, cores=frame.orc.num_threads(), cpu=cpu_model(), kind="port",
+                sample=(f"oracle (CPU restatement, OpenMP) binning + forward + adjoint of {n_slices}/{CPU_SLICES} "
+                        f"of the frame (slices of every {CPU_SLICES}th primitive and tile), {frac:.2f} frames in "
+                        f"{t:.2f} s; inputs built on the host"))
 
 
 def reference_arm(args, rank, world):
+    """The reference's algorithm on the host cores: the oracle (the CPU
+    restatement of the reference's kernels; the reference's Warp kernels
+    cannot be imported here) over slices of the frame, each timed step one
+    slice (1/16 of the frame's work), frames/s = (steps / 16) / time."""
     if rank != 0:
         return
-    from oracle import oracle as orc
-
-    orc.build()
-    dev = "cuda" if torch.cuda.is_available() else "cpu"
-    cfg, scene, cam, adj, adj_off, target = build_workload(dev, 0, args.tile, args.workload)
-    sample = args.cpu_sample_tiles or 200
-    for _ in range(args.warmup):
-        cpu_baseline(cfg, scene, cam, adj, adj_off, target, max(sample // 10, 1), args.tile)
-    vals = [cpu_baseline(cfg, scene, cam, adj, adj_off, target, sample, args.tile) for _ in range(args.steps)]
-    v = statistics.median([x["value"] for x in vals])
-    cb = dict(vals[-1])
-    cb["value"] = v
+    frame = OracleFrame(args.workload, args.tile)
+    for k in range(args.warmup):
+        frame.run_slice(k % CPU_SLICES, CPU_SLICES)
+    times = [frame.run_slice(k % CPU_SLICES, CPU_SLICES) for k in range(args.steps)]
+    t = sum(times)
+    v = (args.steps / CPU_SLICES) / t
+    cb = dict(value=v, unit=UNIT, cores=frame.orc.num_threads(), cpu=cpu_model(), kind="port",
+              sample=(f"{args.steps} steps, each 1/{CPU_SLICES} of the frame (binning of every {CPU_SLICES}th "
+                      f"primitive, forward + adjoint of every {CPU_SLICES}th tile); {args.steps / CPU_SLICES:.2f} "
+                      f"frames in {t:.2f} s"))
     line = dict(metric=METRIC, value=v, unit=UNIT, n_gpus=world, steps=args.steps, warmup=args.warmup,
-                ms_per_step=1000.0 / v, higher_is_better=True, scaling="weak", vs_baseline=None, dtype="f32",
-                data="synthetic", impl="reference",
-                config=dict(workload=args.workload, prims=cfg["n"], width=cfg["width"], height=cfg["height"],
-                            tile=args.tile, parallelism="cpu-openmp"),
-                cpu_baseline=cb, e2e=dict(value=v, unit=UNIT, h2d_bytes_per_step=0, d2h_bytes_per_step=0))
+                ms_per_step=1000.0 * t / args.steps, higher_is_better=True, scaling="weak", vs_baseline=None,
+                dtype="f32", data="synthetic", impl="reference",
+                config=dict(workload=args.workload, prims=frame.cfg["n"], width=frame.cfg["width"],
+                            height=frame.cfg["height"], tile=args.tile, parallelism="cpu-openmp",
+                            step=f"1/{CPU_SLICES} frame"),
+                cpu_baseline=cb, e2e=dict(value=v, unit=UNIT, h2d_bytes_per_step=0, d2h_bytes_per_step=0),
+                note=("the reference's Warp kernels are not importable on this image (no warp module); the "
+                      "timed CPU implementation is the oracle, the reference's kernels restated in C"))
     print(json.dumps(line), flush=True)
 
 
@@ -323,12 +374,11 @@ def batch_main(args, world, rank, local, dev):
                                log=(lambda m: print(m, file=sys.stderr, flush=True)) if rank == 0 else None)
     tune_s = time.perf_counter() - t0
     step.capture()
-    reducer = GradReducer([step.grads[k] for k in sorted(step.grads)] + [step.grad_sh]) if world > 1 else None
 
     def run():
         loss = step.run()
-        if reducer is not None:
-            reducer()
+        if world > 1:  # the step's gradients live in one flat buffer: summed in place
+            step.grad_buffer.allreduce()
         return loss
 
     def barrier():
@@ -626,9 +676,9 @@ def trace_main(args, dev):
                             l2="inputs larger than L2, no flush"),
                 clocks=clk, e2e=dict(value=1000.0 / e2e_ms, unit="frames/s", h2d_bytes_per_step=target.numel() * 4,
                                      d2h_bytes_per_step=4),
-                # per step: the walk (pf_trace_forward), then the adjoint's walk, segment and resume launches
-                # and seven gradient sanitising launches (pf_trace_backward)
-                gpu_launches=args.steps * (1 + 3 + 7))
+                # per step: the recording walk (pf_trace_forward_record), then the adjoint's segment and
+                # resume launches and seven gradient sanitising launches (pf_trace_backward_recorded)
+                gpu_launches=args.steps * (1 + 2 + 7))
     if not args.no_cpu_baseline:
         line["cpu_baseline"] = trace_cpu_baseline(sc, rgb, adj, off, pm, cam, st, cfg)
     print(json.dumps(line), flush=True)
@@ -1065,7 +1115,8 @@ def main():
                          d2h_bytes_per_step=4),
                 roofline=dict(bound="hbm", kernel=dominant, achieved=achieved, peak=peak, unit="GB/s",
                               frac=achieved / peak, peak_source=peak_kind,
-                              traffic=load_traffic(dominant, args.workload),
+                              traffic=(capture_traffic(dominant, args.workload) or (None, None))[0],
+                              traffic_source=(capture_traffic(dominant, args.workload) or (None, None))[1],
                               algorithmic_bytes=dom_bytes, ms=dom_ms, fwd_ms=fwd_ms, bwd_ms=bwd_ms),
                 gpu_launches=None)
     # kernels per step: pack 1, binning with tile order, prefetch 1, SH 1, forward 1, backward 1 + 7 sanitise
@@ -1076,9 +1127,8 @@ def main():
             dh, dw, levels = (dh + 1) // 2, (dw + 1) // 2, levels + 1
         line["gpu_launches"] += args.steps * levels
         line["config"]["camera"] = "generic: 150-degree equidistant fisheye ray maps"
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(cfg, scene, cam, adj, adj_off, target, args.cpu_sample_tiles or 200,
-                                            args.tile)
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and not fisheye:
+        line["cpu_baseline"] = cpu_baseline_line(OracleFrame(args.workload, args.tile), args.cpu_slices)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:

@@ -341,6 +341,28 @@ PF_API int pf_trace_backward(const pf_trace_inputs *in, const float *color, cons
                              float *grad_texel_sites, float *grad_texel_rgb, float *grad_texel_height,
                              int32_t segments_per_ray, void *workspace, size_t workspace_bytes, void *stream);
 
+/* The walk of pf_trace_forward (f32 attributes, no visit log) that also
+ * writes the adjoint's segment records into `workspace` (the layout and size
+ * of pf_trace_backward_workspace_size for segments_per_ray): up to
+ * segments_per_ray records per ray and the walk state of each ray with more.
+ * pf_trace_backward_recorded then starts the adjoint from those records, so
+ * the walk is not repeated.  No counterpart in the reference (its tracer has
+ * no adjoint); outputs as pf_trace_forward. */
+PF_API int pf_trace_forward_record(const pf_trace_inputs *in, float *color, float *log_t, float *depth, float *normal,
+                                   int32_t *depth_seg, float *depth_sigma, int32_t *visit_count, int32_t *status,
+                                   int32_t segments_per_ray, void *workspace, size_t workspace_bytes, void *stream);
+/* pf_trace_backward without its walk: `workspace` holds the records that
+ * pf_trace_forward_record wrote with the same inputs and segments_per_ray
+ * (the workspace is only read).  Same arguments and gradients as
+ * pf_trace_backward. */
+PF_API int pf_trace_backward_recorded(const pf_trace_inputs *in, const float *color, const float *normal,
+                                      const int32_t *depth_seg, const float *depth_sigma, const float *grad_color,
+                                      const float *grad_log_t, const float *grad_depth, const float *grad_normal,
+                                      float *grad_points, float *grad_radii, float *grad_normals,
+                                      float *grad_density, float *grad_texel_sites, float *grad_texel_rgb,
+                                      float *grad_texel_height, int32_t segments_per_ray, const void *workspace,
+                                      size_t workspace_bytes, void *stream);
+
 /* Training labels of the ray-proposal network (no counterpart in the
  * reference): the walk of pf_trace_forward (f32 attributes) writing, per
  * pixel ray, the colour and the first cell after whose compositing the

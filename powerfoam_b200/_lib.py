@@ -156,6 +156,10 @@ _SIGS = {
     "pf_trace_backward_workspace_size": [ctypes.POINTER(PfTraceInputs), c_i32, ctypes.POINTER(ctypes.c_size_t)],
     "pf_trace_backward": [ctypes.POINTER(PfTraceInputs), c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp,
                           c_vp, c_vp, c_vp, c_vp, c_vp, c_i32, c_vp, ctypes.c_size_t, c_vp],
+    "pf_trace_forward_record": [ctypes.POINTER(PfTraceInputs), c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_i32,
+                                c_vp, ctypes.c_size_t, c_vp],
+    "pf_trace_backward_recorded": [ctypes.POINTER(PfTraceInputs), c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp,
+                                   c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_i32, c_vp, ctypes.c_size_t, c_vp],
     "pf_start_cell_workspace_size": [c_i64, ctypes.POINTER(ctypes.c_size_t)],
     "pf_start_cell": [c_vp, c_vp, c_i64, ctypes.POINTER(c_f), c_vp, ctypes.c_size_t, c_vp, c_vp],
     "pf_sh_texel_rgb": [c_vp, c_vp, c_i64, c_i32, ctypes.POINTER(c_f), c_vp, c_vp],

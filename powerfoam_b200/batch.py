@@ -42,7 +42,7 @@ def _pow2_at_least(n):
 
 class BatchStep:
     def __init__(self, device, cameras, tile_width=8, chunk=1, order="longest", transmittance_threshold=1e-3,
-                 headroom=1.25, split=False):
+                 headroom=1.25, split=False, world=1):
         if not 1 <= len(cameras) <= _lib.PF_BATCH_MAX_VIEWS:
             raise ValueError(f"1..{_lib.PF_BATCH_MAX_VIEWS} views per batch")
         if tile_width not in TILE_WIDTHS:
@@ -55,6 +55,7 @@ class BatchStep:
         self.chunk = int(chunk)
         self.order = order
         self.split = bool(split)
+        self.world = int(world)  # ranks exchanging grad_buffer (its fields are padded to a multiple)
         self.thr = float(transmittance_threshold)
         self.headroom = headroom
         self.graph = None
@@ -99,7 +100,16 @@ class BatchStep:
             self.texel_rgb = [f32(t, "texel_rgb") for t in texel_rgb]
         else:
             self.texel_rgb = [torch.empty((n, S, 3), dtype=torch.float32, device=dev) for _ in range(V)]
-        self.grad_sh = torch.zeros((n, 16, 3), dtype=torch.float32, device=dev) if sh is not None else None
+        # every per-primitive gradient in one flat buffer (multiview.GradBuffer): a multi-GPU step
+        # exchanges it in place
+        from .multiview import GradBuffer
+
+        fields = {"points": (n, 3), "radii": (n,), "normals": (n, 3), "density": (n,), "texel_sites": (n, S, 3),
+                  "texel_height": (n, S)}
+        if sh is not None:
+            fields["sh"] = (n, 16, 3)
+        self.grad_buffer = GradBuffer(fields, dev, world=self.world)
+        self.grad_sh = self.grad_buffer.view("sh") if sh is not None else None
         self.spheres = torch.empty((n, 4), dtype=torch.float32, device=dev)
         self.nsigmas = torch.empty((n, 4), dtype=torch.float32, device=dev)
         self.adj_diff = torch.empty((self.adjacency.shape[0], 4), dtype=torch.float16, device=dev)
@@ -113,10 +123,8 @@ class BatchStep:
         self.early_stop = [e(T, dt=torch.int32) for T in self.n_tiles]
         self.tile_contrib_pairs = [e(T, dt=torch.int32) for T in self.n_tiles]
         self.grad_texel_rgb = [e(n, S, 3) for _ in range(V)]
-        self.grads = {k: torch.empty_like(t) for k, t in (("points", self.points), ("radii", self.radii),
-                                                           ("normals", self.normals), ("density", self.density),
-                                                           ("texel_sites", self.texel_sites),
-                                                           ("texel_height", self.texel_height))}
+        self.grads = {k: self.grad_buffer.view(k) for k in ("points", "radii", "normals", "density", "texel_sites",
+                                                             "texel_height")}
         self.tile_loss = e(sum(self.n_tiles))
         self.loss = e(V)
         self.status = torch.zeros(1, dtype=torch.int32, device=dev)

@@ -157,6 +157,36 @@ PF_D bool trace_pixel(const Cam& cam, int64_t tid, int& pi, int& pj) {
     return pi < cam.H && pj < cam.W;
 }
 
+// Segment records of the adjoint (see pf_trace_backward): one per segment
+// of a ray (a walked cell with dt > 0), written by the recording forward or
+// by the adjoint's own walk.
+struct SegRec {
+    int32_t cell;
+    float tn, tf;
+    uint32_t ids;  // tn_id in the low, tf_id in the high 16 bits (|id| < 2^15)
+    float trans;
+    v3 C, N;
+    int32_t seg;
+};
+
+PF_D uint32_t pack_ids(int tn_id, int tf_id) { return ((uint32_t)tn_id & 0xffffu) | ((uint32_t)tf_id << 16); }
+
+struct SegWs {
+    int64_t n;       // ray slots
+    int kb;          // recorded segments per ray
+    int32_t* count;  // [n] recorded segments
+    float4* rec;     // [kb][n][3]
+    int32_t* n_over; // overflow rays
+    int32_t* over;   // [n] their slots
+    float4* state;   // [n][3] their walk state
+};
+
+PF_D void store_rec(float4* p, const SegRec& r) {
+    p[0] = make_float4(__int_as_float(r.cell), r.tn, r.tf, __uint_as_float(r.ids));
+    p[1] = make_float4(r.trans, r.C.x, r.C.y, r.C.z);
+    p[2] = make_float4(r.N.x, r.N.y, r.N.z, __int_as_float(r.seg));
+}
+
 // Labels of the ray-proposal network (no counterpart in the reference): the
 // first cell after whose compositing the transmittance is below `thr`, the t
 // at which the ray enters it and the number of cells walked before it.
@@ -167,16 +197,24 @@ struct LabelOut {
     int32_t* step;
 };
 
-template <typename A, bool LABELS = false>
+// REC: also write the adjoint's segment records (W): up to W.kb per ray, the
+// walk state of a ray with more left on W's overflow list for the adjoint's
+// resume launch -- the records pf_trace_backward's own walk would write, so
+// the adjoint can start at its segment launch.
+template <typename A, bool LABELS = false, bool REC = false>
 __global__ void __launch_bounds__(128)
 trace_fwd_kernel(TraceParams P, int64_t nthreads, float* __restrict__ color, float* __restrict__ log_t_out,
                  float* __restrict__ depth, float* __restrict__ normal, int32_t* __restrict__ depth_seg,
                  float* __restrict__ depth_sigma, int32_t* __restrict__ visit_log, int visit_cap,
-                 int32_t* __restrict__ visit_count, int32_t* __restrict__ status, LabelOut lab = LabelOut{}) {
+                 int32_t* __restrict__ visit_count, int32_t* __restrict__ status, LabelOut lab = LabelOut{},
+                 SegWs W = SegWs{}) {
     int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (tid >= nthreads) return;
     int pi, pj;
-    if (!trace_pixel(P.cam, tid, pi, pj)) return;
+    if (!trace_pixel(P.cam, tid, pi, pj)) {
+        if (REC) W.count[tid] = 0;
+        return;
+    }
     const int64_t px = (int64_t)pi * P.cam.W + pj;
     const v3 o = P.cam.eye;
     const v3 d = ray_dir(P.cam, pi, pj);
@@ -190,6 +228,7 @@ trace_fwd_kernel(TraceParams P, int64_t nthreads, float* __restrict__ color, flo
     float dout = 0.f, dsig = 0.f;
     float lab_t = -1.0f;
     int32_t lab_cell = -1, lab_step = -1;
+    int nrec = 0;  // REC: segments recorded
     for (;;) {
         float trans = expf(log_t);
         if (trans < P.thr || prim == kNoCell) break;
@@ -200,6 +239,15 @@ trace_fwd_kernel(TraceParams P, int64_t nthreads, float* __restrict__ color, flo
         if (prim < 0 || prim >= P.N) {
             st = PF_ERR_ARGS;
             break;
+        }
+        if (REC && nrec == W.kb) {  // the rest of this ray's segments go to the resume launch
+            const int32_t k = atomicAdd(W.n_over, 1);
+            W.over[k] = (int32_t)tid;
+            W.state[3 * (int64_t)k] = make_float4(__int_as_float(prim), __int_as_float(steps), log_t,
+                                                   __int_as_float(seg));
+            W.state[3 * (int64_t)k + 1] = make_float4(rgb.x, rgb.y, rgb.z, nacc.x);
+            W.state[3 * (int64_t)k + 2] = make_float4(nacc.y, nacc.z, 0.f, 0.f);
+            nrec = W.kb + 1;  // saved once; the walk goes on unrecorded
         }
         if (visit_log && steps < visit_cap) visit_log[px * visit_cap + steps] = prim;
         const float cell_entry = pt_near;
@@ -214,6 +262,11 @@ trace_fwd_kernel(TraceParams P, int64_t nthreads, float* __restrict__ color, flo
         if (length(v) < 4.0f * radius) hit = false;
         int32_t next = kNoCell;
         float pt_far = 1e10f;
+        int tn_id = 0, tf_id = 0;  // REC: surfaces bounding the segment (as walk_step)
+        if (REC) {
+            tn_id = tn < 1e-8f ? -2 : -1;
+            tf_id = tf < 1e-8f ? -2 : -1;
+        }
         const int32_t a0 = __ldg(&P.adj_off[prim]), a1 = __ldg(&P.adj_off[prim + 1]);
         for (int32_t e = a0; e < a1; e++) {
             uint2 raw = __ldg(&P.adj_diff[e]);
@@ -225,9 +278,14 @@ trace_fwd_kernel(TraceParams P, int64_t nthreads, float* __restrict__ color, flo
                 next = __ldg(&P.adj[e]);
                 pt_far = t_face;
             }
+            if (REC) {
+                if (dp >= 0.0f && t_face < tf) tf_id = e - a0;
+                if (dp < 0.0f && t_face > tn) tn_id = e - a0;
+            }
             tf = dp >= 0.0f ? fmin_t(t_face, tf) : tf;
             tn = dp < 0.0f ? fmax_t(t_face, tn) : tn;
         }
+        const float pre_tn = tn, pre_tf = tf;
         v3 pn = mk(ldT(nsig, 4 * (int64_t)prim), ldT(nsig, 4 * (int64_t)prim + 1), ldT(nsig, 4 * (int64_t)prim + 2));
         float sigma = ldT(nsig, 4 * (int64_t)prim + 3);
         if (!hit || tn > tf || sigma < 1e-3f) {
@@ -269,9 +327,23 @@ trace_fwd_kernel(TraceParams P, int64_t nthreads, float* __restrict__ color, flo
                 lab_cell = cell;
                 lab_step = steps - 1;
             }
+            if (REC && nrec < W.kb) {
+                SegRec r;
+                r.cell = cell;
+                r.tn = pre_tn;
+                r.tf = pre_tf;
+                r.ids = pack_ids(tn_id, tf_id);
+                r.trans = trans;
+                r.C = rgb;
+                r.N = nacc;
+                r.seg = seg;
+                store_rec(W.rec + 3 * ((int64_t)nrec * W.n + tid), r);
+                nrec++;
+            }
             seg++;
         }
     }
+    if (REC) W.count[tid] = nrec > W.kb ? W.kb : nrec;
     if (LABELS) {
         lab.t[px] = lab_t;
         lab.cell[px] = lab_cell;
@@ -574,16 +646,6 @@ PF_D float plane_local_bwd4(v3 o, v3 d, float tn, v3 po, v3 pn, float radius, co
 // before the texture plane (ids as in WalkStep), the transmittance before
 // it, the colour and normal accumulated up to and including it, and its
 // index among the ray's segments.
-struct SegRec {
-    int32_t cell;
-    float tn, tf;
-    uint32_t ids;  // tn_id in the low, tf_id in the high 16 bits (|id| < 2^15)
-    float trans;
-    v3 C, N;
-    int32_t seg;
-};
-
-PF_D uint32_t pack_ids(int tn_id, int tf_id) { return ((uint32_t)tn_id & 0xffffu) | ((uint32_t)tf_id << 16); }
 
 // Per-pixel inputs of the adjoint: the forward's colour / normal / depth
 // segment and the loss gradients (any may be null where the reference's
@@ -730,22 +792,6 @@ PF_D PlaneRes cell_plane(const TraceParams& P, v3 o, v3 d, int32_t cell, float t
 // Launches 1 and 2 carry no per-ray loop around the gradient work, so the
 // walk runs at the forward's register count and occupancy and the gradient
 // work on full warps (only about one walked cell in five is a segment).
-struct SegWs {
-    int64_t n;       // ray slots
-    int kb;          // recorded segments per ray
-    int32_t* count;  // [n] recorded segments
-    float4* rec;     // [kb][n][3]
-    int32_t* n_over; // overflow rays
-    int32_t* over;   // [n] their slots
-    float4* state;   // [n][3] their walk state
-};
-
-PF_D void store_rec(float4* p, const SegRec& r) {
-    p[0] = make_float4(__int_as_float(r.cell), r.tn, r.tf, __uint_as_float(r.ids));
-    p[1] = make_float4(r.trans, r.C.x, r.C.y, r.C.z);
-    p[2] = make_float4(r.N.x, r.N.y, r.N.z, __int_as_float(r.seg));
-}
-
 PF_D SegRec load_rec(const float4* p) {
     const float4 a = p[0], b = p[1], c = p[2];
     SegRec r;
@@ -1271,12 +1317,33 @@ extern "C" int pf_trace_backward_workspace_size(const pf_trace_inputs* in, int32
     return PF_OK;
 }
 
-extern "C" int pf_trace_backward(const pf_trace_inputs* in, const float* color, const float* normal,
-                                 const int32_t* depth_seg, const float* depth_sigma, const float* grad_color,
-                                 const float* grad_log_t, const float* grad_depth, const float* grad_normal,
-                                 float* grad_points, float* grad_radii, float* grad_normals, float* grad_density,
-                                 float* grad_texel_sites, float* grad_texel_rgb, float* grad_texel_height,
-                                 int32_t segments_per_ray, void* workspace, size_t workspace_bytes, void* stream) {
+static SegWs seg_ws(const pf_trace_inputs* in, int kb, void* workspace) {
+    const int64_t n = trace_slots(in);
+    size_t off[5];
+    seg_ws_layout(n, kb, off);
+    char* ws = (char*)workspace;
+    return SegWs{n, kb, (int32_t*)(ws + off[0]), (float4*)(ws + off[1]), (int32_t*)(ws + off[2]),
+                 (int32_t*)(ws + off[3]), (float4*)(ws + off[4])};
+}
+
+static int check_seg_ws(const pf_trace_inputs* in, int32_t segments_per_ray, const void* workspace,
+                        size_t workspace_bytes, const char* who) {
+    size_t need = 0;
+    if (pf_trace_backward_workspace_size(in, segments_per_ray, &need) != PF_OK) return PF_ERR_ARGS;
+    if (!workspace || workspace_bytes < need || ((uintptr_t)workspace & 255))
+        return pf_fail(PF_ERR_ARGS, who);
+    return PF_OK;
+}
+
+// walk = true: the adjoint's own recording walk first; false: the records of
+// pf_trace_forward_record are in the workspace already
+static int trace_backward_impl(const pf_trace_inputs* in, const float* color, const float* normal,
+                               const int32_t* depth_seg, const float* depth_sigma, const float* grad_color,
+                               const float* grad_log_t, const float* grad_depth, const float* grad_normal,
+                               float* grad_points, float* grad_radii, float* grad_normals, float* grad_density,
+                               float* grad_texel_sites, float* grad_texel_rgb, float* grad_texel_height,
+                               int32_t segments_per_ray, void* workspace, size_t workspace_bytes, void* stream,
+                               bool walk) {
     TraceParams P;
     const char* why = "";
     if (!fill_trace(in, P, &why)) return pf_fail(PF_ERR_ARGS, why);
@@ -1285,10 +1352,9 @@ extern "C" int pf_trace_backward(const pf_trace_inputs* in, const float* color, 
         !grad_texel_rgb || !grad_texel_height || (grad_depth && (!depth_seg || !depth_sigma)) ||
         (grad_normal && !normal))
         return pf_fail(PF_ERR_ARGS, "pf_trace_backward: missing argument");
-    size_t need = 0;
-    if (pf_trace_backward_workspace_size(in, segments_per_ray, &need) != PF_OK) return PF_ERR_ARGS;
-    if (!workspace || workspace_bytes < need || ((uintptr_t)workspace & 255))
-        return pf_fail(PF_ERR_ARGS, "pf_trace_backward: workspace missing, too small or not 256-byte aligned");
+    if (check_seg_ws(in, segments_per_ray, workspace, workspace_bytes,
+                     "pf_trace_backward: workspace missing, too small or not 256-byte aligned") != PF_OK)
+        return PF_ERR_ARGS;
     cudaStream_t st = (cudaStream_t)stream;
     const size_t N = (size_t)P.N, S = (size_t)P.S;
     float* outs[7] = {grad_points, grad_radii, grad_normals, grad_density, grad_texel_sites, grad_texel_rgb,
@@ -1301,15 +1367,12 @@ extern "C" int pf_trace_backward(const pf_trace_inputs* in, const float* color, 
     TraceGrads G{grad_points,      grad_radii,     grad_normals,      grad_density,
                  grad_texel_sites, grad_texel_rgb, grad_texel_height, vec4};
     TraceAdjIn A{color, normal, depth_seg, depth_sigma, grad_color, grad_log_t, grad_depth, grad_normal};
-    const int64_t n = trace_slots(in);
-    size_t off[5];
-    seg_ws_layout(n, segments_per_ray, off);
-    char* ws = (char*)workspace;
-    SegWs W{n, segments_per_ray, (int32_t*)(ws + off[0]), (float4*)(ws + off[1]), (int32_t*)(ws + off[2]),
-            (int32_t*)(ws + off[3]), (float4*)(ws + off[4])};
-    cudaMemsetAsync(W.n_over, 0, sizeof(int32_t), st);
-    const unsigned blocks = (unsigned)((n + 127) / 128);
-    trace_bwd_walk_kernel<<<blocks, 128, 0, st>>>(P, W);
+    const SegWs W = seg_ws(in, segments_per_ray, workspace);
+    const unsigned blocks = (unsigned)((W.n + 127) / 128);
+    if (walk) {
+        cudaMemsetAsync(W.n_over, 0, sizeof(int32_t), st);
+        trace_bwd_walk_kernel<<<blocks, 128, 0, st>>>(P, W);
+    }
     if (segments_per_ray > 0)
         trace_bwd_segment_kernel<<<dim3(blocks, std::min(segments_per_ray, kSegStride)), 128, 0, st>>>(P, W, A, G);
     static_assert(trace_resume_smem() <= 48 * 1024, "resume queue above the default shared-memory limit");
@@ -1321,6 +1384,53 @@ extern "C" int pf_trace_backward(const pf_trace_inputs* in, const float* color, 
                 outs[i], k);
         }
     return pf_check_launch("pf_trace_backward");
+}
+
+extern "C" int pf_trace_backward(const pf_trace_inputs* in, const float* color, const float* normal,
+                                 const int32_t* depth_seg, const float* depth_sigma, const float* grad_color,
+                                 const float* grad_log_t, const float* grad_depth, const float* grad_normal,
+                                 float* grad_points, float* grad_radii, float* grad_normals, float* grad_density,
+                                 float* grad_texel_sites, float* grad_texel_rgb, float* grad_texel_height,
+                                 int32_t segments_per_ray, void* workspace, size_t workspace_bytes, void* stream) {
+    return trace_backward_impl(in, color, normal, depth_seg, depth_sigma, grad_color, grad_log_t, grad_depth,
+                               grad_normal, grad_points, grad_radii, grad_normals, grad_density, grad_texel_sites,
+                               grad_texel_rgb, grad_texel_height, segments_per_ray, workspace, workspace_bytes,
+                               stream, true);
+}
+
+extern "C" int pf_trace_backward_recorded(const pf_trace_inputs* in, const float* color, const float* normal,
+                                          const int32_t* depth_seg, const float* depth_sigma,
+                                          const float* grad_color, const float* grad_log_t, const float* grad_depth,
+                                          const float* grad_normal, float* grad_points, float* grad_radii,
+                                          float* grad_normals, float* grad_density, float* grad_texel_sites,
+                                          float* grad_texel_rgb, float* grad_texel_height, int32_t segments_per_ray,
+                                          const void* workspace, size_t workspace_bytes, void* stream) {
+    return trace_backward_impl(in, color, normal, depth_seg, depth_sigma, grad_color, grad_log_t, grad_depth,
+                               grad_normal, grad_points, grad_radii, grad_normals, grad_density, grad_texel_sites,
+                               grad_texel_rgb, grad_texel_height, segments_per_ray, const_cast<void*>(workspace),
+                               workspace_bytes, stream, false);
+}
+
+extern "C" int pf_trace_forward_record(const pf_trace_inputs* in, float* color, float* log_t, float* depth,
+                                       float* normal, int32_t* depth_seg, float* depth_sigma, int32_t* visit_count,
+                                       int32_t* status, int32_t segments_per_ray, void* workspace,
+                                       size_t workspace_bytes, void* stream) {
+    TraceParams P;
+    const char* why = "";
+    if (!fill_trace(in, P, &why)) return pf_fail(PF_ERR_ARGS, why);
+    if (in->attr_half) return pf_fail(PF_ERR_ARGS, "pf_trace_forward_record: attributes must be f32");
+    if (!color) return pf_fail(PF_ERR_ARGS, "pf_trace_forward_record: missing argument");
+    if (check_seg_ws(in, segments_per_ray, workspace, workspace_bytes,
+                     "pf_trace_forward_record: workspace missing, too small or not 256-byte aligned") != PF_OK)
+        return PF_ERR_ARGS;
+    cudaStream_t st = (cudaStream_t)stream;
+    const SegWs W = seg_ws(in, segments_per_ray, workspace);
+    cudaMemsetAsync(W.n_over, 0, sizeof(int32_t), st);
+    const unsigned grid = (unsigned)((W.n + 127) / 128);
+    trace_fwd_kernel<float, false, true><<<grid, 128, 0, st>>>(P, W.n, color, log_t, depth, normal, depth_seg,
+                                                              depth_sigma, nullptr, 0, visit_count, status,
+                                                              LabelOut{}, W);
+    return pf_check_launch("pf_trace_forward_record");
 }
 
 extern "C" int pf_start_cell_workspace_size(int64_t n_prims, size_t* bytes) {

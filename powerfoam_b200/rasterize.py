@@ -201,6 +201,10 @@ class Rasterizer:
         self.scratch = torch.zeros(64, dtype=torch.int32, device=self.device)
         # persistent device status word of the sync-free mode (see class docstring)
         self.status = torch.zeros(1, dtype=torch.int32, device=self.device)
+        # optional multiview.GradBuffer with multiview.raster_fields: the
+        # adjoint then writes the gradients into its views (the cross-GPU
+        # exchange runs on the buffer with no copies)
+        self.grad_buffer = None
         _lib.load()
 
     def check(self):
@@ -372,13 +376,21 @@ class Rasterizer:
         gn = None if grad_normal_in is None else _f32(grad_normal_in, "grad")
         gq = None if (grad_quantile_depths_in is None or dq is None) else _f32(grad_quantile_depths_in, "grad")
         gcon = None if grad_contrib_in is None else _f32(grad_contrib_in, "grad")
-        out = dict(points=torch.empty((n, 3), dtype=torch.float32, device=dev),
-                   radii=torch.empty(n, dtype=torch.float32, device=dev),
-                   normals=torch.empty((n, 3), dtype=torch.float32, device=dev),
-                   density=torch.empty(n, dtype=torch.float32, device=dev),
-                   sites=torch.empty((n, S, 3), dtype=torch.float32, device=dev),
-                   rgb=torch.empty((n, S, 3), dtype=torch.float32, device=dev),
-                   height=torch.empty((n, S), dtype=torch.float32, device=dev))
+        gb = self.grad_buffer
+        if gb is not None:
+            if gb.n != n or tuple(gb.layout["texel_sites"][2]) != (n, S, 3):
+                raise ValueError("grad_buffer does not match the primitive count / texel sites")
+            v = gb.views()
+            out = dict(points=v["points"], radii=v["radii"], normals=v["normals"], density=v["density"],
+                       sites=v["texel_sites"], rgb=v["texel_rgb"], height=v["texel_height"])
+        else:
+            out = dict(points=torch.empty((n, 3), dtype=torch.float32, device=dev),
+                       radii=torch.empty(n, dtype=torch.float32, device=dev),
+                       normals=torch.empty((n, 3), dtype=torch.float32, device=dev),
+                       density=torch.empty(n, dtype=torch.float32, device=dev),
+                       sites=torch.empty((n, S, 3), dtype=torch.float32, device=dev),
+                       rgb=torch.empty((n, S, 3), dtype=torch.float32, device=dev),
+                       height=torch.empty((n, S), dtype=torch.float32, device=dev))
         inp = self._inputs(camera, spheres, nsig, sites, rgb, height, adjacency, adjacency_offsets, adj_diff,
                            grad_ctx.bins, dq, None, grad_ctx.thr, ray_maps=grad_ctx.ray_maps)
         _timed_call("pf_raster_backward", _lib.ctypes.byref(inp), _lib.ptr(early_stop), _lib.ptr(log_t), _lib.ptr(gc),

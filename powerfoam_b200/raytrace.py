@@ -30,6 +30,7 @@ class TraceResult:
     visit_count: torch.Tensor
     visits: torch.Tensor = None
     status: int = 0
+    records: tuple = None  # (workspace, segments_per_ray) of a recording walk
 
 
 class RayTraceGradFn(torch.autograd.Function):
@@ -66,6 +67,10 @@ class RayTracer:
         # gives the same gradients), 48 bytes per pixel each; None: 96,
         # lowered so the records stay within RECORD_BYTES
         self.segments_per_ray = None
+        # the differentiable forward writes the adjoint's segment records
+        # (pf_trace_forward_record), so the adjoint does not walk again; False:
+        # plain forward, and the adjoint repeats the walk (pf_trace_backward)
+        self.record_segments = True
         _lib.load()
 
     def _inputs(self, camera, start, spheres, nsig, sites, rgb, height, adjacency, adjacency_offsets,
@@ -102,11 +107,27 @@ class RayTracer:
                 texel_height.to(self.tscalar).contiguous(), adjacency.to(torch.int32).contiguous(),
                 adjacency_offsets.to(torch.int32).contiguous(), adjacency_diff.contiguous())
 
+    def _segments_per_ray(self, camera):
+        kb = self.segments_per_ray
+        if kb is None:
+            slots = ((int(camera.height) + 7) // 8) * ((int(camera.width) + 7) // 8) * 64
+            kb = max(1, min(96, RECORD_BYTES // (48 * slots)))
+        return int(kb)
+
+    def _records(self, inp, kb):
+        """The adjoint's segment-record workspace (256-byte aligned)."""
+        nbytes = _lib.ctypes.c_size_t(0)
+        _lib.call("pf_trace_backward_workspace_size", _lib.ctypes.byref(inp), kb, _lib.ctypes.byref(nbytes))
+        ws = torch.empty(nbytes.value + 256, dtype=torch.uint8, device=self.device)
+        return ws, (ws.data_ptr() + 255) & ~255, nbytes.value
+
     def trace(self, camera, start, points, radii, density, normals, texel_sites, texel_rgb, texel_height, adjacency,
               adjacency_offsets, adjacency_diff, transmittance_threshold=1e-3, max_steps=DEFAULT_MAX_STEPS,
-              depth_quantile=0.5, visit_cap=0, check_status=True):
+              depth_quantile=0.5, visit_cap=0, check_status=True, record=False):
         """Walk every pixel's ray.  ``start`` is one cell index or an (H, W)
-        int32 tensor of per-ray start cells."""
+        int32 tensor of per-ray start cells.  ``record``: also write the
+        adjoint's segment records (pf_trace_forward_record; f32, no visit
+        log), returned in ``records`` for the backward."""
         H, W = camera.height, camera.width
         dev = self.device
         args = self._prep(points, radii, density, normals, texel_sites, texel_rgb, texel_height, adjacency,
@@ -125,9 +146,20 @@ class RayTracer:
         )
         status = torch.zeros(1, dtype=torch.int32, device=dev)
         inp = self._inputs(camera, start, *args, transmittance_threshold, max_steps, depth_quantile)
-        _lib.call("pf_trace_forward", _lib.ctypes.byref(inp), _lib.ptr(r.color), _lib.ptr(r.log_t),
-                  _lib.ptr(r.depth), _lib.ptr(r.normal), _lib.ptr(r.depth_seg), _lib.ptr(r.depth_sigma),
-                  _lib.ptr(r.visits), int(visit_cap), _lib.ptr(r.visit_count), _lib.ptr(status), _lib.stream_ptr())
+        if record:
+            if visit_cap:
+                raise ValueError("a recording walk keeps no visit log")
+            kb = self._segments_per_ray(camera)
+            ws, ws_ptr, nbytes = self._records(inp, kb)
+            _lib.call("pf_trace_forward_record", _lib.ctypes.byref(inp), _lib.ptr(r.color), _lib.ptr(r.log_t),
+                      _lib.ptr(r.depth), _lib.ptr(r.normal), _lib.ptr(r.depth_seg), _lib.ptr(r.depth_sigma),
+                      _lib.ptr(r.visit_count), _lib.ptr(status), kb, ws_ptr, nbytes, _lib.stream_ptr())
+            r.records = (ws, ws_ptr, nbytes, kb)
+        else:
+            _lib.call("pf_trace_forward", _lib.ctypes.byref(inp), _lib.ptr(r.color), _lib.ptr(r.log_t),
+                      _lib.ptr(r.depth), _lib.ptr(r.normal), _lib.ptr(r.depth_seg), _lib.ptr(r.depth_sigma),
+                      _lib.ptr(r.visits), int(visit_cap), _lib.ptr(r.visit_count), _lib.ptr(status),
+                      _lib.stream_ptr())
         if check_status:
             r.status = int(status.item())
             if r.status != _lib.PF_OK:
@@ -148,9 +180,13 @@ class RayTracer:
         if self.attr_dtype != "float":
             raise ValueError("Forward pass only supports float precision")
         max_steps = DEFAULT_MAX_STEPS if max_steps is None else max_steps
+        # with gradients wanted, the walk writes the adjoint's segment records (the adjoint then does not
+        # walk again); ctx.needs_input_grad follows the apply() arguments: points ... texel_height are 3-9
+        record = self.record_segments and any(ctx.needs_input_grad[3:10])
         r = self.trace(camera, start, points.detach(), radii.detach(), density.detach(), normals.detach(),
                        texel_sites.detach(), texel_rgb.detach(), texel_height.detach(), adjacency, adjacency_offsets,
-                       adjacency_diff, thr, max_steps, depth_quantile)
+                       adjacency_diff, thr, max_steps, depth_quantile, record=record)
+        ctx.records = r.records
         ctx.tracer = self
         ctx.camera = camera
         ctx.start = start
@@ -175,20 +211,19 @@ class RayTracer:
         out = [torch.empty(s, dtype=torch.float32, device=dev) for s in ((n, 3), (n,), (n, 3), (n,), (n, S, 3),
                                                                          (n, S, 3), (n, S))]
         c = lambda t: None if t is None else t.float().contiguous()
-        kb = self.segments_per_ray
-        if kb is None:
-            slots = ((int(ctx.camera.height) + 7) // 8) * ((int(ctx.camera.width) + 7) // 8) * 64
-            kb = max(1, min(96, RECORD_BYTES // (48 * slots)))
-        kb = int(kb)
-        nbytes = _lib.ctypes.c_size_t(0)
-        _lib.call("pf_trace_backward_workspace_size", _lib.ctypes.byref(inp), kb, _lib.ctypes.byref(nbytes))
-        ws = torch.empty(nbytes.value + 256, dtype=torch.uint8, device=dev)
-        ws_ptr = (ws.data_ptr() + 255) & ~255
-        _lib.call("pf_trace_backward", _lib.ctypes.byref(inp), _lib.ptr(color), _lib.ptr(normal),
-                  _lib.ptr(depth_seg), _lib.ptr(depth_sigma), _lib.ptr(c(g_color)), _lib.ptr(c(g_log_t)),
-                  _lib.ptr(c(g_depth)), _lib.ptr(c(g_normal)), *[_lib.ptr(t) for t in out], kb, ws_ptr,
-                  nbytes.value, _lib.stream_ptr())
-        del ctx.tracer, ctx.camera, ctx.start
+        grads_in = (_lib.ptr(c(g_color)), _lib.ptr(c(g_log_t)), _lib.ptr(c(g_depth)), _lib.ptr(c(g_normal)))
+        if ctx.records is not None:  # the forward's segment records
+            ws, ws_ptr, nbytes, kb = ctx.records
+            _lib.call("pf_trace_backward_recorded", _lib.ctypes.byref(inp), _lib.ptr(color), _lib.ptr(normal),
+                      _lib.ptr(depth_seg), _lib.ptr(depth_sigma), *grads_in, *[_lib.ptr(t) for t in out], kb,
+                      ws_ptr, nbytes, _lib.stream_ptr())
+        else:
+            kb = self._segments_per_ray(ctx.camera)
+            ws, ws_ptr, nbytes = self._records(inp, kb)
+            _lib.call("pf_trace_backward", _lib.ctypes.byref(inp), _lib.ptr(color), _lib.ptr(normal),
+                      _lib.ptr(depth_seg), _lib.ptr(depth_sigma), *grads_in, *[_lib.ptr(t) for t in out], kb,
+                      ws_ptr, nbytes, _lib.stream_ptr())
+        del ctx.tracer, ctx.camera, ctx.start, ctx.records
         g_pts, g_rad, g_nrm, g_den, g_sites, g_rgb, g_h = out
         return (None, None, None, g_pts, g_rad, g_den, g_nrm, g_sites, g_rgb, g_h, None, None, None, None, None,
                 None)

@@ -402,3 +402,32 @@ def test_nonfinite_attribute_raises(field):
     assert e.value.code == _lib.PF_ERR_NONFINITE
     R.forward(*args(sc))
     assert R.check()
+
+
+def test_gradients_into_a_flat_buffer():
+    """With Rasterizer.grad_buffer the adjoint writes every gradient into one
+    flat buffer (the multi-GPU exchange sums it in place): autograd's .grad
+    tensors are views of it and equal the gradients of the default path."""
+    from powerfoam_b200.multiview import GradBuffer, raster_fields
+
+    sc = np_scene(64, 500, -0.6, 0.6, 0.03, 0.15)
+    cam = torch_cam(np_camera((0.1, 0.3, 2.2), (0, 0, 0), 56, 40, 55.0))
+    adj, adj_off = (to_t(a) for a in cech_np(sc["points"], sc["radii"]))
+    w = to_t(np.random.default_rng(2).standard_normal((40, 56, 3)).astype(np.float32))
+    grads = []
+    for use_buffer in (False, True):
+        R = Rasterizer(Args(), "cuda")
+        if use_buffer:
+            R.grad_buffer = GradBuffer(raster_fields(500, 8), "cuda", world=3)
+        t = _params(sc)
+        out = R.forward(cam, None, t["points"], t["radii"], t["density"], t["normals"], t["texel_sites"],
+                        t["texel_rgb"], t["texel_height"], adj, adj_off, None, False)
+        (out[0] * w).sum().backward()
+        grads.append({k: v.grad for k, v in t.items()})
+        if use_buffer:
+            lo = R.grad_buffer.flat.data_ptr()
+            hi = lo + R.grad_buffer.flat.numel() * 4
+            for k, g in grads[-1].items():
+                assert lo <= g.data_ptr() < hi, k
+    for k in grads[0]:
+        assert_close_rel(grads[1][k].cpu().numpy(), grads[0][k].cpu().numpy(), 1e-5, k)

@@ -108,10 +108,12 @@ def test_trace_adjoint_matches_oracle(seed, thr, W, H):
 
 @pytest.mark.parametrize("kb", [0, 1, 3])
 @pytest.mark.parametrize("seed,thr", [(0, 1e-3), (2, 0.3)])
-def test_trace_adjoint_overflow(seed, thr, kb):
+@pytest.mark.parametrize("rec", [True, False])
+def test_trace_adjoint_overflow(seed, thr, kb, rec):
     """Few recorded segments per ray: most rays overflow and are finished by
-    the resume launch from their saved walk state (kb = 0: all of them)."""
-    _adjoint_case(seed, thr, 29, 21, kb)
+    the resume launch from their saved walk state (kb = 0: all of them);
+    records from the forward or from the adjoint's own walk."""
+    _adjoint_case(seed, thr, 29, 21, kb, record=rec)
 
 
 @pytest.mark.parametrize("S", [4, 6])
@@ -128,7 +130,7 @@ def test_trace_adjoint_per_ray_start_cells(kb):
     _adjoint_case(6, 1e-3, 29, 21, kb, per_ray_start=True)
 
 
-def _adjoint_case(seed, thr, W, H, kb, S=8, per_ray_start=False):
+def _adjoint_case(seed, thr, W, H, kb, S=8, per_ray_start=False, record=True):
     sc = np_scene(80 + seed, 300, -0.6, 0.6, 0.05, 0.15, S=S, height_scale=0.2)
     cam = np_camera((0.3, 0.2 * seed, 2.2), (0, 0, 0), W, H, 55.0)
     tp = {k: to_t(v).requires_grad_(True) for k, v in sc.items()}
@@ -141,6 +143,7 @@ def _adjoint_case(seed, thr, W, H, kb, S=8, per_ray_start=False):
         cells[: H // 2] = int(s)
     R = RayTracer(Args(), "cuda")
     R.segments_per_ray = kb
+    R.record_segments = record
     start = s if cells is None else to_t(cells)
     color, log_t, depth, normal = R.forward(torch_cam(cam), start, tp["points"], tp["radii"], tp["density"],
                                             tp["normals"], tp["texel_sites"], tp["texel_rgb"], tp["texel_height"],
@@ -175,8 +178,9 @@ def _adjoint_case(seed, thr, W, H, kb, S=8, per_ray_start=False):
 def test_trace_adjoint_paths_agree_at_scale():
     """131,072 primitives, 320x240: the gradient launch over recorded
     segments (96 per ray), records of one segment (nearly every ray resumed)
-    and none (every ray walked by the resume launch) give the same gradients
-    (the atomics sum in different orders: 1e-5 normwise)."""
+    and none (every ray walked by the resume launch), with the records
+    written by the forward or by the adjoint's own walk, give the same
+    gradients (the atomics sum in different orders: 1e-5 normwise)."""
     from powerfoam_b200 import synthetic
     from powerfoam_b200.adjacency import power_adjacency
 
@@ -188,9 +192,10 @@ def test_trace_adjoint_paths_agree_at_scale():
     s = start_cell(sc["points"], sc["radii"], cam.eye)
     tw = torch.rand((240, 320, 3), generator=torch.Generator().manual_seed(9)).cuda()
     grads = []
-    for kb in (96, 1, 0):
+    for kb, rec in ((96, True), (96, False), (1, True), (1, False), (0, True)):
         R = RayTracer(Args(), "cuda")
         R.segments_per_ray = kb
+        R.record_segments = rec
         p = {k: sc[k].clone().requires_grad_(True) for k in ["points", "radii", "density", "normals", "texel_sites",
                                                              "texel_height"]}
         c = rgb.clone().requires_grad_(True)
