@@ -65,6 +65,9 @@ def parse():
     p.add_argument("--no-autotune", action="store_true", help="batch workloads: use --tile, chunk 1")
     p.add_argument("--proposal-prims", type=int, default=0,
                    help="proposal workload: primitive count (default 6,291,456; radii scale with the spacing)")
+    p.add_argument("--proposal-scene", default="clouds", choices=["clouds", "shells"],
+                   help="proposal workload: the configuration's Gaussian clouds, or opaque shells (radius 0.12, "
+                   "thickness 0.02, density x30) in empty space")
     return p.parse_args()
 
 
@@ -509,7 +512,8 @@ def proposal_main(args, dev):
     walk's own labels (the bound a perfect proposal reaches)."""
     from powerfoam_b200 import synthetic
     from powerfoam_b200.adjacency import power_adjacency, power_adjacency_diff, start_cell
-    from powerfoam_b200.proposal import ProposalNet, SeededTracer, make_training_rays, trace_labels
+    from powerfoam_b200.proposal import (ProposalNet, SeededTracer, box_exit, camera_rays, make_training_rays,
+                                         trace_labels)
     from powerfoam_b200.raytrace import RayTracer
 
     cfg = dict(synthetic.CONFIGS["trace6m"])
@@ -518,8 +522,9 @@ def proposal_main(args, dev):
         cfg["n"] = args.proposal_prims
         cfg["r_range"] = tuple(r * s for r in cfg["r_range"])
     log = lambda m: print(m, file=sys.stderr, flush=True)  # noqa: E731
+    shells = (0.12, 0.02, 30.0) if args.proposal_scene == "shells" else None
     sc = synthetic.make_scene(cfg["n"], seed=cfg["seed"], mixture=cfg["mixture"], sigma=cfg["sigma"],
-                              r_range=cfg["r_range"], device=dev)
+                              r_range=cfg["r_range"], device=dev, shells=shells)
     t0 = time.perf_counter()
     adj, off = power_adjacency(sc["points"], sc["radii"])
     log(f"power adjacency {time.perf_counter() - t0:.1f} s, {adj.shape[0]} edges")
@@ -530,10 +535,12 @@ def proposal_main(args, dev):
                   sc["texel_height"], adj, off, pm)
     tr = RayTracer(Args(), dev)
 
+    box = (sc["points"].min(0).values, sc["points"].max(0).values)
+
     def labelled(seed0, k):
         cams = [synthetic.orbit_camera(seed0 + i, 32, 32, cfg["vfov"], device=dev) for i in range(k)]
         return make_training_rays(tr, cams, scene_args, [start_cell(sc["points"], sc["radii"], c.eye) for c in cams],
-                                  label_transmittance=0.999)
+                                  label_transmittance=0.999, box=box)
 
     t0 = time.perf_counter()
     rays8, val = labelled(10000, 2048), labelled(50000, 256)
@@ -543,7 +550,11 @@ def proposal_main(args, dev):
     hist = net.train(rays8, steps=5000, batch=65536, lr=1e-3, overshoot_weight=100.0, margin=0.1, graph_steps=100)
     torch.cuda.synchronize()
     train_s = time.perf_counter() - t0
-    seeded = SeededTracer(tr, net, sc["points"], sc["radii"], conf_threshold=net.calibrate(val))
+    t0 = time.perf_counter()
+    seeded = SeededTracer(tr, net, sc["points"], sc["radii"], conf_threshold=net.calibrate(val, max_unsafe_frac=1e-4),
+                          adjacency=adj, adjacency_offsets=off)
+    torch.cuda.synchronize()
+    vmap_s = time.perf_counter() - t0
     st = start_cell(sc["points"], sc["radii"], ev.eye)
 
     def timed(fn):
@@ -568,22 +579,32 @@ def proposal_main(args, dev):
     n_seeded = int(seeded.n_seeded.item()) // (args.steps + max(args.warmup, 3))
     lab = trace_labels(tr, ev, st, scene_args, label_transmittance=0.999)
     hit = lab["label_cell"] >= 0
+    # where the plain walk's cells go: rays that never reach a significant cell, and the cells
+    # hit rays walk before their first significant one (what a proposal can skip)
+    vc = plain.visit_count
+    stats = dict(nohit_rays=int((~hit).sum()), cells_nohit_rays=int(vc[~hit].sum()),
+                 cells_before_label=int(lab["label_step"][hit].sum()))
     one = torch.ones_like(lab["label_t"])
-    t_lab = torch.where(hit, lab["label_t"] - net.margin, -one).contiguous()
-    conf_lab = torch.where(hit, one, 0 * one).contiguous()
+    # the bound of a perfect proposal: hit rays seeded at their first significant cell, the others
+    # where they leave the primitives' box
+    t_exit = box_exit(camera_rays(ev), box[0], box[1]).view_as(lab["label_t"])
+    t_lab = (torch.where(hit, lab["label_t"], t_exit) - net.margin).contiguous()
+    conf_lab = one.contiguous()
     ideal_r, ideal_ms = timed(lambda: tr.trace(ev, seeded.locator.seed(ev, t_lab, conf_lab, 0.5, st), *scene_args,
                                                 check_status=False))
     H, W = cfg["height"], cfg["width"]
     line = dict(metric=METRIC, value=plain_ms / seed_ms, unit="x (plain / proposal-seeded frame time)", n_gpus=1,
                 steps=args.steps, warmup=max(args.warmup, 3), ms_per_step=seed_ms, higher_is_better=True,
                 scaling="weak", vs_baseline=None, dtype="f32 walk, bf16 network", data="synthetic",
-                config=dict(workload="proposal", prims=cfg["n"], width=W, height=H, plain_ms=plain_ms,
+                config=dict(workload="proposal", scene=args.proposal_scene, prims=cfg["n"], width=W, height=H,
+                            plain_ms=plain_ms,
                             seeded_ms=seed_ms, psnr_db=psnr(seed_r.color, plain.color), seeded_rays=n_seeded,
                             rays=H * W, threshold=seeded.conf_threshold, cells_plain=int(plain.visit_count.sum()),
                             cells_seeded=int(seed_r.visit_count.sum()), label_seed_ms=ideal_ms,
                             label_seed_psnr_db=psnr(ideal_r.color, plain.color),
                             label_seed_cells=int(ideal_r.visit_count.sum()), label_s=label_s, train_s=train_s,
-                            train_rays=int(rays8.shape[0]), loss_first=hist[0], loss_last=hist[-1]))
+                            train_rays=int(rays8.shape[0]), loss_first=hist[0], loss_last=hist[-1],
+                            voxel_map_s=vmap_s, **stats))
     print(json.dumps(line), flush=True)
 
 
@@ -599,8 +620,9 @@ def trace_main(args, dev):
     from powerfoam_b200.raytrace import RayTracer
 
     cfg = synthetic.CONFIGS["trace1m"]
+    shells = (0.12, 0.02, 30.0) if args.proposal_scene == "shells" else None
     sc = synthetic.make_scene(cfg["n"], seed=cfg["seed"], mixture=cfg["mixture"], sigma=cfg["sigma"],
-                              r_range=cfg["r_range"], device=dev)
+                              r_range=cfg["r_range"], device=dev, shells=shells)
     t0 = time.perf_counter()
     adj, off = power_adjacency(sc["points"], sc["radii"])
     torch.cuda.synchronize()

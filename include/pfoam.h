@@ -128,7 +128,8 @@ PF_API int pf_bin(const pf_camera *cam, int32_t tile_width, const float *spheres
  * No counterpart in the reference.  Limits: n_prims <= 65536,
  * pair_capacity <= 262144, at most 16384 tiles; larger problems return
  * PF_ERR_ARGS.  The first call on a device caches the array's address: make it
- * before any stream capture.  All calls share the array, so calls that may
+ * before any stream capture; a cudaDeviceReset afterwards leaves the cached
+ * address stale and is not supported.  All calls share the array, so calls that may
  * overlap on the GPU race and must be serialised by the caller.  Outputs and
  * *status as for pf_bin. */
 PF_API int pf_bin_noalloc(const pf_camera *cam, int32_t tile_width, const float *spheres, int64_t n_prims,
@@ -403,6 +404,33 @@ PF_API int pf_seed_start_cells(const float *points, const float *radii, int64_t 
                                const pf_camera *cam, const float *t_entry, const float *confidence,
                                float conf_threshold, int32_t default_start, int32_t *start_cells,
                                int32_t *n_seeded, void *stream);
+
+/* Point location by voxel map (no counterpart in the reference).
+ * pf_voxel_map_build: for a res^3 grid of cubic voxels over the box
+ * [box_lo, box_hi] (host, 3 floats each; edge max extent / res, res <= 1024),
+ * the power cell of every voxel centre (pf_locate_cells' rule; workspace: a
+ * built locator), cells (res^3) x-fastest; PF_ERR_SEED in *status (device,
+ * optional) if a centre was not settled.  Once per scene.
+ * pf_seed_start_cells_vmap: pf_seed_start_cells from the map: a seed point
+ * starts at its voxel's cell and walks along the segment from the voxel
+ * centre to the point across the power faces of `adjacency` (the tracer's
+ * exit rule on exact float32 faces) until the segment ends in the current
+ * cell; more than max_walk_steps crossings leave the ray unseeded.
+ * pf_locate_cells_vmap: the same location for points (n,3); -1 where the
+ * walk gave up. */
+PF_API int pf_voxel_map_build(const float *points, const float *radii, int64_t n_prims, const void *workspace,
+                              const float *box_lo, const float *box_hi, int32_t res, int32_t *cells, int32_t *status,
+                              void *stream);
+PF_API int pf_seed_start_cells_vmap(const float *points, const float *radii, int64_t n_prims,
+                                    const int32_t *adjacency, const int32_t *adjacency_offsets, const int32_t *cells,
+                                    const float *box_lo, const float *box_hi, int32_t res, const pf_camera *cam,
+                                    const float *t_entry, const float *confidence, float conf_threshold,
+                                    int32_t default_start, int32_t max_walk_steps, int32_t *start_cells,
+                                    int32_t *n_seeded, void *stream);
+PF_API int pf_locate_cells_vmap(const float *points, const float *radii, int64_t n_prims, const int32_t *adjacency,
+                                const int32_t *adjacency_offsets, const int32_t *cells, const float *box_lo,
+                                const float *box_hi, int32_t res, const float *queries, int64_t n_queries,
+                                int32_t max_walk_steps, int32_t *out, void *stream);
 
 /* ---------------------------------------------------------------------- */
 /* Ray-proposal network (no counterpart in the reference): 6-frequency

@@ -173,6 +173,12 @@ _SIGS = {
     "pf_locate_cells": [c_vp, c_vp, c_i64, c_vp, c_vp, c_i64, c_vp, c_vp, c_vp],
     "pf_seed_start_cells": [c_vp, c_vp, c_i64, c_vp, ctypes.POINTER(PfCamera), c_vp, c_vp, c_f, c_i32, c_vp, c_vp,
                             c_vp],
+    "pf_voxel_map_build": [c_vp, c_vp, c_i64, c_vp, ctypes.POINTER(c_f), ctypes.POINTER(c_f), c_i32, c_vp, c_vp,
+                           c_vp],
+    "pf_seed_start_cells_vmap": [c_vp, c_vp, c_i64, c_vp, c_vp, c_vp, ctypes.POINTER(c_f), ctypes.POINTER(c_f), c_i32,
+                                 ctypes.POINTER(PfCamera), c_vp, c_vp, c_f, c_i32, c_i32, c_vp, c_vp, c_vp],
+    "pf_locate_cells_vmap": [c_vp, c_vp, c_i64, c_vp, c_vp, c_vp, ctypes.POINTER(c_f), ctypes.POINTER(c_f), c_i32,
+                             c_vp, c_i64, c_i32, c_vp, c_vp],
     "pf_mlp_param_count": [],
     "pf_mlp_image_bytes": [],
     "pf_mlp_pack": [c_vp, c_vp, c_vp],

@@ -382,6 +382,131 @@ __global__ void locate_kernel(Locator L, const float* __restrict__ q, int64_t n,
     if (!exact && status) atomicMax(status, PF_ERR_SEED);
 }
 
+// ---------------------------------------------------------------------------
+// Point location by voxel map + walk (no counterpart in the reference, which
+// only locates the camera, benchmark.py:320-324).  A res^3 grid over a box
+// keeps the power cell of each voxel centre (exact, locate_point, built once
+// per scene); a point then starts at its voxel's cell and walks along the
+// segment from the voxel centre to the point across power faces -- the
+// tracer's exit rule (raytrace.py:160-241) on exact float32 faces -- until the
+// segment ends inside the current cell.
+struct VoxelGrid {
+    float lo[3];
+    float h, inv_h;
+    int res;
+};
+
+PF_D int64_t voxel_of(const VoxelGrid& g, v3 x, v3* centre) {
+    const float xs[3] = {x.x, x.y, x.z};
+    int c[3];
+    for (int k = 0; k < 3; k++) {
+        const float f = floorf((xs[k] - g.lo[k]) * g.inv_h);
+        const int v = (f == f) ? __float2int_rz(fminf(fmaxf(f, -1.0f), (float)g.res)) : 0;
+        c[k] = v < 0 ? 0 : (v >= g.res ? g.res - 1 : v);
+    }
+    *centre = mk(g.lo[0] + ((float)c[0] + 0.5f) * g.h, g.lo[1] + ((float)c[1] + 0.5f) * g.h,
+                 g.lo[2] + ((float)c[2] + 0.5f) * g.h);
+    return ((int64_t)c[2] * g.res + c[1]) * g.res + c[0];
+}
+
+__global__ void voxel_map_kernel(Locator L, VoxelGrid g, int32_t* __restrict__ cells, int32_t* __restrict__ status) {
+    const int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t n = (int64_t)g.res * g.res * g.res;
+    if (v >= n) return;
+    const int ix = (int)(v % g.res), iy = (int)((v / g.res) % g.res), iz = (int)(v / ((int64_t)g.res * g.res));
+    const v3 c = mk(g.lo[0] + ((float)ix + 0.5f) * g.h, g.lo[1] + ((float)iy + 0.5f) * g.h,
+                    g.lo[2] + ((float)iz + 0.5f) * g.h);
+    bool exact;
+    cells[v] = locate_point(L, c, &exact);
+    if (!exact && status) atomicMax(status, PF_ERR_SEED);
+}
+
+// the cell containing x, walking from cell `c` (which contains p0) along
+// p0 -> x; *ok = false when max_steps faces were crossed without reaching x
+PF_D int32_t walk_to_point(const float* __restrict__ pts, const float* __restrict__ radii,
+                           const int32_t* __restrict__ adj, const int32_t* __restrict__ adj_off, int64_t N,
+                           int32_t c, v3 p0, v3 x, int max_steps, bool* ok) {
+    const v3 u = x - p0;
+    for (int step = 0; step <= max_steps; step++) {
+        if (c < 0 || c >= N) break;
+        const v3 ci = mk(__ldg(pts + 3 * c), __ldg(pts + 3 * c + 1), __ldg(pts + 3 * c + 2));
+        const float ri = __ldg(radii + c);
+        const float pi = dot(ci, ci) - ri * ri;
+        float s_exit = 1.0f;  // the segment ends at x
+        int32_t next = -1;
+        const int32_t e1 = __ldg(adj_off + c + 1);
+        for (int32_t e = __ldg(adj_off + c); e < e1; e++) {
+            const int32_t j = __ldg(adj + e);
+            const v3 cj = mk(__ldg(pts + 3 * j), __ldg(pts + 3 * j + 1), __ldg(pts + 3 * j + 2));
+            const float rj = __ldg(radii + j);
+            // power face between c and j: 2 x.(cj - ci) = (|cj|^2 - rj^2) - (|ci|^2 - ri^2)
+            const v3 nrm = cj - ci;
+            const float nu = dot(nrm, u);
+            if (!(nu > 0.0f)) continue;
+            const float s = (0.5f * ((dot(cj, cj) - rj * rj) - pi) - dot(nrm, p0)) / nu;
+            if (s < s_exit) {
+                s_exit = s;
+                next = j;
+            }
+        }
+        if (next < 0) {
+            *ok = true;
+            return c;
+        }
+        c = next;
+    }
+    *ok = false;
+    return c;
+}
+
+// start cell of every pixel ray from the voxel map: the cell containing
+// eye + t d where the proposal is confident (conf >= conf_thr, t > 0), else
+// the default start (also when the walk needs more than max_steps faces)
+__global__ void seed_vmap_kernel(const float* __restrict__ pts, const float* __restrict__ radii,
+                                 const int32_t* __restrict__ adj, const int32_t* __restrict__ adj_off, int64_t N,
+                                 const int32_t* __restrict__ vcells, VoxelGrid g, Cam cam,
+                                 const float* __restrict__ t_entry, const float* __restrict__ conf, float conf_thr,
+                                 int32_t default_start, int max_steps, int32_t* __restrict__ start_cells,
+                                 int32_t* __restrict__ n_seeded) {
+    const int64_t px = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t n = (int64_t)cam.W * cam.H;
+    bool seeded = false;
+    if (px < n) {
+        int32_t cell = default_start;
+        const float t = t_entry[px];
+        if (conf[px] >= conf_thr && t > 0.0f) {
+            const int pi = (int)(px / cam.W), pj = (int)(px % cam.W);
+            const v3 x = cam.eye + t * ray_dir(cam, pi, pj);
+            v3 p0;
+            const int64_t v = voxel_of(g, x, &p0);
+            bool ok;
+            const int32_t c = walk_to_point(pts, radii, adj, adj_off, N, vcells[v], p0, x, max_steps, &ok);
+            if (ok) {
+                cell = c;
+                seeded = true;
+            }
+        }
+        start_cells[px] = cell;
+    }
+    const unsigned b = __ballot_sync(0xffffffffu, seeded);
+    if ((threadIdx.x & 31) == 0 && b && n_seeded) atomicAdd(n_seeded, __popc(b));
+}
+
+// points located through the voxel map (as seed_vmap_kernel), -1 where the walk gave up
+__global__ void locate_vmap_kernel(const float* __restrict__ pts, const float* __restrict__ radii,
+                                   const int32_t* __restrict__ adj, const int32_t* __restrict__ adj_off, int64_t N,
+                                   const int32_t* __restrict__ vcells, VoxelGrid g, const float* __restrict__ q,
+                                   int64_t nq, int max_steps, int32_t* __restrict__ out) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nq) return;
+    const v3 x = mk(q[3 * i], q[3 * i + 1], q[3 * i + 2]);
+    v3 p0;
+    const int64_t v = voxel_of(g, x, &p0);
+    bool ok;
+    const int32_t c = walk_to_point(pts, radii, adj, adj_off, N, vcells[v], p0, x, max_steps, &ok);
+    out[i] = ok ? c : -1;
+}
+
 // start cell of every pixel ray: the cell containing eye + t d where the
 // proposal is confident (conf >= conf_thr, t > 0), else the default start
 __global__ void seed_kernel(Locator L, Cam cam, const float* __restrict__ t_entry, const float* __restrict__ conf,
@@ -872,6 +997,65 @@ extern "C" int pf_seed_start_cells(const float* points, const float* radii, int6
     seed_kernel<<<(unsigned)((n + 127) / 128), 128, 0, (cudaStream_t)stream>>>(
         loc, load_cam(*cam), t_entry, confidence, conf_threshold, default_start, start_cells, n_seeded);
     return pf_check_launch("pf_seed_start_cells");
+}
+
+static bool voxel_grid(const float* lo, const float* hi, int32_t res, VoxelGrid* g) {
+    if (!lo || !hi || res < 1 || res > 1024) return false;
+    float ext = 0.f;
+    for (int k = 0; k < 3; k++) {
+        if (!(hi[k] >= lo[k])) return false;
+        ext = fmaxf(ext, hi[k] - lo[k]);
+    }
+    ext = fmaxf(ext, 1e-6f);
+    for (int k = 0; k < 3; k++) g->lo[k] = lo[k];
+    g->h = ext / (float)res;
+    g->inv_h = 1.0f / g->h;
+    g->res = res;
+    return true;
+}
+
+extern "C" int pf_voxel_map_build(const float* points, const float* radii, int64_t n_prims, const void* workspace,
+                                  const float* box_lo, const float* box_hi, int32_t res, int32_t* cells,
+                                  int32_t* status, void* stream) {
+    VoxelGrid g;
+    if (n_prims <= 0 || !points || !radii || !workspace || !cells || !voxel_grid(box_lo, box_hi, res, &g))
+        return pf_fail(PF_ERR_ARGS, "pf_voxel_map_build: bad arguments");
+    Locator loc = locator_view(points, radii, n_prims, (char*)workspace);
+    const int64_t n = (int64_t)res * res * res;
+    voxel_map_kernel<<<(unsigned)((n + 127) / 128), 128, 0, (cudaStream_t)stream>>>(loc, g, cells, status);
+    return pf_check_launch("pf_voxel_map_build");
+}
+
+extern "C" int pf_seed_start_cells_vmap(const float* points, const float* radii, int64_t n_prims,
+                                        const int32_t* adjacency, const int32_t* adjacency_offsets,
+                                        const int32_t* cells, const float* box_lo, const float* box_hi, int32_t res,
+                                        const pf_camera* cam, const float* t_entry, const float* confidence,
+                                        float conf_threshold, int32_t default_start, int32_t max_walk_steps,
+                                        int32_t* start_cells, int32_t* n_seeded, void* stream) {
+    VoxelGrid g;
+    if (n_prims <= 0 || !points || !radii || !adjacency_offsets || !cells || !cam || !t_entry || !confidence ||
+        !start_cells || cam->width < 2 || cam->height < 2 || default_start < 0 || default_start >= n_prims ||
+        max_walk_steps < 0 || !voxel_grid(box_lo, box_hi, res, &g))
+        return pf_fail(PF_ERR_ARGS, "pf_seed_start_cells_vmap: bad arguments");
+    const int64_t n = (int64_t)cam->width * cam->height;
+    seed_vmap_kernel<<<(unsigned)((n + 127) / 128), 128, 0, (cudaStream_t)stream>>>(
+        points, radii, adjacency, adjacency_offsets, n_prims, cells, g, load_cam(*cam), t_entry, confidence,
+        conf_threshold, default_start, max_walk_steps, start_cells, n_seeded);
+    return pf_check_launch("pf_seed_start_cells_vmap");
+}
+
+extern "C" int pf_locate_cells_vmap(const float* points, const float* radii, int64_t n_prims,
+                                    const int32_t* adjacency, const int32_t* adjacency_offsets, const int32_t* cells,
+                                    const float* box_lo, const float* box_hi, int32_t res, const float* queries,
+                                    int64_t n_queries, int32_t max_walk_steps, int32_t* out, void* stream) {
+    VoxelGrid g;
+    if (n_prims <= 0 || !points || !radii || !adjacency_offsets || !cells || n_queries < 0 ||
+        (n_queries > 0 && (!queries || !out)) || max_walk_steps < 0 || !voxel_grid(box_lo, box_hi, res, &g))
+        return pf_fail(PF_ERR_ARGS, "pf_locate_cells_vmap: bad arguments");
+    if (n_queries == 0) return PF_OK;
+    locate_vmap_kernel<<<(unsigned)((n_queries + 127) / 128), 128, 0, (cudaStream_t)stream>>>(
+        points, radii, adjacency, adjacency_offsets, n_prims, cells, g, queries, n_queries, max_walk_steps, out);
+    return pf_check_launch("pf_locate_cells_vmap");
 }
 
 extern "C" int pf_morton_workspace_size(int64_t n_prims, size_t* bytes) {

@@ -616,7 +616,9 @@ extern "C" int pf_bin_generic(const pf_camera* cam, const float* ray_maps, int32
 //
 // The first call on a device looks up the array's device address (with that
 // device current) and caches it; make that first call before any stream
-// capture.  Every call shares the one array: calls whose work may overlap on
+// capture.  The cached address belongs to the device's primary context: a
+// cudaDeviceReset (or another context made current on that device) leaves it
+// stale, and calls after one are not supported.  Every call shares the one array: calls whose work may overlap on
 // the GPU (different streams, or different host threads, without ordering
 // between them) race on it and must be serialised by the caller.  No part of
 // the scratch needs to start at zero: every buffer in it is written before it

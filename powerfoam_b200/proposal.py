@@ -121,18 +121,27 @@ class ProposalNet:
         self.check()
         return history
 
-    def calibrate(self, rays8, max_unsafe=0, floor=0.9):
+    def calibrate(self, rays8, max_unsafe=0, floor=0.9, max_unsafe_frac=0.0):
         """Confidence threshold from held-out labelled rays (n, 8): the plain
         walk judges each seed, and the threshold sits just above the
-        confidence of the (max_unsafe + 1)-th most confident seed that would
-        have started past its first significant cell (never below `floor`)."""
+        confidence of the (k + 1)-th most confident seed that would have
+        started past its first significant cell, k = max(max_unsafe,
+        max_unsafe_frac * n) (never below `floor`; rays flagged as never
+        reaching one are safe anywhere)."""
         rays8 = rays8.to(torch.float32).contiguous()
         t, c = self.forward(rays=rays8[:, :6].contiguous())
         lab = rays8[:, 6]
-        unsafe = (lab >= 0) & (t - self.margin > lab)
+        # a ray flagged as never reaching a significant cell is safe wherever it is seeded
+        unsafe = (lab >= 0) & (rays8[:, 7] == 0) & (t - self.margin > lab)
+        k = max(int(max_unsafe), int(max_unsafe_frac * rays8.shape[0]))
         cu = torch.sort(c[unsafe], descending=True).values
-        thr = float(cu[max_unsafe]) if cu.numel() > max_unsafe else 0.0
+        thr = float(cu[k]) if cu.numel() > k else 0.0
         return max(floor, math.nextafter(thr, 2.0))
+
+    def seed_fraction(self, rays8, threshold):
+        """Share of the rays (n, 8) the gate at `threshold` would seed."""
+        t, c = self.forward(rays=rays8[:, :6].to(torch.float32).contiguous())
+        return float(((c >= threshold) & (t - self.margin > 0)).float().mean())
 
     def check(self):
         s = int(self.status.item())
@@ -185,15 +194,37 @@ def camera_rays(camera):
     return torch.cat([o, d], dim=-1).reshape(-1, 6)
 
 
-def make_training_rays(tracer, cameras, scene_args, start_cells, label_transmittance=LABEL_TRANSMITTANCE):
-    """(n, 8) training rays (origin, direction, label t or -1, 0) from the
-    plain walk of every pixel of every camera."""
+def box_exit(rays, lo, hi):
+    """Distance along each ray (n, 6: origin, unit direction) at which it
+    leaves the box [lo, hi]; 0 for rays that miss it or leave behind."""
+    o, d = rays[:, :3], rays[:, 3:6]
+    inv = 1.0 / torch.where(d == 0, torch.full_like(d, 1e-30), d)
+    t0, t1 = (lo - o) * inv, (hi - o) * inv
+    t_near = torch.minimum(t0, t1).max(-1).values
+    t_far = torch.maximum(t0, t1).min(-1).values
+    return torch.where((t_far >= t_near) & (t_far > 0), t_far, torch.zeros_like(t_far))
+
+
+def make_training_rays(tracer, cameras, scene_args, start_cells, label_transmittance=LABEL_TRANSMITTANCE,
+                       box=None):
+    """(n, 8) training rays (origin, direction, label t, no-hit flag) from the
+    plain walk of every pixel of every camera.  The label is the entry t of the
+    first cell after which the transmittance is below label_transmittance.
+    Rays that never get there have label -1, or with ``box`` (lo, hi) of the
+    primitives the t at which they leave it and flag 1: seeding them there
+    skips a walk that composites next to nothing (the transmittance stays
+    above label_transmittance all the way)."""
     parts = []
     for cam, start in zip(cameras, start_cells):
         lab = trace_labels(tracer, cam, start, scene_args, label_transmittance)
         r = camera_rays(cam)
         t = lab["label_t"].reshape(-1, 1)
-        parts.append(torch.cat([r, t, torch.zeros_like(t)], dim=-1))
+        flag = torch.zeros_like(t)
+        if box is not None:
+            miss = t[:, 0] < 0
+            t = torch.where(miss[:, None], box_exit(r, box[0], box[1])[:, None], t)
+            flag = miss[:, None].to(t.dtype)
+        parts.append(torch.cat([r, t, flag], dim=-1))
     return torch.cat(parts, 0).contiguous()
 
 
@@ -227,16 +258,67 @@ class CellLocator:
         return start
 
 
+class VoxelLocator:
+    """Point location through a voxel map (pf_voxel_map_build): the power cell
+    of every voxel centre of a res^3 grid over the primitives' bounding box,
+    located exactly once per scene; a point then walks from its voxel's cell
+    across the power faces of `adjacency` to the cell that contains it (a few
+    faces), where CellLocator searches a grid of primitives for every query."""
+
+    def __init__(self, points, radii, adjacency, adjacency_offsets, res=256, max_walk_steps=64):
+        self.points = points.float().contiguous()
+        self.radii = radii.float().contiguous()
+        self.adjacency = adjacency.to(torch.int32).contiguous()
+        self.adjacency_offsets = adjacency_offsets.to(torch.int32).contiguous()
+        self.res = int(res)
+        self.max_walk_steps = int(max_walk_steps)
+        lo = self.points.min(0).values.cpu().tolist()
+        hi = self.points.max(0).values.cpu().tolist()
+        self.box = ((_lib.c_f * 3)(*lo), (_lib.c_f * 3)(*hi))
+        exact = CellLocator(self.points, self.radii)
+        self.cells = torch.empty(self.res ** 3, dtype=torch.int32, device=self.points.device)
+        status = torch.zeros(1, dtype=torch.int32, device=self.points.device)
+        _lib.call("pf_voxel_map_build", _lib.ptr(self.points), _lib.ptr(self.radii), self.points.shape[0],
+                  _lib.ptr(exact.ws), self.box[0], self.box[1], self.res, _lib.ptr(self.cells), _lib.ptr(status),
+                  _lib.stream_ptr())
+        st = int(status.item())
+        if st != _lib.PF_OK:
+            raise _lib.PfError(st, "a voxel centre could not be located")
+
+    def _common(self):
+        return (_lib.ptr(self.points), _lib.ptr(self.radii), self.points.shape[0], _lib.ptr(self.adjacency),
+                _lib.ptr(self.adjacency_offsets), _lib.ptr(self.cells), self.box[0], self.box[1], self.res)
+
+    def locate(self, queries):
+        """Cells containing queries (n, 3); -1 where the walk gave up."""
+        q = queries.float().contiguous()
+        out = torch.empty(q.shape[0], dtype=torch.int32, device=q.device)
+        _lib.call("pf_locate_cells_vmap", *self._common(), _lib.ptr(q), q.shape[0], self.max_walk_steps,
+                  _lib.ptr(out), _lib.stream_ptr())
+        return out
+
+    def seed(self, camera, t_entry, confidence, conf_threshold, default_start, n_seeded=None):
+        H, W = camera.height, camera.width
+        start = torch.empty((H, W), dtype=torch.int32, device=self.points.device)
+        _lib.call("pf_seed_start_cells_vmap", *self._common(), _lib.ctypes.byref(camera.to_pf()),
+                  _lib.ptr(t_entry), _lib.ptr(confidence), float(conf_threshold), int(default_start),
+                  self.max_walk_steps, _lib.ptr(start), _lib.ptr(n_seeded), _lib.stream_ptr())
+        return start
+
+
 class SeededTracer:
     """Proposal-seeded cell walk: network forward over the pixel rays, start
     cells from the locator where the confidence reaches the threshold, then
     the tracer's walk from those cells (plain start cell elsewhere)."""
 
-    def __init__(self, tracer, net, points, radii, conf_threshold=0.9):
+    def __init__(self, tracer, net, points, radii, conf_threshold=0.9, adjacency=None, adjacency_offsets=None,
+                 voxel_res=256):
         self.tracer = tracer
         self.net = net
         self.conf_threshold = conf_threshold
-        self.locator = CellLocator(points, radii)
+        # with the walk's adjacency: voxel-map location (a few faces per seed), else the grid search
+        self.locator = (VoxelLocator(points, radii, adjacency, adjacency_offsets, voxel_res)
+                        if adjacency is not None else CellLocator(points, radii))
         self.n_seeded = torch.zeros(1, dtype=torch.int32, device=tracer.device)
 
     def start_cells(self, camera, default_start):

@@ -60,21 +60,36 @@ def morton_order_cpu(points):
 
 
 def make_scene(n, seed=0, mixture=0, sigma=0.15, r_range=(0.01, 0.05), n_sites=8, sh_std=0.2, device="cuda",
-               morton=True):
+               morton=True, shells=None):
+    """``shells`` = (radius, thickness, density scale): the mixture's
+    components are spherical shells of that radius and thickness around the
+    means instead of Gaussians, their density scaled, and the 10 % background
+    points get density 0 (opaque shells in empty space)."""
     g = torch.Generator().manual_seed(seed)
+    background = torch.zeros(n, dtype=torch.bool)
     if mixture:
         means = torch.rand(mixture, 3, generator=g) * 2 - 1
         n_uni = n // 10
         comp = torch.randint(0, mixture, (n - n_uni,), generator=g)
-        pts_m = means[comp] + torch.randn(n - n_uni, 3, generator=g) * sigma
+        if shells is None:
+            pts_m = means[comp] + torch.randn(n - n_uni, 3, generator=g) * sigma
+        else:
+            u = torch.randn(n - n_uni, 3, generator=g)
+            u = u / u.norm(dim=-1, keepdim=True)
+            rad = shells[0] + shells[1] * (torch.rand(n - n_uni, 1, generator=g) - 0.5)
+            pts_m = means[comp] + u * rad
         pts_u = torch.rand(n_uni, 3, generator=g) * 2 - 1
         points = torch.cat([pts_m, pts_u], 0)
-        points = points[torch.randperm(n, generator=g)]
+        background[n - n_uni:] = True
+        perm0 = torch.randperm(n, generator=g)
+        points, background = points[perm0], background[perm0]
     else:
         points = torch.rand(n, 3, generator=g) * 2 - 1
     lr = torch.rand(n, generator=g) * (math.log(r_range[1]) - math.log(r_range[0])) + math.log(r_range[0])
     radii = torch.exp(lr)
     density = torch.nn.functional.softplus(torch.randn(n, generator=g)) * 10
+    if shells is not None:
+        density = torch.where(background, torch.zeros_like(density), density * shells[2])
     q = torch.randn(n, 4, generator=g)
     normals, tangents, bitangents = quat_frames(q)
     s2 = torch.randn(n, n_sites, 2, generator=g) * 0.1

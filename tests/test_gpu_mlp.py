@@ -195,23 +195,60 @@ def test_locate_cells_match_brute_force():
     assert np.array_equal(got, np.argmin(pd, axis=1).astype(np.int32))
 
 
+@pytest.mark.parametrize("res", [8, 64])
+def test_voxel_map_location_matches_brute_force(res):
+    """Points located from the voxel map (their voxel's cell, then a walk
+    across power faces) are in the cell of least power distance: the same
+    cell, or one whose power distance equals it to float32 rounding (a point
+    on a face).  Coarse (8^3, long walks) and fine (64^3) maps; points inside,
+    near sites and far outside the primitives' box."""
+    from powerfoam_b200.adjacency import power_adjacency
+    from powerfoam_b200.proposal import VoxelLocator
+
+    sc = np_scene(43, 5000, -0.8, 0.8, 0.01, 0.06)
+    pts, rad = sc["points"], sc["radii"]
+    adj, off = power_adjacency(to_t(pts), to_t(rad))
+    rng = np.random.default_rng(44)
+    q = np.concatenate([rng.uniform(-1.0, 1.0, (4000, 3)), pts[:500] + 1e-4,
+                        rng.uniform(-3, 3, (300, 3))]).astype(np.float32)
+    loc = VoxelLocator(to_t(pts), to_t(rad), adj, off, res=res, max_walk_steps=256)
+    got = loc.locate(to_t(q)).cpu().numpy()
+    assert (got >= 0).all()
+    d = q[:, None, :].astype(np.float64) - pts[None, :, :].astype(np.float64)
+    pd = (d * d).sum(-1) - (rad.astype(np.float64) ** 2)[None, :]
+    rows = np.arange(q.shape[0])
+    best = np.argmin(pd, axis=1)
+    same = got == best
+    gap = pd[rows, got] - pd[rows, best]
+    assert same.mean() >= 0.999
+    assert (gap[~same] <= 1e-5 * (1.0 + np.abs(pd[rows, best][~same]))).all()
+
+
 def psnr(a, b):
     mse = float(((a.double() - b.double()) ** 2).mean())
     return 10 * np.log10(1.0 / max(mse, 1e-20))
 
 
 def test_trained_proposal_seeds_at_50db():
-    """Train on plain-walk labels of 2M rays (2048 small random views),
-    calibrate the confidence gate on 256 more, evaluate on held-out views:
-    the seeded walk keeps >= 50 dB PSNR against the plain walk and visits no
-    more cells.  Seeding from the plain walk's own labels through the same
-    point location shows the headroom a perfect proposal would have (>= 50 dB
-    with fewer cells); the trained network's share of it is printed."""
+    """Train on plain-walk labels of 2M rays (2048 small random views of a
+    scene of opaque shells in empty space; rays
+    that never reach a significant cell labelled with the distance at which
+    they leave the primitives' box), calibrate the confidence gate on 256
+    more, evaluate on held-out views: the network seeds a real share of the
+    rays, the seeded walk visits fewer cells than the plain walk and keeps
+    >= 50 dB PSNR against it.  Seeding from the plain walk's own labels
+    through the same voxel-map location shows the headroom a perfect
+    proposal would have (>= 50 dB with fewer cells)."""
+    from powerfoam_b200.proposal import box_exit
     from powerfoam_b200 import synthetic
 
+    # opaque shells in empty space: most rays never reach a significant cell, so a proposal has
+    # something to skip (on the cloud scene of the 6.3M-primitive workload even seeding from the
+    # plain walk's own labels saves no time: bench.py --workload proposal)
     n = 60000
     scale = (6291456 / n) ** (1 / 3)
-    sc = synthetic.make_scene(n, seed=4, mixture=64, sigma=0.1, r_range=(0.001 * scale, 0.01 * scale))
+    sc = synthetic.make_scene(n, seed=4, mixture=16, sigma=0.1, r_range=(0.001 * scale, 0.01 * scale),
+                              shells=(0.12, 0.02, 30.0))
     rgb = synthetic.texel_rgb(sc, synthetic.front_camera(64, 64, 50.0))
     adj, off = build_power_adjacency(sc["points"], sc["radii"])
     pm = power_adjacency_diff(sc["points"], sc["radii"], adj, off)
@@ -223,16 +260,22 @@ def test_trained_proposal_seeds_at_50db():
         cams = [synthetic.orbit_camera(seed0 + i, w, h, 50.0) for i in range(k)]
         return cams, [start_cell(sc["points"], sc["radii"], c.eye) for c in cams]
 
+    box = (sc["points"].min(0).values, sc["points"].max(0).values)
+
     def labelled(seed0, k):
         cams, starts = views(seed0, k, 32, 32)
-        return make_training_rays(tr, cams, args, starts, label_transmittance=0.999)
+        return make_training_rays(tr, cams, args, starts, label_transmittance=0.999, box=box)
 
     rays8 = labelled(10000, 2048)
     val = labelled(50000, 256)
     net = ProposalNet("cuda", seed=1)
-    hist = net.train(rays8, steps=3000, batch=65536, lr=1e-3, overshoot_weight=100.0, margin=0.1, graph_steps=100)
+    hist = net.train(rays8, steps=5000, batch=65536, lr=1e-3, overshoot_weight=100.0, margin=0.1, graph_steps=100)
     assert hist[-1][0] < hist[0][0] and hist[-1][1] < hist[0][1]
-    seeded_tr = SeededTracer(tr, net, sc["points"], sc["radii"], conf_threshold=net.calibrate(val))
+    thr = net.calibrate(val, max_unsafe_frac=1e-4)
+    print(f"calibrated threshold {thr:.5f}: {net.seed_fraction(val, thr):.3f} of the held-out rays seeded "
+          f"(strict: {net.calibrate(val):.5f}, {net.seed_fraction(val, net.calibrate(val)):.3f})")
+    seeded_tr = SeededTracer(tr, net, sc["points"], sc["radii"], conf_threshold=thr, adjacency=adj,
+                             adjacency_offsets=off)
     for ev in (synthetic.orbit_camera(900 + i, 256, 192, 50.0) for i in range(2)):
         st = start_cell(sc["points"], sc["radii"], ev.eye)
         plain = tr.trace(ev, st, *args)
@@ -241,13 +284,15 @@ def test_trained_proposal_seeds_at_50db():
         lab = trace_labels(tr, ev, st, args, label_transmittance=0.999)
         hit = lab["label_cell"] >= 0
         one = torch.ones_like(lab["label_t"])
-        t_lab = torch.where(hit, lab["label_t"] - net.margin, -one).contiguous()
-        ideal_start = seeded_tr.locator.seed(ev, t_lab, torch.where(hit, one, 0 * one).contiguous(), 0.5, st)
+        t_exit = box_exit(camera_rays(ev), box[0], box[1]).view_as(lab["label_t"])
+        t_lab = (torch.where(hit, lab["label_t"], t_exit) - net.margin).contiguous()
+        ideal_start = seeded_tr.locator.seed(ev, t_lab, one.contiguous(), 0.5, st)
         ideal = tr.trace(ev, ideal_start, *args)
         torch.cuda.synchronize()
         v_plain, v_seed, v_ideal = (int(r.visit_count.sum()) for r in (plain, seeded, ideal))
         p, p_ideal = psnr(seeded.color, plain.color), psnr(ideal.color, plain.color)
         print(f"threshold {seeded_tr.conf_threshold:.5f}: seeded {int(seeded_tr.n_seeded.item())}/{256 * 192} "
               f"rays, {p:.1f} dB, cells {v_seed}/{v_plain}; label seeding {p_ideal:.1f} dB, cells {v_ideal}")
-        assert p >= 50.0 and v_seed <= v_plain
+        assert int(seeded_tr.n_seeded.item()) >= 0.05 * 256 * 192
+        assert p >= 50.0 and v_seed < v_plain
         assert p_ideal >= 50.0 and v_ideal < v_plain

@@ -84,3 +84,28 @@ def test_noalloc_rejects_problems_above_its_limits():
     rc = lib.pf_bin_noalloc(ctypes.byref(c), 8, _lib.ptr(sph), 1000, 1 << 20, _lib.ptr(out), _lib.ptr(out), None,
                             None, None, _lib.ptr(out), _lib.ptr(out), _lib.stream_ptr())
     assert rc == _lib.PF_ERR_ARGS
+
+
+def test_noalloc_at_its_limits():
+    """The largest problem the static array is sized for -- 65,536
+    primitives, a pair capacity of 262,144 and 16,384 tiles (1024 x 1024 at
+    tile 8) -- bins exactly as pf_bin does; one tile more (1160 x 904: 145 x
+    113 = 16,385 tiles) is refused with PF_ERR_ARGS before anything runs."""
+    tw, cap = 8, 1 << 18
+    sc = np_scene(103, 1 << 16, -1.0, 1.0, 0.002, 0.01)
+    cam = np_camera((0.3, 0.2, 2.5), (0, 0, 0), 1024, 1024, 55.0)
+    sph = to_t(packed(sc)[0])
+    T = (1024 // tw) * (1024 // tw)
+    assert T == 1 << 14
+    a = _bin("noalloc", cam, tw, sph, cap)
+    b = _bin("pf_bin", cam, tw, sph, cap, _workspace(sph.shape[0], cap, T))
+    assert a["n"] == b["n"] and a["n"] > 0
+    for k in ["offs", "prims", "keys", "vis", "order"]:
+        assert np.array_equal(a[k], b[k]), k
+    lib = _lib.load()
+    c = torch_cam(np_camera((0.0, 0.0, 2.5), (0, 0, 0), 1160, 904, 55.0)).to_pf()
+    out = torch.zeros(8, dtype=torch.int64, device="cuda")
+    rc = lib.pf_bin_noalloc(ctypes.byref(c), tw, _lib.ptr(sph), 1000, 1024, _lib.ptr(out), _lib.ptr(out), None, None,
+                            None, _lib.ptr(out), _lib.ptr(out), _lib.stream_ptr())
+    assert rc == _lib.PF_ERR_ARGS
+    assert b"16384" in lib.pf_last_error()
