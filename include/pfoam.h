@@ -444,10 +444,12 @@ PF_API int pf_locate_cells_vmap(const float *points, const float *radii, int64_t
  * pf_mlp_forward: rays (n,6) = origin, unit direction, or every pixel ray of
  *   `cam` when rays is NULL; writes t_entry (world units) and confidence.
  * pf_mlp_train_step: one minibatch of `batch` rays drawn (hashed with *step
- *   and seed) from rays (n,8) = origin, direction, label t (< 0: no hit), pad;
- *   loss = asymmetric squared error of t / 6 (overshoot_weight on
- *   over-estimates) + cross-entropy of the confidence against "seed is safe"
- *   (hit and t_pred - margin <= t); ADDS the mean-loss gradient into grad and
+ *   and seed) from rays (n,8) = origin, direction, label t (< 0: no label),
+ *   no-hit flag (nonzero: the ray never reaches a significant cell and t is
+ *   where it leaves the primitives' box); loss = asymmetric squared error of
+ *   t / 6 (overshoot_weight on over-estimates of unflagged rays) +
+ *   cross-entropy of the confidence against "seed is safe" (t >= 0 and either
+ *   flagged or t_pred - margin <= t); ADDS the mean-loss gradient into grad and
  *   the loss sums into loss[0..1] (may be NULL).
  * pf_mlp_adam: Adam on the master weights, clears grad, writes the image and
  *   advances *step (done: a device word, zero before the first call).
@@ -529,6 +531,27 @@ PF_API int pf_batch_render(const pf_batch_scene *scene, const pf_batch_view *vie
                            float *tile_loss, float *grad_points, float *grad_radii, float *grad_normals,
                            float *grad_density, float *grad_texel_sites, float *grad_texel_height,
                            int32_t *status, void *stream);
+
+/* Schedule tuner for pf_batch_render at one tile width (the views binned at
+ * that width): for each candidate, `warmup` untimed calls, then `iters` calls
+ * timed with CUDA events on `stream`; writes each candidate's mean ms and the
+ * index of the fastest into *best.  The host waits for every candidate's
+ * events (not capturable); the outputs hold the last call's results.  The
+ * tile width itself is swept by the caller, which bins the views at each
+ * width (powerfoam_b200/batch.py autotune). */
+typedef struct pf_batch_schedule {
+    int32_t chunk;
+    int32_t order; /* PF_BATCH_ORDER_* */
+    int32_t split;
+    float ms;      /* written */
+} pf_batch_schedule;
+
+PF_API int pf_batch_autotune(const pf_batch_scene *scene, const pf_batch_view *views, int32_t n_views,
+                             int32_t tile_width, pf_batch_schedule *candidates, int32_t n_candidates,
+                             int32_t warmup, int32_t iters, void *workspace, size_t workspace_bytes,
+                             float *tile_loss, float *grad_points, float *grad_radii, float *grad_normals,
+                             float *grad_density, float *grad_texel_sites, float *grad_texel_height,
+                             int32_t *status, int32_t *best, void *stream);
 
 /* ---------------------------------------------------------------------- */
 /* Texel colour pre-step for the synthetic scenes: degree-3 real SH (16

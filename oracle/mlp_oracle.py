@@ -127,13 +127,14 @@ def loss_value(params, rays8, idx, w_over=10.0, margin=0.02, safe=None):
     fixes the confidence targets (they are a step function of the output)."""
     rb = np.asarray(rays8, np.float32)[idx]
     t_lab = rb[:, 6].astype(np.float64)
+    flagged = rb[:, 7] != 0
     _, _, _, zs = forward(params, rb[:, :6], cache=True, exact=True)
     z0, z1 = zs[3][:, 0], zs[3][:, 1]
     hit = t_lab >= 0
     e = z0 - t_lab / T_SCALE
-    w = np.where(e > 0, w_over, 1.0)
+    w = np.where((e > 0) & ~flagged, w_over, 1.0)
     if safe is None:
-        safe = (hit & (z0 * T_SCALE - margin <= t_lab)).astype(np.float64)
+        safe = (hit & (flagged | (z0 * T_SCALE - margin <= t_lab))).astype(np.float64)
     p = 1.0 / (1.0 + np.exp(-z1))
     lt = np.where(hit, w * e * e, 0.0)
     lc = -(safe * np.log(p) + (1 - safe) * np.log(1 - p))
@@ -146,14 +147,15 @@ def train_grad(params, rays8, batch, step, seed, w_over=10.0, margin=0.02, exact
     idx = batch_indices(batch, r.shape[0], step, seed)
     rb = r[idx]
     t_lab = rb[:, 6].astype(np.float64)
+    flagged = rb[:, 7] != 0  # never reaches a significant cell: any seed is safe, no overshoot weight
     W = [_round(w, exact).astype(np.float64) for w in layers(params)]
     _, _, acts, zs = forward(params, rb[:, :6], cache=True, exact=exact)
     z0 = zs[3][:, 0].astype(np.float64)
     z1 = zs[3][:, 1].astype(np.float64)
     hit = t_lab >= 0
     e = z0 - t_lab / T_SCALE
-    w = np.where(e > 0, w_over, 1.0)
-    safe = (hit & (z0 * T_SCALE - margin <= t_lab)).astype(np.float64)
+    w = np.where((e > 0) & ~flagged, w_over, 1.0)
+    safe = (hit & (flagged | (z0 * T_SCALE - margin <= t_lab))).astype(np.float64)
     p = 1.0 / (1.0 + np.exp(-z1))
     if exact:
         g0 = np.where(hit, 2.0 * w * e / batch, 0.0)

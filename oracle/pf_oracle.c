@@ -1475,6 +1475,13 @@ int FN(orc_raster_visualize)(const orc_camera *camera, int TW, const float *sphe
 /*    start_idx, as the reference does);                                     */
 /*  - a step cap (the reference loops without bound); hitting it sets the   */
 /*    ray's status to ORC_ERR_STEP_CAP;                                      */
+/*  - the cycle guard (cycle_closed): the next cell is a function of the    */
+/*    current one (raytrace.py:183-199), so a ray that returns to a cell    */
+/*    with no hit since (sphere hit, tn <= tf, sigma >= 1e-3) repeats those */
+/*    cells forever with an unchanged transmittance -- the reference never  */
+/*    returns from such a ray.  The walk keeps the cell of step 0, 1, 2, 4, */
+/*    ... (Brent's power-of-two saves) and ends when it comes back to it    */
+/*    with no hit since; rays the reference finishes never meet the guard;  */
 /*  - depth (first crossing of T < depth_quantile, visualization_kernel's   */
 /*    formula), normal (sum alpha*T*n, forward_kernel's formula), final      */
 /*    log transmittance, and the visited-cell log (every cell whose sphere  */
@@ -1483,6 +1490,15 @@ int FN(orc_raster_visualize)(const orc_camera *camera, int TW, const float *sphe
 /* cell's sigma (-1 / 0 when the ray never crosses the quantile); they are   */
 /* the only state the backward needs besides the forward outputs.            */
 #define NO_CELL 0x7FFFFFFF
+
+static int cycle_closed(int32_t *saved, int *hit_since, int32_t prim, int steps) {
+    if (prim == *saved && !*hit_since) return 1;
+    if ((steps & (steps - 1)) == 0) {
+        *saved = prim;
+        *hit_since = 0;
+    }
+    return 0;
+}
 
 /* (c_j - c_i, pm_j - pm_i) of neighbour e: from the float16 encoding of
  * benchmark.py:296-302, or exactly from the spheres when adj_diff == NULL
@@ -1542,10 +1558,13 @@ static int FN(trace_walk)(const orc_camera *camera, const float *spheres, const 
         real dout = 0, dsig = 0;
         real lab_t = -1;
         int32_t lab_cell = -1, lab_step = -1;
+        int32_t cg_saved = -1;
+        int cg_hit = 0;
         for (;;) {
             real trans = r_exp(log_t);
             if (trans < (real)thr || prim == NO_CELL) break;
             if (steps >= max_steps) { st = ORC_ERR_STEP_CAP; break; }
+            if (cycle_closed(&cg_saved, &cg_hit, prim, steps)) break;
             if (visit_log && steps < visit_cap) visit_log[px * visit_cap + steps] = prim;
             const real cell_entry = pt_near;
             const int32_t cell = prim;
@@ -1577,6 +1596,7 @@ static int FN(trace_walk)(const orc_camera *camera, const float *spheres, const 
                 pt_near = rmax(pt_near, pt_far);
                 continue;
             }
+            cg_hit = 1;
             plane_res pr = plane_fwd_local(o, d, tn, center, pn, radius, sites + (int64_t)prim * S * 3,
                                            rgbs + (int64_t)prim * S * 3, heights + (int64_t)prim * S, S);
             tf = pr.dp >= K(0.0) ? rmin(pr.t_surf, tf) : tf;
@@ -1906,6 +1926,7 @@ int FN(orc_num_threads)(void) {
 
 typedef struct {
     int hit;         /* contributes */
+    int pre_hit;     /* sphere hit, tn <= tf, sigma >= 1e-3 (before the texture plane) */
     real tn, tf, dt; /* final segment */
     int tn_id, tf_id, pre_tn_id, pre_tf_id; /* -2 none, -1 sphere, k face, n_adj plane */
     real pre_tn;     /* t_near before the plane (query depth of the texture) */
@@ -1952,7 +1973,9 @@ static void trace_step(v3 o, v3 d, const float *spheres, const float *nsigmas, c
     sg->pn = pn;
     sg->radius = radius;
     sg->hit = 0;
+    sg->pre_hit = 0;
     if (!hit || tn > tf || sigma < K(1e-3)) return;
+    sg->pre_hit = 1;
     sg->pre_tn = tn;
     sg->pre_tn_id = tn_id;
     sg->pre_tf_id = tf_id;
@@ -2116,14 +2139,18 @@ int FN(orc_trace_backward)(const orc_camera *camera, const float *spheres, const
         real log_t = 0;
         int32_t prim = start_cells ? start_cells[px] : start_idx;
         int steps = 0, seg = 0;
+        int32_t cg_saved = -1;
+        int cg_hit = 0;
         for (;;) {
             real trans = r_exp(log_t);
             if (trans < (real)thr || prim == NO_CELL || steps >= max_steps) break;
+            if (cycle_closed(&cg_saved, &cg_hit, prim, steps)) break;
             steps++;
             trace_seg sg;
             trace_step(o, d, spheres, nsigmas, sites, rgbs, heights, S, adj, adj_off, adj_diff, prim, &sg);
             int32_t cur = prim;
             prim = sg.next;
+            if (sg.pre_hit) cg_hit = 1;
             if (!sg.hit) continue;
             real sigma = sg.sigma, dt = sg.dt;
             real dlt = -sigma * dt;

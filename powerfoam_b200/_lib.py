@@ -126,6 +126,10 @@ class PfBatchView(ctypes.Structure):
     ]
 
 
+class PfBatchSchedule(ctypes.Structure):
+    _fields_ = [("chunk", c_i32), ("order", c_i32), ("split", c_i32), ("ms", c_f)]
+
+
 PF_BATCH_MAX_VIEWS = 64
 PF_BATCH_ORDER_LONGEST = 0
 PF_BATCH_ORDER_VIEW = 1
@@ -167,6 +171,9 @@ _SIGS = {
     "pf_batch_workspace_size": [ctypes.POINTER(PfBatchView), c_i32, c_i32, ctypes.POINTER(ctypes.c_size_t)],
     "pf_batch_render": [ctypes.POINTER(PfBatchScene), ctypes.POINTER(PfBatchView), c_i32, c_i32, c_i32, c_i32, c_i32,
                         c_vp, ctypes.c_size_t, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp],
+    "pf_batch_autotune": [ctypes.POINTER(PfBatchScene), ctypes.POINTER(PfBatchView), c_i32, c_i32,
+                          ctypes.POINTER(PfBatchSchedule), c_i32, c_i32, c_i32, c_vp, ctypes.c_size_t, c_vp, c_vp,
+                          c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, ctypes.POINTER(c_i32), c_vp],
     "pf_trace_labels": [ctypes.POINTER(PfTraceInputs), c_f, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp],
     "pf_locator_workspace_size": [c_i64, ctypes.POINTER(ctypes.c_size_t)],
     "pf_locator_build": [c_vp, c_vp, c_i64, c_vp, ctypes.c_size_t, c_vp],

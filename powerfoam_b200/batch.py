@@ -272,6 +272,28 @@ class BatchStep:
         self.graph = g
         return g
 
+    def tune_schedules(self, schedules, iters=3, warmup=1):
+        """Time the render launch (pf_batch_autotune) for every (chunk, order,
+        split) in `schedules` on this step's bins; returns (mean ms per
+        schedule, index of the fastest).  One eager step first brings the
+        bins and colours up to date; the host waits for the timings."""
+        if not self.bound:
+            raise RuntimeError("bind() the inputs first")
+        self._launch()
+        cands = (_lib.PfBatchSchedule * len(schedules))()
+        for c, (ch, order, split) in zip(cands, schedules):
+            if order not in ORDERS:
+                raise ValueError(f"order must be one of {sorted(ORDERS)}")
+            c.chunk, c.order, c.split, c.ms = int(ch), ORDERS[order], int(bool(split)), 0.0
+        best = _lib.c_i32(-1)
+        g = self.grads
+        _lib.call("pf_batch_autotune", _lib.ctypes.byref(self._scene), self._views, len(self.cameras),
+                  self.tile_width, cands, len(schedules), int(warmup), int(iters), _lib.ptr(self.batch_ws),
+                  self.batch_ws.numel(), _lib.ptr(self.tile_loss), _lib.ptr(g["points"]), _lib.ptr(g["radii"]),
+                  _lib.ptr(g["normals"]), _lib.ptr(g["density"]), _lib.ptr(g["texel_sites"]),
+                  _lib.ptr(g["texel_height"]), _lib.ptr(self.status), _lib.ctypes.byref(best), _lib.stream_ptr())
+        return [float(c.ms) for c in cands], int(best.value)
+
     def set_schedule(self, chunk=None, order=None, split=None):
         """Change the work-queue chunk / order / fused-or-split schedule (drops
         a captured graph)."""
@@ -348,13 +370,18 @@ def autotune(device, cameras, bind_kwargs, tile_widths=TILE_WIDTHS, chunks=CHUNK
              splits=(False, True), iters=3, warmup=1, cache_path=None, use_cache=True, transmittance_threshold=1e-3,
              log=None, prune=1.3):
     """Sweep tile width x work-queue chunk x item order x fused / split
-    schedule over the real step and return (best BatchStep bound and ready,
-    table).  Each candidate is timed with CUDA events over `iters` eager runs
-    after `warmup`.  Tile widths are swept in the given order; once a width's
-    best time exceeds `prune` x the best so far, the remaining widths are
-    skipped (step time grows monotonically with the width on these
-    workloads).  The winner is cached in a JSON file keyed by tune_key(); a
-    cached entry skips the sweep."""
+    schedule and return (best BatchStep bound and ready, table).  Per tile
+    width the views are binned at that width and pf_batch_autotune times the
+    render launch for every schedule (CUDA events, `iters` runs after
+    `warmup`); the width's best schedule is then timed over the whole step
+    (colour pre-step, binning, render, adjoint pre-step: the binning's cost
+    depends on the width), and the width with the fastest step wins.  Table
+    rows: one per (width, schedule) with its render_ms, step_ms on each
+    width's best row (None elsewhere).  Tile widths are swept in the given
+    order; once a width's step time exceeds `prune` x the best so far, the
+    remaining widths are skipped (step time grows monotonically with the width
+    on these workloads).  The winner is cached in a JSON file keyed by
+    tune_key(); a cached entry skips the sweep."""
     cache_path = cache_path or default_cache_path()
     n = bind_kwargs["points"].shape[0]
     S = bind_kwargs["texel_sites"].shape[1]
@@ -376,30 +403,34 @@ def autotune(device, cameras, bind_kwargs, tile_widths=TILE_WIDTHS, chunks=CHUNK
     if use_cache and key in cache:
         best = cache[key]
         return make(best), best.get("table", [])
+    scheds = [(ch, order, bool(split)) for split in splits for order in orders for ch in chunks]
     table = []
     best = None
     for tw in tile_widths:
+        t0 = time.perf_counter()
         step = BatchStep(device, cameras, tw, 1, "longest", transmittance_threshold)
         step.bind(**bind_kwargs)
-        for split in splits:
-            for order in orders:
-                for ch in chunks:
-                    step.set_schedule(chunk=ch, order=order, split=split)
-                    t0 = time.perf_counter()
-                    ms = time_step(step, iters=iters, warmup=warmup)
-                    row = {"tile_width": tw, "chunk": ch, "order": order, "split": bool(split), "ms": ms}
-                    table.append(row)
-                    if log:
-                        log(f"autotune tile={tw} chunk={ch} order={order} split={bool(split)}: {ms:.3f} ms "
-                            f"({time.perf_counter() - t0:.1f} s)")
-                    if best is None or ms < best["ms"]:
-                        best = dict(row)
+        times, bi = step.tune_schedules(scheds, iters=iters, warmup=warmup)
+        rows = [{"tile_width": tw, "chunk": ch, "order": order, "split": split, "render_ms": ms, "step_ms": None}
+                for (ch, order, split), ms in zip(scheds, times)]
+        ch, order, split = scheds[bi]
+        step.set_schedule(chunk=ch, order=order, split=split)
+        rows[bi]["step_ms"] = time_step(step, iters=iters, warmup=warmup)
+        table += rows
+        if log:
+            for r in rows:
+                log(f"autotune tile={tw} chunk={r['chunk']} order={r['order']} split={r['split']}: render "
+                    f"{r['render_ms']:.3f} ms" + (f", step {r['step_ms']:.3f} ms" if r["step_ms"] else ""))
+            log(f"autotune tile={tw}: {time.perf_counter() - t0:.1f} s")
+        width_best = rows[bi]
+        if best is None or width_best["step_ms"] < best["step_ms"]:
+            best = dict(width_best)
         del step
         torch.cuda.empty_cache()
-        width_best = min(r["ms"] for r in table if r["tile_width"] == tw)
-        if prune and width_best > prune * best["ms"]:
+        if prune and width_best["step_ms"] > prune * best["step_ms"]:
             if log:
-                log(f"autotune: tile {tw} is {width_best / best['ms']:.2f}x the best; larger widths skipped")
+                log(f"autotune: tile {tw} is {width_best['step_ms'] / best['step_ms']:.2f}x the best; larger widths "
+                    "skipped")
             break
     best["table"] = table
     cache[key] = best

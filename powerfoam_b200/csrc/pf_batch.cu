@@ -431,3 +431,54 @@ extern "C" int pf_batch_render(const pf_batch_scene* scene, const pf_batch_view*
     }
     return pf_check_launch("pf_batch_render");
 }
+
+// Schedule tuner: every candidate (chunk, order, split) is run `warmup` times
+// untimed and `iters` times between two CUDA events on `stream`; the host
+// waits for each candidate's end event, so the call is not capturable.
+extern "C" int pf_batch_autotune(const pf_batch_scene* scene, const pf_batch_view* views, int32_t n_views,
+                                 int32_t tile_width, pf_batch_schedule* cands, int32_t n_cands, int32_t warmup,
+                                 int32_t iters, void* workspace, size_t workspace_bytes, float* tile_loss,
+                                 float* grad_points, float* grad_radii, float* grad_normals, float* grad_density,
+                                 float* grad_texel_sites, float* grad_texel_height, int32_t* status, int32_t* best,
+                                 void* stream) {
+    if (!cands || n_cands < 1 || !best || warmup < 0 || iters < 1)
+        return pf_fail(PF_ERR_ARGS, "pf_batch_autotune: need candidates, a best index, warmup >= 0, iters >= 1");
+    cudaEvent_t ev[2];
+    if (cudaEventCreate(&ev[0]) != cudaSuccess) return pf_fail(PF_ERR_CUDA, "pf_batch_autotune: event");
+    if (cudaEventCreate(&ev[1]) != cudaSuccess) {
+        cudaEventDestroy(ev[0]);
+        return pf_fail(PF_ERR_CUDA, "pf_batch_autotune: event");
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    int rc = PF_OK;
+    *best = -1;
+    float best_ms = 0.f;
+    for (int32_t c = 0; c < n_cands && rc == PF_OK; c++) {
+        pf_batch_schedule& s = cands[c];
+        auto run = [&]() {
+            return pf_batch_render(scene, views, n_views, tile_width, s.chunk, s.order, s.split, workspace,
+                                   workspace_bytes, tile_loss, grad_points, grad_radii, grad_normals, grad_density,
+                                   grad_texel_sites, grad_texel_height, status, stream);
+        };
+        for (int32_t i = 0; i < warmup && rc == PF_OK; i++) rc = run();
+        if (rc != PF_OK) break;
+        cudaEventRecord(ev[0], st);
+        for (int32_t i = 0; i < iters && rc == PF_OK; i++) rc = run();
+        if (rc != PF_OK) break;
+        cudaEventRecord(ev[1], st);
+        if (cudaEventSynchronize(ev[1]) != cudaSuccess) {
+            rc = pf_fail(PF_ERR_CUDA, "pf_batch_autotune: a timed run failed");
+            break;
+        }
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, ev[0], ev[1]);
+        s.ms = ms / (float)iters;
+        if (*best < 0 || s.ms < best_ms) {
+            *best = c;
+            best_ms = s.ms;
+        }
+    }
+    cudaEventDestroy(ev[0]);
+    cudaEventDestroy(ev[1]);
+    return rc;
+}

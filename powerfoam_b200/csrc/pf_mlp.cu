@@ -437,7 +437,7 @@ __global__ void __launch_bounds__(128, 1) mlp_forward_kernel(FwdArgs A) {
 }
 
 struct TrainArgs {
-    const float* rays;  // (n_rays, 8): origin, unit direction, label t (< 0: no hit), unused
+    const float* rays;  // (n_rays, 8): origin, unit direction, label t (< 0: no label), no-hit flag
     int64_t n_rays;
     int batch;
     const int* step;  // device step counter (sampling seed)
@@ -476,12 +476,13 @@ __global__ void __launch_bounds__(128, 1) mlp_train_kernel(TrainArgs A) {
         const int bi = t * kRays + r;
         const bool valid = bi < A.batch;
         float u[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 1.f};
-        float t_lab = -1.0f;
+        float t_lab = -1.0f, nohit = 0.0f;
         if (valid) {
             const uint32_t h = mix32(mix32((uint32_t)bi * 2654435761u + A.seed) ^ (uint32_t)step * 0x9e3779b9u);
             const int64_t i = (int64_t)(h % (uint32_t)A.n_rays);
             for (int k = 0; k < 6; k++) u[k] = __ldg(&A.rays[8 * i + k]);
             t_lab = __ldg(&A.rays[8 * i + 6]);
+            nohit = __ldg(&A.rays[8 * i + 7]);
             u[0] *= (1.0f / 3.0f);
             u[1] *= (1.0f / 3.0f);
             u[2] *= (1.0f / 3.0f);
@@ -495,14 +496,16 @@ __global__ void __launch_bounds__(128, 1) mlp_train_kernel(TrainArgs A) {
         // loss gradient of this ray
         float g0 = 0.f, g1 = 0.f;
         if (valid) {
-            const bool hit = t_lab >= 0.0f;
+            // a flagged ray never reaches a significant cell: its label (where it leaves the
+            // primitives' box) is the furthest useful seed, and any seed is safe
+            const bool hit = t_lab >= 0.0f, flagged = nohit != 0.0f;
             if (hit) {
                 const float e = out[0] - t_lab / kTScale;
-                const float w = e > 0.0f ? A.w_over : 1.0f;
+                const float w = (e > 0.0f && !flagged) ? A.w_over : 1.0f;
                 lt += w * e * e;
                 g0 = 2.0f * w * e * inv_b;
             }
-            const float safe = (hit && out[0] * kTScale - A.margin <= t_lab) ? 1.0f : 0.0f;
+            const float safe = (hit && (flagged || out[0] * kTScale - A.margin <= t_lab)) ? 1.0f : 0.0f;
             const float p = sigmoid(out[1]);
             lc += -(safe * logf(fmaxf(p, 1e-12f)) + (1.0f - safe) * logf(fmaxf(1.0f - p, 1e-12f)));
             g1 = (p - safe) * inv_b;

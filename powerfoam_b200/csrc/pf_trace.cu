@@ -197,6 +197,33 @@ struct LabelOut {
     int32_t* step;
 };
 
+// A walk's next cell is a function of its current cell alone (the exit face
+// with the smallest t among those the ray leaves through, raytrace.py:183-199),
+// so a ray that comes back to a cell repeats the same cells forever.  If none
+// of them was a hit (sphere hit, non-empty interval, density >= 1e-3) its
+// transmittance never changes and the reference's loop (raytrace.py:162-241)
+// never ends: the float16 face planes of neighbouring cells need not agree, so
+// a ray running almost along a face can bounce between two cells.  The guard
+// keeps the cell of step 0, 1, 2, 4, 8, ... (Brent's power-of-two saves) and
+// ends the walk when it returns to that cell with no hit since, as if the ray
+// had left the foam.  A ray the reference finishes never returns to a cell
+// without a hit in between, so its result is unchanged.  Every walk (forward,
+// labels, recording, the adjoint's walk and resume) applies the same guard at
+// the same place: after the end tests, before the step.
+struct CycleGuard {
+    int32_t saved = -1;
+    bool hit = false;
+};
+
+PF_D bool cycle_closed(CycleGuard& g, int32_t prim, int steps) {
+    if (prim == g.saved && !g.hit) return true;
+    if ((steps & (steps - 1)) == 0) {
+        g.saved = prim;
+        g.hit = false;
+    }
+    return false;
+}
+
 // REC: also write the adjoint's segment records (W): up to W.kb per ray, the
 // walk state of a ray with more left on W's overflow list for the adjoint's
 // resume launch -- the records pf_trace_backward's own walk would write, so
@@ -229,6 +256,7 @@ trace_fwd_kernel(TraceParams P, int64_t nthreads, float* __restrict__ color, flo
     float lab_t = -1.0f;
     int32_t lab_cell = -1, lab_step = -1;
     int nrec = 0;  // REC: segments recorded
+    CycleGuard cg;
     for (;;) {
         float trans = expf(log_t);
         if (trans < P.thr || prim == kNoCell) break;
@@ -246,9 +274,11 @@ trace_fwd_kernel(TraceParams P, int64_t nthreads, float* __restrict__ color, flo
             W.state[3 * (int64_t)k] = make_float4(__int_as_float(prim), __int_as_float(steps), log_t,
                                                    __int_as_float(seg));
             W.state[3 * (int64_t)k + 1] = make_float4(rgb.x, rgb.y, rgb.z, nacc.x);
-            W.state[3 * (int64_t)k + 2] = make_float4(nacc.y, nacc.z, 0.f, 0.f);
+            W.state[3 * (int64_t)k + 2] = make_float4(nacc.y, nacc.z, __int_as_float(cg.saved),
+                                                       __int_as_float((int)cg.hit));
             nrec = W.kb + 1;  // saved once; the walk goes on unrecorded
         }
+        if (cycle_closed(cg, prim, steps)) break;
         if (visit_log && steps < visit_cap) visit_log[px * visit_cap + steps] = prim;
         const float cell_entry = pt_near;
         const int32_t cell = prim;
@@ -293,6 +323,7 @@ trace_fwd_kernel(TraceParams P, int64_t nthreads, float* __restrict__ color, flo
             pt_near = fmax_t(pt_near, pt_far);
             continue;
         }
+        cg.hit = true;
         int64_t b3 = (int64_t)prim * P.S * 3;
         PlaneRes pr;
         if constexpr (std::is_same<A, float>::value) {
@@ -822,6 +853,7 @@ trace_bwd_walk_kernel(TraceParams P, SegWs W) {
     float log_t = 0.f;
     int32_t prim = P.start_cells ? P.start_cells[px] : P.start_idx;
     int steps = 0, seg = 0, nrec = 0;
+    CycleGuard cg;
     for (;;) {
         const float trans = expf(log_t);
         if (trans < P.thr || prim == kNoCell || steps >= P.max_steps || prim < 0 || prim >= P.N) break;
@@ -831,14 +863,17 @@ trace_bwd_walk_kernel(TraceParams P, SegWs W) {
             W.state[3 * (int64_t)k] = make_float4(__int_as_float(prim), __int_as_float(steps), log_t,
                                                    __int_as_float(seg));
             W.state[3 * (int64_t)k + 1] = make_float4(Cacc.x, Cacc.y, Cacc.z, Nacc.x);
-            W.state[3 * (int64_t)k + 2] = make_float4(Nacc.y, Nacc.z, 0.f, 0.f);
+            W.state[3 * (int64_t)k + 2] = make_float4(Nacc.y, Nacc.z, __int_as_float(cg.saved),
+                                                       __int_as_float((int)cg.hit));
             break;
         }
+        if (cycle_closed(cg, prim, steps)) break;
         steps++;
         const WalkStep ws = walk_step(P, o, d, prim);
         const int32_t cur = prim;
         prim = ws.next;
         if (!ws.hit) continue;
+        cg.hit = true;
         const PlaneRes pr = cell_plane(P, o, d, cur, ws.tn);
         const float tf = pr.dp >= 0.0f ? fmin_t(pr.t_surf, ws.tf) : ws.tf;
         const float tn = pr.dp < 0.0f ? fmax_t(pr.t_surf, ws.tn) : ws.tn;
@@ -963,6 +998,7 @@ trace_bwd_resume_kernel(TraceParams P, SegWs W, TraceAdjIn A, TraceGrads G) {
     float log_t = 0.f;
     int32_t prim = kNoCell;
     int steps = 0, seg = 0;
+    CycleGuard cg;
     if (alive) {
         trace_pixel(P.cam, W.over[pos], pi, pj);
         const float4 a = W.state[3 * pos], b = W.state[3 * pos + 1], c = W.state[3 * pos + 2];
@@ -972,6 +1008,8 @@ trace_bwd_resume_kernel(TraceParams P, SegWs W, TraceAdjIn A, TraceGrads G) {
         seg = __float_as_int(a.w);
         Cacc = mk(b.x, b.y, b.z);
         Nacc = mk(b.w, c.x, c.y);
+        cg.saved = __float_as_int(c.z);
+        cg.hit = __float_as_int(c.w) != 0;
     }
     const int64_t px = (int64_t)pi * P.cam.W + pj;
     const v3 o = P.cam.eye;
@@ -984,13 +1022,15 @@ trace_bwd_resume_kernel(TraceParams P, SegWs W, TraceAdjIn A, TraceGrads G) {
         // walk until kTrQueue hits are queued or the ray ends
         int cnt = 0;
         while (alive && cnt < kTrQueue) {
-            if (expf(log_t) < P.thr || prim == kNoCell || steps >= P.max_steps || prim < 0 || prim >= P.N) {
+            if (expf(log_t) < P.thr || prim == kNoCell || steps >= P.max_steps || prim < 0 || prim >= P.N ||
+                cycle_closed(cg, prim, steps)) {
                 alive = false;
                 break;
             }
             steps++;
             const WalkStep ws = walk_step(P, o, d, prim);
             if (ws.hit) {
+                cg.hit = true;
                 float* q = Q + (lane * kTrQueue + cnt) * kTrItem;
                 q[kQCell] = __int_as_float(prim);
                 q[kQTn] = ws.tn;

@@ -252,3 +252,29 @@ def assert_quantiles_close(a, b, tol=1e-5, max_flips=2):
     b = np.asarray(b, np.float64)
     bad = (np.abs(a - b) > tol).any(-1)
     assert int(bad.sum()) <= max_flips, f"{int(bad.sum())} pixels' quantile depths differ"
+
+
+def cycle_scene(cycle_density=0.0, S=8):
+    """Three cells on the x axis whose float16 face records disagree: cell 0
+    (a sphere the rays cross, density 5) exits into cell 1 at x = 1.5, cell 1
+    into cell 2 at x = 2, and cell 2's face back to cell 1 (at x = 2.5) faces
+    +x as well, so a ray along +x walks 0, 1, 2, 1, 2, ... forever -- the
+    reference's walk never returns.  With cycle_density > 0 the spheres of
+    cells 1 and 2 lie on the rays, so every lap absorbs and the walk ends on
+    the transmittance.  Returns (scene dict, adjacency, offsets, float16
+    face records (n_adj, 4)) and a camera at the origin looking along +x."""
+    rng = np.random.default_rng(7)
+    centers = np.array([[1.0, 0.0, 0.0], [1.75, 0.0, 0.0], [2.25, 0.0, 0.0]], F32)
+    radii = np.array([0.2, 0.2, 0.2], F32)
+    if cycle_density <= 0:  # off the rays: cells 1 and 2 are crossed without a hit
+        centers[1:, 1] = 3.0
+    density = np.array([5.0, cycle_density, cycle_density], F32)
+    normals = np.tile(np.array([[1.0, 0.0, 0.0]], F32), (3, 1))
+    sites = (centers[:, None, :] + rng.uniform(-0.1, 0.1, (3, S, 3))).astype(F32)
+    sc = dict(points=centers, radii=radii, density=density, normals=normals, texel_sites=sites,
+              texel_rgb=rng.uniform(0.1, 0.9, (3, S, 3)).astype(F32), texel_height=np.zeros((3, S), F32))
+    adj = np.array([1, 2, 1], np.int32)
+    off = np.array([0, 1, 2, 3], np.int32)
+    faces = np.array([[1.0, 0.0, 0.0, 1.5], [1.0, 0.0, 0.0, 2.0], [1.0, 0.0, 0.0, 2.5]], np.float16)
+    cam = np_camera((0.0, 0.0, 0.0), (1.0, 0.0, 0.0), 8, 6, 4.0)
+    return sc, adj, off, faces, cam

@@ -193,8 +193,12 @@ def test_autotune_sweeps_and_caches(tmp_path):
     path = str(tmp_path / "tune.json")
     step, table = autotune("cuda", tcams, kw, tile_widths=(8, 16), chunks=(1, 2), orders=("longest",), iters=1,
                            warmup=1, cache_path=path, prune=0)
-    assert len(table) == 8
-    best = min(table, key=lambda r: r["ms"])
+    assert len(table) == 8 and all(r["render_ms"] > 0 for r in table)
+    for tw in (8, 16):  # each width's step was timed with its fastest render schedule
+        rows = [r for r in table if r["tile_width"] == tw]
+        timed = [r for r in rows if r["step_ms"] is not None]
+        assert len(timed) == 1 and timed[0]["render_ms"] == min(r["render_ms"] for r in rows)
+    best = min((r for r in table if r["step_ms"] is not None), key=lambda r: r["step_ms"])
     assert (step.tile_width, step.chunk, step.order, step.split) == (best["tile_width"], best["chunk"],
                                                                      best["order"], best["split"])
     cache = json.load(open(path))
@@ -206,3 +210,22 @@ def test_autotune_sweeps_and_caches(tmp_path):
     assert (step2.tile_width, step2.chunk) == (step.tile_width, step.chunk)
     step2.run()
     step2.check()
+
+
+def test_schedule_tuner_through_the_c_abi():
+    """pf_batch_autotune times every schedule, picks the fastest, and leaves
+    the outputs of a valid render (equal to a plain run's image)."""
+    sc, adj, adj_off, cams, rgbs, targets = make_case(seed=14, n=300)
+    tcams = [torch_cam(c) for c in cams]
+    step = BatchStep("cuda", tcams, 8, 1, "longest")
+    step.bind(**bind_kwargs(sc, adj, adj_off, rgbs, targets))
+    step.run()
+    ref = [c.clone() for c in step.color]
+    scheds = [(1, "longest", False), (4, "view", False), (2, "longest", True)]
+    times, best = step.tune_schedules(scheds, iters=2, warmup=1)
+    assert len(times) == 3 and all(t > 0 for t in times) and times[best] == min(times)
+    torch.cuda.synchronize()
+    for a, b in zip(ref, step.color):
+        assert torch.equal(a, b)
+    with pytest.raises(ValueError):
+        step.tune_schedules([(1, "random", False)])

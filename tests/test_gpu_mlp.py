@@ -65,7 +65,8 @@ def random_rays(n, seed, with_labels=False):
         return r
     t = rng.uniform(1.0, 4.0, n)
     t[rng.uniform(size=n) < 0.3] = -1.0
-    return np.concatenate([r, t[:, None], np.zeros((n, 1))], 1).astype(np.float32)
+    flag = (t >= 0) & (rng.uniform(size=n) < 0.25)  # no-hit rays labelled where they leave the box
+    return np.concatenate([r, t[:, None], flag[:, None]], 1).astype(np.float32)
 
 
 def test_forward_matches_oracle():

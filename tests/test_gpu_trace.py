@@ -242,3 +242,56 @@ def test_trace_backward_workspace_checks():
     _lib.call("pf_trace_backward", _lib.ctypes.byref(inp), _lib.ptr(color), None, None, None, _lib.ptr(g), None,
               None, None, *[_lib.ptr(t) for t in out], 8, base, nbytes.value, _lib.stream_ptr())
     torch.cuda.synchronize()
+
+
+@pytest.mark.parametrize("cycle_density", [0.0, 3.0])
+def test_cycle_guard_matches_oracle(cycle_density):
+    """Face records that send the rays round two cells: without hits in the
+    cycle every walk ends where it comes back to a saved cell (the reference
+    would loop for ever); with hits it walks on until the transmittance
+    ends it.  Visited cells bit-exact against the oracle."""
+    from tests.helpers import cycle_scene
+
+    sc, adj, off, faces, cam = cycle_scene(cycle_density)
+    tp = {k: to_t(v) for k, v in sc.items()}
+    R = RayTracer(Args(), "cuda")
+    r = R.trace(torch_cam(cam), 0, tp["points"], tp["radii"], tp["density"], tp["normals"], tp["texel_sites"],
+                tp["texel_rgb"], tp["texel_height"], to_t(adj), to_t(off), to_t(faces), 1e-3, visit_cap=64)
+    sph, nsig, _ = packed(sc)
+    o = orc.trace_forward(orc_cam(cam), sph, nsig, sc["texel_sites"], sc["texel_rgb"], sc["texel_height"], adj, off,
+                          faces.view(np.uint16), 0, thr=1e-3, visit_cap=64)
+    assert (o["status"] == 0).all()
+    assert np.array_equal(r.visit_count.cpu().numpy(), o["visit_count"])
+    assert np.array_equal(r.visits.cpu().numpy(), o["visits"])
+    assert max_abs(r.color.cpu(), o["color"]) <= 1e-5
+
+
+@pytest.mark.parametrize("kb,rec", [(None, True), (1, True), (1, False), (0, True)])
+@pytest.mark.parametrize("cycle_density", [0.0, 3.0])
+def test_cycle_guard_adjoint_matches_oracle(cycle_density, kb, rec):
+    """The adjoint's walks apply the same guard, including the resume launch
+    that takes over a ray's saved walk state (kb = 0, 1)."""
+    from tests.helpers import assert_close_rel, cycle_scene
+
+    sc, adj, off, faces, cam = cycle_scene(cycle_density)
+    tp = {k: to_t(v).requires_grad_(True) for k, v in sc.items()}
+    R = RayTracer(Args(), "cuda")
+    R.segments_per_ray = kb
+    R.record_segments = rec
+    color, log_t, depth, normal = R.forward(torch_cam(cam), 0, tp["points"], tp["radii"], tp["density"],
+                                            tp["normals"], tp["texel_sites"], tp["texel_rgb"], tp["texel_height"],
+                                            to_t(adj), to_t(off), to_t(faces), 1e-3)
+    H, W = cam["height"], cam["width"]
+    rng = np.random.default_rng(3)
+    wC, wL = rng.standard_normal((H, W, 3)).astype(np.float32), rng.standard_normal((H, W)).astype(np.float32)
+    ((color * to_t(wC)).sum() + (log_t * to_t(wL)).sum()).backward()
+    sph, nsig, _ = packed(sc)
+    f = orc.trace_forward(orc_cam(cam), sph, nsig, sc["texel_sites"], sc["texel_rgb"], sc["texel_height"], adj, off,
+                          faces.view(np.uint16), 0, thr=1e-3)
+    assert max_abs(color.detach().cpu(), f["color"]) <= 1e-5
+    g = orc.trace_backward(orc_cam(cam), sph, nsig, sc["texel_sites"], sc["texel_rgb"], sc["texel_height"], adj, off,
+                           faces.view(np.uint16), f, wC, wL, None, None, 0, thr=1e-3)
+    assert_close_rel(tp["density"].grad.cpu().numpy(), g["nsigmas"][:, 3], 1e-4, "density")
+    assert_close_rel(tp["texel_rgb"].grad.cpu().numpy(), g["texel_rgb"], 1e-4, "rgb")
+    assert_close_rel(tp["points"].grad.cpu().numpy(), g["spheres"][:, :3], 1e-4, "points")
+    assert float(tp["density"].grad[0].abs()) > 0

@@ -17,7 +17,8 @@ def rays(n, seed):
     d /= np.linalg.norm(d, axis=1, keepdims=True)
     t = rng.uniform(1.0, 4.0, n)
     t[rng.uniform(size=n) < 0.3] = -1.0
-    return np.concatenate([o, d, t[:, None], np.zeros((n, 1))], 1).astype(np.float32)
+    flag = (t >= 0) & (rng.uniform(size=n) < 0.25)  # no-hit rays labelled where they leave the box
+    return np.concatenate([o, d, t[:, None], flag[:, None]], 1).astype(np.float32)
 
 
 def test_backward_matches_finite_differences():
