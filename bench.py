@@ -551,7 +551,7 @@ def proposal_main(args, dev):
     torch.cuda.synchronize()
     train_s = time.perf_counter() - t0
     t0 = time.perf_counter()
-    seeded = SeededTracer(tr, net, sc["points"], sc["radii"], conf_threshold=net.calibrate(val, max_unsafe_frac=1e-4),
+    seeded = SeededTracer(tr, net, sc["points"], sc["radii"], conf_threshold=net.calibrate(val),
                           adjacency=adj, adjacency_offsets=off)
     torch.cuda.synchronize()
     vmap_s = time.perf_counter() - t0
@@ -592,6 +592,9 @@ def proposal_main(args, dev):
     conf_lab = one.contiguous()
     ideal_r, ideal_ms = timed(lambda: tr.trace(ev, seeded.locator.seed(ev, t_lab, conf_lab, 0.5, st), *scene_args,
                                                 check_status=False))
+    # the two parts of the label-seeded frame: locating the seeds, and the walk from them
+    ideal_start, locate_ms = timed(lambda: seeded.locator.seed(ev, t_lab, conf_lab, 0.5, st))
+    _, ideal_walk_ms = timed(lambda: tr.trace(ev, ideal_start, *scene_args, check_status=False))
     H, W = cfg["height"], cfg["width"]
     line = dict(metric=METRIC, value=plain_ms / seed_ms, unit="x (plain / proposal-seeded frame time)", n_gpus=1,
                 steps=args.steps, warmup=max(args.warmup, 3), ms_per_step=seed_ms, higher_is_better=True,
@@ -600,7 +603,8 @@ def proposal_main(args, dev):
                             plain_ms=plain_ms,
                             seeded_ms=seed_ms, psnr_db=psnr(seed_r.color, plain.color), seeded_rays=n_seeded,
                             rays=H * W, threshold=seeded.conf_threshold, cells_plain=int(plain.visit_count.sum()),
-                            cells_seeded=int(seed_r.visit_count.sum()), label_seed_ms=ideal_ms,
+                            cells_seeded=int(seed_r.visit_count.sum()), label_seed_ms=ideal_ms, label_seed_locate_ms=locate_ms,
+                            label_seed_walk_ms=ideal_walk_ms,
                             label_seed_psnr_db=psnr(ideal_r.color, plain.color),
                             label_seed_cells=int(ideal_r.visit_count.sum()), label_s=label_s, train_s=train_s,
                             train_rays=int(rays8.shape[0]), loss_first=hist[0], loss_last=hist[-1],
