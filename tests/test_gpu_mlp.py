@@ -271,7 +271,9 @@ def test_trained_proposal_seeds_at_50db():
     val = labelled(50000, 256)
     net = ProposalNet("cuda", seed=1)
     hist = net.train(rays8, steps=5000, batch=65536, lr=1e-3, overshoot_weight=100.0, margin=0.1, graph_steps=100)
-    assert hist[-1][0] < hist[0][0] and hist[-1][1] < hist[0][1]
+    # the entry-distance loss falls; the confidence targets move with the predictions (a seed's
+    # safety depends on the predicted t), so that loss is only required to be well below chance (ln 2)
+    assert hist[-1][0] < hist[0][0] and hist[-1][1] < 0.3
     # strict gate: no held-out seed past its first significant cell (a budget of 1e-4 of the
     # held-out rays let eval views drop below 50 dB)
     thr = net.calibrate(val)
