@@ -71,17 +71,35 @@ def parse():
     return p.parse_args()
 
 
-# DRAM bytes (read + write) per launch of the dominant kernel from one ncu
-# capture of the same command (dram__bytes_read.sum + dram__bytes_write.sum),
-# with the summary that records it; None where no capture of the current
-# kernel exists.
-TRAFFIC = {
-    ("raster1m", "pf_raster_backward"): None,
+# Per launch of the dominant kernel, from one ncu capture of the same command
+# (`ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum,smsp__inst_executed.sum ... -k
+# regex:raster_bwd_kernel -s 1 -c 1 python bench.py --steps 2 --warmup 1 --no-cpu-baseline`, one
+# pass): DRAM bytes read + written, and warp instructions for the issue roofline.  Recorded once
+# per kernel change; the bench line carries them as capture metadata next to its live timings.
+CAPTURES = {
+    ("raster1m", "pf_raster_backward"): dict(
+        traffic=816.77e6 + 206.06e6, warp_instructions=11_715_679_565,
+        source="ncu capture of raster_bwd_kernel<8, 0> (second launch of `python bench.py --steps 2 --warmup 1 "
+               "--no-cpu-baseline`): dram__bytes_read.sum + dram__bytes_write.sum, smsp__inst_executed.sum"),
 }
+SMS, SCHEDULERS_PER_SM = 148, 4
 
 
 def capture_traffic(kernel, workload):
-    return TRAFFIC.get((workload, kernel))
+    c = CAPTURES.get((workload, kernel))
+    return (c["traffic"], c["source"]) if c else None
+
+
+def issue_roofline(kernel, workload, ms, sm_mhz):
+    """Warp instructions of the captured launch / issue slots of the live
+    launch time (148 SMs x 4 schedulers x clock x time)."""
+    c = CAPTURES.get((workload, kernel))
+    if not c or not ms:
+        return None
+    mhz = sm_mhz or 1965.0
+    slots = SMS * SCHEDULERS_PER_SM * mhz * 1e6 * ms * 1e-3
+    return dict(warp_instructions=c["warp_instructions"], issue_slots=slots,
+                frac=c["warp_instructions"] / slots, sm_mhz=mhz, source=c["source"])
 
 
 def load_peaks():
@@ -1143,7 +1161,8 @@ def main():
                               frac=achieved / peak, peak_source=peak_kind,
                               traffic=(capture_traffic(dominant, args.workload) or (None, None))[0],
                               traffic_source=(capture_traffic(dominant, args.workload) or (None, None))[1],
-                              algorithmic_bytes=dom_bytes, ms=dom_ms, fwd_ms=fwd_ms, bwd_ms=bwd_ms),
+                              algorithmic_bytes=dom_bytes, ms=dom_ms, fwd_ms=fwd_ms, bwd_ms=bwd_ms,
+                              issue=issue_roofline(dominant, args.workload, dom_ms, (clk or {}).get("sm_mhz"))),
                 gpu_launches=None)
     # kernels per step: pack 1, binning with tile order, prefetch 1, SH 1, forward 1, backward 1 + 7 sanitise
     line["gpu_launches"] = args.steps * (1 + bin_launches(st["T"]) + 1 + 1 + 1 + 1 + 7)

@@ -71,6 +71,18 @@ constexpr int kSmBar = kSmH3 + 20480;
 constexpr int kSmEnd = kSmBar + 64;
 constexpr int kSmBytes = kSmEnd + 1024;  // + alignment slack
 
+// inference layout: no gradient buffers, the activations ping-pong between two
+// buffers (layer 3 overwrites layer 1's output, which layer 2 has consumed),
+// 96 KB so two blocks share an SM and one encodes while the other waits for
+// the tensor core
+constexpr int kFsX = 33792;
+constexpr int kFsHa = kFsX + 20480;
+constexpr int kFsHb = kFsHa + 20480;
+constexpr int kFsBar = kFsHb + 20480;
+constexpr int kFsEnd = kFsBar + 64;
+constexpr int kFsBytes = kFsEnd + 1024;
+constexpr uint32_t kFsTmCols = 128;  // layer outputs only
+
 // TMEM columns: activations / data gradients, then the four dW accumulators
 constexpr uint32_t kTmAcc = 0;
 __host__ __device__ constexpr uint32_t tm_grad(int l) { return 128 + 80 * l; }
@@ -246,6 +258,7 @@ struct Ctx {
     uint32_t phase;
     int* status;
     bool ok;
+    uint32_t cols;  // TMEM columns held
 };
 
 // commit, then every thread waits for the tensor core.  The outcome is made
@@ -326,47 +339,52 @@ PF_D void load_weights(uint8_t* sm, const uint8_t* __restrict__ img) {
 }
 
 // TMEM allocation by warp 0; every thread learns the base address
-PF_D void setup(Ctx& c, uint8_t* sm, int* status) {
+PF_D void setup(Ctx& c, uint8_t* sm, int* status, int bar_off = kSmBar, uint32_t cols = kTmCols) {
     c.sm = sm;
     c.sbase = smem_u32(sm);
-    c.bar = c.sbase + kSmBar;
+    c.bar = c.sbase + bar_off;
     c.phase = 0;
     c.status = status;
     c.ok = true;
-    uint32_t slot = c.sbase + kSmBar + 16;
+    c.cols = cols;
+    uint32_t slot = c.sbase + bar_off + 16;
     if (threadIdx.x == 0) mbar_init(c.bar, 1);
-    if (threadIdx.x < 32) tmem_alloc(slot, kTmCols);
+    if (threadIdx.x < 32) tmem_alloc(slot, cols);
     fence_before();
     __syncthreads();
     fence_after();
-    c.tmem = *reinterpret_cast<volatile uint32_t*>(sm + kSmBar + 16);
+    c.tmem = *reinterpret_cast<volatile uint32_t*>(sm + bar_off + 16);
 }
 
 PF_D void teardown(Ctx& c) {
     fence_before();
     __syncthreads();
     fence_after();
-    if (threadIdx.x < 32) tmem_free(c.tmem, kTmCols);
+    if (threadIdx.x < 32) tmem_free(c.tmem, c.cols);
 }
 
 // forward of one tile whose encoded rays are in the X buffer; leaves H1..H3
-// and the two outputs of this thread's ray in out[2]; masks for the adjoint
+// and the two outputs of this thread's ray in out[2]; masks for the adjoint.
+// INF: the inference layout (H3 overwrites H1).
+template <bool INF = false>
 PF_D bool forward_tile(Ctx& c, float out[2], uint32_t m1[2], uint32_t m2[2], uint32_t m3[2]) {
+    constexpr int X = INF ? kFsX : kSmX, H1 = INF ? kFsHa : kSmH1, H2 = INF ? kFsHb : kSmH2,
+                  H3 = INF ? kFsHa : kSmH3;
     const uint32_t W = c.sbase + kSmW;
     publish();
-    if (threadIdx.x == 0) issue_forward(c.tmem + kTmAcc, c.sbase + kSmX, W + img_off(0), 64);
+    if (threadIdx.x == 0) issue_forward(c.tmem + kTmAcc, c.sbase + X, W + img_off(0), 64);
     if (!commit_wait(c)) return false;
-    relu_store(c, kTmAcc, c.sm + kSmH1, m1);
+    relu_store(c, kTmAcc, c.sm + H1, m1);
     publish();
-    if (threadIdx.x == 0) issue_forward(c.tmem + kTmAcc, c.sbase + kSmH1, W + img_off(1), 64);
+    if (threadIdx.x == 0) issue_forward(c.tmem + kTmAcc, c.sbase + H1, W + img_off(1), 64);
     if (!commit_wait(c)) return false;
-    relu_store(c, kTmAcc, c.sm + kSmH2, m2);
+    relu_store(c, kTmAcc, c.sm + H2, m2);
     publish();
-    if (threadIdx.x == 0) issue_forward(c.tmem + kTmAcc, c.sbase + kSmH2, W + img_off(2), 64);
+    if (threadIdx.x == 0) issue_forward(c.tmem + kTmAcc, c.sbase + H2, W + img_off(2), 64);
     if (!commit_wait(c)) return false;
-    relu_store(c, kTmAcc, c.sm + kSmH3, m3);
+    relu_store(c, kTmAcc, c.sm + H3, m3);
     publish();
-    if (threadIdx.x == 0) issue_forward(c.tmem + kTmAcc, c.sbase + kSmH3, W + img_off(3), 16);
+    if (threadIdx.x == 0) issue_forward(c.tmem + kTmAcc, c.sbase + H3, W + img_off(3), 16);
     if (!commit_wait(c)) return false;
     float v[16];
     tmem_ld16(c.tmem + ((uint32_t)(threadIdx.x & ~31) << 16) + kTmAcc, v);
@@ -375,9 +393,9 @@ PF_D bool forward_tile(Ctx& c, float out[2], uint32_t m1[2], uint32_t m2[2], uin
     return true;
 }
 
-PF_D void put_features(uint8_t* sm, const float f[80]) {
+PF_D void put_features(uint8_t* sm, const float f[80], int x_off = kSmX) {
 #pragma unroll
-    for (int ch = 0; ch < 10; ch++) put_chunk(sm + kSmX, kRays, threadIdx.x, ch, f + 8 * ch);
+    for (int ch = 0; ch < 10; ch++) put_chunk(sm + x_off, kRays, threadIdx.x, ch, f + 8 * ch);
 }
 
 PF_D float sigmoid(float x) { return 1.0f / (1.0f + expf(-x)); }
@@ -392,12 +410,12 @@ struct FwdArgs {
     int* status;
 };
 
-__global__ void __launch_bounds__(128, 1) mlp_forward_kernel(FwdArgs A) {
+__global__ void __launch_bounds__(128, 2) mlp_forward_kernel(FwdArgs A) {
     extern __shared__ uint8_t smraw[];
     uint8_t* sm = (uint8_t*)(((uintptr_t)smraw + 1023) & ~(uintptr_t)1023);
     Ctx c;
     load_weights(sm, A.img);
-    setup(c, sm, A.status);
+    setup(c, sm, A.status, kFsBar, kFsTmCols);
     const int64_t tiles = (A.n + kRays - 1) / kRays;
     for (int64_t t = blockIdx.x; t < tiles && c.ok; t += gridDim.x) {
         const int64_t i = t * kRays + threadIdx.x;
@@ -423,10 +441,10 @@ __global__ void __launch_bounds__(128, 1) mlp_forward_kernel(FwdArgs A) {
         }
         float f[80];
         encode(u, f);
-        put_features(sm, f);
+        put_features(sm, f, kFsX);
         float out[2];
         uint32_t m1[2], m2[2], m3[2];
-        if (!forward_tile(c, out, m1, m2, m3)) break;
+        if (!forward_tile<true>(c, out, m1, m2, m3)) break;
         if (valid) {
             A.t_out[i] = out[0] * kTScale;
             A.conf_out[i] = sigmoid(out[1]);
@@ -746,11 +764,11 @@ extern "C" int pf_mlp_forward(const uint8_t* image, const float* rays, int64_t n
     A.conf_out = confidence;
     A.status = (int*)status;
     if (n_rays == 0) return PF_OK;
-    int rc = set_smem((const void*)mlp_forward_kernel, kSmBytes);
+    int rc = set_smem((const void*)mlp_forward_kernel, kFsBytes);
     if (rc) return rc;
     const int64_t tiles = (n_rays + kRays - 1) / kRays;
-    const unsigned grid = (unsigned)std::min<int64_t>(tiles, sm_count());
-    mlp_forward_kernel<<<grid, 128, kSmBytes, (cudaStream_t)stream>>>(A);
+    const unsigned grid = (unsigned)std::min<int64_t>(tiles, 2 * (int64_t)sm_count());
+    mlp_forward_kernel<<<grid, 128, kFsBytes, (cudaStream_t)stream>>>(A);
     return pf_check_launch("pf_mlp_forward");
 }
 

@@ -445,3 +445,50 @@ def test_trace1m_adjoint_whole_frame(trace1m, varied):
     assert_close_rel(_np(t["texel_height"].grad), g["texel_height"], 1e-4, "height")
     if varied:
         assert_close_rel(_np(t["texel_sites"].grad), g["texel_sites"], 1e-4, "sites")
+
+
+# ---------------------------------------------------------------------------
+# The cycle guard at scale: 1,048,576 primitives of opaque shells, 2048 x 1536
+
+
+def test_shells1m_cycling_rays_bit_exact():
+    """On the shells scene some rays come back to a cell they walked (float16
+    faces of neighbouring cells that disagree); before the cycle guard they
+    ran to the 65,536-step cap.  The 2,048 longest walks of the frame and
+    2,048 random rays: visited cells bit-exact against the oracle, every walk
+    ends without the step cap, and the sample holds walks that revisit a cell
+    (the guard's subjects)."""
+    from powerfoam_b200.adjacency import power_adjacency, power_adjacency_diff, start_cell
+
+    cfg = dict(synthetic.CONFIGS["trace6m"])
+    n = 1048576
+    r_scale = (cfg["n"] / n) ** (1 / 3)
+    sc_t = synthetic.make_scene(n, seed=cfg["seed"], mixture=cfg["mixture"], sigma=cfg["sigma"],
+                                r_range=tuple(r * r_scale for r in cfg["r_range"]), shells=(0.12, 0.02, 30.0))
+    adj, off = power_adjacency(sc_t["points"], sc_t["radii"])
+    pm = power_adjacency_diff(sc_t["points"], sc_t["radii"], adj, off)
+    cam = synthetic.orbit_camera(4242, 2048, 1536, cfg["vfov"])
+    rgb = synthetic.texel_rgb(sc_t, cam)
+    st = start_cell(sc_t["points"], sc_t["radii"], cam.eye)
+    cap = 256
+    tr = RayTracer(TArgs(), "cuda")
+    r = tr.trace(cam, st, sc_t["points"], sc_t["radii"], sc_t["density"], sc_t["normals"], sc_t["texel_sites"], rgb,
+                 sc_t["texel_height"], adj, off, pm, 1e-3, visit_cap=cap)  # raises on the step cap
+    vc_all = _np(r.visit_count).reshape(-1)
+    assert vc_all.max() <= cap
+    HW = cam.height * cam.width
+    longest = np.argsort(vc_all, kind="stable")[-2048:]
+    rng = np.random.default_rng(4242)
+    pix = np.unique(np.concatenate([longest, rng.choice(HW, 2048, replace=False)]))
+    sc = _scene_np(sc_t, rgb)
+    sph, nsig, _ = packed(sc)
+    o = orc.trace_forward_pixels(_ocam(cam), sph, nsig, sc["texel_sites"], sc["texel_rgb"], sc["texel_height"],
+                                 _np(adj), _np(off), _np(pm).view(np.uint16), pix, st, thr=1e-3, visit_cap=cap)
+    assert o["rc"] == 0 and (o["status"] == 0).all()
+    assert np.array_equal(vc_all[pix], o["visit_count"])
+    pix_t = torch.from_numpy(pix).cuda()
+    visits = _np(r.visits.reshape(HW, cap)[pix_t])
+    assert np.array_equal(visits, o["visits"])
+    assert max_abs(_np(r.color).reshape(-1, 3)[pix], o["color"]) <= 1e-5
+    revisit = sum(len(set(v[v >= 0].tolist())) < int((v >= 0).sum()) for v in visits)
+    assert revisit > 0
