@@ -62,6 +62,9 @@ def parse():
                    "(proposal-seeded vs plain cell walk)")
     p.add_argument("--cpu-slices", type=int, default=4, help="slices (1/16 of a frame each) the CPU baseline times")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--sync-free", action="store_true",
+                   help="raster workloads: Rasterizer(host_sync=False), no host read of the pair count per call "
+                   "(overflow and non-finite inputs are checked once after the timed steps)")
     p.add_argument("--no-autotune", action="store_true", help="batch workloads: use --tile, chunk 1")
     p.add_argument("--proposal-prims", type=int, default=0,
                    help="proposal workload: primitive count (default 6,291,456; radii scale with the spacing)")
@@ -527,11 +530,13 @@ def proposal_main(args, dev):
     held-out view.  Reported: plain and seeded frame times (the seeded time
     includes the network forward and the cell location), PSNR of the seeded
     frame against the plain one, and the same for seeding from the plain
-    walk's own labels (the bound a perfect proposal reaches)."""
+    walk's own labels (the bound a perfect proposal reaches), for the
+    occupancy-grid seeding (the conservative proposal without a network) and
+    for the network with the occupancy seeding as its fallback."""
     from powerfoam_b200 import synthetic
     from powerfoam_b200.adjacency import power_adjacency, power_adjacency_diff, start_cell
-    from powerfoam_b200.proposal import (ProposalNet, SeededTracer, box_exit, camera_rays, make_training_rays,
-                                         trace_labels)
+    from powerfoam_b200.proposal import (OccupancySeeder, ProposalNet, SeededTracer, box_exit, camera_rays,
+                                         make_training_rays, trace_labels)
     from powerfoam_b200.raytrace import RayTracer
 
     cfg = dict(synthetic.CONFIGS["trace6m"])
@@ -613,6 +618,15 @@ def proposal_main(args, dev):
     # the two parts of the label-seeded frame: locating the seeds, and the walk from them
     ideal_start, locate_ms = timed(lambda: seeded.locator.seed(ev, t_lab, conf_lab, 0.5, st))
     _, ideal_walk_ms = timed(lambda: tr.trace(ev, ideal_start, *scene_args, check_status=False))
+    # the conservative proposal without a network (occupancy grid), alone and as the gate's fallback
+    t0 = time.perf_counter()
+    occ = OccupancySeeder(sc["points"], sc["radii"], sc["density"], seeded.locator, res=128)
+    torch.cuda.synchronize()
+    occ_build_s = time.perf_counter() - t0
+    occ_r, occ_ms = timed(lambda: tr.trace(ev, occ.start_cells(ev, st), *scene_args, check_status=False))
+    seeded.occupancy = occ
+    comb_r, comb_ms = timed(lambda: seeded.render(ev, st, scene_args))
+    seeded.occupancy = None
     H, W = cfg["height"], cfg["width"]
     line = dict(metric=METRIC, value=plain_ms / seed_ms, unit="x (plain / proposal-seeded frame time)", n_gpus=1,
                 steps=args.steps, warmup=max(args.warmup, 3), ms_per_step=seed_ms, higher_is_better=True,
@@ -626,7 +640,11 @@ def proposal_main(args, dev):
                             label_seed_psnr_db=psnr(ideal_r.color, plain.color),
                             label_seed_cells=int(ideal_r.visit_count.sum()), label_s=label_s, train_s=train_s,
                             train_rays=int(rays8.shape[0]), loss_first=hist[0], loss_last=hist[-1],
-                            voxel_map_s=vmap_s, **stats))
+                            voxel_map_s=vmap_s, occupancy_ms=occ_ms, occupancy_psnr_db=psnr(occ_r.color, plain.color),
+                            occupancy_cells=int(occ_r.visit_count.sum()), occupancy_build_s=occ_build_s,
+                            network_occupancy_ms=comb_ms,
+                            network_occupancy_psnr_db=psnr(comb_r.color, plain.color),
+                            network_occupancy_cells=int(comb_r.visit_count.sum()), **stats))
     print(json.dumps(line), flush=True)
 
 
@@ -1060,7 +1078,8 @@ def main():
 
         cam.ray_maps = synthetic.fisheye_ray_maps(cam, 150.0)
         args.no_cpu_baseline = True
-    R = rasterize.Rasterizer(ArgsGeneric() if fisheye else Args(), dev, tile_width=args.tile)
+    R = rasterize.Rasterizer(ArgsGeneric() if fisheye else Args(), dev, tile_width=args.tile,
+                             host_sync=not args.sync_free)
     step, params = make_step(R, scene, cam, adj, adj_off, target_dev, world)
 
     def barrier():
@@ -1141,6 +1160,7 @@ def main():
     torch.cuda.synchronize()
     st = algorithmic_bytes(R.last_stats, cfg["height"], cfg["width"])
     R.collect_stats = False
+    R.check()  # with --sync-free: a pair-buffer overflow or non-finite input in any step raises here
     peak, peak_kind = load_peaks()
     dominant = "pf_raster_backward" if bwd_ms >= fwd_ms else "pf_raster_forward"
     dom_ms = max(bwd_ms, fwd_ms)
@@ -1164,8 +1184,8 @@ def main():
                               algorithmic_bytes=dom_bytes, ms=dom_ms, fwd_ms=fwd_ms, bwd_ms=bwd_ms,
                               issue=issue_roofline(dominant, args.workload, dom_ms, (clk or {}).get("sm_mhz"))),
                 gpu_launches=None)
-    # kernels per step: pack 1, binning with tile order, prefetch 1, SH 1, forward 1, backward 1 + 7 sanitise
-    line["gpu_launches"] = args.steps * (1 + bin_launches(st["T"]) + 1 + 1 + 1 + 1 + 7)
+    # kernels per step: pack 1, binning with tile order, prefetch 1, SH 1, forward 1, backward 1 + 1 sanitise
+    line["gpu_launches"] = args.steps * (1 + bin_launches(st["T"]) + 1 + 1 + 1 + 1 + 1)
     if fisheye:  # the cone hierarchy: one leaf launch and one per merged level
         dh, dw, levels = (cfg["height"] + 1) // 2, (cfg["width"] + 1) // 2, 1
         while dh > 1 or dw > 1:

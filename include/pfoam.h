@@ -432,6 +432,28 @@ PF_API int pf_locate_cells_vmap(const float *points, const float *radii, int64_t
                                 const float *box_hi, int32_t res, const float *queries, int64_t n_queries,
                                 int32_t max_walk_steps, int32_t *out, void *stream);
 
+/* Occupancy seeding (no counterpart in the reference): a conservative,
+ * unlearned proposal.  pf_occupancy_build sets one bit per voxel of a res^3
+ * grid over [box_lo, box_hi] (cubic voxels of the largest extent / res, bit
+ * v = (z res + y) res + x) wherever the bounding box of a primitive with
+ * density >= sigma_min (NaN counts), grown by one voxel, reaches; `bits` holds
+ * pf_occupancy_words(res) words and is cleared first; a non-finite centre or
+ * radius raises PF_ERR_NONFINITE in *status.  The walk composites only inside
+ * spheres of density >= 1e-3 (raytrace.py:201-206), so with sigma_min <= 1e-3
+ * a ray meets nothing before the first set voxel on its path.
+ * pf_occupancy_entry: per pixel ray of `cam`, the distance at which it enters
+ * the first set voxel (3-D DDA from where it enters the box), or the box exit
+ * when it meets none, minus `margin`; confidence 1 where that skips part of
+ * the ray, 0 where it does not (rays that miss the box or start in a set
+ * voxel; t_entry -1 for a miss).  The two outputs are pf_seed_start_cells_vmap's
+ * t_entry and confidence (threshold 0.5). */
+PF_API int pf_occupancy_words(int32_t res, int64_t *words);
+PF_API int pf_occupancy_build(const float *points, const float *radii, const float *density, int64_t n_prims,
+                              const float *box_lo, const float *box_hi, int32_t res, float sigma_min, uint32_t *bits,
+                              int32_t *status, void *stream);
+PF_API int pf_occupancy_entry(const uint32_t *bits, const float *box_lo, const float *box_hi, int32_t res,
+                              const pf_camera *cam, float margin, float *t_entry, float *confidence, void *stream);
+
 /* ---------------------------------------------------------------------- */
 /* Ray-proposal network (no counterpart in the reference): 6-frequency
  * positional encoding of (origin / 3, unit direction) -> 3 x 64 ReLU -> (entry

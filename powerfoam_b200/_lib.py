@@ -171,6 +171,11 @@ _SIGS = {
     "pf_batch_workspace_size": [ctypes.POINTER(PfBatchView), c_i32, c_i32, ctypes.POINTER(ctypes.c_size_t)],
     "pf_batch_render": [ctypes.POINTER(PfBatchScene), ctypes.POINTER(PfBatchView), c_i32, c_i32, c_i32, c_i32, c_i32,
                         c_vp, ctypes.c_size_t, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp],
+    "pf_occupancy_words": [c_i32, ctypes.POINTER(c_i64)],
+    "pf_occupancy_build": [c_vp, c_vp, c_vp, c_i64, ctypes.POINTER(c_f), ctypes.POINTER(c_f), c_i32, c_f, c_vp, c_vp,
+                           c_vp],
+    "pf_occupancy_entry": [c_vp, ctypes.POINTER(c_f), ctypes.POINTER(c_f), c_i32, ctypes.POINTER(PfCamera), c_f, c_vp,
+                           c_vp, c_vp],
     "pf_batch_autotune": [ctypes.POINTER(PfBatchScene), ctypes.POINTER(PfBatchView), c_i32, c_i32,
                           ctypes.POINTER(PfBatchSchedule), c_i32, c_i32, c_i32, c_vp, ctypes.c_size_t, c_vp, c_vp,
                           c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, ctypes.POINTER(c_i32), c_vp],

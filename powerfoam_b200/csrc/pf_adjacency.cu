@@ -999,6 +999,116 @@ extern "C" int pf_seed_start_cells(const float* points, const float* radii, int6
     return pf_check_launch("pf_seed_start_cells");
 }
 
+// ---------------------------------------------------------------------------
+// Occupancy seeding (no counterpart in the reference).  One bit per voxel of
+// a res^3 grid over the primitives' box, set wherever the bounding box of a
+// primitive whose density is not below sigma_min, grown by one voxel, reaches.
+// The walk composites only inside spheres with density >= 1e-3
+// (raytrace.py:201-206: a cell adds nothing unless its sphere is hit and
+// sigma >= 1e-3), so a ray meets no compositing before the first set voxel on
+// its path, and a walk seeded there composites what the plain walk does.
+__global__ void occupancy_kernel(const float* __restrict__ pts, const float* __restrict__ radii,
+                                 const float* __restrict__ density, int64_t N, VoxelGrid g, float sigma_min,
+                                 uint32_t* __restrict__ bits, int32_t* __restrict__ status) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    if (density[i] < sigma_min) return;  // a NaN density counts as occupied, as the walk treats it
+    const float c[3] = {pts[3 * i], pts[3 * i + 1], pts[3 * i + 2]};
+    const float r = radii[i];
+    if (!isfinite(c[0]) || !isfinite(c[1]) || !isfinite(c[2]) || !isfinite(r)) {
+        atomicMax(status, PF_ERR_NONFINITE);
+        return;
+    }
+    int a[3], b[3];
+    for (int k = 0; k < 3; k++) {
+        const float fa = floorf((c[k] - r - g.lo[k]) * g.inv_h) - 1.0f;
+        const float fb = floorf((c[k] + r - g.lo[k]) * g.inv_h) + 1.0f;
+        a[k] = (int)fminf(fmaxf(fa, 0.0f), (float)(g.res - 1));
+        b[k] = (int)fminf(fmaxf(fb, 0.0f), (float)(g.res - 1));
+    }
+    for (int z = a[2]; z <= b[2]; z++)
+        for (int y = a[1]; y <= b[1]; y++)
+            for (int x = a[0]; x <= b[0]; x++) {
+                const int64_t v = ((int64_t)z * g.res + y) * g.res + x;
+                atomicOr(&bits[v >> 5], 1u << (v & 31));
+            }
+}
+
+// Per pixel ray: the distance at which it enters the first set voxel (a 3-D
+// DDA from where it enters the grid's box), minus `margin`; rays that meet no
+// set voxel get the box exit minus `margin`.  confidence = 1 where that skips
+// part of the ray (t > 0 inside the box), else 0 (rays that miss the box, or
+// start in a set voxel).
+__global__ void occupancy_entry_kernel(const uint32_t* __restrict__ bits, VoxelGrid g, Cam cam, float margin,
+                                       float* __restrict__ t_out, float* __restrict__ conf_out) {
+    const int64_t px = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t n = (int64_t)cam.W * cam.H;
+    if (px >= n) return;
+    const int pi = (int)(px / cam.W), pj = (int)(px % cam.W);
+    const v3 dv = ray_dir(cam, pi, pj);
+    const float o[3] = {cam.eye.x, cam.eye.y, cam.eye.z}, d[3] = {dv.x, dv.y, dv.z};
+    const float span = g.h * (float)g.res;
+    float t0 = 0.0f, t1 = 3.0e38f;
+    bool inside = true;
+    for (int k = 0; k < 3; k++) {
+        const float lo = g.lo[k], hi = g.lo[k] + span;
+        if (d[k] == 0.0f) {
+            if (o[k] < lo || o[k] > hi) inside = false;
+        } else {
+            float ta = (lo - o[k]) / d[k], tb = (hi - o[k]) / d[k];
+            if (ta > tb) {
+                const float tt = ta;
+                ta = tb;
+                tb = tt;
+            }
+            t0 = fmaxf(t0, ta);
+            t1 = fminf(t1, tb);
+        }
+    }
+    if (!inside || !(t1 > t0)) {
+        t_out[px] = -1.0f;
+        conf_out[px] = 0.0f;
+        return;
+    }
+    int ix[3], step[3];
+    float tmax[3], tdelta[3];
+    for (int k = 0; k < 3; k++) {
+        const float p = o[k] + t0 * d[k];
+        const float f = floorf((p - g.lo[k]) * g.inv_h);
+        ix[k] = (int)fminf(fmaxf(f, 0.0f), (float)(g.res - 1));
+        if (d[k] > 0.0f) {
+            step[k] = 1;
+            tmax[k] = (g.lo[k] + (float)(ix[k] + 1) * g.h - o[k]) / d[k];
+            tdelta[k] = g.h / d[k];
+        } else if (d[k] < 0.0f) {
+            step[k] = -1;
+            tmax[k] = (g.lo[k] + (float)ix[k] * g.h - o[k]) / d[k];
+            tdelta[k] = -g.h / d[k];
+        } else {
+            step[k] = 0;
+            tmax[k] = 3.0e38f;
+            tdelta[k] = 3.0e38f;
+        }
+    }
+    float t = t0;
+    bool hit = false;
+    for (int it = 0; it < 3 * g.res + 3; it++) {  // a ray crosses at most 3 res voxels of the grid
+        const int64_t v = ((int64_t)ix[2] * g.res + ix[1]) * g.res + ix[0];
+        if ((__ldg(&bits[v >> 5]) >> (v & 31)) & 1u) {
+            hit = true;
+            break;
+        }
+        const int k = (tmax[0] < tmax[1]) ? (tmax[0] < tmax[2] ? 0 : 2) : (tmax[1] < tmax[2] ? 1 : 2);
+        t = tmax[k];
+        ix[k] += step[k];
+        if (ix[k] < 0 || ix[k] >= g.res || t >= t1) break;
+        tmax[k] += tdelta[k];
+    }
+    const float ts = (hit ? t : t1) - margin;
+    t_out[px] = ts;
+    conf_out[px] = ts > t0 ? 1.0f : 0.0f;
+}
+
 static bool voxel_grid(const float* lo, const float* hi, int32_t res, VoxelGrid* g) {
     if (!lo || !hi || res < 1 || res > 1024) return false;
     float ext = 0.f;
@@ -1202,4 +1312,39 @@ extern "C" int pf_steiner_select(const float* samples, const float* radii, int64
     steiner_select_kernel<<<1, kSelectThreads, 0, st>>>(samples, radii, n, seed, threshold, scratch, selected,
                                                          n_selected);
     return pf_check_launch("pf_steiner_select");
+}
+
+extern "C" int pf_occupancy_words(int32_t res, int64_t* words) {
+    if (res < 1 || res > 1024 || !words) return pf_fail(PF_ERR_ARGS, "pf_occupancy_words: res must be in [1, 1024]");
+    *words = ((int64_t)res * res * res + 31) / 32;
+    return PF_OK;
+}
+
+extern "C" int pf_occupancy_build(const float* points, const float* radii, const float* density, int64_t n_prims,
+                                  const float* box_lo, const float* box_hi, int32_t res, float sigma_min,
+                                  uint32_t* bits, int32_t* status, void* stream) {
+    VoxelGrid g;
+    if (n_prims < 0 || (n_prims > 0 && (!points || !radii || !density)) || !bits || !status ||
+        !voxel_grid(box_lo, box_hi, res, &g))
+        return pf_fail(PF_ERR_ARGS, "pf_occupancy_build: bad arguments");
+    cudaStream_t st = (cudaStream_t)stream;
+    const int64_t words = ((int64_t)res * res * res + 31) / 32;
+    cudaMemsetAsync(bits, 0, sizeof(uint32_t) * (size_t)words, st);
+    if (n_prims > 0)
+        occupancy_kernel<<<(unsigned)((n_prims + 255) / 256), 256, 0, st>>>(points, radii, density, n_prims, g,
+                                                                           sigma_min, bits, status);
+    return pf_check_launch("pf_occupancy_build");
+}
+
+extern "C" int pf_occupancy_entry(const uint32_t* bits, const float* box_lo, const float* box_hi, int32_t res,
+                                  const pf_camera* cam, float margin, float* t_entry, float* confidence,
+                                  void* stream) {
+    VoxelGrid g;
+    if (!bits || !cam || !t_entry || !confidence || cam->width < 2 || cam->height < 2 || !(margin >= 0.0f) ||
+        !voxel_grid(box_lo, box_hi, res, &g))
+        return pf_fail(PF_ERR_ARGS, "pf_occupancy_entry: bad arguments");
+    const int64_t n = (int64_t)cam->width * cam->height;
+    occupancy_entry_kernel<<<(unsigned)((n + 127) / 128), 128, 0, (cudaStream_t)stream>>>(bits, g, load_cam(*cam),
+                                                                                          margin, t_entry, confidence);
+    return pf_check_launch("pf_occupancy_entry");
 }

@@ -84,12 +84,37 @@ raster_bwd_kernel(RasterParams P, BwdIn in, GradOut go) {
     }
 }
 
-__global__ void zero_nonfinite_kernel(float* __restrict__ a, int64_t n) {
-    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    for (; i < n; i += stride) {
-        float v = a[i];
-        if (!isfinite(v)) a[i] = 0.0f;
+// the gradient arrays of one adjoint, sanitised in one launch: array a covers
+// elements [start[a], start[a + 1]) of the combined index range; arrays whose
+// address is 16-byte aligned and whose length is a multiple of 4 go by float4
+struct SanitizeList {
+    float* ptr[7];
+    int64_t start[8];  // in units of the array's access (float4 or float)
+    bool vec[7];
+};
+
+__global__ void zero_nonfinite_list_kernel(SanitizeList L) {
+    const int64_t total = L.start[7];
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += stride) {
+        int a = 0;
+#pragma unroll
+        for (int k = 1; k < 7; k++) a += i >= L.start[k] ? 1 : 0;
+        const int64_t j = i - L.start[a];
+        if (L.vec[a]) {
+            float4* p = reinterpret_cast<float4*>(L.ptr[a]) + j;
+            float4 v = *p;
+            if (!isfinite(v.x) || !isfinite(v.y) || !isfinite(v.z) || !isfinite(v.w)) {
+                v.x = isfinite(v.x) ? v.x : 0.0f;
+                v.y = isfinite(v.y) ? v.y : 0.0f;
+                v.z = isfinite(v.z) ? v.z : 0.0f;
+                v.w = isfinite(v.w) ? v.w : 0.0f;
+                *p = v;
+            }
+        } else {
+            float* p = L.ptr[a] + j;
+            if (!isfinite(*p)) *p = 0.0f;
+        }
     }
 }
 
@@ -203,11 +228,16 @@ extern "C" int pf_raster_backward(const pf_raster_inputs* in, const int32_t* ear
         else if (P.TW == 16) launch_bwd<16>(P, bi, go, st);
         else launch_bwd<32>(P, bi, go, st);
     }
-    for (int i = 0; i < 7; i++)
-        if (lens[i]) {
-            int64_t n = (int64_t)lens[i];
-            unsigned grid = (unsigned)std::min<int64_t>((n + 255) / 256, 148 * 16);
-            zero_nonfinite_kernel<<<grid, 256, 0, st>>>(outs[i], n);
-        }
+    SanitizeList L;
+    L.start[0] = 0;
+    for (int i = 0; i < 7; i++) {
+        L.ptr[i] = outs[i];
+        L.vec[i] = lens[i] % 4 == 0 && ((uintptr_t)outs[i] % 16) == 0;
+        L.start[i + 1] = L.start[i] + (int64_t)(L.vec[i] ? lens[i] / 4 : lens[i]);
+    }
+    if (L.start[7] > 0) {
+        const unsigned grid = (unsigned)std::min<int64_t>((L.start[7] + 255) / 256, 148 * 16);
+        zero_nonfinite_list_kernel<<<grid, 256, 0, st>>>(L);
+    }
     return pf_check_launch("pf_raster_backward");
 }

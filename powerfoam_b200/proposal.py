@@ -306,16 +306,71 @@ class VoxelLocator:
         return start
 
 
+class OccupancySeeder:
+    """A conservative proposal without a network (pf_occupancy_build,
+    pf_occupancy_entry): each pixel ray starts in the cell that contains the
+    point where it enters the first voxel of a res^3 grid that a primitive of
+    density >= sigma_min reaches (`margin` earlier, one voxel by default), or
+    where it leaves the primitives' box when it meets none.  The walk
+    composites only inside spheres of density >= 1e-3, so the seeded walk
+    skips only cells that add nothing; the cells are located through
+    `locator` (a VoxelLocator)."""
+
+    def __init__(self, points, radii, density, locator, res=128, sigma_min=1e-3, margin=None):
+        self.locator = locator
+        self.res = int(res)
+        dev = locator.points.device
+        words = _lib.c_i64(0)
+        _lib.call("pf_occupancy_words", self.res, _lib.ctypes.byref(words))
+        self.bits = torch.zeros(words.value, dtype=torch.int32, device=dev)
+        self.status = torch.zeros(1, dtype=torch.int32, device=dev)
+        pts = points.float().contiguous()
+        rad = radii.float().contiguous()
+        den = density.float().contiguous()
+        # the grid holds every sphere whole: a ray can cross a sphere's part beyond its centre's box
+        grow = float(rad.max()) if rad.numel() else 0.0
+        lo = [a - grow for a in locator.box[0]]
+        hi = [b + grow for b in locator.box[1]]
+        self.h = max(max(b - a for a, b in zip(lo, hi)), 1e-6) / self.res
+        lo, hi = [a - self.h for a in lo], [b + self.h for b in hi]
+        self.h = max(max(b - a for a, b in zip(lo, hi)), 1e-6) / self.res
+        self.box = ((_lib.c_f * 3)(*lo), (_lib.c_f * 3)(*hi))
+        self.margin = self.h if margin is None else float(margin)
+        _lib.call("pf_occupancy_build", _lib.ptr(pts), _lib.ptr(rad), _lib.ptr(den), pts.shape[0], self.box[0],
+                  self.box[1], self.res, float(sigma_min), _lib.ptr(self.bits), _lib.ptr(self.status),
+                  _lib.stream_ptr())
+
+    def entry(self, camera):
+        """(t_entry, confidence), (H, W) each, for pf_seed_start_cells_vmap."""
+        H, W = camera.height, camera.width
+        dev = self.bits.device
+        t = torch.empty((H, W), dtype=torch.float32, device=dev)
+        c = torch.empty((H, W), dtype=torch.float32, device=dev)
+        _lib.call("pf_occupancy_entry", _lib.ptr(self.bits), self.box[0], self.box[1], self.res,
+                  _lib.ctypes.byref(camera.to_pf()), self.margin, _lib.ptr(t), _lib.ptr(c), _lib.stream_ptr())
+        return t, c
+
+    def start_cells(self, camera, default_start, n_seeded=None):
+        t, c = self.entry(camera)
+        return self.locator.seed(camera, t, c, 0.5, default_start, n_seeded)
+
+    def check(self):
+        s = int(self.status.item())
+        if s != _lib.PF_OK:
+            raise _lib.PfError(s, "a primitive centre or radius is not finite")
+
+
 class SeededTracer:
     """Proposal-seeded cell walk: network forward over the pixel rays, start
     cells from the locator where the confidence reaches the threshold, then
     the tracer's walk from those cells (plain start cell elsewhere)."""
 
     def __init__(self, tracer, net, points, radii, conf_threshold=0.9, adjacency=None, adjacency_offsets=None,
-                 voxel_res=256):
+                 voxel_res=256, occupancy=None):
         self.tracer = tracer
         self.net = net
         self.conf_threshold = conf_threshold
+        self.occupancy = occupancy  # an OccupancySeeder: rays the gate does not seed start at its safe entry
         # with the walk's adjacency: voxel-map location (a few faces per seed), else the grid search
         self.locator = (VoxelLocator(points, radii, adjacency, adjacency_offsets, voxel_res)
                         if adjacency is not None else CellLocator(points, radii))
@@ -326,7 +381,14 @@ class SeededTracer:
         significant cell, so the seed point is backed off by the margin."""
         t, c = self.net.forward(camera=camera)
         t.sub_(self.net.margin)
-        return self.locator.seed(camera, t, c, self.conf_threshold, default_start, self.n_seeded)
+        if self.occupancy is None:
+            return self.locator.seed(camera, t, c, self.conf_threshold, default_start, self.n_seeded)
+        # both seeds are safe: the later one of the two wherever both apply
+        t_o, c_o = self.occupancy.entry(camera)
+        net_ok, occ_ok = c >= self.conf_threshold, c_o > 0.5
+        t = torch.where(net_ok & occ_ok, torch.maximum(t, t_o), torch.where(net_ok, t, t_o)).contiguous()
+        c = (net_ok | occ_ok).float().contiguous()
+        return self.locator.seed(camera, t, c, 0.5, default_start, self.n_seeded)
 
     def render(self, camera, default_start, scene_args, **kw):
         start = self.start_cells(camera, default_start)
