@@ -228,9 +228,10 @@ def algorithmic_bytes(stats, H, W):
     T = es.shape[0]
     lens = offs[1:] - offs[:-1]
     tile_of = torch.repeat_interleave(torch.arange(T, device=offs.device), lens)
-    pos = torch.arange(bins.n_pairs, device=offs.device) - offs[:-1][tile_of]
+    n_pairs = int(bins.n_pairs)  # a device scalar after a sync-free call
+    pos = torch.arange(n_pairs, device=offs.device) - offs[:-1][tile_of]
     visited = pos < es[tile_of]
-    prims = bins.tile_prims.long()[visited]
+    prims = bins.tile_prims[:n_pairs].long()[visited]
     ao = stats["adjacency_offsets"].long()
     deg = (ao[prims + 1] - ao[prims]).sum().item()
     V = int(visited.sum().item())
@@ -238,7 +239,7 @@ def algorithmic_bytes(stats, H, W):
     N = stats["n_prims"]
     fwd = 256 * V + 8 * deg + 4 * V + 8 * (T + 1) + 32 * H * W + 4 * N
     bwd = 256 * V + 8 * deg + 4 * V + 36 * H * W + 2 * 256 * U
-    return dict(fwd=fwd, bwd=bwd, V=V, U=U, deg=deg, pairs=bins.n_pairs, T=T)
+    return dict(fwd=fwd, bwd=bwd, V=V, U=U, deg=deg, pairs=n_pairs, T=T)
 
 
 def cpu_model():
