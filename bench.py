@@ -62,9 +62,10 @@ def parse():
                    "(proposal-seeded vs plain cell walk)")
     p.add_argument("--cpu-slices", type=int, default=4, help="slices (1/16 of a frame each) the CPU baseline times")
     p.add_argument("--no-cpu-baseline", action="store_true")
-    p.add_argument("--sync-free", action="store_true",
-                   help="raster workloads: Rasterizer(host_sync=False), no host read of the pair count per call "
-                   "(overflow and non-finite inputs are checked once after the timed steps)")
+    p.add_argument("--host-sync", action="store_true",
+                   help="raster workloads: Rasterizer(host_sync=True), the reference's host read of the pair count "
+                   "per call; by default the step runs sync-free (host_sync=False: the host queues steps ahead "
+                   "of the GPU, and overflow or non-finite inputs are checked once after the timed steps)")
     p.add_argument("--no-autotune", action="store_true", help="batch workloads: use --tile, chunk 1")
     p.add_argument("--proposal-prims", type=int, default=0,
                    help="proposal workload: primitive count (default 6,291,456; radii scale with the spacing)")
@@ -673,6 +674,7 @@ def trace_main(args, dev):
     rgb = synthetic.texel_rgb(sc, cam)
     st = start_cell(sc["points"], sc["radii"], cam.eye)
     tr = RayTracer(Args(), dev)
+    tr.host_sync = args.host_sync  # default: the forward never waits on the host; checked after the timing
     names = ["points", "radii", "density", "normals", "texel_sites", "texel_height"]
     params = {k: sc[k].clone().requires_grad_(True) for k in names}
     rgb_p = rgb.clone().requires_grad_(True)
@@ -705,6 +707,7 @@ def trace_main(args, dev):
     b.record()
     torch.cuda.synchronize()
     clk = clocks.stop()
+    tr.check()  # a walk stopped early in any timed step raises here
     ms = a.elapsed_time(b) / args.steps
     # targets uploaded on a copy stream into two buffers, as in the rasterizer workload
     t_dev = [torch.empty_like(target) for _ in range(2)]
@@ -726,6 +729,7 @@ def trace_main(args, dev):
         loss_host[i].copy_(loss.detach(), non_blocking=True)
     e1.record()
     torch.cuda.synchronize()
+    tr.check()
     e2e_ms = e0.elapsed_time(e1) / args.steps
     r = tr.trace(cam, st, sc["points"], sc["radii"], sc["density"], sc["normals"], sc["texel_sites"], rgb,
                  sc["texel_height"], adj, off, pm)
@@ -1080,7 +1084,7 @@ def main():
         cam.ray_maps = synthetic.fisheye_ray_maps(cam, 150.0)
         args.no_cpu_baseline = True
     R = rasterize.Rasterizer(ArgsGeneric() if fisheye else Args(), dev, tile_width=args.tile,
-                             host_sync=not args.sync_free)
+                             host_sync=args.host_sync)
     step, params = make_step(R, scene, cam, adj, adj_off, target_dev, world)
 
     def barrier():
@@ -1161,7 +1165,7 @@ def main():
     torch.cuda.synchronize()
     st = algorithmic_bytes(R.last_stats, cfg["height"], cfg["width"])
     R.collect_stats = False
-    R.check()  # with --sync-free: a pair-buffer overflow or non-finite input in any step raises here
+    R.check()  # sync-free: a pair-buffer overflow or non-finite input in any step raises here
     peak, peak_kind = load_peaks()
     dominant = "pf_raster_backward" if bwd_ms >= fwd_ms else "pf_raster_forward"
     dom_ms = max(bwd_ms, fwd_ms)

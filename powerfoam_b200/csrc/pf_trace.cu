@@ -1185,17 +1185,45 @@ PF_D float sh_raw(const float b[16], const float* c, int ch) {
     return acc + 0.5f;
 }
 
+// vec: sh and out 16-byte aligned and S % 4 == 0 -- the 48 coefficients are
+// read as 12 float4 and the S x 3 broadcast colours written as float4 (the
+// same sums in the same order either way)
 __global__ void sh_texel_rgb_kernel(const float* __restrict__ pts, const float* __restrict__ sh, int64_t N, int S,
-                                    v3 eye, float* __restrict__ out) {
+                                    v3 eye, float* __restrict__ out, bool vec) {
     int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= N) return;
     float b[16];
     sh_basis(normalize(mk(pts[3 * p], pts[3 * p + 1], pts[3 * p + 2]) - eye), b);
-    const float* c = sh + p * 48;
+    float c[48];
+    if (vec) {
+        const float4* c4 = reinterpret_cast<const float4*>(sh + p * 48);
+#pragma unroll
+        for (int i = 0; i < 12; i++) {
+            const float4 v = __ldg(c4 + i);
+            c[4 * i] = v.x;
+            c[4 * i + 1] = v.y;
+            c[4 * i + 2] = v.z;
+            c[4 * i + 3] = v.w;
+        }
+    } else {
+#pragma unroll
+        for (int i = 0; i < 48; i++) c[i] = __ldg(sh + p * 48 + i);
+    }
+    float rgb[3];
+#pragma unroll
     for (int ch = 0; ch < 3; ch++) {
-        float acc = sh_raw(b, c, ch);
-        acc = acc > 0.0f ? acc : 0.0f;
-        for (int s = 0; s < S; s++) out[(p * S + s) * 3 + ch] = acc;
+        const float acc = sh_raw(b, c, ch);
+        rgb[ch] = acc > 0.0f ? acc : 0.0f;
+    }
+    if (vec) {
+        float4* o4 = reinterpret_cast<float4*>(out + p * S * 3);
+        for (int q = 0; q < 3 * S / 4; q++) {
+            const int e = 4 * q;  // element e of the row is channel e % 3
+            o4[q] = make_float4(rgb[e % 3], rgb[(e + 1) % 3], rgb[(e + 2) % 3], rgb[(e + 3) % 3]);
+        }
+    } else {
+        for (int s = 0; s < S; s++)
+            for (int ch = 0; ch < 3; ch++) out[(p * S + s) * 3 + ch] = rgb[ch];
     }
 }
 
@@ -1497,8 +1525,9 @@ extern "C" int pf_sh_texel_rgb(const float* points, const float* sh, int64_t n_p
     if (n_prims < 0 || n_sites < 0 || !eye_host || (n_prims > 0 && (!points || !sh || !texel_rgb)))
         return pf_fail(PF_ERR_ARGS, "pf_sh_texel_rgb: bad arguments");
     if (n_prims == 0) return PF_OK;
+    const bool vec = n_sites % 4 == 0 && ((uintptr_t)sh % 16) == 0 && ((uintptr_t)texel_rgb % 16) == 0;
     sh_texel_rgb_kernel<<<(unsigned)((n_prims + 255) / 256), 256, 0, (cudaStream_t)stream>>>(
-        points, sh, n_prims, n_sites, mk(eye_host[0], eye_host[1], eye_host[2]), texel_rgb);
+        points, sh, n_prims, n_sites, mk(eye_host[0], eye_host[1], eye_host[2]), texel_rgb, vec);
     return pf_check_launch("pf_sh_texel_rgb");
 }
 

@@ -71,7 +71,23 @@ class RayTracer:
         # (pf_trace_forward_record), so the adjoint does not walk again; False:
         # plain forward, and the adjoint repeats the walk (pf_trace_backward)
         self.record_segments = True
+        # host_sync (default True): the differentiable forward reads its status
+        # word back and raises at once (step cap, bad cell index); False: the
+        # forward never waits on the host (a training loop queues steps ahead),
+        # the kernels raise the persistent device word ``status`` and check()
+        # reports it
+        self.host_sync = True
+        self.status = torch.zeros(1, dtype=torch.int32, device=self.device)
         _lib.load()
+
+    def check(self):
+        """Raise PfError if a forward since the last check stopped a walk
+        early (host_sync=False mode; one host read); clears the word."""
+        st = int(self.status.item())
+        if st != _lib.PF_OK:
+            self.status.zero_()
+            raise _lib.PfError(st, "cell walk stopped early (step cap or invalid cell index)")
+        return True
 
     def _inputs(self, camera, start, spheres, nsig, sites, rgb, height, adjacency, adjacency_offsets,
                 adjacency_diff, thr, max_steps, depth_quantile):
@@ -123,11 +139,12 @@ class RayTracer:
 
     def trace(self, camera, start, points, radii, density, normals, texel_sites, texel_rgb, texel_height, adjacency,
               adjacency_offsets, adjacency_diff, transmittance_threshold=1e-3, max_steps=DEFAULT_MAX_STEPS,
-              depth_quantile=0.5, visit_cap=0, check_status=True, record=False):
+              depth_quantile=0.5, visit_cap=0, check_status=True, record=False, status=None):
         """Walk every pixel's ray.  ``start`` is one cell index or an (H, W)
         int32 tensor of per-ray start cells.  ``record``: also write the
         adjoint's segment records (pf_trace_forward_record; f32, no visit
-        log), returned in ``records`` for the backward."""
+        log), returned in ``records`` for the backward.  ``status``: a device
+        int32 word the kernels raise (not cleared here); a fresh one when None."""
         H, W = camera.height, camera.width
         dev = self.device
         args = self._prep(points, radii, density, normals, texel_sites, texel_rgb, texel_height, adjacency,
@@ -144,7 +161,8 @@ class RayTracer:
             visit_count=torch.empty((H, W), dtype=torch.int32, device=dev),
             visits=torch.empty((H, W, visit_cap), dtype=torch.int32, device=dev) if visit_cap else None,
         )
-        status = torch.zeros(1, dtype=torch.int32, device=dev)
+        if status is None:
+            status = torch.zeros(1, dtype=torch.int32, device=dev)
         inp = self._inputs(camera, start, *args, transmittance_threshold, max_steps, depth_quantile)
         if record:
             if visit_cap:
@@ -185,7 +203,8 @@ class RayTracer:
         record = self.record_segments and any(ctx.needs_input_grad[3:10])
         r = self.trace(camera, start, points.detach(), radii.detach(), density.detach(), normals.detach(),
                        texel_sites.detach(), texel_rgb.detach(), texel_height.detach(), adjacency, adjacency_offsets,
-                       adjacency_diff, thr, max_steps, depth_quantile, record=record)
+                       adjacency_diff, thr, max_steps, depth_quantile, record=record, check_status=self.host_sync,
+                       status=None if self.host_sync else self.status)
         ctx.records = r.records
         ctx.tracer = self
         ctx.camera = camera

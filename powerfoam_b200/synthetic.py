@@ -162,7 +162,7 @@ def texel_rgb(scene, camera, n_sites=8):
     pts = scene["points"]
     n = pts.shape[0]
     out = torch.empty((n, n_sites, 3), dtype=torch.float32, device=pts.device)
-    e = (_lib.ctypes.c_float * 3)(*[float(v) for v in camera.eye.float().cpu().tolist()])
+    e = camera.to_pf().eye  # the camera's cached C struct: no device read per call
     _lib.call("pf_sh_texel_rgb", _lib.ptr(pts), _lib.ptr(scene["sh"]), n, n_sites, e, _lib.ptr(out),
               _lib.stream_ptr())
     return out

@@ -295,3 +295,27 @@ def test_cycle_guard_adjoint_matches_oracle(cycle_density, kb, rec):
     assert_close_rel(tp["texel_rgb"].grad.cpu().numpy(), g["texel_rgb"], 1e-4, "rgb")
     assert_close_rel(tp["points"].grad.cpu().numpy(), g["spheres"][:, :3], 1e-4, "points")
     assert float(tp["density"].grad[0].abs()) > 0
+
+
+def test_sync_free_forward_reports_the_step_cap_on_check():
+    """host_sync=False: the differentiable forward does not read its status
+    back; a walk stopped by the step cap raises at check(), which clears the
+    word."""
+    sc = np_scene(62, 300, -0.6, 0.6, 0.05, 0.15)
+    cam = np_camera((0.0, 0.0, 2.2), (0, 0, 0), 24, 16, 55.0)
+    tp = {k: to_t(v).requires_grad_(True) for k, v in sc.items()}
+    adj, off = build_power_adjacency(tp["points"].detach(), tp["radii"].detach())
+    pm = power_adjacency_diff(tp["points"].detach(), tp["radii"].detach(), adj, off)
+    s = start_cell(tp["points"].detach(), tp["radii"].detach(), torch.from_numpy(cam["eye"]))
+    R = RayTracer(Args(), "cuda")
+    R.host_sync = False
+    args = (torch_cam(cam), s, tp["points"], tp["radii"], tp["density"], tp["normals"], tp["texel_sites"],
+            tp["texel_rgb"], tp["texel_height"], adj, off, pm, 1e-3)
+    color, _, _, _ = R.forward(*args)
+    color.sum().backward()
+    assert R.check()
+    R.forward(*args, max_steps=2)
+    with pytest.raises(_lib.PfError) as e:
+        R.check()
+    assert e.value.code == _lib.PF_ERR_STEP_CAP
+    assert R.check()
