@@ -62,6 +62,9 @@ def parse():
                    "(proposal-seeded vs plain cell walk)")
     p.add_argument("--cpu-slices", type=int, default=4, help="slices (1/16 of a frame each) the CPU baseline times")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-segment-records", action="store_true",
+                   help="raster workloads: the adjoint clips the sphere intervals again instead of reading the "
+                   "forward's segment records (Rasterizer.record_segments = False)")
     p.add_argument("--host-sync", action="store_true",
                    help="raster workloads: Rasterizer(host_sync=True), the reference's host read of the pair count "
                    "per call; by default the step runs sync-free (host_sync=False: the host queues steps ahead "
@@ -1085,6 +1088,7 @@ def main():
         args.no_cpu_baseline = True
     R = rasterize.Rasterizer(ArgsGeneric() if fisheye else Args(), dev, tile_width=args.tile,
                              host_sync=args.host_sync)
+    R.record_segments = not args.no_segment_records
     step, params = make_step(R, scene, cam, adj, adj_off, target_dev, world)
 
     def barrier():

@@ -36,7 +36,7 @@ extern "C" {
 #define PF_ERR_CELL 6      /* a power cell exceeded its plane / neighbour capacity */
 #define PF_ERR_NONFINITE 7 /* a primitive attribute is NaN or infinite */
 
-#define PF_ABI_VERSION 2
+#define PF_ABI_VERSION 3
 
 #if defined(__GNUC__)
 #define PF_API __attribute__((visibility("default")))
@@ -90,6 +90,22 @@ typedef struct pf_raster_inputs {
                                     backward, or NULL for the pinhole rays;
                                     the benchmark and viewer paths are
                                     pinhole only, as in the reference */
+    float *segments;             /* optional (pairs x tw^2) float4 segment
+                                    records of the hit (primitive, pixel)
+                                    pairs, indexed by the pair's place in
+                                    tile_prims and the pixel's place in its
+                                    tile: the sphere interval clipped by the
+                                    power faces and the ids of the surfaces
+                                    bounding it.  pf_raster_forward writes
+                                    them (tile widths 8 and 16) and
+                                    pf_raster_backward reads them instead of
+                                    clipping again; NULL: none.  16-byte
+                                    aligned */
+    uint32_t *segment_masks;     /* (pairs x tw^2 / 32) per pair and warp of
+                                    32 pixels, the pixels whose ray hits the
+                                    sphere; required with segments */
+    int64_t segment_pairs;       /* pairs the two arrays hold (>= the pairs
+                                    in tile_prims) */
 } pf_raster_inputs;
 
 /* ---------------------------------------------------------------------- */

@@ -67,6 +67,9 @@ class PfRasterInputs(ctypes.Structure):
         ("tile_order", c_vp),
         ("scratch", c_vp),
         ("ray_maps", c_vp),
+        ("segments", c_vp),
+        ("segment_masks", c_vp),
+        ("segment_pairs", c_i64),
     ]
 
 

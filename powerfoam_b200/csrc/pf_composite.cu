@@ -34,8 +34,9 @@
 
 namespace pf {
 
-// GEN: a generic camera (per-pixel rays from ray maps)
-template <int TW, bool GEN = false>
+// GEN: a generic camera (per-pixel rays from ray maps); REC: write the
+// adjoint's segment records (the compacted layouts only)
+template <int TW, bool GEN = false, bool REC = false>
 __global__ void __launch_bounds__(Layout<TW>::THREADS) raster_fwd_kernel(RasterParams P, FwdOut out) {
     constexpr int G = Layout<TW>::G;
     constexpr bool COMPACT = Layout<TW>::PPL == 1;
@@ -51,7 +52,7 @@ __global__ void __launch_bounds__(Layout<TW>::THREADS) raster_fwd_kernel(RasterP
         if (tile < 0) break;
         if constexpr (COMPACT)
             // generic cameras keep the pixels' ray origins after the stages
-            fwd_tile_c<G, GEN>(P, out, tile, warp, lane, reinterpret_cast<FwdCStage*>(fwd_dyn)[warp], ss,
+            fwd_tile_c<G, GEN, REC>(P, out, tile, warp, lane, reinterpret_cast<FwdCStage*>(fwd_dyn)[warp], ss,
                                reinterpret_cast<float4*>(reinterpret_cast<FwdCStage*>(fwd_dyn) + G) + 32 * warp);
         else
             fwd_tile<G, Layout<TW>::PPL, GEN>(P, out, tile, warp, lane, stage[warp], ss);
@@ -65,7 +66,7 @@ constexpr size_t fwd_dyn_bytes() {
 }
 
 
-template <int TW, bool GEN = false>
+template <int TW, bool GEN = false, bool REC = false>
 __global__ void __launch_bounds__(Layout<TW>::THREADS, Layout<TW>::BWD_MIN_BLOCKS)
 raster_bwd_kernel(RasterParams P, BwdIn in, GradOut go) {
     constexpr int G = Layout<TW>::G;
@@ -80,7 +81,7 @@ raster_bwd_kernel(RasterParams P, BwdIn in, GradOut go) {
     for (;;) {
         int64_t tile = next_tile<G>(P, static_next, lane, nullptr);
         if (tile < 0) break;
-        bwd_tile<G, Layout<TW>::PPL, GEN>(P, in, go, tile, warp, lane, stage[warp], bs);
+        bwd_tile<G, Layout<TW>::PPL, GEN, REC>(P, in, go, tile, warp, lane, stage[warp], bs);
     }
 }
 
@@ -131,22 +132,30 @@ static unsigned composite_grid(const RasterParams& P, K kernel, size_t dyn_smem)
     return (unsigned)std::max<int64_t>(1, std::min<int64_t>(groups, resident));
 }
 
-template <int TW, bool GEN>
+template <int TW, bool GEN, bool REC>
 static int launch_fwd_t(const RasterParams& P, const FwdOut& out, cudaStream_t st) {
     const size_t dyn = fwd_dyn_bytes<TW, GEN>();
     if (dyn > 0) {
-        cudaError_t e = cudaFuncSetAttribute(raster_fwd_kernel<TW, GEN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)dyn);
+        cudaError_t e = cudaFuncSetAttribute(raster_fwd_kernel<TW, GEN, REC>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
         if (e != cudaSuccess) return pf_fail(PF_ERR_CUDA, cudaGetErrorString(e));
     }
-    unsigned grid = composite_grid<TW>(P, raster_fwd_kernel<TW, GEN>, dyn);
-    raster_fwd_kernel<TW, GEN><<<grid, Layout<TW>::THREADS, dyn, st>>>(P, out);
+    unsigned grid = composite_grid<TW>(P, raster_fwd_kernel<TW, GEN, REC>, dyn);
+    raster_fwd_kernel<TW, GEN, REC><<<grid, Layout<TW>::THREADS, dyn, st>>>(P, out);
     return PF_OK;
+}
+
+template <int TW, bool GEN>
+static int launch_fwd_g(const RasterParams& P, const FwdOut& out, cudaStream_t st) {
+    if constexpr (Layout<TW>::PPL == 1) {
+        if (P.seg) return launch_fwd_t<TW, GEN, true>(P, out, st);
+    }
+    return launch_fwd_t<TW, GEN, false>(P, out, st);
 }
 
 template <int TW>
 static int launch_fwd(const RasterParams& P, const FwdOut& out, cudaStream_t st) {
-    return P.ray_maps ? launch_fwd_t<TW, true>(P, out, st) : launch_fwd_t<TW, false>(P, out, st);
+    return P.ray_maps ? launch_fwd_g<TW, true>(P, out, st) : launch_fwd_g<TW, false>(P, out, st);
 }
 
 }  // namespace pf
@@ -183,20 +192,31 @@ extern "C" int pf_raster_forward(const pf_raster_inputs* in, int32_t return_poin
     return pf_check_launch("pf_raster_forward");
 }
 
-template <int TW, bool GEN>
+template <int TW, bool GEN, bool REC>
 static void launch_bwd_t(const RasterParams& P, const BwdIn& bi, const GradOut& go, cudaStream_t st) {
     const size_t dyn = sizeof(BwdStage) * Layout<TW>::G;
-    cudaFuncSetAttribute(raster_bwd_kernel<TW, GEN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
-    unsigned grid = composite_grid<TW>(P, raster_bwd_kernel<TW, GEN>, dyn);
-    raster_bwd_kernel<TW, GEN><<<grid, Layout<TW>::THREADS, dyn, st>>>(P, bi, go);
+    cudaFuncSetAttribute(raster_bwd_kernel<TW, GEN, REC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
+    unsigned grid = composite_grid<TW>(P, raster_bwd_kernel<TW, GEN, REC>, dyn);
+    raster_bwd_kernel<TW, GEN, REC><<<grid, Layout<TW>::THREADS, dyn, st>>>(P, bi, go);
+}
+
+template <int TW, bool GEN>
+static void launch_bwd_g(const RasterParams& P, const BwdIn& bi, const GradOut& go, cudaStream_t st) {
+    if constexpr (Layout<TW>::PPL == 1) {
+        if (P.seg) {
+            launch_bwd_t<TW, GEN, true>(P, bi, go, st);
+            return;
+        }
+    }
+    launch_bwd_t<TW, GEN, false>(P, bi, go, st);
 }
 
 template <int TW>
 static void launch_bwd(const RasterParams& P, const BwdIn& bi, const GradOut& go, cudaStream_t st) {
     if (P.ray_maps)
-        launch_bwd_t<TW, true>(P, bi, go, st);
+        launch_bwd_g<TW, true>(P, bi, go, st);
     else
-        launch_bwd_t<TW, false>(P, bi, go, st);
+        launch_bwd_g<TW, false>(P, bi, go, st);
 }
 
 extern "C" int pf_raster_backward(const pf_raster_inputs* in, const int32_t* early_stop, const float* log_t,

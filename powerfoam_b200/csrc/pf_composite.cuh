@@ -433,7 +433,10 @@ PF_D int seg_search(const int* off, int n, int x) {
 // GEN: per-pixel rays of a generic camera; `org` (32 per warp, shared) then
 // holds the pixels' ray origins, and faces are staged with the ray-independent
 // face_offset, each pair subtracting its own origin's dot product.
-template <int G, bool GEN = false>
+// REC: also write each hit pair's segment record (the sphere interval after
+// the power faces and the ids of its bounding surfaces) and each primitive's
+// hit mask, which the adjoint reads instead of clipping again (P.seg).
+template <int G, bool GEN = false, bool REC = false>
 PF_D void fwd_tile_c(const RasterParams& P, const FwdOut& out, int64_t tile, int wig, int lane, FwdCStage& cs,
                      StopState& ss, float4* org = nullptr) {
     const v3 o = P.cam.eye;
@@ -484,6 +487,10 @@ PF_D void fwd_tile_c(const RasterParams& P, const FwdOut& out, int64_t tile, int
             const bool hit = a.g.oob ? false : ray_sphere(ray_org<GEN>(a, o), a.g.d, mk(s4.x, s4.y, s4.z), s4.w, tn, tf);
             const uint32_t m = __ballot_sync(0xffffffffu, hit);
             if (lane == 0) cs.mask[kk] = m;
+            if (REC && lane == 0) {
+                const int64_t pi = start + k0 + kk;
+                if (pi < P.seg_pairs) P.seg_mask[pi * G + wig] = m;
+            }
         }
         __syncwarp();
         int kb = 0;
@@ -545,16 +552,21 @@ PF_D void fwd_tile_c(const RasterParams& P, const FwdOut& out, int64_t tile, int
                     const int32_t prim = cs.pid[kk];
                     float tn, tf;
                     ray_sphere(po, d, center, radius, tn, tf);
+                    int tn_id = tn < 1e-8f ? -2 : -1, tf_id = tf < 1e-8f ? -2 : -1;  // REC (as the adjoint)
                     if (!big) {
-                        const int f1 = cs.face_off[r + 1];
+                        const int f0 = cs.face_off[r], f1 = cs.face_off[r + 1];
 #pragma unroll 2
-                        for (int q = cs.face_off[r]; q < f1; q++) {
+                        for (int q = f0; q < f1; q++) {
                             const float4 f = cs.face[q];
                             const v3 fn = mk(f.x, f.y, f.z);
                             const float dp = dot(d, fn);
                             const float num = GEN ? f.w - dot(po, fn) : f.w;
                             if (face_may_clip(dp, num, tn, tf)) {
                                 const float t_face = num / dp;
+                                if (REC) {
+                                    tf_id = (dp >= 0.0f && t_face < tf) ? q - f0 : tf_id;
+                                    tn_id = (dp < 0.0f && t_face > tn) ? q - f0 : tn_id;
+                                }
                                 tf = dp >= 0.0f ? fmin_t(t_face, tf) : tf;
                                 tn = dp < 0.0f ? fmax_t(t_face, tn) : tn;
                             }
@@ -571,10 +583,19 @@ PF_D void fwd_tile_c(const RasterParams& P, const FwdOut& out, int64_t tile, int
                             const float dp = dot(d, f.n);
                             if (face_may_clip(dp, f.num, tn, tf)) {
                                 const float t_face = f.num / dp;
+                                if (REC) {
+                                    tf_id = (dp >= 0.0f && t_face < tf) ? e - a0 : tf_id;
+                                    tn_id = (dp < 0.0f && t_face > tn) ? e - a0 : tn_id;
+                                }
                                 tf = dp >= 0.0f ? fmin_t(t_face, tf) : tf;
                                 tn = dp < 0.0f ? fmax_t(t_face, tn) : tn;
                             }
                         }
+                    }
+                    if (REC) {
+                        const int64_t pi = start + k0 + kk;
+                        if (pi < P.seg_pairs)
+                            P.seg[pi * (32 * G) + wig * 32 + p] = make_float4(tn, tf, pack_seg_ids(tn_id, tf_id), 0.f);
                     }
                     if (tn < tf) {  // else the plane, which only shrinks [tn, tf], leaves dt <= 0 (or NaN)
                         const float4 n4 = cs.nsg[kk];
@@ -884,9 +905,13 @@ struct BwdIn {
     const float* g_contrib;
 };
 
-template <int G, int PPL, bool GEN = false>
+// REC: the hit masks and the clipped sphere intervals come from the
+// forward's segment records (P.seg), so the sphere tests and the face
+// clipping are not repeated (one pixel per lane only).
+template <int G, int PPL, bool GEN = false, bool REC = false>
 PF_D void bwd_tile(const RasterParams& P, const BwdIn& in, const GradOut& go, int64_t tile, int wig, int lane,
                    WarpStage& ws, BwdStage& bs) {
+    static_assert(!REC || PPL == 1, "segment records are written by the pair-compacted forward");
     const int TS = P.TW * P.TW;
     const v3 o = P.cam.eye;
     const float HW = (float)(P.cam.H * P.cam.W);
@@ -932,9 +957,23 @@ PF_D void bwd_tile(const RasterParams& P, const BwdIn& in, const GradOut& go, in
             const float4 s4 = ws.sph[kk];
             const v3 center = mk(s4.x, s4.y, s4.z);
             const float radius = s4.w;
-            a.hit = a.g.oob ? false : ray_sphere(ray_org<GEN>(a, o), a.g.d, center, radius, a.tn, a.tf);
-            if (PPL == 2) b.hit = b.g.oob ? false : ray_sphere(ray_org<GEN>(b, o), b.g.d, center, radius, b.tn, b.tf);
-            if (!__any_sync(0xffffffffu, a.hit || b.hit)) continue;  // no output changes (see forward)
+            if constexpr (REC) {
+                const int64_t pi = start + k;
+                const uint32_t m = pi < P.seg_pairs ? __ldg(&P.seg_mask[pi * G + wig]) : 0u;
+                if (m == 0u) continue;  // no output changes (see forward)
+                a.hit = (m >> lane) & 1u;
+                if (a.hit) {
+                    const float4 r = __ldg(&P.seg[pi * (32 * G) + wig * 32 + lane]);
+                    a.tn = r.x;
+                    a.tf = r.y;
+                    unpack_seg_ids(r.z, a.tn_id, a.tf_id);
+                }
+            } else {
+                a.hit = a.g.oob ? false : ray_sphere(ray_org<GEN>(a, o), a.g.d, center, radius, a.tn, a.tf);
+                if (PPL == 2)
+                    b.hit = b.g.oob ? false : ray_sphere(ray_org<GEN>(b, o), b.g.d, center, radius, b.tn, b.tf);
+                if (!__any_sync(0xffffffffu, a.hit || b.hit)) continue;  // no output changes (see forward)
+            }
             const int32_t prim = ws.pid[kk];
             const float4 n4 = ws.nsg[kk];
             const v3 pn = mk(n4.x, n4.y, n4.z);
@@ -942,6 +981,7 @@ PF_D void bwd_tile(const RasterParams& P, const BwdIn& in, const GradOut& go, in
             const int32_t a0 = __ldg(&P.adj_off[prim]);
             const int n_adj = __ldg(&P.adj_off[prim + 1]) - a0;
             const float cc = dot(center, center), rr = radius * radius;
+            if constexpr (!REC) {
             a.tn_id = a.tn < 1e-8f ? -2 : -1;
             a.tf_id = a.tf < 1e-8f ? -2 : -1;
             b.tn_id = b.tn < 1e-8f ? -2 : -1;
@@ -979,6 +1019,7 @@ PF_D void bwd_tile(const RasterParams& P, const BwdIn& in, const GradOut& go, in
                 }
                 __syncwarp();
             }
+            }  // !REC
             // The texture plane only shrinks [tn, tf] (and a NaN end never
             // gives dt > 0), so a lane whose faces left tn >= tf adds nothing:
             // with no such lane left the primitive is done (28 % of the hit

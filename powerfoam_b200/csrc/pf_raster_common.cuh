@@ -28,7 +28,21 @@ struct RasterParams {
     const int32_t* tile_order;  // processing order of the tiles (NULL: 0..T-1)
     int* queue;                 // work-queue counter (NULL: one group per tile)
     const float* ray_maps;      // (H,W,6) per-pixel origin, direction (generic camera) or NULL
+    float4* seg;                // segment records (pairs x TW^2) or NULL
+    uint32_t* seg_mask;         // hit masks (pairs x TW^2 / 32)
+    int64_t seg_pairs;          // pairs the two arrays hold
 };
+
+// segment record ids: the surfaces bounding a segment (-2 behind the eye, -1
+// the sphere, else the face's place in the adjacency list), 16 bits each
+PF_D float pack_seg_ids(int tn_id, int tf_id) {
+    return __uint_as_float(((uint32_t)(tn_id + 2) & 0xffffu) | ((uint32_t)(tf_id + 2) << 16));
+}
+PF_D void unpack_seg_ids(float v, int& tn_id, int& tf_id) {
+    const uint32_t u = __float_as_uint(v);
+    tn_id = (int)(u & 0xffffu) - 2;
+    tf_id = (int)(u >> 16) - 2;
+}
 
 // ---------------------------------------------------------------------------
 // group collectives: G == 1 -> warp vote; G > 1 -> block barrier with reduction
@@ -259,6 +273,14 @@ inline bool fill_params(const pf_raster_inputs* in, RasterParams& P, bool need_f
     P.gt = in->ray_gt;
     P.thr = in->transmittance_threshold;
     P.tile_order = in->tile_order;
+    P.seg = (float4*)in->segments;
+    P.seg_mask = in->segment_masks;
+    P.seg_pairs = in->segments ? in->segment_pairs : 0;
+    if (in->segments && (!in->segment_masks || ((uintptr_t)in->segments % 16) != 0 || in->segment_pairs < 0 ||
+                         (in->tile_width != 8 && in->tile_width != 16))) {
+        *why = "segments need segment_masks, 16-byte alignment, segment_pairs >= 0 and tile width 8 or 16";
+        return false;
+    }
     P.queue = (int*)in->scratch;
     P.ray_maps = in->ray_maps;
     return true;

@@ -27,6 +27,9 @@ from . import _lib
 
 TILE_WIDTH = 8
 TILE_SIZE = TILE_WIDTH * TILE_WIDTH
+# device bytes the forward may use for the adjoint's segment records; larger
+# problems clip again in the adjoint
+SEGMENT_BYTES = 8 << 30
 
 # Optional instrumentation: when set, called as hook(name, "begin" | "end")
 # around every library call of the forward / backward (bench.py records CUDA
@@ -205,6 +208,11 @@ class Rasterizer:
         # adjoint then writes the gradients into its views (the cross-GPU
         # exchange runs on the buffer with no copies)
         self.grad_buffer = None
+        # tile widths 8 and 16: when gradients are wanted, the forward writes
+        # each hit (primitive, pixel) pair's clipped sphere interval and
+        # bounding-surface ids (16 bytes per pixel of every listed pair, up to
+        # SEGMENT_BYTES), which the adjoint reads instead of clipping again
+        self.record_segments = True
         _lib.load()
 
     def check(self):
@@ -262,6 +270,13 @@ class Rasterizer:
         _lib.call("pf_adjacency_prefetch", _lib.ptr(spheres), _lib.ptr(adjacency), _lib.ptr(adjacency_offsets),
                   spheres.shape[0], _lib.ptr(adj_diff), _lib.stream_ptr())
         return adj_diff
+
+    @staticmethod
+    def _set_segments(inp, segs):
+        seg, mask, pairs = segs
+        inp.segments = _lib.ptr(seg)
+        inp.segment_masks = _lib.ptr(mask)
+        inp.segment_pairs = int(pairs)
 
     def _inputs(self, camera, spheres, nsig, sites, rgb, height, adjacency, adjacency_offsets, adj_diff, bins,
                 depth_quantiles=None, ray_gt=None, thr=1e-3, attr_half=False, ray_maps=None):
@@ -329,6 +344,15 @@ class Rasterizer:
         stats = torch.empty(self.num_tiles(camera), dtype=torch.int32, device=dev) if self.collect_stats else None
         inp = self._inputs(camera, spheres, nsig, sites, rgb, height, adjacency, adjacency_offsets, adj_diff, bins,
                            dq, gt, transmittance_threshold, ray_maps=ray_maps)
+        segs = None
+        if (grad_ctx is not None and self.record_segments and self.tile_width in (8, 16)
+                and any(grad_ctx.needs_input_grad[3:10])):
+            pairs = bins.tile_prims.numel()  # the pair buffer's capacity (sync-free) or count
+            per_pair = self.tile_width * self.tile_width
+            if 0 < pairs * per_pair * 16 <= SEGMENT_BYTES:
+                segs = (torch.empty((pairs * per_pair, 4), dtype=torch.float32, device=dev),
+                        torch.empty(pairs * per_pair // 32, dtype=torch.int32, device=dev), pairs)
+                self._set_segments(inp, segs)
         _timed_call("pf_raster_forward", _lib.ctypes.byref(inp), int(bool(return_point_err)), _lib.ptr(color),
                     _lib.ptr(log_t), _lib.ptr(nd), _lib.ptr(normal), _lib.ptr(qd), _lib.ptr(err), _lib.ptr(contrib),
                     _lib.ptr(perr), _lib.ptr(early_stop), _lib.ptr(stats), _lib.stream_ptr())
@@ -343,6 +367,7 @@ class Rasterizer:
             grad_ctx.thr = transmittance_threshold
             grad_ctx.bins = bins
             grad_ctx.ray_maps = ray_maps
+            grad_ctx.segments = segs
             grad_ctx.save_for_backward(dq, spheres, nsig, sites, rgb, height, adjacency, adjacency_offsets,
                                        adj_diff, early_stop, log_t)
         opacity = 1.0 - torch.exp(log_t)
@@ -393,11 +418,13 @@ class Rasterizer:
                        height=torch.empty((n, S), dtype=torch.float32, device=dev))
         inp = self._inputs(camera, spheres, nsig, sites, rgb, height, adjacency, adjacency_offsets, adj_diff,
                            grad_ctx.bins, dq, None, grad_ctx.thr, ray_maps=grad_ctx.ray_maps)
+        if grad_ctx.segments is not None:
+            self._set_segments(inp, grad_ctx.segments)
         _timed_call("pf_raster_backward", _lib.ctypes.byref(inp), _lib.ptr(early_stop), _lib.ptr(log_t), _lib.ptr(gc),
                     _lib.ptr(go), _lib.ptr(gnd), _lib.ptr(gn), _lib.ptr(gq), _lib.ptr(gcon), _lib.ptr(out["points"]),
                     _lib.ptr(out["radii"]), _lib.ptr(out["normals"]), _lib.ptr(out["density"]),
                     _lib.ptr(out["sites"]), _lib.ptr(out["rgb"]), _lib.ptr(out["height"]), _lib.stream_ptr())
-        del grad_ctx.rasterizer, grad_ctx.camera, grad_ctx.bins
+        del grad_ctx.rasterizer, grad_ctx.camera, grad_ctx.bins, grad_ctx.segments
         grads = (None, None, None, out["points"], out["radii"], out["density"], out["normals"], out["sites"],
                  out["rgb"], out["height"], None, None, None, None)
         return grads + (None,) * (grad_ctx.n_inputs - 14)

@@ -431,3 +431,34 @@ def test_gradients_into_a_flat_buffer():
                 assert lo <= g.data_ptr() < hi, k
     for k in grads[0]:
         assert_close_rel(grads[1][k].cpu().numpy(), grads[0][k].cpu().numpy(), 1e-5, k)
+
+
+@pytest.mark.parametrize("tw", [8, 16])
+def test_segment_records_give_the_clipping_adjoint(tw):
+    """The adjoint that reads the forward's segment records (sphere interval
+    after the power faces, bounding ids) against the one that clips again:
+    the same images, and gradients equal up to the order of the float
+    atomics; an oversized record budget falls back to clipping."""
+    import powerfoam_b200.rasterize as rz
+
+    sc = np_scene(63, 900, -0.6, 0.6, 0.03, 0.15)
+    cam = torch_cam(np_camera((0.25, 0.2, 2.2), (0, 0, 0), 83, 61, 55.0))  # ragged tiles
+    adj, adj_off = (to_t(a) for a in cech_np(sc["points"], sc["radii"]))
+    rng = np.random.default_rng(10)
+    w = [to_t(rng.standard_normal(s).astype(np.float32)) for s in ((61, 83, 3), (61, 83), (61, 83, 3))]
+    res = []
+    for rec, budget in ((True, rz.SEGMENT_BYTES), (False, rz.SEGMENT_BYTES), (True, 16)):
+        R = Rasterizer(Args(), "cuda", tile_width=tw)
+        R.record_segments = rec
+        old, rz.SEGMENT_BYTES = rz.SEGMENT_BYTES, budget
+        try:
+            res.append(_render_grads(R, cam, _params(sc), adj, adj_off, w))
+        finally:
+            rz.SEGMENT_BYTES = old
+    (imgs, grads) = res[0]
+    for other_imgs, other_grads in res[1:]:
+        for a, b in zip(imgs, other_imgs):
+            assert torch.equal(a, b)
+        for k in grads:
+            d = (grads[k] - other_grads[k]).norm() / grads[k].norm().clamp_min(1e-30)
+            assert d.item() <= 1e-5, k
