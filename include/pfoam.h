@@ -104,8 +104,13 @@ typedef struct pf_raster_inputs {
     uint32_t *segment_masks;     /* (pairs x tw^2 / 32) per pair and warp of
                                     32 pixels, the pixels whose ray hits the
                                     sphere; required with segments */
-    int64_t segment_pairs;       /* pairs the two arrays hold (>= the pairs
-                                    in tile_prims) */
+    int64_t segment_pairs;       /* pairs the arrays hold (>= the pairs in
+                                    tile_prims) */
+    float *segment_planes;       /* optional, with segments: (pairs x tw^2 x
+                                    3) float4, the texture-plane result of
+                                    each pair whose clipped interval is not
+                                    empty, so that the adjoint does not
+                                    evaluate the plane again; NULL: none */
 } pf_raster_inputs;
 
 /* ---------------------------------------------------------------------- */

@@ -66,7 +66,7 @@ constexpr size_t fwd_dyn_bytes() {
 }
 
 
-template <int TW, bool GEN = false, bool REC = false>
+template <int TW, bool GEN = false, int REC = 0>
 __global__ void __launch_bounds__(Layout<TW>::THREADS, Layout<TW>::BWD_MIN_BLOCKS)
 raster_bwd_kernel(RasterParams P, BwdIn in, GradOut go) {
     constexpr int G = Layout<TW>::G;
@@ -192,7 +192,7 @@ extern "C" int pf_raster_forward(const pf_raster_inputs* in, int32_t return_poin
     return pf_check_launch("pf_raster_forward");
 }
 
-template <int TW, bool GEN, bool REC>
+template <int TW, bool GEN, int REC>
 static void launch_bwd_t(const RasterParams& P, const BwdIn& bi, const GradOut& go, cudaStream_t st) {
     const size_t dyn = sizeof(BwdStage) * Layout<TW>::G;
     cudaFuncSetAttribute(raster_bwd_kernel<TW, GEN, REC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
@@ -203,12 +203,16 @@ static void launch_bwd_t(const RasterParams& P, const BwdIn& bi, const GradOut& 
 template <int TW, bool GEN>
 static void launch_bwd_g(const RasterParams& P, const BwdIn& bi, const GradOut& go, cudaStream_t st) {
     if constexpr (Layout<TW>::PPL == 1) {
+        if (P.seg && P.seg_plane) {
+            launch_bwd_t<TW, GEN, 2>(P, bi, go, st);
+            return;
+        }
         if (P.seg) {
-            launch_bwd_t<TW, GEN, true>(P, bi, go, st);
+            launch_bwd_t<TW, GEN, 1>(P, bi, go, st);
             return;
         }
     }
-    launch_bwd_t<TW, GEN, false>(P, bi, go, st);
+    launch_bwd_t<TW, GEN, 0>(P, bi, go, st);
 }
 
 template <int TW>

@@ -601,6 +601,10 @@ PF_D void fwd_tile_c(const RasterParams& P, const FwdOut& out, int64_t tile, int
                         const float4 n4 = cs.nsg[kk];
                         const PlaneRes pr = plane_fwd_tex(po, d, tn, center, mk(n4.x, n4.y, n4.z), radius,
                                                           global_texels(P, prim), P.S);
+                        if (REC && P.seg_plane) {
+                            const int64_t pi = start + k0 + kk;
+                            if (pi < P.seg_pairs) store_plane(P.seg_plane + (pi * (32 * G) + wig * 32 + p) * 3, pr);
+                        }
                         const float tf2 = pr.dp >= 0.0f ? fmin_t(pr.t_surf, tf) : tf;
                         const float tn2 = pr.dp < 0.0f ? fmax_t(pr.t_surf, tn) : tn;
                         cs.rec[j & 63] = make_float4(tf2 - tn2, pr.rgb.x, pr.rgb.y, pr.rgb.z);
@@ -905,10 +909,11 @@ struct BwdIn {
     const float* g_contrib;
 };
 
-// REC: the hit masks and the clipped sphere intervals come from the
+// REC >= 1: the hit masks and the clipped sphere intervals come from the
 // forward's segment records (P.seg), so the sphere tests and the face
-// clipping are not repeated (one pixel per lane only).
-template <int G, int PPL, bool GEN = false, bool REC = false>
+// clipping are not repeated; REC == 2: the texture-plane results too
+// (P.seg_plane).  One pixel per lane only.
+template <int G, int PPL, bool GEN = false, int REC = 0>
 PF_D void bwd_tile(const RasterParams& P, const BwdIn& in, const GradOut& go, int64_t tile, int wig, int lane,
                    WarpStage& ws, BwdStage& bs) {
     static_assert(!REC || PPL == 1, "segment records are written by the pair-compacted forward");
@@ -1047,7 +1052,11 @@ PF_D void bwd_tile(const RasterParams& P, const BwdIn& in, const GradOut& go, in
                     const float _t_near = t_near;
                     const int _t_near_id = t_near_id, _t_far_id = t_far_id;
                     const v3 xo = ray_org<GEN>(x, o);
-                    PlaneRes pr = plane_fwd_smem(xo, d, t_near, center, pn, radius, ws, P.S);
+                    PlaneRes pr;
+                    if constexpr (REC == 2)
+                        pr = load_plane(P.seg_plane + ((start + k) * (32 * G) + wig * 32 + lane) * 3);
+                    else
+                        pr = plane_fwd_smem(xo, d, t_near, center, pn, radius, ws, P.S);
                     t_far_id = (pr.dp >= 0.0f && pr.t_surf < t_far) ? n_adj : t_far_id;
                     t_far = pr.dp >= 0.0f ? fmin_t(pr.t_surf, t_far) : t_far;
                     t_near_id = (pr.dp < 0.0f && pr.t_surf > t_near) ? n_adj : t_near_id;

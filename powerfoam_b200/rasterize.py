@@ -27,9 +27,10 @@ from . import _lib
 
 TILE_WIDTH = 8
 TILE_SIZE = TILE_WIDTH * TILE_WIDTH
-# device bytes the forward may use for the adjoint's segment records; larger
-# problems clip again in the adjoint
-SEGMENT_BYTES = 8 << 30
+# device bytes the forward may use for the adjoint's segment records (64 per
+# pixel of every listed pair with the texture-plane results, 16 without);
+# larger problems keep the intervals only, or clip again in the adjoint
+SEGMENT_BYTES = 24 << 30
 
 # Optional instrumentation: when set, called as hook(name, "begin" | "end")
 # around every library call of the forward / backward (bench.py records CUDA
@@ -96,7 +97,8 @@ class Binner:
     per call, re-binning with a larger capacity when the estimate was too
     small, and PfError(PF_ERR_NONFINITE) when the status reports a NaN or
     infinite attribute.  Sync-free (``sync=False``): the first call sizes the
-    pair buffer with one read (1.25x headroom, a power of two); later calls
+    pair buffer with one read (1.25x headroom, rounded up to a multiple of
+    65,536 pairs); later calls
     read nothing back, so they can be captured in a CUDA graph; an overflow
     then empties the tile lists and raises PF_ERR_OVERFLOW in the caller's
     persistent ``status`` word, which the caller checks when it chooses."""
@@ -106,6 +108,10 @@ class Binner:
         self.capacity = 0
         self.headroom = headroom
         self.ws = None
+
+    @staticmethod
+    def _round(n):
+        return ((int(n) + 65535) >> 16) << 16
 
     def _ensure(self, n_prims, cap, num_tiles):
         nbytes = _lib.ctypes.c_size_t(0)
@@ -161,11 +167,11 @@ class Binner:
                 raise _lib.PfError(st, "a primitive attribute is NaN or infinite")
             if n <= cap:
                 break
-            cap = 1 << (int(n * self.headroom) - 1).bit_length()
+            cap = self._round(n * self.headroom)
             status.zero_()
         self.capacity = max(self.capacity, cap)
         if not sync:  # sized: later calls read nothing back
-            self.capacity = max(self.capacity, 1 << (int(max(n, 1) * self.headroom) - 1).bit_length())
+            self.capacity = max(self.capacity, self._round(max(n, 1) * self.headroom))
         return TileBins(t_off, t_prims[:n], n, vis.bool(), keys[:n] if return_keys else None, t_ord)
 
 
@@ -210,8 +216,9 @@ class Rasterizer:
         self.grad_buffer = None
         # tile widths 8 and 16: when gradients are wanted, the forward writes
         # each hit (primitive, pixel) pair's clipped sphere interval and
-        # bounding-surface ids (16 bytes per pixel of every listed pair, up to
-        # SEGMENT_BYTES), which the adjoint reads instead of clipping again
+        # bounding-surface ids, and its texture-plane result (64 bytes per
+        # pixel of every listed pair, up to SEGMENT_BYTES), which the adjoint
+        # reads instead of clipping and evaluating the plane again
         self.record_segments = True
         _lib.load()
 
@@ -273,10 +280,11 @@ class Rasterizer:
 
     @staticmethod
     def _set_segments(inp, segs):
-        seg, mask, pairs = segs
+        seg, mask, pairs, planes = segs
         inp.segments = _lib.ptr(seg)
         inp.segment_masks = _lib.ptr(mask)
         inp.segment_pairs = int(pairs)
+        inp.segment_planes = _lib.ptr(planes)
 
     def _inputs(self, camera, spheres, nsig, sites, rgb, height, adjacency, adjacency_offsets, adj_diff, bins,
                 depth_quantiles=None, ray_gt=None, thr=1e-3, attr_half=False, ray_maps=None):
@@ -349,9 +357,12 @@ class Rasterizer:
                 and any(grad_ctx.needs_input_grad[3:10])):
             pairs = bins.tile_prims.numel()  # the pair buffer's capacity (sync-free) or count
             per_pair = self.tile_width * self.tile_width
-            if 0 < pairs * per_pair * 16 <= SEGMENT_BYTES:
-                segs = (torch.empty((pairs * per_pair, 4), dtype=torch.float32, device=dev),
-                        torch.empty(pairs * per_pair // 32, dtype=torch.int32, device=dev), pairs)
+            slots = pairs * per_pair
+            if 0 < slots * 16 <= SEGMENT_BYTES:
+                planes = (torch.empty((slots * 3, 4), dtype=torch.float32, device=dev)
+                          if slots * 64 <= SEGMENT_BYTES else None)
+                segs = (torch.empty((slots, 4), dtype=torch.float32, device=dev),
+                        torch.empty(slots // 32, dtype=torch.int32, device=dev), pairs, planes)
                 self._set_segments(inp, segs)
         _timed_call("pf_raster_forward", _lib.ctypes.byref(inp), int(bool(return_point_err)), _lib.ptr(color),
                     _lib.ptr(log_t), _lib.ptr(nd), _lib.ptr(normal), _lib.ptr(qd), _lib.ptr(err), _lib.ptr(contrib),

@@ -436,9 +436,10 @@ def test_gradients_into_a_flat_buffer():
 @pytest.mark.parametrize("tw", [8, 16])
 def test_segment_records_give_the_clipping_adjoint(tw):
     """The adjoint that reads the forward's segment records (sphere interval
-    after the power faces, bounding ids) against the one that clips again:
-    the same images, and gradients equal up to the order of the float
-    atomics; an oversized record budget falls back to clipping."""
+    after the power faces, bounding ids, texture-plane results) against the
+    one that clips and evaluates the plane again: the same images, and
+    gradients equal up to the order of the float atomics; record budgets
+    that hold the intervals only, or nothing, give the same."""
     import powerfoam_b200.rasterize as rz
 
     sc = np_scene(63, 900, -0.6, 0.6, 0.03, 0.15)
@@ -446,8 +447,12 @@ def test_segment_records_give_the_clipping_adjoint(tw):
     adj, adj_off = (to_t(a) for a in cech_np(sc["points"], sc["radii"]))
     rng = np.random.default_rng(10)
     w = [to_t(rng.standard_normal(s).astype(np.float32)) for s in ((61, 83, 3), (61, 83), (61, 83, 3))]
+    probe = Rasterizer(Args(), "cuda", tile_width=tw)
+    probe.collect_stats = True
+    _render_grads(probe, cam, _params(sc), adj, adj_off, w)
+    slots = probe.last_stats["bins"].tile_prims.numel() * tw * tw
     res = []
-    for rec, budget in ((True, rz.SEGMENT_BYTES), (False, rz.SEGMENT_BYTES), (True, 16)):
+    for rec, budget in ((True, rz.SEGMENT_BYTES), (False, rz.SEGMENT_BYTES), (True, 32 * slots), (True, 8 * slots)):
         R = Rasterizer(Args(), "cuda", tile_width=tw)
         R.record_segments = rec
         old, rz.SEGMENT_BYTES = rz.SEGMENT_BYTES, budget
