@@ -37,7 +37,8 @@ namespace pf {
 // GEN: a generic camera (per-pixel rays from ray maps); REC: write the
 // adjoint's segment records (the compacted layouts only)
 template <int TW, bool GEN = false, bool REC = false>
-__global__ void __launch_bounds__(Layout<TW>::THREADS) raster_fwd_kernel(RasterParams P, FwdOut out) {
+__global__ void __launch_bounds__(Layout<TW>::THREADS, Layout<TW>::FWD_MIN_BLOCKS)
+raster_fwd_kernel(RasterParams P, FwdOut out) {
     constexpr int G = Layout<TW>::G;
     constexpr bool COMPACT = Layout<TW>::PPL == 1;
     // the per-pixel layouts stage per warp here; the compacted one keeps its
