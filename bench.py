@@ -84,23 +84,30 @@ def parse():
 # pass): DRAM bytes read + written, and warp instructions for the issue roofline.  Recorded once
 # per kernel change; the bench line carries them as capture metadata next to its live timings.
 CAPTURES = {
-    ("raster1m", "pf_raster_backward"): dict(
+    # the adjoint that reads the forward's segment records (the default)
+    ("raster1m", "pf_raster_backward", True): dict(
+        traffic=4.56e9 + 261.81e6, warp_instructions=6_874_060_237,
+        source="ncu capture of raster_bwd_kernel<8, 0, 2> (second launch of `python bench.py --steps 2 --warmup 1 "
+               "--no-cpu-baseline`): dram__bytes_read.sum + dram__bytes_write.sum, smsp__inst_executed.sum"),
+    # the adjoint that clips again (--no-segment-records)
+    ("raster1m", "pf_raster_backward", False): dict(
         traffic=816.77e6 + 206.06e6, warp_instructions=11_715_679_565,
         source="ncu capture of raster_bwd_kernel<8, 0> (second launch of `python bench.py --steps 2 --warmup 1 "
-               "--no-cpu-baseline`): dram__bytes_read.sum + dram__bytes_write.sum, smsp__inst_executed.sum"),
+               "--no-cpu-baseline --no-segment-records`): dram__bytes_read.sum + dram__bytes_write.sum, "
+               "smsp__inst_executed.sum"),
 }
 SMS, SCHEDULERS_PER_SM = 148, 4
 
 
-def capture_traffic(kernel, workload):
-    c = CAPTURES.get((workload, kernel))
+def capture_traffic(kernel, workload, records):
+    c = CAPTURES.get((workload, kernel, records))
     return (c["traffic"], c["source"]) if c else None
 
 
-def issue_roofline(kernel, workload, ms, sm_mhz):
+def issue_roofline(kernel, workload, records, ms, sm_mhz):
     """Warp instructions of the captured launch / issue slots of the live
     launch time (148 SMs x 4 schedulers x clock x time)."""
-    c = CAPTURES.get((workload, kernel))
+    c = CAPTURES.get((workload, kernel, records))
     if not c or not ms:
         return None
     mhz = sm_mhz or 1965.0
@@ -243,7 +250,36 @@ def algorithmic_bytes(stats, H, W):
     N = stats["n_prims"]
     fwd = 256 * V + 8 * deg + 4 * V + 8 * (T + 1) + 32 * H * W + 4 * N
     bwd = 256 * V + 8 * deg + 4 * V + 36 * H * W + 2 * 256 * U
-    return dict(fwd=fwd, bwd=bwd, V=V, U=U, deg=deg, pairs=n_pairs, T=T)
+    rec = segment_record_bytes(stats, visited)
+    # the forward writes the segment records, the adjoint reads them (and skips the face records)
+    if rec:
+        fwd += rec["bytes"]
+        bwd += rec["bytes"] - 8 * deg
+    return dict(fwd=fwd, bwd=bwd, V=V, U=U, deg=deg, pairs=n_pairs, T=T, records=rec)
+
+
+def segment_record_bytes(stats, visited, chunk=1 << 18):
+    """Bytes of the segment records of the visited pairs: 4 B of hit mask per
+    (pair, warp), 16 B per hit pixel, 48 B of texture-plane result per hit
+    pixel whose clipped interval is not empty (counted from the records)."""
+    segs = stats.get("segments")
+    if segs is None:
+        return None
+    seg, mask, pairs, planes = segs
+    ts = stats["tile_width"] ** 2
+    g = ts // 32
+    idx = torch.nonzero(visited).flatten()
+    hits = nonempty = 0
+    bit = torch.arange(32, device=mask.device, dtype=torch.int32)
+    for c in range(0, idx.numel(), chunk):
+        p = idx[c:c + chunk]
+        m = mask.view(pairs, g)[p]                                    # (n, g)
+        h = ((m[..., None] >> bit) & 1).bool().reshape(-1, ts)        # (n, ts)
+        r = seg.view(pairs, ts, -1)[p]                                # (n, ts, 4 or 16)
+        hits += int(h.sum())
+        nonempty += int((h & (r[..., 0] < r[..., 1])).sum())
+    b = 4 * idx.numel() * g + 16 * hits + (48 * nonempty if planes else 0)
+    return dict(bytes=b, hit_pixels=hits, nonempty_pixels=nonempty)
 
 
 def cpu_model():
@@ -1171,6 +1207,7 @@ def main():
     R.collect_stats = False
     R.check()  # sync-free: a pair-buffer overflow or non-finite input in any step raises here
     peak, peak_kind = load_peaks()
+    recs = st["records"] is not None
     dominant = "pf_raster_backward" if bwd_ms >= fwd_ms else "pf_raster_forward"
     dom_ms = max(bwd_ms, fwd_ms)
     dom_bytes = st["bwd"] if dominant == "pf_raster_backward" else st["fwd"]
@@ -1188,10 +1225,11 @@ def main():
                          d2h_bytes_per_step=4),
                 roofline=dict(bound="hbm", kernel=dominant, achieved=achieved, peak=peak, unit="GB/s",
                               frac=achieved / peak, peak_source=peak_kind,
-                              traffic=(capture_traffic(dominant, args.workload) or (None, None))[0],
-                              traffic_source=(capture_traffic(dominant, args.workload) or (None, None))[1],
+                              traffic=(capture_traffic(dominant, args.workload, recs) or (None, None))[0],
+                              traffic_source=(capture_traffic(dominant, args.workload, recs) or (None, None))[1],
                               algorithmic_bytes=dom_bytes, ms=dom_ms, fwd_ms=fwd_ms, bwd_ms=bwd_ms,
-                              issue=issue_roofline(dominant, args.workload, dom_ms, (clk or {}).get("sm_mhz"))),
+                              issue=issue_roofline(dominant, args.workload, recs, dom_ms, (clk or {}).get("sm_mhz")),
+                              segment_records=st["records"]),
                 gpu_launches=None)
     # kernels per step: pack 1, binning with tile order, prefetch 1, SH 1, forward 1, backward 1 + 1 sanitise
     line["gpu_launches"] = args.steps * (1 + bin_launches(st["T"]) + 1 + 1 + 1 + 1 + 1)

@@ -90,27 +90,26 @@ typedef struct pf_raster_inputs {
                                     backward, or NULL for the pinhole rays;
                                     the benchmark and viewer paths are
                                     pinhole only, as in the reference */
-    float *segments;             /* optional (pairs x tw^2) float4 segment
-                                    records of the hit (primitive, pixel)
-                                    pairs, indexed by the pair's place in
-                                    tile_prims and the pixel's place in its
-                                    tile: the sphere interval clipped by the
-                                    power faces and the ids of the surfaces
-                                    bounding it.  pf_raster_forward writes
-                                    them (tile widths 8 and 16) and
-                                    pf_raster_backward reads them instead of
-                                    clipping again; NULL: none.  16-byte
+    float *segments;             /* optional segment records of the hit
+                                    (primitive, pixel) pairs, one slot per
+                                    pixel of every pair in tile_prims (slot =
+                                    pair x tw^2 + the pixel's place in its
+                                    tile): a float4 with the sphere interval
+                                    clipped by the power faces and the ids of
+                                    the surfaces bounding it, then, with
+                                    segment_planes, three float4 of the
+                                    texture-plane result (64 bytes per slot).
+                                    pf_raster_forward writes them (tile widths
+                                    8 and 16) and pf_raster_backward reads
+                                    them instead of clipping and evaluating
+                                    the plane again; NULL: none.  16-byte
                                     aligned */
     uint32_t *segment_masks;     /* (pairs x tw^2 / 32) per pair and warp of
                                     32 pixels, the pixels whose ray hits the
                                     sphere; required with segments */
     int64_t segment_pairs;       /* pairs the arrays hold (>= the pairs in
                                     tile_prims) */
-    float *segment_planes;       /* optional, with segments: (pairs x tw^2 x
-                                    3) float4, the texture-plane result of
-                                    each pair whose clipped interval is not
-                                    empty, so that the adjoint does not
-                                    evaluate the plane again; NULL: none */
+    int32_t segment_planes;      /* 1: the slots hold the plane results */
 } pf_raster_inputs;
 
 /* ---------------------------------------------------------------------- */

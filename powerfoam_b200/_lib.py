@@ -70,7 +70,7 @@ class PfRasterInputs(ctypes.Structure):
         ("segments", c_vp),
         ("segment_masks", c_vp),
         ("segment_pairs", c_i64),
-        ("segment_planes", c_vp),
+        ("segment_planes", c_i32),
     ]
 
 

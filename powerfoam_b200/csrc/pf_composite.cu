@@ -204,7 +204,7 @@ static void launch_bwd_t(const RasterParams& P, const BwdIn& bi, const GradOut& 
 template <int TW, bool GEN>
 static void launch_bwd_g(const RasterParams& P, const BwdIn& bi, const GradOut& go, cudaStream_t st) {
     if constexpr (Layout<TW>::PPL == 1) {
-        if (P.seg && P.seg_plane) {
+        if (P.seg && P.seg_stride == 4) {
             launch_bwd_t<TW, GEN, 2>(P, bi, go, st);
             return;
         }

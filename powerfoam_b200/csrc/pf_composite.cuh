@@ -599,15 +599,17 @@ PF_D void fwd_tile_c(const RasterParams& P, const FwdOut& out, int64_t tile, int
                     if (REC) {
                         const int64_t pi = start + k0 + kk;
                         if (pi < P.seg_pairs)
-                            P.seg[pi * (32 * G) + wig * 32 + p] = make_float4(tn, tf, pack_seg_ids(tn_id, tf_id), 0.f);
+                            P.seg[(pi * (32 * G) + wig * 32 + p) * P.seg_stride] =
+                                make_float4(tn, tf, pack_seg_ids(tn_id, tf_id), 0.f);
                     }
                     if (tn < tf) {  // else the plane, which only shrinks [tn, tf], leaves dt <= 0 (or NaN)
                         const float4 n4 = cs.nsg[kk];
                         const PlaneRes pr = plane_fwd_tex(po, d, tn, center, mk(n4.x, n4.y, n4.z), radius,
                                                           global_texels(P, prim), P.S);
-                        if (REC && P.seg_plane) {
+                        if (REC && P.seg_stride == 4) {
                             const int64_t pi = start + k0 + kk;
-                            if (pi < P.seg_pairs) store_plane(P.seg_plane + (pi * (32 * G) + wig * 32 + p) * 3, pr);
+                            if (pi < P.seg_pairs)
+                                store_plane(P.seg + (pi * (32 * G) + wig * 32 + p) * 4, pr);
                         }
                         const float tf2 = pr.dp >= 0.0f ? fmin_t(pr.t_surf, tf) : tf;
                         const float tn2 = pr.dp < 0.0f ? fmax_t(pr.t_surf, tn) : tn;
@@ -916,7 +918,7 @@ struct BwdIn {
 // REC >= 1: the hit masks and the clipped sphere intervals come from the
 // forward's segment records (P.seg), so the sphere tests and the face
 // clipping are not repeated; REC == 2: the texture-plane results too
-// (P.seg_plane).  One pixel per lane only.
+// (P.seg_stride == 4).  One pixel per lane only.
 template <int G, int PPL, bool GEN = false, int REC = 0>
 PF_D void bwd_tile(const RasterParams& P, const BwdIn& in, const GradOut& go, int64_t tile, int wig, int lane,
                    WarpStage& ws, BwdStage& bs) {
@@ -972,7 +974,7 @@ PF_D void bwd_tile(const RasterParams& P, const BwdIn& in, const GradOut& go, in
                 if (m == 0u) continue;  // no output changes (see forward)
                 a.hit = (m >> lane) & 1u;
                 if (a.hit) {
-                    const float4 r = __ldg(&P.seg[pi * (32 * G) + wig * 32 + lane]);
+                    const float4 r = __ldg(&P.seg[(pi * (32 * G) + wig * 32 + lane) * P.seg_stride]);
                     a.tn = r.x;
                     a.tf = r.y;
                     unpack_seg_ids(r.z, a.tn_id, a.tf_id);
@@ -1058,7 +1060,7 @@ PF_D void bwd_tile(const RasterParams& P, const BwdIn& in, const GradOut& go, in
                     const v3 xo = ray_org<GEN>(x, o);
                     PlaneRes pr;
                     if constexpr (REC == 2)
-                        pr = load_plane(P.seg_plane + ((start + k) * (32 * G) + wig * 32 + lane) * 3);
+                        pr = load_plane(P.seg + ((start + k) * (32 * G) + wig * 32 + lane) * 4);
                     else
                         pr = plane_fwd_smem(xo, d, t_near, center, pn, radius, ws, P.S);
                     t_far_id = (pr.dp >= 0.0f && pr.t_surf < t_far) ? n_adj : t_far_id;

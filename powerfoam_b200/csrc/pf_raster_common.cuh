@@ -28,20 +28,22 @@ struct RasterParams {
     const int32_t* tile_order;  // processing order of the tiles (NULL: 0..T-1)
     int* queue;                 // work-queue counter (NULL: one group per tile)
     const float* ray_maps;      // (H,W,6) per-pixel origin, direction (generic camera) or NULL
-    float4* seg;                // segment records (pairs x TW^2) or NULL
+    float4* seg;                // segment records, seg_stride float4 per slot (pairs x TW^2), or NULL
     uint32_t* seg_mask;         // hit masks (pairs x TW^2 / 32)
     int64_t seg_pairs;          // pairs the arrays hold
-    float4* seg_plane;          // texture-plane results (pairs x TW^2 x 3) or NULL
+    int seg_stride;             // 4: the slots hold the plane results (float4 1..3), 1: intervals only
 };
 
-// texture-plane result of a segment record (3 float4 per slot)
-PF_D void store_plane(float4* dst, const PlaneRes& r) {
-    dst[0] = make_float4(r.rgb.x, r.rgb.y, r.rgb.z, r.height);
-    dst[1] = make_float4(r.wsum, r._wsum, r.t_surf, r.dp);
-    dst[2] = make_float4(r._t_surf, r._dp, 0.f, 0.f);
+// texture-plane result in float4 1..3 of a 64-byte slot (the interval is
+// float4 0): a pixel with a non-empty interval moves two whole 32-byte
+// sectors, one with an empty interval the first only
+PF_D void store_plane(float4* slot, const PlaneRes& r) {
+    slot[1] = make_float4(r.rgb.x, r.rgb.y, r.rgb.z, r.height);
+    slot[2] = make_float4(r.wsum, r._wsum, r.t_surf, r.dp);
+    slot[3] = make_float4(r._t_surf, r._dp, 0.f, 0.f);
 }
-PF_D PlaneRes load_plane(const float4* src) {
-    const float4 a = __ldg(src), b = __ldg(src + 1), c = __ldg(src + 2);
+PF_D PlaneRes load_plane(const float4* slot) {
+    const float4 a = __ldg(slot + 1), b = __ldg(slot + 2), c = __ldg(slot + 3);
     PlaneRes r;
     r.rgb = mk(a.x, a.y, a.z);
     r.height = a.w;
@@ -297,11 +299,7 @@ inline bool fill_params(const pf_raster_inputs* in, RasterParams& P, bool need_f
     P.seg = (float4*)in->segments;
     P.seg_mask = in->segment_masks;
     P.seg_pairs = in->segments ? in->segment_pairs : 0;
-    P.seg_plane = in->segments ? (float4*)in->segment_planes : nullptr;
-    if (in->segment_planes && ((uintptr_t)in->segment_planes % 16) != 0) {
-        *why = "segment_planes must be 16-byte aligned";
-        return false;
-    }
+    P.seg_stride = in->segment_planes ? 4 : 1;
     if (in->segments && (!in->segment_masks || ((uintptr_t)in->segments % 16) != 0 || in->segment_pairs < 0 ||
                          (in->tile_width != 8 && in->tile_width != 16))) {
         *why = "segments need segment_masks, 16-byte alignment, segment_pairs >= 0 and tile width 8 or 16";

@@ -284,7 +284,7 @@ class Rasterizer:
         inp.segments = _lib.ptr(seg)
         inp.segment_masks = _lib.ptr(mask)
         inp.segment_pairs = int(pairs)
-        inp.segment_planes = _lib.ptr(planes)
+        inp.segment_planes = int(planes)
 
     def _inputs(self, camera, spheres, nsig, sites, rgb, height, adjacency, adjacency_offsets, adj_diff, bins,
                 depth_quantiles=None, ray_gt=None, thr=1e-3, attr_half=False, ray_maps=None):
@@ -359,9 +359,8 @@ class Rasterizer:
             per_pair = self.tile_width * self.tile_width
             slots = pairs * per_pair
             if 0 < slots * 16 <= SEGMENT_BYTES:
-                planes = (torch.empty((slots * 3, 4), dtype=torch.float32, device=dev)
-                          if slots * 64 <= SEGMENT_BYTES else None)
-                segs = (torch.empty((slots, 4), dtype=torch.float32, device=dev),
+                planes = slots * 64 <= SEGMENT_BYTES  # 64-byte slots with the plane results, else 16
+                segs = (torch.empty((slots * (4 if planes else 1), 4), dtype=torch.float32, device=dev),
                         torch.empty(slots // 32, dtype=torch.int32, device=dev), pairs, planes)
                 self._set_segments(inp, segs)
         _timed_call("pf_raster_forward", _lib.ctypes.byref(inp), int(bool(return_point_err)), _lib.ptr(color),
@@ -369,7 +368,8 @@ class Rasterizer:
                     _lib.ptr(perr), _lib.ptr(early_stop), _lib.ptr(stats), _lib.stream_ptr())
         if self.collect_stats:
             self.last_stats = dict(bins=bins, early_stop=early_stop, contrib_pairs=stats,
-                                   adjacency_offsets=adjacency_offsets, camera=camera, n_prims=n)
+                                   adjacency_offsets=adjacency_offsets, camera=camera, n_prims=n, segments=segs,
+                                   tile_width=self.tile_width)
 
         if grad_ctx is not None:
             grad_ctx.rasterizer = self
