@@ -269,17 +269,20 @@ def segment_record_bytes(stats, visited, chunk=1 << 18):
     ts = stats["tile_width"] ** 2
     g = ts // 32
     idx = torch.nonzero(visited).flatten()
-    hits = nonempty = 0
+    hits = nonempty = faced = 0
     bit = torch.arange(32, device=mask.device, dtype=torch.int32)
     for c in range(0, idx.numel(), chunk):
         p = idx[c:c + chunk]
         m = mask.view(pairs, g)[p]                                    # (n, g)
         h = ((m[..., None] >> bit) & 1).bool().reshape(-1, ts)        # (n, ts)
         r = seg.view(pairs, ts, -1)[p]                                # (n, ts, 4 or 16)
+        ne = h & (r[..., 0] < r[..., 1])
         hits += int(h.sum())
-        nonempty += int((h & (r[..., 0] < r[..., 1])).sum())
+        nonempty += int(ne.sum())
+        ids = r[..., 2].contiguous().view(torch.int32)
+        faced += int((ne & (((ids & 0xFFFF) >= 2) | ((ids >> 16) >= 2))).sum())  # a power face bounds it
     b = 4 * idx.numel() * g + 16 * hits + (48 * nonempty if planes else 0)
-    return dict(bytes=b, hit_pixels=hits, nonempty_pixels=nonempty)
+    return dict(bytes=b, hit_pixels=hits, nonempty_pixels=nonempty, face_bounded_pixels=faced)
 
 
 def cpu_model():
