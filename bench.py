@@ -258,31 +258,34 @@ def algorithmic_bytes(stats, H, W):
     return dict(fwd=fwd, bwd=bwd, V=V, U=U, deg=deg, pairs=n_pairs, T=T, records=rec)
 
 
-def segment_record_bytes(stats, visited, chunk=1 << 18):
-    """Bytes of the segment records of the visited pairs: 4 B of hit mask per
-    (pair, warp), 16 B per hit pixel, 48 B of texture-plane result per hit
-    pixel whose clipped interval is not empty (counted from the records)."""
+def segment_record_bytes(stats, visited):
+    """Bytes of the segment records of the visited pairs: 8 B of hit mask and
+    record offset per (pair, warp), 16 B per hit pixel with a record, 48 B of
+    texture-plane result per such pixel whose clipped interval is not empty
+    (counted from the records themselves)."""
     segs = stats.get("segments")
     if segs is None:
         return None
-    seg, mask, pairs, planes = segs
-    ts = stats["tile_width"] ** 2
-    g = ts // 32
-    idx = torch.nonzero(visited).flatten()
-    hits = nonempty = faced = 0
-    bit = torch.arange(32, device=mask.device, dtype=torch.int32)
-    for c in range(0, idx.numel(), chunk):
-        p = idx[c:c + chunk]
-        m = mask.view(pairs, g)[p]                                    # (n, g)
-        h = ((m[..., None] >> bit) & 1).bool().reshape(-1, ts)        # (n, ts)
-        r = seg.view(pairs, ts, -1)[p]                                # (n, ts, 4 or 16)
-        ne = h & (r[..., 0] < r[..., 1])
-        hits += int(h.sum())
-        nonempty += int(ne.sum())
-        ids = r[..., 2].contiguous().view(torch.int32)
-        faced += int((ne & (((ids & 0xFFFF) >= 2) | ((ids >> 16) >= 2))).sum())  # a power face bounds it
-    b = 4 * idx.numel() * g + 16 * hits + (48 * nonempty if planes else 0)
-    return dict(bytes=b, hit_pixels=hits, nonempty_pixels=nonempty, face_bounded_pixels=faced)
+    seg, mask, offs, count, pairs, cap, planes = segs
+    g = stats["tile_width"] ** 2 // 32
+    vis = torch.nonzero(visited).flatten()
+    m = mask.view(pairs, g)[vis].flatten().long() & 0xFFFFFFFF
+    o = offs.view(pairs, g)[vis].flatten().long()
+    bit = torch.arange(32, device=m.device)
+    cnt = ((m[:, None] >> bit) & 1).sum(-1)
+    ok = o >= 0
+    cnt, o = cnt[ok], o[ok]
+    n = int(cnt.sum())
+    start = torch.cumsum(cnt, 0) - cnt
+    idx = torch.repeat_interleave(o, cnt) + (torch.arange(n, device=m.device) - torch.repeat_interleave(start, cnt))
+    r = seg.view(cap, -1)[idx, :3]
+    ne = r[:, 0] < r[:, 1]
+    ids = r[:, 2].contiguous().view(torch.int32)
+    faced = int((ne & (((ids & 0xFFFF) >= 2) | ((ids >> 16) >= 2))).sum())  # a power face bounds it
+    nonempty = int(ne.sum())
+    b = 8 * vis.numel() * g + 16 * n + (48 * nonempty if planes else 0)
+    return dict(bytes=b, hit_pixels=n, nonempty_pixels=nonempty, face_bounded_pixels=faced, capacity=cap,
+                reserved=int(count.item()), clipped_again_pairs=int((~ok).sum()))
 
 
 def cpu_model():

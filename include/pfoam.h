@@ -90,26 +90,33 @@ typedef struct pf_raster_inputs {
                                     backward, or NULL for the pinhole rays;
                                     the benchmark and viewer paths are
                                     pinhole only, as in the reference */
-    float *segments;             /* optional segment records of the hit
-                                    (primitive, pixel) pairs, one slot per
-                                    pixel of every pair in tile_prims (slot =
-                                    pair x tw^2 + the pixel's place in its
-                                    tile): a float4 with the sphere interval
-                                    clipped by the power faces and the ids of
-                                    the surfaces bounding it, then, with
-                                    segment_planes, three float4 of the
-                                    texture-plane result (64 bytes per slot).
-                                    pf_raster_forward writes them (tile widths
-                                    8 and 16) and pf_raster_backward reads
-                                    them instead of clipping and evaluating
-                                    the plane again; NULL: none.  16-byte
-                                    aligned */
+    float *segments;             /* optional segment records, one per hit
+                                    (primitive, pixel) pair: a float4 with the
+                                    sphere interval clipped by the power faces
+                                    and the ids of the surfaces bounding it,
+                                    then, with segment_planes, three float4 of
+                                    the texture-plane result (64 bytes a
+                                    record, else 16).  pf_raster_forward
+                                    (tile widths 8 and 16) reserves the
+                                    records of each warp's hits per 32
+                                    primitives and writes them;
+                                    pf_raster_backward reads them instead of
+                                    clipping and evaluating the plane again.
+                                    NULL: none.  16-byte aligned */
     uint32_t *segment_masks;     /* (pairs x tw^2 / 32) per pair and warp of
                                     32 pixels, the pixels whose ray hits the
-                                    sphere; required with segments */
-    int64_t segment_pairs;       /* pairs the arrays hold (>= the pairs in
-                                    tile_prims) */
-    int32_t segment_planes;      /* 1: the slots hold the plane results */
+                                    sphere */
+    int32_t *segment_offsets;    /* (pairs x tw^2 / 32) per pair and warp,
+                                    the index of its first record (the hits
+                                    follow in pixel order), -1 when the
+                                    buffer was full: the adjoint then clips
+                                    again for that pair */
+    int64_t *segment_count;      /* device counter of the records reserved;
+                                    zero before the forward */
+    int64_t segment_pairs;       /* pairs the mask and offset arrays hold
+                                    (>= the pairs in tile_prims) */
+    int64_t segment_capacity;    /* records the buffer holds (< 2^31) */
+    int32_t segment_planes;      /* 1: the records hold the plane results */
 } pf_raster_inputs;
 
 /* ---------------------------------------------------------------------- */

@@ -69,7 +69,10 @@ class PfRasterInputs(ctypes.Structure):
         ("ray_maps", c_vp),
         ("segments", c_vp),
         ("segment_masks", c_vp),
+        ("segment_offsets", c_vp),
+        ("segment_count", c_vp),
         ("segment_pairs", c_i64),
+        ("segment_capacity", c_i64),
         ("segment_planes", c_i32),
     ]
 

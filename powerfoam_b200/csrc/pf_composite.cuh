@@ -392,6 +392,7 @@ struct FwdCStage {
     float rec_tn[64];   // per pair: segment start (quantile depths)
     float4 dir[32];     // ray direction of each lane's pixel
     uint32_t mask[32];  // hit mask of each staged primitive
+    int32_t off[32];    // its first segment record (REC), -1: none
     int pair_off[33];
     int face_off[33];
 };
@@ -491,12 +492,31 @@ PF_D void fwd_tile_c(const RasterParams& P, const FwdOut& out, int64_t tile, int
             const bool hit = a.g.oob ? false : ray_sphere(ray_org<GEN>(a, o), a.g.d, mk(s4.x, s4.y, s4.z), s4.w, tn, tf);
             const uint32_t m = __ballot_sync(0xffffffffu, hit);
             if (lane == 0) cs.mask[kk] = m;
-            if (REC && lane == 0) {
-                const int64_t pi = start + k0 + kk;
-                if (pi < P.seg_pairs) P.seg_mask[pi * G + wig] = m;
-            }
         }
         __syncwarp();
+        if (REC) {
+            // one reservation per 32 primitives: the warp's hit pixels of primitive kk get the
+            // records off[kk] + (their rank among its hit pixels)
+            const int hits = lane < kn ? __popc(cs.mask[lane]) : 0;
+            const int incl = warp_incl_scan(hits, lane);
+            const int all = __shfl_sync(0xffffffffu, incl, 31);
+            long long base = -1;
+            if (lane == 0 && all > 0) {
+                const unsigned long long b = atomicAdd(P.seg_count, (unsigned long long)all);
+                base = (b + (unsigned long long)all <= (unsigned long long)P.seg_cap) ? (long long)b : -1;
+            }
+            base = __shfl_sync(0xffffffffu, base, 0);
+            if (lane < kn) {
+                const int32_t off = base >= 0 ? (int32_t)(base + incl - hits) : -1;
+                cs.off[lane] = off;
+                const int64_t pi = start + k0 + lane;
+                if (pi < P.seg_pairs) {
+                    P.seg_mask[pi * G + wig] = cs.mask[lane];
+                    P.seg_off[pi * G + wig] = off;
+                }
+            }
+            __syncwarp();
+        }
         int kb = 0;
         while (kb < kn && !stopped) {
             // sub-batch [kb, kb + nsub): primitives whose faces fit the staging area
@@ -596,21 +616,16 @@ PF_D void fwd_tile_c(const RasterParams& P, const FwdOut& out, int64_t tile, int
                             }
                         }
                     }
-                    if (REC) {
-                        const int64_t pi = start + k0 + kk;
-                        if (pi < P.seg_pairs)
-                            P.seg[(pi * (32 * G) + wig * 32 + p) * P.seg_stride] =
-                                make_float4(tn, tf, pack_seg_ids(tn_id, tf_id), 0.f);
+                    int64_t rec = -1;  // REC: this pair's record
+                    if (REC && cs.off[kk] >= 0) {
+                        rec = (int64_t)cs.off[kk] + __popc(cs.mask[kk] & ((1u << p) - 1u));
+                        P.seg[rec * P.seg_stride] = make_float4(tn, tf, pack_seg_ids(tn_id, tf_id), 0.f);
                     }
                     if (tn < tf) {  // else the plane, which only shrinks [tn, tf], leaves dt <= 0 (or NaN)
                         const float4 n4 = cs.nsg[kk];
                         const PlaneRes pr = plane_fwd_tex(po, d, tn, center, mk(n4.x, n4.y, n4.z), radius,
                                                           global_texels(P, prim), P.S);
-                        if (REC && P.seg_stride == 4) {
-                            const int64_t pi = start + k0 + kk;
-                            if (pi < P.seg_pairs)
-                                store_plane(P.seg + (pi * (32 * G) + wig * 32 + p) * 4, pr);
-                        }
+                        if (REC && P.seg_stride == 4 && rec >= 0) store_plane(P.seg + rec * 4, pr);
                         const float tf2 = pr.dp >= 0.0f ? fmin_t(pr.t_surf, tf) : tf;
                         const float tn2 = pr.dp < 0.0f ? fmax_t(pr.t_surf, tn) : tn;
                         cs.rec[j & 63] = make_float4(tf2 - tn2, pr.rgb.x, pr.rgb.y, pr.rgb.z);
@@ -968,16 +983,29 @@ PF_D void bwd_tile(const RasterParams& P, const BwdIn& in, const GradOut& go, in
             const float4 s4 = ws.sph[kk];
             const v3 center = mk(s4.x, s4.y, s4.z);
             const float radius = s4.w;
+            int64_t rec = -1;  // REC: this lane's record
+            bool clip = !REC;  // warp-uniform: clip and evaluate the plane here
             if constexpr (REC) {
                 const int64_t pi = start + k;
-                const uint32_t m = pi < P.seg_pairs ? __ldg(&P.seg_mask[pi * G + wig]) : 0u;
+                uint32_t m = 0u;
+                int32_t off = -1;
+                if (pi < P.seg_pairs) {
+                    m = __ldg(&P.seg_mask[pi * G + wig]);
+                    off = __ldg(&P.seg_off[pi * G + wig]);
+                }
                 if (m == 0u) continue;  // no output changes (see forward)
-                a.hit = (m >> lane) & 1u;
-                if (a.hit) {
-                    const float4 r = __ldg(&P.seg[(pi * (32 * G) + wig * 32 + lane) * P.seg_stride]);
-                    a.tn = r.x;
-                    a.tf = r.y;
-                    unpack_seg_ids(r.z, a.tn_id, a.tf_id);
+                if (off >= 0) {
+                    a.hit = (m >> lane) & 1u;
+                    if (a.hit) {
+                        rec = (int64_t)off + __popc(m & ((1u << lane) - 1u));
+                        const float4 r = __ldg(&P.seg[rec * P.seg_stride]);
+                        a.tn = r.x;
+                        a.tf = r.y;
+                        unpack_seg_ids(r.z, a.tn_id, a.tf_id);
+                    }
+                } else {  // the forward found the record buffer full: as without records
+                    clip = true;
+                    a.hit = a.g.oob ? false : ray_sphere(ray_org<GEN>(a, o), a.g.d, center, radius, a.tn, a.tf);
                 }
             } else {
                 a.hit = a.g.oob ? false : ray_sphere(ray_org<GEN>(a, o), a.g.d, center, radius, a.tn, a.tf);
@@ -992,7 +1020,7 @@ PF_D void bwd_tile(const RasterParams& P, const BwdIn& in, const GradOut& go, in
             const int32_t a0 = __ldg(&P.adj_off[prim]);
             const int n_adj = __ldg(&P.adj_off[prim + 1]) - a0;
             const float cc = dot(center, center), rr = radius * radius;
-            if constexpr (!REC) {
+            if (clip) {
             a.tn_id = a.tn < 1e-8f ? -2 : -1;
             a.tf_id = a.tf < 1e-8f ? -2 : -1;
             b.tn_id = b.tn < 1e-8f ? -2 : -1;
@@ -1030,7 +1058,7 @@ PF_D void bwd_tile(const RasterParams& P, const BwdIn& in, const GradOut& go, in
                 }
                 __syncwarp();
             }
-            }  // !REC
+            }  // clip
             // The texture plane only shrinks [tn, tf] (and a NaN end never
             // gives dt > 0), so a lane whose faces left tn >= tf adds nothing:
             // with no such lane left the primitive is done (28 % of the hit
@@ -1059,8 +1087,8 @@ PF_D void bwd_tile(const RasterParams& P, const BwdIn& in, const GradOut& go, in
                     const int _t_near_id = t_near_id, _t_far_id = t_far_id;
                     const v3 xo = ray_org<GEN>(x, o);
                     PlaneRes pr;
-                    if constexpr (REC == 2)
-                        pr = load_plane(P.seg + ((start + k) * (32 * G) + wig * 32 + lane) * 4);
+                    if (REC == 2 && !clip)
+                        pr = load_plane(P.seg + rec * 4);
                     else
                         pr = plane_fwd_smem(xo, d, t_near, center, pn, radius, ws, P.S);
                     t_far_id = (pr.dp >= 0.0f && pr.t_surf < t_far) ? n_adj : t_far_id;

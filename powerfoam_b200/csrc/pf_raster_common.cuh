@@ -28,13 +28,16 @@ struct RasterParams {
     const int32_t* tile_order;  // processing order of the tiles (NULL: 0..T-1)
     int* queue;                 // work-queue counter (NULL: one group per tile)
     const float* ray_maps;      // (H,W,6) per-pixel origin, direction (generic camera) or NULL
-    float4* seg;                // segment records, seg_stride float4 per slot (pairs x TW^2), or NULL
+    float4* seg;                // segment records, seg_stride float4 each, or NULL
     uint32_t* seg_mask;         // hit masks (pairs x TW^2 / 32)
-    int64_t seg_pairs;          // pairs the arrays hold
-    int seg_stride;             // 4: the slots hold the plane results (float4 1..3), 1: intervals only
+    int32_t* seg_off;           // first record of each (pair, warp), -1: none (pairs x TW^2 / 32)
+    unsigned long long* seg_count;  // records reserved
+    int64_t seg_pairs;          // pairs the mask and offset arrays hold
+    int64_t seg_cap;            // records the buffer holds
+    int seg_stride;             // 4: the records hold the plane results (float4 1..3), 1: intervals only
 };
 
-// texture-plane result in float4 1..3 of a 64-byte slot (the interval is
+// texture-plane result in float4 1..3 of a 64-byte record (the interval is
 // float4 0): a pixel with a non-empty interval moves two whole 32-byte
 // sectors, one with an empty interval the first only
 PF_D void store_plane(float4* slot, const PlaneRes& r) {
@@ -298,11 +301,17 @@ inline bool fill_params(const pf_raster_inputs* in, RasterParams& P, bool need_f
     P.tile_order = in->tile_order;
     P.seg = (float4*)in->segments;
     P.seg_mask = in->segment_masks;
+    P.seg_off = in->segment_offsets;
+    P.seg_count = (unsigned long long*)in->segment_count;
     P.seg_pairs = in->segments ? in->segment_pairs : 0;
+    P.seg_cap = in->segments ? in->segment_capacity : 0;
     P.seg_stride = in->segment_planes ? 4 : 1;
-    if (in->segments && (!in->segment_masks || ((uintptr_t)in->segments % 16) != 0 || in->segment_pairs < 0 ||
+    if (in->segments && (!in->segment_masks || !in->segment_offsets || !in->segment_count ||
+                         ((uintptr_t)in->segments % 16) != 0 || in->segment_pairs < 0 ||
+                         in->segment_capacity < 0 || in->segment_capacity >= ((int64_t)1 << 31) ||
                          (in->tile_width != 8 && in->tile_width != 16))) {
-        *why = "segments need segment_masks, 16-byte alignment, segment_pairs >= 0 and tile width 8 or 16";
+        *why = "segments need segment_masks, segment_offsets, segment_count, 16-byte alignment, "
+               "0 <= segment_capacity < 2^31 and tile width 8 or 16";
         return false;
     }
     P.queue = (int*)in->scratch;

@@ -28,8 +28,8 @@ from . import _lib
 TILE_WIDTH = 8
 TILE_SIZE = TILE_WIDTH * TILE_WIDTH
 # device bytes the forward may use for the adjoint's segment records (64 per
-# pixel of every listed pair with the texture-plane results, 16 without);
-# larger problems keep the intervals only, or clip again in the adjoint
+# hit pixel with the texture-plane results, 16 without); larger buffers keep
+# the intervals only, or none (the adjoint then clips again)
 SEGMENT_BYTES = 24 << 30
 
 # Optional instrumentation: when set, called as hook(name, "begin" | "end")
@@ -216,21 +216,50 @@ class Rasterizer:
         self.grad_buffer = None
         # tile widths 8 and 16: when gradients are wanted, the forward writes
         # each hit (primitive, pixel) pair's clipped sphere interval and
-        # bounding-surface ids, and its texture-plane result (64 bytes per
-        # pixel of every listed pair, up to SEGMENT_BYTES), which the adjoint
-        # reads instead of clipping and evaluating the plane again
+        # bounding-surface ids, and its texture-plane result (a 64-byte
+        # record; up to SEGMENT_BYTES), which the adjoint reads instead of
+        # clipping and evaluating the plane again.  The record buffer is sized
+        # from the last count read back (host_sync: every call; sync-free: the
+        # first call and check()); pairs beyond a full buffer are clipped
+        # again in the adjoint.
         self.record_segments = True
+        self.rec_capacity = 0
+        self.rec_count = torch.zeros(1, dtype=torch.int64, device=self.device)
         _lib.load()
 
     def check(self):
         """Raise PfError if a sync-free call reported overflow or non-finite
         attributes since the last check (one host read); clears the word."""
-        st = int(self.status.item())
+        st, n_rec = (int(v) for v in torch.stack([self.status[0].long(), self.rec_count[0]]).tolist())
+        self._grow_records(n_rec)
         if st != _lib.PF_OK:
             self.status.zero_()
             raise _lib.PfError(st, "a sync-free rasterizer call overflowed its pair buffer (re-run it: the "
                                    "capacity is re-sized) or met a non-finite attribute")
         return True
+
+    def _grow_records(self, n_rec):
+        if n_rec > self.rec_capacity:
+            self.rec_capacity = min(Binner._round(n_rec * 1.25), (1 << 31) - (1 << 16))
+
+    def _segment_buffers(self, pairs):
+        """Record buffer, hit masks, offsets and counter for a forward over
+        `pairs` listed pairs, or None when the budget holds none."""
+        per_pair = self.tile_width * self.tile_width
+        if self.host_sync and self.rec_capacity > 0:
+            self._grow_records(int(self.rec_count.item()))  # the previous call's count
+        if self.rec_capacity == 0:  # first call: a quarter of the listed pixels
+            self.rec_capacity = min(Binner._round(max(pairs * per_pair // 4, 1)), (1 << 31) - (1 << 16))
+        cap = self.rec_capacity
+        planes = cap * 64 <= SEGMENT_BYTES
+        if pairs <= 0 or (not planes and cap * 16 > SEGMENT_BYTES):
+            return None
+        dev = self.device
+        self.rec_count.zero_()
+        return (torch.empty((cap * (4 if planes else 1), 4), dtype=torch.float32, device=dev),
+                torch.empty(pairs * per_pair // 32, dtype=torch.int32, device=dev),
+                torch.empty(pairs * per_pair // 32, dtype=torch.int32, device=dev), self.rec_count, pairs, cap,
+                planes)
 
     def _call_status(self):
         return torch.zeros(1, dtype=torch.int32, device=self.device) if self.host_sync else self.status
@@ -280,10 +309,13 @@ class Rasterizer:
 
     @staticmethod
     def _set_segments(inp, segs):
-        seg, mask, pairs, planes = segs
+        seg, mask, offs, count, pairs, cap, planes = segs
         inp.segments = _lib.ptr(seg)
         inp.segment_masks = _lib.ptr(mask)
+        inp.segment_offsets = _lib.ptr(offs)
+        inp.segment_count = _lib.ptr(count)
         inp.segment_pairs = int(pairs)
+        inp.segment_capacity = int(cap)
         inp.segment_planes = int(planes)
 
     def _inputs(self, camera, spheres, nsig, sites, rgb, height, adjacency, adjacency_offsets, adj_diff, bins,
@@ -355,13 +387,8 @@ class Rasterizer:
         segs = None
         if (grad_ctx is not None and self.record_segments and self.tile_width in (8, 16)
                 and any(grad_ctx.needs_input_grad[3:10])):
-            pairs = bins.tile_prims.numel()  # the pair buffer's capacity (sync-free) or count
-            per_pair = self.tile_width * self.tile_width
-            slots = pairs * per_pair
-            if 0 < slots * 16 <= SEGMENT_BYTES:
-                planes = slots * 64 <= SEGMENT_BYTES  # 64-byte slots with the plane results, else 16
-                segs = (torch.empty((slots * (4 if planes else 1), 4), dtype=torch.float32, device=dev),
-                        torch.empty(slots // 32, dtype=torch.int32, device=dev), pairs, planes)
+            segs = self._segment_buffers(bins.tile_prims.numel())  # the pair buffer's capacity or count
+            if segs is not None:
                 self._set_segments(inp, segs)
         _timed_call("pf_raster_forward", _lib.ctypes.byref(inp), int(bool(return_point_err)), _lib.ptr(color),
                     _lib.ptr(log_t), _lib.ptr(nd), _lib.ptr(normal), _lib.ptr(qd), _lib.ptr(err), _lib.ptr(contrib),

@@ -438,8 +438,9 @@ def test_segment_records_give_the_clipping_adjoint(tw):
     """The adjoint that reads the forward's segment records (sphere interval
     after the power faces, bounding ids, texture-plane results) against the
     one that clips and evaluates the plane again: the same images, and
-    gradients equal up to the order of the float atomics; record budgets
-    that hold the intervals only, or nothing, give the same."""
+    gradients equal up to the order of the float atomics; so do budgets that
+    hold the intervals only or nothing, and a record buffer too small for
+    most primitives (those are clipped again in the adjoint)."""
     import powerfoam_b200.rasterize as rz
 
     sc = np_scene(63, 900, -0.6, 0.6, 0.03, 0.15)
@@ -450,11 +451,15 @@ def test_segment_records_give_the_clipping_adjoint(tw):
     probe = Rasterizer(Args(), "cuda", tile_width=tw)
     probe.collect_stats = True
     _render_grads(probe, cam, _params(sc), adj, adj_off, w)
-    slots = probe.last_stats["bins"].tile_prims.numel() * tw * tw
+    cap = probe.rec_capacity
+    n_rec = int(probe.rec_count.item())
+    assert 0 < n_rec <= cap
     res = []
-    for rec, budget in ((True, rz.SEGMENT_BYTES), (False, rz.SEGMENT_BYTES), (True, 32 * slots), (True, 8 * slots)):
+    for rec, budget, capacity in ((True, rz.SEGMENT_BYTES, 0), (False, rz.SEGMENT_BYTES, 0), (True, 32 * cap, 0),
+                                  (True, 8 * cap, 0), (True, rz.SEGMENT_BYTES, n_rec // 8)):
         R = Rasterizer(Args(), "cuda", tile_width=tw)
         R.record_segments = rec
+        R.rec_capacity = capacity
         old, rz.SEGMENT_BYTES = rz.SEGMENT_BYTES, budget
         try:
             res.append(_render_grads(R, cam, _params(sc), adj, adj_off, w))
