@@ -1237,8 +1237,9 @@ def main():
                               issue=issue_roofline(dominant, args.workload, recs, dom_ms, (clk or {}).get("sm_mhz")),
                               segment_records=st["records"]),
                 gpu_launches=None)
-    # kernels per step: pack 1, binning with tile order, prefetch 1, SH 1, forward 1, backward 1 + 1 sanitise
-    line["gpu_launches"] = args.steps * (1 + bin_launches(st["T"]) + 1 + 1 + 1 + 1 + 1)
+    # kernels per step: pack 1, binning with tile order, prefetch 1, SH 1, forward 1, backward 1 + 1 sanitise;
+    # with segment records the backward is two launches (the one that does not apply returns at once)
+    line["gpu_launches"] = args.steps * (1 + bin_launches(st["T"]) + 1 + 1 + 1 + 1 + 1 + (1 if recs else 0))
     if fisheye:  # the cone hierarchy: one leaf launch and one per merged level
         dh, dw, levels = (cfg["height"] + 1) // 2, (cfg["width"] + 1) // 2, 1
         while dh > 1 or dw > 1:

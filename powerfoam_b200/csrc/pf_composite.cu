@@ -67,9 +67,15 @@ constexpr size_t fwd_dyn_bytes() {
 }
 
 
-template <int TW, bool GEN = false, int REC = 0>
+// REC > 0: launched twice, without and with FB; the launch that does not fit
+// the forward's record count (all hits recorded, or some not) returns at once
+template <int TW, bool GEN = false, int REC = 0, bool FB = true>
 __global__ void __launch_bounds__(Layout<TW>::THREADS, Layout<TW>::BWD_MIN_BLOCKS)
 raster_bwd_kernel(RasterParams P, BwdIn in, GradOut go) {
+    if constexpr (REC > 0) {
+        const bool full = *(volatile unsigned long long*)P.seg_count > (unsigned long long)P.seg_cap;
+        if (full != FB) return;
+    }
     constexpr int G = Layout<TW>::G;
     __shared__ WarpStage stage[G];
     extern __shared__ float4 dyn_smem[];
@@ -82,7 +88,7 @@ raster_bwd_kernel(RasterParams P, BwdIn in, GradOut go) {
     for (;;) {
         int64_t tile = next_tile<G>(P, static_next, lane, nullptr);
         if (tile < 0) break;
-        bwd_tile<G, Layout<TW>::PPL, GEN, REC>(P, in, go, tile, warp, lane, stage[warp], bs);
+        bwd_tile<G, Layout<TW>::PPL, GEN, REC, FB>(P, in, go, tile, warp, lane, stage[warp], bs);
     }
 }
 
@@ -193,23 +199,32 @@ extern "C" int pf_raster_forward(const pf_raster_inputs* in, int32_t return_poin
     return pf_check_launch("pf_raster_forward");
 }
 
-template <int TW, bool GEN, int REC>
+template <int TW, bool GEN, int REC, bool FB = true>
 static void launch_bwd_t(const RasterParams& P, const BwdIn& bi, const GradOut& go, cudaStream_t st) {
     const size_t dyn = sizeof(BwdStage) * Layout<TW>::G;
-    cudaFuncSetAttribute(raster_bwd_kernel<TW, GEN, REC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
-    unsigned grid = composite_grid<TW>(P, raster_bwd_kernel<TW, GEN, REC>, dyn);
-    raster_bwd_kernel<TW, GEN, REC><<<grid, Layout<TW>::THREADS, dyn, st>>>(P, bi, go);
+    cudaFuncSetAttribute(raster_bwd_kernel<TW, GEN, REC, FB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
+    unsigned grid = composite_grid<TW>(P, raster_bwd_kernel<TW, GEN, REC, FB>, dyn);
+    raster_bwd_kernel<TW, GEN, REC, FB><<<grid, Layout<TW>::THREADS, dyn, st>>>(P, bi, go);
+}
+
+// with records: the launch for a forward that recorded every hit, then the one
+// for a forward that found the buffer full (each returns at once when the
+// other applies)
+template <int TW, bool GEN, int REC>
+static void launch_bwd_rec(const RasterParams& P, const BwdIn& bi, const GradOut& go, cudaStream_t st) {
+    launch_bwd_t<TW, GEN, REC, false>(P, bi, go, st);
+    launch_bwd_t<TW, GEN, REC, true>(P, bi, go, st);
 }
 
 template <int TW, bool GEN>
 static void launch_bwd_g(const RasterParams& P, const BwdIn& bi, const GradOut& go, cudaStream_t st) {
     if constexpr (Layout<TW>::PPL == 1) {
         if (P.seg && P.seg_stride == 4) {
-            launch_bwd_t<TW, GEN, 2>(P, bi, go, st);
+            launch_bwd_rec<TW, GEN, 2>(P, bi, go, st);
             return;
         }
         if (P.seg) {
-            launch_bwd_t<TW, GEN, 1>(P, bi, go, st);
+            launch_bwd_rec<TW, GEN, 1>(P, bi, go, st);
             return;
         }
     }

@@ -934,10 +934,16 @@ struct BwdIn {
 // forward's segment records (P.seg), so the sphere tests and the face
 // clipping are not repeated; REC == 2: the texture-plane results too
 // (P.seg_stride == 4).  One pixel per lane only.
-template <int G, int PPL, bool GEN = false, int REC = 0>
+// FB: some (pair, warp) may have no records (the forward found the buffer
+// full) and is clipped here; without FB every hit has its record, and the
+// masks and record offsets of the 32 staged primitives are staged with them
+// (in the stage's face area, which the clipping alone uses).
+template <int G, int PPL, bool GEN = false, int REC = 0, bool FB = true>
 PF_D void bwd_tile(const RasterParams& P, const BwdIn& in, const GradOut& go, int64_t tile, int wig, int lane,
                    WarpStage& ws, BwdStage& bs) {
     static_assert(!REC || PPL == 1, "segment records are written by the pair-compacted forward");
+    uint32_t* const st_mask = reinterpret_cast<uint32_t*>(ws.face);
+    int32_t* const st_off = reinterpret_cast<int32_t*>(ws.face) + 32;
     const int TS = P.TW * P.TW;
     const v3 o = P.cam.eye;
     const float HW = (float)(P.cam.H * P.cam.W);
@@ -978,6 +984,18 @@ PF_D void bwd_tile(const RasterParams& P, const BwdIn& in, const GradOut& go, in
     for (int k1 = es - 1; k1 >= 0; k1 -= 32) {
         const int k0 = k1 - 31;  // batch [k0, k1]; may start below 0
         stage_prims(ws, P, start, k0, es, lane);
+        if constexpr (REC && !FB) {
+            const int kl = k0 + lane;
+            uint32_t m = 0u;
+            int32_t off = -1;
+            if (kl >= 0 && kl < es && start + kl < P.seg_pairs) {
+                m = __ldg(&P.seg_mask[(start + kl) * G + wig]);
+                off = __ldg(&P.seg_off[(start + kl) * G + wig]);
+            }
+            st_mask[lane] = m;
+            st_off[lane] = off;
+            __syncwarp();
+        }
         for (int k = k1; k >= 0 && k >= k0; k--) {
             const int kk = k - k0;
             const float4 s4 = ws.sph[kk];
@@ -986,15 +1004,20 @@ PF_D void bwd_tile(const RasterParams& P, const BwdIn& in, const GradOut& go, in
             int64_t rec = -1;  // REC: this lane's record
             bool clip = !REC;  // warp-uniform: clip and evaluate the plane here
             if constexpr (REC) {
-                const int64_t pi = start + k;
                 uint32_t m = 0u;
                 int32_t off = -1;
-                if (pi < P.seg_pairs) {
-                    m = __ldg(&P.seg_mask[pi * G + wig]);
-                    off = __ldg(&P.seg_off[pi * G + wig]);
+                if constexpr (FB) {
+                    const int64_t pi = start + k;
+                    if (pi < P.seg_pairs) {
+                        m = __ldg(&P.seg_mask[pi * G + wig]);
+                        off = __ldg(&P.seg_off[pi * G + wig]);
+                    }
+                } else {
+                    m = st_mask[kk];
+                    off = st_off[kk];
                 }
                 if (m == 0u) continue;  // no output changes (see forward)
-                if (off >= 0) {
+                if (!FB || off >= 0) {
                     a.hit = (m >> lane) & 1u;
                     if (a.hit) {
                         rec = (int64_t)off + __popc(m & ((1u << lane) - 1u));
@@ -1003,7 +1026,7 @@ PF_D void bwd_tile(const RasterParams& P, const BwdIn& in, const GradOut& go, in
                         a.tf = r.y;
                         unpack_seg_ids(r.z, a.tn_id, a.tf_id);
                     }
-                } else {  // the forward found the record buffer full: as without records
+                } else if constexpr (FB) {  // the forward found the record buffer full: as without records
                     clip = true;
                     a.hit = a.g.oob ? false : ray_sphere(ray_org<GEN>(a, o), a.g.d, center, radius, a.tn, a.tf);
                 }
