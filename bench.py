@@ -274,6 +274,7 @@ def segment_record_bytes(stats, visited):
     bit = torch.arange(32, device=m.device)
     cnt = ((m[:, None] >> bit) & 1).sum(-1)
     ok = o >= 0
+    clipped = int(((~ok) & (cnt > 0)).sum())  # hit (pair, warp)s the full buffer left without records
     cnt, o = cnt[ok], o[ok]
     n = int(cnt.sum())
     start = torch.cumsum(cnt, 0) - cnt
@@ -285,7 +286,7 @@ def segment_record_bytes(stats, visited):
     nonempty = int(ne.sum())
     b = 8 * vis.numel() * g + 16 * n + (48 * nonempty if planes else 0)
     return dict(bytes=b, hit_pixels=n, nonempty_pixels=nonempty, face_bounded_pixels=faced, capacity=cap,
-                reserved=int(count.item()), clipped_again_pairs=int((~ok).sum()))
+                reserved=int(count.item()), clipped_again_pairs=clipped)
 
 
 def cpu_model():
