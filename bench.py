@@ -63,8 +63,8 @@ def parse():
     p.add_argument("--cpu-slices", type=int, default=4, help="slices (1/16 of a frame each) the CPU baseline times")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-segment-records", action="store_true",
-                   help="raster workloads: the adjoint clips the sphere intervals again instead of reading the "
-                   "forward's segment records (Rasterizer.record_segments = False)")
+                   help="raster and batch workloads: the adjoint clips the sphere intervals again instead of "
+                   "reading the forward's segment records (record_segments = False)")
     p.add_argument("--host-sync", action="store_true",
                    help="raster workloads: Rasterizer(host_sync=True), the reference's host read of the pair count "
                    "per call; by default the step runs sync-free (host_sync=False: the host queues steps ahead "
@@ -86,9 +86,10 @@ def parse():
 CAPTURES = {
     # the adjoint that reads the forward's segment records (the default)
     ("raster1m", "pf_raster_backward", True): dict(
-        traffic=4.56e9 + 261.81e6, warp_instructions=6_874_060_237,
-        source="ncu capture of raster_bwd_kernel<8, 0, 2> (second launch of `python bench.py --steps 2 --warmup 1 "
-               "--no-cpu-baseline`): dram__bytes_read.sum + dram__bytes_write.sum, smsp__inst_executed.sum"),
+        traffic=4.185e9 + 260.91e6, warp_instructions=6_747_949_514,
+        source="ncu capture of raster_bwd_kernel<8, 0, 2, false> (the second step's adjoint, `-k regex:raster_ -s 3 "
+               "-c 6` on `python bench.py --steps 2 --warmup 1 --no-cpu-baseline`): dram__bytes_read.sum + "
+               "dram__bytes_write.sum, smsp__inst_executed.sum"),
     # the adjoint that clips again (--no-segment-records)
     ("raster1m", "pf_raster_backward", False): dict(
         traffic=816.77e6 + 206.06e6, warp_instructions=11_715_679_565,
@@ -438,11 +439,12 @@ def batch_main(args, world, rank, local, dev):
     if args.no_autotune:
         from powerfoam_b200.batch import BatchStep
 
-        step = BatchStep(dev, cams, args.tile, 1, "longest")
+        step = BatchStep(dev, cams, args.tile, 1, "longest", record_segments=not args.no_segment_records)
         step.bind(**kw)
         table = []
     else:
         step, table = autotune(dev, cams, kw, chunks=(1, 4), iters=1, warmup=1,
+                               record_segments=not args.no_segment_records,
                                log=(lambda m: print(m, file=sys.stderr, flush=True)) if rank == 0 else None)
     tune_s = time.perf_counter() - t0
     step.capture()
@@ -462,6 +464,11 @@ def batch_main(args, world, rank, local, dev):
         run()
     barrier()
     step.check()
+    if step.graph is None:  # check() grew the segment record buffer: capture the step again
+        step.capture()
+        for _ in range(max(args.warmup, 3)):
+            run()
+        barrier()
     clocks = ClockSampler(local)
     clocks.start()
     time.sleep(0.3)
@@ -521,6 +528,7 @@ def batch_main(args, world, rank, local, dev):
     del R, params
     alg = 0
     pairs = 0
+    rec_bytes = rec_hits = rec_clipped = 0
     for v, c in enumerate(cams):
         class _B:
             pass
@@ -530,9 +538,21 @@ def batch_main(args, world, rank, local, dev):
         bins.tile_prims = step.tile_prims[v][:n_p]
         bins.n_pairs = n_p
         pairs += n_p
+        segs = None
+        if step.segs is not None:  # the view's slice of the batch's masks and offsets
+            g = step.tile_width ** 2 // 32
+            base, cap_v = sum(step.capacity[:v]), step.capacity[v]
+            sl = slice(base * g, (base + cap_v) * g)
+            segs = (step.segs[0], step.seg_masks[sl], step.seg_offs[sl], step.rec_count, cap_v, step.segs[1],
+                    step.segs[2])
         st = algorithmic_bytes(dict(bins=bins, early_stop=step.early_stop[v], adjacency_offsets=adj_off,
-                                    contrib_pairs=step.tile_contrib_pairs[v], n_prims=cfg["n"]), c.height, c.width)
+                                    contrib_pairs=step.tile_contrib_pairs[v], n_prims=cfg["n"], segments=segs,
+                                    tile_width=step.tile_width), c.height, c.width)
         alg += st["fwd"] + st["bwd"]
+        if st["records"]:
+            rec_bytes += st["records"]["bytes"]
+            rec_hits += st["records"]["hit_pixels"]
+            rec_clipped += st["records"]["clipped_again_pairs"]
     peak, peak_kind = load_peaks()
     achieved = alg / (k_ms * 1e-3) / 1e9
     n_views = len(cams_all)
@@ -541,7 +561,9 @@ def batch_main(args, world, rank, local, dev):
     # pack 1, neighbour encoding 1, SH pre-step V, binning per view, the batch launch (work list: keys 1
     # + three 5-kernel radix passes when ordered by length; the persistent kernel 1; 6 + V sanitise), SH adjoint V
     per_step = 1 + 1 + V + sum(bin_launches(T, with_order=False) for T in step.n_tiles)
-    per_step += 1 + (15 if step.order == "longest" else 0) + (2 if step.split else 1) + 6 + V + V
+    # (split: forward, then the adjoint, which comes as two launches with segment records)
+    per_step += 1 + (15 if step.order == "longest" else 0) + ((3 if step.segs else 2) if step.split else 1)
+    per_step += 6 + V + V
     line = dict(metric="batched multi-view fwd+bwd, views/s", value=n_views * 1000.0 / ms,
                 unit="views/s (32 views per step)", n_gpus=world, steps=args.steps, warmup=max(args.warmup, 3),
                 ms_per_step=ms, higher_is_better=True, scaling="strong", vs_baseline=None, dtype="f32",
@@ -550,6 +572,9 @@ def batch_main(args, world, rank, local, dev):
                             tile=step.tile_width, chunk=step.chunk, order=step.order, split=step.split,
                             autotune_s=tune_s,
                             per_view_calls_ms=sequential_ms,
+                            segment_records=None if step.segs is None else dict(
+                                capacity=step.segs[1], planes=step.segs[2], reserved=int(step.rec_count.item()),
+                                hit_pixels=rec_hits, bytes=rec_bytes, clipped_again_pairs=rec_clipped),
                             autotune=table, graph="one CUDA graph per step",
                             l2="inputs larger than L2 (805 MB of primitive records), no flush",
                             parallelism=f"view-dp{world}"),

@@ -551,6 +551,16 @@ typedef struct pf_batch_scene {
     const int32_t *adjacency_offsets;  /* (N+1) */
     const uint16_t *adjacency_diff;    /* (E,4) pf_adjacency_prefetch encoding */
     float transmittance_threshold;
+    /* optional segment records for the whole batch (tile widths 8 and 16), as
+     * pf_raster_inputs.segments: the forward launch writes them, the adjoint
+     * reads them; the masks and offsets of view v start at its
+     * segment_pair_base (in pairs); the counter is zeroed by the call */
+    float *segments;
+    uint32_t *segment_masks;
+    int32_t *segment_offsets;
+    int64_t *segment_count;
+    int64_t segment_capacity;          /* records (< 2^31) */
+    int32_t segment_planes;            /* 1: records hold the plane results */
 } pf_batch_scene;
 
 typedef struct pf_batch_view {
@@ -568,6 +578,8 @@ typedef struct pf_batch_view {
     int32_t *early_stop;           /* (T) */
     int32_t *tile_contrib_pairs;   /* (T) or NULL */
     float *grad_texel_rgb;         /* (N,S,3); views may share one array (summed) */
+    int64_t segment_pair_base;     /* with segments: the view's first pair in the mask / offset arrays */
+    int64_t segment_pairs;         /* its pairs there (>= the pairs in tile_prims) */
 } pf_batch_view;
 
 /* tile_loss holds one float per tile of every view, the views' tiles

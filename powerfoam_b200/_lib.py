@@ -111,6 +111,12 @@ class PfBatchScene(ctypes.Structure):
         ("adjacency_offsets", c_vp),
         ("adjacency_diff", c_vp),
         ("transmittance_threshold", c_f),
+        ("segments", c_vp),
+        ("segment_masks", c_vp),
+        ("segment_offsets", c_vp),
+        ("segment_count", c_vp),
+        ("segment_capacity", c_i64),
+        ("segment_planes", c_i32),
     ]
 
 
@@ -130,6 +136,8 @@ class PfBatchView(ctypes.Structure):
         ("early_stop", c_vp),
         ("tile_contrib_pairs", c_vp),
         ("grad_texel_rgb", c_vp),
+        ("segment_pair_base", c_i64),
+        ("segment_pairs", c_i64),
     ]
 
 

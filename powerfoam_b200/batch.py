@@ -42,7 +42,7 @@ def _pow2_at_least(n):
 
 class BatchStep:
     def __init__(self, device, cameras, tile_width=8, chunk=1, order="longest", transmittance_threshold=1e-3,
-                 headroom=1.25, split=False, world=1):
+                 headroom=1.25, split=False, world=1, record_segments=True, segment_bytes=None):
         if not 1 <= len(cameras) <= _lib.PF_BATCH_MAX_VIEWS:
             raise ValueError(f"1..{_lib.PF_BATCH_MAX_VIEWS} views per batch")
         if tile_width not in TILE_WIDTHS:
@@ -61,6 +61,16 @@ class BatchStep:
         self.graph = None
         self.bound = False
         self.kernel_events = None  # a list: eager runs append (start, end) events around pf_batch_render
+        # segment records (tile widths 8 and 16), as Rasterizer keeps them: the
+        # forward stores every hit pixel's interval and plane result, the
+        # adjoint reads them instead of clipping again.  One buffer for the
+        # batch, sized by a counting launch at bind() and grown by check();
+        # pairs past a full buffer are clipped again in the adjoint.
+        self.record_segments = bool(record_segments) and tile_width in (8, 16)
+        self.segment_bytes = segment_bytes
+        self.rec_capacity = 0
+        self.segs = None  # (record buffer, capacity in records, plane results stored)
+        self.seg_masks = self.seg_offs = None
         _lib.load()
         tw = tile_width
         self.n_tiles = [(1 + (c.height - 1) // tw) * (1 + (c.width - 1) // tw) for c in self.cameras]
@@ -132,8 +142,10 @@ class BatchStep:
         self.tile_offsets = [e(T + 1, dt=torch.int64) for T in self.n_tiles]
         self.tile_prims = [None] * V
         self.capacity = [0] * V
+        self.rec_count = torch.zeros(1, dtype=torch.int64, device=dev)
         self._size_bins()
         self._build_structs()
+        self._size_records()
         self.bound = True
         self.graph = None
 
@@ -168,9 +180,51 @@ class BatchStep:
         _lib.call("pf_batch_workspace_size", self._views, len(self.cameras), self.tile_width, _lib.ctypes.byref(ws))
         self.batch_ws = torch.empty(max(ws.value, 256), dtype=torch.uint8, device=self.device)
 
+    def _record_budget(self):
+        """segment_bytes when given; else half the device memory still free
+        (a batch of many views needs more records than one frame)."""
+        if self.segment_bytes is not None:
+            return int(self.segment_bytes)
+        free, _ = torch.cuda.mem_get_info(self.device)
+        free += torch.cuda.memory_reserved(self.device) - torch.cuda.memory_allocated(self.device)
+        return free // 2
+
+    def _size_records(self):
+        """Masks and offsets for every view's pair capacity; the record buffer
+        from a counting launch (capacity 0: every reservation is refused and
+        counted), 1.25x the count, 64 bytes a record with the plane results,
+        16 without, none when even that exceeds the budget."""
+        self.segs = None
+        if not self.record_segments:
+            self._build_structs()
+            return
+        from .rasterize import Binner
+
+        dev = self.device
+        n = max(sum(self.capacity) * (self.tile_width * self.tile_width // 32), 1)
+        if self.seg_masks is None or self.seg_masks.numel() != n:
+            self.seg_masks = torch.empty(n, dtype=torch.int32, device=dev)
+            self.seg_offs = torch.empty(n, dtype=torch.int32, device=dev)
+        if self.rec_capacity == 0:
+            self.segs = (torch.empty((1, 4), dtype=torch.float32, device=dev), 0, True)
+            self._build_structs()
+            self._launch()
+            self.rec_capacity = min(Binner._round(max(int(self.rec_count.item()) * 1.25, 1)), (1 << 31) - (1 << 16))
+            self.segs = None
+        cap = self.rec_capacity
+        budget = self._record_budget()
+        planes = cap * 64 <= budget
+        if planes or cap * 16 <= budget:
+            self.segs = (torch.empty((cap * (4 if planes else 1), 4), dtype=torch.float32, device=dev), cap, planes)
+        self._build_structs()
+
     def _fill_views(self):
+        base = 0
         for v, c in enumerate(self.cameras):
             w = self._views[v]
+            w.segment_pair_base = base
+            w.segment_pairs = self.capacity[v]
+            base += self.capacity[v]
             w.cam = self.cams_pf[v]
             w.tile_offsets = _lib.ptr(self.tile_offsets[v])
             w.tile_prims = _lib.ptr(self.tile_prims[v])
@@ -199,6 +253,14 @@ class BatchStep:
         sc.adjacency_offsets = _lib.ptr(self.adjacency_offsets)
         sc.adjacency_diff = _lib.ptr(self.adj_diff)
         sc.transmittance_threshold = self.thr
+        if self.segs is not None:
+            seg, cap, planes = self.segs
+            sc.segments = _lib.ptr(seg)
+            sc.segment_masks = _lib.ptr(self.seg_masks)
+            sc.segment_offsets = _lib.ptr(self.seg_offs)
+            sc.segment_count = _lib.ptr(self.rec_count)
+            sc.segment_capacity = int(cap)
+            sc.segment_planes = int(planes)
         self._scene = sc
 
     # ------------------------------------------------------------------
@@ -308,8 +370,19 @@ class BatchStep:
         self.graph = None
 
     def check(self):
-        """Raise if any device status word reports a problem (host sync)."""
+        """Raise if any device status word reports a problem (host sync).  A
+        segment record count past the buffer grows it (and drops a captured
+        graph: capture() again)."""
         bs = self.bin_scalars.cpu()
+        if self.segs is not None:
+            n_rec = int(self.rec_count.item())
+            if n_rec > self.rec_capacity:
+                from .rasterize import Binner
+
+                self.rec_capacity = min(Binner._round(n_rec * 1.25), (1 << 31) - (1 << 16))
+                self.graph = None  # it holds the old buffer
+                self.segs = None
+                self._size_records()
         for v in range(len(self.cameras)):
             n, st = int(bs[v, 0]), int(bs[v, 1]) & 0xffffffff  # the status is the slot's low int32 word
             if st != _lib.PF_OK:
@@ -340,15 +413,16 @@ def default_cache_path():
                           os.path.join(os.path.expanduser("~"), ".cache", "powerfoam_b200", "autotune.json"))
 
 
-def tune_key(device, cameras, n_prims, n_sites):
-    """Cache key: GPU name, primitive count, sites and the views' resolutions."""
+def tune_key(device, cameras, n_prims, n_sites, record_segments=True):
+    """Cache key: GPU name, primitive count, sites, the views' resolutions
+    and, when the adjoint clips again, a "|clip" suffix."""
     name = torch.cuda.get_device_name(device).replace(" ", "_")
     res = sorted(f"{c.width}x{c.height}" for c in cameras)
     counts = {}
     for r in res:
         counts[r] = counts.get(r, 0) + 1
     views = ",".join(f"{k}*{v}" for k, v in sorted(counts.items()))
-    return f"{name}|N={n_prims}|S={n_sites}|views={views}"
+    return f"{name}|N={n_prims}|S={n_sites}|views={views}" + ("" if record_segments else "|clip")
 
 
 def time_step(step, iters=3, warmup=1):
@@ -368,7 +442,7 @@ def time_step(step, iters=3, warmup=1):
 
 def autotune(device, cameras, bind_kwargs, tile_widths=TILE_WIDTHS, chunks=CHUNKS, orders=("longest", "view"),
              splits=(False, True), iters=3, warmup=1, cache_path=None, use_cache=True, transmittance_threshold=1e-3,
-             log=None, prune=1.3):
+             log=None, prune=1.3, record_segments=True):
     """Sweep tile width x work-queue chunk x item order x fused / split
     schedule and return (best BatchStep bound and ready, table).  Per tile
     width the views are binned at that width and pf_batch_autotune times the
@@ -385,7 +459,7 @@ def autotune(device, cameras, bind_kwargs, tile_widths=TILE_WIDTHS, chunks=CHUNK
     cache_path = cache_path or default_cache_path()
     n = bind_kwargs["points"].shape[0]
     S = bind_kwargs["texel_sites"].shape[1]
-    key = tune_key(device, cameras, n, S)
+    key = tune_key(device, cameras, n, S, record_segments)
     cache = {}
     if os.path.exists(cache_path):
         try:
@@ -396,7 +470,7 @@ def autotune(device, cameras, bind_kwargs, tile_widths=TILE_WIDTHS, chunks=CHUNK
 
     def make(best):
         step = BatchStep(device, cameras, best["tile_width"], best["chunk"], best["order"], transmittance_threshold,
-                         split=best.get("split", False))
+                         split=best.get("split", False), record_segments=record_segments)
         step.bind(**bind_kwargs)
         return step
 
@@ -408,7 +482,8 @@ def autotune(device, cameras, bind_kwargs, tile_widths=TILE_WIDTHS, chunks=CHUNK
     best = None
     for tw in tile_widths:
         t0 = time.perf_counter()
-        step = BatchStep(device, cameras, tw, 1, "longest", transmittance_threshold)
+        step = BatchStep(device, cameras, tw, 1, "longest", transmittance_threshold,
+                         record_segments=record_segments)
         step.bind(**bind_kwargs)
         times, bi = step.tune_schedules(scheds, iters=iters, warmup=warmup)
         rows = [{"tile_width": tw, "chunk": ch, "order": order, "split": split, "render_ms": ms, "step_ms": None}

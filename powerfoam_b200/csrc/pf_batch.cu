@@ -43,6 +43,8 @@ struct BatchView {
     int32_t* early_stop;
     int32_t* tile_contrib_pairs;
     float* g_rgb;
+    int64_t seg_pair_base;  // the view's first (pair) entry in the segment mask / offset arrays
+    int64_t seg_pairs;      // its pairs there
 };
 
 struct BatchParams {
@@ -84,6 +86,12 @@ PF_D void load_view(const BatchParams& B, int v, BatchShared& sh) {
     sh.P.tile_off = V.tile_off;
     sh.P.tile_prims = V.tile_prims;
     sh.P.rgb = V.rgb;
+    if (B.base.seg) {  // the view's slice of the segment masks and offsets
+        const int64_t g = (int64_t)B.base.TW * B.base.TW / 32;
+        sh.P.seg_mask = B.base.seg_mask + V.seg_pair_base * g;
+        sh.P.seg_off = B.base.seg_off + V.seg_pair_base * g;
+        sh.P.seg_pairs = V.seg_pairs;
+    }
     sh.out = FwdOut{V.color, V.log_t, V.nd, V.normal, nullptr, nullptr, V.contrib, nullptr, V.early_stop,
                     V.tile_contrib_pairs, 0, B.status};
     sh.in = BwdIn{V.early_stop, V.log_t, V.g_color, nullptr, nullptr, nullptr, nullptr, nullptr};
@@ -108,9 +116,16 @@ struct BatchKernel {
                                     : (Layout<TW>::PPL == 1 ? sizeof(FwdCStage) : 0);
 };
 
-template <int TW, int PH>
+// REC > 0: the forward writes segment records and the adjoint reads them (as
+// pf_raster_forward / pf_raster_backward); the adjoint-only launch comes in
+// the pair without / with FB, of which the one that does not apply returns
+template <int TW, int PH, int REC = 0, bool FB = true>
 __global__ void __launch_bounds__(Layout<TW>::THREADS, BatchKernel<TW, PH>::MIN_BLOCKS)
 batch_step_kernel(const __grid_constant__ BatchParams B) {
+    if constexpr (REC > 0 && PH == kBwdOnly) {
+        const bool full = *(volatile unsigned long long*)B.base.seg_count > (unsigned long long)B.base.seg_cap;
+        if (full != FB) return;
+    }
     constexpr int G = Layout<TW>::G, PPL = Layout<TW>::PPL;
     constexpr int TS = TW * TW;
     constexpr bool FWD = PH != kBwdOnly, BWD = PH != kFwdOnly;
@@ -148,7 +163,7 @@ batch_step_kernel(const __grid_constant__ BatchParams B) {
                 view = v;
             }
             if constexpr (FWD) {
-                if constexpr (PPL == 1) fwd_tile_c<G>(sh.P, sh.out, tile, warp, lane, fs, ss);
+                if constexpr (PPL == 1) fwd_tile_c<G, false, (REC > 0)>(sh.P, sh.out, tile, warp, lane, fs, ss);
                 else fwd_tile<G, PPL>(sh.P, sh.out, tile, warp, lane, stage[warp], ss);
                 // dL/dcolor of this thread's own pixels (written by it in the forward)
                 float l = 0.f;
@@ -181,7 +196,8 @@ batch_step_kernel(const __grid_constant__ BatchParams B) {
                     for (int r = 0; r < kAccRows; r++) bs.acc[r][lane] = 0.f;  // the forward used this area
                     __syncwarp();
                 }
-                bwd_tile<G, PPL>(sh.P, sh.in, sh.go, tile, warp, lane, stage[warp], bs);
+                bwd_tile<G, PPL, false, (PPL == 1 ? REC : 0), FB, PH == kFused>(sh.P, sh.in, sh.go, tile, warp, lane,
+                                                                                stage[warp], bs);
             }
         }
     }
@@ -234,30 +250,44 @@ inline BatchLayout batch_layout(int64_t n_items) {
     return L;
 }
 
-template <int TW, int PH>
+template <int TW, int PH, int REC = 0, bool FB = true>
 static int launch_phase(const BatchParams& B, cudaStream_t st) {
     const size_t dyn = BatchKernel<TW, PH>::STAGE * Layout<TW>::G;
-    cudaError_t e =
-        cudaFuncSetAttribute(batch_step_kernel<TW, PH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
+    cudaError_t e = cudaFuncSetAttribute(batch_step_kernel<TW, PH, REC, FB>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
     if (e != cudaSuccess) return pf_fail(PF_ERR_CUDA, cudaGetErrorString(e));
     int dev = 0, sms = 148, per_sm = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_step_kernel<TW, PH>, Layout<TW>::THREADS, dyn);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_step_kernel<TW, PH, REC, FB>, Layout<TW>::THREADS,
+                                                  dyn);
     if (per_sm < 1) return pf_fail(PF_ERR_CUDA, "pf_batch_render: kernel does not fit on an SM");
     const int64_t items_per_pop = std::max(B.chunk, 1);
     const int64_t pops = (B.n_items + items_per_pop - 1) / items_per_pop;
     const unsigned grid = (unsigned)std::max<int64_t>(1, std::min<int64_t>((int64_t)sms * per_sm, pops));
-    batch_step_kernel<TW, PH><<<grid, Layout<TW>::THREADS, dyn, st>>>(B);
+    batch_step_kernel<TW, PH, REC, FB><<<grid, Layout<TW>::THREADS, dyn, st>>>(B);
     return PF_OK;
+}
+
+template <int TW, int REC>
+static int launch_batch_rec(const BatchParams& B, bool split, cudaStream_t st) {
+    if (!split) return launch_phase<TW, kFused, REC, true>(B, st);  // a tile's adjoint follows its forward
+    int rc = launch_phase<TW, kFwdOnly, REC>(B, st);
+    if (rc != PF_OK) return rc;
+    if constexpr (REC > 0) {
+        rc = launch_phase<TW, kBwdOnly, REC, false>(B, st);
+        if (rc != PF_OK) return rc;
+    }
+    return launch_phase<TW, kBwdOnly, REC, true>(B, st);
 }
 
 template <int TW>
 static int launch_batch(const BatchParams& B, bool split, cudaStream_t st) {
-    if (!split) return launch_phase<TW, kFused>(B, st);
-    int rc = launch_phase<TW, kFwdOnly>(B, st);
-    if (rc != PF_OK) return rc;
-    return launch_phase<TW, kBwdOnly>(B, st);
+    if constexpr (Layout<TW>::PPL == 1) {
+        if (B.base.seg && B.base.seg_stride == 4) return launch_batch_rec<TW, 2>(B, split, st);
+        if (B.base.seg) return launch_batch_rec<TW, 1>(B, split, st);
+    }
+    return launch_batch_rec<TW, 0>(B, split, st);
 }
 
 static int batch_params(const pf_batch_scene* sc, const pf_batch_view* views, int32_t n_views, int32_t tile_width,
@@ -297,6 +327,21 @@ static int batch_params(const pf_batch_scene* sc, const pf_batch_view* views, in
     P.thr = sc->transmittance_threshold;
     P.tile_order = nullptr;
     P.queue = nullptr;
+    if (sc->segments) {
+        if ((tile_width != 8 && tile_width != 16) || !sc->segment_masks || !sc->segment_offsets ||
+            !sc->segment_count || ((uintptr_t)sc->segments % 16) != 0 || sc->segment_capacity < 0 ||
+            sc->segment_capacity >= ((int64_t)1 << 31)) {
+            *why = "pf_batch: segments need tile width 8 or 16, masks, offsets, a counter, 16-byte alignment and "
+                   "0 <= segment_capacity < 2^31";
+            return 0;
+        }
+        P.seg = (float4*)sc->segments;
+        P.seg_mask = sc->segment_masks;
+        P.seg_off = sc->segment_offsets;
+        P.seg_count = (unsigned long long*)sc->segment_count;
+        P.seg_cap = sc->segment_capacity;
+        P.seg_stride = sc->segment_planes ? 4 : 1;
+    }
     B.n_views = n_views;
     int64_t base = 0;
     for (int v = 0; v < n_views; v++) {
@@ -335,6 +380,12 @@ static int batch_params(const pf_batch_scene* sc, const pf_batch_view* views, in
         V.early_stop = w.early_stop;
         V.tile_contrib_pairs = w.tile_contrib_pairs;
         V.g_rgb = w.grad_texel_rgb;
+        V.seg_pair_base = w.segment_pair_base;
+        V.seg_pairs = sc->segments ? w.segment_pairs : 0;
+        if (sc->segments && (w.segment_pair_base < 0 || w.segment_pairs < 0)) {
+            *why = "pf_batch: bad segment pair range";
+            return 0;
+        }
     }
     B.n_items = base;
     return 1;
@@ -396,6 +447,7 @@ extern "C" int pf_batch_render(const pf_batch_scene* scene, const pf_batch_view*
     B.status = (int*)status;
     B.tile_loss = tile_loss;
     cudaMemsetAsync(B.queue, 0, 2 * sizeof(int), st);
+    if (B.base.seg) cudaMemsetAsync(B.base.seg_count, 0, sizeof(int64_t), st);
     // work list
     uint32_t* k0 = (uint32_t*)(ws + L.k0);
     uint32_t* v0 = (uint32_t*)(ws + L.v0);

@@ -938,7 +938,9 @@ struct BwdIn {
 // full) and is clipped here; without FB every hit has its record, and the
 // masks and record offsets of the 32 staged primitives are staged with them
 // (in the stage's face area, which the clipping alone uses).
-template <int G, int PPL, bool GEN = false, int REC = 0, bool FB = true>
+// COH: the records were written earlier in the same launch (a fused
+// forward + adjoint), so they are read through L2, not the read-only path.
+template <int G, int PPL, bool GEN = false, int REC = 0, bool FB = true, bool COH = false>
 PF_D void bwd_tile(const RasterParams& P, const BwdIn& in, const GradOut& go, int64_t tile, int wig, int lane,
                    WarpStage& ws, BwdStage& bs) {
     static_assert(!REC || PPL == 1, "segment records are written by the pair-compacted forward");
@@ -989,8 +991,8 @@ PF_D void bwd_tile(const RasterParams& P, const BwdIn& in, const GradOut& go, in
             uint32_t m = 0u;
             int32_t off = -1;
             if (kl >= 0 && kl < es && start + kl < P.seg_pairs) {
-                m = __ldg(&P.seg_mask[(start + kl) * G + wig]);
-                off = __ldg(&P.seg_off[(start + kl) * G + wig]);
+                m = seg_load<COH>(&P.seg_mask[(start + kl) * G + wig]);
+                off = seg_load<COH>(&P.seg_off[(start + kl) * G + wig]);
             }
             st_mask[lane] = m;
             st_off[lane] = off;
@@ -1009,8 +1011,8 @@ PF_D void bwd_tile(const RasterParams& P, const BwdIn& in, const GradOut& go, in
                 if constexpr (FB) {
                     const int64_t pi = start + k;
                     if (pi < P.seg_pairs) {
-                        m = __ldg(&P.seg_mask[pi * G + wig]);
-                        off = __ldg(&P.seg_off[pi * G + wig]);
+                        m = seg_load<COH>(&P.seg_mask[pi * G + wig]);
+                        off = seg_load<COH>(&P.seg_off[pi * G + wig]);
                     }
                 } else {
                     m = st_mask[kk];
@@ -1021,7 +1023,7 @@ PF_D void bwd_tile(const RasterParams& P, const BwdIn& in, const GradOut& go, in
                     a.hit = (m >> lane) & 1u;
                     if (a.hit) {
                         rec = (int64_t)off + __popc(m & ((1u << lane) - 1u));
-                        const float4 r = __ldg(&P.seg[rec * P.seg_stride]);
+                        const float4 r = seg_load<COH>(&P.seg[rec * P.seg_stride]);
                         a.tn = r.x;
                         a.tf = r.y;
                         unpack_seg_ids(r.z, a.tn_id, a.tf_id);
@@ -1111,7 +1113,7 @@ PF_D void bwd_tile(const RasterParams& P, const BwdIn& in, const GradOut& go, in
                     const v3 xo = ray_org<GEN>(x, o);
                     PlaneRes pr;
                     if (REC == 2 && !clip)
-                        pr = load_plane(P.seg + rec * 4);
+                        pr = load_plane<COH>(P.seg + rec * 4);
                     else
                         pr = plane_fwd_smem(xo, d, t_near, center, pn, radius, ws, P.S);
                     t_far_id = (pr.dp >= 0.0f && pr.t_surf < t_far) ? n_adj : t_far_id;

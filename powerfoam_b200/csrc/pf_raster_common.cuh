@@ -45,8 +45,19 @@ PF_D void store_plane(float4* slot, const PlaneRes& r) {
     slot[2] = make_float4(r.wsum, r._wsum, r.t_surf, r.dp);
     slot[3] = make_float4(r._t_surf, r._dp, 0.f, 0.f);
 }
+// Segment-record loads: through the read-only path when the records were
+// written by an earlier launch, through L2 (ld.global.cg) when the forward
+// that wrote them runs in the same launch (the read-only path is only valid
+// for data that no thread writes during the launch).
+template <bool COH, class T>
+PF_D T seg_load(const T* p) {
+    if constexpr (COH) return __ldcg(p);
+    else return __ldg(p);
+}
+
+template <bool COH = false>
 PF_D PlaneRes load_plane(const float4* slot) {
-    const float4 a = __ldg(slot + 1), b = __ldg(slot + 2), c = __ldg(slot + 3);
+    const float4 a = seg_load<COH>(slot + 1), b = seg_load<COH>(slot + 2), c = seg_load<COH>(slot + 3);
     PlaneRes r;
     r.rgb = mk(a.x, a.y, a.z);
     r.height = a.w;

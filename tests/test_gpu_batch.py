@@ -229,3 +229,48 @@ def test_schedule_tuner_through_the_c_abi():
         assert torch.equal(a, b)
     with pytest.raises(ValueError):
         step.tune_schedules([(1, "random", False)])
+
+
+@pytest.mark.parametrize("tw,split", [(8, False), (8, True), (16, False), (16, True)])
+def test_batch_segment_records_give_the_clipping_adjoint(tw, split):
+    """The batch launch with segment records (the forward stores each hit
+    pixel's interval and plane result, the adjoint reads them) against the
+    one that clips again: the same images and losses, gradients equal up to
+    the order of the float atomics; so do a budget that holds the intervals
+    only and a record buffer too small for most pairs (those are clipped
+    again).  check() grows a buffer that a count outran."""
+    sc, adj, adj_off, cams, rgbs, targets = make_case(seed=13)
+    kw = bind_kwargs(sc, adj, adj_off, rgbs, targets)
+    res = []
+    for rec, budget, capacity in ((False, None, 0), (True, None, 0), (True, None, 0.1), (True, "intervals", 0)):
+        step = BatchStep("cuda", [torch_cam(c) for c in cams], tile_width=tw, chunk=2, split=split,
+                         record_segments=rec)
+        step.bind(**kw)
+        if rec:
+            n_rec = int(step.rec_count.item())
+            assert n_rec > 0 and step.segs is not None
+            if budget == "intervals":
+                step.segment_bytes = 16 * step.rec_capacity
+                step._size_records()
+                assert step.segs[2] is False
+        if capacity:  # a buffer for an eighth of the records
+            step.rec_capacity = max(n_rec // 8, 1)
+            step._size_records()
+            assert step.rec_capacity < n_rec
+        loss = step.run().clone()
+        res.append((loss, [c.clone() for c in step.color], {k: g.clone() for k, g in step.grads.items()},
+                    [g.clone() for g in step.grad_texel_rgb]))
+        if rec and capacity:
+            step.check()  # grows the buffer and drops the graph
+            assert step.rec_capacity >= int(step.rec_count.item())
+        else:
+            step.check()
+    loss0, col0, g0, rgb0 = res[0]
+    for loss, col, g, rgb in res[1:]:
+        assert torch.equal(loss, loss0)
+        for a, b in zip(col, col0):
+            assert torch.equal(a, b)
+        for k in g0:
+            assert_close_rel(g[k].cpu().numpy(), g0[k].cpu().numpy(), 1e-5, k)
+        for a, b in zip(rgb, rgb0):
+            assert_close_rel(a.cpu().numpy(), b.cpu().numpy(), 1e-5, "rgb")
