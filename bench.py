@@ -526,44 +526,79 @@ def batch_main(args, world, rank, local, dev):
     torch.cuda.synchronize()
     sequential_ms = s0.elapsed_time(s1)
     del R, params
-    alg = 0
-    pairs = 0
-    rec_bytes = rec_hits = rec_clipped = 0
-    for v, c in enumerate(cams):
+    V = len(cams)
+    n_groups = step.seg_groups[-1] + 1 if step.segs is not None else 1
+    # pack 1, neighbour encoding 1, SH pre-step V, binning per view, the batch launch (work list: keys 1
+    # + three 5-kernel radix passes when ordered by length; per record group the persistent kernel once
+    # fused, or forward + adjoint split, the adjoint as two launches with segment records; 6 + V
+    # sanitise), SH adjoint V
+    per_step = 1 + 1 + V + sum(bin_launches(T, with_order=False) for T in step.n_tiles)
+    per_step += 1 + (15 if step.order == "longest" else 0)
+    per_step += n_groups * ((3 if step.segs else 2) if step.split else 1)
+    per_step += 6 + V + V
+    groups_info = None if step.segs is None else dict(groups=n_groups, capacity=step.segs[1], planes=step.segs[2],
+                                                      view_records=step.view_records)
+    totals = dict(alg=0, pairs=0, rec_bytes=0, rec_hits=0, rec_clipped=0)
+
+    def add_view_bytes(s, v, c):
+        """Algorithmic bytes of view v of BatchStep s (its slice of the masks
+        and offsets; its group's counter)."""
         class _B:
             pass
         bins = _B()
-        bins.tile_offsets = step.tile_offsets[v]
-        n_p = int(step.bin_scalars[v, 0])
-        bins.tile_prims = step.tile_prims[v][:n_p]
+        bins.tile_offsets = s.tile_offsets[v]
+        n_p = int(s.bin_scalars[v, 0])
+        bins.tile_prims = s.tile_prims[v][:n_p]
         bins.n_pairs = n_p
-        pairs += n_p
+        totals["pairs"] += n_p
         segs = None
-        if step.segs is not None:  # the view's slice of the batch's masks and offsets
-            g = step.tile_width ** 2 // 32
-            base, cap_v = sum(step.capacity[:v]), step.capacity[v]
+        if s.segs is not None:
+            g = s.tile_width ** 2 // 32
+            base, cap_v = sum(s.capacity[:v]), s.capacity[v]
             sl = slice(base * g, (base + cap_v) * g)
-            segs = (step.segs[0], step.seg_masks[sl], step.seg_offs[sl], step.rec_count, cap_v, step.segs[1],
-                    step.segs[2])
-        st = algorithmic_bytes(dict(bins=bins, early_stop=step.early_stop[v], adjacency_offsets=adj_off,
-                                    contrib_pairs=step.tile_contrib_pairs[v], n_prims=cfg["n"], segments=segs,
-                                    tile_width=step.tile_width), c.height, c.width)
-        alg += st["fwd"] + st["bwd"]
+            grp = s.seg_groups[v]
+            segs = (s.segs[0], s.seg_masks[sl], s.seg_offs[sl], s.rec_count[grp:grp + 1], cap_v, s.segs[1],
+                    s.segs[2])
+        st = algorithmic_bytes(dict(bins=bins, early_stop=s.early_stop[v], adjacency_offsets=adj_off,
+                                    contrib_pairs=s.tile_contrib_pairs[v], n_prims=cfg["n"], segments=segs,
+                                    tile_width=s.tile_width), c.height, c.width)
+        totals["alg"] += st["fwd"] + st["bwd"]
         if st["records"]:
-            rec_bytes += st["records"]["bytes"]
-            rec_hits += st["records"]["hit_pixels"]
-            rec_clipped += st["records"]["clipped_again_pairs"]
+            totals["rec_bytes"] += st["records"]["bytes"]
+            totals["rec_hits"] += st["records"]["hit_pixels"]
+            totals["rec_clipped"] += st["records"]["clipped_again_pairs"]
+
+    if n_groups == 1:
+        for v, c in enumerate(cams):
+            add_view_bytes(step, v, c)
+    else:
+        # the record buffer holds the last group's records only: each group's are counted on a
+        # step over that group's views (untimed)
+        from powerfoam_b200.batch import BatchStep
+
+        groups = list(step.seg_groups)
+        sched = dict(tile_width=step.tile_width, chunk=step.chunk, order=step.order, split=step.split)
+        step.graph = None
+        step.segs = None
+        step.seg_masks = step.seg_offs = None
+        torch.cuda.empty_cache()
+        for g in range(n_groups):
+            vs = [v for v in range(V) if groups[v] == g]
+            sub = BatchStep(dev, [cams[v] for v in vs], **sched)
+            sub.bind(**dict(kw, targets=[targets[v] for v in vs]))
+            sub.run()
+            torch.cuda.synchronize()
+            groups_info.setdefault("sub_step_groups", []).append(sub.seg_groups[-1] + 1)
+            for i, v in enumerate(vs):
+                add_view_bytes(sub, i, cams[v])
+            del sub
+            torch.cuda.empty_cache()
+    alg, pairs = totals["alg"], totals["pairs"]
+    rec_bytes, rec_hits, rec_clipped = totals["rec_bytes"], totals["rec_hits"], totals["rec_clipped"]
     peak, peak_kind = load_peaks()
     achieved = alg / (k_ms * 1e-3) / 1e9
     n_views = len(cams_all)
     pixels = sum(c.width * c.height for c in cams_all)
-    V = len(cams)
-    # pack 1, neighbour encoding 1, SH pre-step V, binning per view, the batch launch (work list: keys 1
-    # + three 5-kernel radix passes when ordered by length; the persistent kernel 1; 6 + V sanitise), SH adjoint V
-    per_step = 1 + 1 + V + sum(bin_launches(T, with_order=False) for T in step.n_tiles)
-    # (split: forward, then the adjoint, which comes as two launches with segment records)
-    per_step += 1 + (15 if step.order == "longest" else 0) + ((3 if step.segs else 2) if step.split else 1)
-    per_step += 6 + V + V
     line = dict(metric="batched multi-view fwd+bwd, views/s", value=n_views * 1000.0 / ms,
                 unit="views/s (32 views per step)", n_gpus=world, steps=args.steps, warmup=max(args.warmup, 3),
                 ms_per_step=ms, higher_is_better=True, scaling="strong", vs_baseline=None, dtype="f32",
@@ -572,9 +607,8 @@ def batch_main(args, world, rank, local, dev):
                             tile=step.tile_width, chunk=step.chunk, order=step.order, split=step.split,
                             autotune_s=tune_s,
                             per_view_calls_ms=sequential_ms,
-                            segment_records=None if step.segs is None else dict(
-                                capacity=step.segs[1], planes=step.segs[2], reserved=int(step.rec_count.item()),
-                                hit_pixels=rec_hits, bytes=rec_bytes, clipped_again_pairs=rec_clipped),
+                            segment_records=None if groups_info is None else dict(
+                                groups_info, hit_pixels=rec_hits, bytes=rec_bytes, clipped_again_pairs=rec_clipped),
                             autotune=table, graph="one CUDA graph per step",
                             l2="inputs larger than L2 (805 MB of primitive records), no flush",
                             parallelism=f"view-dp{world}"),

@@ -36,7 +36,7 @@ extern "C" {
 #define PF_ERR_CELL 6      /* a power cell exceeded its plane / neighbour capacity */
 #define PF_ERR_NONFINITE 7 /* a primitive attribute is NaN or infinite */
 
-#define PF_ABI_VERSION 3
+#define PF_ABI_VERSION 4
 
 #if defined(__GNUC__)
 #define PF_API __attribute__((visibility("default")))
@@ -551,10 +551,14 @@ typedef struct pf_batch_scene {
     const int32_t *adjacency_offsets;  /* (N+1) */
     const uint16_t *adjacency_diff;    /* (E,4) pf_adjacency_prefetch encoding */
     float transmittance_threshold;
-    /* optional segment records for the whole batch (tile widths 8 and 16), as
+    /* optional segment records (tile widths 8 and 16), as
      * pf_raster_inputs.segments: the forward launch writes them, the adjoint
      * reads them; the masks and offsets of view v start at its
-     * segment_pair_base (in pairs); the counter is zeroed by the call */
+     * segment_pair_base (in pairs).  The views render in record groups
+     * (pf_batch_view.segment_group: 0 for the first view, then the previous
+     * view's group or the next one), one group after the other, each reusing
+     * the record buffer with its own counter: segment_count holds one int64
+     * per group (the last view's group + 1), zeroed by the call */
     float *segments;
     uint32_t *segment_masks;
     int32_t *segment_offsets;
@@ -580,6 +584,7 @@ typedef struct pf_batch_view {
     float *grad_texel_rgb;         /* (N,S,3); views may share one array (summed) */
     int64_t segment_pair_base;     /* with segments: the view's first pair in the mask / offset arrays */
     int64_t segment_pairs;         /* its pairs there (>= the pairs in tile_prims) */
+    int32_t segment_group;         /* with segments: its record group (see pf_batch_scene) */
 } pf_batch_view;
 
 /* tile_loss holds one float per tile of every view, the views' tiles

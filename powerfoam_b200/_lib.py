@@ -138,6 +138,7 @@ class PfBatchView(ctypes.Structure):
         ("grad_texel_rgb", c_vp),
         ("segment_pair_base", c_i64),
         ("segment_pairs", c_i64),
+        ("segment_group", c_i32),
     ]
 
 

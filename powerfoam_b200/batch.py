@@ -71,6 +71,8 @@ class BatchStep:
         self.rec_capacity = 0
         self.segs = None  # (record buffer, capacity in records, plane results stored)
         self.seg_masks = self.seg_offs = None
+        self.seg_groups = [0] * len(self.cameras)  # record group per view (non-decreasing)
+        self.view_records = None  # records per view, from the counting launch
         _lib.load()
         tw = tile_width
         self.n_tiles = [(1 + (c.height - 1) // tw) * (1 + (c.width - 1) // tw) for c in self.cameras]
@@ -142,7 +144,7 @@ class BatchStep:
         self.tile_offsets = [e(T + 1, dt=torch.int64) for T in self.n_tiles]
         self.tile_prims = [None] * V
         self.capacity = [0] * V
-        self.rec_count = torch.zeros(1, dtype=torch.int64, device=dev)
+        self.rec_count = torch.zeros(V, dtype=torch.int64, device=dev)  # one counter per record group
         self._size_bins()
         self._build_structs()
         self._size_records()
@@ -190,27 +192,21 @@ class BatchStep:
         return free // 2
 
     def _size_records(self):
-        """Masks and offsets for every view's pair capacity; the record buffer
-        from a counting launch (capacity 0: every reservation is refused and
-        counted), 1.25x the count, 64 bytes a record with the plane results,
-        16 without, none when even that exceeds the budget."""
+        """Masks and offsets for every view's pair capacity and the record
+        buffer: capacity and record groups from a counting launch when none is
+        set, 64 bytes a record with the plane results, 16 without (intervals
+        only), none when even that exceeds the budget."""
         self.segs = None
         if not self.record_segments:
             self._build_structs()
             return
-        from .rasterize import Binner
-
         dev = self.device
         n = max(sum(self.capacity) * (self.tile_width * self.tile_width // 32), 1)
         if self.seg_masks is None or self.seg_masks.numel() != n:
             self.seg_masks = torch.empty(n, dtype=torch.int32, device=dev)
             self.seg_offs = torch.empty(n, dtype=torch.int32, device=dev)
         if self.rec_capacity == 0:
-            self.segs = (torch.empty((1, 4), dtype=torch.float32, device=dev), 0, True)
-            self._build_structs()
-            self._launch()
-            self.rec_capacity = min(Binner._round(max(int(self.rec_count.item()) * 1.25, 1)), (1 << 31) - (1 << 16))
-            self.segs = None
+            self._count_records()
         cap = self.rec_capacity
         budget = self._record_budget()
         planes = cap * 64 <= budget
@@ -218,12 +214,35 @@ class BatchStep:
             self.segs = (torch.empty((cap * (4 if planes else 1), 4), dtype=torch.float32, device=dev), cap, planes)
         self._build_structs()
 
+    def _count_records(self):
+        """One step with every view in its own record group and capacity 0
+        (every reservation is refused and counted): the records per view, then
+        the groups (record_groups) and the capacity, the largest group."""
+        from .rasterize import Binner
+
+        V = len(self.cameras)
+        self.seg_groups = list(range(V))
+        self.segs = (torch.empty((1, 4), dtype=torch.float32, device=self.device), 0, True)
+        self._build_structs()
+        self._launch()
+        self.view_records = [int(c) for c in self.rec_count[:V].tolist()]
+        self.segs = None
+        need = [max(int(c * self.headroom), 1) for c in self.view_records]
+        budget = self._record_budget()
+        limit = (1 << 31) - (1 << 16)
+        # the largest group that fits, less the rounding of the capacity
+        size = lambda per: min(budget // per, limit) - (1 << 16)
+        per = 64 if max(need) <= size(64) else 16
+        self.seg_groups, sums = record_groups(need, max(size(per), 1))
+        self.rec_capacity = min(Binner._round(max(sums)), limit)
+
     def _fill_views(self):
         base = 0
         for v, c in enumerate(self.cameras):
             w = self._views[v]
             w.segment_pair_base = base
             w.segment_pairs = self.capacity[v]
+            w.segment_group = self.seg_groups[v]
             base += self.capacity[v]
             w.cam = self.cams_pf[v]
             w.tile_offsets = _lib.ptr(self.tile_offsets[v])
@@ -371,17 +390,15 @@ class BatchStep:
 
     def check(self):
         """Raise if any device status word reports a problem (host sync).  A
-        segment record count past the buffer grows it (and drops a captured
-        graph: capture() again)."""
+        record group whose count outran the record buffer makes it count the
+        records again and size the groups and the buffer anew (and drop a
+        captured graph: capture() again)."""
         bs = self.bin_scalars.cpu()
         if self.segs is not None:
-            n_rec = int(self.rec_count.item())
-            if n_rec > self.rec_capacity:
-                from .rasterize import Binner
-
-                self.rec_capacity = min(Binner._round(n_rec * 1.25), (1 << 31) - (1 << 16))
+            n_groups = self.seg_groups[-1] + 1
+            if max(self.rec_count[:n_groups].tolist()) > self.rec_capacity:
                 self.graph = None  # it holds the old buffer
-                self.segs = None
+                self.rec_capacity = 0  # count again, per view
                 self._size_records()
         for v in range(len(self.cameras)):
             n, st = int(bs[v, 0]), int(bs[v, 1]) & 0xffffffff  # the status is the slot's low int32 word
@@ -394,6 +411,20 @@ class BatchStep:
 
     def pair_counts(self):
         return self.bin_scalars[:, 0].tolist()
+
+
+def record_groups(need, size):
+    """Contiguous record groups of the views, in order: a view joins the
+    current group while the group's records stay within `size`, else it
+    starts the next one (a view larger than `size` gets a group of its own).
+    Returns the group of each view and the records of each group."""
+    groups, sums = [], []
+    for n in need:
+        if not sums or (sums[-1] > 0 and sums[-1] + n > size):
+            sums.append(0)
+        groups.append(len(sums) - 1)
+        sums[-1] += n
+    return groups, sums
 
 
 def _check(t, name, dtype):

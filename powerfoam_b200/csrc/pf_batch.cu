@@ -45,6 +45,7 @@ struct BatchView {
     float* g_rgb;
     int64_t seg_pair_base;  // the view's first (pair) entry in the segment mask / offset arrays
     int64_t seg_pairs;      // its pairs there
+    int32_t seg_group;      // the record group it renders in (0 without records)
 };
 
 struct BatchParams {
@@ -211,7 +212,10 @@ __global__ void batch_keys_kernel(const __grid_constant__ BatchParams B, uint32_
     while (v + 1 < B.n_views && B.views[v + 1].item_base <= g) v++;
     const int64_t t = g - B.views[v].item_base;
     const int64_t len = B.views[v].tile_off[t + 1] - B.views[v].tile_off[t];
-    if (keys) keys[g] = 0xffffffu - (uint32_t)std::min<int64_t>(len, 0xffffff);
+    // record group (6 bits) above the list length (18 bits, longer lists tie): group-major,
+    // longest first within a group
+    if (keys)
+        keys[g] = ((uint32_t)B.views[v].seg_group << 18) | (0x3ffffu - (uint32_t)std::min<int64_t>(len, 0x3ffff));
     vals[g] = ((uint32_t)v << 24) | (uint32_t)t;
 }
 
@@ -245,7 +249,7 @@ inline BatchLayout batch_layout(int64_t n_items) {
     const int64_t nb = radix_blocks(std::max<int64_t>(n_items, 1));
     L.rhist = take(sizeof(uint32_t) * (size_t)(256 * nb));
     L.rpart = take(sizeof(uint32_t) * (size_t)(scan_blocks(256 * nb) + 1));
-    L.queue = take(256);
+    L.queue = take(sizeof(int) * 2 * kMaxViews);  // two work counters per record group
     L.bytes = off;
     return L;
 }
@@ -382,8 +386,14 @@ static int batch_params(const pf_batch_scene* sc, const pf_batch_view* views, in
         V.g_rgb = w.grad_texel_rgb;
         V.seg_pair_base = w.segment_pair_base;
         V.seg_pairs = sc->segments ? w.segment_pairs : 0;
+        V.seg_group = sc->segments ? w.segment_group : 0;
         if (sc->segments && (w.segment_pair_base < 0 || w.segment_pairs < 0)) {
             *why = "pf_batch: bad segment pair range";
+            return 0;
+        }
+        const int32_t prev = v > 0 ? views[v - 1].segment_group : 0;
+        if (sc->segments && (w.segment_group < prev || w.segment_group > prev + (v > 0 ? 1 : 0))) {
+            *why = "pf_batch: segment groups must start at 0 and grow by 0 or 1 from one view to the next";
             return 0;
         }
     }
@@ -446,8 +456,12 @@ extern "C" int pf_batch_render(const pf_batch_scene* scene, const pf_batch_view*
     B.queue = (int*)(ws + L.queue);
     B.status = (int*)status;
     B.tile_loss = tile_loss;
-    cudaMemsetAsync(B.queue, 0, 2 * sizeof(int), st);
-    if (B.base.seg) cudaMemsetAsync(B.base.seg_count, 0, sizeof(int64_t), st);
+    // with segment records the views render in groups (non-decreasing segment_group), one
+    // after the other, each with its own work counters and record counter, reusing the one
+    // record buffer
+    const int n_groups = B.base.seg ? B.views[n_views - 1].seg_group + 1 : 1;
+    cudaMemsetAsync(B.queue, 0, 2 * sizeof(int) * (size_t)n_groups, st);
+    if (B.base.seg) cudaMemsetAsync(B.base.seg_count, 0, sizeof(int64_t) * (size_t)n_groups, st);
     // work list
     uint32_t* k0 = (uint32_t*)(ws + L.k0);
     uint32_t* v0 = (uint32_t*)(ws + L.v0);
@@ -463,11 +477,28 @@ extern "C" int pf_batch_render(const pf_batch_scene* scene, const pf_batch_view*
         uint32_t* kf = radix_final_key_buffer(k0, k1, 24);
         radix_sort_pairs(k0, v0, k1, v1, kf, items, B.n_items, nullptr, 24, rs, st);
     }
+    static BatchParams Bg;  // a group's launch parameters
     int rc = PF_OK;
-    if (B.n_items > 0) {
-        if (tile_width == 8) rc = launch_batch<8>(B, split != 0, st);
-        else if (tile_width == 16) rc = launch_batch<16>(B, split != 0, st);
-        else rc = launch_batch<32>(B, split != 0, st);
+    for (int g = 0, v = 0; g < n_groups && rc == PF_OK; g++) {
+        // a group's items follow each other in both orders (group-major keys, or view order)
+        int64_t first = -1, n = 0;
+        for (; v < n_views && B.views[v].seg_group == g; v++) {
+            if (first < 0) first = B.views[v].item_base;
+            n += B.views[v].T;
+        }
+        if (n == 0) continue;
+        const BatchParams* Bp = &B;
+        if (n_groups > 1) {
+            Bg = B;
+            Bg.items = B.items + first;
+            Bg.n_items = n;
+            Bg.queue = B.queue + 2 * g;
+            Bg.base.seg_count = B.base.seg_count + g;
+            Bp = &Bg;
+        }
+        if (tile_width == 8) rc = launch_batch<8>(*Bp, split != 0, st);
+        else if (tile_width == 16) rc = launch_batch<16>(*Bp, split != 0, st);
+        else rc = launch_batch<32>(*Bp, split != 0, st);
     }
     if (rc != PF_OK) return rc;
     auto sanitize = [&](float* a, size_t n) {

@@ -25,7 +25,7 @@ def test_library_exports_every_declared_symbol():
     lib = _lib.load()
     for s in declared_symbols():
         assert hasattr(lib, s), s
-    assert lib.pf_abi_version() == 3
+    assert lib.pf_abi_version() == 4
     # every binding in the Python layer names a declared symbol
     assert set(_lib.exported_symbols()) <= set(declared_symbols())
 

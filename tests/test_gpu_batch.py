@@ -237,34 +237,39 @@ def test_batch_segment_records_give_the_clipping_adjoint(tw, split):
     pixel's interval and plane result, the adjoint reads them) against the
     one that clips again: the same images and losses, gradients equal up to
     the order of the float atomics; so do a budget that holds the intervals
-    only and a record buffer too small for most pairs (those are clipped
-    again).  check() grows a buffer that a count outran."""
+    only, a record buffer too small for most pairs (those are clipped again),
+    and every view in a record group of its own (the groups render one after
+    the other, reusing the buffer).  check() counts again and grows a buffer
+    that a group's count outran."""
     sc, adj, adj_off, cams, rgbs, targets = make_case(seed=13)
     kw = bind_kwargs(sc, adj, adj_off, rgbs, targets)
     res = []
-    for rec, budget, capacity in ((False, None, 0), (True, None, 0), (True, None, 0.1), (True, "intervals", 0)):
+    for case in ("clip", "records", "small", "intervals", "groups"):
         step = BatchStep("cuda", [torch_cam(c) for c in cams], tile_width=tw, chunk=2, split=split,
-                         record_segments=rec)
+                         record_segments=case != "clip")
         step.bind(**kw)
-        if rec:
-            n_rec = int(step.rec_count.item())
-            assert n_rec > 0 and step.segs is not None
-            if budget == "intervals":
-                step.segment_bytes = 16 * step.rec_capacity
-                step._size_records()
-                assert step.segs[2] is False
-        if capacity:  # a buffer for an eighth of the records
+        if case != "clip":
+            n_rec = sum(step.view_records)
+            assert n_rec > 0 and step.segs is not None and step.segs[2] is True
+            assert step.seg_groups == [0] * len(cams)  # the whole batch fits one group
+        if case == "intervals":
+            step.segment_bytes = 16 * step.rec_capacity
+            step._size_records()
+            assert step.segs[2] is False
+        if case == "small":  # a buffer for an eighth of the records
             step.rec_capacity = max(n_rec // 8, 1)
             step._size_records()
-            assert step.rec_capacity < n_rec
+        if case == "groups":
+            step.seg_groups = list(range(len(cams)))
+            step._size_records()
         loss = step.run().clone()
         res.append((loss, [c.clone() for c in step.color], {k: g.clone() for k, g in step.grads.items()},
                     [g.clone() for g in step.grad_texel_rgb]))
-        if rec and capacity:
-            step.check()  # grows the buffer and drops the graph
-            assert step.rec_capacity >= int(step.rec_count.item())
-        else:
-            step.check()
+        if case == "groups":
+            assert step.rec_count.tolist() == step.view_records  # one counter per group, here per view
+        step.check()
+        if case == "small":  # counted again and grown
+            assert step.rec_capacity >= n_rec and step.graph is None
     loss0, col0, g0, rgb0 = res[0]
     for loss, col, g, rgb in res[1:]:
         assert torch.equal(loss, loss0)
@@ -274,3 +279,21 @@ def test_batch_segment_records_give_the_clipping_adjoint(tw, split):
             assert_close_rel(g[k].cpu().numpy(), g0[k].cpu().numpy(), 1e-5, k)
         for a, b in zip(rgb, rgb0):
             assert_close_rel(a.cpu().numpy(), b.cpu().numpy(), 1e-5, "rgb")
+
+
+def test_batch_record_groups_through_the_c_abi():
+    """Record groups as pf_batch_render takes them: 0 for the first view,
+    then the previous view's group or the next; anything else is refused with
+    PF_ERR_ARGS before any launch."""
+    sc, adj, adj_off, cams, rgbs, targets = make_case(seed=17)
+    step = BatchStep("cuda", [torch_cam(c) for c in cams], tile_width=8)
+    step.bind(**bind_kwargs(sc, adj, adj_off, rgbs, targets))
+    for bad in ([0, 1, 0], [0, 2, 2], [1, 1, 1]):
+        step.seg_groups = bad
+        step._size_records()
+        with pytest.raises(_lib.PfError):
+            step.run()
+    step.seg_groups = [0, 1, 1]
+    step._size_records()
+    step.run()
+    step.check()
