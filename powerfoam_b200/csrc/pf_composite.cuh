@@ -996,6 +996,12 @@ PF_D void bwd_tile(const RasterParams& P, const BwdIn& in, const GradOut& go, in
             }
             st_mask[lane] = m;
             st_off[lane] = off;
+            // the records of a (pair, warp) are one contiguous run, most of them still in DRAM:
+            // fetched into L2 for the whole batch now (staging them one batch ahead, or the
+            // texels too, measured slower)
+            if (m != 0u)
+                prefetch_l2_bulk(P.seg + (int64_t)off * P.seg_stride,
+                                 (uint32_t)__popc(m) * (uint32_t)P.seg_stride * 16u);
             __syncwarp();
         }
         for (int k = k1; k >= 0 && k >= k0; k--) {

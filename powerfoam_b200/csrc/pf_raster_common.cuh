@@ -49,6 +49,13 @@ PF_D void store_plane(float4* slot, const PlaneRes& r) {
 // written by an earlier launch, through L2 (ld.global.cg) when the forward
 // that wrote them runs in the same launch (the read-only path is only valid
 // for data that no thread writes during the launch).
+// Bring `bytes` at `p` into L2 ahead of use (cp.async.bulk.prefetch, no
+// registers written); skipped unless both are 16-byte multiples.
+PF_D void prefetch_l2_bulk(const void* p, uint32_t bytes) {
+    if (bytes != 0u && (((uintptr_t)p | bytes) & 15u) == 0)
+        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
+
 template <bool COH, class T>
 PF_D T seg_load(const T* p) {
     if constexpr (COH) return __ldcg(p);
