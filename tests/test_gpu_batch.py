@@ -297,3 +297,30 @@ def test_batch_record_groups_through_the_c_abi():
     step._size_records()
     step.run()
     step.check()
+
+
+def test_batch_segment_records_with_an_empty_view_and_ragged_tiles():
+    """A view that looks away from the scene (no sphere hits, no records) between
+    two ragged views, every view in a record group of its own and all in one:
+    the same images and gradients as without records."""
+    views = [((0.2, 0.5, 2.3), 61, 37, 55.0), ((0.0, 0.0, 3.0), 23, 19, 40.0), ((1.2, -0.8, 1.9), 45, 27, 50.0)]
+    sc, adj, adj_off, cams, rgbs, targets = make_case(seed=19, views=views)
+    cams[1] = np_camera((0.0, 0.0, 3.0), (0.0, 0.0, 6.0), 23, 19, 40.0)  # facing away
+    kw = bind_kwargs(sc, adj, adj_off, rgbs, targets)
+    res = []
+    for rec, groups in ((False, None), (True, None), (True, [0, 1, 2])):
+        step = BatchStep("cuda", [torch_cam(c) for c in cams], tile_width=8, split=True, record_segments=rec)
+        step.bind(**kw)
+        if rec:
+            assert step.view_records[1] == 0 and step.view_records[0] > 0 and step.view_records[2] > 0
+        if groups:
+            step.seg_groups = groups
+            step._size_records()
+        step.run()
+        step.check()
+        res.append(([c.clone() for c in step.color], {k: g.clone() for k, g in step.grads.items()}))
+    for col, g in res[1:]:
+        for a, b in zip(col, res[0][0]):
+            assert torch.equal(a, b)
+        for k in g:
+            assert_close_rel(g[k].cpu().numpy(), res[0][1][k].cpu().numpy(), 1e-5, k)
