@@ -936,16 +936,21 @@ struct BwdIn {
 // (P.seg_stride == 4).  One pixel per lane only.
 // FB: some (pair, warp) may have no records (the forward found the buffer
 // full) and is clipped here; without FB every hit has its record, and the
-// masks and record offsets of the 32 staged primitives are staged with them
-// (in the stage's face area, which the clipping alone uses).
+// masks, record offsets and neighbour ranges of the 32 staged primitives are
+// staged with them (in the stage's face area, which the clipping alone uses).
 // COH: the records were written earlier in the same launch (a fused
 // forward + adjoint), so they are read through L2, not the read-only path.
 template <int G, int PPL, bool GEN = false, int REC = 0, bool FB = true, bool COH = false>
 PF_D void bwd_tile(const RasterParams& P, const BwdIn& in, const GradOut& go, int64_t tile, int wig, int lane,
                    WarpStage& ws, BwdStage& bs) {
     static_assert(!REC || PPL == 1, "segment records are written by the pair-compacted forward");
+    // without FB the face area (128 words) holds the staged batch's hit masks, record offsets and
+    // neighbour ranges instead
     uint32_t* const st_mask = reinterpret_cast<uint32_t*>(ws.face);
     int32_t* const st_off = reinterpret_cast<int32_t*>(ws.face) + 32;
+    int32_t* const st_a0 = reinterpret_cast<int32_t*>(ws.face) + 64;
+    int32_t* const st_nadj = reinterpret_cast<int32_t*>(ws.face) + 96;
+    static_assert(sizeof(WarpStage::face) >= 128 * sizeof(int32_t), "staging area");
     const int TS = P.TW * P.TW;
     const v3 o = P.cam.eye;
     const float HW = (float)(P.cam.H * P.cam.W);
@@ -999,9 +1004,16 @@ PF_D void bwd_tile(const RasterParams& P, const BwdIn& in, const GradOut& go, in
             // the records of a (pair, warp) are one contiguous run, most of them still in DRAM:
             // fetched into L2 for the whole batch now (staging them one batch ahead, or the
             // texels too, measured slower)
-            if (m != 0u)
+            if (m != 0u) {
                 prefetch_l2_bulk(P.seg + (int64_t)off * P.seg_stride,
                                  (uint32_t)__popc(m) * (uint32_t)P.seg_stride * 16u);
+                // the primitive's neighbour range, so that a live primitive's neighbour staging
+                // below waits on two dependent loads instead of three
+                const int32_t pr = ws.pid[lane];
+                const int32_t q0 = __ldg(&P.adj_off[pr]);
+                st_a0[lane] = q0;
+                st_nadj[lane] = __ldg(&P.adj_off[pr + 1]) - q0;
+            }
             __syncwarp();
         }
         for (int k = k1; k >= 0 && k >= k0; k--) {
@@ -1048,8 +1060,15 @@ PF_D void bwd_tile(const RasterParams& P, const BwdIn& in, const GradOut& go, in
             const float4 n4 = ws.nsg[kk];
             const v3 pn = mk(n4.x, n4.y, n4.z);
             const float sigma = n4.w;
-            const int32_t a0 = __ldg(&P.adj_off[prim]);
-            const int n_adj = __ldg(&P.adj_off[prim + 1]) - a0;
+            int32_t a0;
+            int n_adj;
+            if constexpr (REC && !FB) {
+                a0 = st_a0[kk];
+                n_adj = st_nadj[kk];
+            } else {
+                a0 = __ldg(&P.adj_off[prim]);
+                n_adj = __ldg(&P.adj_off[prim + 1]) - a0;
+            }
             const float cc = dot(center, center), rr = radius * radius;
             if (clip) {
             a.tn_id = a.tn < 1e-8f ? -2 : -1;
