@@ -1114,15 +1114,18 @@ PF_D void bwd_tile(const RasterParams& P, const BwdIn& in, const GradOut& go, in
             // with no such lane left the primitive is done (28 % of the hit
             // primitives at 1M primitives, 1080p).
             if (!__any_sync(0xffffffffu, (a.hit && a.tn < a.tf) || (PPL == 2 && b.hit && b.tn < b.tf))) continue;
-            // neighbour slots used by the face adjoint (read across lanes after
-            // stage_texels' barrier)
+            // the texels and the neighbour slots used by the face adjoint, copied
+            // asynchronously so that the texels' latency hides under the neighbour
+            // ids' and spheres' (read across lanes after the barrier)
+            stage_texels_async(ws, P, prim, lane);
             for (int e = lane; e < min(n_adj, kFaceSlots); e += 32) {
                 int32_t nb = __ldg(&P.adj[a0 + e]);
                 bs.nbr_id[e] = nb;
-                bs.nbr_sph[e] = __ldg(&P.spheres[nb]);
+                cp_async16(&bs.nbr_sph[e], &P.spheres[nb]);
                 bs.face_acc[e] = make_float4(0.f, 0.f, 0.f, 0.f);
             }
-            stage_texels(ws, P, prim, lane);
+            cp_async_wait_all();
+            __syncwarp();
             const float cg = in.g_contrib ? __ldg(&in.g_contrib[prim]) : 0.f;
             bool any_contrib = false;
             float g_c0 = 0.f, g_c1 = 0.f, g_c2 = 0.f, g_r = 0.f, g_n0 = 0.f, g_n1 = 0.f, g_n2 = 0.f, g_s = 0.f;

@@ -151,6 +151,30 @@ PF_D void stage_prims(WarpStage& ws, const RasterParams& P, int64_t start, int k
     __syncwarp();
 }
 
+// Asynchronous global -> shared copies (cp.async, 4 or 16 bytes, aligned to
+// their size); cp_async_wait_all waits for this thread's copies only.
+PF_D void cp_async4(void* smem, const void* gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(s), "l"(gmem) : "memory");
+}
+PF_D void cp_async16(void* smem, const void* gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gmem) : "memory");
+}
+PF_D void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+// stage_texels without waiting: the copies land after cp_async_wait_all and
+// a __syncwarp
+PF_D void stage_texels_async(WarpStage& ws, const RasterParams& P, int32_t prim, int lane) {
+    const int S = P.S;
+    int64_t b3 = (int64_t)prim * S * 3;
+    if (lane < 3 * S) {
+        cp_async4(&ws.ts[lane], &P.sites[b3 + lane]);
+        cp_async4(&ws.tr[lane], &P.rgb[b3 + lane]);
+    }
+    if (lane < S) cp_async4(&ws.th[lane], &P.height[(int64_t)prim * S + lane]);
+}
+
 PF_D void stage_texels(WarpStage& ws, const RasterParams& P, int32_t prim, int lane) {
     const int S = P.S;
     int64_t b3 = (int64_t)prim * S * 3;
