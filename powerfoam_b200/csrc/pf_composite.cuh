@@ -13,6 +13,7 @@ namespace pf {
 
 constexpr int kAccRows = 64;
 constexpr int kFaceSlots = 16;
+static_assert(kFaceSlots <= 32, "one neighbour slot per lane");
 
 // Group layout per tile width: TW = 8 and 16 use one pixel per lane (G = 2
 // and 8 warps per tile), TW = 32 two pixels per lane (G = 16).
@@ -1023,6 +1024,7 @@ PF_D void bwd_tile(const RasterParams& P, const BwdIn& in, const GradOut& go, in
             const float radius = s4.w;
             int64_t rec = -1;  // REC: this lane's record
             bool clip = !REC;  // warp-uniform: clip and evaluate the plane here
+            int32_t nb_pre = 0;  // REC without FB: this lane's neighbour slot id
             if constexpr (REC) {
                 uint32_t m = 0u;
                 int32_t off = -1;
@@ -1037,6 +1039,9 @@ PF_D void bwd_tile(const RasterParams& P, const BwdIn& in, const GradOut& go, in
                     off = st_off[kk];
                 }
                 if (m == 0u) continue;  // no output changes (see forward)
+                if constexpr (!FB) {  // the first neighbour slots' ids, loaded while the record loads
+                    if (lane < min(st_nadj[kk], kFaceSlots)) nb_pre = __ldg(&P.adj[st_a0[kk] + lane]);
+                }
                 if (!FB || off >= 0) {
                     a.hit = (m >> lane) & 1u;
                     if (a.hit) {
@@ -1119,7 +1124,9 @@ PF_D void bwd_tile(const RasterParams& P, const BwdIn& in, const GradOut& go, in
             // ids' and spheres' (read across lanes after the barrier)
             stage_texels_async(ws, P, prim, lane);
             for (int e = lane; e < min(n_adj, kFaceSlots); e += 32) {
-                int32_t nb = __ldg(&P.adj[a0 + e]);
+                int32_t nb;
+                if constexpr (REC && !FB) nb = nb_pre;  // e == lane (kFaceSlots <= 32)
+                else nb = __ldg(&P.adj[a0 + e]);
                 bs.nbr_id[e] = nb;
                 cp_async16(&bs.nbr_sph[e], &P.spheres[nb]);
                 bs.face_acc[e] = make_float4(0.f, 0.f, 0.f, 0.f);
