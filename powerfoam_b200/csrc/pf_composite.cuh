@@ -1119,6 +1119,11 @@ PF_D void bwd_tile(const RasterParams& P, const BwdIn& in, const GradOut& go, in
             // with no such lane left the primitive is done (28 % of the hit
             // primitives at 1M primitives, 1080p).
             if (!__any_sync(0xffffffffu, (a.hit && a.tn < a.tf) || (PPL == 2 && b.hit && b.tn < b.tf))) continue;
+            // the record's plane part, loaded now so that it arrives during the staging below
+            PlaneRes pr_pre;
+            if constexpr (REC == 2 && !FB) {
+                if (a.hit && a.tn < a.tf) pr_pre = load_plane<COH>(P.seg + rec * 4);
+            }
             // the texels and the neighbour slots used by the face adjoint, copied
             // asynchronously so that the texels' latency hides under the neighbour
             // ids' and spheres' (read across lanes after the barrier)
@@ -1147,7 +1152,9 @@ PF_D void bwd_tile(const RasterParams& P, const BwdIn& in, const GradOut& go, in
                     const int _t_near_id = t_near_id, _t_far_id = t_far_id;
                     const v3 xo = ray_org<GEN>(x, o);
                     PlaneRes pr;
-                    if (REC == 2 && !clip)
+                    if (REC == 2 && !FB)
+                        pr = pr_pre;
+                    else if (REC == 2 && !clip)
                         pr = load_plane<COH>(P.seg + rec * 4);
                     else
                         pr = plane_fwd_smem(xo, d, t_near, center, pn, radius, ws, P.S);
