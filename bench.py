@@ -86,7 +86,7 @@ def parse():
 CAPTURES = {
     # the adjoint that reads the forward's segment records (the default)
     ("raster1m", "pf_raster_backward", True): dict(
-        traffic=4.185e9 + 260.91e6, warp_instructions=6_747_949_514,
+        traffic=4.523e9 + 283.23e6, warp_instructions=6_956_738_056,
         source="ncu capture of raster_bwd_kernel<8, 0, 2, false> (the second step's adjoint, `-k regex:raster_ -s 3 "
                "-c 6` on `python bench.py --steps 2 --warmup 1 --no-cpu-baseline`): dram__bytes_read.sum + "
                "dram__bytes_write.sum, smsp__inst_executed.sum"),
