@@ -65,6 +65,9 @@ def parse():
     p.add_argument("--no-segment-records", action="store_true",
                    help="raster and batch workloads: the adjoint clips the sphere intervals again instead of "
                    "reading the forward's segment records (record_segments = False)")
+    p.add_argument("--graph", action="store_true",
+                   help="raster workloads, one GPU: time the step as CUDA graph replays (the sync-free step is "
+                   "captured whole) instead of eager calls")
     p.add_argument("--host-sync", action="store_true",
                    help="raster workloads: Rasterizer(host_sync=True), the reference's host read of the pair count "
                    "per call; by default the step runs sync-free (host_sync=False: the host queues steps ahead "
@@ -1201,8 +1204,34 @@ def main():
     for _ in range(max(args.warmup, 3)):
         step()
     barrier()
+    # --graph: the whole step (colour pre-step, binning, forward, loss, adjoint) captured in
+    # CUDA graphs, one per target buffer of the end-to-end loop; graph 0 reads the resident
+    # target.  Possible because the step runs sync-free (nothing is read back per call).
+    t_dev = [target_dev, torch.empty_like(target_dev)]
+    graphs = None
+    if args.graph:
+        if world > 1 or args.host_sync:
+            raise SystemExit("--graph: one GPU and the sync-free step only")
+        t_dev[1].copy_(target_dev)
+        side = torch.cuda.Stream()
+        side.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(side):
+            for _ in range(2):
+                step(t_dev[0])
+                step(t_dev[1])
+        torch.cuda.current_stream().wait_stream(side)
+        graphs = []
+        for b in range(2):
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(g):
+                lo = step(t_dev[b])
+            graphs.append((g, lo))
+        for _ in range(max(args.warmup, 3)):
+            graphs[0][0].replay()
+        barrier()
 
-    # per-call device times of the compositing kernels, recorded live
+    # per-call device times of the compositing kernels, recorded live (eagerly after the
+    # timed loop when it replays graphs)
     events = {"pf_raster_forward": [], "pf_raster_backward": []}
     pending = {}
 
@@ -1218,16 +1247,25 @@ def main():
     clocks.start()
     time.sleep(0.3)
     barrier()
-    rasterize.PROFILE_HOOK = hook
+    rasterize.PROFILE_HOOK = None if graphs else hook
     start = torch.cuda.Event(enable_timing=True)
     end = torch.cuda.Event(enable_timing=True)
     start.record()
     for _ in range(args.steps):
-        loss = step()
+        if graphs:
+            graphs[0][0].replay()
+        else:
+            loss = step()
     end.record()
     barrier()
     rasterize.PROFILE_HOOK = None
     clk = clocks.stop()
+    if graphs:
+        rasterize.PROFILE_HOOK = hook
+        for _ in range(3):
+            step()
+        barrier()
+        rasterize.PROFILE_HOOK = None
     ms = start.elapsed_time(end) / args.steps
     if world > 1:
         ms = max_over_ranks(ms, dev)
@@ -1242,7 +1280,6 @@ def main():
     # loss that read it.
     target_host = target.pin_memory()
     loss_host = torch.empty(args.steps, dtype=torch.float32).pin_memory()
-    t_dev = [torch.empty_like(target_dev) for _ in range(2)]
     copy_stream = torch.cuda.Stream()
     ready = [torch.cuda.Event() for _ in range(2)]
     consumed = [torch.cuda.Event() for _ in range(2)]
@@ -1256,7 +1293,12 @@ def main():
         with torch.cuda.stream(copy_stream):
             t_dev[b].copy_(target_host, non_blocking=True)
             ready[b].record(copy_stream)
-        loss = step(t_dev[b], ready[b])
+        if graphs:  # the upload ran during the previous step's replay
+            torch.cuda.current_stream().wait_event(ready[b])
+            graphs[b][0].replay()
+            loss = graphs[b][1]
+        else:
+            loss = step(t_dev[b], ready[b])
         consumed[b].record()
         loss_host[i].copy_(loss.detach(), non_blocking=True)
     e1.record()
@@ -1285,6 +1327,7 @@ def main():
                 config=dict(workload=args.workload, prims=cfg["n"], width=cfg["width"], height=cfg["height"],
                             tile=args.tile, vfov=cfg["vfov"], pairs=st["pairs"], visited_pairs=st["V"],
                             l2="inputs larger than L2 (256 MB of primitive records), no flush",
+                            step_mode="CUDA graph replays" if graphs else "eager calls, sync-free",
                             parallelism=f"view-dp{world}"),
                 clocks=clk,
                 e2e=dict(value=world * 1000.0 / e2e_ms, unit=UNIT, h2d_bytes_per_step=target.numel() * 4,

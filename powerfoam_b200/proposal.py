@@ -121,18 +121,20 @@ class ProposalNet:
         self.check()
         return history
 
-    def calibrate(self, rays8, max_unsafe=0, floor=0.9, max_unsafe_frac=0.0):
+    def calibrate(self, rays8, max_unsafe=0, floor=0.9, max_unsafe_frac=0.0, t_slack=0.0):
         """Confidence threshold from held-out labelled rays (n, 8): the plain
         walk judges each seed, and the threshold sits just above the
         confidence of the (k + 1)-th most confident seed that would have
         started past its first significant cell, k = max(max_unsafe,
         max_unsafe_frac * n) (never below `floor`; rays flagged as never
-        reaching one are safe anywhere)."""
+        reaching one are safe anywhere).  t_slack > 0 counts a seed as unsafe
+        already when it starts within t_slack of that cell: a more
+        conservative gate for rays unlike the held-out ones."""
         rays8 = rays8.to(torch.float32).contiguous()
         t, c = self.forward(rays=rays8[:, :6].contiguous())
         lab = rays8[:, 6]
         # a ray flagged as never reaching a significant cell is safe wherever it is seeded
-        unsafe = (lab >= 0) & (rays8[:, 7] == 0) & (t - self.margin > lab)
+        unsafe = (lab >= 0) & (rays8[:, 7] == 0) & (t - self.margin + float(t_slack) > lab)
         k = max(int(max_unsafe), int(max_unsafe_frac * rays8.shape[0]))
         cu = torch.sort(c[unsafe], descending=True).values
         thr = float(cu[k]) if cu.numel() > k else 0.0

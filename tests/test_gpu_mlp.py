@@ -274,9 +274,10 @@ def test_trained_proposal_seeds_at_50db():
     # the entry-distance loss falls; the confidence targets move with the predictions (a seed's
     # safety depends on the predicted t), so that loss is only required to be well below chance (ln 2)
     assert hist[-1][0] < hist[0][0] and hist[-1][1] < 0.3
-    # strict gate: no held-out seed past its first significant cell (a budget of 1e-4 of the
-    # held-out rays let eval views drop below 50 dB)
-    thr = net.calibrate(val)
+    # strict gate: no held-out seed past its first significant cell, nor within one margin of it
+    # (a budget of 1e-4 of the held-out rays, or the gate without that slack, let eval views drop
+    # below 50 dB: training differs from run to run in the order of its float atomics)
+    thr = net.calibrate(val, t_slack=net.margin)
     print(f"calibrated threshold {thr:.5f}: {net.seed_fraction(val, thr):.3f} of the held-out rays seeded")
     seeded_tr = SeededTracer(tr, net, sc["points"], sc["radii"], conf_threshold=thr, adjacency=adj,
                              adjacency_offsets=off)
