@@ -908,7 +908,10 @@ trace_bwd_walk_kernel(TraceParams P, SegWs W) {
 // without a block launched for every index up to kb.
 constexpr int kSegStride = 8;
 
-__global__ void __launch_bounds__(128)
+// 6 resident blocks (80 registers, some spilled): the launch waits mostly on its
+// record and texel loads, and 4 blocks at 125 registers left too few warps to hide
+// them (trace1m: 7.19 -> 7.14 ms per step; 8 blocks at 64 registers: 7.48 ms)
+__global__ void __launch_bounds__(128, 6)
 trace_bwd_segment_kernel(TraceParams P, SegWs W, TraceAdjIn A, TraceGrads G) {
     const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (tid >= W.n) return;
