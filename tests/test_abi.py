@@ -68,3 +68,37 @@ def test_trace_backward_workspace_size_without_a_gpu():
         assert lib.pf_trace_backward_workspace_size(ctypes.byref(inp), kb, ctypes.byref(n)) == _lib.PF_ERR_ARGS
     inp.cam.width = 0
     assert lib.pf_trace_backward_workspace_size(ctypes.byref(inp), 4, ctypes.byref(n)) == _lib.PF_ERR_ARGS
+
+
+def test_struct_layouts_match_the_header(tmp_path):
+    """Every ctypes mirror in the Python layer has the C struct's size and
+    field offsets (a C program compiled against include/pfoam.h prints them)."""
+    import shutil
+    import subprocess
+
+    import pytest
+
+    from powerfoam_b200 import _lib
+
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    mirrors = {"pf_camera": _lib.PfCamera, "pf_raster_inputs": _lib.PfRasterInputs,
+               "pf_trace_inputs": _lib.PfTraceInputs, "pf_batch_scene": _lib.PfBatchScene,
+               "pf_batch_view": _lib.PfBatchView, "pf_batch_schedule": _lib.PfBatchSchedule}
+    lines = ["#include <stdio.h>", "#include <stddef.h>", '#include "pfoam.h"', "int main(void) {"]
+    for cname, py in mirrors.items():
+        lines.append(f'    printf("{cname} sizeof %zu\\n", sizeof({cname}));')
+        for fname, _ in py._fields_:
+            lines.append(f'    printf("{cname} {fname} %zu\\n", offsetof({cname}, {fname}));')
+    lines += ["    return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    subprocess.run([cc, "-std=c11", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split("\n")
+    got = {tuple(l.split()[:2]): int(l.split()[2]) for l in out if l.strip()}
+    for cname, py in mirrors.items():
+        assert got[(cname, "sizeof")] == ctypes.sizeof(py), cname
+        for fname, _ in py._fields_:
+            assert got[(cname, fname)] == getattr(py, fname).offset, (cname, fname)
