@@ -839,6 +839,10 @@ PF_D void ray_plane_bwd_d(v3 eye, v3 dir, v3 p, v3 n, float h, v3& dtdp, v3& dtd
 }
 
 // texture.py:74-186, accumulating into this lane's column of bs.acc
+// ASSIGN: the gradient table's rows are still zero for this lane (one pixel
+// per lane: the first pass writes each colour and site row at most once), so
+// they are stored instead of read, added and stored.
+template <bool ASSIGN = false>
 PF_D void plane_bwd_acc(v3 o, v3 d, float _t_near, v3 po, v3 pn, float radius, const WarpStage& ws, int S,
                         const PlaneRes& pr, v3 dLdrgb_in, float dLdt_surf_in, BwdStage& bs, int lane, v3& dLdpo_out,
                         v3& dLdpn_out, float& dLd_t_near_out) {
@@ -860,14 +864,23 @@ PF_D void plane_bwd_acc(v3 o, v3 d, float _t_near, v3 po, v3 pn, float radius, c
         if (!(w / weight_sum < 1e-3f)) {
             v3 dwds = ((2.0f * kTemp * w) * inv_rr) * df;
             v3 rgb_grad = w * rgb_scale;
-            bs.acc[32 + 3 * i][lane] += rgb_grad.x;
-            bs.acc[33 + 3 * i][lane] += rgb_grad.y;
-            bs.acc[34 + 3 * i][lane] += rgb_grad.z;
             float grad_dp = dot(dLdrgb_in, mk(ws.tr[3 * i], ws.tr[3 * i + 1], ws.tr[3 * i + 2]));
             v3 site_grad = ((grad_dp - grad_dp_in) * inv_ws) * dwds;
-            bs.acc[8 + 3 * i][lane] += site_grad.x;
-            bs.acc[9 + 3 * i][lane] += site_grad.y;
-            bs.acc[10 + 3 * i][lane] += site_grad.z;
+            if constexpr (ASSIGN) {
+                bs.acc[32 + 3 * i][lane] = rgb_grad.x;
+                bs.acc[33 + 3 * i][lane] = rgb_grad.y;
+                bs.acc[34 + 3 * i][lane] = rgb_grad.z;
+                bs.acc[8 + 3 * i][lane] = site_grad.x;
+                bs.acc[9 + 3 * i][lane] = site_grad.y;
+                bs.acc[10 + 3 * i][lane] = site_grad.z;
+            } else {
+                bs.acc[32 + 3 * i][lane] += rgb_grad.x;
+                bs.acc[33 + 3 * i][lane] += rgb_grad.y;
+                bs.acc[34 + 3 * i][lane] += rgb_grad.z;
+                bs.acc[8 + 3 * i][lane] += site_grad.x;
+                bs.acc[9 + 3 * i][lane] += site_grad.y;
+                bs.acc[10 + 3 * i][lane] += site_grad.z;
+            }
             dLdpt = dLdpt - site_grad;
         }
     }
@@ -1208,7 +1221,7 @@ PF_D void bwd_tile(const RasterParams& P, const BwdIn& in, const GradOut& go, in
                         else dLdt_surf = 0.0f;
                         v3 _dc, _dn;
                         float dLd_t_near;
-                        plane_bwd_acc(xo, d, _t_near, center, pn, radius, ws, P.S, pr, dLdcolor, dLdt_surf, bs, lane,
+                        plane_bwd_acc<PPL == 1>(xo, d, _t_near, center, pn, radius, ws, P.S, pr, dLdcolor, dLdt_surf, bs, lane,
                                       _dc, _dn, dLd_t_near);
                         dLdcenter = dLdcenter + _dc;
                         dLdnormal = dLdnormal + _dn;
@@ -1266,14 +1279,14 @@ PF_D void bwd_tile(const RasterParams& P, const BwdIn& in, const GradOut& go, in
                 if (PPL == 2) swap_pix(a, b);
             }
             if (__any_sync(0xffffffffu, any_contrib)) {
-                bs.acc[0][lane] += g_c0;
-                bs.acc[1][lane] += g_c1;
-                bs.acc[2][lane] += g_c2;
-                bs.acc[3][lane] += g_r;
-                bs.acc[4][lane] += g_n0;
-                bs.acc[5][lane] += g_n1;
-                bs.acc[6][lane] += g_n2;
-                bs.acc[7][lane] += g_s;
+                bs.acc[0][lane] = g_c0;  // rows 0-7 are written once per primitive (zero before)
+                bs.acc[1][lane] = g_c1;
+                bs.acc[2][lane] = g_c2;
+                bs.acc[3][lane] = g_r;
+                bs.acc[4][lane] = g_n0;
+                bs.acc[5][lane] = g_n1;
+                bs.acc[6][lane] = g_n2;
+                bs.acc[7][lane] = g_s;
                 __syncwarp();
                 // sum rows 2l, 2l+1 over the 32 columns, four at a time (128-bit
                 // accesses rotated by lane: each 8-lane phase hits distinct banks),
