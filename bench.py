@@ -91,8 +91,9 @@ CAPTURES = {
     ("raster1m", "pf_raster_backward", True): dict(
         traffic=4.523e9 + 283.23e6, warp_instructions=6_956_738_056,
         source="ncu capture of raster_bwd_kernel<8, 0, 2, false> (the second step's adjoint, `-k regex:raster_ -s 3 "
-               "-c 6` on `python bench.py --steps 2 --warmup 1 --no-cpu-baseline`): dram__bytes_read.sum + "
-               "dram__bytes_write.sum, smsp__inst_executed.sum"),
+               "-c 6` on `python bench.py --steps 2 --warmup 1 --no-cpu-baseline`), on the build before the "
+               "adjoint stored its first gradient-table writes (which removed shared-memory loads, so the current "
+               "launch issues fewer): dram__bytes_read.sum + dram__bytes_write.sum, smsp__inst_executed.sum"),
     # the adjoint that clips again (--no-segment-records)
     ("raster1m", "pf_raster_backward", False): dict(
         traffic=816.77e6 + 206.06e6, warp_instructions=11_715_679_565,
