@@ -102,3 +102,45 @@ def test_struct_layouts_match_the_header(tmp_path):
         assert got[(cname, "sizeof")] == ctypes.sizeof(py), cname
         for fname, _ in py._fields_:
             assert got[(cname, fname)] == getattr(py, fname).offset, (cname, fname)
+
+
+def test_batch_argument_checks_without_a_gpu():
+    """pf_batch_render checks its scene and views before any CUDA call:
+    record groups must start at 0 and grow by at most one per view, the
+    segment buffer must be 16-byte aligned and its capacity below 2^31.
+    (The pointers below are placeholders: nothing dereferences them.)"""
+    from powerfoam_b200 import _lib
+
+    lib = _lib.load()
+    fake = 1 << 20  # a 16-byte-aligned placeholder address
+
+    def make(groups, segments=fake, capacity=1024):
+        sc = _lib.PfBatchScene()
+        sc.n_sites, sc.n_prims = 8, 16
+        for f in ("spheres", "nsigmas", "texel_sites", "texel_height", "adjacency", "adjacency_offsets",
+                  "adjacency_diff", "segment_masks", "segment_offsets", "segment_count"):
+            setattr(sc, f, fake)
+        sc.segments, sc.segment_capacity, sc.segment_planes = segments, capacity, 1
+        views = (_lib.PfBatchView * len(groups))()
+        for v, g in enumerate(groups):
+            w = views[v]
+            w.cam.width, w.cam.height = 24, 16
+            for f in ("tile_offsets", "tile_prims", "texel_rgb", "target", "color", "log_t", "normal_distance",
+                      "normal", "grad_color", "contrib", "early_stop", "tile_contrib_pairs", "grad_texel_rgb"):
+                setattr(w, f, fake)
+            w.segment_pair_base, w.segment_pairs, w.segment_group = 64 * v, 64, g
+        return sc, views
+
+    def render(sc, views):
+        return lib.pf_batch_render(ctypes.byref(sc), views, len(views), 8, 1, 0, 0, None, 0, None, None, None, None,
+                                   None, None, None, None, None)
+
+    for groups in ([0, 2, 2], [1, 1, 1], [0, 1, 0]):
+        assert render(*make(groups)) == _lib.PF_ERR_ARGS
+        assert b"segment groups" in lib.pf_last_error()
+    assert render(*make([0, 0, 1], segments=fake + 4)) == _lib.PF_ERR_ARGS
+    assert b"16-byte alignment" in lib.pf_last_error()
+    assert render(*make([0, 0, 1], capacity=1 << 31)) == _lib.PF_ERR_ARGS
+    # well-formed views pass the checks and stop at the missing workspace and outputs
+    assert render(*make([0, 1, 1])) == _lib.PF_ERR_ARGS
+    assert b"missing argument" in lib.pf_last_error()
