@@ -144,3 +144,33 @@ def test_batch_argument_checks_without_a_gpu():
     # well-formed views pass the checks and stop at the missing workspace and outputs
     assert render(*make([0, 1, 1])) == _lib.PF_ERR_ARGS
     assert b"missing argument" in lib.pf_last_error()
+
+
+def test_raster_segment_argument_checks_without_a_gpu():
+    """pf_raster_forward refuses segment records without masks, offsets or a
+    counter, off 16-byte alignment, with a capacity of 2^31 or more, or at
+    tile width 32, before any CUDA call (placeholder pointers, never
+    dereferenced)."""
+    from powerfoam_b200 import _lib
+
+    lib = _lib.load()
+    fake = 1 << 20
+
+    def inputs(**over):
+        inp = _lib.PfRasterInputs()
+        inp.cam.width, inp.cam.height = 24, 16
+        inp.tile_width, inp.n_sites, inp.n_prims = 8, 8, 16
+        for f in ("spheres", "nsigmas", "texel_sites", "texel_rgb", "texel_height", "adjacency",
+                  "adjacency_offsets", "adjacency_diff", "tile_offsets", "tile_prims", "segments", "segment_masks",
+                  "segment_offsets", "segment_count"):
+            setattr(inp, f, fake)
+        inp.segment_pairs, inp.segment_capacity, inp.segment_planes = 64, 1024, 1
+        for k, v in over.items():
+            setattr(inp, k, v)
+        return inp
+
+    for over in (dict(segment_masks=None), dict(segment_count=None), dict(segments=fake + 8),
+                 dict(segment_capacity=1 << 31), dict(segment_capacity=-1), dict(tile_width=32)):
+        inp = inputs(**over)
+        assert lib.pf_raster_forward(ctypes.byref(inp), 0, *([None] * 11)) == _lib.PF_ERR_ARGS, over
+        assert b"segment" in lib.pf_last_error(), over
